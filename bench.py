@@ -1,0 +1,336 @@
+#!/usr/bin/env python
+"""Benchmark: Mrays/s of the geodesic spectral ray tracer on B200.
+
+A "step" is one render of the workload (default: the Kerr a=0.9 thin-disk scene
+at 1024^2, 64 spectral bins, tolerance 1e-8) on each GPU. Multi-GPU runs are
+weak-scaled: every rank renders its own frame (rays are independent; there is
+no data-path collective), and the value is all ranks' rays / max-over-ranks
+device time.
+
+`--impl reference` times the reference's CPU algorithm instead: the FP64 C++
+restatement of the reference's CPU integrator (the reference is Julia, which
+is not installed), on the host's cores, on a bounded pixel sample.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Mrays/s Kerr 1024² at ≤1e-3 rel err: FP32-mixed vs FP64 on 1 B200; adjoint grad/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="kerr_thin_disk")
+    ap.add_argument("--x-pix", type=int, default=1024)
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--no-fp64-leg", action="store_true", help="skip the FP64 comparison leg")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample", type=int, default=2048, help="rays in the CPU baseline sample")
+    ap.add_argument("--block-warps", type=int, default=0)
+    ap.add_argument("--ctas-per-sm", type=int, default=0)
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing
+# ---------------------------------------------------------------------------
+def dist_init(n):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def all_max(v, world):
+    if world <= 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(v)], device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------
+# clocks
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index=0):
+        self.index = index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                for line in out.stdout.strip().splitlines():
+                    self.rows.append([c.strip() for c in line.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for i, n in enumerate(names):
+                if len(r) > 5 + i and r[5 + i].lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+# ---------------------------------------------------------------------------
+# the CPU legs (oracle restatement of the reference's CPU integrator)
+# ---------------------------------------------------------------------------
+def cpu_sample_ids(P, n):
+    n = min(n, P)
+    return np.unique(np.linspace(0, P - 1, n).round().astype(np.int64))
+
+
+def cpu_time(scene, cam, colors, n, threads=0):
+    from oracle import oracle as O
+    O.build()
+    P = cam.x_pix * cam.y_pix
+    ids = cpu_sample_ids(P, n)
+    t = time.perf_counter()
+    O.render(scene, cam, colors, pixel_ids=ids, threads=threads, want=("xyz", "class", "steps"))
+    dt = time.perf_counter() - t
+    cores = threads if threads > 0 else (os.cpu_count() or 1)
+    return ids.size / dt / 1e6, ids.size, dt, cores
+
+
+def run_reference(args):
+    """--impl reference: the reference's CPU algorithm (oracle port), rank 0 only."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from rtwca_b200 import configs
+    scene, cam, colors = configs.workload(args.workload, x_pix=args.x_pix)
+    for _ in range(args.warmup):
+        cpu_time(scene, cam, colors, max(64, args.cpu_sample // 8))
+    vals = []
+    t_all = 0.0
+    for _ in range(args.steps):
+        v, n, dt, cores = cpu_time(scene, cam, colors, args.cpu_sample)
+        vals.append(v)
+        t_all += dt
+    value = float(np.mean(vals))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_all / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{args.workload} {args.x_pix}x{cam.y_pix}, 64 bins, tol {cam.tolerance:g}",
+                   "sample_rays_per_step": n},
+        "cpu_baseline": {"value": value, "unit": "Mrays/s", "cores": cores, "kind": "port",
+                         "sample": f"{n} evenly spaced pixels of the {args.x_pix}^2 frame per step, "
+                                   "C++ FP64 restatement of the reference's CPU integrator, OpenMP"},
+        "e2e": {"value": value, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# the B200 arm
+# ---------------------------------------------------------------------------
+def op_model(renderer, scene_kind, stats, n_bins):
+    """Algorithmic FP operations of one render from the library's own operation
+    counts (rtw_op_counts) and the render's counters."""
+    oc = renderer.op_counts(scene_kind)
+    att = stats["step_attempts"]
+    emit_att = stats["emitting_steps"]
+    spec = stats["spectral_steps"]
+    # 6 right-hand sides per attempt (k1 is carried); emitting attempts are
+    # counted as emitting in all 6 stages (an upper bound of that share)
+    flops = (att * (6 * oc["rhs_vacuum"] + oc["step_overhead"]) + emit_att * 6 * (oc["rhs_emit"] - oc["rhs_vacuum"])
+             + spec * n_bins * oc["bin_step"])
+    mufu = (att * (6 * oc["rhs_vacuum_mufu"] + oc["step_overhead_mufu"])
+            + emit_att * 6 * (oc["rhs_emit_mufu"] - oc["rhs_vacuum_mufu"]) + spec * n_bins * oc["bin_step_mufu"])
+    return flops, mufu, oc
+
+
+def run_b200(args):
+    import torch
+    from rtwca_b200 import Renderer, abi, configs
+
+    rank, world, local = dist_init(args.gpus)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    scene, cam, colors = configs.workload(args.workload, x_pix=args.x_pix)
+    P = cam.x_pix * cam.y_pix
+    N = len(colors)
+    prec = abi.PREC_MIXED if args.precision == "mixed" else abi.PREC_FP64
+    r = Renderer(local)
+    stream = torch.cuda.current_stream(dev)
+    # device outputs (inputs are the camera descriptors, uploaded by every render)
+    xyz = torch.empty((P, 3), dtype=torch.float32, device=dev)
+    cls = torch.empty(P, dtype=torch.uint8, device=dev)
+    steps = torch.empty(P, dtype=torch.int32, device=dev)
+    out = abi.Outputs()
+    out.xyz, out.term_class, out.steps, out.on_device = xyz.data_ptr(), cls.data_ptr(), steps.data_ptr(), 1
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
+
+    def params(p):
+        return r.params(colors, precision=p, stream=stream.cuda_stream, block_warps=args.block_warps,
+                        ctas_per_sm=args.ctas_per_sm)
+
+    def timed_renders(p, k, w):
+        prm = params(p)
+        for _ in range(w):
+            r.render_raw(scene, [cam], prm, out)
+        torch.cuda.synchronize()
+        barrier(world)
+        torch.cuda.synchronize()
+        total = 0.0
+        kernel = 0.0
+        st = None
+        for _ in range(k):
+            flush.fill_(1.0)  # evict L2 between timed renders
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            r.render_raw(scene, [cam], prm, out)
+            e1.record(stream)
+            e1.synchronize()
+            total += e0.elapsed_time(e1)
+            st = r.stats()
+            kernel += st["kernel_ms"]
+        torch.cuda.synchronize()
+        barrier(world)
+        return total, kernel, st
+
+    peaks = r.measure_peaks() if rank == 0 else None
+    with ClockSampler(local) as clk:
+        total_ms, kernel_ms, st = timed_renders(prec, args.steps, args.warmup)
+    total_ms = all_max(total_ms, world)
+    value = world * P * args.steps / (total_ms * 1e-3) / 1e6
+    ms_per_step = total_ms / args.steps
+
+    # FP64 comparison leg (same workload, same timing rules)
+    fp64 = None
+    if not args.no_fp64_leg and prec == abi.PREC_MIXED:
+        t64, _, st64 = timed_renders(abi.PREC_FP64, max(1, args.steps // 2), 1)
+        t64 = all_max(t64, world)
+        fp64 = {"value": world * P * max(1, args.steps // 2) / (t64 * 1e-3) / 1e6,
+                "ms_per_step": t64 / max(1, args.steps // 2)}
+
+    # end to end through the public API: host pinned outputs, synchronous call
+    hx = torch.empty((P, 3), dtype=torch.float32, pin_memory=True)
+    hc = torch.empty(P, dtype=torch.uint8, pin_memory=True)
+    hs = torch.empty(P, dtype=torch.int32, pin_memory=True)
+    hout = abi.Outputs()
+    hout.xyz, hout.term_class, hout.steps, hout.on_device = hx.data_ptr(), hc.data_ptr(), hs.data_ptr(), 0
+    prm = r.params(colors, precision=prec, block_warps=args.block_warps, ctas_per_sm=args.ctas_per_sm)
+    r.render_raw(scene, [cam], prm, hout)
+    barrier(world)
+    e2e_ms = 0.0
+    ke = max(1, args.steps // 2)
+    for _ in range(ke):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        r.render_raw(scene, [cam], prm, hout)   # synchronous: H2D frames/bins, kernel, D2H outputs
+        e2e_ms += r.stats()["total_ms"]
+    e2e_ms = all_max(e2e_ms, world)
+    e2e_val = world * P * ke / (e2e_ms * 1e-3) / 1e6
+    h2d = 8 * 4 * 128 + 256  # bins table + one frame descriptor
+    d2h = P * (12 + 1 + 4)
+
+    if rank == 0:
+        flops, mufu, oc = op_model(r, scene.kind, st, N)
+        kms = kernel_ms / args.steps
+        achieved = flops / (kms * 1e-3) / 1e12
+        peak = peaks["fp32_flops"] / 1e12 if prec == abi.PREC_MIXED else peaks["fp64_flops"] / 1e12
+        cpu = None
+        if not args.no_cpu_baseline:
+            v, n, dt, cores = cpu_time(scene, cam, colors, args.cpu_sample)
+            cpu = {"value": v, "unit": "Mrays/s", "cores": cores, "kind": "port",
+                   "sample": f"{n} evenly spaced pixels of the {args.x_pix}^2 frame ({dt:.1f} s), C++ FP64 "
+                             "restatement of the reference's CPU integrator, OpenMP"}
+        line = {
+            "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64" if prec == abi.PREC_MIXED else "f64", "data": "synthetic",
+            "config": {"workload": f"{args.workload} {cam.x_pix}x{cam.y_pix}, 64 bins, tol {cam.tolerance:g}, "
+                                   f"{'FP32-mixed' if prec == abi.PREC_MIXED else 'FP64'}",
+                       "rays_per_gpu": P, "parallelism": f"weak x{world} (one frame per GPU)",
+                       "l2": "flushed (256 MB write) between timed renders"},
+            "fp64": fp64,
+            "roofline": {"bound": "fp32" if prec == abi.PREC_MIXED else "fp64", "achieved": achieved, "peak": peak,
+                         "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                         "peak_source": "measured in-run FMA microbenchmark (rtw_measure_peaks)",
+                         "mufu_gops": mufu / (kms * 1e-3) / 1e9,
+                         "mufu_peak_gops": peaks["mufu_ops"] / 1e9},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_val, "unit": "Mrays/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": args.steps,
+            "clocks": clk.summary(),
+            "counters": {k: st[k] for k in ("step_attempts", "rejected_steps", "promoted_steps", "spectral_steps",
+                                            "emitting_steps", "escape_substeps", "nan_rays")},
+        }
+        print(json.dumps(line), flush=True)
+    r.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

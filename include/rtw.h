@@ -1,0 +1,263 @@
+/*
+ * rtw.h - C ABI of librtw_b200.so, the B200 geodesic spectral ray tracer.
+ *
+ * The library integrates camera rays backwards through a curved spacetime
+ * with an adaptive Dormand-Prince RK45 step loop, co-integrating the
+ * "slow-light" radiative transfer (invariant intensity I_nu/nu^3 and optical
+ * depth tau_nu per spectral bin), and reduces each ray's spectrum to linear
+ * CIE XYZ. It is a drop-in for the integrator behind the reference's render
+ * call:
+ *
+ *   gen_image(; camera_pos, camera_dir, speed, camera_point, x_pix, max_steps,
+ *              colors, returnrays, tolerance, max_dt_scale, fov_hor, fov_vert,
+ *              print_num_pix, ray_bundles)
+ *     main/Iterators/LttM/LttM.jl:104-209 (CPU), main/Iterators/5P/5P.jl:135-282 (GPU)
+ *
+ * and for the per-scene ".source" plugin contract (metric, Christoffel
+ * symbols, singularity guards, emitter, step cap, termination), e.g.
+ *   main/Kerr.source/source_geometry.jl:55-315, main/Kerr.source/source_model.jl:9-189.
+ *
+ * Every entry point takes plain pointers and sizes; no C++ or torch types
+ * cross this boundary. All functions return rtw_status and never abort the
+ * process; the text of the last error of a context is in rtw_last_error().
+ */
+#ifndef RTW_H
+#define RTW_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RTW_ABI_VERSION 1
+/* Largest number of spectral bins (reference `colors`) one render takes. */
+#define RTW_MAX_BINS 128
+/* Largest number of frames (cameras) one batched render takes. */
+#define RTW_MAX_FRAMES 4096
+
+typedef enum rtw_status {
+    RTW_OK = 0,
+    RTW_ERR_INVALID_CAMERA = 1, /* camera on a coordinate singularity
+                                   (reference: is_singularity, 5P.jl:140-143) */
+    RTW_ERR_INVALID_PARAM = 2,  /* a size, pointer or parameter out of range   */
+    RTW_ERR_CUDA = 3,           /* a CUDA runtime call failed                  */
+    RTW_ERR_ITER_LIMIT = 4,     /* a device loop hit its iteration cap         */
+    RTW_ERR_NAN = 5,            /* non-finite values in the initial data       */
+    RTW_ERR_NO_DEVICE = 6,      /* no CUDA device / wrong architecture         */
+    RTW_ERR_UNSUPPORTED = 7,    /* feature not built (e.g. ray bundles)        */
+    RTW_ERR_OOM = 8             /* device allocation failed                    */
+} rtw_status;
+
+/* Scene kinds: the ".source" folders of the reference that are on the hot path,
+ * with their constants turned into runtime parameters (rtw_scene). */
+typedef enum rtw_scene_kind {
+    /* Minkowski_Sphere_Spherical.source: flat space in (t,r,theta,phi),
+       emitting sphere r <= r_out. */
+    RTW_SCENE_MINKOWSKI_SPHERE = 0,
+    /* Schwarzschild_Simple_Disk_Spherical.source: wedge disk
+       r_in <= r <= r_out, theta_lo <= theta <= theta_hi. */
+    RTW_SCENE_SCHWARZSCHILD_DISK = 1,
+    /* Kerr.source (Boyer-Lindquist): wedge disk with Keplerian emitter,
+       ZAMO outside it; spin is a runtime value. */
+    RTW_SCENE_KERR_DISK = 2,
+    /* Kerr with a thickened, optically thin disk: rho = (r/r0)^-2
+       exp(-z^2 / 2 (h r)^2), alpha = a_nu * rho, j = alpha B_nu(T),
+       T = temperature (r/r0)^t_index, for r_in <= r <= r_out. */
+    RTW_SCENE_KERR_THICK_DISK = 3
+} rtw_scene_kind;
+
+/* How a ray ended. The reference's calc_terminate (e.g. Kerr.source/
+ * source_model.jl:168-182) returns only a Bool; the class is the first of its
+ * predicates that holds, in the reference's order. */
+typedef enum rtw_term_class {
+    RTW_CLASS_NONE = 0,     /* not traced                                       */
+    RTW_CLASS_ESCAPE = 1,   /* r > escape_radius                                */
+    RTW_CLASS_HORIZON = 2,  /* r <= (1 + 10 tol) r_horizon                      */
+    RTW_CLASS_THICK = 3,    /* every tau slot >= -log(tol): hit disk / body      */
+    RTW_CLASS_WINDING = 4,  /* phi > winding_limit (8 pi)                       */
+    RTW_CLASS_MAXSTEPS = 5, /* step_count >= max_steps (checked first)          */
+    RTW_CLASS_NAN = 6       /* the final geodesic state is not finite           */
+} rtw_term_class;
+
+typedef enum rtw_precision {
+    RTW_PREC_FP64 = 0,  /* every stage, RHS and RT update in FP64             */
+    RTW_PREC_MIXED = 1  /* FP64 state + controller, FP32 stages/RHS/RT with
+                           Kahan-compensated intensities, per-ray FP64 stages
+                           near the horizon and the polar axis               */
+} rtw_precision;
+
+typedef enum rtw_integrator {
+    /* Reference semantics (integrators_LttM.jl:147-150,199,219): the next
+       step's k1 is the weighted average slope sum(b_i k_i), not f(y). */
+    RTW_DP45_REF_COMPAT = 0,
+    /* Textbook FSAL Dormand-Prince: the next step's k1 is k7 = f(y). */
+    RTW_DP45_FSAL = 1
+} rtw_integrator;
+
+/* Scene parameters. Fields a scene kind does not use are ignored.
+ * rtw_scene_default() fills the reference's values for a kind. */
+typedef struct rtw_scene {
+    int32_t kind;           /* rtw_scene_kind */
+    int32_t ref_precision;  /* 1: Kerr Christoffel symbols in FP32 as the
+                               reference's CPU path computes them
+                               (Kerr.source/source_geometry.jl:196-197) */
+    double mass;            /* M (G = c = 1); reference M = 1 */
+    double spin;            /* Kerr a (|a| < M); reference 0.998 */
+    double r_in;            /* emitter inner radius (disk) */
+    double r_out;           /* emitter outer radius (disk) / sphere radius */
+    double theta_lo;        /* wedge lower polar angle */
+    double theta_hi;        /* wedge upper polar angle */
+    double temperature;     /* blackbody temperature, K */
+    double a_nu;            /* absorption coefficient, 1 / map unit */
+    double escape_radius;   /* reference: 100 */
+    double winding_limit;   /* reference: 8 pi */
+    double rho_r0;          /* thick disk: reference radius r0 (6 M) */
+    double rho_h;           /* thick disk: scale height / r (0.1) */
+    double rho_index;       /* thick disk: density power law (-2) */
+    double t_index;         /* thick disk: temperature power law (-0.75) */
+} rtw_scene;
+
+/* One camera (= one frame of a batch). Mirrors the camera keywords of
+ * gen_image and initialize_camera (initialization.jl:190-331). */
+typedef struct rtw_camera {
+    double position[4];     /* camera_pos: (t, r, theta, phi) */
+    double direction[2];    /* camera_dir: direction of the camera's
+                               3-velocity relative to the local tetrad */
+    double speed;           /* speed (beta), |beta| < 1 */
+    double pointing[3];     /* camera_point: roll, pitch, yaw */
+    int32_t x_pix;          /* x_pix: horizontal pixels */
+    int32_t y_pix;          /* out: round(x_pix * tan(fov_vert/2) / tan(fov_hor/2)) */
+    double fov_hor;         /* degrees */
+    double fov_vert;        /* degrees */
+    double tolerance;       /* abs_tol = rel_tol for every state component */
+    int64_t max_steps;      /* step-attempt cap per ray */
+} rtw_camera;
+
+typedef struct rtw_render_params {
+    int32_t n_colors;           /* number of spectral bins, 1..RTW_MAX_BINS */
+    int32_t precision;          /* rtw_precision */
+    const double* colors_nm;    /* [n_colors] wavelengths in nm (reference
+                                   `colors`); host memory */
+    double max_dt_scale;        /* reference max_dt_scale (default 0.1) */
+    int32_t integrator;         /* rtw_integrator */
+    int32_t ray_bundles;        /* must be 0 (bundles are not built) */
+    double promote_dr;          /* MIXED: FP64 stages while r - r_horizon < promote_dr M
+                                   (0: default 1e-4; < 0: never) */
+    double promote_sin;         /* MIXED: FP64 stages while sin(theta) < promote_sin
+                                   (0: default 1e-3; < 0: never) */
+    int32_t block_warps;        /* warps per CTA (0: autotuned / default) */
+    int32_t ctas_per_sm;        /* resident CTAs per SM (0: default) */
+    void* stream;               /* cudaStream_t to run on; NULL: the context's
+                                   stream, and rtw_render returns when done */
+    int32_t pixel_order;        /* 0: row order; 1: 8x4 tiles (internal order,
+                                   outputs are always row order) */
+    int32_t reserved;
+} rtw_render_params;
+
+/* Output buffers, owned by the caller. Pixel p of frame f is at
+ * frame_offset(f) + i + x_pix * j, with i the horizontal index (reference
+ * canvas index i, initialization.jl:213-214) and j the vertical one. NULL
+ * pointers are skipped. */
+typedef struct rtw_outputs {
+    float* xyz;             /* [P][3] linear CIE XYZ (color_theory.jl:96-108
+                               before the xyY conversion) */
+    uint8_t* term_class;    /* [P] rtw_term_class */
+    uint32_t* steps;        /* [P] step attempts (incl. rejected) */
+    float* spectrum;        /* [P][n_colors] final invariant intensity
+                               I_nu/nu^3 per bin (reference Ray[9+2c]) */
+    double* final_state;    /* [P][8] final (t,r,theta,phi,k^t,k^r,k^theta,k^phi) */
+    float* tau;             /* [P] final optical depth (every tau slot of the
+                               reference's state holds this value: the emitters
+                               are grey) */
+    int32_t on_device;      /* 1: device pointers; 0: host pointers */
+    int32_t reserved;
+} rtw_outputs;
+
+typedef struct rtw_stats {
+    uint64_t rays;              /* rays traced by the last render */
+    uint64_t step_attempts;     /* DP45 step attempts, all rays */
+    uint64_t rejected_steps;    /* rejected attempts, all rays */
+    uint64_t promoted_steps;    /* MIXED: attempts run with FP64 stages */
+    uint64_t spectral_steps;    /* attempts whose spectral slots were updated */
+    uint64_t emitting_steps;    /* attempts with emission in some stage */
+    uint64_t escape_substeps;   /* polar Euler sub-steps */
+    uint64_t nan_rays;          /* rays of class RTW_CLASS_NAN */
+    double kernel_ms;           /* device time of the trace kernel */
+    double total_ms;            /* device time of the whole render call */
+} rtw_stats;
+
+/* Algorithmic operation counts of the trace kernel's arithmetic for one scene
+ * kind (add/sub/mul = 1 flop, an FMA = 2; div/sqrt/exp = 1 flop + 1 MUFU op;
+ * sincos/pow = 2 + 2), counted by running the kernel's own formulas on the
+ * host with a counting scalar. */
+typedef struct rtw_op_counts {
+    double rhs_vacuum;          /* one right-hand side outside every emitter */
+    double rhs_vacuum_mufu;
+    double rhs_emit;            /* one right-hand side inside the emitter    */
+    double rhs_emit_mufu;
+    double step_overhead;       /* one DP45 attempt without its 6 right-hand
+                                   sides: stage sums, error norm, controller */
+    double step_overhead_mufu;
+    double bin_step;            /* one spectral bin of one updated attempt   */
+    double bin_step_mufu;
+} rtw_op_counts;
+
+typedef struct rtw_ctx rtw_ctx;
+
+/* Creates a context on CUDA device `device` (its own stream, cached device
+ * buffers). Replaces the CuArray set-up of 5P.jl:177-198. */
+rtw_status rtw_create(rtw_ctx** out, int32_t device);
+/* Frees the context and its device buffers. NULL is accepted. */
+void rtw_destroy(rtw_ctx* ctx);
+/* Text of the context's last error ("" if none); valid until the next call. */
+const char* rtw_last_error(const rtw_ctx* ctx);
+/* ABI version (RTW_ABI_VERSION) of the loaded library. */
+int32_t rtw_abi_version(void);
+
+/* Fills the reference's constants for a scene kind (Kerr.source,
+ * Schwarzschild_Simple_Disk_Spherical.source, Minkowski_Sphere_Spherical.source
+ * source_model.jl / source_geometry.jl constants). */
+rtw_status rtw_scene_default(int32_t kind, rtw_scene* out);
+
+/* Sets cam->y_pix = round(x_pix tan(fov_vert/2) / tan(fov_hor/2)) with ties to
+ * even (initialization.jl:197-200) and returns the pixel count in *n_pix. */
+rtw_status rtw_camera_pixels(rtw_camera* cam, int64_t* n_pix);
+
+/* Host FP64 initial data of one camera, the reference's initialize_camera
+ * (initialization.jl:190-331): rays_out[P][8] = (x^mu, k^mu) per pixel,
+ * pixel order as in rtw_outputs. The spectral slots start at zero. */
+rtw_status rtw_camera_rays(const rtw_scene* scene, const rtw_camera* cam,
+                           double* rays_out, int64_t n_pix);
+
+/* Trapezoid CIE weights for the bins (precompute_CIE_weights,
+ * color_theory.jl:79-91, generalised to non-uniform spacing) and the
+ * per-bin factor nu^3 c / lambda^2 of ray_to_I_lambda (color_theory.jl:73). */
+rtw_status rtw_cie_weights(const double* colors_nm, int32_t n_colors,
+                           double* w_x, double* w_y, double* w_z, double* i_lambda_factor);
+
+/* Renders n_cams frames of one scene in one persistent launch. Replaces the
+ * integrate + colour part of gen_image (5P.jl:158-249, LttM.jl:141-176).
+ * With params->stream == NULL the call is synchronous. */
+rtw_status rtw_render(rtw_ctx* ctx, const rtw_scene* scene,
+                      const rtw_camera* cams, int32_t n_cams,
+                      const rtw_render_params* params, rtw_outputs* out);
+
+/* Counters and device times of the last rtw_render on this context
+ * (synchronises the context's stream). */
+rtw_status rtw_get_stats(rtw_ctx* ctx, rtw_stats* out);
+
+/* Measured issue peaks of this GPU from short in-library microbenchmarks:
+ * FP32 FMA, FP64 FMA (flop/s, an FMA counted as 2) and MUFU ex2 (op/s). */
+rtw_status rtw_measure_peaks(rtw_ctx* ctx, double* fp32_flops, double* fp64_flops,
+                             double* mufu_ops);
+
+/* Operation counts used for the roofline of a render (see rtw_op_counts above). */
+rtw_status rtw_get_op_counts(int32_t kind, rtw_op_counts* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RTW_H */

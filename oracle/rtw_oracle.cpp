@@ -1,0 +1,893 @@
+// rtw_oracle.cpp - TEST INFRASTRUCTURE ONLY (the checker; never the product).
+//
+// A plain C++17 FP64 restatement of the reference's CPU ("LttM") render path,
+// used by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg to
+// check and time the CUDA library. Nothing in the product path (rtwca_b200/,
+// librtw_b200.so) links, loads or calls this file.
+//
+// Parity status: parity unpinned against the reference itself. The reference
+// is Julia, Julia is not installed on any machine of this build, and the
+// reference's own tests pin no numerical results (its "tests" are timing runs
+// that write PNGs that are not in the repository). This restatement is pinned
+// instead against analytic known answers (flat-space straight lines, null-norm
+// and Killing-constant conservation, the Schwarzschild critical impact
+// parameter, an opaque blackbody sphere, a uniform slab, the CIE fit) in
+// tests/test_oracle_physics.py, and against committed golden fixtures that it
+// produced (tests/golden/).
+//
+// What it restates, file:line within the reference project:
+//   integrate_ray / ray_kernel / gen_image   main/Iterators/LttM/LttM.jl:11-80,104-176
+//   calc_ray_derivative! / RKDP_Step_w_buffer!  main/Iterators/LttM/integrators_LttM.jl:9-224
+//   initialize_camera                        main/initialization.jl:190-331
+//   rotation / boost matrices                main/gen_geometry.jl:9-103
+//   calc_freq_shift                          main/gen_geometry.jl:373-390
+//   constants, DP_Butcher                    main/64BitConstants.jl:6-38
+//   CIE fit, weights, I_lambda               main/color_theory.jl:11-108
+//   Heaviside                                main/my_special_functions.jl:9-15
+//   scenes: main/Minkowski_Sphere_Spherical.source/, main/Schwarzschild_Simple_
+//           Disk_Spherical.source/, main/Kerr.source/ (geometry + model files).
+//
+// Deliberate differences from the reference, shared with the CUDA library:
+//  * Scene constants (spin, disk extent, temperature, a_nu, escape radius) are
+//    runtime values of rtw_scene instead of per-scene `const`s.
+//  * Outside every emitter (a_nu = j_nu = 0) both RT slopes are exactly 0. The
+//    reference computes -inv(g)*0*exp(-tau)/nu^3, which is NaN when a stage
+//    point lies inside the horizon (sqrt of a negative in the ZAMO velocity);
+//    the reference's CPU path throws a DomainError there instead.
+//  * CIE trapezoid weights use the local bin widths; for the reference's
+//    uniform `colors` they equal precompute_CIE_weights (color_theory.jl:79-91).
+//  * The Kerr Christoffel symbols are FP64 unless scene.ref_precision = 1,
+//    which computes them in FP32 as the reference's CPU path does
+//    (Kerr.source/source_geometry.jl:196-197).
+//  * The termination class is the first predicate of calc_terminate that holds,
+//    in the reference's order; RTW_CLASS_NAN marks a non-finite final state.
+
+#include "../include/rtw.h"
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+#include <algorithm>
+#include <omp.h>
+
+namespace {
+
+// Float64(pi) as the reference rebinds it in CPU mode (initialization.jl:61-62).
+constexpr double kPi = 3.141592653589793;
+// 64BitConstants.jl:13-25
+constexpr double kPlanckH = 6.62607015e-34;
+constexpr double kLightC = 299792458.0;
+constexpr double kBoltzmann = 1.380649e-23;
+constexpr double kNoDivZero = 1e-24;
+const double kEmissionScale = 2 * kPlanckH * kLightC * 1e27;
+const double kFFactor = kPlanckH * kLightC * 1e9 / kBoltzmann;
+
+// Dormand-Prince tableau (64BitConstants.jl:28-37): rows 2..6 stage
+// coefficients (column 1 is c_i), row 7 = b, row 9 = b*.
+struct Tableau {
+    double a[10][9];
+    Tableau() {
+        std::memset(a, 0, sizeof(a));
+        a[2][1] = 1.0 / 5;  a[2][2] = 1.0 / 5;
+        a[3][1] = 3.0 / 10; a[3][2] = 3.0 / 40; a[3][3] = 9.0 / 40;
+        a[4][1] = 4.0 / 5;  a[4][2] = 44.0 / 45; a[4][3] = -56.0 / 15; a[4][4] = 32.0 / 9;
+        a[5][1] = 8.0 / 9;  a[5][2] = 19372.0 / 6561; a[5][3] = -25360.0 / 2187;
+        a[5][4] = 64448.0 / 6561; a[5][5] = -212.0 / 729;
+        a[6][1] = 1; a[6][2] = 9017.0 / 3168; a[6][3] = -355.0 / 33; a[6][4] = 46732.0 / 5247;
+        a[6][5] = 49.0 / 176; a[6][6] = -5103.0 / 18656;
+        a[7][1] = 1; a[7][2] = 35.0 / 384; a[7][3] = 0; a[7][4] = 500.0 / 1113;
+        a[7][5] = 125.0 / 192; a[7][6] = -2187.0 / 6784; a[7][7] = 11.0 / 84;
+        a[9][2] = 5179.0 / 57600; a[9][4] = 7571.0 / 16695; a[9][5] = 393.0 / 640;
+        a[9][6] = -92097.0 / 339200; a[9][7] = 187.0 / 2100; a[9][8] = 1.0 / 40;
+    }
+};
+const Tableau kDP;
+
+// Julia's mod(x, y) for floats: result has the sign of y.
+inline double jl_mod(double x, double y) {
+    double r = std::fmod(x, y);
+    if (r != 0 && ((r < 0) != (y < 0))) r += y;
+    return r;
+}
+
+inline double sq(double x) { return x * x; }
+
+// ----------------------------------------------------------------------------
+// Scenes (".source" plugins), restated with runtime constants.
+// ----------------------------------------------------------------------------
+struct OScene {
+    int kind = 0;
+    bool refprec = false;
+    double M = 1, a = 0, rs = 2, r_ev = 2, r_in = 6, r_out = 12, th_lo = 0, th_hi = kPi;
+    double T = 5778, anu = 1, esc = 100, wind = 8 * kPi;
+    double rho_r0 = 6, rho_h = 0.1, rho_idx = -2, t_idx = -0.75;
+
+    explicit OScene(const rtw_scene& s) {
+        kind = s.kind;
+        refprec = s.ref_precision != 0;
+        M = s.mass;
+        a = s.spin;
+        r_in = s.r_in; r_out = s.r_out; th_lo = s.theta_lo; th_hi = s.theta_hi;
+        T = s.temperature; anu = s.a_nu; esc = s.escape_radius; wind = s.winding_limit;
+        rho_r0 = s.rho_r0; rho_h = s.rho_h; rho_idx = s.rho_index; t_idx = s.t_index;
+        if (kind == RTW_SCENE_SCHWARZSCHILD_DISK) a = 0;
+        if (refprec) {
+            // the reference's Float32 literals (Kerr source_geometry.jl:7,13,
+            // source_model.jl:44,60)
+            a = (double)(float)a;
+            anu = (double)(float)anu;
+            T = (double)(float)T;
+        }
+        rs = 2 * M;
+        if (kind == RTW_SCENE_KERR_DISK || kind == RTW_SCENE_KERR_THICK_DISK) {
+            // Kerr source_geometry.jl:17
+            if (refprec) {
+                float rsf = (float)rs, af = (float)a;
+                r_ev = (double)(rsf / 2 + std::sqrt((rsf * rsf / 4) - af * af));
+            } else {
+                r_ev = rs / 2 + std::sqrt((rs * rs / 4) - a * a);
+            }
+        } else {
+            r_ev = rs;
+        }
+    }
+
+    bool is_kerr() const { return kind == RTW_SCENE_KERR_DISK || kind == RTW_SCENE_KERR_THICK_DISK; }
+
+    // --- geometry -----------------------------------------------------------
+    // Kerr calc_metric_params, source_geometry.jl:55-60
+    void kerr_params(double r, double th, double& Sig, double& Del, double& A) const {
+        Sig = r * r + sq(a * std::cos(th));
+        Del = r * r - r * rs + a * a;
+        A = (r * r + a * a) * Sig + rs * r * sq(a * std::sin(th));
+    }
+
+    // calc_lower_metric!: Kerr :66-75, Schwarzschild :15-21, Minkowski :10-16
+    void lower_metric(const double* x, double g[4][4]) const {
+        for (int i = 0; i < 4; ++i)
+            for (int j = 0; j < 4; ++j) g[i][j] = (i == j) ? 1.0 : 0.0;
+        const double r = x[1], th = x[2];
+        if (is_kerr()) {
+            double Sig, Del, A;
+            kerr_params(r, th, Sig, Del, A);
+            g[0][0] = -(1.0 - rs * r / Sig);
+            g[0][3] = -rs * a * r * sq(std::sin(th)) / Sig;
+            g[3][0] = g[0][3];
+            g[1][1] = Sig / Del;
+            g[2][2] = Sig;
+            g[3][3] = (A / Sig) * sq(std::sin(th));
+        } else if (kind == RTW_SCENE_SCHWARZSCHILD_DISK) {
+            g[0][0] = -(1.0 - rs / r);
+            g[1][1] = 1.0 / (1.0 - rs / r);
+            g[2][2] = r * r;
+            g[3][3] = sq(r * std::sin(th));
+        } else {
+            g[0][0] = -1.0;
+            g[1][1] = 1.0;
+            g[2][2] = r * r;
+            g[3][3] = sq(r * std::sin(th));
+        }
+    }
+
+    // calc_inv_vierbein: Kerr :112-121, Schwarzschild :53-60, Minkowski :45-50
+    void inv_vierbein(const double* x, double e[4][4]) const {
+        for (int i = 0; i < 4; ++i)
+            for (int j = 0; j < 4; ++j) e[i][j] = (i == j) ? 1.0 : 0.0;
+        const double r = x[1], th = x[2];
+        if (is_kerr()) {
+            double Sig, Del, A;
+            kerr_params(r, th, Sig, Del, A);
+            e[0][0] = std::sqrt(A / (Sig * Del));
+            e[3][0] = (rs * a * r / A) * e[0][0];
+            e[1][1] = std::sqrt(Del / Sig);
+            e[2][2] = 1.0 / std::sqrt(Sig);
+            e[3][3] = std::sqrt(Sig / A) / std::sin(th);
+        } else if (kind == RTW_SCENE_SCHWARZSCHILD_DISK) {
+            e[0][0] = 1.0 / std::sqrt(1.0 - rs / r);
+            e[1][1] = std::sqrt(1.0 - rs / r);
+            e[2][2] = 1.0 / r;
+            e[3][3] = 1.0 / (r * std::sin(th) + kNoDivZero);
+        } else {
+            e[2][2] = 1.0 / (r + kNoDivZero);
+            e[3][3] = 1.0 / (r * std::sin(th) + kNoDivZero);
+        }
+    }
+
+    template <class F>
+    void kerr_christoffel(F r, F th, F al, F rsv, double G[4][4][4]) const {
+        const F two = 2;
+        const F Sig = r * r + (al * std::cos(th)) * (al * std::cos(th));
+        const F Del = r * r - r * rsv + al * al;
+        const F A = (r * r + al * al) * Sig + rsv * r * (al * std::sin(th)) * (al * std::sin(th));
+        const F s = std::sin(th), c = std::cos(th), s2t = std::sin(two * th);
+        const F cot = c / s;  // cot(theta)
+        const F ac2 = (al * c) * (al * c), as2 = (al * s) * (al * s);
+        const F Sig2 = Sig * Sig, Sig3 = Sig * Sig * Sig;
+        // Kerr source_geometry.jl:203-240
+        G[0][0][1] = rsv * (r * r + al * al) * (r * r - ac2) / (two * Sig2 * Del);
+        G[0][1][0] = G[0][0][1];
+        G[0][0][2] = -rsv * al * al * r * s2t / (two * Sig2);
+        G[0][2][0] = G[0][0][2];
+        G[0][1][3] = rsv * al * s * s * (ac2 * (al * al - r * r) - r * r * (al * al + 3 * r * r)) / (two * Sig2 * Del);
+        G[0][3][1] = G[0][1][3];
+        G[0][2][3] = rsv * al * al * al * r * s * s * s * c / Sig2;
+        G[0][3][2] = G[0][2][3];
+        G[1][0][0] = rsv * Del * (r * r - al * al * c * c) / (two * Sig3);
+        G[1][0][3] = -Del * rsv * al * s * s * (r * r - ac2) / (two * Sig3);
+        G[1][3][0] = G[1][0][3];
+        G[1][1][1] = (two * r * as2 - rsv * (r * r - ac2)) / (two * Sig * Del);
+        G[1][1][2] = -al * al * s2t / (two * Sig);
+        G[1][2][1] = G[1][1][2];
+        G[1][2][2] = -r * Del / Sig;
+        G[1][3][3] = Del * s * s * (-two * r * Sig2 + rsv * as2 * (r * r - ac2)) / (two * Sig3);
+        G[2][0][0] = -rsv * al * al * r * s2t / (two * Sig3);
+        G[2][0][3] = rsv * al * r * (r * r + al * al) * s2t / (two * Sig3);
+        G[2][3][0] = G[2][0][3];
+        G[2][1][1] = al * al * s2t / (two * Sig * Del);
+        G[2][1][2] = r / Sig;
+        G[2][2][1] = G[2][1][2];
+        G[2][2][2] = -al * al * s2t / (two * Sig);
+        G[2][3][3] = -s2t * (A * Sig + (r * r + al * al) * rsv * r * as2) / (two * Sig3);
+        G[3][0][1] = rsv * al * (r * r - ac2) / (two * Sig2 * Del);
+        G[3][1][0] = G[3][0][1];
+        G[3][0][2] = -rsv * al * r * cot / Sig2;
+        G[3][2][0] = G[3][0][2];
+        const F hs = al * al * s2t / two;
+        G[3][1][3] = (two * r * Sig2 + rsv * (hs * hs - r * r * (Sig + r * r + al * al))) / (two * Sig2 * Del);
+        G[3][3][1] = G[3][1][3];
+        G[3][2][3] = cot * (Sig2 + rsv * r * as2) / Sig2;
+        G[3][3][2] = G[3][2][3];
+    }
+
+    // calc_christoffel_udd!: Kerr :195-243, Schwarzschild :109-128, Minkowski :93-108
+    void christoffel(const double* x, double G[4][4][4]) const {
+        std::memset(G, 0, sizeof(double) * 64);
+        const double r = x[1], th = x[2];
+        if (is_kerr()) {
+            if (refprec)
+                kerr_christoffel<float>((float)r, (float)th, (float)a, (float)rs, G);
+            else
+                kerr_christoffel<double>(r, th, a, rs, G);
+        } else if (kind == RTW_SCENE_SCHWARZSCHILD_DISK) {
+            G[0][0][1] = rs / (2 * r * (r - rs));
+            G[0][1][0] = G[0][0][1];
+            G[1][0][0] = rs * (r - rs) / (2 * r * r * r);
+            G[1][1][1] = -rs / (2 * r * (r - rs));
+            G[1][2][2] = -(r - rs);
+            G[1][3][3] = -(r - rs) * sq(std::sin(th));
+            G[2][1][2] = 1.0 / r;
+            G[2][2][1] = G[2][1][2];
+            G[2][3][3] = -std::sin(th) * std::cos(th);
+            G[3][1][3] = 1.0 / r;
+            G[3][3][1] = G[3][1][3];
+            G[3][2][3] = std::cos(th) / std::sin(th);
+            G[3][3][2] = G[3][2][3];
+        } else {
+            G[1][2][2] = -r;
+            G[1][3][3] = -r * sq(std::sin(th));
+            G[2][1][2] = 1.0 / (r + kNoDivZero);
+            G[2][2][1] = G[2][1][2];
+            G[2][3][3] = -std::sin(th) * std::cos(th);
+            G[3][1][3] = 1.0 / (r + kNoDivZero);
+            G[3][3][1] = G[3][1][3];
+            G[3][2][3] = std::cos(th) / std::sin(th);
+            G[3][3][2] = G[3][2][3];
+        }
+    }
+
+    // near_singularity: Kerr :249-269 (= Schwarzschild :134-154), Minkowski :114-132
+    bool near_singularity(const double* x, double h, double tol, double* temp) const {
+        const double th_new = x[2] + h * x[6];
+        const double r_new = x[1] + h * x[5];
+        if (kind == RTW_SCENE_MINKOWSKI_SPHERE) {
+            const double lim = 10 * tol / std::fabs(r_new + kNoDivZero);
+            if (std::fabs(th_new) <= lim) {
+                *temp = 2 * std::fabs(x[2]) / (std::fabs(x[6] * 37) + kNoDivZero);
+                return true;
+            } else if (std::fabs(th_new - kPi) <= lim) {
+                *temp = 2 * std::fabs((x[2] - kPi) / (std::fabs(x[6] * 37) + kNoDivZero));
+                return true;
+            } else if (std::fabs(r_new) <= 100 * tol) {
+                *temp = 2 * tol / (std::fabs(x[5] * 37) + kNoDivZero);
+                return true;
+            }
+            *temp = h;
+            return false;
+        }
+        if (std::fabs(th_new) <= tol) {
+            *temp = 2 * std::fabs(x[2]) / (std::fabs(x[6] * 37) + kNoDivZero);
+            return true;
+        } else if (std::fabs(th_new - kPi) <= tol) {
+            *temp = 2 * std::fabs((x[2] - kPi) / (std::fabs(x[6] * 37) + kNoDivZero));
+            return true;
+        }
+        *temp = h;
+        return false;
+    }
+
+    // keepinbounds!: Kerr :275-301 (= Schwarzschild :160-186), Minkowski :138-163
+    void keepinbounds(double* x) const {
+        if (kind == RTW_SCENE_MINKOWSKI_SPHERE && x[1] <= 0) {
+            x[1] = -x[1] + kNoDivZero;
+            x[5] = -x[5];
+            x[2] -= kPi;
+            x[6] = -x[6];
+        }
+        if (x[2] < 0) {
+            x[2] = -x[2];
+            x[3] -= kPi;
+            x[6] = -x[6];
+        }
+        x[2] = jl_mod(x[2], 2 * kPi);
+        if (x[2] >= kPi) {
+            x[2] = 2 * kPi - x[2];
+            x[3] += kPi;
+            x[6] = -x[6];
+        }
+    }
+
+    // is_singularity: Kerr :307-315 and the other scenes
+    bool is_singularity(const double* pos) const {
+        if (std::fabs(pos[1]) <= (double)1e-32f) return true;
+        if (std::fabs(pos[2]) <= (double)1e-32f || std::fabs(pos[2] - kPi) <= 1e-32) return true;
+        return false;
+    }
+
+    // --- model --------------------------------------------------------------
+    // is_fire: Kerr model :73-80, Schwarzschild :73-80, Minkowski :76-83
+    bool is_fire(const double* x) const {
+        const double r = x[1], th = x[2];
+        switch (kind) {
+        case RTW_SCENE_MINKOWSKI_SPHERE: return r <= r_out;
+        case RTW_SCENE_SCHWARZSCHILD_DISK:
+        case RTW_SCENE_KERR_DISK:
+            return r_in <= r && r <= r_out && th_lo <= th && th <= th_hi;
+        case RTW_SCENE_KERR_THICK_DISK: return r_in <= r && r <= r_out;
+        }
+        return false;
+    }
+
+    // get_source_velocity!: Kerr model :109-137, Schwarzschild :112-133, Minkowski :111-117
+    void source_velocity(const double* x, double u[4]) const {
+        const double r = x[1], th = x[2];
+        u[0] = 1; u[1] = 0; u[2] = 0; u[3] = 0;
+        if (kind == RTW_SCENE_MINKOWSKI_SPHERE) return;
+        if (kind == RTW_SCENE_SCHWARZSCHILD_DISK) {
+            if (is_fire(x)) {
+                u[0] = 1.0 / std::sqrt(1 - 3 * M / r);
+                u[3] = (1.0 / std::sqrt(1 - 3 * M / r)) * std::sqrt(M / (r * r * r));
+            } else {
+                u[0] = 1.0 / std::sqrt(1 - 2 * M / r);
+            }
+            return;
+        }
+        if (is_fire(x)) {
+            const double r32 = std::pow(r, 1.5);
+            const double Om = std::sqrt(M) / (r32 + a * std::sqrt(M));
+            const double D = r32 - 3 * M * std::sqrt(r) + 2 * a * std::sqrt(M);
+            const double ut = (r32 + a * std::sqrt(M)) / (std::pow(r, 0.75) * std::sqrt(D));
+            u[0] = ut;
+            u[3] = ut * Om;
+        } else {
+            const double Aa = std::sqrt(r * r + sq(a * std::cos(th)));
+            const double B = r * r + a * a - 2 * M * r;
+            const double C = sq(r * r + a * a) - B * sq(a * std::sin(th));
+            const double ut = std::sqrt(C) / (Aa * std::sqrt(B));
+            const double Om = 2 * a * M * r / C;
+            u[0] = ut;
+            u[3] = ut * Om;
+        }
+    }
+
+    // calc_radiative_coefficients + calc_planck (Kerr model :18-21,57-67 and
+    // the other scenes). fluid: temperature (and density for the thick disk).
+    void radiative(const double* x, double nu, double* a_nu, double* j_nu) const {
+        if (!is_fire(x)) {
+            *a_nu = 0;
+            *j_nu = 0;
+            return;
+        }
+        double Tl = T, al = anu;
+        if (kind == RTW_SCENE_KERR_THICK_DISK) {
+            const double r = x[1];
+            const double z = r * std::cos(x[2]);
+            const double hz = rho_h * r;
+            const double rho = std::pow(r / rho_r0, rho_idx) * std::exp(-(z * z) / (2 * hz * hz));
+            Tl = T * std::pow(r / rho_r0, t_idx);
+            al = anu * rho;
+        }
+        *a_nu = al;
+        *j_nu = al * (kEmissionScale * (nu * nu * nu) / (std::exp(kFFactor * nu / Tl) - 1));
+    }
+
+    // pad_max_dt: Kerr model :86-103, Schwarzschild :86-106, Minkowski :89-105
+    double pad_max_dt(const double* x, double scale) const {
+        double eps;
+        // Kerr casts the scale to Float32 (Kerr model :92-96); the other scenes
+        // keep it in Float64 except for the Float32 literal 1f-1.
+        if (is_kerr()) scale = (double)(float)scale;
+        if (x[2] < kPi / 8 || x[2] > 7 * kPi / 8) {
+            eps = std::min(scale, (double)1e-1f);
+        } else if (kind == RTW_SCENE_SCHWARZSCHILD_DISK && x[1] <= 1.5 * (3 * M)) {
+            eps = scale / 10;
+        } else {
+            eps = scale;
+        }
+        double first;
+        if (is_kerr())
+            first = std::fabs(1.0 / (eps / std::fabs(x[5]))) + kNoDivZero;
+        else
+            first = std::fabs(1.0 / (eps / (std::fabs(x[5]) + kNoDivZero))) + kNoDivZero;
+        const double second =
+            std::fabs(1.0 / (eps * std::min(x[2], kPi - x[2]) / (std::fabs(x[6]) + kNoDivZero) + kNoDivZero));
+        const double third = std::fabs(1.0 / (eps / (std::fabs(x[7]) + kNoDivZero) + kNoDivZero));
+        double m = std::min(1.0 / (first + second + third + kNoDivZero), 0.5);
+        m = std::max(m, (double)1e-12f);
+        return m;
+    }
+
+    // calc_terminate: Kerr model :168-182, Schwarzschild :156-170, Minkowski :131-145.
+    // Returns the class of the first predicate that holds, or 0.
+    int terminate(const double* ray, int L, double tol, long long max_steps, long long step_count) const {
+        if ((double)step_count >= (double)max_steps) return RTW_CLASS_MAXSTEPS;
+        if (ray[1] > esc) return RTW_CLASS_ESCAPE;
+        if (kind != RTW_SCENE_MINKOWSKI_SPHERE && ray[1] <= (1 + 10 * tol) * r_ev) return RTW_CLASS_HORIZON;
+        if (ray[3] > wind) return RTW_CLASS_WINDING;
+        const double thick = -std::log(tol);
+        for (int i = 9; i < L; i += 2)
+            if (ray[i] < thick) return 0;
+        return RTW_CLASS_THICK;
+    }
+};
+
+// ----------------------------------------------------------------------------
+// Integrator (integrators_LttM.jl), one ray's buffers.
+// ----------------------------------------------------------------------------
+struct RayWork {
+    int L = 0, N = 0;
+    const double* freq = nullptr;  // colors_freq, nm^-1
+    double tol = 1e-4;
+    double scale = 0.1;
+    bool fsal = false;
+    std::vector<double> last_slope, next_slope, buffer, y, k2, k3, k4, k5, k6, k7;
+    double G[4][4][4];
+    double g[4][4];
+    double u[4];
+    void init(int N_, const double* f, double tol_, double scale_, bool fsal_) {
+        N = N_;
+        L = 8 + 2 * N;
+        freq = f;
+        tol = tol_;
+        scale = scale_;
+        fsal = fsal_;
+        for (auto* v : {&last_slope, &next_slope, &buffer, &y, &k2, &k3, &k4, &k5, &k6, &k7}) v->assign(L, 0.0);
+    }
+};
+
+// calc_ray_derivative!, integrators_LttM.jl:9-48
+void rhs(const OScene& sc, RayWork& w, const double* R, double* slope) {
+    for (int i = 0; i < 4; ++i) slope[i] = R[i + 4];
+    sc.christoffel(R, w.G);
+    for (int i = 0; i < 4; ++i) {
+        double acc = 0;
+        for (int j = 0; j < 4; ++j)
+            for (int k = 0; k < 4; ++k) acc -= w.G[i][j][k] * R[4 + j] * R[4 + k];
+        slope[4 + i] = acc;
+    }
+    sc.lower_metric(R, w.g);
+    sc.source_velocity(R, w.u);
+    // calc_freq_shift, gen_geometry.jl:373-390
+    double fs = 0;
+    for (int j = 0; j < 4; ++j) {
+        double ps = 0;
+        for (int i = 0; i < 4; ++i) ps += w.g[i][j] * R[i + 4];
+        fs -= w.u[j] * ps;
+    }
+    for (int c = 0; c < w.N; ++c) {
+        const double nu = w.freq[c] * fs;
+        double a_nu, j_nu;
+        sc.radiative(R, nu, &a_nu, &j_nu);
+        if (a_nu == 0 && j_nu == 0) {
+            slope[8 + 2 * c] = 0;
+            slope[9 + 2 * c] = 0;
+        } else {
+            slope[8 + 2 * c] = -(1.0 / fs) * j_nu * std::exp(-R[9 + 2 * c]) / (nu * nu * nu);
+            slope[9 + 2 * c] = -(1.0 / fs) * a_nu;
+        }
+    }
+}
+
+// RKDP_Step_w_buffer!, integrators_LttM.jl:54-224. Returns the new step size;
+// *rejected is the reject flag. counters[0] counts polar Euler sub-steps.
+double dp45_step(const OScene& sc, RayWork& w, double* R, double h, bool prev_rejected, bool* rejected,
+                 long long* escape_substeps) {
+    const int L = w.L;
+    double* k1 = w.last_slope.data();
+    const double max_dt = sc.pad_max_dt(R, w.scale);
+    double temp;
+    if (sc.near_singularity(R, h, w.tol, &temp)) {
+        for (int i = 0; i < L; ++i) R[i] -= temp * k1[i];
+        sc.keepinbounds(R);
+        if (escape_substeps) ++*escape_substeps;
+        for (int it = 0; it < 36; ++it) {
+            if (!sc.terminate(R, L, w.tol, 2, 1)) {
+                rhs(sc, w, R, k1);
+                for (int j = 0; j < L; ++j) R[j] -= temp * k1[j];
+                sc.keepinbounds(R);
+                if (escape_substeps) ++*escape_substeps;
+            }
+        }
+        if (sc.terminate(R, L, w.tol, 2, 1)) {
+            *rejected = false;
+            return h;
+        }
+        rhs(sc, w, R, k1);
+        h = -sc.pad_max_dt(R, w.scale);
+    }
+    const auto& A = kDP.a;
+    double* buf = w.buffer.data();
+    double *k2 = w.k2.data(), *k3 = w.k3.data(), *k4 = w.k4.data(), *k5 = w.k5.data(), *k6 = w.k6.data(),
+           *k7 = w.k7.data();
+    for (int i = 0; i < L; ++i) buf[i] = R[i] + h * k1[i] * A[2][2];
+    rhs(sc, w, buf, k2);
+    for (int i = 0; i < L; ++i) buf[i] = R[i] + h * (k1[i] * A[3][2] + k2[i] * A[3][3]);
+    rhs(sc, w, buf, k3);
+    for (int i = 0; i < L; ++i) buf[i] = R[i] + h * (k1[i] * A[4][2] + k2[i] * A[4][3] + k3[i] * A[4][4]);
+    rhs(sc, w, buf, k4);
+    for (int i = 0; i < L; ++i)
+        buf[i] = R[i] + h * (k1[i] * A[5][2] + k2[i] * A[5][3] + k3[i] * A[5][4] + k4[i] * A[5][5]);
+    rhs(sc, w, buf, k5);
+    for (int i = 0; i < L; ++i)
+        buf[i] = R[i] + h * (k1[i] * A[6][2] + k2[i] * A[6][3] + k3[i] * A[6][4] + k4[i] * A[6][5] + k5[i] * A[6][6]);
+    rhs(sc, w, buf, k6);
+    double* ns = w.next_slope.data();
+    for (int i = 0; i < L; ++i)
+        ns[i] = k1[i] * A[7][2] + k3[i] * A[7][4] + k4[i] * A[7][5] + k5[i] * A[7][6] + k6[i] * A[7][7];
+    for (int i = 0; i < L; ++i) buf[i] = R[i] + h * ns[i];
+    rhs(sc, w, buf, k7);
+    double* y = w.y.data();
+    for (int i = 0; i < L; ++i) y[i] = R[i] + h * ns[i];
+    for (int i = 0; i < L; ++i)
+        buf[i] = y[i] - R[i] -
+                 h * (k1[i] * A[9][2] + k3[i] * A[9][4] + k4[i] * A[9][5] + k5[i] * A[9][6] + k6[i] * A[9][7] +
+                      k7[i] * A[9][8]);
+    double err = 0;
+    for (int i = 0; i < L; ++i) {
+        const double tol = w.tol + std::max(std::fabs(R[i]), std::fabs(y[i])) * w.tol;
+        err += sq(buf[i] / tol);
+    }
+    err = std::sqrt(err / L);
+    double hn = 0.9 * h * std::pow(1.0 / err, 1.0 / 5);
+    if (std::fabs(hn) > max_dt) hn = -max_dt;
+    const double* newk1 = w.fsal ? k7 : ns;
+    if (err == 0 || !std::isfinite(hn)) {
+        sc.keepinbounds(y);
+        for (int i = 0; i < L; ++i) {
+            k1[i] = newk1[i];
+            R[i] = y[i];
+        }
+        *rejected = false;
+        return h;
+    } else if (err > 1) {
+        if (prev_rejected && std::fabs(hn) >= std::fabs(h)) hn = h / 2;
+        sc.keepinbounds(R);
+        *rejected = true;
+        return hn;
+    }
+    if (std::fabs(hn) > 5 * std::fabs(h)) hn = 5 * h;
+    sc.keepinbounds(y);
+    for (int i = 0; i < L; ++i) {
+        k1[i] = newk1[i];
+        R[i] = y[i];
+    }
+    *rejected = false;
+    return hn;
+}
+
+// ----------------------------------------------------------------------------
+// Camera (initialization.jl:190-331, gen_geometry.jl:9-103)
+// ----------------------------------------------------------------------------
+typedef double Mat4[4][4];
+
+void matmul(const Mat4 A, const Mat4 B, Mat4 C) {
+    Mat4 t;
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) {
+            double s = 0;
+            for (int k = 0; k < 4; ++k) s += A[i][k] * B[k][j];
+            t[i][j] = s;
+        }
+    std::memcpy(C, t, sizeof(Mat4));
+}
+
+// gen_intrinsic_rotation_matrix, gen_geometry.jl:9-40
+void intrinsic_rotation(const double p[3], Mat4 R) {
+    Mat4 Rx = {{0}}, Ry = {{0}}, Rz = {{0}};
+    Rx[0][0] = 1; Rx[1][1] = 1;
+    Rx[2][2] = std::cos(p[0]); Rx[3][2] = std::sin(p[0]); Rx[2][3] = -std::sin(p[0]); Rx[3][3] = std::cos(p[0]);
+    Ry[0][0] = 1;
+    Ry[1][1] = std::cos(p[1]); Ry[3][1] = -std::sin(p[1]); Ry[2][2] = 1; Ry[1][3] = std::sin(p[1]);
+    Ry[3][3] = std::cos(p[1]);
+    Rz[0][0] = 1;
+    Rz[1][1] = std::cos(p[2]); Rz[2][1] = std::sin(p[2]); Rz[1][2] = -std::sin(p[2]); Rz[2][2] = std::cos(p[2]);
+    Rz[3][3] = 1;
+    Mat4 t;
+    matmul(Rz, Ry, t);
+    matmul(t, Rx, R);
+}
+
+// gen_final_rotation_matrix, gen_geometry.jl:47-87
+void final_rotation(const double dir[2], Mat4 R) {
+    const double d[3] = {std::sin(dir[0]) * std::cos(dir[1]), std::sin(dir[0]) * std::sin(dir[1]), std::cos(dir[0])};
+    double k[3] = {0.0 * d[2] - 1.0 * d[1], 1.0 * d[0] - 0.0 * d[2], 0.0 * d[1] - 0.0 * d[0]};
+    const double mag = std::sqrt(k[0] * k[0] + k[1] * k[1] + k[2] * k[2]);
+    const double yaw[3] = {0, 0, kPi / 2 + dir[1]};
+    Mat4 Ri;
+    intrinsic_rotation(yaw, Ri);
+    if (mag > 0) {
+        for (double& v : k) v /= mag;
+        double K[3][3] = {{0, -k[2], k[1]}, {k[2], 0, -k[0]}, {-k[1], k[0], 0}};
+        double KK[3][3];
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+                double s = 0;
+                for (int m = 0; m < 3; ++m) s += K[i][m] * K[m][j];
+                KK[i][j] = s;
+            }
+        Mat4 R4 = {{0}};
+        R4[0][0] = 1;
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j)
+                R4[1 + i][1 + j] = (i == j ? 1.0 : 0.0) + std::sin(dir[0]) * K[i][j] + (1 - std::cos(dir[0])) * KK[i][j];
+        Mat4 T;
+        for (int i = 0; i < 4; ++i)
+            for (int j = 0; j < 4; ++j) T[i][j] = R4[j][i];
+        matmul(T, Ri, R);
+    } else {
+        std::memcpy(R, Ri, sizeof(Mat4));
+    }
+}
+
+// lorentz_boost_z, gen_geometry.jl:93-103
+void boost_z(double beta, Mat4 L) {
+    std::memset(L, 0, sizeof(Mat4));
+    const double gamma = 1 / std::sqrt(1 - beta * beta);
+    L[0][0] = gamma; L[3][0] = -beta * gamma; L[0][3] = -beta * gamma;
+    L[1][1] = 1; L[2][2] = 1; L[3][3] = gamma;
+}
+
+struct CameraGeom {
+    int xp = 0, yp = 0;
+    double W = 0, H = 0, rh = 0, rv = 0;
+    Mat4 M;  // e * R2 * L * R
+};
+
+bool camera_geom(const OScene& sc, const rtw_camera& cam, CameraGeom& cg) {
+    const double fh = kPi * cam.fov_hor / 180, fv = kPi * cam.fov_vert / 180;
+    cg.W = std::tan(fh / 2);
+    cg.H = std::tan(fv / 2);
+    cg.xp = cam.x_pix;
+    cg.yp = (int)std::nearbyint(cam.x_pix * cg.H / cg.W);
+    cg.rh = 2 * cg.W / (cg.xp + 1);
+    cg.rv = 2 * cg.H / (cg.yp + 1);
+    Mat4 R, L, R2, e, t1, t2;
+    intrinsic_rotation(cam.pointing, R);
+    boost_z(-cam.speed, L);
+    final_rotation(cam.direction, R2);
+    sc.inv_vierbein(cam.position, e);
+    matmul(e, R2, t1);
+    matmul(t1, L, t2);
+    matmul(t2, R, cg.M);
+    return true;
+}
+
+// Initial state of pixel (i, j), 0-based (initialization.jl:213-240,327).
+void camera_ray(const CameraGeom& cg, const rtw_camera& cam, int i, int j, double* S) {
+    const double w = cg.rh * ((i + 1) - 0.5) - cg.W;
+    const double h = cg.rv * ((j + 1) - 0.5) - cg.H;
+    const double th = std::atan(std::sqrt(w * w + h * h));
+    double ph;
+    if (w > 0) ph = std::atan(h / w);
+    else if (w < 0 && h >= 0) ph = std::atan(h / w) + kPi;
+    else if (w < 0 && h < 0) ph = std::atan(h / w) - kPi;
+    else if (w == 0 && h > 0) ph = kPi / 2;
+    else if (w == 0 && h < 0) ph = -kPi / 2;
+    else ph = 0;
+    const double v[4] = {1, -std::sin(th) * std::cos(ph), -std::sin(th) * std::sin(ph), -std::cos(th)};
+    for (int k = 0; k < 4; ++k) S[k] = cam.position[k];
+    for (int r = 0; r < 4; ++r) {
+        double s = 0;
+        for (int k = 0; k < 4; ++k) s += cg.M[r][k] * v[k];
+        S[4 + r] = s;
+    }
+}
+
+// ----------------------------------------------------------------------------
+// CIE (color_theory.jl)
+// ----------------------------------------------------------------------------
+const double kCie[4][7] = {
+    {0.362, 1.056, -0.065, 0.821, 0.286, 1.217, 0.681},
+    {442.0, 599.8, 501.1, 568.8, 530.9, 437.0, 459.0},
+    {0.0624, 0.0264, 0.0490, 0.0213, 0.0613, 0.0845, 0.0385},
+    {0.0374, 0.0323, 0.0382, 0.0247, 0.0322, 0.0278, 0.0725}};
+
+inline double heaviside(double x) { return x >= 0 ? 1.0 : 0.0; }
+inline double selector(double x, double y, double z) { return y * (1 - heaviside(x)) + z * heaviside(x); }
+double cie_lobes(double wl, int first, int n) {
+    double s = 0;
+    for (int i = first; i < first + n; ++i) {
+        const double d = wl - kCie[1][i];
+        s = s + kCie[0][i] * std::exp((-1.0 / 2) * sq(d * selector(d, kCie[2][i], kCie[3][i])));
+    }
+    return s;
+}
+
+void cie_weights(const double* colors, int n, double* wx, double* wy, double* wz, double* fac) {
+    for (int i = 0; i < n; ++i) {
+        double w;
+        if (n == 1) w = 1.0;
+        else if (i == 0) w = (colors[1] - colors[0]) / 2;
+        else if (i == n - 1) w = (colors[n - 1] - colors[n - 2]) / 2;
+        else w = (colors[i + 1] - colors[i - 1]) / 2;
+        wx[i] = cie_lobes(colors[i], 0, 3) * w;
+        wy[i] = cie_lobes(colors[i], 3, 2) * w;
+        wz[i] = cie_lobes(colors[i], 5, 2) * w;
+        const double f = 1.0 / colors[i];
+        fac[i] = f * f * f * kLightC / (colors[i] * colors[i]);
+    }
+}
+
+}  // namespace
+
+// ----------------------------------------------------------------------------
+// C API for tests (ctypes). Outputs are double precision.
+// ----------------------------------------------------------------------------
+extern "C" {
+
+int oracle_abi_version(void) { return RTW_ABI_VERSION; }
+
+int oracle_cie(const double* colors, int n, double* wx, double* wy, double* wz, double* fac) {
+    if (!colors || n <= 0) return RTW_ERR_INVALID_PARAM;
+    cie_weights(colors, n, wx, wy, wz, fac);
+    return RTW_OK;
+}
+
+double oracle_cie_eval(int which, double wl) {
+    if (which == 0) return cie_lobes(wl, 0, 3);
+    if (which == 1) return cie_lobes(wl, 3, 2);
+    return cie_lobes(wl, 5, 2);
+}
+
+int oracle_constants(double* emission_scale, double* f_factor) {
+    *emission_scale = kEmissionScale;
+    *f_factor = kFFactor;
+    return RTW_OK;
+}
+
+int oracle_camera_rays(const rtw_scene* scene, rtw_camera* cam, double* rays, long long n_pix) {
+    OScene sc(*scene);
+    CameraGeom cg;
+    camera_geom(sc, *cam, cg);
+    cam->y_pix = cg.yp;
+    if ((long long)cg.xp * cg.yp != n_pix) return RTW_ERR_INVALID_PARAM;
+    for (int j = 0; j < cg.yp; ++j)
+        for (int i = 0; i < cg.xp; ++i) camera_ray(cg, *cam, i, j, rays + 8 * ((long long)i + (long long)cg.xp * j));
+    return RTW_OK;
+}
+
+// Slope of a full state R[8 + 2N] (calc_ray_derivative!).
+int oracle_rhs(const rtw_scene* scene, const double* colors_nm, int n_colors, const double* R, double* slope) {
+    OScene sc(*scene);
+    std::vector<double> freq(n_colors);
+    for (int c = 0; c < n_colors; ++c) freq[c] = 1.0 / colors_nm[c];
+    RayWork w;
+    w.init(n_colors, freq.data(), 1e-4, 0.1, false);
+    rhs(sc, w, R, slope);
+    return RTW_OK;
+}
+
+int oracle_metric(const rtw_scene* scene, const double* x, double* g16) {
+    OScene sc(*scene);
+    double g[4][4];
+    sc.lower_metric(x, g);
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) g16[4 * i + j] = g[i][j];
+    return RTW_OK;
+}
+
+double oracle_pad_max_dt(const rtw_scene* scene, const double* x, double scale) {
+    OScene sc(*scene);
+    return sc.pad_max_dt(x, scale);
+}
+
+// Traces the pixels `pixel_ids` (or all pixels when pixel_ids == NULL) of one
+// camera. Outputs are indexed by position in the pixel list:
+//   xyz[n][3], cls[n], steps[n], spectrum[n][N] (Ray[9+2c]), tau[n][N]
+//   (Ray[10+2c]), state[n][8]; NULL pointers are skipped. counters (may be
+//   NULL): [0] step attempts, [1] rejected, [2] polar Euler sub-steps.
+// n_threads <= 0: all OpenMP threads. Returns rtw_status.
+int oracle_render(const rtw_scene* scene, rtw_camera* cam, const double* colors_nm, int n_colors,
+                  double max_dt_scale, int integrator, const long long* pixel_ids, long long n_ids, double* xyz,
+                  unsigned char* cls, unsigned int* steps, double* spectrum, double* tau, double* state,
+                  long long* counters, int n_threads) {
+    if (!scene || !cam || !colors_nm || n_colors <= 0 || n_colors > RTW_MAX_BINS) return RTW_ERR_INVALID_PARAM;
+    OScene sc(*scene);
+    if (sc.is_singularity(cam->position)) return RTW_ERR_INVALID_CAMERA;
+    CameraGeom cg;
+    camera_geom(sc, *cam, cg);
+    cam->y_pix = cg.yp;
+    const long long P = (long long)cg.xp * cg.yp;
+    const long long n = pixel_ids ? n_ids : P;
+    std::vector<double> freq(n_colors), wx(n_colors), wy(n_colors), wz(n_colors), fac(n_colors);
+    for (int c = 0; c < n_colors; ++c) freq[c] = 1.0 / colors_nm[c];
+    cie_weights(colors_nm, n_colors, wx.data(), wy.data(), wz.data(), fac.data());
+    const int N = n_colors, L = 8 + 2 * N;
+    const double tol = cam->tolerance;
+    const long long max_steps = cam->max_steps;
+    int nt = n_threads > 0 ? n_threads : omp_get_max_threads();
+    const long long chunk = std::max(1LL, (n + 100LL * nt - 1) / (100LL * nt));
+    long long tot_steps = 0, tot_rej = 0, tot_esc = 0;
+#pragma omp parallel num_threads(nt) reduction(+ : tot_steps, tot_rej, tot_esc)
+    {
+        RayWork w;
+        w.init(N, freq.data(), tol, max_dt_scale, integrator == RTW_DP45_FSAL);
+        std::vector<double> ray(L);
+#pragma omp for schedule(dynamic, chunk)
+        for (long long q = 0; q < n; ++q) {
+            const long long p = pixel_ids ? pixel_ids[q] : q;
+            const int i = (int)(p % cg.xp), j = (int)(p / cg.xp);
+            std::fill(ray.begin(), ray.end(), 0.0);
+            camera_ray(cg, *cam, i, j, ray.data());
+            // integrate_ray, LttM.jl:11-59
+            double dt = -sc.pad_max_dt(ray.data(), max_dt_scale);
+            rhs(sc, w, ray.data(), w.last_slope.data());
+            w.next_slope = w.last_slope;
+            bool rejected = false;
+            long long step_count = 0;
+            long long esc = 0;
+            int klass = 0;
+            while (true) {
+                bool rj = false;
+                dt = dp45_step(sc, w, ray.data(), dt, rejected, &rj, &esc);
+                rejected = rj;
+                tot_rej += rj ? 1 : 0;
+                ++step_count;
+                klass = sc.terminate(ray.data(), L, tol, max_steps, step_count);
+                if (klass) break;
+            }
+            for (int k = 0; k < 8; ++k)
+                if (!std::isfinite(ray[k])) klass = RTW_CLASS_NAN;
+            tot_steps += step_count;
+            tot_esc += esc;
+            if (cls) cls[q] = (unsigned char)klass;
+            if (steps) steps[q] = (unsigned int)step_count;
+            if (xyz) {
+                double X = 0, Y = 0, Z = 0;
+                for (int c = 0; c < N; ++c) {
+                    const double il = ray[8 + 2 * c] * freq[c] * freq[c] * freq[c] * kLightC / (colors_nm[c] * colors_nm[c]);
+                    X += il * wx[c];
+                    Y += il * wy[c];
+                    Z += il * wz[c];
+                }
+                xyz[3 * q + 0] = X;
+                xyz[3 * q + 1] = Y;
+                xyz[3 * q + 2] = Z;
+            }
+            if (spectrum)
+                for (int c = 0; c < N; ++c) spectrum[(long long)N * q + c] = ray[8 + 2 * c];
+            if (tau)
+                for (int c = 0; c < N; ++c) tau[(long long)N * q + c] = ray[9 + 2 * c];
+            if (state)
+                for (int k = 0; k < 8; ++k) state[8 * q + k] = ray[k];
+        }
+    }
+    if (counters) {
+        counters[0] = tot_steps;
+        counters[1] = tot_rej;
+        counters[2] = tot_esc;
+    }
+    return RTW_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,627 @@
+// rtw_capi.cu - host side of the C ABI declared in include/rtw.h: context,
+// camera set-up (FP64), CIE tables, validation, device buffers, launch.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "rtw_internal.h"
+
+namespace rtw {
+cudaError_t launch_kind_0(const KParams&, int, int, int, cudaStream_t);
+cudaError_t launch_kind_1(const KParams&, int, int, int, cudaStream_t);
+cudaError_t launch_kind_2(const KParams&, int, int, int, cudaStream_t);
+cudaError_t launch_kind_3(const KParams&, int, int, int, cudaStream_t);
+const void* kernel_ptr_0(int, int);
+const void* kernel_ptr_1(int, int);
+const void* kernel_ptr_2(int, int);
+const void* kernel_ptr_3(int, int);
+
+static const void* kernel_ptr(int kind, int precision, int np) {
+    switch (kind) {
+    case 0: return kernel_ptr_0(precision, np);
+    case 1: return kernel_ptr_1(precision, np);
+    case 2: return kernel_ptr_2(precision, np);
+    default: return kernel_ptr_3(precision, np);
+    }
+}
+
+cudaError_t launch_trace(const KParams& p, int precision, int grid, int block, cudaStream_t stream) {
+    switch (p.sc.kind) {
+    case 0: return launch_kind_0(p, precision, grid, block, stream);
+    case 1: return launch_kind_1(p, precision, grid, block, stream);
+    case 2: return launch_kind_2(p, precision, grid, block, stream);
+    default: return launch_kind_3(p, precision, grid, block, stream);
+    }
+}
+
+size_t spec_bytes_per_warp(int precision, int np) {
+    return precision == RTW_PREC_MIXED ? (size_t)3 * 32 * np * sizeof(float) : (size_t)2 * 32 * np * sizeof(double);
+}
+
+cudaError_t trace_attributes(int kind, int precision, int np, cudaFuncAttributes* attr) {
+    return cudaFuncGetAttributes(attr, kernel_ptr(kind, precision, np));
+}
+
+namespace {
+
+constexpr double kPi = 3.141592653589793;
+constexpr double kNoDivZero = 1e-24;
+constexpr double kLightC = 299792458.0;
+
+typedef double M4[4][4];
+
+void mul4(const M4 a, const M4 b, M4 c) {
+    M4 t;
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) {
+            double s = 0;
+            for (int k = 0; k < 4; ++k) s += a[i][k] * b[k][j];
+            t[i][j] = s;
+        }
+    std::memcpy(c, t, sizeof(M4));
+}
+
+// roll-pitch-yaw R_z R_y R_x (gen_geometry.jl:9-40)
+void rot_intrinsic(const double* p, M4 out) {
+    M4 rx = {{0}}, ry = {{0}}, rz = {{0}}, t;
+    const double c0 = std::cos(p[0]), s0 = std::sin(p[0]);
+    const double c1 = std::cos(p[1]), s1 = std::sin(p[1]);
+    const double c2 = std::cos(p[2]), s2 = std::sin(p[2]);
+    rx[0][0] = 1; rx[1][1] = 1; rx[2][2] = c0; rx[3][2] = s0; rx[2][3] = -s0; rx[3][3] = c0;
+    ry[0][0] = 1; ry[1][1] = c1; ry[3][1] = -s1; ry[2][2] = 1; ry[1][3] = s1; ry[3][3] = c1;
+    rz[0][0] = 1; rz[1][1] = c2; rz[2][1] = s2; rz[1][2] = -s2; rz[2][2] = c2; rz[3][3] = 1;
+    mul4(rz, ry, t);
+    mul4(t, rx, out);
+}
+
+// rotation of the tetrad axes onto the velocity direction, Rodrigues form,
+// transposed, then the yaw fix pi/2 + direction[2] (gen_geometry.jl:47-87)
+void rot_final(const double* dir, M4 out) {
+    const double d0 = std::sin(dir[0]) * std::cos(dir[1]);
+    const double d1 = std::sin(dir[0]) * std::sin(dir[1]);
+    double kx = -d1, ky = d0, kz = 0.0;  // (0,0,1) x d
+    const double mag = std::sqrt(kx * kx + ky * ky + kz * kz);
+    const double yaw[3] = {0, 0, kPi / 2 + dir[1]};
+    M4 ry;
+    rot_intrinsic(yaw, ry);
+    if (!(mag > 0)) {
+        std::memcpy(out, ry, sizeof(M4));
+        return;
+    }
+    kx /= mag; ky /= mag; kz /= mag;
+    const double K[3][3] = {{0, -kz, ky}, {kz, 0, -kx}, {-ky, kx, 0}};
+    const double sa = std::sin(dir[0]), ca = 1 - std::cos(dir[0]);
+    M4 r4 = {{0}};
+    r4[0][0] = 1;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            double kk = 0;
+            for (int m = 0; m < 3; ++m) kk += K[i][m] * K[m][j];
+            // stored transposed
+            r4[1 + j][1 + i] = (i == j ? 1.0 : 0.0) + sa * K[i][j] + ca * kk;
+        }
+    mul4(r4, ry, out);
+}
+
+// z boost (gen_geometry.jl:93-103)
+void boost(double beta, M4 out) {
+    std::memset(out, 0, sizeof(M4));
+    const double g = 1 / std::sqrt(1 - beta * beta);
+    out[0][0] = g; out[3][0] = -beta * g; out[0][3] = -beta * g;
+    out[1][1] = 1; out[2][2] = 1; out[3][3] = g;
+}
+
+bool is_kerr(int kind) { return kind == RTW_SCENE_KERR_DISK || kind == RTW_SCENE_KERR_THICK_DISK; }
+
+double horizon_radius(const rtw_scene& s) {
+    if (is_kerr(s.kind)) return s.mass + std::sqrt(s.mass * s.mass - s.spin * s.spin);
+    if (s.kind == RTW_SCENE_SCHWARZSCHILD_DISK) return 2 * s.mass;
+    return 0.0;
+}
+
+// inverse tetrad at the camera (calc_inv_vierbein of each scene)
+void inv_tetrad(const rtw_scene& s, const double* x, M4 e) {
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) e[i][j] = i == j ? 1.0 : 0.0;
+    const double r = x[1], th = x[2];
+    if (is_kerr(s.kind)) {
+        const double a = s.spin, rs = 2 * s.mass;
+        const double sig = r * r + (a * std::cos(th)) * (a * std::cos(th));
+        const double del = r * r - r * rs + a * a;
+        const double A = (r * r + a * a) * sig + rs * r * (a * std::sin(th)) * (a * std::sin(th));
+        e[0][0] = std::sqrt(A / (sig * del));
+        e[3][0] = (rs * a * r / A) * e[0][0];
+        e[1][1] = std::sqrt(del / sig);
+        e[2][2] = 1 / std::sqrt(sig);
+        e[3][3] = std::sqrt(sig / A) / std::sin(th);
+    } else if (s.kind == RTW_SCENE_SCHWARZSCHILD_DISK) {
+        const double rs = 2 * s.mass;
+        e[0][0] = 1 / std::sqrt(1 - rs / r);
+        e[1][1] = std::sqrt(1 - rs / r);
+        e[2][2] = 1 / r;
+        e[3][3] = 1 / (r * std::sin(th) + kNoDivZero);
+    } else {
+        e[2][2] = 1 / (r + kNoDivZero);
+        e[3][3] = 1 / (r * std::sin(th) + kNoDivZero);
+    }
+}
+
+bool on_singularity(const double* pos) {
+    return std::fabs(pos[1]) <= (double)1e-32f || std::fabs(pos[2]) <= (double)1e-32f || std::fabs(pos[2] - kPi) <= 1e-32;
+}
+
+// Bardeen-Press-Teukolsky ISCO with the exponents of Kerr.source/source_geometry.jl:20-37
+double reference_isco(double M, double a) {
+    const double chi = a / M;
+    const double z1 = 1 + std::cbrt(1 - chi * chi) * (std::pow(1 + chi, 1.5) + std::pow(1 - chi, 1.5));
+    const double z2 = std::sqrt(3 * chi * chi + z1 * z1);
+    return (double)(float)(M * (3 + z2 - std::sqrt((3 - z1) * (3 + z1 + 2 * z2))));
+}
+
+const double kCie[4][7] = {
+    {0.362, 1.056, -0.065, 0.821, 0.286, 1.217, 0.681},
+    {442.0, 599.8, 501.1, 568.8, 530.9, 437.0, 459.0},
+    {0.0624, 0.0264, 0.0490, 0.0213, 0.0613, 0.0845, 0.0385},
+    {0.0374, 0.0323, 0.0382, 0.0247, 0.0322, 0.0278, 0.0725}};
+
+// multi-lobe Gaussian CIE fit (color_theory.jl:11-61)
+double cie_fit(double wl, int first, int count) {
+    double v = 0;
+    for (int i = first; i < first + count; ++i) {
+        const double d = wl - kCie[1][i];
+        const double inv_w = d >= 0 ? kCie[3][i] : kCie[2][i];
+        v += kCie[0][i] * std::exp(-0.5 * (d * inv_w) * (d * inv_w));
+    }
+    return v;
+}
+
+}  // namespace
+}  // namespace rtw
+
+using namespace rtw;
+
+struct rtw_ctx {
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    void* d_frames = nullptr;
+    size_t frames_cap = 0;
+    double* d_bins = nullptr;
+    unsigned long long* d_ctl = nullptr;  // [0] work counter, then DevStats
+    void* d_spec = nullptr;
+    size_t spec_cap = 0;
+    void* d_out = nullptr;
+    size_t out_cap = 0;
+    float* d_sink = nullptr;
+    std::string err;
+    rtw_stats last{};
+    bool have_last = false;
+};
+
+namespace {
+
+rtw_status fail(rtw_ctx* ctx, rtw_status st, const std::string& msg) {
+    if (ctx) ctx->err = msg;
+    return st;
+}
+
+rtw_status cuda_fail(rtw_ctx* ctx, cudaError_t e, const char* what) {
+    return fail(ctx, RTW_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define RTW_CUDA(call, what)                              \
+    do {                                                  \
+        cudaError_t e_ = (call);                          \
+        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, what); \
+    } while (0)
+
+rtw_status ensure(rtw_ctx* ctx, void** ptr, size_t* cap, size_t need) {
+    if (need <= *cap && *ptr) return RTW_OK;
+    if (*ptr) cudaFree(*ptr);
+    *ptr = nullptr;
+    *cap = 0;
+    cudaError_t e = cudaMalloc(ptr, need);
+    if (e != cudaSuccess) {
+        *ptr = nullptr;
+        return fail(ctx, RTW_ERR_OOM, std::string("cudaMalloc failed: ") + cudaGetErrorString(e));
+    }
+    *cap = need;
+    return RTW_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t rtw_abi_version(void) { return RTW_ABI_VERSION; }
+
+rtw_status rtw_create(rtw_ctx** out, int32_t device) {
+    if (!out) return RTW_ERR_INVALID_PARAM;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) return RTW_ERR_NO_DEVICE;
+    if (device < 0 || device >= n) return RTW_ERR_INVALID_PARAM;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return RTW_ERR_NO_DEVICE;
+    if (prop.major != 10) return RTW_ERR_NO_DEVICE;  // built for sm_100a only
+    if (cudaSetDevice(device) != cudaSuccess) return RTW_ERR_CUDA;
+    rtw_ctx* ctx = new rtw_ctx();
+    ctx->device = device;
+    ctx->num_sms = prop.multiProcessorCount;
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete ctx;
+        return RTW_ERR_CUDA;
+    }
+    for (auto& e : ctx->ev) cudaEventCreate(&e);
+    if (cudaMalloc((void**)&ctx->d_ctl, 256) != cudaSuccess || cudaMalloc((void**)&ctx->d_bins, 4 * RTW_MAX_BINS * sizeof(double)) != cudaSuccess) {
+        rtw_destroy(ctx);
+        return RTW_ERR_OOM;
+    }
+    *out = ctx;
+    return RTW_OK;
+}
+
+void rtw_destroy(rtw_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    cudaFree(ctx->d_frames);
+    cudaFree(ctx->d_bins);
+    cudaFree(ctx->d_ctl);
+    cudaFree(ctx->d_spec);
+    cudaFree(ctx->d_out);
+    cudaFree(ctx->d_sink);
+    for (auto& e : ctx->ev)
+        if (e) cudaEventDestroy(e);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+const char* rtw_last_error(const rtw_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+rtw_status rtw_scene_default(int32_t kind, rtw_scene* s) {
+    if (!s) return RTW_ERR_INVALID_PARAM;
+    std::memset(s, 0, sizeof(*s));
+    s->kind = kind;
+    s->mass = 1.0;
+    s->escape_radius = 100.0;
+    s->winding_limit = 8 * kPi;
+    s->rho_r0 = 6.0;
+    s->rho_h = 0.1;
+    s->rho_index = -2.0;
+    s->t_index = -0.75;
+    s->theta_lo = 0;
+    s->theta_hi = kPi;
+    switch (kind) {
+    case RTW_SCENE_MINKOWSKI_SPHERE:  // Minkowski_Sphere_Spherical.source/source_model.jl:44-83
+        s->r_in = 0; s->r_out = 1; s->temperature = 5778; s->a_nu = 1;
+        break;
+    case RTW_SCENE_SCHWARZSCHILD_DISK:  // Schwarzschild ... source_model.jl:44-80
+        s->r_in = 6; s->r_out = 12; s->theta_lo = 15 * kPi / 32; s->theta_hi = 17 * kPi / 32;
+        s->temperature = 5778; s->a_nu = 1;
+        break;
+    case RTW_SCENE_KERR_DISK:  // Kerr.source: source_geometry.jl:13, source_model.jl:44-80
+        s->spin = (double)0.998f;
+        s->r_in = reference_isco(1.0, s->spin); s->r_out = 12;
+        s->theta_lo = 31 * kPi / 64; s->theta_hi = 33 * kPi / 64;
+        s->temperature = 5778; s->a_nu = (double)1e-1f;
+        break;
+    case RTW_SCENE_KERR_THICK_DISK:
+        s->spin = 0.9;
+        s->r_in = 2.320883041761887;  // prograde ISCO of a = 0.9
+        s->r_out = 30; s->temperature = 1e4; s->a_nu = 0.05;
+        break;
+    default:
+        return RTW_ERR_INVALID_PARAM;
+    }
+    return RTW_OK;
+}
+
+rtw_status rtw_camera_pixels(rtw_camera* cam, int64_t* n_pix) {
+    if (!cam || cam->x_pix <= 0 || !(cam->fov_hor > 0 && cam->fov_hor < 180) || !(cam->fov_vert > 0 && cam->fov_vert < 180))
+        return RTW_ERR_INVALID_PARAM;
+    const double W = std::tan(kPi * cam->fov_hor / 180 / 2), H = std::tan(kPi * cam->fov_vert / 180 / 2);
+    const double yp = std::nearbyint(cam->x_pix * H / W);
+    if (!(yp >= 1 && yp < 1e9)) return RTW_ERR_INVALID_PARAM;
+    cam->y_pix = (int32_t)yp;
+    if (n_pix) *n_pix = (int64_t)cam->x_pix * cam->y_pix;
+    return RTW_OK;
+}
+
+static rtw_status build_frame(const rtw_scene& s, rtw_camera& cam, FrameDesc& f) {
+    rtw_status st = rtw_camera_pixels(&cam, nullptr);
+    if (st != RTW_OK) return st;
+    if (on_singularity(cam.position)) return RTW_ERR_INVALID_CAMERA;
+    if (!(std::fabs(cam.speed) < 1)) return RTW_ERR_INVALID_PARAM;
+    const double fh = kPi * cam.fov_hor / 180, fv = kPi * cam.fov_vert / 180;
+    f.W = std::tan(fh / 2);
+    f.H = std::tan(fv / 2);
+    f.xp = cam.x_pix;
+    f.yp = cam.y_pix;
+    f.rh = 2 * f.W / (f.xp + 1);
+    f.rv = 2 * f.H / (f.yp + 1);
+    M4 R, L, R2, e, t1, t2, M;
+    rot_intrinsic(cam.pointing, R);
+    boost(-cam.speed, L);
+    rot_final(cam.direction, R2);
+    inv_tetrad(s, cam.position, e);
+    mul4(e, R2, t1);
+    mul4(t1, L, t2);
+    mul4(t2, R, M);
+    for (int i = 0; i < 4; ++i) f.pos[i] = cam.position[i];
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) {
+            f.M[4 * i + j] = M[i][j];
+            if (!std::isfinite(M[i][j])) return RTW_ERR_NAN;
+        }
+    if (!(cam.tolerance > 0 && cam.tolerance < 1) || cam.max_steps <= 0) return RTW_ERR_INVALID_PARAM;
+    f.tol = cam.tolerance;
+    f.r_term = (1 + 10 * cam.tolerance) * horizon_radius(s);
+    f.thick = -std::log(cam.tolerance);
+    f.max_steps = cam.max_steps;
+    return RTW_OK;
+}
+
+rtw_status rtw_camera_rays(const rtw_scene* scene, const rtw_camera* camin, double* rays, int64_t n_pix) {
+    if (!scene || !camin || !rays) return RTW_ERR_INVALID_PARAM;
+    rtw_camera cam = *camin;
+    FrameDesc f;
+    rtw_status st = build_frame(*scene, cam, f);
+    if (st != RTW_OK) return st;
+    if ((int64_t)f.xp * f.yp != n_pix) return RTW_ERR_INVALID_PARAM;
+    for (int j = 0; j < f.yp; ++j)
+        for (int i = 0; i < f.xp; ++i) {
+            double* S = rays + 8 * ((int64_t)i + (int64_t)f.xp * j);
+            const double w = f.rh * ((i + 1) - 0.5) - f.W;
+            const double hh = f.rv * ((j + 1) - 0.5) - f.H;
+            const double th = std::atan(std::sqrt(w * w + hh * hh));
+            double ph;
+            if (w > 0) ph = std::atan(hh / w);
+            else if (w < 0 && hh >= 0) ph = std::atan(hh / w) + kPi;
+            else if (w < 0 && hh < 0) ph = std::atan(hh / w) - kPi;
+            else if (w == 0 && hh > 0) ph = kPi / 2;
+            else if (w == 0 && hh < 0) ph = -kPi / 2;
+            else ph = 0;
+            const double v[4] = {1, -std::sin(th) * std::cos(ph), -std::sin(th) * std::sin(ph), -std::cos(th)};
+            for (int k = 0; k < 4; ++k) S[k] = f.pos[k];
+            for (int r = 0; r < 4; ++r) {
+                double acc = 0;
+                for (int k = 0; k < 4; ++k) acc += f.M[4 * r + k] * v[k];
+                S[4 + r] = acc;
+            }
+        }
+    return RTW_OK;
+}
+
+rtw_status rtw_cie_weights(const double* colors, int32_t n, double* wx, double* wy, double* wz, double* fac) {
+    if (!colors || n <= 0 || n > RTW_MAX_BINS) return RTW_ERR_INVALID_PARAM;
+    for (int i = 0; i < n; ++i)
+        if (!(colors[i] > 0)) return RTW_ERR_INVALID_PARAM;
+    for (int i = 0; i < n; ++i) {
+        double w;
+        if (n == 1) w = 1.0;
+        else if (i == 0) w = (colors[1] - colors[0]) / 2;
+        else if (i == n - 1) w = (colors[n - 1] - colors[n - 2]) / 2;
+        else w = (colors[i + 1] - colors[i - 1]) / 2;
+        if (wx) wx[i] = cie_fit(colors[i], 0, 3) * w;
+        if (wy) wy[i] = cie_fit(colors[i], 3, 2) * w;
+        if (wz) wz[i] = cie_fit(colors[i], 5, 2) * w;
+        const double nu = 1.0 / colors[i];
+        if (fac) fac[i] = nu * nu * nu * kLightC / (colors[i] * colors[i]);
+    }
+    return RTW_OK;
+}
+
+rtw_status rtw_render(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* cams, int32_t n_cams,
+                      const rtw_render_params* prm, rtw_outputs* out) {
+    if (!ctx) return RTW_ERR_INVALID_PARAM;
+    ctx->err.clear();
+    if (!scene || !cams || !prm || !out) return fail(ctx, RTW_ERR_INVALID_PARAM, "null argument");
+    if (n_cams <= 0 || n_cams > RTW_MAX_FRAMES) return fail(ctx, RTW_ERR_INVALID_PARAM, "n_cams out of range");
+    if (prm->n_colors <= 0 || prm->n_colors > RTW_MAX_BINS || !prm->colors_nm)
+        return fail(ctx, RTW_ERR_INVALID_PARAM, "n_colors must be 1..128 with colors_nm set");
+    if (prm->ray_bundles) return fail(ctx, RTW_ERR_UNSUPPORTED, "ray bundles are not built");
+    if (scene->ref_precision) return fail(ctx, RTW_ERR_UNSUPPORTED, "ref_precision is an oracle-only switch");
+    if (prm->precision != RTW_PREC_FP64 && prm->precision != RTW_PREC_MIXED)
+        return fail(ctx, RTW_ERR_INVALID_PARAM, "precision");
+    if (prm->integrator != RTW_DP45_REF_COMPAT && prm->integrator != RTW_DP45_FSAL)
+        return fail(ctx, RTW_ERR_INVALID_PARAM, "integrator");
+    if (scene->kind < 0 || scene->kind > RTW_SCENE_KERR_THICK_DISK) return fail(ctx, RTW_ERR_INVALID_PARAM, "scene kind");
+    if (!(prm->max_dt_scale > 0)) return fail(ctx, RTW_ERR_INVALID_PARAM, "max_dt_scale must be > 0");
+    if (is_kerr(scene->kind) && !(std::fabs(scene->spin) < scene->mass))
+        return fail(ctx, RTW_ERR_INVALID_PARAM, "Kerr spin must satisfy |a| < M");
+    if (!(scene->mass > 0)) return fail(ctx, RTW_ERR_INVALID_PARAM, "mass must be > 0");
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, RTW_ERR_CUDA, "cudaSetDevice");
+    cudaStream_t st = prm->stream ? (cudaStream_t)prm->stream : ctx->stream;
+
+    // frames
+    std::vector<FrameDesc> frames(n_cams);
+    long long total = 0;
+    for (int f = 0; f < n_cams; ++f) {
+        rtw_camera cam = cams[f];
+        rtw_status s = build_frame(*scene, cam, frames[f]);
+        if (s == RTW_ERR_INVALID_CAMERA) return fail(ctx, s, "camera " + std::to_string(f) + " is on a coordinate singularity");
+        if (s != RTW_OK) return fail(ctx, s, "camera " + std::to_string(f) + " parameters invalid or non-finite");
+        frames[f].ray_begin = total;
+        total += (long long)frames[f].xp * frames[f].yp;
+    }
+    // bins
+    const int N = prm->n_colors;
+    std::vector<double> bins(4 * RTW_MAX_BINS, 0.0);
+    std::vector<double> wx(N), wy(N), wz(N), fac(N);
+    if (rtw_cie_weights(prm->colors_nm, N, wx.data(), wy.data(), wz.data(), fac.data()) != RTW_OK)
+        return fail(ctx, RTW_ERR_INVALID_PARAM, "colors_nm must be positive");
+    for (int c = 0; c < N; ++c) {
+        bins[c] = 1.0 / prm->colors_nm[c];
+        bins[RTW_MAX_BINS + c] = fac[c] * wx[c];
+        bins[2 * RTW_MAX_BINS + c] = fac[c] * wy[c];
+        bins[3 * RTW_MAX_BINS + c] = fac[c] * wz[c];
+    }
+    const int np = N <= 32 ? 32 : (N <= 64 ? 64 : 128);
+
+    // launch shape
+    const int warps = prm->block_warps > 0 ? std::min(prm->block_warps, 8) : 4;
+    const int block = 32 * warps;
+    int per_sm = prm->ctas_per_sm;
+    if (per_sm <= 0) {
+        int occ = 0;
+        RTW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel_ptr(scene->kind, prm->precision, np), block, 0),
+                 "occupancy query");
+        per_sm = std::max(1, occ);
+    }
+    const int grid = ctx->num_sms * per_sm;
+    const size_t spec_need = (size_t)grid * warps * spec_bytes_per_warp(prm->precision, np);
+
+    rtw_status s;
+    if ((s = ensure(ctx, &ctx->d_frames, &ctx->frames_cap, sizeof(FrameDesc) * n_cams)) != RTW_OK) return s;
+    if ((s = ensure(ctx, &ctx->d_spec, &ctx->spec_cap, spec_need)) != RTW_OK) return s;
+
+    // outputs
+    float* xyz = out->xyz;
+    uint8_t* cls = out->term_class;
+    uint32_t* steps = out->steps;
+    float* spectrum = out->spectrum;
+    double* fstate = out->final_state;
+    float* tau = out->tau;
+    size_t off_xyz = 0, off_cls = 0, off_steps = 0, off_spec = 0, off_state = 0, off_tau = 0;
+    if (!out->on_device) {
+        size_t o = 0;
+        auto take = [&](bool want, size_t bytes, size_t& off) {
+            if (want) {
+                off = o;
+                o += (bytes + 255) & ~(size_t)255;
+            }
+        };
+        take(xyz != nullptr, sizeof(float) * 3 * total, off_xyz);
+        take(cls != nullptr, sizeof(uint8_t) * total, off_cls);
+        take(steps != nullptr, sizeof(uint32_t) * total, off_steps);
+        take(spectrum != nullptr, sizeof(float) * N * total, off_spec);
+        take(fstate != nullptr, sizeof(double) * 8 * total, off_state);
+        take(tau != nullptr, sizeof(float) * total, off_tau);
+        if ((s = ensure(ctx, &ctx->d_out, &ctx->out_cap, std::max<size_t>(o, 256))) != RTW_OK) return s;
+        char* base = (char*)ctx->d_out;
+        xyz = xyz ? (float*)(base + off_xyz) : nullptr;
+        cls = cls ? (uint8_t*)(base + off_cls) : nullptr;
+        steps = steps ? (uint32_t*)(base + off_steps) : nullptr;
+        spectrum = spectrum ? (float*)(base + off_spec) : nullptr;
+        fstate = fstate ? (double*)(base + off_state) : nullptr;
+        tau = tau ? (float*)(base + off_tau) : nullptr;
+    }
+
+    KParams p;
+    std::memset(&p, 0, sizeof(p));
+    DevScene& d = p.sc;
+    d.kind = scene->kind;
+    d.refprec = 0;
+    d.M = scene->mass;
+    d.a = is_kerr(scene->kind) ? scene->spin : 0.0;
+    d.rs = 2 * scene->mass;
+    d.r_ev = horizon_radius(*scene);
+    d.r_in = scene->r_in; d.r_out = scene->r_out;
+    d.th_lo = scene->theta_lo; d.th_hi = scene->theta_hi;
+    d.T = scene->temperature; d.anu = scene->a_nu;
+    d.esc = scene->escape_radius; d.wind = scene->winding_limit;
+    d.rho_r0 = scene->rho_r0; d.rho_h = scene->rho_h; d.rho_idx = scene->rho_index; d.t_idx = scene->t_index;
+    d.sqrtM = std::sqrt(scene->mass);
+    d.r_pm = is_kerr(scene->kind) ? 2 * std::sqrt(scene->mass * scene->mass - scene->spin * scene->spin) : 0.0;
+    p.frames = (const FrameDesc*)ctx->d_frames;
+    p.n_frames = n_cams;
+    p.n_bins = N;
+    p.total_rays = total;
+    p.max_dt_scale = prm->max_dt_scale;
+    // promotion thresholds: < 0 disables, 0 takes the default
+    const double pdr = prm->promote_dr < 0 ? -1.0 : (prm->promote_dr > 0 ? prm->promote_dr : 1e-4);
+    const double psn = prm->promote_sin < 0 ? 0.0 : (prm->promote_sin > 0 ? std::min(prm->promote_sin, 1.0) : 1e-3);
+    p.promote_dr = pdr * scene->mass;
+    p.promote_theta = std::asin(psn);
+    p.fsal = prm->integrator == RTW_DP45_FSAL;
+    p.pixel_order = prm->pixel_order;
+    p.bin_nu = ctx->d_bins;
+    p.bin_fx = ctx->d_bins + RTW_MAX_BINS;
+    p.bin_fy = ctx->d_bins + 2 * RTW_MAX_BINS;
+    p.bin_fz = ctx->d_bins + 3 * RTW_MAX_BINS;
+    p.spec = ctx->d_spec;
+    p.np = np;
+    p.counter = ctx->d_ctl;
+    p.stats = (DevStats*)(ctx->d_ctl + 1);
+    p.xyz = xyz; p.cls = cls; p.steps = steps; p.spectrum = spectrum; p.final_state = fstate; p.tau = tau;
+
+    RTW_CUDA(cudaEventRecord(ctx->ev[0], st), "event");
+    RTW_CUDA(cudaMemcpyAsync(ctx->d_frames, frames.data(), sizeof(FrameDesc) * n_cams, cudaMemcpyHostToDevice, st), "frames H2D");
+    RTW_CUDA(cudaMemcpyAsync(ctx->d_bins, bins.data(), sizeof(double) * 4 * RTW_MAX_BINS, cudaMemcpyHostToDevice, st), "bins H2D");
+    RTW_CUDA(cudaMemsetAsync(ctx->d_ctl, 0, sizeof(unsigned long long) + sizeof(DevStats), st), "reset counters");
+    RTW_CUDA(cudaEventRecord(ctx->ev[1], st), "event");
+    RTW_CUDA(launch_trace(p, prm->precision, grid, block, st), "trace kernel launch");
+    RTW_CUDA(cudaEventRecord(ctx->ev[2], st), "event");
+    if (!out->on_device) {
+        if (out->xyz) RTW_CUDA(cudaMemcpyAsync(out->xyz, xyz, sizeof(float) * 3 * total, cudaMemcpyDeviceToHost, st), "xyz D2H");
+        if (out->term_class) RTW_CUDA(cudaMemcpyAsync(out->term_class, cls, total, cudaMemcpyDeviceToHost, st), "class D2H");
+        if (out->steps) RTW_CUDA(cudaMemcpyAsync(out->steps, steps, sizeof(uint32_t) * total, cudaMemcpyDeviceToHost, st), "steps D2H");
+        if (out->spectrum) RTW_CUDA(cudaMemcpyAsync(out->spectrum, spectrum, sizeof(float) * N * total, cudaMemcpyDeviceToHost, st), "spectrum D2H");
+        if (out->final_state) RTW_CUDA(cudaMemcpyAsync(out->final_state, fstate, sizeof(double) * 8 * total, cudaMemcpyDeviceToHost, st), "state D2H");
+        if (out->tau) RTW_CUDA(cudaMemcpyAsync(out->tau, tau, sizeof(float) * total, cudaMemcpyDeviceToHost, st), "tau D2H");
+    }
+    RTW_CUDA(cudaEventRecord(ctx->ev[3], st), "event");
+    ctx->have_last = true;
+    std::memset(&ctx->last, 0, sizeof(ctx->last));
+    ctx->last.rays = (uint64_t)total;
+    if (!prm->stream) {
+        RTW_CUDA(cudaStreamSynchronize(st), "trace kernel");
+    }
+    return RTW_OK;
+}
+
+rtw_status rtw_get_stats(rtw_ctx* ctx, rtw_stats* out) {
+    if (!ctx || !out) return RTW_ERR_INVALID_PARAM;
+    if (!ctx->have_last) return fail(ctx, RTW_ERR_INVALID_PARAM, "no render yet");
+    RTW_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    RTW_CUDA(cudaEventSynchronize(ctx->ev[3]), "sync");
+    DevStats ds;
+    RTW_CUDA(cudaMemcpy(&ds, ctx->d_ctl + 1, sizeof(ds), cudaMemcpyDeviceToHost), "stats D2H");
+    float k = 0, t = 0;
+    cudaEventElapsedTime(&k, ctx->ev[1], ctx->ev[2]);
+    cudaEventElapsedTime(&t, ctx->ev[0], ctx->ev[3]);
+    out->rays = ds.rays;
+    out->step_attempts = ds.step_attempts;
+    out->rejected_steps = ds.rejected_steps;
+    out->promoted_steps = ds.promoted_steps;
+    out->spectral_steps = ds.spectral_steps;
+    out->emitting_steps = ds.emitting_steps;
+    out->escape_substeps = ds.escape_substeps;
+    out->nan_rays = ds.nan_rays;
+    out->kernel_ms = k;
+    out->total_ms = t;
+    return RTW_OK;
+}
+
+rtw_status rtw_measure_peaks(rtw_ctx* ctx, double* fp32, double* fp64, double* mufu) {
+    if (!ctx) return RTW_ERR_INVALID_PARAM;
+    RTW_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    if (!ctx->d_sink) RTW_CUDA(cudaMalloc((void**)&ctx->d_sink, 64), "sink");
+    const int block = 256, grid = ctx->num_sms * 8;
+    double* outs[3] = {fp32, fp64, mufu};
+    const int iters[3] = {4096, 1024, 1024};
+    for (int w = 0; w < 3; ++w) {
+        // warm-up
+        RTW_CUDA(launch_peak_probe(w, grid, block, 16, ctx->d_sink, ctx->stream), "probe");
+        RTW_CUDA(cudaEventRecord(ctx->ev[0], ctx->stream), "event");
+        RTW_CUDA(launch_peak_probe(w, grid, block, iters[w], ctx->d_sink, ctx->stream), "probe");
+        RTW_CUDA(cudaEventRecord(ctx->ev[1], ctx->stream), "event");
+        RTW_CUDA(cudaEventSynchronize(ctx->ev[1]), "probe sync");
+        float ms = 0;
+        cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]);
+        const double ops = (double)grid * block * iters[w] * 16 * 8;
+        const double per = (w == 2) ? 1.0 : 2.0;  // FMA = 2 flops
+        if (outs[w]) *outs[w] = ops * per / (ms * 1e-3);
+    }
+    ctx->have_last = false;
+    return RTW_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,93 @@
+// rtw_internal.h - types shared by the host side of the C ABI and the trace
+// kernels (not part of the public ABI).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/rtw.h"
+
+namespace rtw {
+
+// One frame (camera) of a batched render: the FP64 camera transform of
+// initialize_camera (initialization.jl:190-331) reduced to what a pixel needs.
+struct FrameDesc {
+    double pos[4];       // camera 4-position
+    double M[16];        // row-major e * R2 * L * R (initialization.jl:254-260,327)
+    double W, H;         // canvas half extents tan(fov/2)
+    double rh, rv;       // inverse pixel densities (initialization.jl:202-203)
+    double tol;          // abs_tol = rel_tol
+    double r_term;       // horizon termination radius (1 + 10 tol) r_horizon
+    double thick;        // -log(tol): optically thick threshold
+    long long ray_begin; // first global ray id of this frame
+    long long max_steps;
+    int xp, yp;
+};
+
+// Scene constants in the form the device functors use.
+struct DevScene {
+    int kind;
+    int refprec;
+    double M, a, rs, r_ev;
+    double r_in, r_out, th_lo, th_hi;
+    double T, anu, esc, wind;
+    double rho_r0, rho_h, rho_idx, t_idx;
+    double sqrtM;
+    double r_pm;  // r+ - r- (Kerr), rs (Schwarzschild: Delta/r = r - rs), 0 (flat)
+};
+
+// Counters one render accumulates on the device (rtw_stats).
+struct DevStats {
+    unsigned long long step_attempts;
+    unsigned long long rejected_steps;
+    unsigned long long promoted_steps;
+    unsigned long long spectral_steps;
+    unsigned long long emitting_steps;
+    unsigned long long escape_substeps;
+    unsigned long long nan_rays;
+    unsigned long long rays;
+};
+
+struct KParams {
+    DevScene sc;
+    const FrameDesc* frames;
+    int n_frames;
+    int n_bins;
+    long long total_rays;
+    double max_dt_scale;
+    double promote_dr;     // MIXED: FP64 stages while r - r_horizon < promote_dr
+    double promote_theta;  // MIXED: FP64 stages while theta < promote_theta or > pi - promote_theta
+    int fsal;
+    int pixel_order;
+    // per-bin tables, [n_bins]: observed frequency (nm^-1) and the factors
+    // nu^3 c / lambda^2 * W_{X,Y,Z} of the XYZ epilogue
+    const double* bin_nu;
+    const double* bin_fx;
+    const double* bin_fy;
+    const double* bin_fz;
+    // spectral scratch: per warp [32 rays][np] for each field
+    void* spec;
+    int np;                      // padded bins per ray row (32 * bins per lane)
+    unsigned long long* counter; // work queue head
+    DevStats* stats;
+    // outputs (device pointers; may be null)
+    float* xyz;
+    uint8_t* cls;
+    uint32_t* steps;
+    float* spectrum;
+    double* final_state;
+    float* tau;
+};
+
+// Launches the trace kernel for p.sc.kind / precision on `stream`.
+// Returns cudaSuccess or the launch error.
+cudaError_t launch_trace(const KParams& p, int precision, int grid, int block, cudaStream_t stream);
+// Bytes of spectral scratch per warp for a precision and padded bin count.
+size_t spec_bytes_per_warp(int precision, int np);
+// Registers / max threads of the kernel that launch_trace would run.
+cudaError_t trace_attributes(int kind, int precision, int np, cudaFuncAttributes* attr);
+
+// Issue-rate microbenchmarks (rtw_measure_peaks).
+cudaError_t launch_peak_probe(int which, int grid, int block, int iters, float* sink, cudaStream_t stream);
+
+}  // namespace rtw

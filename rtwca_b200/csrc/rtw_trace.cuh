@@ -1,0 +1,640 @@
+// rtw_trace.cuh - the persistent trace kernel.
+//
+// Work decomposition (B200-first, not the reference's one-thread-per-pixel
+// grid-stride loop of 5P.jl:73-99):
+//  * A persistent grid; each warp owns 32 ray slots, one per lane. Lanes whose
+//    ray terminated take the next rays from a global work counter with one
+//    warp-aggregated atomic (ballot + popc), so warps stay full until the
+//    queue drains (compaction by refill).
+//  * Geodesic phase, one lane per ray: one adaptive Dormand-Prince attempt
+//    (RKDP_Step_w_buffer!, integrators_LttM.jl:54-224) over the 8 geodesic
+//    components plus the common optical depth tau (the emitters are grey, so
+//    every tau slot of the reference's state is the same number). The seven
+//    right-hand sides also yield the emitter numbers (A, X) of every stage.
+//  * Spectral phase, warp-cooperative: for every ray of the warp whose
+//    spectral slots change in this attempt (emission in a stage, or a
+//    nonzero carried slope), the 32 lanes split its spectral bins, compute
+//    the six new stage slopes of each bin, the 5th-order update and the
+//    embedded error, reduce the error over the warp, and commit the bins if
+//    the attempt is accepted. The per-bin state (intensity, carried slope)
+//    lives in a per-warp scratch area [32 rays][np], read and written
+//    coalesced along the bins.
+//  * The step controller, termination test and the XYZ epilogue (a warp
+//    reduction over bins) follow.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "rtw_internal.h"
+#include "rtw_scenes.cuh"
+
+namespace rtw {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+// Dormand-Prince coefficients (64BitConstants.jl:28-37)
+constexpr double a21 = 1.0 / 5;
+constexpr double a31 = 3.0 / 40, a32 = 9.0 / 40;
+constexpr double a41 = 44.0 / 45, a42 = -56.0 / 15, a43 = 32.0 / 9;
+constexpr double a51 = 19372.0 / 6561, a52 = -25360.0 / 2187, a53 = 64448.0 / 6561, a54 = -212.0 / 729;
+constexpr double a61 = 9017.0 / 3168, a62 = -355.0 / 33, a63 = 46732.0 / 5247, a64 = 49.0 / 176,
+                 a65 = -5103.0 / 18656;
+constexpr double b1 = 35.0 / 384, b3 = 500.0 / 1113, b4 = 125.0 / 192, b5 = -2187.0 / 6784, b6 = 11.0 / 84;
+constexpr double bs1 = 5179.0 / 57600, bs3 = 7571.0 / 16695, bs4 = 393.0 / 640, bs5 = -92097.0 / 339200,
+                 bs6 = 187.0 / 2100, bs7 = 1.0 / 40;
+constexpr double e1 = b1 - bs1, e3 = b3 - bs3, e4 = b4 - bs4, e5 = b5 - bs5, e6 = b6 - bs6, e7 = -bs7;
+
+// Spectral scratch layout of one warp: for each field, [32 rays][np] values of
+// type SR. Fields: 0 = intensity (high part), 1 = carried slope k1,
+// 2 = intensity low part (MIXED only: Kahan compensation).
+template <bool MIXED>
+struct SpecTraits;
+template <>
+struct SpecTraits<false> {
+    typedef double SR;
+    static constexpr int kFields = 2;
+};
+template <>
+struct SpecTraits<true> {
+    typedef float SR;
+    static constexpr int kFields = 3;
+};
+
+// Intensity slope of a bin: -A / (exp(X nu) - 1).
+__device__ __forceinline__ float bin_slope(float A, float X2, float nu) {
+    // X2 = X * log2(e): one MUFU ex2 per bin and stage
+    return (A == 0.0f) ? 0.0f : __fdividef(-A, exp2f(X2 * nu) - 1.0f);
+}
+__device__ __forceinline__ double bin_slope(double A, double X, double nu) {
+    return (A == 0.0) ? 0.0 : -A / (exp(X * nu) - 1.0);
+}
+template <class SR>
+__device__ __forceinline__ SR x_for_bins(SR X);
+template <>
+__device__ __forceinline__ float x_for_bins<float>(float X) { return X * 1.4426950408889634f; }
+template <>
+__device__ __forceinline__ double x_for_bins<double>(double X) { return X; }
+
+__device__ __forceinline__ float rabs(float v) { return fabsf(v); }
+__device__ __forceinline__ double rabs(double v) { return fabs(v); }
+__device__ __forceinline__ float rmax(float a, float b) { return fmaxf(a, b); }
+__device__ __forceinline__ double rmax(double a, double b) { return fmax(a, b); }
+
+// Compensated (TwoSum) add into hi/lo.
+__device__ __forceinline__ void kahan_add(float& hi, float& lo, float t) {
+    const float s = hi + t;
+    const float bp = s - hi;
+    const float err = (hi - (s - bp)) + (t - bp);
+    hi = s;
+    lo += err;
+}
+
+// Step controller of RKDP_Step_w_buffer! (integrators_LttM.jl:185-224). CT is
+// the arithmetic of the error norm: double on the FP64 path, float on the
+// mixed path (err^(-1/5) then via the MUFU log2/exp2 pair).
+__device__ __forceinline__ double err_pow(double err) { return pow(1.0 / err, 1.0 / 5); }
+__device__ __forceinline__ double err_pow(float err) { return (double)exp2f(-0.2f * __log2f(err)); }
+
+template <class CT>
+__device__ __forceinline__ void decide(CT err2, int L, double h, double max_dt, bool prev_rej, bool& accept,
+                                       double& hnext) {
+    const CT err = sqrt(err2 / CT(L));
+    double hn = 0.9 * h * err_pow(err);
+    if (fabs(hn) > max_dt) hn = -max_dt;
+    if (err == CT(0) || !isfinite(hn)) {
+        accept = true;
+        hnext = h;
+    } else if (err > CT(1)) {
+        if (prev_rej && fabs(hn) >= fabs(h)) hn = h / 2;
+        accept = false;
+        hnext = hn;
+    } else {
+        if (fabs(hn) > 5 * fabs(h)) hn = 5 * h;
+        accept = true;
+        hnext = hn;
+    }
+}
+
+// One Dormand-Prince attempt of the geodesic + tau components in arithmetic R.
+// x: FP64 state (8 geodesic + tau); k1: carried slope. Outputs the tentative
+// state y (FP64), the slope carried to the next step, the emitter numbers of
+// stages 2..7 and the un-normalised squared error (arithmetic CT) of the
+// geodesic and tau components (the tau term counted once per bin). Stage
+// vectors carry a 10th entry, r - r_horizon, formed from the FP64 state.
+template <class SC, class R, class K, class SR, class CT>
+RTW_HD void dp45_attempt(const DevScene& s, const double* x, const K* k1in, double h, double tol,
+                                             int nbins, bool fsal, double* y, K* nk1, SR* A, SR* X, CT& err2,
+                                             bool& emit) {
+    R k[7][9];
+    R xr[9], z[10], cmb[9];
+    Emit<R> em;
+    const R hr = R(h);
+    const R d0 = R(x[1] - s.r_ev);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+        k[0][i] = R(k1in[i]);
+        xr[i] = R(x[i]);
+    }
+#define RTW_STAGE(EXPR, J)                                   \
+    _Pragma("unroll") for (int i = 0; i < 9; ++i) {          \
+        cmb[i] = EXPR;                                       \
+        z[i] = xr[i] + hr * cmb[i];                          \
+    }                                                        \
+    z[9] = d0 + hr * cmb[1];                                 \
+    SC::template rhs<R>(s, z, k[J], em);                     \
+    A[J - 1] = SR(em.A);                                     \
+    X[J - 1] = SR(em.X);
+    RTW_STAGE(k[0][i] * R(a21), 1)
+    RTW_STAGE(k[0][i] * R(a31) + k[1][i] * R(a32), 2)
+    RTW_STAGE(k[0][i] * R(a41) + k[1][i] * R(a42) + k[2][i] * R(a43), 3)
+    RTW_STAGE(k[0][i] * R(a51) + k[1][i] * R(a52) + k[2][i] * R(a53) + k[3][i] * R(a54), 4)
+    RTW_STAGE(k[0][i] * R(a61) + k[1][i] * R(a62) + k[2][i] * R(a63) + k[3][i] * R(a64) + k[4][i] * R(a65), 5)
+#undef RTW_STAGE
+    R ns[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i)
+        ns[i] = k[0][i] * R(b1) + k[2][i] * R(b3) + k[3][i] * R(b4) + k[4][i] * R(b5) + k[5][i] * R(b6);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+        y[i] = x[i] + h * (double)ns[i];
+        z[i] = R(y[i]);
+    }
+    z[9] = R(y[1] - s.r_ev);
+    SC::template rhs<R>(s, z, k[6], em);
+    A[5] = SR(em.A);
+    X[5] = SR(em.X);
+    CT acc = 0;
+    const CT hc = CT(h), tc = CT(tol);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+        const R e = k[0][i] * R(e1) + k[2][i] * R(e3) + k[3][i] * R(e4) + k[4][i] * R(e5) + k[5][i] * R(e6) +
+                    k[6][i] * R(e7);
+        const CT d = hc * CT(e);
+        const CT tl = tc + cmax(cabs(CT(x[i])), cabs(CT(y[i]))) * tc;
+        const CT q = cdiv(d, tl);
+        acc += (i < 8 ? CT(1) : (CT)nbins) * q * q;
+    }
+    err2 = acc;
+#pragma unroll
+    for (int i = 0; i < 9; ++i) nk1[i] = K(fsal ? k[6][i] : ns[i]);
+    // stage 2 carries no weight in the bin update (b2 = b*2 = 0)
+    emit = false;
+#pragma unroll
+    for (int j = 1; j < 6; ++j) emit |= (A[j] != SR(0));
+}
+
+// The promoted (FP64-stage) attempt of the mixed path, kept out of line so
+// that its register demand does not set the register budget of the hot FP32
+// path; it runs for few rays.
+template <class SC, class K, class SR, class CT>
+__device__ __noinline__ void dp45_attempt_fp64(const DevScene& s, const double* x, const K* k1in, double h,
+                                                double tol, int nbins, bool fsal, double* y, K* nk1, SR* A, SR* X,
+                                                CT& err2, bool& emit) {
+    dp45_attempt<SC, double, K, SR, CT>(s, x, k1in, h, tol, nbins, fsal, y, nk1, A, X, err2, emit);
+}
+
+// Camera ray of pixel (i, j) of a frame (initialization.jl:213-240,327), FP64.
+__device__ __forceinline__ void camera_ray(const FrameDesc& f, int i, int j, double* x) {
+    const double w = f.rh * ((i + 1) - 0.5) - f.W;
+    const double hh = f.rv * ((j + 1) - 0.5) - f.H;
+    const double th = atan(sqrt(w * w + hh * hh));
+    double ph;
+    if (w > 0) ph = atan(hh / w);
+    else if (w < 0 && hh >= 0) ph = atan(hh / w) + kPi;
+    else if (w < 0 && hh < 0) ph = atan(hh / w) - kPi;
+    else if (w == 0 && hh > 0) ph = kPi / 2;
+    else if (w == 0 && hh < 0) ph = -kPi / 2;
+    else ph = 0;
+    double st, ct, sp, cp;
+    sincos(th, &st, &ct);
+    sincos(ph, &sp, &cp);
+    const double v[4] = {1.0, -st * cp, -st * sp, -ct};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) x[k] = f.pos[k];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        double sacc = 0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) sacc += f.M[4 * r + k] * v[k];
+        x[4 + r] = sacc;
+    }
+    x[8] = 0.0;
+}
+
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    return v;
+}
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    return v;
+}
+
+// Launch bounds: the mixed kernel is capped at 128 registers (4 CTAs of 128
+// threads per SM); its rare FP64 paths spill instead of the hot FP32 path.
+template <int KIND, bool MIXED, int BPL>
+__global__ void __launch_bounds__(128, MIXED ? 4 : 2) trace_kernel(const KParams p) {
+    typedef typename SceneOf<KIND>::type SC;
+    typedef SpecTraits<MIXED> ST;
+    typedef typename ST::SR SR;
+    typedef typename ST::SR K;  // carried slope type
+    typedef typename ST::SR R;  // stage arithmetic (promoted to double per ray)
+    typedef typename ST::SR CT; // step-controller arithmetic
+
+    const int lane = threadIdx.x & 31;
+    const long long warp_id = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int N = p.n_bins;
+    const int np = p.np;
+    const int L = 8 + 2 * N;
+    const DevScene& s = p.sc;
+    SR* spec = reinterpret_cast<SR*>(p.spec) + warp_id * (long long)ST::kFields * 32 * np;
+    SR* sI = spec;                  // [32][np]
+    SR* sK = spec + 32 * np;        // [32][np]
+    SR* sL = spec + 2 * 32 * np;    // [32][np] (MIXED only)
+
+    // per-lane bin frequencies
+    SR nub[BPL];
+#pragma unroll
+    for (int b = 0; b < BPL; ++b) {
+        const int c = lane + 32 * b;
+        nub[b] = c < N ? (SR)p.bin_nu[c] : SR(0);
+    }
+
+    // lane ray state
+    bool active = false, dry = false;
+    long long gid = 0;  // global output index
+    double x[10];
+    K k1[9];
+    double h = 0, tol = 0, r_term = 0, thick = 0;
+    long long max_steps = 0;
+    long long nsteps = 0;
+    bool prev_rej = false, spec_live = false;
+    // local counters
+    unsigned long long c_att = 0, c_rej = 0, c_pro = 0, c_spec = 0, c_emit = 0, c_esc = 0, c_nan = 0, c_rays = 0;
+
+    for (;;) {
+        // ---------------- refill -----------------------------------------
+        const unsigned empty = __ballot_sync(kFull, !active);
+        bool fresh = false;
+        Emit<double> em0;
+        em0.A = 0; em0.X = 0; em0.ktau = 0;
+        if (empty && !dry) {
+            unsigned long long base = 0;
+            const unsigned n = __popc(empty);
+            if (lane == 0) base = atomicAdd(p.counter, (unsigned long long)n);
+            base = __shfl_sync(kFull, base, 0);
+            if ((long long)(base + n) >= p.total_rays) dry = true;
+            if (!active) {
+                const long long id = (long long)base + __popc(empty & ((1u << lane) - 1u));
+                if (id < p.total_rays) {
+                    // frame lookup
+                    int lo = 0, hi = p.n_frames - 1;
+                    while (lo < hi) {
+                        const int mid = (lo + hi + 1) >> 1;
+                        if (p.frames[mid].ray_begin <= id) lo = mid; else hi = mid - 1;
+                    }
+                    const FrameDesc& f = p.frames[lo];
+                    const long long local = id - f.ray_begin;
+                    int pi, pj;
+                    if (p.pixel_order == 1) {
+                        // 8x4 tiles in row-major tile order; partial edge tiles
+                        // are handled by mapping through the tile grid.
+                        const int tw = 8, th = 4;
+                        const int ntx = (f.xp + tw - 1) / tw;
+                        long long rem = local;
+                        // full-height tile rows
+                        const int full_rows = f.yp / th;
+                        const long long per_row = (long long)th * f.xp;
+                        const int trow = (int)(rem / per_row);
+                        if (trow < full_rows) {
+                            rem -= (long long)trow * per_row;
+                            const int full_cols = f.xp / tw;
+                            const long long in_full = (long long)full_cols * tw * th;
+                            if (rem < in_full) {
+                                const int tc = (int)(rem / (tw * th));
+                                const int w = (int)(rem % (tw * th));
+                                pi = tc * tw + (w % tw);
+                                pj = trow * th + w / tw;
+                            } else {
+                                const int w = (int)(rem - in_full);
+                                const int rw = f.xp - full_cols * tw;
+                                pi = full_cols * tw + (w % rw);
+                                pj = trow * th + w / rw;
+                            }
+                        } else {
+                            rem -= (long long)full_rows * per_row;
+                            pi = (int)(rem % f.xp);
+                            pj = full_rows * th + (int)(rem / f.xp);
+                        }
+                        (void)ntx;
+                    } else {
+                        pi = (int)(local % f.xp);
+                        pj = (int)(local / f.xp);
+                    }
+                    gid = f.ray_begin + pi + (long long)f.xp * pj;
+                    camera_ray(f, pi, pj, x);
+                    x[9] = 0.0;
+                    tol = f.tol;
+                    r_term = f.r_term;
+                    thick = f.thick;
+                    max_steps = f.max_steps;
+                    h = -pad_max_dt<KIND, CT>(s, x, p.max_dt_scale);
+                    double kd[9];
+                    SC::template rhs<double>(s, x, kd, em0);
+#pragma unroll
+                    for (int i = 0; i < 9; ++i) k1[i] = (K)kd[i];
+                    nsteps = 0;
+                    prev_rej = false;
+                    spec_live = em0.A != 0.0;
+                    active = true;
+                    fresh = true;
+                    ++c_rays;
+                }
+            }
+        }
+        // spectral init of fresh rays: I = 0, k1 = slope at the camera
+        {
+            unsigned fm = __ballot_sync(kFull, fresh);
+            while (fm) {
+                const int r = __ffs(fm) - 1;
+                fm &= fm - 1;
+                const SR A0 = (SR)__shfl_sync(kFull, em0.A, r);
+                const SR X0 = x_for_bins<SR>((SR)__shfl_sync(kFull, em0.X, r));
+#pragma unroll
+                for (int b = 0; b < BPL; ++b) {
+                    const int c = lane + 32 * b;
+                    if (c < N) {
+                        sI[r * np + c] = SR(0);
+                        sK[r * np + c] = bin_slope(A0, X0, nub[b]);
+                        if constexpr (MIXED) sL[r * np + c] = SR(0);
+                    }
+                }
+            }
+        }
+        const unsigned act = __ballot_sync(kFull, active);
+        if (!act) break;
+
+        // ---------------- geodesic phase ---------------------------------
+        double y[9];
+        K nk1[9];
+        SR A[6], X[6];
+        CT err2 = 0;
+        double max_dt = 0, hnext = h;
+        bool emit = false, esc_done = false, decided = false, accept = false;
+        if (active) {
+            ++c_att;
+            max_dt = pad_max_dt<KIND, CT>(s, x, p.max_dt_scale);
+            double temp;
+            if (near_singularity<KIND>(x, h, tol, &temp)) {
+                // Polar / origin escape (integrators_LttM.jl:62-105): 37 explicit
+                // Euler steps of size temp through the coordinate singularity,
+                // FP64, the spectral slots of this ray updated by this lane.
+                SR* rI = sI + lane * np;
+                SR* rK = sK + lane * np;
+                SR* rL = sL + lane * np;
+                auto euler_spec = [&](double tmp) {
+                    for (int c = 0; c < N; ++c) {
+                        const SR t = (SR)(-tmp) * rK[c];
+                        if constexpr (MIXED) {
+                            float hi = (float)rI[c], lo = (float)rL[c];
+                            kahan_add(hi, lo, (float)t);
+                            rI[c] = (SR)hi;
+                            rL[c] = (SR)lo;
+                        } else {
+                            rI[c] = rI[c] + t;
+                        }
+                    }
+                };
+                auto slope_spec = [&](const Emit<double>& e) {
+                    const SR Ae = (SR)e.A, Xe = x_for_bins<SR>((SR)e.X);
+                    bool nz = false;
+                    for (int c = 0; c < N; ++c) {
+                        const SR v = bin_slope(Ae, Xe, (SR)p.bin_nu[c]);
+                        rK[c] = v;
+                        nz |= v != SR(0);
+                    }
+                    return nz;
+                };
+#pragma unroll
+                for (int i = 0; i < 9; ++i) x[i] -= temp * (double)k1[i];
+                euler_spec(temp);
+                keep_in_bounds<KIND>(x);
+                ++c_esc;
+                for (int it = 0; it < 36; ++it) {
+                    if (!terminate_geo<KIND>(s, x, r_term, thick)) {
+                        double kd[9];
+                        Emit<double> e;
+                        SC::template rhs<double>(s, x, kd, e);
+#pragma unroll
+                        for (int i = 0; i < 9; ++i) k1[i] = (K)kd[i];
+                        spec_live = slope_spec(e);
+#pragma unroll
+                        for (int i = 0; i < 9; ++i) x[i] -= temp * (double)k1[i];
+                        euler_spec(temp);
+                        keep_in_bounds<KIND>(x);
+                        ++c_esc;
+                    }
+                }
+                if (terminate_geo<KIND>(s, x, r_term, thick)) {
+                    esc_done = true;
+                    decided = true;
+                    accept = true;
+                    hnext = h;
+                } else {
+                    double kd[9];
+                    Emit<double> e;
+                    SC::template rhs<double>(s, x, kd, e);
+#pragma unroll
+                    for (int i = 0; i < 9; ++i) k1[i] = (K)kd[i];
+                    spec_live = slope_spec(e);
+                    h = -pad_max_dt<KIND, CT>(s, x, p.max_dt_scale);
+                }
+            }
+            if (!esc_done) {
+                bool promote = false;
+                if (MIXED) {
+                    promote = (x[1] - s.r_ev < p.promote_dr) || (x[2] < p.promote_theta) ||
+                              (x[2] > kPi - p.promote_theta);
+                }
+                if (promote) {
+                    ++c_pro;
+                    dp45_attempt_fp64<SC, K, SR, CT>(s, x, k1, h, tol, N, p.fsal != 0, y, nk1, A, X, err2, emit);
+                } else {
+                    dp45_attempt<SC, R, K, SR, CT>(s, x, k1, h, tol, N, p.fsal != 0, y, nk1, A, X, err2, emit);
+                }
+                if (emit) ++c_emit;
+            }
+        }
+
+        // ---------------- spectral phase (warp-cooperative) --------------
+        const bool need = active && !esc_done && (emit || spec_live);
+        unsigned nm = __ballot_sync(kFull, need);
+        if (need) ++c_spec;
+        while (nm) {
+            const int r = __ffs(nm) - 1;
+            nm &= nm - 1;
+            SR Ar[6], Xr[6];
+#pragma unroll
+            for (int j = 0; j < 6; ++j) {
+                Ar[j] = __shfl_sync(kFull, A[j], r);
+                Xr[j] = x_for_bins<SR>(__shfl_sync(kFull, X[j], r));
+            }
+            const double hr = __shfl_sync(kFull, h, r);
+            const double tr = __shfl_sync(kFull, tol, r);
+            const SR hs = (SR)hr;
+            const SR ts = (SR)tr;
+            SR yv[BPL], yl[BPL], nk[BPL];
+            SR acc = 0;
+#pragma unroll
+            for (int b = 0; b < BPL; ++b) {
+                const int c = lane + 32 * b;
+                yv[b] = 0; yl[b] = 0; nk[b] = 0;
+                if (c < N) {
+                    const SR I = sI[r * np + c];
+                    const SR kk1 = sK[r * np + c];
+                    const SR kk3 = bin_slope(Ar[1], Xr[1], nub[b]);
+                    const SR kk4 = bin_slope(Ar[2], Xr[2], nub[b]);
+                    const SR kk5 = bin_slope(Ar[3], Xr[3], nub[b]);
+                    const SR kk6 = bin_slope(Ar[4], Xr[4], nub[b]);
+                    const SR kk7 = bin_slope(Ar[5], Xr[5], nub[b]);
+                    // (k2 has zero weight in both the 5th-order update and the
+                    // error estimate, and the intensity slopes do not depend on
+                    // the intensity, so stage 2 needs no bin work.)
+                    const SR ns = kk1 * SR(b1) + kk3 * SR(b3) + kk4 * SR(b4) + kk5 * SR(b5) + kk6 * SR(b6);
+                    const SR es = kk1 * SR(e1) + kk3 * SR(e3) + kk4 * SR(e4) + kk5 * SR(e5) + kk6 * SR(e6) +
+                                  kk7 * SR(e7);
+                    SR yy, ylo = 0;
+                    if constexpr (MIXED) {
+                        float hi = (float)I, lo = (float)sL[r * np + c];
+                        kahan_add(hi, lo, (float)(hs * ns));
+                        yy = (SR)hi;
+                        ylo = (SR)lo;
+                    } else {
+                        yy = I + hs * ns;
+                    }
+                    const SR d = hs * es;
+                    const SR tl = ts + rmax(rabs(I), rabs(yy)) * ts;
+                    const SR q = cdiv(d, tl);
+                    acc += q * q;
+                    yv[b] = yy;
+                    yl[b] = ylo;
+                    nk[b] = p.fsal ? kk7 : ns;
+                }
+            }
+            acc = warp_sum(acc);
+            acc = __shfl_sync(kFull, acc, 0);
+            int dec = 0;
+            if (lane == r) {
+                decide<CT>(err2 + (CT)acc, L, h, max_dt, prev_rej, accept, hnext);
+                decided = true;
+                dec = accept ? 1 : 0;
+            }
+            dec = __shfl_sync(kFull, dec, r);
+            bool nz = false;
+            if (dec) {
+#pragma unroll
+                for (int b = 0; b < BPL; ++b) {
+                    const int c = lane + 32 * b;
+                    if (c < N) {
+                        sI[r * np + c] = yv[b];
+                        sK[r * np + c] = nk[b];
+                        if constexpr (MIXED) sL[r * np + c] = yl[b];
+                        nz |= nk[b] != SR(0);
+                    }
+                }
+            }
+            nz = __any_sync(kFull, nz);
+            if (lane == r && dec) spec_live = nz;
+        }
+
+        // ---------------- controller + commit ----------------------------
+        int cls = 0;
+        if (active) {
+            if (!decided) decide<CT>(err2, L, h, max_dt, prev_rej, accept, hnext);
+            if (!esc_done) {
+                if (accept) {
+                    keep_in_bounds<KIND>(y);
+#pragma unroll
+                    for (int i = 0; i < 9; ++i) {
+                        x[i] = y[i];
+                        k1[i] = nk1[i];
+                    }
+                    prev_rej = false;
+                } else {
+                    keep_in_bounds<KIND>(x);
+                    prev_rej = true;
+                    ++c_rej;
+                }
+                h = hnext;
+            } else {
+                prev_rej = false;
+            }
+            ++nsteps;
+            if (nsteps >= max_steps) cls = RTW_CLASS_MAXSTEPS;
+            else cls = terminate_geo<KIND>(s, x, r_term, thick);
+            if (cls) {
+                bool fin = true;
+#pragma unroll
+                for (int i = 0; i < 8; ++i) fin &= isfinite(x[i]);
+                if (!fin) {
+                    cls = RTW_CLASS_NAN;
+                    ++c_nan;
+                }
+            }
+        }
+
+        // ---------------- epilogue: XYZ, outputs -------------------------
+        const bool fin = active && cls != 0;
+        unsigned fm = __ballot_sync(kFull, fin);
+        while (fm) {
+            const int r = __ffs(fm) - 1;
+            fm &= fm - 1;
+            const long long og = __shfl_sync(kFull, gid, r);
+            float X_ = 0, Y_ = 0, Z_ = 0;
+#pragma unroll
+            for (int b = 0; b < BPL; ++b) {
+                const int c = lane + 32 * b;
+                if (c < N) {
+                    double I = (double)sI[r * np + c];
+                    if constexpr (MIXED) I += (double)sL[r * np + c];
+                    X_ += (float)(I * p.bin_fx[c]);
+                    Y_ += (float)(I * p.bin_fy[c]);
+                    Z_ += (float)(I * p.bin_fz[c]);
+                    if (p.spectrum) p.spectrum[og * N + c] = (float)I;
+                }
+            }
+            X_ = warp_sum(X_);
+            Y_ = warp_sum(Y_);
+            Z_ = warp_sum(Z_);
+            if (lane == r && p.xyz) {
+                p.xyz[3 * og + 0] = X_;
+                p.xyz[3 * og + 1] = Y_;
+                p.xyz[3 * og + 2] = Z_;
+            }
+        }
+        if (fin) {
+            if (p.cls) p.cls[gid] = (uint8_t)cls;
+            if (p.steps) p.steps[gid] = (uint32_t)nsteps;
+            if (p.final_state) {
+#pragma unroll
+                for (int i = 0; i < 8; ++i) p.final_state[8 * gid + i] = x[i];
+            }
+            if (p.tau) p.tau[gid] = (float)x[8];
+            active = false;
+        }
+    }
+
+    // counters
+    atomicAdd(&p.stats->step_attempts, c_att);
+    atomicAdd(&p.stats->rejected_steps, c_rej);
+    atomicAdd(&p.stats->promoted_steps, c_pro);
+    atomicAdd(&p.stats->spectral_steps, c_spec);
+    atomicAdd(&p.stats->emitting_steps, c_emit);
+    atomicAdd(&p.stats->escape_substeps, c_esc);
+    atomicAdd(&p.stats->nan_rays, c_nan);
+    atomicAdd(&p.stats->rays, c_rays);
+}
+
+}  // namespace rtw

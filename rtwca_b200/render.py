@@ -1,0 +1,244 @@
+"""Host side of the render call, mirroring the reference's Julia API.
+
+``initialize_world(name)`` selects a scene the way the reference's
+initialize_world (main/initialization.jl:78-172) ``include``s a ``.source``
+folder, and returns its default camera (position, direction, pointing, beta).
+``gen_image(...)`` takes the keyword arguments of the reference's gen_image
+(main/Iterators/LttM/LttM.jl:104-107, main/Iterators/5P/5P.jl:135-138) with the
+same meaning and defaults, and calls librtw_b200.so through its C ABI.
+
+Differences, by design of the library: gen_image returns linear CIE XYZ
+[y_pix, x_pix, 3] in the reference's image orientation (the reference converts
+to xyY, normalises brightness and converts to RGB{N0f16}; ``xyz_to_srgb`` gives
+that last step as an informational helper), and ``ray_bundles=True`` raises
+RTW_ERR_UNSUPPORTED.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import abi
+
+PI = math.pi
+
+
+class Renderer:
+    """One library context (one CUDA device, one stream, cached device buffers)."""
+
+    def __init__(self, device: int = 0):
+        self._lib = abi.load()
+        self._ctx = C.c_void_p()
+        st = self._lib.rtw_create(C.byref(self._ctx), int(device))
+        abi.check(st, f"rtw_create(device={device})")
+
+    def close(self) -> None:
+        if self._ctx:
+            self._lib.rtw_destroy(self._ctx)
+            self._ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._ctx
+
+    def last_error(self) -> str:
+        return (self._lib.rtw_last_error(self._ctx) or b"").decode()
+
+    @staticmethod
+    def params(colors_nm, precision=abi.PREC_FP64, integrator=abi.DP45_REF_COMPAT, max_dt_scale=0.1,
+               block_warps=0, ctas_per_sm=0, promote_dr=0.0, promote_sin=0.0, stream=None,
+               pixel_order=0, ray_bundles=False):
+        colors = np.ascontiguousarray(np.asarray(colors_nm, dtype=np.float64))
+        p = abi.RenderParams()
+        p.n_colors = int(colors.size)
+        p.precision = int(precision)
+        p.colors_nm = colors.ctypes.data_as(C.POINTER(C.c_double))
+        p.max_dt_scale = float(max_dt_scale)
+        p.integrator = int(integrator)
+        p.ray_bundles = int(bool(ray_bundles))
+        p.promote_dr = float(promote_dr)
+        p.promote_sin = float(promote_sin)
+        p.block_warps = int(block_warps)
+        p.ctas_per_sm = int(ctas_per_sm)
+        p.stream = stream
+        p.pixel_order = int(pixel_order)
+        p._keep = colors  # keep the array alive with the struct
+        return p
+
+    def render_raw(self, scene: abi.Scene, cams, params: abi.RenderParams, outputs: abi.Outputs) -> None:
+        """rtw_render with caller-provided output pointers (host or device)."""
+        cams = list(cams)
+        arr = (abi.Camera * len(cams))(*cams)
+        st = self._lib.rtw_render(self._ctx, C.byref(scene), arr, len(cams), C.byref(params), C.byref(outputs))
+        abi.check(st, self.last_error())
+
+    def render(self, scene: abi.Scene, cams, colors_nm, *, want=("xyz", "class", "steps"), **kw) -> dict:
+        """Renders frames into new host numpy arrays; returns a dict of arrays
+        indexed by global pixel (frames concatenated, pixel i + x_pix * j)."""
+        cams = list(cams)
+        total = 0
+        for c in cams:
+            c.y_pix = abi.y_pixels(c.x_pix, c.fov_hor, c.fov_vert)
+            total += c.x_pix * c.y_pix
+        n = len(np.atleast_1d(colors_nm))
+        res = {}
+        out = abi.Outputs()
+        if "xyz" in want:
+            res["xyz"] = np.zeros((total, 3), np.float32)
+            out.xyz = res["xyz"].ctypes.data
+        if "class" in want:
+            res["class"] = np.zeros(total, np.uint8)
+            out.term_class = res["class"].ctypes.data
+        if "steps" in want:
+            res["steps"] = np.zeros(total, np.uint32)
+            out.steps = res["steps"].ctypes.data
+        if "spectrum" in want:
+            res["spectrum"] = np.zeros((total, n), np.float32)
+            out.spectrum = res["spectrum"].ctypes.data
+        if "state" in want:
+            res["state"] = np.zeros((total, 8), np.float64)
+            out.final_state = res["state"].ctypes.data
+        if "tau" in want:
+            res["tau"] = np.zeros(total, np.float32)
+            out.tau = res["tau"].ctypes.data
+        out.on_device = 0
+        self.render_raw(scene, cams, self.params(colors_nm, **kw), out)
+        return res
+
+    def stats(self) -> dict:
+        s = abi.Stats()
+        abi.check(self._lib.rtw_get_stats(self._ctx, C.byref(s)), self.last_error())
+        return {f: getattr(s, f) for f, _ in abi.Stats._fields_}
+
+    def op_counts(self, kind: int) -> dict:
+        return abi.op_counts(kind)
+
+    def measure_peaks(self) -> dict:
+        a, b, c = C.c_double(), C.c_double(), C.c_double()
+        abi.check(self._lib.rtw_measure_peaks(self._ctx, C.byref(a), C.byref(b), C.byref(c)), self.last_error())
+        return {"fp32_flops": a.value, "fp64_flops": b.value, "mufu_ops": c.value}
+
+
+# ---------------------------------------------------------------------------
+# The reference's world/scene selection and render call
+# ---------------------------------------------------------------------------
+
+@dataclass
+class World:
+    scene: abi.Scene
+    position: list
+    direction: list
+    pointing: list
+    beta: float
+
+
+_WORLDS = {
+    # initialization.jl:80-89
+    "schwarzschild_t,r,θ,ϕ_simpledisk": (abi.SCENE_SCHWARZSCHILD_DISK, [0, 25, PI / 3, 0], [PI / 2, 0],
+                                          [0.0, 0.0, -PI / 2], 0.0),
+    # initialization.jl:90-99
+    "kerr_boyer_lindquist": (abi.SCENE_KERR_DISK, [0, 25, 0.52 * PI, 0], [PI / 2, 0], [0.0, 0.0, -PI / 2], 0.0),
+    # initialization.jl:110-119
+    "minkowski_t,r,θ,ϕ_sphere": (abi.SCENE_MINKOWSKI_SPHERE, [0, 4, PI / 2, 0], [PI / 2, 0],
+                                 [0.0, 0.0, -PI / 2], 0.0),
+}
+
+_current: World | None = None
+_renderer: Renderer | None = None
+
+
+def available_worlds() -> list:
+    return sorted(_WORLDS)
+
+
+def initialize_world(input_string: str):
+    """Selects a scene and returns its default (position, direction, pointing, beta)
+    (initialization.jl:78-172). Scenes that need the reference's missing textures
+    (wormhole, Cartesian sphere) and the M87*/synchrotron work-in-progress scenes
+    are not on this library's path and raise ValueError."""
+    global _current
+    key = input_string.lower()
+    if key not in _WORLDS:
+        raise ValueError(f"unknown or unsupported world {input_string!r}; available: {available_worlds()}")
+    kind, pos, d, pt, beta = _WORLDS[key]
+    _current = World(abi.scene_default(kind), list(pos), list(d), list(pt), beta)
+    return list(pos), list(d), list(pt), beta
+
+
+def set_scene(scene: abi.Scene) -> None:
+    """Selects an explicit scene (runtime parameters instead of a .source folder)."""
+    global _current
+    _current = World(scene, [0, 0, 0, 0], [0, 0], [0, 0, 0], 0.0)
+
+
+def _get_renderer() -> Renderer:
+    global _renderer
+    if _renderer is None:
+        _renderer = Renderer(0)
+    return _renderer
+
+
+def gen_image(*, camera_pos=(0, 0, 0, 0), camera_dir=(0.0, 0.0), speed=0.0, camera_point=(0.0, 0.0, 0.0),
+              x_pix=100, max_steps=1e3, colors=(400, 550, 700), returnrays=False, tolerance=1e-4,
+              max_dt_scale=1e-1, fov_hor=85, fov_vert=60, print_num_pix=False, ray_bundles=False,
+              precision="fp64", integrator="ref_compat", renderer: Renderer | None = None):
+    """The reference's gen_image (LttM.jl:104-209 / 5P.jl:135-282) on the B200.
+
+    Returns the linear XYZ image [y_pix, x_pix, 3] in the reference's orientation
+    (transpose(reverse(img, dims=2))), and with ``returnrays`` also the final
+    ray states [x_pix, y_pix, 8 + 2 len(colors)] in the reference's layout
+    (t, r, theta, phi, k^t, k^r, k^theta, k^phi, I_1, tau_1, I_2, tau_2, ...).
+    A camera on a coordinate singularity raises abi.RTWError(RTW_ERR_INVALID_CAMERA)
+    (the reference prints and returns a blank image, 5P.jl:140-143)."""
+    if _current is None:
+        raise RuntimeError("call initialize_world(name) or set_scene(scene) first")
+    r = renderer or _get_renderer()
+    cam = abi.make_camera(camera_pos, camera_dir, speed, camera_point, int(x_pix), fov_hor, fov_vert,
+                          tolerance, int(max_steps))
+    if print_num_pix:
+        print("Number of Pixels ", cam.x_pix * cam.y_pix)
+    prec = {"fp64": abi.PREC_FP64, "mixed": abi.PREC_MIXED}[precision]
+    integ = {"ref_compat": abi.DP45_REF_COMPAT, "fsal": abi.DP45_FSAL}[integrator]
+    want = ("xyz", "class", "steps") + (("spectrum", "state", "tau") if returnrays else ())
+    res = r.render(_current.scene, [cam], colors, want=want, precision=prec, integrator=integ,
+                   max_dt_scale=max_dt_scale, ray_bundles=ray_bundles)
+    xp, yp = cam.x_pix, cam.y_pix
+    img = res["xyz"].reshape(yp, xp, 3)[::-1].copy()
+    if not returnrays:
+        return img
+    n = len(np.atleast_1d(colors))
+    rays = np.zeros((xp, yp, 8 + 2 * n))
+    st = res["state"].reshape(yp, xp, 8).transpose(1, 0, 2)
+    rays[:, :, :8] = st
+    rays[:, :, 8::2] = res["spectrum"].reshape(yp, xp, n).transpose(1, 0, 2)
+    rays[:, :, 9::2] = res["tau"].reshape(yp, xp, 1).transpose(1, 0, 2)
+    return img, rays
+
+
+def xyz_to_srgb(xyz: np.ndarray) -> np.ndarray:
+    """Informational: brightness-normalised sRGB of a linear XYZ image in the way
+    gen_image finishes (Y scaled to [0, max Y], then XYZ -> sRGB, D65)."""
+    xyz = np.asarray(xyz, dtype=np.float64)
+    ymax = np.nanmax(xyz[..., 1]) if xyz.size else 0.0
+    if not ymax > 0:
+        return np.zeros_like(xyz)
+    x = xyz / ymax
+    m = np.array([[3.2404542, -1.5371385, -0.4985314], [-0.9692660, 1.8760108, 0.0415560],
+                  [0.0556434, -0.2040259, 1.0572252]])
+    lin = np.clip(x @ m.T, 0, 1)
+    return np.where(lin <= 0.0031308, 12.92 * lin, 1.055 * np.power(lin, 1 / 2.4) - 0.055)
