@@ -144,10 +144,11 @@ typedef struct rtw_render_params {
     int32_t integrator;         /* rtw_integrator */
     int32_t ray_bundles;        /* must be 0 (bundles are not built) */
     double promote_dr;          /* MIXED: FP64 stages while r - r_horizon < promote_dr M
-                                   (0: default 1e-4; < 0: never) */
+                                   (<= 0: never, the default: the FP32 stages
+                                   carry r - r_horizon from the FP64 state) */
     double promote_sin;         /* MIXED: FP64 stages while sin(theta) < promote_sin
-                                   (0: default 1e-3; < 0: never) */
-    int32_t block_warps;        /* warps per CTA (0: autotuned / default) */
+                                   (0: default 1e-2; < 0: never) */
+    int32_t block_warps;        /* warps per CTA, 1..4 (0: default 4) */
     int32_t ctas_per_sm;        /* resident CTAs per SM (0: default) */
     void* stream;               /* cudaStream_t to run on; NULL: the context's
                                    stream, and rtw_render returns when done */
@@ -252,6 +253,17 @@ rtw_status rtw_get_stats(rtw_ctx* ctx, rtw_stats* out);
  * FP32 FMA, FP64 FMA (flop/s, an FMA counted as 2) and MUFU ex2 (op/s). */
 rtw_status rtw_measure_peaks(rtw_ctx* ctx, double* fp32_flops, double* fp64_flops,
                              double* mufu_ops);
+
+/* Evaluates a scene's right-hand side on the host with the trace kernel's own
+ * device functors, in FP64 (fp32 = 0) or in the FP32 form of the mixed path
+ * (fp32 = 1; host sin/cos/exp stand in for the device's MUFU forms). The
+ * geodesic and common-tau part of calc_ray_derivative!
+ * (integrators_LttM.jl:9-48): state[9] = (t, r, theta, phi, k^t, k^r,
+ * k^theta, k^phi, tau) -> slope[9]; emit[3] (may be NULL) = the emitter
+ * numbers A = a_nu emission_scale exp(-tau) / g, X = f_factor g / T and
+ * ktau = -a_nu / g, from which the intensity slope of bin c is
+ * -A / (exp(X nu_c) - 1). */
+rtw_status rtw_scene_rhs(const rtw_scene* scene, int32_t fp32, const double* state, double* slope, double* emit);
 
 /* Operation counts used for the roofline of a render (see rtw_op_counts above). */
 rtw_status rtw_get_op_counts(int32_t kind, rtw_op_counts* out);

@@ -8,10 +8,12 @@ from __future__ import annotations
 
 import ctypes as C
 import math
+import os
 from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
-LIB_PATH = PKG / "librtw_b200.so"
+# RTW_LIB_PATH selects another build of the same library (e.g. a tuning variant)
+LIB_PATH = Path(os.environ.get("RTW_LIB_PATH", PKG / "librtw_b200.so"))
 
 ABI_VERSION = 1
 MAX_BINS = 128
@@ -127,6 +129,8 @@ SIGNATURES = {
     "rtw_get_stats": (C.c_int, [_P, C.POINTER(Stats)]),
     "rtw_measure_peaks": (C.c_int, [_P] + [C.POINTER(C.c_double)] * 3),
     "rtw_get_op_counts": (C.c_int, [C.c_int32, C.POINTER(OpCounts)]),
+    "rtw_scene_rhs": (C.c_int, [C.POINTER(Scene), C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                C.POINTER(C.c_double)]),
 }
 
 _lib = None
@@ -169,6 +173,18 @@ def op_counts(kind: int) -> dict:
     oc = OpCounts()
     check(load().rtw_get_op_counts(kind, C.byref(oc)), "op_counts")
     return {f: getattr(oc, f) for f, _ in OpCounts._fields_}
+
+
+def scene_rhs(scene: Scene, state, fp32: bool = False):
+    """Host evaluation of the kernel's right-hand side: (slope[9], (A, X, ktau))."""
+    import numpy as np
+    st = np.ascontiguousarray(state, dtype=np.float64)
+    out = np.zeros(9)
+    em = np.zeros(3)
+    D = C.POINTER(C.c_double)
+    check(load().rtw_scene_rhs(C.byref(scene), int(fp32), st.ctypes.data_as(D), out.ctypes.data_as(D),
+                               em.ctypes.data_as(D)), "scene_rhs")
+    return out, em
 
 
 def scene_default(kind: int) -> Scene:

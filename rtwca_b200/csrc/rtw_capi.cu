@@ -181,6 +181,24 @@ double cie_fit(double wl, int first, int count) {
 }
 
 }  // namespace
+
+void make_dev_scene(const rtw_scene& scene, DevScene& d) {
+    std::memset(&d, 0, sizeof(d));
+    d.kind = scene.kind;
+    d.refprec = 0;
+    d.M = scene.mass;
+    d.a = is_kerr(scene.kind) ? scene.spin : 0.0;
+    d.rs = 2 * scene.mass;
+    d.r_ev = horizon_radius(scene);
+    d.r_in = scene.r_in; d.r_out = scene.r_out;
+    d.th_lo = scene.theta_lo; d.th_hi = scene.theta_hi;
+    d.T = scene.temperature; d.anu = scene.a_nu;
+    d.esc = scene.escape_radius; d.wind = scene.winding_limit;
+    d.rho_r0 = scene.rho_r0; d.rho_h = scene.rho_h; d.rho_idx = scene.rho_index; d.t_idx = scene.t_index;
+    d.sqrtM = std::sqrt(scene.mass);
+    d.r_pm = is_kerr(scene.kind) ? 2 * std::sqrt(scene.mass * scene.mass - scene.spin * scene.spin) : 0.0;
+}
+
 }  // namespace rtw
 
 using namespace rtw;
@@ -466,7 +484,7 @@ rtw_status rtw_render(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* ca
     const int np = N <= 32 ? 32 : (N <= 64 ? 64 : 128);
 
     // launch shape
-    const int warps = prm->block_warps > 0 ? std::min(prm->block_warps, 8) : 4;
+    const int warps = prm->block_warps > 0 ? std::min(prm->block_warps, 4) : 4;  // kernel launch bound: 128 threads
     const int block = 32 * warps;
     int per_sm = prm->ctas_per_sm;
     if (per_sm <= 0) {
@@ -516,28 +534,16 @@ rtw_status rtw_render(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* ca
 
     KParams p;
     std::memset(&p, 0, sizeof(p));
-    DevScene& d = p.sc;
-    d.kind = scene->kind;
-    d.refprec = 0;
-    d.M = scene->mass;
-    d.a = is_kerr(scene->kind) ? scene->spin : 0.0;
-    d.rs = 2 * scene->mass;
-    d.r_ev = horizon_radius(*scene);
-    d.r_in = scene->r_in; d.r_out = scene->r_out;
-    d.th_lo = scene->theta_lo; d.th_hi = scene->theta_hi;
-    d.T = scene->temperature; d.anu = scene->a_nu;
-    d.esc = scene->escape_radius; d.wind = scene->winding_limit;
-    d.rho_r0 = scene->rho_r0; d.rho_h = scene->rho_h; d.rho_idx = scene->rho_index; d.t_idx = scene->t_index;
-    d.sqrtM = std::sqrt(scene->mass);
-    d.r_pm = is_kerr(scene->kind) ? 2 * std::sqrt(scene->mass * scene->mass - scene->spin * scene->spin) : 0.0;
+    make_dev_scene(*scene, p.sc);
     p.frames = (const FrameDesc*)ctx->d_frames;
     p.n_frames = n_cams;
     p.n_bins = N;
     p.total_rays = total;
     p.max_dt_scale = prm->max_dt_scale;
-    // promotion thresholds: < 0 disables, 0 takes the default
-    const double pdr = prm->promote_dr < 0 ? -1.0 : (prm->promote_dr > 0 ? prm->promote_dr : 1e-4);
-    const double psn = prm->promote_sin < 0 ? 0.0 : (prm->promote_sin > 0 ? std::min(prm->promote_sin, 1.0) : 1e-3);
+    // promotion thresholds: < 0 disables, 0 takes the default (horizon: off,
+    // the FP32 stages carry r - r+ from the FP64 state; poles: sin < 1e-2)
+    const double pdr = prm->promote_dr > 0 ? prm->promote_dr : -1.0;
+    const double psn = prm->promote_sin < 0 ? 0.0 : (prm->promote_sin > 0 ? std::min(prm->promote_sin, 1.0) : 1e-2);
     p.promote_dr = pdr * scene->mass;
     p.promote_theta = std::asin(psn);
     p.fsal = prm->integrator == RTW_DP45_FSAL;

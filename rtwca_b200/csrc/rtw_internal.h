@@ -79,6 +79,9 @@ struct KParams {
     float* tau;
 };
 
+// Scene constants of the device functors from the public scene struct.
+void make_dev_scene(const rtw_scene& scene, DevScene& d);
+
 // Launches the trace kernel for p.sc.kind / precision on `stream`.
 // Returns cudaSuccess or the launch error.
 cudaError_t launch_trace(const KParams& p, int precision, int grid, int block, cudaStream_t stream);

@@ -1,6 +1,8 @@
-// rtw_opcount.cu - algorithmic operation counts of the trace kernel's
-// arithmetic, obtained by running the same scene functors and Dormand-Prince
-// attempt on the host with a counting scalar. Used for the roofline: the
+// rtw_opcount.cu - host evaluations of the trace kernel's own device functors:
+// (1) rtw_scene_rhs: the scene right-hand side in FP64 (or FP32), for checking
+// the kernel's formulas against the oracle without a GPU; (2) algorithmic
+// operation counts of the kernel's arithmetic, obtained by running the same
+// scene functors and Dormand-Prince attempt on the host with a counting scalar. Used for the roofline: the
 // achieved FLOP/s of a render is these counts times the render's counters
 // (step attempts, emitting attempts, spectral attempts) over its device time.
 //
@@ -74,14 +76,14 @@ static void count_kind(const DevScene& sc, const double* xv, const double* xe, r
     out->rhs_emit = (double)g_tally.flops;
     out->rhs_emit_mufu = (double)g_tally.mufu;
     // one whole attempt at the vacuum point: 6 right-hand sides + the rest
-    CS k1[9], nk1[9], A[6], X[6], err2;
-    double y[9];
+    CS k1[9], ns[9], nk1[9], A[6], X[6], err2;
     for (int i = 0; i < 9; ++i) k1[i] = k[i];
     bool emit = false;
     g_tally = Tally();
-    dp45_attempt<SCN, CS, CS, CS, CS>(sc, xv, k1, -1e-3, 1e-8, 64, false, y, nk1, A, X, err2, emit);
-    // controller (decide): sqrt, log2/exp2, ~12 flops of compares/products
-    const double controller_flops = 12, controller_mufu = 3;
+    dp45_attempt<SCN, CS, CS, CS, CS>(sc, xv, k1, -1e-3, 1e-8, 64, false, ns, nk1, A, X, 1, err2, emit);
+    // controller (decide: sqrt, log2/exp2, ~12 flops) and the FP64 update
+    // x + h ns of an accepted attempt (9 FMA)
+    const double controller_flops = 12 + 18, controller_mufu = 3;
     out->step_overhead = (double)g_tally.flops - 6 * out->rhs_vacuum + controller_flops;
     out->step_overhead_mufu = (double)g_tally.mufu - 6 * out->rhs_vacuum_mufu + controller_mufu;
     // spectral work per bin of one attempt (warp-cooperative phase): five new
@@ -120,6 +122,44 @@ extern "C" rtw_status rtw_get_op_counts(int32_t kind, rtw_op_counts* out) {
     case 1: count_kind<1>(sc, xv, xe, out); break;
     case 2: count_kind<2>(sc, xv, xe, out); break;
     default: count_kind<3>(sc, xv, xe, out); break;
+    }
+    return RTW_OK;
+}
+
+namespace rtw {
+template <int KIND, class R>
+static void host_rhs(const DevScene& sc, const double* state, double* slope, double* emit) {
+    typedef typename SceneOf<KIND>::type SCN;
+    R z[10], k[9];
+    Emit<R> em;
+    for (int i = 0; i < 9; ++i) z[i] = R(state[i]);
+    z[9] = R(state[1] - sc.r_ev);
+    SCN::template rhs<R>(sc, z, k, em);
+    for (int i = 0; i < 9; ++i) slope[i] = double(k[i]);
+    if (emit) {
+        emit[0] = double(em.A);
+        emit[1] = double(em.X);
+        emit[2] = double(em.ktau);
+    }
+}
+}  // namespace rtw
+
+extern "C" rtw_status rtw_scene_rhs(const rtw_scene* scene, int32_t fp32, const double* state, double* slope,
+                                    double* emit) {
+    using namespace rtw;
+    if (!scene || !state || !slope || scene->kind < 0 || scene->kind > RTW_SCENE_KERR_THICK_DISK)
+        return RTW_ERR_INVALID_PARAM;
+    DevScene sc;
+    make_dev_scene(*scene, sc);
+    switch (scene->kind * 2 + (fp32 ? 1 : 0)) {
+    case 0: host_rhs<0, double>(sc, state, slope, emit); break;
+    case 1: host_rhs<0, float>(sc, state, slope, emit); break;
+    case 2: host_rhs<1, double>(sc, state, slope, emit); break;
+    case 3: host_rhs<1, float>(sc, state, slope, emit); break;
+    case 4: host_rhs<2, double>(sc, state, slope, emit); break;
+    case 5: host_rhs<2, float>(sc, state, slope, emit); break;
+    case 6: host_rhs<3, double>(sc, state, slope, emit); break;
+    default: host_rhs<3, float>(sc, state, slope, emit); break;
     }
     return RTW_OK;
 }

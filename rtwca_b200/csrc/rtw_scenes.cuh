@@ -82,11 +82,22 @@ RTW_HD float rinv(float x) {
 
 // Blackbody grey emitter at redshift factor g with temperature T and
 // absorption a_nu (calc_planck + calc_radiative_coefficients).
+// exp(-tau) of a stage point. A stage that enters an absorber mid-step can
+// carry a large negative stage tau (the tableau has negative coefficients);
+// in FP32, exp(-tau) would overflow to inf and turn the embedded error into
+// NaN, which the reference's controller accepts. The FP32 form saturates at
+// exp(80): the slope stays finite and huge, the error rejects the step, as the
+// FP64 form does.
+RTW_HD float attenuation(float tau) { return rexp_(fminf(-tau, 80.0f)); }
+RTW_HD double attenuation(double tau) { return rexp_(-tau); }
+template <class R>
+RTW_HD R attenuation(R tau) { return rexp_(-tau); }
+
 template <class R>
 RTW_HD Emit<R> bb_emit(R a_nu, R T, R g, R tau) {
     Emit<R> e;
     const R ig = rinv(g);
-    e.A = a_nu * R(kEmissionScale) * rexp_(-tau) * ig;
+    e.A = a_nu * R(kEmissionScale) * attenuation(tau) * ig;
     e.X = R(kFFactor) * g / T;
     e.ktau = -a_nu * ig;
     return e;
@@ -175,7 +186,7 @@ struct KerrScene {
         R sn, cs;
         rsincos(th, &sn, &cs);
         const R r2 = r * r, a2 = a * a, s2 = sn * sn;
-        const R ac2 = a2 * cs * cs, as2 = a2 * s2;
+        const R ac2 = a2 * cs * cs, as2 = a2 * s2;  // a^2 cos^2, a^2 sin^2
         const R Sig = r2 + ac2;
         // Delta = r^2 - rs r + a^2 = (r - r+)(r - r-). FP32 stages use the
         // factored form with z[9] = r - r+ carried from the FP64 state, which
@@ -183,47 +194,43 @@ struct KerrScene {
         const R Del = sizeof(R) == 4 ? z[9] * (z[9] + R(s.r_pm)) : r2 - rs * r + a2;
         const R ra2 = r2 + a2;
         const R Aa = ra2 * Sig + rs * r * as2;
-        const R iS = rinv(Sig), iD = rinv(Del), isn = rinv(sn);
-        const R iS2 = iS * iS, iS3 = iS2 * iS;
-        const R hiS2D = R(0.5) * iS2 * iD;  // 1 / (2 Sig^2 Del)
-        const R hiS3 = R(0.5) * iS3;        // 1 / (2 Sig^3)
-        const R s2t = R(2) * sn * cs;       // sin(2 theta)
-        const R cot = cs * isn;
-        const R dr = r2 - ac2;              // r^2 - a^2 cos^2
-        const R Sig2 = Sig * Sig;
-        // t
-        const R Gt_tr = rs * ra2 * dr * hiS2D;
-        const R Gt_tth = -rs * a2 * r * s2t * R(0.5) * iS2;
-        const R Gt_rph = rs * a * s2 * (ac2 * (a2 - r2) - r2 * (a2 + R(3) * r2)) * hiS2D;
-        const R Gt_thph = rs * a2 * a * r * s2 * sn * cs * iS2;
-        // r
-        const R Gr_tt = rs * Del * dr * hiS3;
-        const R Gr_tph = -Del * rs * a * s2 * dr * hiS3;
-        const R Gr_rr = (R(2) * r * as2 - rs * dr) * R(0.5) * iS * iD;
-        const R Gr_rth = -a2 * s2t * R(0.5) * iS;
+        const R iS = rinv(Sig), iD = rinv(Del), cot = cs * rinv(sn);
+        const R iS2 = iS * iS;
+        const R P = rs * iS2;             // rs / Sig^2
+        const R Q = R(0.5) * P * iD;      // rs / (2 Sig^2 Del)
+        const R iS3h = R(0.5) * iS2 * iS; // 1 / (2 Sig^3)
+        const R sc = sn * cs;             // sin(2 theta) / 2
+        const R dr = r2 - ac2;            // r^2 - a^2 cos^2
+        // The 30 nonzero Christoffel symbols of Kerr.source/source_geometry.jl:203-240,
+        // written around shared factors (Gamma^t_tr = Q (r^2+a^2) dr,
+        // Gamma^phi_tr = Q a dr, Gamma^r_tphi = -a sin^2 Gamma^r_tt,
+        // Gamma^theta_tt = Gamma^t_ttheta / Sig, Gamma^theta_thth = Gamma^r_rth,
+        // Gamma^theta_rr = -Gamma^r_rth / Delta, ...).
+        const R Gt_tth = -P * a2 * r * sc;
+        const R Gt_thph = -Gt_tth * a * s2;
+        const R Gt_rph = Q * a * s2 * (ac2 * (a2 - r2) - r2 * (a2 + R(3) * r2));
+        const R Gp_tth = -P * a * r * cot;
+        const R Gp_rph = r * iD + Q * (as2 * ac2 - r2 * (Sig + ra2));
+        const R Gp_thph = cot * (R(1) + P * r * as2);
+        const R Gr_tt = rs * Del * dr * iS3h;
+        const R Gr_rth = -a2 * sc * iS;
+        const R Gr_rr = (r * as2 - R(0.5) * rs * dr) * iS * iD;
         const R Gr_thth = -r * Del * iS;
-        const R Gr_phph = Del * s2 * (-R(2) * r * Sig2 + rs * as2 * dr) * hiS3;
-        // theta
-        const R Gh_tt = -rs * a2 * r * s2t * hiS3;
-        const R Gh_tph = rs * a * r * ra2 * s2t * hiS3;
-        const R Gh_rr = a2 * s2t * R(0.5) * iS * iD;
+        const R Gr_phph = Del * s2 * (rs * as2 * dr - R(2) * r * Sig * Sig) * iS3h;
+        const R Gh_tt = Gt_tth * iS;
+        const R Gh_tph = P * iS * a * r * ra2 * sc;
+        const R Gh_rr = -Gr_rth * iD;
         const R Gh_rth = r * iS;
-        const R Gh_thth = -a2 * s2t * R(0.5) * iS;
-        const R Gh_phph = -s2t * (Aa * Sig + ra2 * rs * r * as2) * hiS3;
-        // phi
-        const R Gp_tr = rs * a * dr * hiS2D;
-        const R Gp_tth = -rs * a * r * cot * iS2;
-        const R hs = a2 * s2t * R(0.5);
-        const R Gp_rph = (R(2) * r * Sig2 + rs * (hs * hs - r2 * (Sig + ra2))) * hiS2D;
-        const R Gp_thph = cot * (Sig2 + rs * r * as2) * iS2;
+        const R Gh_phph = -R(2) * sc * (Aa * Sig + ra2 * rs * r * as2) * iS3h;
+        const R Qdr_ktkr = Q * dr * kt * kr;
 
         k[0] = kt; k[1] = kr; k[2] = kth; k[3] = kph;
-        k[4] = -R(2) * (Gt_tr * kt * kr + Gt_tth * kt * kth + Gt_rph * kr * kph + Gt_thph * kth * kph);
-        k[5] = -(Gr_tt * kt * kt + R(2) * Gr_tph * kt * kph + Gr_rr * kr * kr + R(2) * Gr_rth * kr * kth +
+        k[4] = -R(2) * (Qdr_ktkr * ra2 + Gt_tth * kt * kth + Gt_rph * kr * kph + Gt_thph * kth * kph);
+        k[5] = -(Gr_tt * (kt * kt - R(2) * a * s2 * kt * kph) + Gr_rr * kr * kr + R(2) * Gr_rth * kr * kth +
                  Gr_thth * kth * kth + Gr_phph * kph * kph);
         k[6] = -(Gh_tt * kt * kt + R(2) * Gh_tph * kt * kph + Gh_rr * kr * kr + R(2) * Gh_rth * kr * kth +
-                 Gh_thth * kth * kth + Gh_phph * kph * kph);
-        k[7] = -R(2) * (Gp_tr * kt * kr + Gp_tth * kt * kth + Gp_rph * kr * kph + Gp_thph * kth * kph);
+                 Gr_rth * kth * kth + Gh_phph * kph * kph);
+        k[7] = -R(2) * (Qdr_ktkr * a + Gp_tth * kt * kth + Gp_rph * kr * kph + Gp_thph * kth * kph);
 
         bool fire;
         if (THICK)
@@ -294,8 +301,8 @@ template <int KIND, class CT = double>
 __device__ __forceinline__ double pad_max_dt(const DevScene& s, const double* xd, double scale_d) {
     constexpr bool kerr = KIND == RTW_SCENE_KERR_DISK || KIND == RTW_SCENE_KERR_THICK_DISK;
     CT scale = (CT)(kerr ? (double)(float)scale_d : scale_d);
-    const CT th = (CT)xd[2], vr = (CT)xd[5], vth = (CT)xd[6], vph = (CT)xd[7];
-    const CT pi = (CT)kPi, ndz = (CT)kNoDivZero;
+    const CT vr = (CT)xd[5], vth = (CT)xd[6], vph = (CT)xd[7];
+    const CT ndz = (CT)kNoDivZero;
     CT eps;
     if (xd[2] < kPi / 8 || xd[2] > 7 * kPi / 8)
         eps = cmin(scale, (CT)1e-1f);
@@ -308,7 +315,10 @@ __device__ __forceinline__ double pad_max_dt(const DevScene& s, const double* xd
         first = cabs(cdiv(CT(1), cdiv(eps, cabs(vr)))) + ndz;
     else
         first = cabs(cdiv(CT(1), cdiv(eps, cabs(vr) + ndz))) + ndz;
-    const CT second = cabs(cdiv(CT(1), cdiv(eps * cmin(th, pi - th), cabs(vth) + ndz) + ndz));
+    // distance to the nearer pole in FP64: in FP32, pi - theta is 0 within
+    // 1.2e-7 of the pole, which would freeze a ray crossing the axis
+    const CT pole = CT(fmin(xd[2], kPi - xd[2]));
+    const CT second = cabs(cdiv(CT(1), cdiv(eps * pole, cabs(vth) + ndz) + ndz));
     const CT third = cabs(cdiv(CT(1), cdiv(eps, cabs(vph) + ndz) + ndz));
     CT m = cmin(cdiv(CT(1), first + second + third + ndz), (CT)0.5);
     return (double)cmax(m, (CT)1e-12f);

@@ -9,12 +9,15 @@
 //  * Geodesic phase, one lane per ray: one adaptive Dormand-Prince attempt
 //    (RKDP_Step_w_buffer!, integrators_LttM.jl:54-224) over the 8 geodesic
 //    components plus the common optical depth tau (the emitters are grey, so
-//    every tau slot of the reference's state is the same number). The seven
-//    right-hand sides also yield the emitter numbers (A, X) of every stage.
+//    every tau slot of the reference's state is the same number). The stages
+//    run as a rolled loop over one inlined right-hand side; the tableau sums
+//    are shifted accumulators, so no register array is indexed dynamically
+//    and the hot code stays small enough for the instruction cache. The
+//    emitter numbers (A, X) of every stage go to shared memory.
 //  * Spectral phase, warp-cooperative: for every ray of the warp whose
 //    spectral slots change in this attempt (emission in a stage, or a
 //    nonzero carried slope), the 32 lanes split its spectral bins, compute
-//    the six new stage slopes of each bin, the 5th-order update and the
+//    the five new stage slopes of each bin, the 5th-order update and the
 //    embedded error, reduce the error over the warp, and commit the bins if
 //    the attempt is accepted. The per-bin state (intensity, carried slope)
 //    lives in a per-warp scratch area [32 rays][np], read and written
@@ -31,8 +34,9 @@
 namespace rtw {
 
 constexpr unsigned kFull = 0xffffffffu;
+constexpr int kMaxWarps = 8;  // warps per CTA
 
-// Dormand-Prince coefficients (64BitConstants.jl:28-37)
+// Dormand-Prince coefficients (64BitConstants.jl:28-37): a_sl, b_l (= a_7l), b*_l.
 constexpr double a21 = 1.0 / 5;
 constexpr double a31 = 3.0 / 40, a32 = 9.0 / 40;
 constexpr double a41 = 44.0 / 45, a42 = -56.0 / 15, a43 = 32.0 / 9;
@@ -43,6 +47,47 @@ constexpr double b1 = 35.0 / 384, b3 = 500.0 / 1113, b4 = 125.0 / 192, b5 = -218
 constexpr double bs1 = 5179.0 / 57600, bs3 = 7571.0 / 16695, bs4 = 393.0 / 640, bs5 = -92097.0 / 339200,
                  bs6 = 187.0 / 2100, bs7 = 1.0 / 40;
 constexpr double e1 = b1 - bs1, e3 = b3 - bs3, e4 = b4 - bs4, e5 = b5 - bs5, e6 = b6 - bs6, e7 = -bs7;
+
+// Shifted-accumulator form of the tableau. S[j] holds the partial sum
+// sum_l a_{t,l} k_l of stage t = s + j while stage s is evaluated; after k_s,
+// S[j] <- S[j+1] + kCoef[s-2][j] k_s with kCoef[s-2][j] = a_{s+1+j, s}
+// (zero past stage 7). init_coef(j) = a_{2+j, 1}; the error weights are b_s - b*_s.
+#define RTW_COEF_TABLE                 \
+    {{a32, a42, a52, a62, 0.0},        \
+     {a43, a53, a63, b3, 0.0},         \
+     {a54, a64, b4, 0.0, 0.0},         \
+     {a65, b5, 0.0, 0.0, 0.0},         \
+     {b6, 0.0, 0.0, 0.0, 0.0},         \
+     {0.0, 0.0, 0.0, 0.0, 0.0}}
+#define RTW_ERR_TABLE {e1, 0.0, e3, e4, e5, e6, e7}
+__constant__ double c_coef_d[6][5] = RTW_COEF_TABLE;
+__constant__ float c_coef_f[6][5] = RTW_COEF_TABLE;
+__constant__ double c_err_d[7] = RTW_ERR_TABLE;
+__constant__ float c_err_f[7] = RTW_ERR_TABLE;
+static const double h_coef[6][5] = RTW_COEF_TABLE;
+static const double h_err[7] = RTW_ERR_TABLE;
+RTW_HD constexpr double init_coef(int j) {
+    return j == 0 ? a21 : j == 1 ? a31 : j == 2 ? a41 : j == 3 ? a51 : j == 4 ? a61 : b1;
+}
+
+template <class R>
+RTW_HD R dp_coef(int it, int j) {
+#ifdef __CUDA_ARCH__
+    if constexpr (sizeof(R) == 4) return R(c_coef_f[it][j]);
+    else return R(c_coef_d[it][j]);
+#else
+    return R(h_coef[it][j]);
+#endif
+}
+template <class R>
+RTW_HD R dp_err(int s1) {
+#ifdef __CUDA_ARCH__
+    if constexpr (sizeof(R) == 4) return R(c_err_f[s1]);
+    else return R(c_err_d[s1]);
+#else
+    return R(h_err[s1]);
+#endif
+}
 
 // Spectral scratch layout of one warp: for each field, [32 rays][np] values of
 // type SR. Fields: 0 = intensity (high part), 1 = carried slope k1,
@@ -62,18 +107,14 @@ struct SpecTraits<true> {
 
 // Intensity slope of a bin: -A / (exp(X nu) - 1).
 __device__ __forceinline__ float bin_slope(float A, float X2, float nu) {
-    // X2 = X * log2(e): one MUFU ex2 per bin and stage
+    // X2 = X * log2(e): one MUFU ex2 and one MUFU rcp per bin and stage
     return (A == 0.0f) ? 0.0f : __fdividef(-A, exp2f(X2 * nu) - 1.0f);
 }
 __device__ __forceinline__ double bin_slope(double A, double X, double nu) {
     return (A == 0.0) ? 0.0 : -A / (exp(X * nu) - 1.0);
 }
-template <class SR>
-__device__ __forceinline__ SR x_for_bins(SR X);
-template <>
-__device__ __forceinline__ float x_for_bins<float>(float X) { return X * 1.4426950408889634f; }
-template <>
-__device__ __forceinline__ double x_for_bins<double>(double X) { return X; }
+__device__ __forceinline__ float x_for_bins(float X) { return X * 1.4426950408889634f; }
+__device__ __forceinline__ double x_for_bins(double X) { return X; }
 
 __device__ __forceinline__ float rabs(float v) { return fabsf(v); }
 __device__ __forceinline__ double rabs(double v) { return fabs(v); }
@@ -116,81 +157,124 @@ __device__ __forceinline__ void decide(CT err2, int L, double h, double max_dt, 
 }
 
 // One Dormand-Prince attempt of the geodesic + tau components in arithmetic R.
-// x: FP64 state (8 geodesic + tau); k1: carried slope. Outputs the tentative
-// state y (FP64), the slope carried to the next step, the emitter numbers of
-// stages 2..7 and the un-normalised squared error (arithmetic CT) of the
-// geodesic and tau components (the tau term counted once per bin). Stage
-// vectors carry a 10th entry, r - r_horizon, formed from the FP64 state.
+// x: FP64 state (8 geodesic + tau); k1: carried slope. Outputs the 5th-order
+// slope ns = sum_l b_l k_l (the new state is x + h ns), the slope carried to
+// the next step (ns, or k7 with FSAL), the emitter numbers of stages 2..7
+// (A[j * stride], X[j * stride]) and the un-normalised squared error
+// (arithmetic CT) of the geodesic and tau components (the tau term counted
+// once per bin). Stage vectors carry a 10th entry, r - r_horizon, formed from
+// the FP64 state. With R = double the stage points are the reference's
+// Ray + h * sum(a k) and the 7th stage is evaluated at y = Ray + h * ns.
 template <class SC, class R, class K, class SR, class CT>
-RTW_HD void dp45_attempt(const DevScene& s, const double* x, const K* k1in, double h, double tol,
-                                             int nbins, bool fsal, double* y, K* nk1, SR* A, SR* X, CT& err2,
-                                             bool& emit) {
-    R k[7][9];
-    R xr[9], z[10], cmb[9];
+RTW_HD void dp45_attempt(const DevScene& s, const double* x, const K* k1in, double h, double tol, int nbins,
+                         bool fsal, K* ns_out, K* nk1, SR* A, SR* X, int stride, CT& err2, bool& emit) {
+    // Components that enter the right-hand side (r, theta, k^mu, tau) carry the
+    // six shifted stage sums; t and phi (indices 0, 3) enter no right-hand side,
+    // so only their b-weighted sum (the 5th-order slope) is kept.
+    constexpr int kC = 7;
+    constexpr int kIdx[kC] = {1, 2, 4, 5, 6, 7, 8};
+    R S[6][kC], es[9], k[9], z[10], xr[kC], nt, np3;
     Emit<R> em;
     const R hr = R(h);
     const R d0 = R(x[1] - s.r_ev);
 #pragma unroll
-    for (int i = 0; i < 9; ++i) {
-        k[0][i] = R(k1in[i]);
-        xr[i] = R(x[i]);
-    }
-#define RTW_STAGE(EXPR, J)                                   \
-    _Pragma("unroll") for (int i = 0; i < 9; ++i) {          \
-        cmb[i] = EXPR;                                       \
-        z[i] = xr[i] + hr * cmb[i];                          \
-    }                                                        \
-    z[9] = d0 + hr * cmb[1];                                 \
-    SC::template rhs<R>(s, z, k[J], em);                     \
-    A[J - 1] = SR(em.A);                                     \
-    X[J - 1] = SR(em.X);
-    RTW_STAGE(k[0][i] * R(a21), 1)
-    RTW_STAGE(k[0][i] * R(a31) + k[1][i] * R(a32), 2)
-    RTW_STAGE(k[0][i] * R(a41) + k[1][i] * R(a42) + k[2][i] * R(a43), 3)
-    RTW_STAGE(k[0][i] * R(a51) + k[1][i] * R(a52) + k[2][i] * R(a53) + k[3][i] * R(a54), 4)
-    RTW_STAGE(k[0][i] * R(a61) + k[1][i] * R(a62) + k[2][i] * R(a63) + k[3][i] * R(a64) + k[4][i] * R(a65), 5)
-#undef RTW_STAGE
-    R ns[9];
+    for (int c = 0; c < kC; ++c) {
+        xr[c] = R(x[kIdx[c]]);
+        const R k1 = R(k1in[kIdx[c]]);
 #pragma unroll
-    for (int i = 0; i < 9; ++i)
-        ns[i] = k[0][i] * R(b1) + k[2][i] * R(b3) + k[3][i] * R(b4) + k[4][i] * R(b5) + k[5][i] * R(b6);
-#pragma unroll
-    for (int i = 0; i < 9; ++i) {
-        y[i] = x[i] + h * (double)ns[i];
-        z[i] = R(y[i]);
+        for (int j = 0; j < 6; ++j) S[j][c] = R(init_coef(j)) * k1;
     }
-    z[9] = R(y[1] - s.r_ev);
-    SC::template rhs<R>(s, z, k[6], em);
-    A[5] = SR(em.A);
-    X[5] = SR(em.X);
-    CT acc = 0;
+    nt = R(b1) * R(k1in[0]);
+    np3 = R(b1) * R(k1in[3]);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) es[i] = R(e1) * R(k1in[i]);
+    z[0] = R(0);
+    z[3] = R(0);
+    emit = false;
+#pragma unroll 1
+    for (int it = 0; it < 6; ++it) {
+#pragma unroll
+        for (int c = 0; c < kC; ++c) z[kIdx[c]] = xr[c] + hr * S[0][c];
+        z[9] = d0 + hr * S[0][0];
+        SC::template rhs<R>(s, z, k, em);
+        A[it * stride] = SR(em.A);
+        X[it * stride] = SR(em.X);
+        if (it > 0) emit = emit || (em.A != R(0));  // stage 2 has no weight in the bin update
+        // Zero tableau entries (b2 = b*2 = 0, stages past 7) enter as 0 * k,
+        // which is an exact 0 for any finite slope.
+        const R ew = dp_err<R>(it + 1);
+#pragma unroll
+        for (int i = 0; i < 9; ++i) es[i] = es[i] + ew * k[i];
+        if (it < 5) {
+            // b_{it+2} is the coefficient into stage 7 (column 4 - it)
+            const R bw = dp_coef<R>(it, 4 - it);
+            nt = nt + bw * k[0];
+            np3 = np3 + bw * k[3];
+#pragma unroll
+            for (int j = 0; j < 5; ++j) {
+                const R cf = dp_coef<R>(it, j);
+#pragma unroll
+                for (int c = 0; c < kC; ++c) S[j][c] = S[j + 1][c] + cf * k[kIdx[c]];
+            }
+        }
+    }
+    // after the 7th stage: z holds y (r, theta, k, tau), S[0] the 5th-order slope
+#pragma unroll
+    for (int c = 0; c < kC; ++c) ns_out[kIdx[c]] = K(S[0][c]);
+    ns_out[0] = K(nt);
+    ns_out[3] = K(np3);
+    if (fsal) {
+#pragma unroll
+        for (int i = 0; i < 9; ++i) nk1[i] = K(k[i]);
+    } else {
+#pragma unroll
+        for (int i = 0; i < 9; ++i) nk1[i] = ns_out[i];
+    }
+    z[0] = R(x[0]) + hr * nt;
+    z[3] = R(x[3]) + hr * np3;
+    CT acc = CT(0);
     const CT hc = CT(h), tc = CT(tol);
 #pragma unroll
     for (int i = 0; i < 9; ++i) {
-        const R e = k[0][i] * R(e1) + k[2][i] * R(e3) + k[3][i] * R(e4) + k[4][i] * R(e5) + k[5][i] * R(e6) +
-                    k[6][i] * R(e7);
-        const CT d = hc * CT(e);
-        const CT tl = tc + cmax(cabs(CT(x[i])), cabs(CT(y[i]))) * tc;
+        const CT d = hc * CT(es[i]);
+        const CT xa = (i == 0 || i == 3) ? CT(x[i]) : CT(xr[i < 3 ? i - 1 : i - 2]);
+        const CT tl = tc + cmax(cabs(xa), cabs(CT(z[i]))) * tc;
         const CT q = cdiv(d, tl);
-        acc += (i < 8 ? CT(1) : (CT)nbins) * q * q;
+        acc += (i < 8 ? CT(1) : CT(nbins)) * q * q;
     }
     err2 = acc;
-#pragma unroll
-    for (int i = 0; i < 9; ++i) nk1[i] = K(fsal ? k[6][i] : ns[i]);
-    // stage 2 carries no weight in the bin update (b2 = b*2 = 0)
-    emit = false;
-#pragma unroll
-    for (int j = 1; j < 6; ++j) emit |= (A[j] != SR(0));
 }
+
+// Outputs of one attempt, returned by value from the out-of-line FP64 attempt
+// so that no lane array of the hot path has its address taken.
+template <class K, class CT>
+struct AttemptOut {
+    K ns[9];
+    K nk1[9];
+    CT err2;
+    bool emit;
+};
 
 // The promoted (FP64-stage) attempt of the mixed path, kept out of line so
 // that its register demand does not set the register budget of the hot FP32
 // path; it runs for few rays.
 template <class SC, class K, class SR, class CT>
-__device__ __noinline__ void dp45_attempt_fp64(const DevScene& s, const double* x, const K* k1in, double h,
-                                                double tol, int nbins, bool fsal, double* y, K* nk1, SR* A, SR* X,
-                                                CT& err2, bool& emit) {
-    dp45_attempt<SC, double, K, SR, CT>(s, x, k1in, h, tol, nbins, fsal, y, nk1, A, X, err2, emit);
+__device__ __noinline__ AttemptOut<K, CT> dp45_attempt_fp64(const DevScene& s, const double* x, const K* k1in,
+                                                             double h, double tol, int nbins, bool fsal, SR* A,
+                                                             SR* X, int stride) {
+    AttemptOut<K, CT> o;
+    dp45_attempt<SC, double, K, SR, CT>(s, x, k1in, h, tol, nbins, fsal, o.ns, o.nk1, A, X, stride, o.err2, o.emit);
+    return o;
+}
+
+// FP64 right-hand side, out of line (initial slope, polar escape).
+template <class SC>
+__device__ __noinline__ void rhs_fp64(const DevScene& s, const double* x9, double* k, Emit<double>* em) {
+    double z[10];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) z[i] = x9[i];
+    z[9] = x9[1] - s.r_ev;
+    SC::template rhs<double>(s, z, k, *em);
 }
 
 // Camera ray of pixel (i, j) of a frame (initialization.jl:213-240,327), FP64.
@@ -221,21 +305,133 @@ __device__ __forceinline__ void camera_ray(const FrameDesc& f, int i, int j, dou
     x[8] = 0.0;
 }
 
+// Pixel (i, j) of the local ray id of a frame. Order 0: row order. Order 1:
+// 8x4 tiles in row-major tile order; the columns right of the last full tile
+// form a narrower tile, rows below the last full tile row are in row order.
+__device__ __forceinline__ void pixel_of(int order, long long local, int xp, int yp, int& pi, int& pj) {
+    if (order != 1) {
+        pi = (int)(local % xp);
+        pj = (int)(local / xp);
+        return;
+    }
+    const int tw = 8, th = 4;
+    const int full_rows = yp / th;
+    const long long per_row = (long long)th * xp;
+    const long long trow = local / per_row;
+    if (trow < full_rows) {
+        const long long rem = local - trow * per_row;
+        const int full_cols = xp / tw;
+        const long long in_full = (long long)full_cols * tw * th;
+        if (rem < in_full) {
+            const int tc = (int)(rem / (tw * th));
+            const int w = (int)(rem % (tw * th));
+            pi = tc * tw + (w % tw);
+            pj = (int)trow * th + w / tw;
+        } else {
+            const int w = (int)(rem - in_full);
+            const int rw = xp - full_cols * tw;
+            pi = full_cols * tw + (w % rw);
+            pj = (int)trow * th + w / rw;
+        }
+    } else {
+        const long long rem = local - (long long)full_rows * per_row;
+        pi = (int)(rem % xp);
+        pj = full_rows * th + (int)(rem / xp);
+    }
+}
+
 __device__ __forceinline__ float warp_sum(float v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
-    return v;
+    return __shfl_sync(kFull, v, 0);  // one association order for every lane
 }
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
-    return v;
+    return __shfl_sync(kFull, v, 0);
 }
 
-// Launch bounds: the mixed kernel is capped at 128 registers (4 CTAs of 128
-// threads per SM); its rare FP64 paths spill instead of the hot FP32 path.
+// Polar / origin escape (integrators_LttM.jl:62-105): 37 explicit Euler steps
+// of size temp through the coordinate singularity, FP64; the spectral slots of
+// this ray (its row of the warp's scratch) are updated by this lane.
+// x and k1 (copies of the lane state) are updated in place. Returns whether
+// the ray terminated inside the escape; otherwise k1 is the slope at the new
+// position and spec_live tells whether any bin slope is nonzero.
+struct EscapeOut {
+    bool terminated;
+    bool spec_live;
+    unsigned substeps;
+};
+template <int KIND, bool MIXED>
+__device__ __noinline__ EscapeOut polar_escape(const KParams& p, double* x, typename SpecTraits<MIXED>::SR* k1,
+                                               double temp, double r_term, double thick,
+                                               typename SpecTraits<MIXED>::SR* rI,
+                                               typename SpecTraits<MIXED>::SR* rK,
+                                               typename SpecTraits<MIXED>::SR* rL, bool spec_live_in) {
+    EscapeOut out;
+    out.terminated = false;
+    out.spec_live = spec_live_in;
+    out.substeps = 0;
+    typedef typename SceneOf<KIND>::type SC;
+    typedef typename SpecTraits<MIXED>::SR SR;
+    const int N = p.n_bins;
+    const DevScene& s = p.sc;
+    auto euler_spec = [&]() {
+        for (int c = 0; c < N; ++c) {
+            const SR t = SR(-temp) * rK[c];
+            if constexpr (MIXED) {
+                float hi = rI[c], lo = rL[c];
+                kahan_add(hi, lo, t);
+                rI[c] = hi;
+                rL[c] = lo;
+            } else {
+                rI[c] = rI[c] + t;
+            }
+        }
+    };
+    auto slope_all = [&]() {
+        double kd[9];
+        Emit<double> e;
+        rhs_fp64<SC>(s, x, kd, &e);
+        for (int i = 0; i < 9; ++i) k1[i] = SR(kd[i]);
+        const SR Ae = SR(e.A), Xe = x_for_bins(SR(e.X));
+        bool nz = false;
+        for (int c = 0; c < N; ++c) {
+            const SR v = bin_slope(Ae, Xe, SR(p.bin_nu[c]));
+            rK[c] = v;
+            nz |= v != SR(0);
+        }
+        out.spec_live = nz;
+    };
+    for (int i = 0; i < 9; ++i) x[i] -= temp * double(k1[i]);
+    euler_spec();
+    keep_in_bounds<KIND>(x);
+    ++out.substeps;
+    for (int it = 0; it < 36; ++it) {
+        if (!terminate_geo<KIND>(s, x, r_term, thick)) {
+            slope_all();
+            for (int i = 0; i < 9; ++i) x[i] -= temp * double(k1[i]);
+            euler_spec();
+            keep_in_bounds<KIND>(x);
+            ++out.substeps;
+        }
+    }
+    if (terminate_geo<KIND>(s, x, r_term, thick)) {
+        out.terminated = true;
+        return out;
+    }
+    slope_all();
+    return out;
+}
+
+// Launch bounds: 128 threads per CTA; RTW_MIXED_MIN_CTAS resident CTAs per SM
+// for the mixed kernel (3: 168 registers per thread, measured faster than 4
+// with spills or 2), 2 for the FP64 kernel.
+#ifndef RTW_MIXED_MIN_CTAS
+#define RTW_MIXED_MIN_CTAS 3
+#endif
 template <int KIND, bool MIXED, int BPL>
-__global__ void __launch_bounds__(128, MIXED ? 4 : 2) trace_kernel(const KParams p) {
+__global__ void __launch_bounds__(128, MIXED ? RTW_MIXED_MIN_CTAS : 2) trace_kernel(const KParams p) {
     typedef typename SceneOf<KIND>::type SC;
     typedef SpecTraits<MIXED> ST;
     typedef typename ST::SR SR;
@@ -243,7 +439,11 @@ __global__ void __launch_bounds__(128, MIXED ? 4 : 2) trace_kernel(const KParams
     typedef typename ST::SR R;  // stage arithmetic (promoted to double per ray)
     typedef typename ST::SR CT; // step-controller arithmetic
 
+    // per-lane emitter numbers of stages 2..7, read by the spectral phase
+    __shared__ SR s_ax[kMaxWarps][2][6][32];
+
     const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
     const long long warp_id = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int N = p.n_bins;
     const int np = p.np;
@@ -253,26 +453,28 @@ __global__ void __launch_bounds__(128, MIXED ? 4 : 2) trace_kernel(const KParams
     SR* sI = spec;                  // [32][np]
     SR* sK = spec + 32 * np;        // [32][np]
     SR* sL = spec + 2 * 32 * np;    // [32][np] (MIXED only)
+    SR* myA = &s_ax[wib][0][0][lane];
+    SR* myX = &s_ax[wib][1][0][lane];
 
     // per-lane bin frequencies
     SR nub[BPL];
 #pragma unroll
     for (int b = 0; b < BPL; ++b) {
         const int c = lane + 32 * b;
-        nub[b] = c < N ? (SR)p.bin_nu[c] : SR(0);
+        nub[b] = c < N ? SR(p.bin_nu[c]) : SR(0);
     }
 
     // lane ray state
     bool active = false, dry = false;
     long long gid = 0;  // global output index
-    double x[10];
+    double x[9];
     K k1[9];
     double h = 0, tol = 0, r_term = 0, thick = 0;
     long long max_steps = 0;
     long long nsteps = 0;
     bool prev_rej = false, spec_live = false;
     // local counters
-    unsigned long long c_att = 0, c_rej = 0, c_pro = 0, c_spec = 0, c_emit = 0, c_esc = 0, c_nan = 0, c_rays = 0;
+    unsigned c_att = 0, c_rej = 0, c_pro = 0, c_spec = 0, c_emit = 0, c_esc = 0, c_nan = 0, c_rays = 0;
 
     for (;;) {
         // ---------------- refill -----------------------------------------
@@ -289,62 +491,25 @@ __global__ void __launch_bounds__(128, MIXED ? 4 : 2) trace_kernel(const KParams
             if (!active) {
                 const long long id = (long long)base + __popc(empty & ((1u << lane) - 1u));
                 if (id < p.total_rays) {
-                    // frame lookup
                     int lo = 0, hi = p.n_frames - 1;
                     while (lo < hi) {
                         const int mid = (lo + hi + 1) >> 1;
                         if (p.frames[mid].ray_begin <= id) lo = mid; else hi = mid - 1;
                     }
                     const FrameDesc& f = p.frames[lo];
-                    const long long local = id - f.ray_begin;
                     int pi, pj;
-                    if (p.pixel_order == 1) {
-                        // 8x4 tiles in row-major tile order; partial edge tiles
-                        // are handled by mapping through the tile grid.
-                        const int tw = 8, th = 4;
-                        const int ntx = (f.xp + tw - 1) / tw;
-                        long long rem = local;
-                        // full-height tile rows
-                        const int full_rows = f.yp / th;
-                        const long long per_row = (long long)th * f.xp;
-                        const int trow = (int)(rem / per_row);
-                        if (trow < full_rows) {
-                            rem -= (long long)trow * per_row;
-                            const int full_cols = f.xp / tw;
-                            const long long in_full = (long long)full_cols * tw * th;
-                            if (rem < in_full) {
-                                const int tc = (int)(rem / (tw * th));
-                                const int w = (int)(rem % (tw * th));
-                                pi = tc * tw + (w % tw);
-                                pj = trow * th + w / tw;
-                            } else {
-                                const int w = (int)(rem - in_full);
-                                const int rw = f.xp - full_cols * tw;
-                                pi = full_cols * tw + (w % rw);
-                                pj = trow * th + w / rw;
-                            }
-                        } else {
-                            rem -= (long long)full_rows * per_row;
-                            pi = (int)(rem % f.xp);
-                            pj = full_rows * th + (int)(rem / f.xp);
-                        }
-                        (void)ntx;
-                    } else {
-                        pi = (int)(local % f.xp);
-                        pj = (int)(local / f.xp);
-                    }
+                    pixel_of(p.pixel_order, id - f.ray_begin, f.xp, f.yp, pi, pj);
                     gid = f.ray_begin + pi + (long long)f.xp * pj;
                     camera_ray(f, pi, pj, x);
-                    x[9] = 0.0;
                     tol = f.tol;
                     r_term = f.r_term;
                     thick = f.thick;
                     max_steps = f.max_steps;
                     h = -pad_max_dt<KIND, CT>(s, x, p.max_dt_scale);
                     double kd[9];
-                    SC::template rhs<double>(s, x, kd, em0);
+                    rhs_fp64<SC>(s, x, kd, &em0);
 #pragma unroll
-                    for (int i = 0; i < 9; ++i) k1[i] = (K)kd[i];
+                    for (int i = 0; i < 9; ++i) k1[i] = K(kd[i]);
                     nsteps = 0;
                     prev_rej = false;
                     spec_live = em0.A != 0.0;
@@ -360,8 +525,8 @@ __global__ void __launch_bounds__(128, MIXED ? 4 : 2) trace_kernel(const KParams
             while (fm) {
                 const int r = __ffs(fm) - 1;
                 fm &= fm - 1;
-                const SR A0 = (SR)__shfl_sync(kFull, em0.A, r);
-                const SR X0 = x_for_bins<SR>((SR)__shfl_sync(kFull, em0.X, r));
+                const SR A0 = SR(__shfl_sync(kFull, em0.A, r));
+                const SR X0 = x_for_bins(SR(__shfl_sync(kFull, em0.X, r)));
 #pragma unroll
                 for (int b = 0; b < BPL; ++b) {
                     const int c = lane + 32 * b;
@@ -377,9 +542,8 @@ __global__ void __launch_bounds__(128, MIXED ? 4 : 2) trace_kernel(const KParams
         if (!act) break;
 
         // ---------------- geodesic phase ---------------------------------
-        double y[9];
-        K nk1[9];
-        SR A[6], X[6];
+        K ns[9];   // 5th-order slope: the new state is x + h ns
+        K nk1[9];  // slope carried to the next attempt
         CT err2 = 0;
         double max_dt = 0, hnext = h;
         bool emit = false, esc_done = false, decided = false, accept = false;
@@ -388,67 +552,29 @@ __global__ void __launch_bounds__(128, MIXED ? 4 : 2) trace_kernel(const KParams
             max_dt = pad_max_dt<KIND, CT>(s, x, p.max_dt_scale);
             double temp;
             if (near_singularity<KIND>(x, h, tol, &temp)) {
-                // Polar / origin escape (integrators_LttM.jl:62-105): 37 explicit
-                // Euler steps of size temp through the coordinate singularity,
-                // FP64, the spectral slots of this ray updated by this lane.
-                SR* rI = sI + lane * np;
-                SR* rK = sK + lane * np;
-                SR* rL = sL + lane * np;
-                auto euler_spec = [&](double tmp) {
-                    for (int c = 0; c < N; ++c) {
-                        const SR t = (SR)(-tmp) * rK[c];
-                        if constexpr (MIXED) {
-                            float hi = (float)rI[c], lo = (float)rL[c];
-                            kahan_add(hi, lo, (float)t);
-                            rI[c] = (SR)hi;
-                            rL[c] = (SR)lo;
-                        } else {
-                            rI[c] = rI[c] + t;
-                        }
-                    }
-                };
-                auto slope_spec = [&](const Emit<double>& e) {
-                    const SR Ae = (SR)e.A, Xe = x_for_bins<SR>((SR)e.X);
-                    bool nz = false;
-                    for (int c = 0; c < N; ++c) {
-                        const SR v = bin_slope(Ae, Xe, (SR)p.bin_nu[c]);
-                        rK[c] = v;
-                        nz |= v != SR(0);
-                    }
-                    return nz;
-                };
+                // out of line on copies, so that x and k1 stay in registers
+                double xe[9];
+                K ke[9];
 #pragma unroll
-                for (int i = 0; i < 9; ++i) x[i] -= temp * (double)k1[i];
-                euler_spec(temp);
-                keep_in_bounds<KIND>(x);
-                ++c_esc;
-                for (int it = 0; it < 36; ++it) {
-                    if (!terminate_geo<KIND>(s, x, r_term, thick)) {
-                        double kd[9];
-                        Emit<double> e;
-                        SC::template rhs<double>(s, x, kd, e);
-#pragma unroll
-                        for (int i = 0; i < 9; ++i) k1[i] = (K)kd[i];
-                        spec_live = slope_spec(e);
-#pragma unroll
-                        for (int i = 0; i < 9; ++i) x[i] -= temp * (double)k1[i];
-                        euler_spec(temp);
-                        keep_in_bounds<KIND>(x);
-                        ++c_esc;
-                    }
+                for (int i = 0; i < 9; ++i) {
+                    xe[i] = x[i];
+                    ke[i] = k1[i];
                 }
-                if (terminate_geo<KIND>(s, x, r_term, thick)) {
+                const EscapeOut eo = polar_escape<KIND, MIXED>(p, xe, ke, temp, r_term, thick, sI + lane * np,
+                                                               sK + lane * np, sL + lane * np, spec_live);
+#pragma unroll
+                for (int i = 0; i < 9; ++i) {
+                    x[i] = xe[i];
+                    k1[i] = ke[i];
+                }
+                spec_live = eo.spec_live;
+                c_esc += eo.substeps;
+                if (eo.terminated) {
                     esc_done = true;
                     decided = true;
                     accept = true;
                     hnext = h;
                 } else {
-                    double kd[9];
-                    Emit<double> e;
-                    SC::template rhs<double>(s, x, kd, e);
-#pragma unroll
-                    for (int i = 0; i < 9; ++i) k1[i] = (K)kd[i];
-                    spec_live = slope_spec(e);
                     h = -pad_max_dt<KIND, CT>(s, x, p.max_dt_scale);
                 }
             }
@@ -460,13 +586,30 @@ __global__ void __launch_bounds__(128, MIXED ? 4 : 2) trace_kernel(const KParams
                 }
                 if (promote) {
                     ++c_pro;
-                    dp45_attempt_fp64<SC, K, SR, CT>(s, x, k1, h, tol, N, p.fsal != 0, y, nk1, A, X, err2, emit);
+                    double xe[9];
+                    K ke[9];
+#pragma unroll
+                    for (int i = 0; i < 9; ++i) {
+                        xe[i] = x[i];
+                        ke[i] = k1[i];
+                    }
+                    const AttemptOut<K, CT> o =
+                        dp45_attempt_fp64<SC, K, SR, CT>(s, xe, ke, h, tol, N, p.fsal != 0, myA, myX, 32);
+#pragma unroll
+                    for (int i = 0; i < 9; ++i) {
+                        ns[i] = o.ns[i];
+                        nk1[i] = o.nk1[i];
+                    }
+                    err2 = o.err2;
+                    emit = o.emit;
                 } else {
-                    dp45_attempt<SC, R, K, SR, CT>(s, x, k1, h, tol, N, p.fsal != 0, y, nk1, A, X, err2, emit);
+                    dp45_attempt<SC, R, K, SR, CT>(s, x, k1, h, tol, N, p.fsal != 0, ns, nk1, myA, myX, 32, err2,
+                                                   emit);
                 }
                 if (emit) ++c_emit;
             }
         }
+        __syncwarp();
 
         // ---------------- spectral phase (warp-cooperative) --------------
         const bool need = active && !esc_done && (emit || spec_live);
@@ -475,18 +618,19 @@ __global__ void __launch_bounds__(128, MIXED ? 4 : 2) trace_kernel(const KParams
         while (nm) {
             const int r = __ffs(nm) - 1;
             nm &= nm - 1;
-            SR Ar[6], Xr[6];
+            SR Ar[5], Xr[5];
 #pragma unroll
-            for (int j = 0; j < 6; ++j) {
-                Ar[j] = __shfl_sync(kFull, A[j], r);
-                Xr[j] = x_for_bins<SR>(__shfl_sync(kFull, X[j], r));
+            for (int j = 0; j < 5; ++j) {  // stages 3..7
+                Ar[j] = s_ax[wib][0][j + 1][r];
+                Xr[j] = x_for_bins(s_ax[wib][1][j + 1][r]);
             }
             const double hr = __shfl_sync(kFull, h, r);
             const double tr = __shfl_sync(kFull, tol, r);
-            const SR hs = (SR)hr;
-            const SR ts = (SR)tr;
+            const SR hs = SR(hr);
+            const SR ts = SR(tr);
             SR yv[BPL], yl[BPL], nk[BPL];
             SR acc = 0;
+            bool nz = false;
 #pragma unroll
             for (int b = 0; b < BPL; ++b) {
                 const int c = lane + 32 * b;
@@ -494,11 +638,11 @@ __global__ void __launch_bounds__(128, MIXED ? 4 : 2) trace_kernel(const KParams
                 if (c < N) {
                     const SR I = sI[r * np + c];
                     const SR kk1 = sK[r * np + c];
-                    const SR kk3 = bin_slope(Ar[1], Xr[1], nub[b]);
-                    const SR kk4 = bin_slope(Ar[2], Xr[2], nub[b]);
-                    const SR kk5 = bin_slope(Ar[3], Xr[3], nub[b]);
-                    const SR kk6 = bin_slope(Ar[4], Xr[4], nub[b]);
-                    const SR kk7 = bin_slope(Ar[5], Xr[5], nub[b]);
+                    const SR kk3 = bin_slope(Ar[0], Xr[0], nub[b]);
+                    const SR kk4 = bin_slope(Ar[1], Xr[1], nub[b]);
+                    const SR kk5 = bin_slope(Ar[2], Xr[2], nub[b]);
+                    const SR kk6 = bin_slope(Ar[3], Xr[3], nub[b]);
+                    const SR kk7 = bin_slope(Ar[4], Xr[4], nub[b]);
                     // (k2 has zero weight in both the 5th-order update and the
                     // error estimate, and the intensity slopes do not depend on
                     // the intensity, so stage 2 needs no bin work.)
@@ -507,10 +651,10 @@ __global__ void __launch_bounds__(128, MIXED ? 4 : 2) trace_kernel(const KParams
                                   kk7 * SR(e7);
                     SR yy, ylo = 0;
                     if constexpr (MIXED) {
-                        float hi = (float)I, lo = (float)sL[r * np + c];
-                        kahan_add(hi, lo, (float)(hs * ns));
-                        yy = (SR)hi;
-                        ylo = (SR)lo;
+                        float hi = I, lo = sL[r * np + c];
+                        kahan_add(hi, lo, hs * ns);
+                        yy = hi;
+                        ylo = lo;
                     } else {
                         yy = I + hs * ns;
                     }
@@ -521,18 +665,17 @@ __global__ void __launch_bounds__(128, MIXED ? 4 : 2) trace_kernel(const KParams
                     yv[b] = yy;
                     yl[b] = ylo;
                     nk[b] = p.fsal ? kk7 : ns;
+                    nz |= nk[b] != SR(0);
                 }
             }
             acc = warp_sum(acc);
-            acc = __shfl_sync(kFull, acc, 0);
             int dec = 0;
             if (lane == r) {
-                decide<CT>(err2 + (CT)acc, L, h, max_dt, prev_rej, accept, hnext);
+                decide<CT>(err2 + CT(acc), L, h, max_dt, prev_rej, accept, hnext);
                 decided = true;
                 dec = accept ? 1 : 0;
             }
             dec = __shfl_sync(kFull, dec, r);
-            bool nz = false;
             if (dec) {
 #pragma unroll
                 for (int b = 0; b < BPL; ++b) {
@@ -541,13 +684,13 @@ __global__ void __launch_bounds__(128, MIXED ? 4 : 2) trace_kernel(const KParams
                         sI[r * np + c] = yv[b];
                         sK[r * np + c] = nk[b];
                         if constexpr (MIXED) sL[r * np + c] = yl[b];
-                        nz |= nk[b] != SR(0);
                     }
                 }
             }
             nz = __any_sync(kFull, nz);
             if (lane == r && dec) spec_live = nz;
         }
+        __syncwarp();
 
         // ---------------- controller + commit ----------------------------
         int cls = 0;
@@ -555,6 +698,9 @@ __global__ void __launch_bounds__(128, MIXED ? 4 : 2) trace_kernel(const KParams
             if (!decided) decide<CT>(err2, L, h, max_dt, prev_rej, accept, hnext);
             if (!esc_done) {
                 if (accept) {
+                    double y[9];
+#pragma unroll
+                    for (int i = 0; i < 9; ++i) y[i] = x[i] + h * double(ns[i]);
                     keep_in_bounds<KIND>(y);
 #pragma unroll
                     for (int i = 0; i < 9; ++i) {
@@ -627,14 +773,14 @@ __global__ void __launch_bounds__(128, MIXED ? 4 : 2) trace_kernel(const KParams
     }
 
     // counters
-    atomicAdd(&p.stats->step_attempts, c_att);
-    atomicAdd(&p.stats->rejected_steps, c_rej);
-    atomicAdd(&p.stats->promoted_steps, c_pro);
-    atomicAdd(&p.stats->spectral_steps, c_spec);
-    atomicAdd(&p.stats->emitting_steps, c_emit);
-    atomicAdd(&p.stats->escape_substeps, c_esc);
-    atomicAdd(&p.stats->nan_rays, c_nan);
-    atomicAdd(&p.stats->rays, c_rays);
+    atomicAdd(&p.stats->step_attempts, (unsigned long long)c_att);
+    atomicAdd(&p.stats->rejected_steps, (unsigned long long)c_rej);
+    atomicAdd(&p.stats->promoted_steps, (unsigned long long)c_pro);
+    atomicAdd(&p.stats->spectral_steps, (unsigned long long)c_spec);
+    atomicAdd(&p.stats->emitting_steps, (unsigned long long)c_emit);
+    atomicAdd(&p.stats->escape_substeps, (unsigned long long)c_esc);
+    atomicAdd(&p.stats->nan_rays, (unsigned long long)c_nan);
+    atomicAdd(&p.stats->rays, (unsigned long long)c_rays);
 }
 
 }  // namespace rtw
