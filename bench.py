@@ -220,12 +220,12 @@ def run_b200(args):
     out.xyz, out.term_class, out.steps, out.on_device = xyz.data_ptr(), cls.data_ptr(), steps.data_ptr(), 1
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
 
-    def params(p):
-        return r.params(colors, precision=p, stream=stream.cuda_stream, block_warps=args.block_warps,
-                        ctas_per_sm=args.ctas_per_sm)
+    def params(p, integ=abi.DP45_REF_COMPAT):
+        return r.params(colors, precision=p, integrator=integ, stream=stream.cuda_stream,
+                        block_warps=args.block_warps, ctas_per_sm=args.ctas_per_sm)
 
-    def timed_renders(p, k, w):
-        prm = params(p)
+    def timed_renders(p, k, w, integ=abi.DP45_REF_COMPAT):
+        prm = params(p, integ)
         for _ in range(w):
             r.render_raw(scene, [cam], prm, out)
         torch.cuda.synchronize()
@@ -263,6 +263,15 @@ def run_b200(args):
         t64 = all_max(t64, world)
         fp64 = {"value": world * P * max(1, args.steps // 2) / (t64 * 1e-3) / 1e6,
                 "ms_per_step": t64 / max(1, args.steps // 2)}
+
+    # textbook FSAL Dormand-Prince (k1 = f(y)) instead of the reference's
+    # carried average slope: same workload, same timing rules
+    fsal = None
+    if not args.no_fp64_leg:
+        tf, _, _ = timed_renders(prec, max(1, args.steps // 2), 1, abi.DP45_FSAL)
+        tf = all_max(tf, world)
+        fsal = {"value": world * P * max(1, args.steps // 2) / (tf * 1e-3) / 1e6,
+                "ms_per_step": tf / max(1, args.steps // 2)}
 
     # end to end through the public API: host pinned outputs, synchronous call
     hx = torch.empty((P, 3), dtype=torch.float32, pin_memory=True)
@@ -305,6 +314,8 @@ def run_b200(args):
                        "rays_per_gpu": P, "parallelism": f"weak x{world} (one frame per GPU)",
                        "l2": "flushed (256 MB write) between timed renders"},
             "fp64": fp64,
+            "fsal": fsal,
+            "integrator": "reference step (k1 = previous sum b_i k_i)",
             "roofline": {"bound": "fp32" if prec == abi.PREC_MIXED else "fp64", "achieved": achieved, "peak": peak,
                          "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
                          "peak_source": "measured in-run FMA microbenchmark (rtw_measure_peaks)",

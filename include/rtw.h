@@ -144,8 +144,7 @@ typedef struct rtw_render_params {
     int32_t integrator;         /* rtw_integrator */
     int32_t ray_bundles;        /* must be 0 (bundles are not built) */
     double promote_dr;          /* MIXED: FP64 stages while r - r_horizon < promote_dr M
-                                   (<= 0: never, the default: the FP32 stages
-                                   carry r - r_horizon from the FP64 state) */
+                                   (0: default 1e-3; < 0: never) */
     double promote_sin;         /* MIXED: FP64 stages while sin(theta) < promote_sin
                                    (0: default 1e-2; < 0: never) */
     int32_t block_warps;        /* warps per CTA, 1..4 (0: default 4) */

@@ -540,9 +540,11 @@ rtw_status rtw_render(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* ca
     p.n_bins = N;
     p.total_rays = total;
     p.max_dt_scale = prm->max_dt_scale;
-    // promotion thresholds: < 0 disables, 0 takes the default (horizon: off,
-    // the FP32 stages carry r - r+ from the FP64 state; poles: sin < 1e-2)
-    const double pdr = prm->promote_dr > 0 ? prm->promote_dr : -1.0;
+    // promotion thresholds: < 0 disables, 0 takes the default. Horizon:
+    // r - r+ < 1e-3 M; there the radial acceleration is a sum of O(1/Delta)
+    // terms that cancel to O(1) and FP32 stages lose every digit before the
+    // (1 + 10 tol) r+ stop. Poles: sin(theta) < 1e-2.
+    const double pdr = prm->promote_dr < 0 ? -1.0 : (prm->promote_dr > 0 ? prm->promote_dr : 1e-3);
     const double psn = prm->promote_sin < 0 ? 0.0 : (prm->promote_sin > 0 ? std::min(prm->promote_sin, 1.0) : 1e-2);
     p.promote_dr = pdr * scene->mass;
     p.promote_theta = std::asin(psn);

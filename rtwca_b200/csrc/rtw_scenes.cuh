@@ -86,9 +86,10 @@ RTW_HD float rinv(float x) {
 // carry a large negative stage tau (the tableau has negative coefficients);
 // in FP32, exp(-tau) would overflow to inf and turn the embedded error into
 // NaN, which the reference's controller accepts. The FP32 form saturates at
-// exp(80): the slope stays finite and huge, the error rejects the step, as the
+// exp(40) (so a_nu emission_scale exp(-tau) / g and the squared error stay
+// finite in FP32): the slope stays huge, the error rejects the step, as the
 // FP64 form does.
-RTW_HD float attenuation(float tau) { return rexp_(fminf(-tau, 80.0f)); }
+RTW_HD float attenuation(float tau) { return rexp_(fminf(-tau, 40.0f)); }
 RTW_HD double attenuation(double tau) { return rexp_(-tau); }
 template <class R>
 RTW_HD R attenuation(R tau) { return rexp_(-tau); }

@@ -1,0 +1,44 @@
+"""Regenerates the golden fixtures of tests/golden/ from the CPU oracle.
+
+The reference (Julia) cannot run on any machine of this build and its own
+tests pin no numerical results, so the fixtures come from the oracle (the
+FP64 restatement of the reference's CPU integrator), pinned itself by
+tests/test_oracle_physics.py and tests/test_ref_integrator.py. Small cases:
+10x10 pixels (flat sphere 16x16, thick disk 8x8), 8 spectral bins, tolerance 1e-8, both step
+modes. Run: python tests/golden/make_golden.py
+"""
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+sys.path.insert(0, str(HERE.parent.parent))
+
+from oracle import oracle as O  # noqa: E402
+from rtwca_b200 import abi, configs  # noqa: E402
+
+CASES = {"minkowski_sphere": 16, "schwarzschild_disk": 10, "kerr_thin_disk": 10, "kerr_thick_disk": 8}
+N_COLORS = 8
+
+
+def case(name, integrator):
+    scene, cam, _ = configs.workload(name, x_pix=CASES[name])
+    colors = configs.log_spaced_colors(N_COLORS)
+    return scene, cam, colors, integrator
+
+
+def main():
+    O.build()
+    for name in CASES:
+        for integ, tag in ((abi.DP45_REF_COMPAT, "ref"), (abi.DP45_FSAL, "fsal")):
+            scene, cam, colors, _ = case(name, integ)
+            res = O.render(scene, cam, colors, integrator=integ)
+            np.savez_compressed(HERE / f"{name}_{tag}.npz", colors=colors, xyz=res["xyz"], term_class=res["class"],
+                                steps=res["steps"], spectrum=res["spectrum"], tau=res["tau"][:, 0],
+                                state=res["state"])
+            print(name, tag, np.bincount(res["class"], minlength=7).tolist())
+
+
+if __name__ == "__main__":
+    main()
