@@ -138,15 +138,17 @@ def cpu_sample_ids(P, n):
     return np.unique(np.linspace(0, P - 1, n).round().astype(np.int64))
 
 
-def cpu_time(scene, cam, colors, n, threads=0):
+def cpu_time(scene, cam, colors, n, threads=0, keep=False):
     from oracle import oracle as O
     O.build()
     P = cam.x_pix * cam.y_pix
     ids = cpu_sample_ids(P, n)
     t = time.perf_counter()
-    O.render(scene, cam, colors, pixel_ids=ids, threads=threads, want=("xyz", "class", "steps"))
+    res = O.render(scene, cam, colors, pixel_ids=ids, threads=threads, want=("xyz", "class", "steps"))
     dt = time.perf_counter() - t
     cores = threads if threads > 0 else (os.cpu_count() or 1)
+    if keep:
+        return ids.size / dt / 1e6, ids.size, dt, cores, res
     return ids.size / dt / 1e6, ids.size, dt, cores
 
 
@@ -300,11 +302,24 @@ def run_b200(args):
         achieved = flops / (kms * 1e-3) / 1e12
         peak = peaks["fp32_flops"] / 1e12 if prec == abi.PREC_MIXED else peaks["fp64_flops"] / 1e12
         cpu = None
+        parity = None
         if not args.no_cpu_baseline:
-            v, n, dt, cores = cpu_time(scene, cam, colors, args.cpu_sample)
+            v, n, dt, cores, ref = cpu_time(scene, cam, colors, args.cpu_sample, keep=True)
             cpu = {"value": v, "unit": "Mrays/s", "cores": cores, "kind": "port",
                    "sample": f"{n} evenly spaced pixels of the {args.x_pix}^2 frame ({dt:.1f} s), C++ FP64 "
                              "restatement of the reference's CPU integrator, OpenMP"}
+            # the same pixels of the (end-to-end) render against the FP64 oracle
+            ids = cpu_sample_ids(P, args.cpu_sample)
+            g_cls = hc.numpy()[ids]
+            g_y = hx.numpy()[ids, 1].astype(np.float64)
+            same = g_cls == ref["class"]
+            y_r = ref["xyz"][:, 1]
+            den = np.maximum(np.abs(y_r), 1e-6 * np.abs(y_r).max() + 1e-300)
+            err = np.abs(g_y - y_r) / den
+            parity = {"pixels": int(ids.size), "class_match": float(np.mean(same)),
+                      "intensity_within_1e-3": float(np.mean(err[same] <= 1e-3)),
+                      "p99_rel_err": float(np.quantile(err[same], 0.99)),
+                      "reference": "FP64 oracle, reference step, same pixels"}
         line = {
             "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
@@ -322,6 +337,7 @@ def run_b200(args):
                          "mufu_gops": mufu / (kms * 1e-3) / 1e9,
                          "mufu_peak_gops": peaks["mufu_ops"] / 1e9},
             "cpu_baseline": cpu,
+            "parity_sample": parity,
             "e2e": {"value": e2e_val, "unit": "Mrays/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": args.steps,
             "clocks": clk.summary(),

@@ -36,6 +36,8 @@ extern "C" {
 #define RTW_MAX_BINS 128
 /* Largest number of frames (cameras) one batched render takes. */
 #define RTW_MAX_FRAMES 4096
+/* Doubles per record of the step trace (rtw_outputs.trace). */
+#define RTW_TRACE_FIELDS 15
 
 typedef enum rtw_status {
     RTW_OK = 0,
@@ -154,6 +156,8 @@ typedef struct rtw_render_params {
     int32_t pixel_order;        /* 0: row order; 1: 8x4 tiles (internal order,
                                    outputs are always row order) */
     int32_t reserved;
+    int64_t trace_ray;          /* global pixel index whose step attempts are
+                                   recorded in rtw_outputs.trace; -1: none */
 } rtw_render_params;
 
 /* Output buffers, owned by the caller. Pixel p of frame f is at
@@ -172,7 +176,14 @@ typedef struct rtw_outputs {
                                reference's state holds this value: the emitters
                                are grey) */
     int32_t on_device;      /* 1: device pointers; 0: host pointers */
-    int32_t reserved;
+    int32_t trace_capacity; /* records that fit in trace */
+    double* trace;          /* [trace_capacity][RTW_TRACE_FIELDS] step attempts
+                               of params->trace_ray: step, the step size of the
+                               next attempt, accepted,
+                               promoted, escaped, err^2 (unnormalised), then
+                               the state t, r, theta, phi, k^t, k^r, k^theta,
+                               k^phi, tau after the attempt; unused records
+                               are NaN */
 } rtw_outputs;
 
 typedef struct rtw_stats {

@@ -18,6 +18,7 @@ LIB_PATH = Path(os.environ.get("RTW_LIB_PATH", PKG / "librtw_b200.so"))
 ABI_VERSION = 1
 MAX_BINS = 128
 MAX_FRAMES = 4096
+TRACE_FIELDS = 15
 
 # rtw_status
 OK = 0
@@ -87,6 +88,7 @@ class RenderParams(C.Structure):
         ("promote_dr", C.c_double), ("promote_sin", C.c_double),
         ("block_warps", C.c_int32), ("ctas_per_sm", C.c_int32),
         ("stream", C.c_void_p), ("pixel_order", C.c_int32), ("reserved", C.c_int32),
+        ("trace_ray", C.c_int64),
     ]
 
 
@@ -94,7 +96,7 @@ class Outputs(C.Structure):
     _fields_ = [
         ("xyz", C.c_void_p), ("term_class", C.c_void_p), ("steps", C.c_void_p),
         ("spectrum", C.c_void_p), ("final_state", C.c_void_p), ("tau", C.c_void_p),
-        ("on_device", C.c_int32), ("reserved", C.c_int32),
+        ("on_device", C.c_int32), ("trace_capacity", C.c_int32), ("trace", C.c_void_p),
     ]
 
 

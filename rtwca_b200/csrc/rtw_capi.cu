@@ -507,7 +507,9 @@ rtw_status rtw_render(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* ca
     float* spectrum = out->spectrum;
     double* fstate = out->final_state;
     float* tau = out->tau;
-    size_t off_xyz = 0, off_cls = 0, off_steps = 0, off_spec = 0, off_state = 0, off_tau = 0;
+    double* trace = out->trace;
+    const bool tracing = prm->trace_ray >= 0 && out->trace && out->trace_capacity > 0;
+    size_t off_xyz = 0, off_cls = 0, off_steps = 0, off_spec = 0, off_state = 0, off_tau = 0, off_trace = 0;
     if (!out->on_device) {
         size_t o = 0;
         auto take = [&](bool want, size_t bytes, size_t& off) {
@@ -522,6 +524,7 @@ rtw_status rtw_render(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* ca
         take(spectrum != nullptr, sizeof(float) * N * total, off_spec);
         take(fstate != nullptr, sizeof(double) * 8 * total, off_state);
         take(tau != nullptr, sizeof(float) * total, off_tau);
+        take(tracing, sizeof(double) * RTW_TRACE_FIELDS * (size_t)out->trace_capacity, off_trace);
         if ((s = ensure(ctx, &ctx->d_out, &ctx->out_cap, std::max<size_t>(o, 256))) != RTW_OK) return s;
         char* base = (char*)ctx->d_out;
         xyz = xyz ? (float*)(base + off_xyz) : nullptr;
@@ -530,6 +533,7 @@ rtw_status rtw_render(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* ca
         spectrum = spectrum ? (float*)(base + off_spec) : nullptr;
         fstate = fstate ? (double*)(base + off_state) : nullptr;
         tau = tau ? (float*)(base + off_tau) : nullptr;
+        trace = tracing ? (double*)(base + off_trace) : nullptr;
     }
 
     KParams p;
@@ -559,11 +563,16 @@ rtw_status rtw_render(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* ca
     p.counter = ctx->d_ctl;
     p.stats = (DevStats*)(ctx->d_ctl + 1);
     p.xyz = xyz; p.cls = cls; p.steps = steps; p.spectrum = spectrum; p.final_state = fstate; p.tau = tau;
+    p.trace = tracing ? trace : nullptr;
+    p.trace_gid = tracing ? prm->trace_ray : -1;
+    p.trace_cap = tracing ? out->trace_capacity : 0;
 
     RTW_CUDA(cudaEventRecord(ctx->ev[0], st), "event");
     RTW_CUDA(cudaMemcpyAsync(ctx->d_frames, frames.data(), sizeof(FrameDesc) * n_cams, cudaMemcpyHostToDevice, st), "frames H2D");
     RTW_CUDA(cudaMemcpyAsync(ctx->d_bins, bins.data(), sizeof(double) * 4 * RTW_MAX_BINS, cudaMemcpyHostToDevice, st), "bins H2D");
     RTW_CUDA(cudaMemsetAsync(ctx->d_ctl, 0, sizeof(unsigned long long) + sizeof(DevStats), st), "reset counters");
+    if (p.trace)  // all-ones bytes: NaN records mark the unused tail
+        RTW_CUDA(cudaMemsetAsync(p.trace, 0xff, sizeof(double) * RTW_TRACE_FIELDS * (size_t)p.trace_cap, st), "trace");
     RTW_CUDA(cudaEventRecord(ctx->ev[1], st), "event");
     RTW_CUDA(launch_trace(p, prm->precision, grid, block, st), "trace kernel launch");
     RTW_CUDA(cudaEventRecord(ctx->ev[2], st), "event");
@@ -574,6 +583,9 @@ rtw_status rtw_render(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* ca
         if (out->spectrum) RTW_CUDA(cudaMemcpyAsync(out->spectrum, spectrum, sizeof(float) * N * total, cudaMemcpyDeviceToHost, st), "spectrum D2H");
         if (out->final_state) RTW_CUDA(cudaMemcpyAsync(out->final_state, fstate, sizeof(double) * 8 * total, cudaMemcpyDeviceToHost, st), "state D2H");
         if (out->tau) RTW_CUDA(cudaMemcpyAsync(out->tau, tau, sizeof(float) * total, cudaMemcpyDeviceToHost, st), "tau D2H");
+        if (tracing)
+            RTW_CUDA(cudaMemcpyAsync(out->trace, trace, sizeof(double) * RTW_TRACE_FIELDS * (size_t)out->trace_capacity,
+                                     cudaMemcpyDeviceToHost, st), "trace D2H");
     }
     RTW_CUDA(cudaEventRecord(ctx->ev[3], st), "event");
     ctx->have_last = true;

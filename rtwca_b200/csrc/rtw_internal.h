@@ -77,6 +77,10 @@ struct KParams {
     float* spectrum;
     double* final_state;
     float* tau;
+    // step trace of one ray (RTW_TRACE_FIELDS doubles per attempt)
+    double* trace;
+    long long trace_gid;
+    int trace_cap;
 };
 
 // Scene constants of the device functors from the public scene struct.

@@ -42,8 +42,8 @@ struct Emit {
     R A, X, ktau;
 };
 
-// FP32 stages use the MUFU forms (absolute error ~5e-7 on [0, pi]; the FP64
-// oracle comparison bounds the effect), FP64 stages the accurate ones.
+// FP32 stages use the MUFU forms (absolute error ~5e-7 on [0, pi]); within
+// sin(theta) < promote_sin of a pole the mixed path runs FP64 stages.
 // (Host versions exist only for the operation-count instantiation.)
 RTW_HD void rsincos(float x, float* s, float* c) {
 #ifdef __CUDA_ARCH__

@@ -435,7 +435,7 @@ __global__ void __launch_bounds__(128, MIXED ? RTW_MIXED_MIN_CTAS : 2) trace_ker
     typedef typename SceneOf<KIND>::type SC;
     typedef SpecTraits<MIXED> ST;
     typedef typename ST::SR SR;
-    typedef typename ST::SR K;  // carried slope type
+    typedef typename ST::SR K;  // carried slope and 5th-order increment
     typedef typename ST::SR R;  // stage arithmetic (promoted to double per ray)
     typedef typename ST::SR CT; // step-controller arithmetic
 
@@ -546,7 +546,7 @@ __global__ void __launch_bounds__(128, MIXED ? RTW_MIXED_MIN_CTAS : 2) trace_ker
         K nk1[9];  // slope carried to the next attempt
         CT err2 = 0;
         double max_dt = 0, hnext = h;
-        bool emit = false, esc_done = false, decided = false, accept = false;
+        bool emit = false, esc_done = false, decided = false, accept = false, traced_promote = false;
         if (active) {
             ++c_att;
             max_dt = pad_max_dt<KIND, CT>(s, x, p.max_dt_scale);
@@ -584,6 +584,7 @@ __global__ void __launch_bounds__(128, MIXED ? RTW_MIXED_MIN_CTAS : 2) trace_ker
                     promote = (x[1] - s.r_ev < p.promote_dr) || (x[2] < p.promote_theta) ||
                               (x[2] > kPi - p.promote_theta);
                 }
+                traced_promote = promote;
                 if (promote) {
                     ++c_pro;
                     double xe[9];
@@ -718,6 +719,17 @@ __global__ void __launch_bounds__(128, MIXED ? RTW_MIXED_MIN_CTAS : 2) trace_ker
                 prev_rej = false;
             }
             ++nsteps;
+            if (gid == p.trace_gid && nsteps <= p.trace_cap) {
+                double* tr = p.trace + (nsteps - 1) * RTW_TRACE_FIELDS;
+                tr[0] = (double)nsteps;
+                tr[1] = h;
+                tr[2] = accept ? 1.0 : 0.0;
+                tr[3] = traced_promote ? 1.0 : 0.0;
+                tr[4] = esc_done ? 1.0 : 0.0;
+                tr[5] = (double)err2;
+#pragma unroll
+                for (int i = 0; i < 9; ++i) tr[6 + i] = x[i];
+            }
             if (nsteps >= max_steps) cls = RTW_CLASS_MAXSTEPS;
             else cls = terminate_geo<KIND>(s, x, r_term, thick);
             if (cls) {

@@ -62,7 +62,7 @@ class Renderer:
     @staticmethod
     def params(colors_nm, precision=abi.PREC_FP64, integrator=abi.DP45_REF_COMPAT, max_dt_scale=0.1,
                block_warps=0, ctas_per_sm=0, promote_dr=0.0, promote_sin=0.0, stream=None,
-               pixel_order=0, ray_bundles=False):
+               pixel_order=0, ray_bundles=False, trace_ray=-1):
         colors = np.ascontiguousarray(np.asarray(colors_nm, dtype=np.float64))
         p = abi.RenderParams()
         p.n_colors = int(colors.size)
@@ -77,6 +77,7 @@ class Renderer:
         p.ctas_per_sm = int(ctas_per_sm)
         p.stream = stream
         p.pixel_order = int(pixel_order)
+        p.trace_ray = int(trace_ray)
         p._keep = colors  # keep the array alive with the struct
         return p
 
@@ -116,6 +117,12 @@ class Renderer:
         if "tau" in want:
             res["tau"] = np.zeros(total, np.float32)
             out.tau = res["tau"].ctypes.data
+        if kw.get("trace_ray", -1) >= 0:
+            cap = int(kw.pop("trace_capacity", 20000))
+            res["trace"] = np.zeros((cap, abi.TRACE_FIELDS))
+            out.trace = res["trace"].ctypes.data
+            out.trace_capacity = cap
+        kw.pop("trace_capacity", None)
         out.on_device = 0
         self.render_raw(scene, cams, self.params(colors_nm, **kw), out)
         return res
