@@ -275,6 +275,28 @@ rtw_status rtw_measure_peaks(rtw_ctx* ctx, double* fp32_flops, double* fp64_flop
  * -A / (exp(X nu_c) - 1). */
 rtw_status rtw_scene_rhs(const rtw_scene* scene, int32_t fp32, const double* state, double* slope, double* emit);
 
+/* Limits of rtw_render_noalloc. */
+#define RTW_NOALLOC_MAX_FRAMES 64
+#define RTW_NOALLOC_SCRATCH_BYTES (24u << 20)
+
+/* Renders like rtw_render but allocates nothing, for callers that cannot call
+ * cudaMalloc (a host that owns all device memory up front, a real-time loop
+ * that must not enter the allocator) or that hold no rtw_ctx. No counterpart
+ * in the reference. Scratch, frame table, bin table and work counter are
+ * file-scope __device__ arrays of the library (24 MiB of scratch; every GPU
+ * that loads the library holds them until exit). Outputs must be device
+ * pointers; at most RTW_NOALLOC_MAX_FRAMES cameras; the scratch caps the
+ * resident warps, so it runs slower than rtw_render. Larger requests return
+ * RTW_ERR_INVALID_PARAM (text in rtw_noalloc_last_error). Runs on the current
+ * device and on params->stream (NULL: default stream, returns when done).
+ * Calls share the arrays: calls that overlap on the GPU race; serialise them.
+ * The first call on a device looks up the arrays' addresses
+ * (cudaGetSymbolAddress); make it before any stream capture. */
+rtw_status rtw_render_noalloc(const rtw_scene* scene, const rtw_camera* cams, int32_t n_cams,
+                              const rtw_render_params* params, rtw_outputs* out);
+/* Text of the calling thread's last rtw_render_noalloc error ("" if none). */
+const char* rtw_noalloc_last_error(void);
+
 /* Operation counts used for the roofline of a render (see rtw_op_counts above). */
 rtw_status rtw_get_op_counts(int32_t kind, rtw_op_counts* out);
 

@@ -19,6 +19,8 @@ ABI_VERSION = 1
 MAX_BINS = 128
 MAX_FRAMES = 4096
 TRACE_FIELDS = 15
+NOALLOC_MAX_FRAMES = 64
+NOALLOC_SCRATCH_BYTES = 24 << 20
 
 # rtw_status
 OK = 0
@@ -131,6 +133,9 @@ SIGNATURES = {
     "rtw_get_stats": (C.c_int, [_P, C.POINTER(Stats)]),
     "rtw_measure_peaks": (C.c_int, [_P] + [C.POINTER(C.c_double)] * 3),
     "rtw_get_op_counts": (C.c_int, [C.c_int32, C.POINTER(OpCounts)]),
+    "rtw_render_noalloc": (C.c_int, [C.POINTER(Scene), C.POINTER(Camera), C.c_int32, C.POINTER(RenderParams),
+                                     C.POINTER(Outputs)]),
+    "rtw_noalloc_last_error": (C.c_char_p, []),
     "rtw_scene_rhs": (C.c_int, [C.POINTER(Scene), C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                 C.POINTER(C.c_double)]),
 }

@@ -19,7 +19,7 @@ CSRC = PKG / "csrc"
 BUILD = PKG / "_build"
 LIB = PKG / "librtw_b200.so"
 
-SOURCES = ["rtw_capi.cu", "rtw_probe.cu", "rtw_opcount.cu", "rtw_kind0.cu", "rtw_kind1.cu", "rtw_kind2.cu", "rtw_kind3.cu"]
+SOURCES = ["rtw_capi.cu", "rtw_probe.cu", "rtw_opcount.cu", "rtw_noalloc.cu", "rtw_kind0.cu", "rtw_kind1.cu", "rtw_kind2.cu", "rtw_kind3.cu"]
 HEADERS = ["rtw_internal.h", "rtw_scenes.cuh", "rtw_trace.cuh", "rtw_launch.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + [

@@ -386,6 +386,23 @@ static rtw_status build_frame(const rtw_scene& s, rtw_camera& cam, FrameDesc& f)
     return RTW_OK;
 }
 
+// Frame descriptors of a batch (used by the allocation-free entry point).
+rtw_status rtw_prepare_frames(const rtw_scene* scene, const rtw_camera* cams, int32_t n_cams, void* frames_out,
+                              int64_t* total_out) {
+    if (!scene || !cams || !frames_out || n_cams <= 0) return RTW_ERR_INVALID_PARAM;
+    FrameDesc* frames = static_cast<FrameDesc*>(frames_out);
+    long long total = 0;
+    for (int f = 0; f < n_cams; ++f) {
+        rtw_camera cam = cams[f];
+        const rtw_status s = build_frame(*scene, cam, frames[f]);
+        if (s != RTW_OK) return s;
+        frames[f].ray_begin = total;
+        total += (long long)frames[f].xp * frames[f].yp;
+    }
+    *total_out = total;
+    return RTW_OK;
+}
+
 rtw_status rtw_camera_rays(const rtw_scene* scene, const rtw_camera* camin, double* rays, int64_t n_pix) {
     if (!scene || !camin || !rays) return RTW_ERR_INVALID_PARAM;
     rtw_camera cam = *camin;
