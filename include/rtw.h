@@ -197,6 +197,9 @@ typedef struct rtw_stats {
     uint64_t nan_rays;          /* rays of class RTW_CLASS_NAN */
     double kernel_ms;           /* device time of the trace kernel */
     double total_ms;            /* device time of the whole render call */
+    uint64_t phase_cycles[4];   /* builds with RTW_PHASE_CLOCKS only (else 0): SM
+                                   cycles summed over warps in refill, geodesic,
+                                   spectral, commit/epilogue */
 } rtw_stats;
 
 /* Algorithmic operation counts of the trace kernel's arithmetic for one scene

@@ -107,7 +107,7 @@ class Stats(C.Structure):
         ("rays", C.c_uint64), ("step_attempts", C.c_uint64), ("rejected_steps", C.c_uint64),
         ("promoted_steps", C.c_uint64), ("spectral_steps", C.c_uint64), ("emitting_steps", C.c_uint64),
         ("escape_substeps", C.c_uint64), ("nan_rays", C.c_uint64),
-        ("kernel_ms", C.c_double), ("total_ms", C.c_double),
+        ("kernel_ms", C.c_double), ("total_ms", C.c_double), ("phase_cycles", C.c_uint64 * 4),
     ]
 
 

@@ -587,7 +587,7 @@ rtw_status rtw_render(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* ca
     RTW_CUDA(cudaEventRecord(ctx->ev[0], st), "event");
     RTW_CUDA(cudaMemcpyAsync(ctx->d_frames, frames.data(), sizeof(FrameDesc) * n_cams, cudaMemcpyHostToDevice, st), "frames H2D");
     RTW_CUDA(cudaMemcpyAsync(ctx->d_bins, bins.data(), sizeof(double) * 4 * RTW_MAX_BINS, cudaMemcpyHostToDevice, st), "bins H2D");
-    RTW_CUDA(cudaMemsetAsync(ctx->d_ctl, 0, sizeof(unsigned long long) + sizeof(DevStats), st), "reset counters");
+    RTW_CUDA(cudaMemsetAsync(ctx->d_ctl, 0, sizeof(unsigned long long) + sizeof(DevStats), st), "reset counters");  // 104 B of 256
     if (p.trace)  // all-ones bytes: NaN records mark the unused tail
         RTW_CUDA(cudaMemsetAsync(p.trace, 0xff, sizeof(double) * RTW_TRACE_FIELDS * (size_t)p.trace_cap, st), "trace");
     RTW_CUDA(cudaEventRecord(ctx->ev[1], st), "event");
@@ -634,6 +634,10 @@ rtw_status rtw_get_stats(rtw_ctx* ctx, rtw_stats* out) {
     out->nan_rays = ds.nan_rays;
     out->kernel_ms = k;
     out->total_ms = t;
+    out->phase_cycles[0] = ds.cyc_refill;
+    out->phase_cycles[1] = ds.cyc_geo;
+    out->phase_cycles[2] = ds.cyc_spec;
+    out->phase_cycles[3] = ds.cyc_commit;
     return RTW_OK;
 }
 

@@ -46,6 +46,8 @@ struct DevStats {
     unsigned long long escape_substeps;
     unsigned long long nan_rays;
     unsigned long long rays;
+    // RTW_PHASE_CLOCKS builds only: SM cycles per phase, summed over warps
+    unsigned long long cyc_refill, cyc_geo, cyc_spec, cyc_commit;
 };
 
 struct KParams {

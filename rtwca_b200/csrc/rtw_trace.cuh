@@ -476,6 +476,19 @@ __global__ void __launch_bounds__(128, MIXED ? RTW_MIXED_MIN_CTAS : 2) trace_ker
     // local counters
     unsigned c_att = 0, c_rej = 0, c_pro = 0, c_spec = 0, c_emit = 0, c_esc = 0, c_nan = 0, c_rays = 0;
 
+#ifdef RTW_PHASE_CLOCKS
+    // profiling build: cycles each warp spends per phase (lane 0 records)
+    unsigned long long cy_ref = 0, cy_geo = 0, cy_spec = 0, cy_com = 0;
+    long long t_mark = clock64();
+#define RTW_PHASE(acc)                       \
+    do {                                     \
+        const long long t_now = clock64();   \
+        acc += (unsigned long long)(t_now - t_mark); \
+        t_mark = t_now;                      \
+    } while (0)
+#else
+#define RTW_PHASE(acc) do {} while (0)
+#endif
     for (;;) {
         // ---------------- refill -----------------------------------------
         const unsigned empty = __ballot_sync(kFull, !active);
@@ -540,6 +553,8 @@ __global__ void __launch_bounds__(128, MIXED ? RTW_MIXED_MIN_CTAS : 2) trace_ker
         }
         const unsigned act = __ballot_sync(kFull, active);
         if (!act) break;
+        __syncwarp();
+        RTW_PHASE(cy_ref);
 
         // ---------------- geodesic phase ---------------------------------
         K ns[9];   // 5th-order slope: the new state is x + h ns
@@ -611,6 +626,7 @@ __global__ void __launch_bounds__(128, MIXED ? RTW_MIXED_MIN_CTAS : 2) trace_ker
             }
         }
         __syncwarp();
+        RTW_PHASE(cy_geo);
 
         // ---------------- spectral phase (warp-cooperative) --------------
         const bool need = active && !esc_done && (emit || spec_live);
@@ -692,6 +708,7 @@ __global__ void __launch_bounds__(128, MIXED ? RTW_MIXED_MIN_CTAS : 2) trace_ker
             if (lane == r && dec) spec_live = nz;
         }
         __syncwarp();
+        RTW_PHASE(cy_spec);
 
         // ---------------- controller + commit ----------------------------
         int cls = 0;
@@ -782,7 +799,17 @@ __global__ void __launch_bounds__(128, MIXED ? RTW_MIXED_MIN_CTAS : 2) trace_ker
             if (p.tau) p.tau[gid] = (float)x[8];
             active = false;
         }
+        __syncwarp();
+        RTW_PHASE(cy_com);
     }
+#ifdef RTW_PHASE_CLOCKS
+    if (lane == 0) {
+        atomicAdd(&p.stats->cyc_refill, cy_ref);
+        atomicAdd(&p.stats->cyc_geo, cy_geo);
+        atomicAdd(&p.stats->cyc_spec, cy_spec);
+        atomicAdd(&p.stats->cyc_commit, cy_com);
+    }
+#endif
 
     // counters
     atomicAdd(&p.stats->step_attempts, (unsigned long long)c_att);

@@ -130,7 +130,9 @@ class Renderer:
     def stats(self) -> dict:
         s = abi.Stats()
         abi.check(self._lib.rtw_get_stats(self._ctx, C.byref(s)), self.last_error())
-        return {f: getattr(s, f) for f, _ in abi.Stats._fields_}
+        d = {f: getattr(s, f) for f, _ in abi.Stats._fields_}
+        d["phase_cycles"] = list(s.phase_cycles)
+        return d
 
     def op_counts(self, kind: int) -> dict:
         return abi.op_counts(kind)
