@@ -43,6 +43,7 @@ def parse():
     ap.add_argument("--no-fp64-leg", action="store_true", help="skip the FP64 comparison leg")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample", type=int, default=2048, help="rays in the CPU baseline sample")
+    ap.add_argument("--no-batched", action="store_true", help="skip the 96-frame batched leg")
     ap.add_argument("--block-warps", type=int, default=0)
     ap.add_argument("--ctas-per-sm", type=int, default=0)
     return ap.parse_args()
@@ -201,6 +202,100 @@ def op_model(renderer, scene_kind, stats, n_bins):
     return flops, mufu, oc
 
 
+def batched_leg(r, world, rank, stream, barrier_fn):
+    """96 Kerr frames (r ~ U[5, 40] M, inclination ~ U[10, 85] deg, numpy
+    default_rng(0); 32 frames each at 256^2, 512^2, 1024^2; tolerance 1e-6 /
+    1e-8 alternating) in ONE persistent, graph-captured, autotuned FP32-mixed
+    launch per GPU (frames sharded over ranks by estimated cost). Per-frame
+    latency from the kernel's global-timer stamps. Against it, FP64 with one
+    frame per launch, on the 24 frames k % 8 in {0, 1} (every size and both
+    tolerances), also run batched-mixed for a like-for-like ratio."""
+    import torch
+    from rtwca_b200 import abi, configs, shard
+
+    scene, cams, colors, meta = configs.batched_frames(96, seed=0)
+    mine = shard.frames_of_rank(cams, world, rank)
+    dev = torch.device("cuda", torch.cuda.current_device())
+
+    def outputs(cs):
+        P = sum(c.x_pix * abi.y_pixels(c.x_pix, c.fov_hor, c.fov_vert) for c in cs)
+        xyz = torch.empty((P, 3), dtype=torch.float32, device=dev)
+        cl = torch.empty(P, dtype=torch.uint8, device=dev)
+        o = abi.Outputs()
+        o.xyz, o.term_class, o.on_device = xyz.data_ptr(), cl.data_ptr(), 1
+        return P, o, (xyz, cl)
+
+    def run(cs, precision, graph, autotune):
+        prm = r.params(colors, precision=precision, stream=stream.cuda_stream, graph=graph, autotune=autotune)
+        P, o, keep = outputs(cs)
+        # warm-up on the same frame list shrunk to 16 px wide (allocations, tuning)
+        small = [abi.make_camera(list(c.position), list(c.direction), c.speed, list(c.pointing), 16, c.fov_hor,
+                                 c.fov_vert, c.tolerance, c.max_steps) for c in cs]
+        r.render_raw(scene, small, prm, outputs(small)[1])
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r.render_raw(scene, cs, prm, o)
+        e1.record(stream)
+        e1.synchronize()
+        return P, e0.elapsed_time(e1), r.stats()
+
+    barrier_fn()
+    cs = [cams[i] for i in mine]
+    P, ms, st = run(cs, abi.PREC_MIXED, True, True)
+    ft = r.frame_times(len(cs))
+    # like-for-like subset: batched mixed vs one frame per launch in FP64
+    sub = [k for k in mine if k % 8 in (0, 1)]
+    sc = [cams[i] for i in sub]
+    Ps, ms_sub, _ = run(sc, abi.PREC_MIXED, True, True) if sc else (0, 0.0, None)
+    ms64, lat64 = 0.0, []
+    prm64 = r.params(colors, precision=abi.PREC_FP64, stream=stream.cuda_stream)
+    if sc:  # warm-up of the FP64 kernel
+        r.render_raw(scene, [sc[0]], prm64, outputs([sc[0]])[1])
+    for c in sc:
+        Pc, o, keep = outputs([c])
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r.render_raw(scene, [c], prm64, o)
+        e1.record(stream)
+        e1.synchronize()
+        t = e0.elapsed_time(e1)
+        ms64 += t
+        lat64.append(ms64)
+    barrier_fn()
+    ms_all = all_max(ms, world)
+    rays_all = sum(cams[i].x_pix * abi.y_pixels(cams[i].x_pix, cams[i].fov_hor, cams[i].fov_vert) for i in range(96))
+    if world > 1:
+        import torch.distributed as dist
+        gathered = [None] * world
+        dist.all_gather_object(gathered, (list(ft["done"]), ms_sub, Ps, ms64, lat64))
+    else:
+        gathered = [(list(ft["done"]), ms_sub, Ps, ms64, lat64)]
+    done = np.concatenate([np.asarray(g[0]) for g in gathered])
+    sub_ms = max(g[1] for g in gathered)
+    sub_rays = sum(g[2] for g in gathered)
+    f64_ms = max(g[3] for g in gathered)
+    f64_lat = np.concatenate([np.asarray(g[4]) for g in gathered]) if sub_rays else np.zeros(1)
+    return {
+        "workload": "kerr_thin_disk, 96 frames (32 x 256^2, 32 x 512^2, 32 x 1024^2), r ~ U[5,40] M, "
+                    "inclination ~ U[10,85] deg, numpy default_rng(0), tol 1e-6/1e-8 alternating",
+        "rays": rays_all, "ms": ms_all, "value": rays_all / (ms_all * 1e-3) / 1e6, "unit": "Mrays/s",
+        "launches_per_gpu": 1, "graph_replayed": st["graph_replayed"],
+        "autotuned": {"block_warps": st["block_warps"], "refill_min": st["refill_min"]},
+        "frame_done_ms": {"p50": float(np.quantile(done, 0.5)), "p99": float(np.quantile(done, 0.99))},
+        "subset_24_frames": {
+            "rays": sub_rays,
+            "batched_mixed": {"ms": sub_ms, "value": sub_rays / (sub_ms * 1e-3) / 1e6},
+            "one_frame_per_launch_fp64": {"ms": f64_ms, "value": sub_rays / (f64_ms * 1e-3) / 1e6,
+                                          "frame_done_ms": {"p50": float(np.quantile(f64_lat, 0.5)),
+                                                            "p99": float(np.quantile(f64_lat, 0.99))}},
+        },
+    }
+
+
 def run_b200(args):
     import torch
     from rtwca_b200 import Renderer, abi, configs
@@ -275,6 +370,10 @@ def run_b200(args):
         fsal = {"value": world * P * max(1, args.steps // 2) / (tf * 1e-3) / 1e6,
                 "ms_per_step": tf / max(1, args.steps // 2)}
 
+    batched = None
+    if not args.no_batched:
+        batched = batched_leg(r, world, rank, stream, lambda: barrier(world))
+
     # end to end through the public API: host pinned outputs, synchronous call
     hx = torch.empty((P, 3), dtype=torch.float32, pin_memory=True)
     hc = torch.empty(P, dtype=torch.uint8, pin_memory=True)
@@ -330,6 +429,7 @@ def run_b200(args):
                        "l2": "flushed (256 MB write) between timed renders"},
             "fp64": fp64,
             "fsal": fsal,
+            "batched": batched,
             "integrator": "reference step (k1 = previous sum b_i k_i)",
             "roofline": {"bound": "fp32" if prec == abi.PREC_MIXED else "fp64", "achieved": achieved, "peak": peak,
                          "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,

@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define RTW_ABI_VERSION 1
+#define RTW_ABI_VERSION 2
 /* Largest number of spectral bins (reference `colors`) one render takes. */
 #define RTW_MAX_BINS 128
 /* Largest number of frames (cameras) one batched render takes. */
@@ -155,9 +155,20 @@ typedef struct rtw_render_params {
                                    stream, and rtw_render returns when done */
     int32_t pixel_order;        /* 0: row order; 1: 8x4 tiles (internal order,
                                    outputs are always row order) */
-    int32_t reserved;
+    int32_t refill_min;         /* compaction interval: a warp takes new rays once
+                                   at least this many of its 32 lanes are free
+                                   (or all are); 0: default 1 */
     int64_t trace_ray;          /* global pixel index whose step attempts are
                                    recorded in rtw_outputs.trace; -1: none */
+    int32_t autotune;           /* 1: block_warps and refill_min (where 0) come
+                                   from a per-context autotuner that times the
+                                   candidates once per scene kind, precision,
+                                   bin count and integrator, on the first
+                                   camera at up to 768 pixels wide */
+    int32_t graph;              /* 1: the launch sequence (frame table upload,
+                                   counter reset, kernel) is captured once in a
+                                   CUDA graph and replayed while the launch
+                                   parameters match; cameras may change */
 } rtw_render_params;
 
 /* Output buffers, owned by the caller. Pixel p of frame f is at
@@ -200,6 +211,10 @@ typedef struct rtw_stats {
     uint64_t phase_cycles[4];   /* builds with RTW_PHASE_CLOCKS only (else 0): SM
                                    cycles summed over warps in refill, geodesic,
                                    spectral, commit/epilogue */
+    int32_t grid;               /* launch shape used: CTAs */
+    int32_t block_warps;        /*   warps per CTA */
+    int32_t refill_min;         /*   compaction interval */
+    int32_t graph_replayed;     /* 1: the render replayed a captured graph */
 } rtw_stats;
 
 /* Algorithmic operation counts of the trace kernel's arithmetic for one scene
@@ -261,6 +276,14 @@ rtw_status rtw_render(rtw_ctx* ctx, const rtw_scene* scene,
 /* Counters and device times of the last rtw_render on this context
  * (synchronises the context's stream). */
 rtw_status rtw_get_stats(rtw_ctx* ctx, rtw_stats* out);
+
+/* Per-frame timing of the last rtw_render on this context, from the device's
+ * global nanosecond timer: done_ms[f] = time from the start of the batch's
+ * first ray to the end of frame f's last ray; span_ms[f] = from frame f's
+ * first ray start to its last ray end (either may be NULL). n_frames must be
+ * the n_cams of that render. No counterpart in the reference (one frame per
+ * gen_image call). */
+rtw_status rtw_get_frame_times(rtw_ctx* ctx, int32_t n_frames, double* done_ms, double* span_ms);
 
 /* Measured issue peaks of this GPU from short in-library microbenchmarks:
  * FP32 FMA, FP64 FMA (flop/s, an FMA counted as 2) and MUFU ex2 (op/s). */

@@ -15,7 +15,7 @@ PKG = Path(__file__).resolve().parent
 # RTW_LIB_PATH selects another build of the same library (e.g. a tuning variant)
 LIB_PATH = Path(os.environ.get("RTW_LIB_PATH", PKG / "librtw_b200.so"))
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 MAX_BINS = 128
 MAX_FRAMES = 4096
 TRACE_FIELDS = 15
@@ -89,8 +89,8 @@ class RenderParams(C.Structure):
         ("max_dt_scale", C.c_double), ("integrator", C.c_int32), ("ray_bundles", C.c_int32),
         ("promote_dr", C.c_double), ("promote_sin", C.c_double),
         ("block_warps", C.c_int32), ("ctas_per_sm", C.c_int32),
-        ("stream", C.c_void_p), ("pixel_order", C.c_int32), ("reserved", C.c_int32),
-        ("trace_ray", C.c_int64),
+        ("stream", C.c_void_p), ("pixel_order", C.c_int32), ("refill_min", C.c_int32),
+        ("trace_ray", C.c_int64), ("autotune", C.c_int32), ("graph", C.c_int32),
     ]
 
 
@@ -108,6 +108,7 @@ class Stats(C.Structure):
         ("promoted_steps", C.c_uint64), ("spectral_steps", C.c_uint64), ("emitting_steps", C.c_uint64),
         ("escape_substeps", C.c_uint64), ("nan_rays", C.c_uint64),
         ("kernel_ms", C.c_double), ("total_ms", C.c_double), ("phase_cycles", C.c_uint64 * 4),
+        ("grid", C.c_int32), ("block_warps", C.c_int32), ("refill_min", C.c_int32), ("graph_replayed", C.c_int32),
     ]
 
 
@@ -131,6 +132,7 @@ SIGNATURES = {
     "rtw_render": (C.c_int, [_P, C.POINTER(Scene), C.POINTER(Camera), C.c_int32,
                              C.POINTER(RenderParams), C.POINTER(Outputs)]),
     "rtw_get_stats": (C.c_int, [_P, C.POINTER(Stats)]),
+    "rtw_get_frame_times": (C.c_int, [_P, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "rtw_measure_peaks": (C.c_int, [_P] + [C.POINTER(C.c_double)] * 3),
     "rtw_get_op_counts": (C.c_int, [C.c_int32, C.POINTER(OpCounts)]),
     "rtw_render_noalloc": (C.c_int, [C.POINTER(Scene), C.POINTER(Camera), C.c_int32, C.POINTER(RenderParams),

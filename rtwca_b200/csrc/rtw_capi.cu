@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -217,6 +218,18 @@ struct rtw_ctx {
     void* d_out = nullptr;
     size_t out_cap = 0;
     float* d_sink = nullptr;
+    unsigned long long* d_fclock = nullptr;  // per-frame timing, 3 words per frame
+    size_t fclock_cap = 0;
+    int last_frames = 0;
+    // autotuner results: (kind, precision, np, integrator) -> (warps, refill_min)
+    std::vector<std::pair<std::array<int, 4>, std::array<int, 2>>> tuned;
+    // captured launch sequence and the pinned staging it reads the frame and
+    // bin tables from
+    cudaGraphExec_t gexec = nullptr;
+    std::vector<unsigned char> gkey;
+    void* h_stage = nullptr;
+    size_t stage_cap = 0;
+    int last_grid = 0, last_warps = 0, last_refill = 0, last_replayed = 0;
     std::string err;
     rtw_stats last{};
     bool have_last = false;
@@ -295,6 +308,9 @@ void rtw_destroy(rtw_ctx* ctx) {
     cudaFree(ctx->d_spec);
     cudaFree(ctx->d_out);
     cudaFree(ctx->d_sink);
+    cudaFree(ctx->d_fclock);
+    if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
+    if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
     for (auto& e : ctx->ev)
         if (e) cudaEventDestroy(e);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -453,6 +469,58 @@ rtw_status rtw_cie_weights(const double* colors, int32_t n, double* wx, double* 
     return RTW_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// Autotuner: times every candidate (warps per CTA x compaction interval) on
+// the first camera at up to 768 pixels wide (about ten rays per resident
+// lane) and keeps the fastest per (kind, precision, bins, integrator).
+rtw_status autotune(rtw_ctx* ctx, const rtw_scene& scene, const rtw_camera& cam0, const rtw_render_params& prm,
+                    int np, std::array<int, 2>& choice) {
+    const std::array<int, 4> key = {scene.kind, prm.precision, np, prm.integrator};
+    for (const auto& kv : ctx->tuned)
+        if (kv.first == key) {
+            choice = kv.second;
+            return RTW_OK;
+        }
+    rtw_camera cam = cam0;
+    cam.x_pix = std::min(cam.x_pix, 768);
+    rtw_render_params q = prm;
+    q.autotune = 0;
+    q.graph = 0;
+    q.stream = nullptr;
+    q.trace_ray = -1;
+    rtw_outputs none;
+    std::memset(&none, 0, sizeof(none));
+    none.on_device = 1;
+    const int warp_c[2] = {4, 2};
+    const int refill_c[3] = {1, 4, 8};
+    float best = 0;
+    choice = {4, 1};
+    for (int pass = 0; pass < 2; ++pass)  // pass 0 warms up the default shape
+        for (int w : warp_c)
+            for (int r : refill_c) {
+                if (pass == 0 && (w != 4 || r != 1)) continue;
+                q.block_warps = w;
+                q.refill_min = r;
+                const rtw_status st = rtw_render(ctx, &scene, &cam, 1, &q, &none);
+                if (st != RTW_OK) return st;
+                float ms = 0;
+                cudaEventElapsedTime(&ms, ctx->ev[1], ctx->ev[2]);
+                if (pass == 1 && (best == 0 || ms < best)) {
+                    best = ms;
+                    choice = {w, r};
+                }
+            }
+    ctx->tuned.push_back({key, choice});
+    return RTW_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 rtw_status rtw_render(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* cams, int32_t n_cams,
                       const rtw_render_params* prm, rtw_outputs* out) {
     if (!ctx) return RTW_ERR_INVALID_PARAM;
@@ -500,8 +568,19 @@ rtw_status rtw_render(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* ca
     }
     const int np = N <= 32 ? 32 : (N <= 64 ? 64 : 128);
 
-    // launch shape
-    const int warps = prm->block_warps > 0 ? std::min(prm->block_warps, 4) : 4;  // kernel launch bound: 128 threads
+    // launch shape: explicit values, else the autotuner's choice, else defaults
+    int warps = prm->block_warps > 0 ? std::min(prm->block_warps, 4) : 0;  // kernel launch bound: 128 threads
+    int refill = prm->refill_min > 0 ? std::min(prm->refill_min, 32) : 0;
+    if (prm->autotune && (warps == 0 || refill == 0)) {
+        std::array<int, 2> choice;
+        const rtw_status ts = autotune(ctx, *scene, cams[0], *prm, np, choice);
+        if (ts != RTW_OK) return ts;
+        ctx->err.clear();
+        if (warps == 0) warps = choice[0];
+        if (refill == 0) refill = choice[1];
+    }
+    if (warps == 0) warps = 4;
+    if (refill == 0) refill = 1;
     const int block = 32 * warps;
     int per_sm = prm->ctas_per_sm;
     if (per_sm <= 0) {
@@ -516,6 +595,8 @@ rtw_status rtw_render(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* ca
     rtw_status s;
     if ((s = ensure(ctx, &ctx->d_frames, &ctx->frames_cap, sizeof(FrameDesc) * n_cams)) != RTW_OK) return s;
     if ((s = ensure(ctx, &ctx->d_spec, &ctx->spec_cap, spec_need)) != RTW_OK) return s;
+    if ((s = ensure(ctx, (void**)&ctx->d_fclock, &ctx->fclock_cap, sizeof(unsigned long long) * 3 * n_cams)) != RTW_OK)
+        return s;
 
     // outputs
     float* xyz = out->xyz;
@@ -583,16 +664,84 @@ rtw_status rtw_render(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* ca
     p.trace = tracing ? trace : nullptr;
     p.trace_gid = tracing ? prm->trace_ray : -1;
     p.trace_cap = tracing ? out->trace_capacity : 0;
+    p.refill_min = refill;
+    p.frame_clock = ctx->d_fclock;
 
-    RTW_CUDA(cudaEventRecord(ctx->ev[0], st), "event");
-    RTW_CUDA(cudaMemcpyAsync(ctx->d_frames, frames.data(), sizeof(FrameDesc) * n_cams, cudaMemcpyHostToDevice, st), "frames H2D");
-    RTW_CUDA(cudaMemcpyAsync(ctx->d_bins, bins.data(), sizeof(double) * 4 * RTW_MAX_BINS, cudaMemcpyHostToDevice, st), "bins H2D");
-    RTW_CUDA(cudaMemsetAsync(ctx->d_ctl, 0, sizeof(unsigned long long) + sizeof(DevStats), st), "reset counters");  // 104 B of 256
-    if (p.trace)  // all-ones bytes: NaN records mark the unused tail
-        RTW_CUDA(cudaMemsetAsync(p.trace, 0xff, sizeof(double) * RTW_TRACE_FIELDS * (size_t)p.trace_cap, st), "trace");
-    RTW_CUDA(cudaEventRecord(ctx->ev[1], st), "event");
-    RTW_CUDA(launch_trace(p, prm->precision, grid, block, st), "trace kernel launch");
-    RTW_CUDA(cudaEventRecord(ctx->ev[2], st), "event");
+    const size_t frames_bytes = sizeof(FrameDesc) * n_cams;
+    const size_t bins_bytes = sizeof(double) * 4 * RTW_MAX_BINS;
+    // the launch sequence up to the kernel: frame and bin tables, counter
+    // resets, kernel, with events around the kernel
+    // (under stream capture the events are recorded as external event nodes,
+    // so that every replay records them)
+    auto enqueue = [&](const void* src_frames, const void* src_bins, bool capturing) -> cudaError_t {
+        auto record = [&](cudaEvent_t ev) {
+            return capturing ? cudaEventRecordWithFlags(ev, st, cudaEventRecordExternal) : cudaEventRecord(ev, st);
+        };
+        cudaError_t e;
+        if ((e = record(ctx->ev[0])) != cudaSuccess) return e;
+        if ((e = cudaMemcpyAsync(ctx->d_frames, src_frames, frames_bytes, cudaMemcpyHostToDevice, st)) != cudaSuccess) return e;
+        if ((e = cudaMemcpyAsync(ctx->d_bins, src_bins, bins_bytes, cudaMemcpyHostToDevice, st)) != cudaSuccess) return e;
+        // counters: 1 + 12 words of the 256-byte control block
+        if ((e = cudaMemsetAsync(ctx->d_ctl, 0, sizeof(unsigned long long) + sizeof(DevStats), st)) != cudaSuccess) return e;
+        if ((e = cudaMemsetAsync(ctx->d_fclock, 0, sizeof(unsigned long long) * 3 * n_cams, st)) != cudaSuccess) return e;
+        if (p.trace)  // all-ones bytes: NaN records mark the unused tail
+            if ((e = cudaMemsetAsync(p.trace, 0xff, sizeof(double) * RTW_TRACE_FIELDS * (size_t)p.trace_cap, st)) != cudaSuccess)
+                return e;
+        if ((e = record(ctx->ev[1])) != cudaSuccess) return e;
+        if ((e = launch_trace(p, prm->precision, grid, block, st)) != cudaSuccess) return e;
+        return record(ctx->ev[2]);
+    };
+    int replayed = 0;
+    if (prm->graph) {
+        // pinned staging for the tables (a captured copy reads its source
+        // address at every replay); wait until the previous render has read it
+        if (ctx->have_last) RTW_CUDA(cudaEventSynchronize(ctx->ev[1]), "previous render");
+        if (ctx->stage_cap < frames_bytes + bins_bytes) {
+            if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
+            ctx->gexec = nullptr;
+            if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
+            ctx->h_stage = nullptr;
+            ctx->stage_cap = 0;
+            RTW_CUDA(cudaHostAlloc(&ctx->h_stage, frames_bytes + bins_bytes, cudaHostAllocDefault), "pinned staging");
+            ctx->stage_cap = frames_bytes + bins_bytes;
+        }
+        char* stage = (char*)ctx->h_stage;
+        std::memcpy(stage, frames.data(), frames_bytes);
+        std::memcpy(stage + frames_bytes, bins.data(), bins_bytes);
+        // replay while everything the capture baked in is unchanged
+        std::vector<unsigned char> key(sizeof(KParams) + 4 * sizeof(int) + sizeof(void*));
+        unsigned char* k = key.data();
+        std::memcpy(k, &p, sizeof(KParams));
+        const int shape[4] = {grid, block, prm->precision, n_cams};
+        std::memcpy(k + sizeof(KParams), shape, sizeof(shape));
+        std::memcpy(k + sizeof(KParams) + sizeof(shape), &st, sizeof(void*));
+        if (ctx->gexec && key == ctx->gkey) {
+            replayed = 1;
+        } else {
+            if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
+            ctx->gexec = nullptr;
+            ctx->gkey.clear();
+            RTW_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "graph capture");
+            const cudaError_t eq = enqueue(stage, stage + frames_bytes, true);
+            cudaGraph_t g = nullptr;
+            const cudaError_t ec = cudaStreamEndCapture(st, &g);
+            if (eq != cudaSuccess) {
+                if (g) cudaGraphDestroy(g);
+                return cuda_fail(ctx, eq, "graph capture of the launch");
+            }
+            if (ec != cudaSuccess) return cuda_fail(ctx, ec, "graph capture end");
+            const cudaError_t ei = cudaGraphInstantiate(&ctx->gexec, g, 0);
+            cudaGraphDestroy(g);
+            if (ei != cudaSuccess) {
+                ctx->gexec = nullptr;
+                return cuda_fail(ctx, ei, "graph instantiate");
+            }
+            ctx->gkey = key;
+        }
+        RTW_CUDA(cudaGraphLaunch(ctx->gexec, st), "graph launch");
+    } else {
+        RTW_CUDA(enqueue(frames.data(), bins.data(), false), "trace launch sequence");
+    }
     if (!out->on_device) {
         if (out->xyz) RTW_CUDA(cudaMemcpyAsync(out->xyz, xyz, sizeof(float) * 3 * total, cudaMemcpyDeviceToHost, st), "xyz D2H");
         if (out->term_class) RTW_CUDA(cudaMemcpyAsync(out->term_class, cls, total, cudaMemcpyDeviceToHost, st), "class D2H");
@@ -608,6 +757,11 @@ rtw_status rtw_render(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* ca
     ctx->have_last = true;
     std::memset(&ctx->last, 0, sizeof(ctx->last));
     ctx->last.rays = (uint64_t)total;
+    ctx->last_frames = n_cams;
+    ctx->last_grid = grid;
+    ctx->last_warps = warps;
+    ctx->last_refill = refill;
+    ctx->last_replayed = replayed;
     if (!prm->stream) {
         RTW_CUDA(cudaStreamSynchronize(st), "trace kernel");
     }
@@ -638,6 +792,32 @@ rtw_status rtw_get_stats(rtw_ctx* ctx, rtw_stats* out) {
     out->phase_cycles[1] = ds.cyc_geo;
     out->phase_cycles[2] = ds.cyc_spec;
     out->phase_cycles[3] = ds.cyc_commit;
+    out->grid = ctx->last_grid;
+    out->block_warps = ctx->last_warps;
+    out->refill_min = ctx->last_refill;
+    out->graph_replayed = ctx->last_replayed;
+    return RTW_OK;
+}
+
+rtw_status rtw_get_frame_times(rtw_ctx* ctx, int32_t n_frames, double* done_ms, double* span_ms) {
+    if (!ctx) return RTW_ERR_INVALID_PARAM;
+    if (!ctx->have_last || ctx->last_frames <= 0) return fail(ctx, RTW_ERR_INVALID_PARAM, "no render yet");
+    if (n_frames != ctx->last_frames) return fail(ctx, RTW_ERR_INVALID_PARAM, "n_frames differs from the last render");
+    RTW_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    RTW_CUDA(cudaEventSynchronize(ctx->ev[3]), "sync");
+    std::vector<unsigned long long> h((size_t)3 * n_frames);
+    RTW_CUDA(cudaMemcpy(h.data(), ctx->d_fclock, sizeof(unsigned long long) * h.size(), cudaMemcpyDeviceToHost),
+             "frame clock D2H");
+    const unsigned long long* start = h.data() + n_frames;
+    const unsigned long long* end = h.data() + 2 * (size_t)n_frames;
+    unsigned long long t0 = ~0ull;
+    for (int f = 0; f < n_frames; ++f)
+        if (start[f]) t0 = std::min(t0, start[f]);
+    for (int f = 0; f < n_frames; ++f) {
+        const bool ok = start[f] != 0 && end[f] != 0;
+        if (done_ms) done_ms[f] = ok ? (double)(end[f] - t0) * 1e-6 : NAN;
+        if (span_ms) span_ms[f] = ok ? (double)(end[f] - start[f]) * 1e-6 : NAN;
+    }
     return RTW_OK;
 }
 

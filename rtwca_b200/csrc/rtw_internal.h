@@ -83,6 +83,13 @@ struct KParams {
     double* trace;
     long long trace_gid;
     int trace_cap;
+    // a warp refills its empty lanes once at least refill_min are empty (or
+    // all are), so that fresh rays start together
+    int refill_min;
+    // per-frame timing (may be null): [n_frames] finished-ray counters, then
+    // [n_frames] global-timer ns when the frame's first ray started, then
+    // [n_frames] when its last ray finished
+    unsigned long long* frame_clock;
 };
 
 // Scene constants of the device functors from the public scene struct.

@@ -371,6 +371,13 @@ __device__ __forceinline__ double warp_sum(double v) {
     return __shfl_sync(kFull, v, 0);
 }
 
+// Device-wide nanosecond clock (PTX %globaltimer).
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
 // Polar / origin escape (integrators_LttM.jl:62-105): 37 explicit Euler steps
 // of size temp through the coordinate singularity, FP64; the spectral slots of
 // this ray (its row of the warp's scratch) are updated by this lane.
@@ -487,6 +494,7 @@ __global__ void __launch_bounds__(128, MIXED ? RTW_MIXED_MIN_CTAS : 2) trace_ker
     // lane ray state
     bool active = false, dry = false;
     long long gid = 0;  // global output index
+    int fi = 0;         // frame of the lane's ray
     double x[9];
     K k1[9];
     double h = 0, tol = 0, r_term = 0, thick = 0;
@@ -515,7 +523,7 @@ __global__ void __launch_bounds__(128, MIXED ? RTW_MIXED_MIN_CTAS : 2) trace_ker
         bool fresh = false;
         Emit<double> em0;
         em0.A = 0; em0.X = 0; em0.ktau = 0;
-        if (empty && !dry) {
+        if (empty && !dry && (__popc(empty) >= p.refill_min || empty == kFull)) {
             unsigned long long base = 0;
             const unsigned n = __popc(empty);
             if (lane == 0) base = atomicAdd(p.counter, (unsigned long long)n);
@@ -530,6 +538,8 @@ __global__ void __launch_bounds__(128, MIXED ? RTW_MIXED_MIN_CTAS : 2) trace_ker
                         if (p.frames[mid].ray_begin <= id) lo = mid; else hi = mid - 1;
                     }
                     const FrameDesc& f = p.frames[lo];
+                    fi = lo;
+                    if (p.frame_clock && id == f.ray_begin) p.frame_clock[p.n_frames + lo] = global_ns();
                     int pi, pj;
                     pixel_of(p.pixel_order, id - f.ray_begin, f.xp, f.yp, pi, pj);
                     gid = f.ray_begin + pi + (long long)f.xp * pj;
@@ -847,6 +857,11 @@ __global__ void __launch_bounds__(128, MIXED ? RTW_MIXED_MIN_CTAS : 2) trace_ker
                 for (int i = 0; i < 8; ++i) p.final_state[8 * gid + i] = x[i];
             }
             if (p.tau) p.tau[gid] = (float)x[8];
+            if (p.frame_clock) {
+                const unsigned long long done = atomicAdd(&p.frame_clock[fi], 1ull) + 1ull;
+                if (done == (unsigned long long)p.frames[fi].xp * (unsigned long long)p.frames[fi].yp)
+                    p.frame_clock[2 * p.n_frames + fi] = global_ns();
+            }
             active = false;
         }
         __syncwarp();

@@ -62,7 +62,7 @@ class Renderer:
     @staticmethod
     def params(colors_nm, precision=abi.PREC_FP64, integrator=abi.DP45_REF_COMPAT, max_dt_scale=0.1,
                block_warps=0, ctas_per_sm=0, promote_dr=0.0, promote_sin=0.0, stream=None,
-               pixel_order=0, ray_bundles=False, trace_ray=-1):
+               pixel_order=0, ray_bundles=False, trace_ray=-1, refill_min=0, autotune=False, graph=False):
         colors = np.ascontiguousarray(np.asarray(colors_nm, dtype=np.float64))
         p = abi.RenderParams()
         p.n_colors = int(colors.size)
@@ -78,6 +78,9 @@ class Renderer:
         p.stream = stream
         p.pixel_order = int(pixel_order)
         p.trace_ray = int(trace_ray)
+        p.refill_min = int(refill_min)
+        p.autotune = int(bool(autotune))
+        p.graph = int(bool(graph))
         p._keep = colors  # keep the array alive with the struct
         return p
 
@@ -133,6 +136,17 @@ class Renderer:
         d = {f: getattr(s, f) for f, _ in abi.Stats._fields_}
         d["phase_cycles"] = list(s.phase_cycles)
         return d
+
+    def frame_times(self, n_frames: int) -> dict:
+        """Per-frame times of the last render (ms, device global timer):
+        'done' = batch start to the frame's last ray, 'span' = the frame's
+        first ray start to its last ray end."""
+        done = np.zeros(n_frames)
+        span = np.zeros(n_frames)
+        dp = done.ctypes.data_as(C.POINTER(C.c_double))
+        sp = span.ctypes.data_as(C.POINTER(C.c_double))
+        abi.check(self._lib.rtw_get_frame_times(self._ctx, int(n_frames), dp, sp), self.last_error())
+        return {"done": done, "span": span}
 
     def op_counts(self, kind: int) -> dict:
         return abi.op_counts(kind)
