@@ -44,6 +44,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample", type=int, default=2048, help="rays in the CPU baseline sample")
     ap.add_argument("--no-batched", action="store_true", help="skip the 96-frame batched leg")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the synchrotron-torus adjoint leg")
+    ap.add_argument("--adjoint-x-pix", type=int, default=512)
     ap.add_argument("--block-warps", type=int, default=0)
     ap.add_argument("--ctas-per-sm", type=int, default=0)
     return ap.parse_args()
@@ -296,6 +298,42 @@ def batched_leg(r, world, rank, stream, barrier_fn):
     }
 
 
+def adjoint_leg(r, x_pix):
+    """Differentiable synchrotron torus: Kerr a = 0.94, inclination 17 deg,
+    x_pix^2 rays, 32 bins over 230 GHz +- 20 %, FP32-mixed, tolerance 1e-6.
+    Loss = sum (I - target)^2 against the image at parameters perturbed by
+    5 % normal deviates from numpy default_rng(1). One rtw_adjoint call =
+    forward render + record pass + reverse sweep (checkpoints every 16
+    accepted steps). Rays that take a polar escape are left out of the
+    gradient (counted in escape_rays). Times are device times of the call."""
+    from rtwca_b200 import abi, configs
+
+    tp = configs.torus_target_params(1)
+    scT, camT, col = configs.torus_problem(x_pix=x_pix, tol=1e-6, params=tp)
+    target = r.render(scT, [camT], col, want=("spectrum",), precision=abi.PREC_MIXED,
+                      integrator=abi.DP45_FSAL)["spectrum"]
+    sc, cam, col = configs.torus_problem(x_pix=x_pix, tol=1e-6)
+    # forward alone, for the ratio (warm-up first)
+    r.render(sc, [cam], col, want=("spectrum",), precision=abi.PREC_MIXED, integrator=abi.DP45_FSAL)
+    r.render(sc, [cam], col, want=("spectrum",), precision=abi.PREC_MIXED, integrator=abi.DP45_FSAL)
+    fwd = r.stats()
+    a = r.adjoint(sc, cam, col, target, precision=abi.PREC_MIXED, exclude_escape_rays=True)
+    P = cam.x_pix * cam.y_pix
+    return {
+        "workload": f"synchrotron torus {cam.x_pix}x{cam.y_pix}, 32 bins 230 GHz +-20%, a=0.94, i=17 deg, tol 1e-6, "
+                    "FP32-mixed, FSAL",
+        "metric": "adjoint grad/s", "value": 1000.0 / a["total_ms"], "unit": "gradients/s",
+        "adjoint_ms": a["total_ms"], "forward_render_ms": fwd["kernel_ms"],
+        "adjoint_over_forward": a["total_ms"] / fwd["kernel_ms"],
+        "parts_ms": {"forward": a["forward_ms"], "record": a["record_ms"], "reverse": a["reverse_ms"]},
+        "forward_Mrays_s": P / fwd["kernel_ms"] / 1e3, "step_attempts": fwd["step_attempts"],
+        "loss": a["loss"], "grad": dict(zip(abi.ADJOINT_PARAMS, [float(v) for v in a["grad"]])),
+        "events": a["events"], "checkpoints": a["checkpoints"], "scratch_GB": a["scratch_bytes"] / 1e9,
+        "escape_rays": a["escape_rays"], "escape_rays_policy": "left out of the gradient",
+        "target_params": tp,
+    }
+
+
 def run_b200(args):
     import torch
     from rtwca_b200 import Renderer, abi, configs
@@ -373,6 +411,9 @@ def run_b200(args):
     batched = None
     if not args.no_batched:
         batched = batched_leg(r, world, rank, stream, lambda: barrier(world))
+    adjoint = None
+    if not args.no_adjoint and rank == 0:
+        adjoint = adjoint_leg(r, args.adjoint_x_pix)
 
     # end to end through the public API: host pinned outputs, synchronous call
     hx = torch.empty((P, 3), dtype=torch.float32, pin_memory=True)
@@ -430,6 +471,7 @@ def run_b200(args):
             "fp64": fp64,
             "fsal": fsal,
             "batched": batched,
+            "adjoint": adjoint,
             "integrator": "reference step (k1 = previous sum b_i k_i)",
             "roofline": {"bound": "fp32" if prec == abi.PREC_MIXED else "fp64", "achieved": achieved, "peak": peak,
                          "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,

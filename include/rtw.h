@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define RTW_ABI_VERSION 2
+#define RTW_ABI_VERSION 3
 /* Largest number of spectral bins (reference `colors`) one render takes. */
 #define RTW_MAX_BINS 128
 /* Largest number of frames (cameras) one batched render takes. */
@@ -67,7 +67,20 @@ typedef enum rtw_scene_kind {
     /* Kerr with a thickened, optically thin disk: rho = (r/r0)^-2
        exp(-z^2 / 2 (h r)^2), alpha = a_nu * rho, j = alpha B_nu(T),
        T = temperature (r/r0)^t_index, for r_in <= r <= r_out. */
-    RTW_SCENE_KERR_THICK_DISK = 3
+    RTW_SCENE_KERR_THICK_DISK = 3,
+    /* Kerr with an optically thin-to-thick thermal synchrotron torus (no
+       reference counterpart; a new .source emitter behind the same RT slot
+       contract, integrators_LttM.jl:33-42). With x = r / r_in and
+       z = r cos(theta):
+         n_e   = n_e0 x^rho_index exp(-z^2 / 2 (rho_h r)^2)
+         B     = b_0 x^b_index          (toroidal, fluid frame)
+         Theta = theta_e0 x^t_index     (kT_e / m_e c^2)
+       tapered by exp(-((r_in - r)/edge_in)^2) inside r_in and by
+       exp(-((r - r_out)/edge_out)^2) outside r_out (zero beyond 4 widths);
+       Keplerian 4-velocity; thermal synchrotron j_nu from the Leung, Gammie
+       & Noble (2011) fit, alpha_nu = j_nu / B_nu(T_e). Per-bin tau. Only
+       the FSAL integrator. */
+    RTW_SCENE_KERR_SYNCHRO_TORUS = 4
 } rtw_scene_kind;
 
 /* How a ray ended. The reference's calc_terminate (e.g. Kerr.source/
@@ -119,6 +132,16 @@ typedef struct rtw_scene {
     double rho_h;           /* thick disk: scale height / r (0.1) */
     double rho_index;       /* thick disk: density power law (-2) */
     double t_index;         /* thick disk: temperature power law (-0.75) */
+    /* synchrotron torus (RTW_SCENE_KERR_SYNCHRO_TORUS); r_in is the torus
+       inner radius, r_out the start of the outer taper, rho_h the Gaussian
+       scale height / r, rho_index / t_index the n_e / Theta_e power laws */
+    double n_e0;            /* electron density at r_in, cm^-3 */
+    double b_0;             /* magnetic field at r_in, gauss */
+    double theta_e0;        /* dimensionless electron temperature at r_in */
+    double b_index;         /* field power law */
+    double edge_in;         /* inner taper width, M */
+    double edge_out;        /* outer taper width, M */
+    double length_cm;       /* GM/c^2 in cm (the map unit) */
 } rtw_scene;
 
 /* One camera (= one frame of a batch). Mirrors the camera keywords of
@@ -284,6 +307,83 @@ rtw_status rtw_get_stats(rtw_ctx* ctx, rtw_stats* out);
  * the n_cams of that render. No counterpart in the reference (one frame per
  * gen_image call). */
 rtw_status rtw_get_frame_times(rtw_ctx* ctx, int32_t n_frames, double* done_ms, double* span_ms);
+
+/* ---- differentiable synchrotron torus: discrete adjoint -------------------
+ * The loss is L = sum over pixels p and bins c of (I_pc - target_pc)^2 with
+ * I the final invariant intensity (the spectrum output). Parameters, in this
+ * order: spin a, camera inclination (position[2], rad), n_e0, b_0, theta_e0.
+ * The gradient is that of the discrete FSAL Dormand-Prince map along each
+ * ray's accepted steps (step sizes held fixed, as in any discrete adjoint of an
+ * adaptive integrator), reversed from states checkpointed every
+ * checkpoint_every accepted steps and recomputed in FP64 in between. The
+ * camera initial data enter through their derivative in a and the
+ * inclination (a central difference of the FP64 camera transform, which is
+ * linear in the transform matrix). No counterpart in the reference (it has
+ * no derivatives); it backs a ChainRulesCore rrule of gen_image. */
+#define RTW_ADJOINT_PARAMS 5
+
+typedef struct rtw_adjoint_params {
+    const float* target;        /* [P][n_colors] target spectrum */
+    int32_t target_on_device;   /* 1: target is a device pointer */
+    int32_t checkpoint_every;   /* accepted steps between stored states (0: 16) */
+    double camera_delta;        /* central-difference step of the camera
+                                   transform in a and inclination (0: 1e-6) */
+    double* per_ray_grad;       /* NULL, or host [P][5]: each ray's share of grad */
+    int32_t escape_rays;        /* rays that take a polar escape (pass within about
+                                   1e-8 rad of the axis): 0 differentiate through the
+                                   escape (spike guard, escape_cuts); 1 leave them out
+                                   of the gradient (their loss still counts). Their
+                                   discrete loss is not smooth at finite-difference
+                                   scales, and the FP32-stage path reaches the axis
+                                   differently from the FP64 one. */
+    int32_t reserved;
+} rtw_adjoint_params;
+
+typedef struct rtw_adjoint_result {
+    double loss;
+    double grad[RTW_ADJOINT_PARAMS];  /* dL/d(a, inclination, n_e0, b_0, theta_e0) */
+    double forward_ms;          /* forward render (image, step counts) */
+    double record_ms;           /* forward re-run that stores step sizes and checkpoints */
+    double reverse_ms;          /* reverse sweep */
+    double total_ms;            /* the whole call, device time */
+    uint64_t events;            /* recorded steps: accepted DP45 steps + polar escapes */
+    uint64_t checkpoints;       /* stored states */
+    uint64_t scratch_bytes;     /* device memory of the records and the sweep */
+    uint64_t escape_rays;       /* rays with at least one polar escape */
+    uint64_t escape_cuts;       /* polar escapes whose local derivative was a spike
+                                   (cotangent growth > 1e3) and that were carried as
+                                   the identity instead */
+} rtw_adjoint_result;
+
+/* Forward render of one camera of a RTW_SCENE_KERR_SYNCHRO_TORUS scene, the
+ * loss against params->target and its gradient. out (may be NULL) receives
+ * the forward outputs (spectrum, class, steps) like rtw_render. */
+rtw_status rtw_adjoint(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* cam,
+                       const rtw_render_params* params, const rtw_adjoint_params* adj,
+                       rtw_outputs* out, rtw_adjoint_result* result);
+
+/* Host FP64 evaluation of the torus right-hand side in the reference's state
+ * layout (state[8 + 2N] = x^mu, k^mu, then (I_c, tau_c) per bin), with the
+ * forward kernel's functions (form 0) or the adjoint's generic ones (form 1:
+ * geodesic acceleration from metric derivatives). For tests. */
+rtw_status rtw_torus_rhs(const rtw_scene* scene, const double* colors_nm, int32_t n_colors, int32_t form,
+                         const double* state, double* slope);
+
+/* Host FP64 vector-Jacobian product of the torus right-hand side, the
+ * adjoint kernel's own function: mu = J^T cot (reference layout) and
+ * pbar[5] = (d slope / d(a, -, n_e0, b_0, theta_e0))^T cot (pbar[1] = 0). */
+rtw_status rtw_torus_vjp(const rtw_scene* scene, const double* colors_nm, int32_t n_colors,
+                         const double* state, const double* cot, double* mu, double* pbar);
+
+/* Host FP64 polar escape of the torus (n_sub sub-steps z <- keep(z - temp
+ * f(z)), temp from the state; Kerr source_geometry.jl:249-269 with
+ * integrators_LttM.jl:62-105) and the adjoint kernel's vector-Jacobian product
+ * of it: end_state, mu = J^T cot, pbar as rtw_torus_vjp. Returns RTW_ERR_NAN
+ * when the adjoint's spike guard replaced the escape's derivative by the
+ * identity. For tests. */
+rtw_status rtw_torus_escape_vjp(const rtw_scene* scene, const double* colors_nm, int32_t n_colors,
+                                const double* state, int32_t n_sub, const double* cot, double* end_state,
+                                double* mu, double* pbar);
 
 /* Measured issue peaks of this GPU from short in-library microbenchmarks:
  * FP32 FMA, FP64 FMA (flop/s, an FMA counted as 2) and MUFU ex2 (op/s). */

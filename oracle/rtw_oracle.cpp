@@ -41,6 +41,15 @@
 //    (Kerr.source/source_geometry.jl:196-197).
 //  * The termination class is the first predicate of calc_terminate that holds,
 //    in the reference's order; RTW_CLASS_NAN marks a non-finite final state.
+//
+// The synchrotron torus (RTW_SCENE_KERR_SYNCHRO_TORUS) has no reference
+// counterpart: it is a new emitter behind the same RT slot contract, restated
+// here independently of the library (K_2 from std::cyl_bessel_k, powers from
+// std::pow, the normalised Keplerian velocity and the toroidal-field angle
+// written out in plain FP64), so that the library's generic-scalar emitter
+// is checked against a second implementation. Its formulas: thermal
+// synchrotron emissivity of Leung, Gammie & Noble 2011 (ApJ 737, 21) with
+// alpha = j / B_nu(T_e).
 
 #include "../include/rtw.h"
 
@@ -102,6 +111,7 @@ struct OScene {
     double M = 1, a = 0, rs = 2, r_ev = 2, r_in = 6, r_out = 12, th_lo = 0, th_hi = kPi;
     double T = 5778, anu = 1, esc = 100, wind = 8 * kPi;
     double rho_r0 = 6, rho_h = 0.1, rho_idx = -2, t_idx = -0.75;
+    double n0 = 0, b0 = 0, th0 = 0, b_idx = 0, edge_in = 1, edge_out = 1, length_cm = 1;
 
     explicit OScene(const rtw_scene& s) {
         kind = s.kind;
@@ -111,6 +121,8 @@ struct OScene {
         r_in = s.r_in; r_out = s.r_out; th_lo = s.theta_lo; th_hi = s.theta_hi;
         T = s.temperature; anu = s.a_nu; esc = s.escape_radius; wind = s.winding_limit;
         rho_r0 = s.rho_r0; rho_h = s.rho_h; rho_idx = s.rho_index; t_idx = s.t_index;
+        n0 = s.n_e0; b0 = s.b_0; th0 = s.theta_e0; b_idx = s.b_index;
+        edge_in = s.edge_in; edge_out = s.edge_out; length_cm = s.length_cm;
         if (kind == RTW_SCENE_SCHWARZSCHILD_DISK) a = 0;
         if (refprec) {
             // the reference's Float32 literals (Kerr source_geometry.jl:7,13,
@@ -120,7 +132,7 @@ struct OScene {
             T = (double)(float)T;
         }
         rs = 2 * M;
-        if (kind == RTW_SCENE_KERR_DISK || kind == RTW_SCENE_KERR_THICK_DISK) {
+        if (is_kerr()) {
             // Kerr source_geometry.jl:17
             if (refprec) {
                 float rsf = (float)rs, af = (float)a;
@@ -133,7 +145,9 @@ struct OScene {
         }
     }
 
-    bool is_kerr() const { return kind == RTW_SCENE_KERR_DISK || kind == RTW_SCENE_KERR_THICK_DISK; }
+    bool is_kerr() const {
+        return kind == RTW_SCENE_KERR_DISK || kind == RTW_SCENE_KERR_THICK_DISK || kind == RTW_SCENE_KERR_SYNCHRO_TORUS;
+    }
 
     // --- geometry -----------------------------------------------------------
     // Kerr calc_metric_params, source_geometry.jl:55-60
@@ -465,6 +479,58 @@ struct RayWork {
     }
 };
 
+// RT slopes of the synchrotron torus (no reference counterpart; the formulas
+// are listed in the file header). slope[8 + 2c] = dI_c, slope[9 + 2c] = dtau_c.
+void torus_bins(const OScene& sc, RayWork& w, const double* R, double* slope) {
+    for (int c = 0; c < w.N; ++c) {
+        slope[8 + 2 * c] = 0;
+        slope[9 + 2 * c] = 0;
+    }
+    const double r = R[1], th = R[2];
+    const double cut_in = std::max(sc.r_in - 4 * sc.edge_in, 1.01 * sc.r_ev);
+    const double cut_out = sc.r_out + 4 * sc.edge_out;
+    if (!(r >= cut_in && r <= cut_out)) return;
+    double taper = 1;
+    if (r < sc.r_in) taper = std::exp(-sq((sc.r_in - r) / sc.edge_in));
+    else if (r > sc.r_out) taper = std::exp(-sq((r - sc.r_out) / sc.edge_out));
+    const double x = r / sc.r_in;
+    const double z = r * std::cos(th), hz = sc.rho_h * r;
+    const double ne = sc.n0 * std::pow(x, sc.rho_idx) * std::exp(-z * z / (2 * hz * hz)) * taper;
+    const double B = sc.b0 * std::pow(x, sc.b_idx);
+    const double Th = sc.th0 * std::pow(x, sc.t_idx);
+    sc.lower_metric(R, w.g);
+    const double Om = std::sqrt(sc.M) / (std::pow(r, 1.5) + sc.a * std::sqrt(sc.M));
+    const double n2 = -(w.g[0][0] + 2 * Om * w.g[0][3] + Om * Om * w.g[3][3]);
+    if (!(n2 > 0)) return;
+    const double ut = 1 / std::sqrt(n2);
+    const double u_t = ut * (w.g[0][0] + Om * w.g[0][3]);
+    const double u_p = ut * (w.g[0][3] + Om * w.g[3][3]);
+    const double gs = -(u_t * R[4] + u_p * R[7]);
+    const double kph_low = w.g[0][3] * R[4] + w.g[3][3] * R[7];
+    const double bb = w.g[3][3] + u_p * u_p;
+    const double bk = kph_low - u_p * gs;
+    if (!(bb > 0) || !(gs > 0)) return;
+    const double c2 = bk * bk / (bb * gs * gs);
+    if (!(1 - c2 > 1e-12)) return;
+    const double sinb = std::sqrt(1 - c2);
+    constexpr double e = 4.80320425e-10, cc = 2.99792458e10, me = 9.1093837015e-28, h = 6.62607015e-27;
+    const double nus = 2.0 / 9.0 * (e * B / (2 * kPi * me * cc)) * Th * Th * sinb;
+    const double k2 = std::cyl_bessel_k(2.0, 1 / Th);
+    for (int c = 0; c < w.N; ++c) {
+        const double nu = gs * kLightC * 1e9 * w.freq[c];  // Hz in the fluid frame
+        const double X = nu / nus;
+        if (!(X > 0) || X > 2.0e5) continue;
+        const double j = ne * std::sqrt(2.0) * kPi * e * e * nus / (3 * cc * k2) *
+                         sq(std::sqrt(X) + std::pow(2.0, 11.0 / 12) * std::pow(X, 1.0 / 6)) *
+                         std::exp(-std::pow(X, 1.0 / 3));
+        const double bnu = 2 * h * nu * nu * nu / (cc * cc) / std::expm1(h * nu / (Th * me * cc * cc));
+        const double j_u = j * sc.length_cm, a_u = j / bnu * sc.length_cm;
+        const double nu_nm = gs * w.freq[c];
+        slope[8 + 2 * c] = -(1 / gs) * j_u * std::exp(-R[9 + 2 * c]) / (nu_nm * nu_nm * nu_nm);
+        slope[9 + 2 * c] = -(1 / gs) * a_u;
+    }
+}
+
 // calc_ray_derivative!, integrators_LttM.jl:9-48
 void rhs(const OScene& sc, RayWork& w, const double* R, double* slope) {
     for (int i = 0; i < 4; ++i) slope[i] = R[i + 4];
@@ -474,6 +540,10 @@ void rhs(const OScene& sc, RayWork& w, const double* R, double* slope) {
         for (int j = 0; j < 4; ++j)
             for (int k = 0; k < 4; ++k) acc -= w.G[i][j][k] * R[4 + j] * R[4 + k];
         slope[4 + i] = acc;
+    }
+    if (sc.kind == RTW_SCENE_KERR_SYNCHRO_TORUS) {
+        torus_bins(sc, w, R, slope);
+        return;
     }
     sc.lower_metric(R, w.g);
     sc.source_velocity(R, w.u);
@@ -562,11 +632,13 @@ double dp45_step(const OScene& sc, RayWork& w, double* R, double h, bool prev_re
     if (std::fabs(hn) > max_dt) hn = -max_dt;
     const double* newk1 = w.fsal ? k7 : ns;
     if (err == 0 || !std::isfinite(hn)) {
+        const double th_before = y[2];
         sc.keepinbounds(y);
         for (int i = 0; i < L; ++i) {
             k1[i] = newk1[i];
             R[i] = y[i];
         }
+        if (sc.kind == RTW_SCENE_KERR_SYNCHRO_TORUS && y[2] != th_before) rhs(sc, w, R, k1);
         *rejected = false;
         return h;
     } else if (err > 1) {
@@ -576,11 +648,17 @@ double dp45_step(const OScene& sc, RayWork& w, double* R, double h, bool prev_re
         return hn;
     }
     if (std::fabs(hn) > 5 * std::fabs(h)) hn = 5 * h;
+    const double th_before = y[2];
     sc.keepinbounds(y);
     for (int i = 0; i < L; ++i) {
         k1[i] = newk1[i];
         R[i] = y[i];
     }
+    // synchrotron torus only: a step reflected through the pole re-evaluates
+    // the carried slope at the new state, so that each step depends on its
+    // start state alone (the reference scenes keep the reference's carried
+    // slope)
+    if (sc.kind == RTW_SCENE_KERR_SYNCHRO_TORUS && y[2] != th_before) rhs(sc, w, R, k1);
     *rejected = false;
     return hn;
 }

@@ -15,7 +15,7 @@ PKG = Path(__file__).resolve().parent
 # RTW_LIB_PATH selects another build of the same library (e.g. a tuning variant)
 LIB_PATH = Path(os.environ.get("RTW_LIB_PATH", PKG / "librtw_b200.so"))
 
-ABI_VERSION = 2
+ABI_VERSION = 3
 MAX_BINS = 128
 MAX_FRAMES = 4096
 TRACE_FIELDS = 15
@@ -43,6 +43,8 @@ SCENE_MINKOWSKI_SPHERE = 0
 SCENE_SCHWARZSCHILD_DISK = 1
 SCENE_KERR_DISK = 2
 SCENE_KERR_THICK_DISK = 3
+SCENE_KERR_SYNCHRO_TORUS = 4
+ADJOINT_PARAMS = ("spin", "inclination", "n_e0", "b_0", "theta_e0")
 
 # rtw_term_class
 CLASS_NONE = 0
@@ -71,6 +73,8 @@ class Scene(C.Structure):
         ("escape_radius", C.c_double), ("winding_limit", C.c_double),
         ("rho_r0", C.c_double), ("rho_h", C.c_double),
         ("rho_index", C.c_double), ("t_index", C.c_double),
+        ("n_e0", C.c_double), ("b_0", C.c_double), ("theta_e0", C.c_double), ("b_index", C.c_double),
+        ("edge_in", C.c_double), ("edge_out", C.c_double), ("length_cm", C.c_double),
     ]
 
 
@@ -112,6 +116,22 @@ class Stats(C.Structure):
     ]
 
 
+class AdjointParams(C.Structure):
+    _fields_ = [
+        ("target", C.c_void_p), ("target_on_device", C.c_int32), ("checkpoint_every", C.c_int32),
+        ("camera_delta", C.c_double), ("per_ray_grad", C.c_void_p), ("escape_rays", C.c_int32),
+        ("reserved", C.c_int32),
+    ]
+
+
+class AdjointResult(C.Structure):
+    _fields_ = [
+        ("loss", C.c_double), ("grad", C.c_double * 5), ("forward_ms", C.c_double), ("record_ms", C.c_double),
+        ("reverse_ms", C.c_double), ("total_ms", C.c_double), ("events", C.c_uint64), ("checkpoints", C.c_uint64),
+        ("scratch_bytes", C.c_uint64), ("escape_rays", C.c_uint64), ("escape_cuts", C.c_uint64),
+    ]
+
+
 class OpCounts(C.Structure):
     _fields_ = [(n, C.c_double) for n in (
         "rhs_vacuum", "rhs_vacuum_mufu", "rhs_emit", "rhs_emit_mufu", "step_overhead", "step_overhead_mufu",
@@ -133,6 +153,15 @@ SIGNATURES = {
                              C.POINTER(RenderParams), C.POINTER(Outputs)]),
     "rtw_get_stats": (C.c_int, [_P, C.POINTER(Stats)]),
     "rtw_get_frame_times": (C.c_int, [_P, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "rtw_adjoint": (C.c_int, [_P, C.POINTER(Scene), C.POINTER(Camera), C.POINTER(RenderParams),
+                              C.POINTER(AdjointParams), C.POINTER(Outputs), C.POINTER(AdjointResult)]),
+    "rtw_torus_rhs": (C.c_int, [C.POINTER(Scene), C.POINTER(C.c_double), C.c_int32, C.c_int32,
+                                C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "rtw_torus_vjp": (C.c_int, [C.POINTER(Scene), C.POINTER(C.c_double), C.c_int32, C.POINTER(C.c_double),
+                                C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "rtw_torus_escape_vjp": (C.c_int, [C.POINTER(Scene), C.POINTER(C.c_double), C.c_int32, C.POINTER(C.c_double),
+                                       C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                       C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "rtw_measure_peaks": (C.c_int, [_P] + [C.POINTER(C.c_double)] * 3),
     "rtw_get_op_counts": (C.c_int, [C.c_int32, C.POINTER(OpCounts)]),
     "rtw_render_noalloc": (C.c_int, [C.POINTER(Scene), C.POINTER(Camera), C.c_int32, C.POINTER(RenderParams),
@@ -226,3 +255,47 @@ def y_pixels(x_pix: int, fov_hor: float, fov_vert: float) -> int:
     W = math.tan(math.pi * fov_hor / 180 / 2)
     H = math.tan(math.pi * fov_vert / 180 / 2)
     return int(round(x_pix * H / W))
+
+
+def torus_rhs(scene: Scene, colors_nm, state, form: int = 0):
+    """Host FP64 torus right-hand side (reference layout: x, k, then (I, tau) per bin)."""
+    import numpy as np
+    c = np.ascontiguousarray(colors_nm, dtype=np.float64)
+    st = np.ascontiguousarray(state, dtype=np.float64)
+    out = np.zeros_like(st)
+    dp = C.POINTER(C.c_double)
+    check(load().rtw_torus_rhs(C.byref(scene), c.ctypes.data_as(dp), int(c.size), int(form), st.ctypes.data_as(dp),
+                               out.ctypes.data_as(dp)), "torus_rhs")
+    return out
+
+
+def torus_vjp(scene: Scene, colors_nm, state, cot):
+    """Host FP64 vector-Jacobian product of the torus right-hand side: (J^T cot, d/d params)."""
+    import numpy as np
+    c = np.ascontiguousarray(colors_nm, dtype=np.float64)
+    st = np.ascontiguousarray(state, dtype=np.float64)
+    ct = np.ascontiguousarray(cot, dtype=np.float64)
+    mu = np.zeros_like(st)
+    pb = np.zeros(5)
+    dp = C.POINTER(C.c_double)
+    check(load().rtw_torus_vjp(C.byref(scene), c.ctypes.data_as(dp), int(c.size), st.ctypes.data_as(dp),
+                               ct.ctypes.data_as(dp), mu.ctypes.data_as(dp), pb.ctypes.data_as(dp)), "torus_vjp")
+    return mu, pb
+
+
+def torus_escape_vjp(scene: Scene, colors_nm, state, n_sub: int, cot):
+    """Host polar escape of the torus and its VJP: (end_state, J^T cot, d/d params, guard_ok)."""
+    import numpy as np
+    c = np.ascontiguousarray(colors_nm, dtype=np.float64)
+    st = np.ascontiguousarray(state, dtype=np.float64)
+    ct = np.ascontiguousarray(cot, dtype=np.float64)
+    end = np.zeros_like(st)
+    mu = np.zeros_like(st)
+    pb = np.zeros(5)
+    dp = C.POINTER(C.c_double)
+    r = load().rtw_torus_escape_vjp(C.byref(scene), c.ctypes.data_as(dp), int(c.size), st.ctypes.data_as(dp),
+                                    int(n_sub), ct.ctypes.data_as(dp), end.ctypes.data_as(dp),
+                                    mu.ctypes.data_as(dp), pb.ctypes.data_as(dp))
+    if r not in (OK, ERR_NAN):
+        check(r, "torus_escape_vjp")
+    return end, mu, pb, r == OK

@@ -145,3 +145,52 @@ def batched_frames(n_frames: int = 96, seed: int = 0, sizes=(256, 512, 1024), to
         cams.append(look_at_camera(float(rs[k]), math.radians(float(incs[k])), 45.0, xp, tol))
         meta.append({"r": float(rs[k]), "inclination_deg": float(incs[k]), "x_pix": xp, "tol": tol})
     return kerr_disk_scene(), cams, log_spaced_colors(64), meta
+
+
+# ---------------------------------------------------------------------------
+# Differentiable synchrotron torus (Kerr a = 0.94, inclination 17 deg, 512^2,
+# 32 bins over 230 GHz +- 20 %). BASELINE-level parameters; the camera
+# distance, field of view and torus extent are choices of this library.
+# ---------------------------------------------------------------------------
+TORUS_DEFAULTS = {"spin": 0.94, "inclination_deg": 17.0, "n_e0": 1e5, "b_0": 10.0, "theta_e0": 10.0}
+
+
+def torus_scene(spin: float = 0.94, n_e0: float = 1e5, b_0: float = 10.0, theta_e0: float = 10.0) -> abi.Scene:
+    """n_e = n_e0 (r/6)^-1.5 exp(-z^2 / 2 (0.3 r)^2), B = b_0 (r/6)^-1 G,
+    Theta_e = theta_e0 (r/6)^-1, tapered inside r = 6 M (width 0.5 M) and
+    beyond 40 M (width 5 M); M87* length scale 9.62e14 cm."""
+    s = abi.scene_default(abi.SCENE_KERR_SYNCHRO_TORUS)
+    s.spin, s.n_e0, s.b_0, s.theta_e0 = float(spin), float(n_e0), float(b_0), float(theta_e0)
+    return s
+
+
+def torus_colors(n: int = 32, f_center: float = 230e9, rel: float = 0.2) -> np.ndarray:
+    """n wavelengths (nm) of frequencies evenly spaced over f_center (1 +- rel),
+    ascending in wavelength."""
+    f = np.linspace(f_center * (1 + rel), f_center * (1 - rel), n)
+    return 299792458.0 * 1e9 / f
+
+
+def torus_camera(x_pix: int = 512, inclination_deg: float = 17.0, r: float = 100.0, fov: float = 28.0,
+                 tol: float = 1e-6, max_steps: int = 20_000) -> abi.Camera:
+    """Static camera at r = 100 M and the given inclination, looking at the
+    hole; 28 deg covers +- 25 M."""
+    return look_at_camera(r, math.radians(inclination_deg), fov, x_pix, tol, max_steps)
+
+
+def torus_target_params(seed: int = 1, rel: float = 0.05) -> dict:
+    """Parameters of the target image: every default perturbed by a relative
+    normal deviate of size rel from numpy default_rng(seed)."""
+    rng = np.random.default_rng(seed)
+    d = rng.standard_normal(len(TORUS_DEFAULTS))
+    return {k: v * (1 + rel * float(e)) for (k, v), e in zip(TORUS_DEFAULTS.items(), d)}
+
+
+def torus_problem(x_pix: int = 512, tol: float = 1e-6, params: dict | None = None):
+    """(scene, camera, colors) of the torus at the given parameters."""
+    p = dict(TORUS_DEFAULTS)
+    if params:
+        p.update(params)
+    scene = torus_scene(p["spin"], p["n_e0"], p["b_0"], p["theta_e0"])
+    cam = torus_camera(x_pix, p["inclination_deg"], tol=tol)
+    return scene, cam, torus_colors()

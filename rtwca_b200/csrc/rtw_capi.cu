@@ -117,7 +117,9 @@ void boost(double beta, M4 out) {
     out[1][1] = 1; out[2][2] = 1; out[3][3] = g;
 }
 
-bool is_kerr(int kind) { return kind == RTW_SCENE_KERR_DISK || kind == RTW_SCENE_KERR_THICK_DISK; }
+bool is_kerr(int kind) {
+    return kind == RTW_SCENE_KERR_DISK || kind == RTW_SCENE_KERR_THICK_DISK || kind == RTW_SCENE_KERR_SYNCHRO_TORUS;
+}
 
 double horizon_radius(const rtw_scene& s) {
     if (is_kerr(s.kind)) return s.mass + std::sqrt(s.mass * s.mass - s.spin * s.spin);
@@ -204,69 +206,9 @@ void make_dev_scene(const rtw_scene& scene, DevScene& d) {
 
 using namespace rtw;
 
-struct rtw_ctx {
-    int device = 0;
-    int num_sms = 148;
-    cudaStream_t stream = nullptr;
-    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
-    void* d_frames = nullptr;
-    size_t frames_cap = 0;
-    double* d_bins = nullptr;
-    unsigned long long* d_ctl = nullptr;  // [0] work counter, then DevStats
-    void* d_spec = nullptr;
-    size_t spec_cap = 0;
-    void* d_out = nullptr;
-    size_t out_cap = 0;
-    float* d_sink = nullptr;
-    unsigned long long* d_fclock = nullptr;  // per-frame timing, 3 words per frame
-    size_t fclock_cap = 0;
-    int last_frames = 0;
-    // autotuner results: (kind, precision, np, integrator) -> (warps, refill_min)
-    std::vector<std::pair<std::array<int, 4>, std::array<int, 2>>> tuned;
-    // captured launch sequence and the pinned staging it reads the frame and
-    // bin tables from
-    cudaGraphExec_t gexec = nullptr;
-    std::vector<unsigned char> gkey;
-    void* h_stage = nullptr;
-    size_t stage_cap = 0;
-    int last_grid = 0, last_warps = 0, last_refill = 0, last_replayed = 0;
-    std::string err;
-    rtw_stats last{};
-    bool have_last = false;
-};
+#include "rtw_ctx.h"
 
-namespace {
 
-rtw_status fail(rtw_ctx* ctx, rtw_status st, const std::string& msg) {
-    if (ctx) ctx->err = msg;
-    return st;
-}
-
-rtw_status cuda_fail(rtw_ctx* ctx, cudaError_t e, const char* what) {
-    return fail(ctx, RTW_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
-}
-
-#define RTW_CUDA(call, what)                              \
-    do {                                                  \
-        cudaError_t e_ = (call);                          \
-        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, what); \
-    } while (0)
-
-rtw_status ensure(rtw_ctx* ctx, void** ptr, size_t* cap, size_t need) {
-    if (need <= *cap && *ptr) return RTW_OK;
-    if (*ptr) cudaFree(*ptr);
-    *ptr = nullptr;
-    *cap = 0;
-    cudaError_t e = cudaMalloc(ptr, need);
-    if (e != cudaSuccess) {
-        *ptr = nullptr;
-        return fail(ctx, RTW_ERR_OOM, std::string("cudaMalloc failed: ") + cudaGetErrorString(e));
-    }
-    *cap = need;
-    return RTW_OK;
-}
-
-}  // namespace
 
 extern "C" {
 
@@ -309,6 +251,7 @@ void rtw_destroy(rtw_ctx* ctx) {
     cudaFree(ctx->d_out);
     cudaFree(ctx->d_sink);
     cudaFree(ctx->d_fclock);
+    torus_free(ctx->torus);
     if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
     if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
     for (auto& e : ctx->ev)
@@ -350,6 +293,16 @@ rtw_status rtw_scene_default(int32_t kind, rtw_scene* s) {
         s->spin = 0.9;
         s->r_in = 2.320883041761887;  // prograde ISCO of a = 0.9
         s->r_out = 30; s->temperature = 1e4; s->a_nu = 0.05;
+        break;
+    case RTW_SCENE_KERR_SYNCHRO_TORUS:
+        // no reference counterpart: n_e = 1e5 (r/6)^-1.5 exp(-z^2/2(0.3 r)^2),
+        // B = 10 (r/6)^-1 G, Theta_e = 10 (r/6)^-1, M87* length scale
+        // (the map_scale of Powehi.source/source_model.jl:7)
+        s->spin = 0.94;
+        s->r_in = 6; s->r_out = 40; s->edge_in = 0.5; s->edge_out = 5;
+        s->rho_h = 0.3; s->rho_index = -1.5; s->t_index = -1.0; s->b_index = -1.0;
+        s->n_e0 = 1e5; s->b_0 = 10; s->theta_e0 = 10; s->length_cm = 9.62e14;
+        s->escape_radius = 110;
         break;
     default:
         return RTW_ERR_INVALID_PARAM;
@@ -530,6 +483,7 @@ rtw_status rtw_render(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* ca
     if (prm->n_colors <= 0 || prm->n_colors > RTW_MAX_BINS || !prm->colors_nm)
         return fail(ctx, RTW_ERR_INVALID_PARAM, "n_colors must be 1..128 with colors_nm set");
     if (prm->ray_bundles) return fail(ctx, RTW_ERR_UNSUPPORTED, "ray bundles are not built");
+    if (scene->kind == RTW_SCENE_KERR_SYNCHRO_TORUS) return torus_render(ctx, scene, cams, n_cams, prm, out);
     if (scene->ref_precision) return fail(ctx, RTW_ERR_UNSUPPORTED, "ref_precision is an oracle-only switch");
     if (prm->precision != RTW_PREC_FP64 && prm->precision != RTW_PREC_MIXED)
         return fail(ctx, RTW_ERR_INVALID_PARAM, "precision");

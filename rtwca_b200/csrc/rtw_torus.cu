@@ -1,0 +1,1307 @@
+// rtw_torus.cu - the synchrotron torus: forward render (FP32-mixed or FP64,
+// FSAL Dormand-Prince, per-bin optical depth) and its discrete adjoint.
+//
+// Forward: one lane per ray, rays taken from a global queue one at a time
+// (per-lane refill; the lanes of a warp do not cooperate here). Per attempt
+// the seven geodesic stages run first (scene functor of rtw_scenes.cuh) and
+// leave six emitter-number sets (cj, nus, Theta, g) in local memory; then
+// each bin runs its own seven tau / I stages from those numbers in registers.
+// The error norm is the reference's RMS over all 8 + 2N components
+// (integrators_LttM.jl:185-224).
+//
+// Adjoint: a count pass (the forward render) gives each ray's number of
+// recorded steps; an exclusive scan gives offsets; a record pass re-runs the
+// forward and stores every accepted step's size (and polar escapes) plus the
+// state every `ck_every` steps. The reverse pass, one lane per ray in FP64,
+// walks the segments backwards: it replays a segment from its checkpoint,
+// then reverses each step through its stages with vector-Jacobian products
+// of the right-hand side built from dual numbers (rtw_dual.cuh).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "rtw_ctx.h"
+#include "rtw_trace.cuh"
+#include "rtw_torus.cuh"
+
+extern "C" rtw_status rtw_prepare_frames(const rtw_scene* scene, const rtw_camera* cams, int32_t n_cams,
+                                         void* frames_out, int64_t* total_out);
+
+namespace rtw {
+
+// FSAL Dormand-Prince: stage s point = y + h sum_{j<s} A[s][j] K_j (row 6 =
+// the 5th-order weights b, whose point is the new state), error weights E.
+#define RTW_TORUS_A                                        \
+    {{0, 0, 0, 0, 0, 0},                                   \
+     {a21, 0, 0, 0, 0, 0},                                 \
+     {a31, a32, 0, 0, 0, 0},                               \
+     {a41, a42, a43, 0, 0, 0},                             \
+     {a51, a52, a53, a54, 0, 0},                           \
+     {a61, a62, a63, a64, a65, 0},                         \
+     {b1, 0, b3, b4, b5, b6}}
+#define RTW_TORUS_E {e1, 0, e3, e4, e5, e6, e7}
+__constant__ double c_tA[7][6] = RTW_TORUS_A;
+__constant__ double c_tE[7] = RTW_TORUS_E;
+static const double h_tA[7][6] = RTW_TORUS_A;
+static const double h_tE[7] = RTW_TORUS_E;
+RTW_HD double tA(int s, int j) {
+#ifdef __CUDA_ARCH__
+    return c_tA[s][j];
+#else
+    return h_tA[s][j];
+#endif
+}
+RTW_HD double tE(int s) {
+#ifdef __CUDA_ARCH__
+    return c_tE[s];
+#else
+    return h_tE[s];
+#endif
+}
+
+// Everything a right-hand side needs.
+struct TorusModel {
+    DevScene geo;  // Kerr geodesic functor (its thin disk switched off)
+    TorusDev tor;
+    TorusBin bins[kTorusMaxBins];
+    int n;         // bins
+};
+
+// FP64 right-hand side on a state y[8 + 2N] = (x^mu, k^mu, tau_c, I_c).
+RTW_HD void torus_f64(const TorusModel& m, const double* y, double* f) {
+    const int N = m.n;
+    double z[10], k[9];
+    for (int i = 0; i < 8; ++i) z[i] = y[i];
+    z[8] = 0;
+    z[9] = y[1] - m.geo.r_ev;
+    Emit<double> em;
+    KerrScene<false>::rhs<double>(m.geo, z, k, em);
+    for (int i = 0; i < 8; ++i) f[i] = k[i];
+    const TorusPt<double> S = torus_point<double>(m.tor, m.tor.a, m.tor.n0, m.tor.B0, m.tor.Th0, y[1], y[2], y[4], y[7]);
+    for (int c = 0; c < N; ++c) {
+        double ft = 0, fi = 0;
+        if (S.on) torus_bin<double>(S.cj, S.nus, S.th, S.g, m.bins[c], ft, fi);
+        f[8 + c] = ft;
+        f[8 + N + c] = fi * exp(-y[8 + c]);
+    }
+}
+
+// mu += J^T kap and pb += (d f / d(a, -, n0, b0, th0))^T kap at state y.
+RTW_HD void torus_vjp(const TorusModel& m, const double* y, const double* kap, double* mu, double* pb) {
+    const int N = m.n;
+    // dx^mu / dl = k^mu
+    for (int i = 0; i < 4; ++i) mu[4 + i] += kap[i];
+    {
+        typedef Dual<double, 7> D7;  // r, theta, k^t, k^r, k^theta, k^phi, a
+        const D7 r = D7::var(y[1], 0), th = D7::var(y[2], 1), a = D7::var(m.tor.a, 6);
+        D7 k[4], acc[4];
+        for (int i = 0; i < 4; ++i) k[i] = D7::var(y[4 + i], 2 + i);
+        kerr_accel<D7>(m.tor.M, a, r, th, k, acc);
+        for (int i = 0; i < 4; ++i) {
+            const double c = kap[4 + i];
+            if (c == 0) continue;
+            mu[1] += c * acc[i].d[0];
+            mu[2] += c * acc[i].d[1];
+            for (int q = 0; q < 4; ++q) mu[4 + q] += c * acc[i].d[2 + q];
+            pb[0] += c * acc[i].d[6];
+        }
+    }
+    typedef Dual<double, 8> D8;  // r, theta, k^t, k^phi, a, n0, b0, th0
+    const TorusPt<D8> S = torus_point<D8>(m.tor, D8::var(m.tor.a, 4), D8::var(m.tor.n0, 5), D8::var(m.tor.B0, 6),
+                                          D8::var(m.tor.Th0, 7), D8::var(y[1], 0), D8::var(y[2], 1),
+                                          D8::var(y[4], 2), D8::var(y[7], 3));
+    if (!S.on) return;
+    double sb[4] = {0, 0, 0, 0};
+    typedef Dual<double, 4> D4;  // cj, nus, Theta, g
+    const D4 cj = D4::var(S.cj.v, 0), nus = D4::var(S.nus.v, 1), tht = D4::var(S.th.v, 2), g = D4::var(S.g.v, 3);
+    for (int c = 0; c < N; ++c) {
+        D4 ft, fi;
+        torus_bin<D4>(cj, nus, tht, g, m.bins[c], ft, fi);
+        const double e = exp(-y[8 + c]);
+        const double kt = kap[8 + c], ki = kap[8 + N + c];
+        for (int q = 0; q < 4; ++q) sb[q] += kt * ft.d[q] + ki * e * fi.d[q];
+        mu[8 + c] += -ki * fi.v * e;  // d (fi exp(-tau)) / d tau
+    }
+    const D8* comp[4] = {&S.cj, &S.nus, &S.th, &S.g};
+    double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int q = 0; q < 4; ++q)
+        for (int t = 0; t < 8; ++t) v[t] += sb[q] * comp[q]->d[t];
+    mu[1] += v[0];
+    mu[2] += v[1];
+    mu[4] += v[2];
+    mu[7] += v[3];
+    pb[0] += v[4];
+    pb[2] += v[5];
+    pb[3] += v[6];
+    pb[4] += v[7];
+}
+
+// keepinbounds! (Kerr source_geometry.jl:275-301) on a full state; returns
+// whether theta was reflected (theta and k^theta change sign, phi shifts).
+RTW_HD bool torus_keep(double* x) {
+    bool refl = false;
+    if (x[2] < 0) {
+        x[2] = -x[2];
+        x[3] -= kPi;
+        x[6] = -x[6];
+        refl = !refl;
+    }
+    if (!(x[2] < 2 * kPi)) {
+        double r = fmod(x[2], 2 * kPi);
+        if (r < 0) r += 2 * kPi;
+        x[2] = r;
+    }
+    if (x[2] >= kPi) {
+        x[2] = 2 * kPi - x[2];
+        x[3] += kPi;
+        x[6] = -x[6];
+        refl = !refl;
+    }
+    return refl;
+}
+
+// pad_max_dt of the Kerr scene (source_model.jl:86-103, the scale cast to
+// Float32) over a generic scalar, for the derivative of the step sizes it sets:
+// x2 = theta, vr, vth, vph = k^r, k^theta, k^phi.
+template <class T>
+RTW_HD T torus_pad(const T& x2, const T& vr, const T& vth, const T& vph, double scale_d) {
+    typedef decltype(val(x2)) B;
+    const double scale = (double)(float)scale_d;
+    const double th = (double)val(x2);
+    const double eps = (th < kPi / 8 || th > 7 * kPi / 8) ? fmin(scale, (double)1e-1f) : scale;
+    auto tab = [](const T& v) { return val(v) < 0 ? -v : v; };
+    const T first = tab(vr) * B(1.0 / eps) + B(kNoDivZero);
+    const T pole = th <= kPi - th ? x2 : T(B(kPi)) - x2;
+    const T second = T(B(1.0)) / (pole * B(eps) / (tab(vth) + B(kNoDivZero)) + B(kNoDivZero));
+    const T third = T(B(1.0)) / (T(B(eps)) / (tab(vph) + B(kNoDivZero)) + B(kNoDivZero));
+    const T m = T(B(1.0)) / (first + second + third + B(kNoDivZero));
+    if (val(m) > 0.5) return T(B(0.5));
+    if (val(m) < (double)1e-12f) return T(B((double)1e-12f));
+    return m;
+}
+
+// d(-pad_max_dt)/dy at y, added to lam with weight w
+RTW_HD void torus_pad_vjp(const double* y, double scale, double w, double* lam) {
+    typedef Dual<double, 4> D4;
+    const D4 m = torus_pad<D4>(D4::var(y[2], 0), D4::var(y[5], 1), D4::var(y[6], 2), D4::var(y[7], 3), scale);
+    lam[2] -= w * m.d[0];
+    lam[5] -= w * m.d[1];
+    lam[6] -= w * m.d[2];
+    lam[7] -= w * m.d[3];
+}
+
+// n_events word: the count, and a flag for rays checkpointed at every step
+// (rays with a polar escape: near the pole the FP64 replay of FP32-stage
+// steps would drift by more than the distance to the axis)
+constexpr uint32_t kDenseCheckpoints = 0x80000000u;
+constexpr uint32_t kEventCount = 0x7fffffffu;
+
+struct TorusKP {
+    TorusModel m;
+    FrameDesc frame;
+    long long total_rays;
+    double max_dt_scale, promote_dr, promote_theta;
+    unsigned long long* counter;
+    DevStats* stats;
+    float* spectrum;  // [P][N]
+    uint8_t* cls;
+    uint32_t* steps;
+    // recording
+    int record;                        // 0: count events, 1: store them
+    uint32_t* n_events;                // [P] (count pass writes, record pass checks)
+    const unsigned long long* ev_off;  // [P] first event of a ray
+    const unsigned long long* ck_off;  // [P] first checkpoint of a ray
+    double* ev_h;                      // [E] step size (DP step) or escape sub-step size
+    uint8_t* ev_kind;                  // [E] 0: DP step with a controller step size, 0x41 / 0x42: DP
+                                       // step of -pad_max_dt of the previous / its own start state,
+                                       // 1 + n: polar escape of n sub-steps
+    double* ck;                        // [C][8 + 2N] states
+    int ck_every;
+    unsigned int* err_flag;            // bit 0: record pass diverged from the count pass
+};
+
+template <class R>
+struct TorusStages {
+    double ns[8];        // 5th-order slope of the geodesic components
+    double es[8];        // error slope sum_j E_j K_j
+    R k7[8];             // slope at the new state (carried, FSAL)
+    TorusPt<R> S[7];     // emitter numbers of stage points 1..6 (index 0 unused)
+};
+
+// The seven geodesic stages of one attempt in arithmetic R from the FP64
+// state x and the carried slope k1.
+template <class R, class K>
+__device__ void torus_geo_stages(const TorusModel& m, const double* x, const K* k1, double h, TorusStages<R>& o) {
+    R Kg[7][8];
+    for (int i = 0; i < 8; ++i) Kg[0][i] = R(k1[i]);
+    const R hr = R(h);
+    const R d0 = R(x[1] - m.geo.r_ev);
+#pragma unroll 1
+    for (int s = 1; s < 7; ++s) {
+        R acc[8];
+        for (int i = 0; i < 8; ++i) acc[i] = R(0);
+        for (int j = 0; j < s; ++j) {
+            const R w = R(tA(s, j));
+            for (int i = 0; i < 8; ++i) acc[i] += w * Kg[j][i];
+        }
+        R z[10], kk[9];
+        for (int i = 0; i < 8; ++i) z[i] = R(x[i]) + hr * acc[i];
+        z[8] = R(0);
+        z[9] = d0 + hr * acc[1];
+        Emit<R> em;
+        KerrScene<false>::rhs<R>(m.geo, z, kk, em);
+        for (int i = 0; i < 8; ++i) Kg[s][i] = kk[i];
+        o.S[s] = torus_point<R>(m.tor, R(m.tor.a), R(m.tor.n0), R(m.tor.B0), R(m.tor.Th0), z[1], z[2], z[4], z[7]);
+        if (s == 6)
+            for (int i = 0; i < 8; ++i) o.ns[i] = (double)acc[i];
+    }
+    for (int i = 0; i < 8; ++i) {
+        R e = R(0);
+        for (int j = 0; j < 7; ++j) e += R(tE(j)) * Kg[j][i];
+        o.es[i] = (double)e;
+        o.k7[i] = Kg[6][i];
+    }
+}
+
+// promoted (FP64-stage) geodesic part of the mixed path, out of line
+template <class K>
+__device__ __noinline__ void torus_geo_stages_fp64(const TorusModel& m, const double* x, const K* k1, double h,
+                                                   TorusStages<double>* o) {
+    torus_geo_stages<double, K>(m, x, k1, h, *o);
+}
+
+// calc_terminate without the step-count predicate; THICK when every bin's
+// tau has reached -log(tol)
+template <class SR>
+__device__ __forceinline__ int torus_terminate(const TorusKP& p, const double* x, const SR* tau, int N) {
+    if (x[1] > p.m.geo.esc) return RTW_CLASS_ESCAPE;
+    if (x[1] <= p.frame.r_term) return RTW_CLASS_HORIZON;
+    if (x[3] > p.m.geo.wind) return RTW_CLASS_WINDING;
+    for (int c = 0; c < N; ++c)
+        if ((double)tau[c] < p.frame.thick) return 0;
+    return RTW_CLASS_THICK;
+}
+
+// Forward kernel. SR: arithmetic of the bins and of the stages (float on the
+// mixed path, with Kahan intensities and per-ray FP64 stages near the horizon
+// and the poles; double on the FP64 path).
+template <bool MIXED>
+__global__ void __launch_bounds__(128) torus_forward(const TorusKP p) {
+    typedef typename SpecTraits<MIXED>::SR SR;
+    const int N = p.m.n;
+    const int D = 8 + 2 * N;
+    unsigned c_att = 0, c_rej = 0, c_pro = 0, c_esc = 0, c_rays = 0, c_nan = 0;
+    for (;;) {
+        const long long id = (long long)atomicAdd(p.counter, 1ull);
+        if (id >= p.total_rays) break;
+        ++c_rays;
+        const int pi = (int)(id % p.frame.xp), pj = (int)(id / p.frame.xp);
+        double x[9];
+        camera_ray(p.frame, pi, pj, x);
+        SR tau[kTorusMaxBins], ihi[kTorusMaxBins], ilo[kTorusMaxBins], kt1[kTorusMaxBins], ki1[kTorusMaxBins];
+        SR k1[8];
+        {
+            double y[8 + 2 * kTorusMaxBins], f[8 + 2 * kTorusMaxBins];
+            for (int i = 0; i < 8; ++i) y[i] = x[i];
+            for (int i = 8; i < D; ++i) y[i] = 0;
+            torus_f64(p.m, y, f);
+            for (int i = 0; i < 8; ++i) k1[i] = SR(f[i]);
+            for (int c = 0; c < N; ++c) {
+                tau[c] = 0; ihi[c] = 0; ilo[c] = 0;
+                kt1[c] = SR(f[8 + c]);
+                ki1[c] = SR(f[8 + N + c]);
+            }
+        }
+        double h = -pad_max_dt<RTW_SCENE_KERR_DISK, SR>(p.m.geo, x, p.max_dt_scale);
+        // where h came from: 0 the controller (held fixed by the adjoint),
+        // 1 -pad_max_dt of the previous accepted step's start state, 2 -pad_max_dt
+        // of the current state
+        uint8_t hsrc = 2;
+        const double tol = p.frame.tol;
+        bool prev_rej = false;
+        long long nsteps = 0;
+        uint32_t n_ev = 0;
+        bool escaped = false;  // a ray with a polar escape stores its state at every step
+        const uint32_t ev_word = p.record ? p.n_events[id] : 0u;
+        const uint32_t ev_cap = ev_word & kEventCount;
+        const uint32_t kc = (ev_word & kDenseCheckpoints) ? 1u : (uint32_t)p.ck_every;
+        const unsigned long long eo = p.record ? p.ev_off[id] : 0ull;
+        const unsigned long long co = p.record ? p.ck_off[id] : 0ull;
+        bool bad = false;
+        // a checkpoint of the state before event n_ev when it starts a segment
+        auto checkpoint = [&]() {
+            if (!p.record || n_ev >= ev_cap || (n_ev % kc) != 0u) return;
+            double* c = p.ck + (co + n_ev / kc) * (unsigned long long)D;
+            for (int i = 0; i < 8; ++i) c[i] = x[i];
+            for (int q = 0; q < N; ++q) {
+                c[8 + q] = (double)tau[q];
+                c[8 + N + q] = (double)ihi[q] + (MIXED ? (double)ilo[q] : 0.0);
+            }
+        };
+        auto push = [&](uint8_t kind, double hv) {
+            if (p.record) {
+                if (n_ev >= ev_cap) {
+                    bad = true;
+                } else {
+                    p.ev_h[eo + n_ev] = hv;
+                    p.ev_kind[eo + n_ev] = kind;
+                }
+            }
+            ++n_ev;
+        };
+        int cls = 0;
+        for (;;) {
+            ++c_att;
+            const double max_dt = pad_max_dt<RTW_SCENE_KERR_DISK, SR>(p.m.geo, x, p.max_dt_scale);
+            double temp;
+            bool done = false;
+            if (near_singularity<RTW_SCENE_KERR_DISK>(x, h, tol, &temp)) {
+                // polar escape (integrators_LttM.jl:62-105) in FP64 on the full state
+                checkpoint();
+                double y[8 + 2 * kTorusMaxBins], f[8 + 2 * kTorusMaxBins];
+                for (int i = 0; i < 8; ++i) {
+                    y[i] = x[i];
+                    f[i] = (double)k1[i];
+                }
+                for (int q = 0; q < N; ++q) {
+                    y[8 + q] = (double)tau[q];
+                    y[8 + N + q] = (double)ihi[q] + (MIXED ? (double)ilo[q] : 0.0);
+                    f[8 + q] = (double)kt1[q];
+                    f[8 + N + q] = (double)ki1[q];
+                }
+                int nsub = 0;
+                for (int it = 0; it < 37; ++it) {
+                    if (it > 0) {
+                        if (torus_terminate<double>(p, y, y + 8, N)) continue;
+                        torus_f64(p.m, y, f);
+                    }
+                    for (int i = 0; i < D; ++i) y[i] -= temp * f[i];
+                    torus_keep(y);
+                    ++nsub;
+                }
+                c_esc += nsub;
+                escaped = true;
+                push((uint8_t)(1 + nsub), temp);
+                for (int i = 0; i < 8; ++i) x[i] = y[i];
+                for (int q = 0; q < N; ++q) {
+                    tau[q] = SR(y[8 + q]);
+                    ihi[q] = SR(y[8 + N + q]);
+                    ilo[q] = MIXED ? SR(y[8 + N + q] - (double)ihi[q]) : SR(0);
+                }
+                if (torus_terminate<double>(p, y, y + 8, N)) {
+                    done = true;
+                    prev_rej = false;
+                } else {
+                    torus_f64(p.m, y, f);
+                    for (int i = 0; i < 8; ++i) k1[i] = SR(f[i]);
+                    for (int q = 0; q < N; ++q) {
+                        kt1[q] = SR(f[8 + q]);
+                        ki1[q] = SR(f[8 + N + q]);
+                    }
+                    h = -pad_max_dt<RTW_SCENE_KERR_DISK, SR>(p.m.geo, x, p.max_dt_scale);
+                    hsrc = 2;
+                }
+            }
+            if (!done) {
+                // geodesic stages
+                TorusStages<SR> st;
+                bool promote = false;
+                if (MIXED)
+                    promote = (x[1] - p.m.geo.r_ev < p.promote_dr) || (x[2] < p.promote_theta) ||
+                              (x[2] > kPi - p.promote_theta);
+                if (promote) {
+                    ++c_pro;
+                    TorusStages<double> sd;
+                    torus_geo_stages_fp64<SR>(p.m, x, k1, h, &sd);
+                    for (int i = 0; i < 8; ++i) {
+                        st.ns[i] = sd.ns[i];
+                        st.es[i] = sd.es[i];
+                        st.k7[i] = SR(sd.k7[i]);
+                    }
+                    for (int s = 1; s < 7; ++s) {
+                        st.S[s].cj = SR(sd.S[s].cj);
+                        st.S[s].nus = SR(sd.S[s].nus);
+                        st.S[s].th = SR(sd.S[s].th);
+                        st.S[s].g = SR(sd.S[s].g);
+                        st.S[s].on = sd.S[s].on;
+                    }
+                } else {
+                    torus_geo_stages<SR, SR>(p.m, x, k1, h, st);
+                }
+                double y[8];
+                double err2 = 0;
+                for (int i = 0; i < 8; ++i) {
+                    y[i] = x[i] + h * st.ns[i];
+                    const double d = h * st.es[i];
+                    const double tl = tol + fmax(fabs(x[i]), fabs(y[i])) * tol;
+                    err2 += (d / tl) * (d / tl);
+                }
+                // bins: seven tau / I stages each
+                SR c_t[kTorusMaxBins], c_h[kTorusMaxBins], c_l[kTorusMaxBins], c_kt[kTorusMaxBins],
+                    c_ki[kTorusMaxBins];
+                const SR hs = SR(h), ts = SR(tol);
+                SR ebins = 0;
+                for (int c = 0; c < N; ++c) {
+                    SR kt[7], ki[7];
+                    kt[0] = kt1[c];
+                    ki[0] = ki1[c];
+                    const SR t0 = tau[c];
+                    SR tp = t0;
+#pragma unroll
+                    for (int s = 1; s < 7; ++s) {
+                        SR a = 0;
+#pragma unroll
+                        for (int j = 0; j < s; ++j) a += SR(tA(s, j)) * kt[j];
+                        tp = t0 + hs * a;
+                        SR ft = 0, fi = 0;
+                        if (st.S[s].on) torus_bin<SR>(st.S[s].cj, st.S[s].nus, st.S[s].th, st.S[s].g, p.m.bins[c], ft, fi);
+                        kt[s] = ft;
+                        ki[s] = fi * texp(-tp);
+                    }
+                    // tp is now the new tau (row 6 of A is b)
+                    SR nsI = 0, et = 0, ei = 0;
+#pragma unroll
+                    for (int j = 0; j < 7; ++j) {
+                        if (j < 6) nsI += SR(tA(6, j)) * ki[j];
+                        et += SR(tE(j)) * kt[j];
+                        ei += SR(tE(j)) * ki[j];
+                    }
+                    SR yh = ihi[c], yl = MIXED ? ilo[c] : SR(0);
+                    if constexpr (MIXED) {
+                        kahan_add(yh, yl, hs * nsI);
+                    } else {
+                        yh = yh + hs * nsI;
+                    }
+                    const SR i0 = ihi[c];
+                    const SR dt_ = hs * et, di = hs * ei;
+                    const SR tlt = ts + rmax(rabs(t0), rabs(tp)) * ts;
+                    const SR tli = ts + rmax(rabs(i0), rabs(yh)) * ts;
+                    ebins += (dt_ / tlt) * (dt_ / tlt) + (di / tli) * (di / tli);
+                    c_t[c] = tp;
+                    c_h[c] = yh;
+                    c_l[c] = yl;
+                    c_kt[c] = kt[6];
+                    c_ki[c] = ki[6];
+                }
+                err2 += (double)ebins;
+                bool accept;
+                double hnext;
+                decide<double>(err2, D, h, max_dt, prev_rej, accept, hnext);
+                const uint8_t next_src = hnext == -max_dt ? (accept ? 1 : 2) : 0;
+                if (accept) {
+                    checkpoint();
+                    push(hsrc ? (uint8_t)(0x40 | hsrc) : (uint8_t)0, h);
+                    for (int i = 0; i < 8; ++i) {
+                        x[i] = y[i];
+                        k1[i] = st.k7[i];
+                    }
+                    for (int c = 0; c < N; ++c) {
+                        tau[c] = c_t[c];
+                        ihi[c] = c_h[c];
+                        ilo[c] = c_l[c];
+                        kt1[c] = c_kt[c];
+                        ki1[c] = c_ki[c];
+                    }
+                    if (torus_keep(x)) {
+                        // reflected through the pole: the carried slope belongs to
+                        // the unreflected point, so take f at the new state
+                        double yy[8 + 2 * kTorusMaxBins], ff[8 + 2 * kTorusMaxBins];
+                        for (int i = 0; i < 8; ++i) yy[i] = x[i];
+                        for (int q = 0; q < N; ++q) {
+                            yy[8 + q] = (double)tau[q];
+                            yy[8 + N + q] = (double)ihi[q] + (MIXED ? (double)ilo[q] : 0.0);
+                        }
+                        torus_f64(p.m, yy, ff);
+                        for (int i = 0; i < 8; ++i) k1[i] = SR(ff[i]);
+                        for (int q = 0; q < N; ++q) {
+                            kt1[q] = SR(ff[8 + q]);
+                            ki1[q] = SR(ff[8 + N + q]);
+                        }
+                    }
+                    prev_rej = false;
+                } else {
+                    torus_keep(x);
+                    prev_rej = true;
+                    ++c_rej;
+                }
+                h = hnext;
+                hsrc = next_src;
+            }
+            ++nsteps;
+            if (nsteps >= p.frame.max_steps) cls = RTW_CLASS_MAXSTEPS;
+            else cls = torus_terminate<SR>(p, x, tau, N);
+            if (cls) break;
+        }
+        bool fin = true;
+        for (int i = 0; i < 8; ++i) fin &= isfinite(x[i]);
+        if (!fin) {
+            cls = RTW_CLASS_NAN;
+            ++c_nan;
+        }
+        if (p.spectrum)
+            for (int c = 0; c < N; ++c)
+                p.spectrum[id * N + c] = (float)((double)ihi[c] + (MIXED ? (double)ilo[c] : 0.0));
+        if (p.cls) p.cls[id] = (uint8_t)cls;
+        if (p.steps) p.steps[id] = (uint32_t)nsteps;
+        if (!p.record && p.n_events) p.n_events[id] = n_ev | (escaped ? kDenseCheckpoints : 0u);
+        if (p.record && (bad || n_ev != ev_cap)) atomicOr(p.err_flag, 1u);
+    }
+    atomicAdd(&p.stats->step_attempts, (unsigned long long)c_att);
+    atomicAdd(&p.stats->rejected_steps, (unsigned long long)c_rej);
+    atomicAdd(&p.stats->promoted_steps, (unsigned long long)c_pro);
+    atomicAdd(&p.stats->escape_substeps, (unsigned long long)c_esc);
+    atomicAdd(&p.stats->nan_rays, (unsigned long long)c_nan);
+    atomicAdd(&p.stats->rays, (unsigned long long)c_rays);
+}
+
+struct TorusRP {
+    TorusKP f;
+    FrameDesc dframe[2];  // d frame / d a, d frame / d inclination (pos and M; the rest as frame)
+    const float* target;
+    const float* spectrum;
+    double* work;                // per lane: work_stride doubles
+    long long work_stride;
+    double* out;                 // [1 + 5 + 2]: loss, gradient, escapes carried as identity, rays with escapes
+    double* per_ray;             // [P][5] per-ray gradients (may be null)
+    int skip_escape_rays;        // 1: rays with a polar escape give no gradient
+    unsigned long long* counter;
+};
+
+// One recorded step of a ray, replayed in FP64: y_out = keep(step(y_in)).
+RTW_HD bool torus_is_dp(uint8_t kind) { return kind == 0 || (kind & 0x40); }
+
+__device__ bool torus_replay(const TorusModel& m, const double* y_in, uint8_t kind, double hv, double* y_out,
+                             double* K, double* Y) {
+    const int N = m.n, D = 8 + 2 * N;
+    if (torus_is_dp(kind)) {
+        // K: [6][D] stage slopes, Y: [D] a stage point
+        torus_f64(m, y_in, K);
+        for (int s = 1; s < 6; ++s) {
+            for (int i = 0; i < D; ++i) {
+                double acc = 0;
+                for (int j = 0; j < s; ++j) acc += tA(s, j) * K[j * D + i];
+                Y[i] = y_in[i] + hv * acc;
+            }
+            torus_f64(m, Y, K + s * D);
+        }
+        for (int i = 0; i < D; ++i) {
+            double acc = 0;
+            for (int j = 0; j < 6; ++j) acc += tA(6, j) * K[j * D + i];
+            y_out[i] = y_in[i] + hv * acc;
+        }
+        return torus_keep(y_out);
+    }
+    for (int i = 0; i < D; ++i) y_out[i] = y_in[i];
+    bool refl = false;
+    for (int it = 0; it < (int)kind - 1; ++it) {
+        torus_f64(m, y_out, K);
+        for (int i = 0; i < D; ++i) y_out[i] -= hv * K[i];
+        refl = torus_keep(y_out);
+    }
+    return refl;  // (the reverse pass replays escapes sub-step by sub-step)
+}
+
+// Sub-step size of the polar escape from y (near_singularity, Kerr
+// source_geometry.jl:249-269): 2 |theta - pole| / (37 |k^theta|), the pole
+// nearer to theta.
+RTW_HD double torus_escape_temp(const double* y) {
+    const double dth = y[2] < 0.5 * kPi ? y[2] : y[2] - kPi;
+    return 2 * fabs(dth) / (fabs(y[6] * 37) + kNoDivZero);
+}
+
+// End state of a polar escape of n sub-steps z <- keep(z - temp f(z)) from y.
+RTW_HD void torus_escape_end(const TorusModel& m, const double* y, int nsub, double* z, double* K) {
+    const int D = 8 + 2 * m.n;
+    const double temp = torus_escape_temp(y);
+    for (int i = 0; i < D; ++i) z[i] = y[i];
+    for (int s = 0; s < nsub; ++s) {
+        torus_f64(m, z, K);
+        for (int i = 0; i < D; ++i) z[i] -= temp * K[i];
+        torus_keep(z);
+    }
+}
+
+// Vector-Jacobian product of a polar escape of n sub-steps from y with
+// sub-step size temp (the recorded value, = torus_escape_temp(y)): lam (the
+// cotangent of the end state) becomes that of y and pb gains the parameter
+// part. The sub-step size depends on y and is differentiated too. Returns
+// false when the escape amplified the geodesic cotangent by more than 1e3
+// (sum |lambda_i y_i|): such an escape passed so close to the axis that its
+// local derivative is a spike narrower than any parameter change, and it is
+// carried as the identity (the state is continuous across the pole) with the
+// exact per-bin tau -> I coupling. Scratch: W [4][D], mu, tmp [D].
+RTW_HD bool torus_escape_vjp(const TorusModel& m, const double* y, int nsub, double temp, double* lam,
+                             double* pb, double* W, double* mu, double* tmp) {
+    const int N = m.n, D = 8 + 2 * N;
+    double* z = W;             // sub-step state
+    double* lin = W + D;       // the cotangent of the end state
+    double* zl = W + 2 * D;    // one sub-step ahead
+    double pbe[kTorusParams] = {0, 0, 0, 0, 0};
+    for (int i = 0; i < D; ++i) lin[i] = lam[i];
+    double gtemp = 0;  // d loss / d temp
+    for (int s = nsub - 1; s >= 0; --s) {
+        // z_s by replay from y (the sub-steps are few and the escapes rare)
+        for (int i = 0; i < D; ++i) z[i] = y[i];
+        for (int t = 0; t < s; ++t) {
+            torus_f64(m, z, tmp);
+            for (int i = 0; i < D; ++i) z[i] -= temp * tmp[i];
+            torus_keep(z);
+        }
+        torus_f64(m, z, tmp);
+        // sub-step s: z_{s+1} = keep(z_s - temp f(z_s))
+        for (int i = 0; i < D; ++i) zl[i] = z[i] - temp * tmp[i];
+        if (torus_keep(zl)) {
+            lam[2] = -lam[2];
+            lam[6] = -lam[6];
+        }
+        for (int i = 0; i < D; ++i) gtemp -= lam[i] * tmp[i];
+        for (int i = 0; i < D; ++i) {
+            zl[i] = -temp * lam[i];
+            mu[i] = 0;
+        }
+        torus_vjp(m, z, zl, mu, pbe);
+        for (int i = 0; i < D; ++i) lam[i] += mu[i];
+    }
+    const double dth = y[2] < 0.5 * kPi ? y[2] : y[2] - kPi;
+    const double den = fabs(y[6] * 37) + kNoDivZero;
+    lam[2] += gtemp * 2 * (dth >= 0 ? 1.0 : -1.0) / den;
+    lam[6] += gtemp * (-2 * fabs(dth) * 37 * (y[6] >= 0 ? 1.0 : -1.0) / (den * den));
+    double na = 0, nb = 0;
+    for (int i = 1; i < 8; ++i) {
+        if (i == 3) continue;
+        na += fabs(lam[i] * y[i]);
+        nb += fabs(lin[i] * y[i]);
+    }
+    for (int c = 0; c < N; ++c) nb += fabs(lin[8 + N + c] * y[8 + N + c]);
+    if (!(na <= 1e3 * nb + 1e-300)) {
+        for (int i = 0; i < D; ++i) lam[i] = lin[i];
+        torus_escape_end(m, y, nsub, z, tmp);
+        for (int c = 0; c < N; ++c) lam[8 + c] -= lin[8 + N + c] * (z[8 + N + c] - y[8 + N + c]);
+        return false;
+    }
+    for (int q = 0; q < kTorusParams; ++q) pb[q] += pbe[q];
+    return true;
+}
+
+// Reverse kernel (FP64). Per lane work area, D = 8 + 2N doubles per row:
+//   Ys [ck_every + 1] segment states, K [6] stage slopes, Yst [6] stage
+//   points, kac [6] stage cotangents, Ze [4] escape evaluations,
+//   lam, mu, tmp [1] each.
+__global__ void __launch_bounds__(128) torus_reverse(const TorusRP p) {
+    const TorusModel& m = p.f.m;
+    const int N = m.n, D = 8 + 2 * N;
+    const int KCmax = p.f.ck_every;
+    const long long slot = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    double* W = p.work + slot * p.work_stride;
+    double* Ys = W;
+    double* Kst = Ys + (long long)(KCmax + 1) * D;
+    double* Yst = Kst + 6 * D;
+    double* kac = Yst + 6 * D;
+    double* Ze = kac + 6 * D;
+    double* lam = Ze + 4 * D;
+    double* mu = lam + D;
+    double* tmp = mu + D;
+    unsigned n_cut = 0;
+    for (;;) {
+        const long long id = (long long)atomicAdd(p.counter, 1ull);
+        if (id >= p.f.total_rays) break;
+        double loss = 0;
+        bool fin = true;
+        for (int i = 0; i < D; ++i) lam[i] = 0;
+        for (int c = 0; c < N; ++c) {
+            const double d = (double)p.spectrum[id * N + c] - (double)p.target[id * N + c];
+            fin &= isfinite(d);
+            lam[8 + N + c] = 2 * d;
+            loss += d * d;
+        }
+        const bool escaped = (p.f.n_events[id] & kDenseCheckpoints) != 0;
+        if (escaped) atomicAdd(&p.out[2 + kTorusParams], 1.0);
+        if (!fin || (escaped && p.skip_escape_rays)) {
+            if (fin) atomicAdd(&p.out[0], loss);
+            if (p.per_ray)
+                for (int q = 0; q < kTorusParams; ++q) p.per_ray[id * kTorusParams + q] = 0;
+            continue;
+        }
+        double pb[kTorusParams] = {0, 0, 0, 0, 0};
+        double pend = 0;  // d loss / d h of a step whose h was set at the previous step's start
+        const uint32_t n_ev = p.f.n_events[id] & kEventCount;
+        const int KC = (p.f.n_events[id] & kDenseCheckpoints) ? 1 : p.f.ck_every;
+        const unsigned long long eo = p.f.ev_off[id], co = p.f.ck_off[id];
+        const int nseg = (int)((n_ev + (uint32_t)KC - 1) / (uint32_t)KC);
+        for (int seg = nseg - 1; seg >= 0; --seg) {
+            const int e0 = seg * KC;
+            const int e1 = min(e0 + KC, (int)n_ev);
+            const double* c = p.f.ck + (co + (unsigned long long)seg) * (unsigned long long)D;
+            for (int i = 0; i < D; ++i) Ys[i] = c[i];
+            unsigned long long refl = 0;
+            for (int e = e0; e < e1; ++e) {
+                const uint8_t kind = p.f.ev_kind[eo + e];
+                const double hv = p.f.ev_h[eo + e];
+                const bool r = torus_replay(m, Ys + (long long)(e - e0) * D, kind, hv,
+                                            Ys + (long long)(e - e0 + 1) * D, Kst, Yst);
+                if (torus_is_dp(kind) && r) refl |= 1ull << (e - e0);
+            }
+            for (int e = e1 - 1; e >= e0; --e) {
+                const double* y = Ys + (long long)(e - e0) * D;
+                const uint8_t kind = p.f.ev_kind[eo + e];
+                const double hv = p.f.ev_h[eo + e];
+                if (torus_is_dp(kind)) {
+                    if (refl >> (e - e0) & 1ull) {
+                        lam[2] = -lam[2];
+                        lam[6] = -lam[6];
+                    }
+                    // stages of the step
+                    for (int i = 0; i < D; ++i) Yst[i] = y[i];
+                    torus_f64(m, y, Kst);
+                    for (int s = 1; s < 6; ++s) {
+                        for (int i = 0; i < D; ++i) {
+                            double acc = 0;
+                            for (int j = 0; j < s; ++j) acc += tA(s, j) * Kst[j * D + i];
+                            Yst[s * D + i] = y[i] + hv * acc;
+                        }
+                        torus_f64(m, Yst + s * D, Kst + s * D);
+                    }
+                    // y' = y + h sum_s b_s K_s, K_s = f(Y_s), Y_s = y + h sum_{j<s} A_sj K_j;
+                    // hbar = d loss / d h, for step sizes set by pad_max_dt
+                    double hbar = 0;
+                    for (int i = 0; i < D; ++i) {
+                        double bk = 0;
+                        for (int s = 0; s < 6; ++s) bk += tA(6, s) * Kst[s * D + i];
+                        hbar += lam[i] * bk;
+                    }
+                    for (int s = 0; s < 6; ++s)
+                        for (int i = 0; i < D; ++i) kac[s * D + i] = hv * tA(6, s) * lam[i];
+                    for (int t = 5; t >= 0; --t) {
+                        for (int i = 0; i < D; ++i) mu[i] = 0;
+                        torus_vjp(m, Yst + t * D, kac + t * D, mu, pb);
+                        for (int i = 0; i < D; ++i) lam[i] += mu[i];
+                        for (int i = 0; i < D && t > 0; ++i) {
+                            double ak = 0;
+                            for (int s = 0; s < t; ++s) ak += tA(t, s) * Kst[s * D + i];
+                            hbar += mu[i] * ak;
+                        }
+                        for (int s = 0; s < t; ++s) {
+                            const double w = hv * tA(t, s);
+                            if (w != 0)
+                                for (int i = 0; i < D; ++i) kac[s * D + i] += w * mu[i];
+                        }
+                    }
+                    // a pending step-size term of the next step lands on this state
+                    if (pend != 0) torus_pad_vjp(y, p.f.max_dt_scale, pend, lam);
+                    pend = 0;
+                    if (kind == 0x42) torus_pad_vjp(y, p.f.max_dt_scale, hbar, lam);
+                    if (kind == 0x41) pend = hbar;
+                } else {
+                    if (!torus_escape_vjp(m, y, (int)kind - 1, hv, lam, pb, Ze, mu, tmp)) ++n_cut;
+                }
+            }
+        }
+        // the camera initial data: d y0 / d(a, inclination)
+        const int pi = (int)(id % p.f.frame.xp), pj = (int)(id / p.f.frame.xp);
+        for (int q = 0; q < 2; ++q) {
+            double dy[9];
+            camera_ray(p.dframe[q], pi, pj, dy);
+            double s = 0;
+            for (int i = 0; i < 8; ++i) s += lam[i] * dy[i];
+            pb[q] += s;
+        }
+        atomicAdd(&p.out[0], loss);
+        for (int q = 0; q < kTorusParams; ++q) atomicAdd(&p.out[1 + q], pb[q]);
+        if (p.per_ray)
+            for (int q = 0; q < kTorusParams; ++q) p.per_ray[id * kTorusParams + q] = pb[q];
+    }
+    if (n_cut) atomicAdd(&p.out[1 + kTorusParams], (double)n_cut);
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+struct TorusBuffers {
+    void* ctl = nullptr;  // counters + stats + err flag + out
+    size_t ctl_cap = 0;
+    void* out = nullptr;  // spectrum, class, steps
+    size_t out_cap = 0;
+    void* nev = nullptr;  // n_events, ev_off, ck_off
+    size_t nev_cap = 0;
+    void* evh = nullptr;
+    size_t evh_cap = 0;
+    void* evk = nullptr;
+    size_t evk_cap = 0;
+    void* ck = nullptr;
+    size_t ck_cap = 0;
+    void* work = nullptr;
+    size_t work_cap = 0;
+    void* tgt = nullptr;
+    size_t tgt_cap = 0;
+};
+
+void torus_free(TorusBuffers* b) {
+    if (!b) return;
+    for (void* q : {b->ctl, b->out, b->nev, b->evh, b->evk, b->ck, b->work, b->tgt})
+        if (q) cudaFree(q);
+    delete b;
+}
+
+namespace {
+
+constexpr double kE = 4.80320425e-10;          // esu
+constexpr double kCcgs = 2.99792458e10;        // cm/s
+constexpr double kMe = 9.1093837015e-28;       // g
+constexpr double kHcgs = 6.62607015e-27;       // erg s
+constexpr double kMec2 = kMe * kCcgs * kCcgs;  // erg
+
+rtw_status torus_model(const rtw_scene& s, const double* colors_nm, int N, TorusModel& m, std::string& why) {
+    std::memset(&m, 0, sizeof(m));
+    if (N <= 0 || N > kTorusMaxBins || !colors_nm) {
+        why = "the torus takes 1..32 bins";
+        return RTW_ERR_INVALID_PARAM;
+    }
+    if (!(s.mass > 0) || !(std::fabs(s.spin) < s.mass) || !(s.r_in > 0) || !(s.r_out >= s.r_in) ||
+        !(s.edge_in > 0) || !(s.edge_out > 0) || !(s.n_e0 >= 0) || !(s.b_0 > 0) || !(s.theta_e0 > 0) ||
+        !(s.length_cm > 0) || !(s.rho_h > 0)) {
+        why = "torus parameters out of range";
+        return RTW_ERR_INVALID_PARAM;
+    }
+    rtw_scene g = s;
+    g.r_in = 1;  // the geodesic functor's thin disk stays empty
+    g.r_out = 0;
+    make_dev_scene(g, m.geo);
+    TorusDev& t = m.tor;
+    t.M = s.mass;
+    t.a = s.spin;
+    t.r_in = s.r_in;
+    t.r_out = s.r_out;
+    t.edge_in = s.edge_in;
+    t.edge_out = s.edge_out;
+    t.cut_in = std::max(s.r_in - 4 * s.edge_in, 1.01 * m.geo.r_ev);
+    t.cut_out = s.r_out + 4 * s.edge_out;
+    t.h_ratio = s.rho_h;
+    t.ne_idx = s.rho_index;
+    t.b_idx = s.b_index;
+    t.t_idx = s.t_index;
+    t.n0 = s.n_e0;
+    t.B0 = s.b_0;
+    t.Th0 = s.theta_e0;
+    t.cj_unit = std::sqrt(2.0) * kPi * kE * kE / (3 * kCcgs) * s.length_cm;
+    t.nuc_unit = kE / (2 * kPi * kMe * kCcgs);
+    for (int c = 0; c < N; ++c) {
+        const double lam = colors_nm[c];
+        if (!(lam > 0)) {
+            why = "colors_nm must be positive";
+            return RTW_ERR_INVALID_PARAM;
+        }
+        const double nu = kLightC * 1e9 / lam;  // Hz
+        m.bins[c].nu_hz = nu;
+        m.bins[c].inv_nu_nm3 = lam * lam * lam;
+        m.bins[c].b0 = 2 * kHcgs * nu * nu * nu / (kCcgs * kCcgs);
+        m.bins[c].hk = kHcgs * nu / kMec2;
+    }
+    m.n = N;
+    return RTW_OK;
+}
+
+// launch shape of the torus kernels: 128 threads, occupancy-limited CTAs
+template <class F>
+int torus_grid(rtw_ctx* ctx, F fn) {
+    int occ = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 128, 0);
+    return ctx->num_sms * std::max(1, occ);
+}
+
+struct TorusRun {
+    TorusKP kp;
+    int grid = 0;
+    long long P = 0;
+};
+
+// validation, model, frame, buffers and kernel parameters of a torus render
+rtw_status torus_setup(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* cam, const rtw_render_params* prm,
+                       TorusRun& run) {
+    if (!scene || !cam || !prm) return fail(ctx, RTW_ERR_INVALID_PARAM, "null argument");
+    if (prm->precision != RTW_PREC_FP64 && prm->precision != RTW_PREC_MIXED)
+        return fail(ctx, RTW_ERR_INVALID_PARAM, "precision");
+    if (prm->integrator != RTW_DP45_FSAL)
+        return fail(ctx, RTW_ERR_UNSUPPORTED, "the synchrotron torus runs the FSAL integrator only");
+    if (prm->ray_bundles) return fail(ctx, RTW_ERR_UNSUPPORTED, "ray bundles are not built");
+    if (!(prm->max_dt_scale > 0)) return fail(ctx, RTW_ERR_INVALID_PARAM, "max_dt_scale must be > 0");
+    std::string why;
+    TorusKP& p = run.kp;
+    std::memset(&p, 0, sizeof(p));
+    rtw_status st = torus_model(*scene, prm->colors_nm, prm->n_colors, p.m, why);
+    if (st != RTW_OK) return fail(ctx, st, why);
+    int64_t total = 0;
+    st = rtw_prepare_frames(scene, cam, 1, &p.frame, &total);
+    if (st == RTW_ERR_INVALID_CAMERA) return fail(ctx, st, "camera is on a coordinate singularity");
+    if (st != RTW_OK) return fail(ctx, st, "camera parameters invalid or non-finite");
+    run.P = total;
+    p.total_rays = total;
+    p.max_dt_scale = prm->max_dt_scale;
+    const double pdr = prm->promote_dr < 0 ? -1.0 : (prm->promote_dr > 0 ? prm->promote_dr : 1e-3);
+    const double psn = prm->promote_sin < 0 ? 0.0 : (prm->promote_sin > 0 ? std::min(prm->promote_sin, 1.0) : 1e-2);
+    p.promote_dr = pdr * scene->mass;
+    p.promote_theta = std::asin(psn);
+    p.ck_every = 16;
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, RTW_ERR_CUDA, "cudaSetDevice");
+    if (!ctx->torus) ctx->torus = new TorusBuffers();
+    TorusBuffers* b = ctx->torus;
+    // control block: counter, stats, err flag, out[6]
+    if ((st = ensure(ctx, &b->ctl, &b->ctl_cap, 1024)) != RTW_OK) return st;
+    unsigned long long* ctl = (unsigned long long*)b->ctl;
+    p.counter = ctl;
+    p.stats = (DevStats*)(ctl + 1);
+    p.err_flag = (unsigned int*)(ctl + 32);
+    run.grid = prm->precision == RTW_PREC_MIXED ? torus_grid(ctx, torus_forward<true>)
+                                                 : torus_grid(ctx, torus_forward<false>);
+    return RTW_OK;
+}
+
+cudaError_t launch_forward(const TorusKP& p, bool mixed, int grid, cudaStream_t st) {
+    void* args[] = {(void*)&p};
+    return cudaLaunchKernel(mixed ? (const void*)torus_forward<true> : (const void*)torus_forward<false>,
+                            dim3(grid), dim3(128), args, 0, st);
+}
+
+}  // namespace
+
+rtw_status torus_render(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* cams, int32_t n_cams,
+                        const rtw_render_params* prm, rtw_outputs* out) {
+    if (n_cams != 1) return fail(ctx, RTW_ERR_UNSUPPORTED, "the synchrotron torus renders one camera per call");
+    TorusRun run;
+    rtw_status st = torus_setup(ctx, scene, cams, prm, run);
+    if (st != RTW_OK) return st;
+    TorusKP& p = run.kp;
+    TorusBuffers* b = ctx->torus;
+    const int N = p.m.n;
+    const long long P = run.P;
+    cudaStream_t s = prm->stream ? (cudaStream_t)prm->stream : ctx->stream;
+    float* spec = out->spectrum;
+    uint8_t* cls = out->term_class;
+    uint32_t* steps = out->steps;
+    if (!out->on_device) {
+        const size_t need = (size_t)P * (sizeof(float) * N + 1 + 4) + 1024;
+        if ((st = ensure(ctx, &b->out, &b->out_cap, need)) != RTW_OK) return st;
+        char* base = (char*)b->out;
+        spec = out->spectrum ? (float*)base : nullptr;
+        steps = out->steps ? (uint32_t*)(base + (((size_t)P * N * 4 + 255) & ~(size_t)255)) : nullptr;
+        cls = out->term_class ? (uint8_t*)(base + (((size_t)P * N * 4 + 255) & ~(size_t)255) +
+                                           (((size_t)P * 4 + 255) & ~(size_t)255))
+                              : nullptr;
+    }
+    p.spectrum = spec;
+    p.cls = cls;
+    p.steps = steps;
+    // the context's counter and stats block, so that rtw_get_stats reads them
+    p.counter = ctx->d_ctl;
+    p.stats = (DevStats*)(ctx->d_ctl + 1);
+    RTW_CUDA(cudaEventRecord(ctx->ev[0], s), "event");
+    RTW_CUDA(cudaMemsetAsync(ctx->d_ctl, 0, sizeof(unsigned long long) + sizeof(DevStats), s), "reset counters");
+    RTW_CUDA(cudaEventRecord(ctx->ev[1], s), "event");
+    RTW_CUDA(launch_forward(p, prm->precision == RTW_PREC_MIXED, run.grid, s), "torus kernel launch");
+    RTW_CUDA(cudaEventRecord(ctx->ev[2], s), "event");
+    if (!out->on_device) {
+        if (out->spectrum)
+            RTW_CUDA(cudaMemcpyAsync(out->spectrum, spec, sizeof(float) * N * P, cudaMemcpyDeviceToHost, s), "D2H");
+        if (out->steps) RTW_CUDA(cudaMemcpyAsync(out->steps, steps, 4 * P, cudaMemcpyDeviceToHost, s), "D2H");
+        if (out->term_class) RTW_CUDA(cudaMemcpyAsync(out->term_class, cls, P, cudaMemcpyDeviceToHost, s), "D2H");
+    }
+    // xyz of a millimetre spectrum is zero: the CIE functions vanish there
+    if (out->xyz) {
+        if (out->on_device) RTW_CUDA(cudaMemsetAsync(out->xyz, 0, sizeof(float) * 3 * P, s), "xyz");
+        else std::memset(out->xyz, 0, sizeof(float) * 3 * P);
+    }
+    RTW_CUDA(cudaEventRecord(ctx->ev[3], s), "event");
+    ctx->have_last = true;
+    ctx->last_frames = 0;
+    ctx->last_grid = run.grid;
+    ctx->last_warps = 4;
+    ctx->last_refill = 1;
+    ctx->last_replayed = 0;
+    if (!prm->stream) RTW_CUDA(cudaStreamSynchronize(s), "torus kernel");
+    return RTW_OK;
+}
+
+}  // namespace rtw
+
+using namespace rtw;
+
+extern "C" {
+
+rtw_status rtw_adjoint(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* cam, const rtw_render_params* prm,
+                       const rtw_adjoint_params* adj, rtw_outputs* out, rtw_adjoint_result* res) {
+    if (!ctx) return RTW_ERR_INVALID_PARAM;
+    ctx->err.clear();
+    if (!scene || !cam || !prm || !adj || !res || !adj->target) return fail(ctx, RTW_ERR_INVALID_PARAM, "null argument");
+    if (scene->kind != RTW_SCENE_KERR_SYNCHRO_TORUS)
+        return fail(ctx, RTW_ERR_UNSUPPORTED, "the adjoint is built for the synchrotron torus");
+    TorusRun run;
+    rtw_status st = torus_setup(ctx, scene, cam, prm, run);
+    if (st != RTW_OK) return st;
+    TorusKP& p = run.kp;
+    TorusBuffers* b = ctx->torus;
+    const int N = p.m.n, D = 8 + 2 * N;
+    const long long P = run.P;
+    const int KC = adj->checkpoint_every > 0 ? std::min(adj->checkpoint_every, 64) : 16;
+    p.ck_every = KC;
+    const double dl = adj->camera_delta > 0 ? adj->camera_delta : 1e-6;
+    const bool mixed = prm->precision == RTW_PREC_MIXED;
+    cudaStream_t s = ctx->stream;
+    std::memset(res, 0, sizeof(*res));
+
+    // derivative of the camera transform in a and the inclination
+    TorusRP rp;
+    std::memset(&rp, 0, sizeof(rp));
+    for (int q = 0; q < 2; ++q) {
+        rtw_scene sp = *scene, sm = *scene;
+        rtw_camera cp = *cam, cm = *cam;
+        if (q == 0) {
+            sp.spin += dl;
+            sm.spin -= dl;
+        } else {
+            cp.position[2] += dl;
+            cm.position[2] -= dl;
+        }
+        FrameDesc fp, fm;
+        int64_t tp = 0, tm = 0;
+        if (rtw_prepare_frames(&sp, &cp, 1, &fp, &tp) != RTW_OK || rtw_prepare_frames(&sm, &cm, 1, &fm, &tm) != RTW_OK)
+            return fail(ctx, RTW_ERR_INVALID_PARAM, "camera transform not differentiable here");
+        FrameDesc d = p.frame;
+        for (int i = 0; i < 4; ++i) d.pos[i] = (fp.pos[i] - fm.pos[i]) / (2 * dl);
+        for (int i = 0; i < 16; ++i) d.M[i] = (fp.M[i] - fm.M[i]) / (2 * dl);
+        rp.dframe[q] = d;
+    }
+
+    // buffers: outputs, event counts and offsets
+    const size_t spec_b = ((size_t)P * N * 4 + 255) & ~(size_t)255;
+    if ((st = ensure(ctx, &b->out, &b->out_cap, spec_b + 2 * (((size_t)P * 4 + 255) & ~(size_t)255))) != RTW_OK)
+        return st;
+    float* spec = (float*)b->out;
+    uint32_t* steps = (uint32_t*)((char*)b->out + spec_b);
+    uint8_t* cls = (uint8_t*)((char*)b->out + spec_b + (((size_t)P * 4 + 255) & ~(size_t)255));
+    const size_t nev_b = ((size_t)P * 4 + 255) & ~(size_t)255;
+    if ((st = ensure(ctx, &b->nev, &b->nev_cap, nev_b + 2 * (size_t)P * 8)) != RTW_OK) return st;
+    uint32_t* nev = (uint32_t*)b->nev;
+    unsigned long long* ev_off = (unsigned long long*)((char*)b->nev + nev_b);
+    unsigned long long* ck_off = ev_off + P;
+    if ((st = ensure(ctx, &b->tgt, &b->tgt_cap, (size_t)P * N * 4)) != RTW_OK) return st;
+    if (adj->target_on_device)
+        RTW_CUDA(cudaMemcpyAsync(b->tgt, adj->target, (size_t)P * N * 4, cudaMemcpyDeviceToDevice, s), "target");
+    else
+        RTW_CUDA(cudaMemcpyAsync(b->tgt, adj->target, (size_t)P * N * 4, cudaMemcpyHostToDevice, s), "target H2D");
+    p.spectrum = spec;
+    p.cls = cls;
+    p.steps = steps;
+    p.n_events = nev;
+
+    cudaEvent_t ev[6];
+    for (auto& e : ev) RTW_CUDA(cudaEventCreate(&e), "event");
+    struct EvGuard {
+        cudaEvent_t* e;
+        ~EvGuard() {
+            for (int i = 0; i < 6; ++i) cudaEventDestroy(e[i]);
+        }
+    } guard{ev};
+
+    // 1. forward: image, step counts, recorded-step counts
+    RTW_CUDA(cudaEventRecord(ev[0], s), "event");
+    RTW_CUDA(cudaMemsetAsync(b->ctl, 0, 1024, s), "reset counters");
+    p.record = 0;
+    RTW_CUDA(launch_forward(p, mixed, run.grid, s), "torus forward");
+    RTW_CUDA(cudaEventRecord(ev[1], s), "event");
+    // offsets (host scan of the counts)
+    std::vector<uint32_t> h_nev(P);
+    RTW_CUDA(cudaMemcpyAsync(h_nev.data(), nev, 4 * P, cudaMemcpyDeviceToHost, s), "counts D2H");
+    RTW_CUDA(cudaStreamSynchronize(s), "forward");
+    std::vector<unsigned long long> h_off(2 * P);
+    unsigned long long E = 0, C = 0;
+    for (long long i = 0; i < P; ++i) {
+        h_off[i] = E;
+        h_off[P + i] = C;
+        const uint32_t n = h_nev[i] & kEventCount;
+        const uint32_t kc = (h_nev[i] & kDenseCheckpoints) ? 1u : (uint32_t)KC;
+        E += n;
+        C += (n + kc - 1) / kc;
+    }
+    RTW_CUDA(cudaMemcpyAsync(ev_off, h_off.data(), 16 * P, cudaMemcpyHostToDevice, s), "offsets H2D");
+    if ((st = ensure(ctx, &b->evh, &b->evh_cap, std::max<size_t>(8 * E, 256))) != RTW_OK) return st;
+    if ((st = ensure(ctx, &b->evk, &b->evk_cap, std::max<size_t>(E, 256))) != RTW_OK) return st;
+    if ((st = ensure(ctx, &b->ck, &b->ck_cap, std::max<size_t>(8 * C * (size_t)D, 256))) != RTW_OK) return st;
+    // 2. record pass
+    p.record = 1;
+    p.ev_off = ev_off;
+    p.ck_off = ck_off;
+    p.ev_h = (double*)b->evh;
+    p.ev_kind = (uint8_t*)b->evk;
+    p.ck = (double*)b->ck;
+    p.spectrum = nullptr;  // the forward pass's image stays
+    p.cls = nullptr;
+    p.steps = nullptr;
+    RTW_CUDA(cudaEventRecord(ev[2], s), "event");
+    RTW_CUDA(cudaMemsetAsync(b->ctl, 0, 8, s), "reset queue");
+    RTW_CUDA(launch_forward(p, mixed, run.grid, s), "torus record");
+    RTW_CUDA(cudaEventRecord(ev[3], s), "event");
+    // 3. reverse pass
+    int occ = 0;
+    RTW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, torus_reverse, 128, 0), "occupancy");
+    const int rgrid = ctx->num_sms * std::max(1, occ);
+    const long long stride = (long long)(KC + 1 + 6 + 6 + 6 + 4 + 3) * D;
+    const size_t work_b = (size_t)rgrid * 128 * stride * 8;
+    const size_t per_ray_b = adj->per_ray_grad ? (size_t)P * kTorusParams * 8 : 0;
+    if ((st = ensure(ctx, &b->work, &b->work_cap, work_b + per_ray_b)) != RTW_OK) return st;
+    rp.f = p;
+    rp.f.spectrum = spec;
+    rp.target = (const float*)b->tgt;
+    rp.spectrum = spec;
+    rp.work = (double*)b->work;
+    rp.work_stride = stride;
+    rp.per_ray = adj->per_ray_grad ? (double*)((char*)b->work + work_b) : nullptr;
+    rp.skip_escape_rays = adj->escape_rays == 1;
+    unsigned long long* ctl = (unsigned long long*)b->ctl;
+    rp.out = (double*)(ctl + 40);
+    rp.counter = ctl + 39;
+    RTW_CUDA(cudaEventRecord(ev[4], s), "event");
+    {
+        void* args[] = {(void*)&rp};
+        RTW_CUDA(cudaLaunchKernel((const void*)torus_reverse, dim3(rgrid), dim3(128), args, 0, s), "torus reverse");
+    }
+    RTW_CUDA(cudaEventRecord(ev[5], s), "event");
+    double h_out[3 + kTorusParams];
+    unsigned int flag = 0;
+    RTW_CUDA(cudaMemcpyAsync(h_out, rp.out, sizeof(h_out), cudaMemcpyDeviceToHost, s), "result D2H");
+    RTW_CUDA(cudaMemcpyAsync(&flag, p.err_flag, 4, cudaMemcpyDeviceToHost, s), "flag D2H");
+    if (rp.per_ray)
+        RTW_CUDA(cudaMemcpyAsync(adj->per_ray_grad, rp.per_ray, per_ray_b, cudaMemcpyDeviceToHost, s), "per-ray D2H");
+    if (out) {
+        if (out->on_device) {
+            if (out->spectrum) RTW_CUDA(cudaMemcpyAsync(out->spectrum, spec, 4 * N * P, cudaMemcpyDeviceToDevice, s), "D2D");
+            if (out->steps) RTW_CUDA(cudaMemcpyAsync(out->steps, steps, 4 * P, cudaMemcpyDeviceToDevice, s), "D2D");
+            if (out->term_class) RTW_CUDA(cudaMemcpyAsync(out->term_class, cls, P, cudaMemcpyDeviceToDevice, s), "D2D");
+        } else {
+            if (out->spectrum) RTW_CUDA(cudaMemcpyAsync(out->spectrum, spec, 4 * N * P, cudaMemcpyDeviceToHost, s), "D2H");
+            if (out->steps) RTW_CUDA(cudaMemcpyAsync(out->steps, steps, 4 * P, cudaMemcpyDeviceToHost, s), "D2H");
+            if (out->term_class) RTW_CUDA(cudaMemcpyAsync(out->term_class, cls, P, cudaMemcpyDeviceToHost, s), "D2H");
+        }
+    }
+    RTW_CUDA(cudaStreamSynchronize(s), "adjoint");
+    if (flag) return fail(ctx, RTW_ERR_CUDA, "record pass diverged from the forward pass");
+    float t01 = 0, t23 = 0, t45 = 0, t05 = 0;
+    cudaEventElapsedTime(&t01, ev[0], ev[1]);
+    cudaEventElapsedTime(&t23, ev[2], ev[3]);
+    cudaEventElapsedTime(&t45, ev[4], ev[5]);
+    cudaEventElapsedTime(&t05, ev[0], ev[5]);
+    res->loss = h_out[0];
+    for (int q = 0; q < kTorusParams; ++q) res->grad[q] = h_out[1 + q];
+    res->forward_ms = t01;
+    res->record_ms = t23;
+    res->reverse_ms = t45;
+    res->total_ms = t05;
+    res->events = E;
+    res->checkpoints = C;
+    res->escape_cuts = (uint64_t)h_out[1 + kTorusParams];
+    res->escape_rays = (uint64_t)h_out[2 + kTorusParams];
+    res->scratch_bytes = 8 * E + E + 8 * C * (size_t)D + work_b + nev_b + 16 * P;
+    ctx->have_last = false;
+    return RTW_OK;
+}
+
+rtw_status rtw_torus_rhs(const rtw_scene* scene, const double* colors_nm, int32_t n_colors, int32_t form,
+                         const double* state, double* slope) {
+    if (!scene || !state || !slope || scene->kind != RTW_SCENE_KERR_SYNCHRO_TORUS) return RTW_ERR_INVALID_PARAM;
+    TorusModel m;
+    std::string why;
+    if (torus_model(*scene, colors_nm, n_colors, m, why) != RTW_OK) return RTW_ERR_INVALID_PARAM;
+    const int N = n_colors, D = 8 + 2 * N;
+    std::vector<double> y(D), f(D);
+    for (int i = 0; i < 8; ++i) y[i] = state[i];
+    for (int c = 0; c < N; ++c) {
+        y[8 + N + c] = state[8 + 2 * c];  // I
+        y[8 + c] = state[9 + 2 * c];      // tau
+    }
+    torus_f64(m, y.data(), f.data());
+    if (form == 1) {
+        double acc[4];
+        const double k[4] = {y[4], y[5], y[6], y[7]};
+        kerr_accel<double>(m.tor.M, m.tor.a, y[1], y[2], k, acc);
+        for (int i = 0; i < 4; ++i) f[4 + i] = acc[i];
+    }
+    for (int i = 0; i < 8; ++i) slope[i] = f[i];
+    for (int c = 0; c < N; ++c) {
+        slope[8 + 2 * c] = f[8 + N + c];
+        slope[9 + 2 * c] = f[8 + c];
+    }
+    return RTW_OK;
+}
+
+rtw_status rtw_torus_escape_vjp(const rtw_scene* scene, const double* colors_nm, int32_t n_colors,
+                                const double* state, int32_t n_sub, const double* cot, double* end_state,
+                                double* mu, double* pbar) {
+    if (!scene || !state || !cot || !mu || !pbar || !end_state || n_sub < 1 || n_sub > 37 ||
+        scene->kind != RTW_SCENE_KERR_SYNCHRO_TORUS)
+        return RTW_ERR_INVALID_PARAM;
+    TorusModel m;
+    std::string why;
+    if (torus_model(*scene, colors_nm, n_colors, m, why) != RTW_OK) return RTW_ERR_INVALID_PARAM;
+    const int N = n_colors, D = 8 + 2 * N;
+    std::vector<double> y(D), lam(D), W(4 * D), mu_(D), tmp(D), e(D);
+    for (int i = 0; i < 8; ++i) {
+        y[i] = state[i];
+        lam[i] = cot[i];
+    }
+    for (int c = 0; c < N; ++c) {
+        y[8 + N + c] = state[8 + 2 * c];
+        y[8 + c] = state[9 + 2 * c];
+        lam[8 + N + c] = cot[8 + 2 * c];
+        lam[8 + c] = cot[9 + 2 * c];
+    }
+    torus_escape_end(m, y.data(), n_sub, e.data(), tmp.data());
+    double pb[kTorusParams] = {0, 0, 0, 0, 0};
+    const bool ok = torus_escape_vjp(m, y.data(), n_sub, torus_escape_temp(y.data()), lam.data(), pb, W.data(),
+                                     mu_.data(), tmp.data());
+    for (int i = 0; i < 8; ++i) {
+        mu[i] = lam[i];
+        end_state[i] = e[i];
+    }
+    for (int c = 0; c < N; ++c) {
+        mu[8 + 2 * c] = lam[8 + N + c];
+        mu[9 + 2 * c] = lam[8 + c];
+        end_state[8 + 2 * c] = e[8 + N + c];
+        end_state[9 + 2 * c] = e[8 + c];
+    }
+    for (int q = 0; q < kTorusParams; ++q) pbar[q] = pb[q];
+    return ok ? RTW_OK : RTW_ERR_NAN;
+}
+
+rtw_status rtw_torus_vjp(const rtw_scene* scene, const double* colors_nm, int32_t n_colors, const double* state,
+                         const double* cot, double* mu, double* pbar) {
+    if (!scene || !state || !cot || !mu || !pbar || scene->kind != RTW_SCENE_KERR_SYNCHRO_TORUS)
+        return RTW_ERR_INVALID_PARAM;
+    TorusModel m;
+    std::string why;
+    if (torus_model(*scene, colors_nm, n_colors, m, why) != RTW_OK) return RTW_ERR_INVALID_PARAM;
+    const int N = n_colors, D = 8 + 2 * N;
+    std::vector<double> y(D), k(D), u(D, 0.0);
+    for (int i = 0; i < 8; ++i) {
+        y[i] = state[i];
+        k[i] = cot[i];
+    }
+    for (int c = 0; c < N; ++c) {
+        y[8 + N + c] = state[8 + 2 * c];
+        y[8 + c] = state[9 + 2 * c];
+        k[8 + N + c] = cot[8 + 2 * c];
+        k[8 + c] = cot[9 + 2 * c];
+    }
+    double pb[kTorusParams] = {0, 0, 0, 0, 0};
+    torus_vjp(m, y.data(), k.data(), u.data(), pb);
+    for (int i = 0; i < 8; ++i) mu[i] = u[i];
+    for (int c = 0; c < N; ++c) {
+        mu[8 + 2 * c] = u[8 + N + c];
+        mu[9 + 2 * c] = u[8 + c];
+    }
+    for (int q = 0; q < kTorusParams; ++q) pbar[q] = pb[q];
+    return RTW_OK;
+}
+
+}  // extern "C"

@@ -137,6 +137,52 @@ class Renderer:
         d["phase_cycles"] = list(s.phase_cycles)
         return d
 
+    def adjoint(self, scene: abi.Scene, cam: abi.Camera, colors_nm, target, *, precision=abi.PREC_MIXED,
+                checkpoint_every: int = 16, camera_delta: float = 0.0, want=("spectrum",), per_ray: bool = False,
+                exclude_escape_rays: bool = False, **kw) -> dict:
+        """Loss sum (I - target)^2 of a synchrotron-torus render and its gradient
+        in (spin, inclination, n_e0, b_0, theta_e0) through rtw_adjoint.
+        target: [P, n_colors] float32 (host array or a CUDA tensor)."""
+        cam.y_pix = abi.y_pixels(cam.x_pix, cam.fov_hor, cam.fov_vert)
+        P = cam.x_pix * cam.y_pix
+        n = len(np.atleast_1d(colors_nm))
+        ap = abi.AdjointParams()
+        on_dev = hasattr(target, "data_ptr")
+        if on_dev:
+            ap.target = target.data_ptr()
+            ap.target_on_device = 1
+        else:
+            tgt = np.ascontiguousarray(target, dtype=np.float32).reshape(P, n)
+            ap.target = tgt.ctypes.data
+            ap.target_on_device = 0
+        ap.checkpoint_every = int(checkpoint_every)
+        ap.camera_delta = float(camera_delta)
+        ap.escape_rays = int(bool(exclude_escape_rays))
+        res = {}
+        if per_ray:
+            res["per_ray_grad"] = np.zeros((P, 5))
+            ap.per_ray_grad = res["per_ray_grad"].ctypes.data
+        out = abi.Outputs()
+        if "spectrum" in want:
+            res["spectrum"] = np.zeros((P, n), np.float32)
+            out.spectrum = res["spectrum"].ctypes.data
+        if "class" in want:
+            res["class"] = np.zeros(P, np.uint8)
+            out.term_class = res["class"].ctypes.data
+        if "steps" in want:
+            res["steps"] = np.zeros(P, np.uint32)
+            out.steps = res["steps"].ctypes.data
+        out.on_device = 0
+        kw.setdefault("integrator", abi.DP45_FSAL)
+        prm = self.params(colors_nm, precision=precision, **kw)
+        r = abi.AdjointResult()
+        st = self._lib.rtw_adjoint(self._ctx, C.byref(scene), C.byref(cam), C.byref(prm), C.byref(ap), C.byref(out),
+                                   C.byref(r))
+        abi.check(st, self.last_error())
+        res.update({f: getattr(r, f) for f, _ in abi.AdjointResult._fields_ if f != "grad"})
+        res["grad"] = np.array(list(r.grad))
+        return res
+
     def frame_times(self, n_frames: int) -> dict:
         """Per-frame times of the last render (ms, device global timer):
         'done' = batch start to the frame's last ray, 'span' = the frame's

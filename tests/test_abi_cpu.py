@@ -32,12 +32,13 @@ def test_every_declared_symbol_is_exported(rtwlib):
 
 
 def test_abi_version(rtwlib):
-    assert rtwlib.rtw_abi_version() == abi.ABI_VERSION == 2
+    assert rtwlib.rtw_abi_version() == abi.ABI_VERSION == 3
 
 
 STRUCTS = {
     "rtw_scene": abi.Scene, "rtw_camera": abi.Camera, "rtw_render_params": abi.RenderParams,
     "rtw_outputs": abi.Outputs, "rtw_stats": abi.Stats, "rtw_op_counts": abi.OpCounts,
+    "rtw_adjoint_params": abi.AdjointParams, "rtw_adjoint_result": abi.AdjointResult,
 }
 
 

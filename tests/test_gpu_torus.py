@@ -1,0 +1,154 @@
+"""The synchrotron torus on the GPU: forward parity against the FP64 oracle
+and the discrete adjoint's gradient against central differences of the
+oracle's loss.
+
+Near-axis rays. Rays that pass within ~1e-5 rad of the polar axis take the
+reference's polar escape (37 Euler sub-steps across the pole,
+Kerr.source/source_geometry.jl:249-269). For some of them the discrete loss is
+not smooth at finite-difference scales: the oracle's own central differences
+change sign and size as the step goes from 1e-3 to 1e-6. The gradient test
+therefore compares per-ray gradients on the pixels whose oracle differences
+agree at two step sizes, and it checks that the excluded pixels are few.
+"""
+import numpy as np
+import pytest
+
+from rtwca_b200 import abi, configs
+
+pytestmark = pytest.mark.gpu
+
+NAMES = ("spin", "inclination_deg", "n_e0", "b_0", "theta_e0")
+
+
+def _problem(xp, tol, params=None, nb=8):
+    sc, cam, col = configs.torus_problem(x_pix=xp, tol=tol, params=params)
+    return sc, cam, col[:: 32 // nb]
+
+
+def _spec_err(g, ref):
+    den = np.maximum(np.abs(ref), 1e-6 * np.abs(ref).max())
+    return np.abs(g.astype(np.float64) - ref) / den
+
+
+def test_torus_fp64_parity(renderer, oracle):
+    sc, cam, col = _problem(16, 1e-8)
+    ref = oracle.render(sc, cam, col, integrator=abi.DP45_FSAL)
+    g = renderer.render(sc, [cam], col, want=("xyz", "class", "steps", "spectrum"), precision=abi.PREC_FP64,
+                        integrator=abi.DP45_FSAL)
+    assert np.mean(g["class"] == ref["class"]) >= 0.999
+    err = _spec_err(g["spectrum"], ref["spectrum"])
+    assert np.mean(err <= 1e-3) >= 0.999, np.quantile(err, 0.99)
+    assert abs(g["steps"].sum() / ref["steps"].sum() - 1) < 0.01
+    assert np.all(g["xyz"] == 0)  # the CIE functions vanish at 1.3 mm
+    st = renderer.stats()
+    assert st["rays"] == 256 and st["step_attempts"] > 0
+
+
+def test_torus_mixed_parity(renderer, oracle):
+    """FP32 stages with FP64 state, Kahan intensities and FP64 stages near the
+    horizon and the poles, at the benchmark tolerance 1e-6. Bars: class >= 98 %,
+    spectra within 1e-3 on >= 97 % of pixel-bins (FP32 stages of the FSAL
+    method are ill-conditioned for rays grazing the axis, as on the thin disk)."""
+    sc, cam, col = _problem(16, 1e-6)
+    ref = oracle.render(sc, cam, col, integrator=abi.DP45_FSAL)
+    g = renderer.render(sc, [cam], col, want=("class", "spectrum"), precision=abi.PREC_MIXED,
+                        integrator=abi.DP45_FSAL)
+    cls = np.mean(g["class"] == ref["class"])
+    err = _spec_err(g["spectrum"], ref["spectrum"])
+    print("mixed torus parity: class", cls, "within 1e-3", np.mean(err <= 1e-3), "p99", np.quantile(err, 0.99))
+    assert cls >= 0.98
+    assert np.mean(err <= 1e-3) >= 0.97
+
+
+def test_torus_rejects(renderer):
+    sc, cam, col = _problem(8, 1e-6)
+    with pytest.raises(abi.RTWError):  # the reference step is not built for the torus
+        renderer.render(sc, [cam], col, precision=abi.PREC_MIXED, integrator=abi.DP45_REF_COMPAT)
+    with pytest.raises(abi.RTWError):  # one camera per call
+        renderer.render(sc, [cam, cam], col, precision=abi.PREC_MIXED, integrator=abi.DP45_FSAL)
+    with pytest.raises(abi.RTWError):  # at most 32 bins
+        renderer.render(sc, [cam], configs.log_spaced_colors(64), precision=abi.PREC_MIXED,
+                        integrator=abi.DP45_FSAL)
+
+
+@pytest.fixture(scope="module")
+def fd_problem(oracle):
+    """8x8 pixels, 4 bins, tolerance 1e-8: the oracle's target (parameters
+    perturbed with numpy default_rng(1)), its per-pixel central differences
+    at relative steps 1e-4 and 1e-5, and the pixels where both agree."""
+    xp, tol, nb = 8, 1e-8, 4
+    sct, camt, col = _problem(xp, tol, configs.torus_target_params(1), nb)
+    target = oracle.render(sct, camt, col, integrator=abi.DP45_FSAL)["spectrum"].astype(np.float32)
+    base = dict(configs.TORUS_DEFAULTS)
+
+    def px_loss(params):
+        s, c, cl = _problem(xp, tol, params, nb)
+        sp = oracle.render(s, c, cl, integrator=abi.DP45_FSAL)["spectrum"]
+        return np.sum((sp - target.astype(np.float64)) ** 2, axis=1)
+
+    fds = []
+    for rel in (1e-4, 1e-5):
+        fd = np.zeros((xp * xp, 5))
+        for q, k in enumerate(NAMES):
+            h = rel * base[k]
+            pp, pm = dict(base), dict(base)
+            pp[k] += h
+            pm[k] -= h
+            fd[:, q] = (px_loss(pp) - px_loss(pm)) / (2 * h) * (180 / np.pi if k == "inclination_deg" else 1)
+        fds.append(fd)
+    stable = np.all(np.abs(fds[0] - fds[1]) <= 1e-3 * np.abs(fds[0]) + 1e-30, axis=1)
+    sc, cam, col = _problem(xp, tol, None, nb)
+    # rays that take a polar escape (oracle counters, one pixel at a time)
+    esc = np.array([oracle.render(sc, cam, col, integrator=abi.DP45_FSAL, pixel_ids=[q])["counters"][2] > 0
+                    for q in range(xp * xp)])
+    return sc, cam, col, target, fds[0], stable, esc
+
+
+def test_adjoint_matches_oracle_differences(renderer, fd_problem):
+    sc, cam, col, target, fd, stable, esc = fd_problem
+    a = renderer.adjoint(sc, cam, col, target, precision=abi.PREC_FP64, per_ray=True)
+    g = a["per_ray_grad"]
+    print("stable pixels", int(stable.sum()), "of", stable.size, "escape cuts", a["escape_cuts"])
+    assert stable.sum() >= 0.9 * stable.size
+    rel = np.abs(g[stable] - fd[stable]) / (np.abs(fd[stable]) + 1e-30)
+    assert np.quantile(rel, 0.99) < 1e-3, np.max(rel, axis=0)
+    # the summed gradient over those pixels, per parameter
+    gs, fs = g[stable].sum(0), fd[stable].sum(0)
+    assert np.all(np.abs(gs - fs) <= 1e-3 * np.abs(fs)), (gs, fs)
+    assert np.all(np.isfinite(a["grad"]))
+    assert np.allclose(a["grad"], g.sum(0), rtol=1e-9)
+
+
+def test_adjoint_loss_and_checkpoint_interval(renderer, fd_problem):
+    sc, cam, col, target, fd, stable, esc = fd_problem
+    img = renderer.render(sc, [cam], col, want=("spectrum",), precision=abi.PREC_FP64, integrator=abi.DP45_FSAL)
+    loss = float(np.sum((img["spectrum"].astype(np.float64) - target.astype(np.float64)) ** 2))
+    runs = [renderer.adjoint(sc, cam, col, target, precision=abi.PREC_FP64, checkpoint_every=k) for k in (4, 16, 64)]
+    for a in runs:
+        assert a["loss"] == pytest.approx(loss, rel=1e-12)
+        assert a["events"] > 0 and a["checkpoints"] > 0
+        # restarting the replay from other checkpoints changes only rounding
+        assert np.allclose(a["grad"], runs[0]["grad"], rtol=1e-9, atol=0)
+    assert runs[0]["checkpoints"] > runs[1]["checkpoints"] > runs[2]["checkpoints"]
+
+
+def test_adjoint_mixed_close_to_fp64(renderer, fd_problem):
+    """The FP32-mixed forward records a slightly different trajectory; on the
+    rays that take no polar escape its gradient stays within 2 % of the FP64
+    one. (Rays grazing the axis approach it through a different sequence of
+    capped steps in FP32 stages; their share is reported, not bounded.)"""
+    sc, cam, col, target, fd, stable, esc = fd_problem
+    a64 = renderer.adjoint(sc, cam, col, target, precision=abi.PREC_FP64, per_ray=True)
+    a32 = renderer.adjoint(sc, cam, col, target, precision=abi.PREC_MIXED, per_ray=True)
+    ok = ~esc
+    g64, g32 = a64["per_ray_grad"][ok].sum(0), a32["per_ray_grad"][ok].sum(0)
+    e64, e32 = a64["per_ray_grad"][esc].sum(0), a32["per_ray_grad"][esc].sum(0)
+    print("escape rays", int(esc.sum()), "mixed / fp64 gradient: others", g32 / g64, "escape rays", e32 / e64)
+    assert ok.sum() >= 0.8 * ok.size
+    assert np.all(np.abs(g32 - g64) <= 2e-2 * np.abs(g64))
+    # leaving the escape rays out: the same rays, the loss unchanged
+    b32 = renderer.adjoint(sc, cam, col, target, precision=abi.PREC_MIXED, per_ray=True, exclude_escape_rays=True)
+    assert b32["escape_rays"] == a32["escape_rays"] == int(esc.sum())
+    assert b32["loss"] == pytest.approx(a32["loss"], rel=1e-12)
+    assert np.all(b32["per_ray_grad"][esc] == 0)
+    assert np.allclose(b32["grad"], g32, rtol=1e-9)

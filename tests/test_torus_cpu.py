@@ -1,0 +1,103 @@
+"""The synchrotron torus on the CPU: the library's host evaluation of the
+torus right-hand side (the same generic-scalar functions the kernels run)
+against the oracle's independent FP64 restatement, the adjoint's generic
+geodesic acceleration against the scene functor, and the vector-Jacobian
+product against central differences of the right-hand side.
+"""
+import numpy as np
+import pytest
+
+from rtwca_b200 import abi, configs
+
+NB = 8
+
+
+def _problem():
+    sc, cam, col = configs.torus_problem(x_pix=16)
+    return sc, col[:: 32 // NB]
+
+
+def _state(sc, N, r, th, rng):
+    """A null ray at (r, theta) with random spatial direction, random tau and I."""
+    a, M = sc.spin, sc.mass
+    Sig = r * r + a * a * np.cos(th) ** 2
+    Del = r * r - 2 * M * r + a * a
+    s2 = np.sin(th) ** 2
+    gtt, gtp = -(1 - 2 * M * r / Sig), -2 * M * a * r * s2 / Sig
+    gpp = (r * r + a * a + 2 * M * a * a * r * s2 / Sig) * s2
+    kr, kth, kph = rng.normal(size=3) * np.array([1.0, 0.1, 0.05])
+    A, B = gtt, 2 * gtp * kph
+    C = gpp * kph ** 2 + Sig / Del * kr ** 2 + Sig * kth ** 2
+    kt = (-B - np.sqrt(B * B - 4 * A * C)) / (2 * A)
+    y = np.zeros(8 + 2 * N)
+    y[:8] = [0.0, r, th, 0.3, kt, kr, kth, kph]
+    y[9::2] = rng.uniform(0, 2, N)      # tau_c
+    y[8::2] = rng.uniform(0, 1e14, N)   # I_c
+    return y
+
+
+POINTS = [(4.3, 1.57), (5.0, 1.4), (6.5, 1.5), (8.0, 1.2), (12.0, 1.7), (20.0, 1.0), (45.0, 1.5)]
+
+
+def test_scene_defaults():
+    s = abi.scene_default(abi.SCENE_KERR_SYNCHRO_TORUS)
+    assert s.kind == abi.SCENE_KERR_SYNCHRO_TORUS
+    assert (s.spin, s.r_in, s.n_e0, s.b_0, s.theta_e0) == (0.94, 6.0, 1e5, 10.0, 10.0)
+    assert s.length_cm == pytest.approx(9.62e14)
+
+
+def test_colors_and_target_params():
+    c = configs.torus_colors()
+    f = 299792458.0 * 1e9 / c
+    assert c.size == 32 and np.all(np.diff(c) > 0)
+    assert f.max() == pytest.approx(276e9) and f.min() == pytest.approx(184e9)
+    t1, t2 = configs.torus_target_params(1), configs.torus_target_params(1)
+    assert t1 == t2 and set(t1) == set(configs.TORUS_DEFAULTS)
+    for k, v in t1.items():
+        assert abs(v / configs.TORUS_DEFAULTS[k] - 1) < 0.25
+
+
+def test_rhs_matches_oracle(oracle):
+    sc, col = _problem()
+    rng = np.random.default_rng(3)
+    for r, th in POINTS:
+        y = _state(sc, NB, r, th, rng)
+        ref = oracle.rhs(sc, col, y)
+        scale = 1e-12 * np.abs(ref).max()
+        for form in (0, 1):
+            f = abi.torus_rhs(sc, col, y, form)
+            err = np.abs(f - ref) / np.maximum(np.abs(ref), scale)
+            assert err.max() < 1e-11, (r, th, form, err.max())
+
+
+def test_vjp_matches_central_differences():
+    sc, col = _problem()
+    rng = np.random.default_rng(5)
+    names = {0: "spin", 2: "n_e0", 3: "b_0", 4: "theta_e0"}
+
+    def rhs(y, **kw):
+        s = configs.torus_scene(**{k: kw.get(k, getattr(sc, k)) for k in ("spin", "n_e0", "b_0", "theta_e0")})
+        return abi.torus_rhs(s, col, y, 0)
+
+    for r, th in [(5.0, 1.4), (6.5, 1.5), (8.0, 1.2), (12.0, 1.7)]:
+        y = _state(sc, NB, r, th, rng)
+        f0 = rhs(y)
+        cot = rng.normal(size=y.size) / np.maximum(np.abs(f0), 1e-30)
+        mu, pb = abi.torus_vjp(sc, col, y, cot)
+        for i in range(y.size):
+            if i in (0, 3):  # t and phi enter no slope
+                assert mu[i] == 0
+                continue
+            h = 1e-6 * max(abs(y[i]), 1e-3)
+            yp, ym = y.copy(), y.copy()
+            yp[i] += h
+            ym[i] -= h
+            fd = (cot @ rhs(yp) - cot @ rhs(ym)) / (2 * h)
+            floor = 1e-6 * np.sum(np.abs(cot * f0)) / max(abs(y[i]), 1e-3)
+            assert abs(fd - mu[i]) <= 1e-5 * abs(fd) + floor, (r, th, i, fd, mu[i])
+        for q, name in names.items():
+            base = getattr(sc, name)
+            h = 1e-6 * base
+            fd = (cot @ rhs(y, **{name: base + h}) - cot @ rhs(y, **{name: base - h})) / (2 * h)
+            assert abs(fd - pb[q]) <= 1e-5 * abs(fd), (r, th, name, fd, pb[q])
+        assert pb[1] == 0  # the inclination enters only the initial data
