@@ -204,6 +204,11 @@ def op_model(renderer, scene_kind, stats, n_bins):
     return flops, mufu, oc
 
 
+# DRAM bytes per step attempt of the FP32-mixed Kerr trace kernel (local-memory
+# spill traffic; the outputs are 17 B per ray), from one ncu capture at 512^2
+TRAFFIC_B_PER_ATTEMPT = 3.2103e9 / 357226998
+
+
 def batched_leg(r, world, rank, stream, barrier_fn):
     """96 Kerr frames (r ~ U[5, 40] M, inclination ~ U[10, 85] deg, numpy
     default_rng(0); 32 frames each at 256^2, 512^2, 1024^2; tolerance 1e-6 /
@@ -474,7 +479,12 @@ def run_b200(args):
             "adjoint": adjoint,
             "integrator": "reference step (k1 = previous sum b_i k_i)",
             "roofline": {"bound": "fp32" if prec == abi.PREC_MIXED else "fp64", "achieved": achieved, "peak": peak,
-                         "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                         "unit": "TFLOP/s", "frac": achieved / peak,
+                         "traffic": (st["step_attempts"] * TRAFFIC_B_PER_ATTEMPT
+                                     if prec == abi.PREC_MIXED and args.workload == "kerr_thin_disk" else None),
+                         "traffic_source": "ncu dram__bytes_read+write of the 512^2 capture "
+                                           "(profiles/trace_kernel_kerr_thin_disk_512.md), 3.21 GB over 357.2 M "
+                                           "step attempts, scaled by this launch's attempts",
                          "peak_source": "measured in-run FMA microbenchmark (rtw_measure_peaks)",
                          "mufu_gops": mufu / (kms * 1e-3) / 1e9,
                          "mufu_peak_gops": peaks["mufu_ops"] / 1e9},
