@@ -482,9 +482,8 @@ def run_b200(args):
                          "unit": "TFLOP/s", "frac": achieved / peak,
                          "traffic": (st["step_attempts"] * TRAFFIC_B_PER_ATTEMPT
                                      if prec == abi.PREC_MIXED and args.workload == "kerr_thin_disk" else None),
-                         "traffic_source": "ncu dram__bytes_read+write of the 512^2 capture "
-                                           "(profiles/trace_kernel_kerr_thin_disk_512.md), 3.21 GB over 357.2 M "
-                                           "step attempts, scaled by this launch's attempts",
+                         "traffic_source": "ncu dram__bytes_read+write of one capture of this kernel at 512^2, "
+                                           "3.21 GB over 357.2 M step attempts, scaled by this launch's attempts",
                          "peak_source": "measured in-run FMA microbenchmark (rtw_measure_peaks)",
                          "mufu_gops": mufu / (kms * 1e-3) / 1e9,
                          "mufu_peak_gops": peaks["mufu_ops"] / 1e9},
