@@ -451,6 +451,49 @@ __device__ __noinline__ EscapeOut polar_escape(const KParams& p, double* x, type
     return out;
 }
 
+// A new ray: its frame (binary search over the frame offsets), pixel, FP64
+// initial state, first step size and slope, and the frame-start stamp. Runs
+// once per ray, so it is kept out of line: its FP64 atan, sincos and 64-bit
+// divisions would otherwise sit between the hot phases of the loop (measured
+// 1-3 % faster, identical results).
+template <class K>
+struct FreshRay {
+    double x[9];
+    K k1[9];
+    long long gid, max_steps;
+    double tol, r_term, thick, h, A, X;
+    int fi;
+};
+template <int KIND, class K, class CT>
+__device__ __noinline__ FreshRay<K> fresh_ray(const KParams& p, long long id) {
+    typedef typename SceneOf<KIND>::type SC;
+    FreshRay<K> o;
+    int lo = 0, hi = p.n_frames - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (p.frames[mid].ray_begin <= id) lo = mid; else hi = mid - 1;
+    }
+    const FrameDesc& f = p.frames[lo];
+    o.fi = lo;
+    if (p.frame_clock && id == f.ray_begin) p.frame_clock[p.n_frames + lo] = global_ns();
+    int pi, pj;
+    pixel_of(p.pixel_order, id - f.ray_begin, f.xp, f.yp, pi, pj);
+    o.gid = f.ray_begin + pi + (long long)f.xp * pj;
+    camera_ray(f, pi, pj, o.x);
+    o.tol = f.tol;
+    o.r_term = f.r_term;
+    o.thick = f.thick;
+    o.max_steps = f.max_steps;
+    o.h = -pad_max_dt<KIND, CT>(p.sc, o.x, p.max_dt_scale);
+    double kd[9];
+    Emit<double> em;
+    rhs_fp64<SC>(p.sc, o.x, kd, &em);
+    for (int i = 0; i < 9; ++i) o.k1[i] = K(kd[i]);
+    o.A = em.A;
+    o.X = em.X;
+    return o;
+}
+
 // Launch bounds: 128 threads per CTA; RTW_MIXED_MIN_CTAS resident CTAs per SM
 // for the mixed kernel (3: 168 registers per thread, measured faster than 4
 // with spills or 2), 2 for the FP64 kernel.
@@ -532,27 +575,21 @@ __global__ void __launch_bounds__(128, MIXED ? RTW_MIXED_MIN_CTAS : 2) trace_ker
             if (!active) {
                 const long long id = (long long)base + __popc(empty & ((1u << lane) - 1u));
                 if (id < p.total_rays) {
-                    int lo = 0, hi = p.n_frames - 1;
-                    while (lo < hi) {
-                        const int mid = (lo + hi + 1) >> 1;
-                        if (p.frames[mid].ray_begin <= id) lo = mid; else hi = mid - 1;
-                    }
-                    const FrameDesc& f = p.frames[lo];
-                    fi = lo;
-                    if (p.frame_clock && id == f.ray_begin) p.frame_clock[p.n_frames + lo] = global_ns();
-                    int pi, pj;
-                    pixel_of(p.pixel_order, id - f.ray_begin, f.xp, f.yp, pi, pj);
-                    gid = f.ray_begin + pi + (long long)f.xp * pj;
-                    camera_ray(f, pi, pj, x);
-                    tol = f.tol;
-                    r_term = f.r_term;
-                    thick = f.thick;
-                    max_steps = f.max_steps;
-                    h = -pad_max_dt<KIND, CT>(s, x, p.max_dt_scale);
-                    double kd[9];
-                    rhs_fp64<SC>(s, x, kd, &em0);
+                    const FreshRay<K> fr = fresh_ray<KIND, K, CT>(p, id);
 #pragma unroll
-                    for (int i = 0; i < 9; ++i) k1[i] = K(kd[i]);
+                    for (int i = 0; i < 9; ++i) {
+                        x[i] = fr.x[i];
+                        k1[i] = fr.k1[i];
+                    }
+                    gid = fr.gid;
+                    fi = fr.fi;
+                    tol = fr.tol;
+                    r_term = fr.r_term;
+                    thick = fr.thick;
+                    max_steps = fr.max_steps;
+                    h = fr.h;
+                    em0.A = fr.A;
+                    em0.X = fr.X;
                     nsteps = 0;
                     prev_rej = false;
                     spec_live = em0.A != 0.0;
