@@ -325,7 +325,7 @@ rtw_status rtw_get_frame_times(rtw_ctx* ctx, int32_t n_frames, double* done_ms, 
 typedef struct rtw_adjoint_params {
     const float* target;        /* [P][n_colors] target spectrum */
     int32_t target_on_device;   /* 1: target is a device pointer */
-    int32_t checkpoint_every;   /* accepted steps between stored states (0: 16) */
+    int32_t checkpoint_every;   /* accepted steps between stored states, 1..16 (0: 16) */
     double camera_delta;        /* central-difference step of the camera
                                    transform in a and inclination (0: 1e-6) */
     double* per_ray_grad;       /* NULL, or host [P][5]: each ray's share of grad */

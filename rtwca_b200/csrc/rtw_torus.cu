@@ -115,16 +115,14 @@ RTW_HD void torus_vjp(const TorusModel& m, const double* y, const double* kap, d
                                           D8::var(m.tor.Th0, 7), D8::var(y[1], 0), D8::var(y[2], 1),
                                           D8::var(y[4], 2), D8::var(y[7], 3));
     if (!S.on) return;
-    double sb[4] = {0, 0, 0, 0};
-    typedef Dual<double, 4> D4;  // cj, nus, Theta, g
-    const D4 cj = D4::var(S.cj.v, 0), nus = D4::var(S.nus.v, 1), tht = D4::var(S.th.v, 2), g = D4::var(S.g.v, 3);
+    double sb[4] = {0, 0, 0, 0};  // cotangent of (cj, nus, Theta, g)
     for (int c = 0; c < N; ++c) {
-        D4 ft, fi;
-        torus_bin<D4>(cj, nus, tht, g, m.bins[c], ft, fi);
+        double ft, fi, dft[4], dfi[4];
+        torus_bin_grad(S.cj.v, S.nus.v, S.th.v, S.g.v, m.bins[c], ft, fi, dft, dfi);
         const double e = exp(-y[8 + c]);
         const double kt = kap[8 + c], ki = kap[8 + N + c];
-        for (int q = 0; q < 4; ++q) sb[q] += kt * ft.d[q] + ki * e * fi.d[q];
-        mu[8 + c] += -ki * fi.v * e;  // d (fi exp(-tau)) / d tau
+        for (int q = 0; q < 4; ++q) sb[q] += kt * dft[q] + ki * e * dfi[q];
+        mu[8 + c] += -ki * fi * e;  // d (fi exp(-tau)) / d tau
     }
     const D8* comp[4] = {&S.cj, &S.nus, &S.th, &S.g};
     double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -563,8 +561,6 @@ struct TorusRP {
     FrameDesc dframe[2];  // d frame / d a, d frame / d inclination (pos and M; the rest as frame)
     const float* target;
     const float* spectrum;
-    double* work;                // per lane: work_stride doubles
-    long long work_stride;
     double* out;                 // [1 + 5 + 2]: loss, gradient, escapes carried as identity, rays with escapes
     double* per_ray;             // [P][5] per-ray gradients (may be null)
     int skip_escape_rays;        // 1: rays with a polar escape give no gradient
@@ -687,24 +683,22 @@ RTW_HD bool torus_escape_vjp(const TorusModel& m, const double* y, int nsub, dou
     return true;
 }
 
+constexpr int kTorusMaxD = 8 + 2 * kTorusMaxBins;  // state components
+constexpr int kTorusMaxCk = 16;                     // recorded steps per checkpoint
+
 // Reverse kernel (FP64). Per lane work area, D = 8 + 2N doubles per row:
-//   Ys [ck_every + 1] segment states, K [6] stage slopes, Yst [6] stage
-//   points, kac [6] stage cotangents, Ze [4] escape evaluations,
-//   lam, mu, tmp [1] each.
+//   Ys [ck_every + 1] segment states, Ks [ck_every][6] the stage slopes of
+//   each replayed step, Yst [6] stage points, kac [6] stage cotangents,
+//   Ze [4] escape evaluations, lam, mu, tmp [1] each.
 __global__ void __launch_bounds__(128) torus_reverse(const TorusRP p) {
     const TorusModel& m = p.f.m;
     const int N = m.n, D = 8 + 2 * N;
-    const int KCmax = p.f.ck_every;
-    const long long slot = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    double* W = p.work + slot * p.work_stride;
-    double* Ys = W;
-    double* Kst = Ys + (long long)(KCmax + 1) * D;
-    double* Yst = Kst + 6 * D;
-    double* kac = Yst + 6 * D;
-    double* Ze = kac + 6 * D;
-    double* lam = Ze + 4 * D;
-    double* mu = lam + D;
-    double* tmp = mu + D;
+    // the work area in local memory, whose layout interleaves the lanes of a
+    // warp, so that the lanes' same-index accesses coalesce (rows of D)
+    double Ys[(kTorusMaxCk + 1) * kTorusMaxD];
+    double Ks[kTorusMaxCk * 6 * kTorusMaxD];
+    double Yst[6 * kTorusMaxD], kac[6 * kTorusMaxD], Ze[4 * kTorusMaxD];
+    double lam[kTorusMaxD], mu[kTorusMaxD], tmp[kTorusMaxD];
     unsigned n_cut = 0;
     for (;;) {
         const long long id = (long long)atomicAdd(p.counter, 1ull);
@@ -742,7 +736,7 @@ __global__ void __launch_bounds__(128) torus_reverse(const TorusRP p) {
                 const uint8_t kind = p.f.ev_kind[eo + e];
                 const double hv = p.f.ev_h[eo + e];
                 const bool r = torus_replay(m, Ys + (long long)(e - e0) * D, kind, hv,
-                                            Ys + (long long)(e - e0 + 1) * D, Kst, Yst);
+                                            Ys + (long long)(e - e0 + 1) * D, Ks + (long long)(e - e0) * 6 * D, Yst);
                 if (torus_is_dp(kind) && r) refl |= 1ull << (e - e0);
             }
             for (int e = e1 - 1; e >= e0; --e) {
@@ -754,17 +748,16 @@ __global__ void __launch_bounds__(128) torus_reverse(const TorusRP p) {
                         lam[2] = -lam[2];
                         lam[6] = -lam[6];
                     }
-                    // stages of the step
+                    // the step's stage slopes from the replay; stage points rebuilt
+                    // with the replay's own arithmetic
+                    const double* Kst = Ks + (long long)(e - e0) * 6 * D;
                     for (int i = 0; i < D; ++i) Yst[i] = y[i];
-                    torus_f64(m, y, Kst);
-                    for (int s = 1; s < 6; ++s) {
+                    for (int s = 1; s < 6; ++s)
                         for (int i = 0; i < D; ++i) {
                             double acc = 0;
                             for (int j = 0; j < s; ++j) acc += tA(s, j) * Kst[j * D + i];
                             Yst[s * D + i] = y[i] + hv * acc;
                         }
-                        torus_f64(m, Yst + s * D, Kst + s * D);
-                    }
                     // y' = y + h sum_s b_s K_s, K_s = f(Y_s), Y_s = y + h sum_{j<s} A_sj K_j;
                     // hbar = d loss / d h, for step sizes set by pad_max_dt
                     double hbar = 0;
@@ -1044,7 +1037,7 @@ rtw_status rtw_adjoint(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* c
     TorusBuffers* b = ctx->torus;
     const int N = p.m.n, D = 8 + 2 * N;
     const long long P = run.P;
-    const int KC = adj->checkpoint_every > 0 ? std::min(adj->checkpoint_every, 64) : 16;
+    const int KC = adj->checkpoint_every > 0 ? std::min(adj->checkpoint_every, kTorusMaxCk) : 16;
     p.ck_every = KC;
     const double dl = adj->camera_delta > 0 ? adj->camera_delta : 1e-6;
     const bool mixed = prm->precision == RTW_PREC_MIXED;
@@ -1147,17 +1140,16 @@ rtw_status rtw_adjoint(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* c
     int occ = 0;
     RTW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, torus_reverse, 128, 0), "occupancy");
     const int rgrid = ctx->num_sms * std::max(1, occ);
-    const long long stride = (long long)(KC + 1 + 6 + 6 + 6 + 4 + 3) * D;
-    const size_t work_b = (size_t)rgrid * 128 * stride * 8;
+    // local-memory work area of the reverse kernel (per resident thread)
+    const size_t work_b = (size_t)rgrid * 128 * (size_t)(kTorusMaxCk + 1 + 6 * kTorusMaxCk + 6 + 6 + 4 + 3) *
+                          kTorusMaxD * 8;
     const size_t per_ray_b = adj->per_ray_grad ? (size_t)P * kTorusParams * 8 : 0;
-    if ((st = ensure(ctx, &b->work, &b->work_cap, work_b + per_ray_b)) != RTW_OK) return st;
+    if ((st = ensure(ctx, &b->work, &b->work_cap, std::max<size_t>(per_ray_b, 256))) != RTW_OK) return st;
     rp.f = p;
     rp.f.spectrum = spec;
     rp.target = (const float*)b->tgt;
     rp.spectrum = spec;
-    rp.work = (double*)b->work;
-    rp.work_stride = stride;
-    rp.per_ray = adj->per_ray_grad ? (double*)((char*)b->work + work_b) : nullptr;
+    rp.per_ray = adj->per_ray_grad ? (double*)b->work : nullptr;
     rp.skip_escape_rays = adj->escape_rays == 1;
     unsigned long long* ctl = (unsigned long long*)b->ctl;
     rp.out = (double*)(ctl + 40);

@@ -182,6 +182,45 @@ RTW_HD void torus_bin(const T& cj, const T& nus, const T& th, const T& g, const 
     ft = -(j * em1 / (g4 * B(bn.b0)));
 }
 
+// torus_bin in FP64 with its partial derivatives in (cj, nus, Theta, g), from
+// the closed-form log-derivatives of the fit: with X = g nu_c / nus,
+//   D_X = dln(P^2 e^{-X^1/3}) / dln X = (X^1/2 + 2^(11/12)/3 X^1/6) / P - X^1/3 / 3
+//   D_y = dln expm1(y) / dln y = y e^y / expm1(y),   y = g hk / Theta
+// ln|fi| = ln cj + ln nus + ln(P^2 e^..)(X) - 4 ln g + const,
+// ln|ft| = ln|fi| + ln expm1(y) + const.
+RTW_HD void torus_bin_grad(double cj, double nus, double th, double g, const TorusBin& bn, double& ft, double& fi,
+                           double* dft, double* dfi) {
+    for (int q = 0; q < 4; ++q) {
+        dft[q] = 0;
+        dfi[q] = 0;
+    }
+    ft = 0;
+    fi = 0;
+    const double X = g * bn.nu_hz / nus;
+    if (!(X > 0) || X > 2.0e5) return;
+    const double lx = log(X);
+    const double x12 = exp(0.5 * lx), x16 = exp(lx / 6.0), x13 = exp(lx / 3.0);
+    const double c = 1.8877486253633868;  // 2^(11/12)
+    const double P = x12 + c * x16;
+    const double j = cj * nus * P * P * exp(-x13);
+    const double g2 = g * g, g4 = g2 * g2;
+    fi = -(j * bn.inv_nu_nm3 / g4);
+    const double y = g * bn.hk / th;
+    const double em1 = expm1(y);
+    ft = -(j * em1 / (g4 * bn.b0));
+    const double DX = (x12 + c / 3.0 * x16) / P - x13 / 3.0;
+    const double Dy = y * (em1 + 1.0) / em1;
+    // d/dS = F * dlnF/dlnS / S
+    dfi[0] = fi / cj;
+    dfi[1] = fi * (1.0 - DX) / nus;
+    dfi[2] = 0;
+    dfi[3] = fi * (DX - 4.0) / g;
+    dft[0] = ft / cj;
+    dft[1] = ft * (1.0 - DX) / nus;
+    dft[2] = -ft * Dy / th;
+    dft[3] = ft * (DX - 4.0 + Dy) / g;
+}
+
 // Kerr geodesic acceleration a^mu = -g^{mu nu} T_nu with
 // T_nu = (k^a d_a g_{nu b}) k^b - (1/2) d_nu g_{ab} k^a k^b (the metric
 // depends on r and theta only). Generic in T for the adjoint's derivatives

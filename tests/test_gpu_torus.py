@@ -123,7 +123,7 @@ def test_adjoint_loss_and_checkpoint_interval(renderer, fd_problem):
     sc, cam, col, target, fd, stable, esc = fd_problem
     img = renderer.render(sc, [cam], col, want=("spectrum",), precision=abi.PREC_FP64, integrator=abi.DP45_FSAL)
     loss = float(np.sum((img["spectrum"].astype(np.float64) - target.astype(np.float64)) ** 2))
-    runs = [renderer.adjoint(sc, cam, col, target, precision=abi.PREC_FP64, checkpoint_every=k) for k in (4, 16, 64)]
+    runs = [renderer.adjoint(sc, cam, col, target, precision=abi.PREC_FP64, checkpoint_every=k) for k in (2, 5, 16)]
     for a in runs:
         assert a["loss"] == pytest.approx(loss, rel=1e-12)
         assert a["events"] > 0 and a["checkpoints"] > 0
