@@ -303,14 +303,17 @@ def batched_leg(r, world, rank, stream, barrier_fn):
     }
 
 
-def adjoint_leg(r, x_pix):
+def adjoint_leg(r, x_pix, world=1, rank=0):
     """Differentiable synchrotron torus: Kerr a = 0.94, inclination 17 deg,
     x_pix^2 rays, 32 bins over 230 GHz +- 20 %, FP32-mixed, tolerance 1e-6.
     Loss = sum (I - target)^2 against the image at parameters perturbed by
     5 % normal deviates from numpy default_rng(1). One rtw_adjoint call =
     forward render + record pass + reverse sweep (checkpoints every 16
     accepted steps). Rays that take a polar escape are left out of the
-    gradient (counted in escape_rays). Times are device times of the call."""
+    gradient (counted in escape_rays). Times are device times of the call.
+    On N GPUs every rank takes the interleaved pixels rank, rank + N, ...
+    (strong scaling) and one all-reduce sums the loss and the gradient; the
+    time is the max over ranks."""
     from rtwca_b200 import abi, configs
 
     tp = configs.torus_target_params(1)
@@ -322,8 +325,20 @@ def adjoint_leg(r, x_pix):
     r.render(sc, [cam], col, want=("spectrum",), precision=abi.PREC_MIXED, integrator=abi.DP45_FSAL)
     r.render(sc, [cam], col, want=("spectrum",), precision=abi.PREC_MIXED, integrator=abi.DP45_FSAL)
     fwd = r.stats()
-    a = r.adjoint(sc, cam, col, target, precision=abi.PREC_MIXED, exclude_escape_rays=True)
+    a = r.adjoint(sc, cam, col, target, precision=abi.PREC_MIXED, exclude_escape_rays=True, rays=(rank, 0, world))
     P = cam.x_pix * cam.y_pix
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        v = torch.tensor([a["loss"]] + list(a["grad"]) + [float(a["escape_rays"]), float(a["events"])],
+                         dtype=torch.float64, device="cuda")
+        dist.all_reduce(v)
+        t = torch.tensor([a["total_ms"], a["forward_ms"], a["record_ms"], a["reverse_ms"]], dtype=torch.float64,
+                         device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        v, t = v.cpu().tolist(), t.cpu().tolist()
+        a["loss"], a["grad"], a["escape_rays"], a["events"] = v[0], v[1:6], int(v[6]), int(v[7])
+        a["total_ms"], a["forward_ms"], a["record_ms"], a["reverse_ms"] = t
     return {
         "workload": f"synchrotron torus {cam.x_pix}x{cam.y_pix}, 32 bins 230 GHz +-20%, a=0.94, i=17 deg, tol 1e-6, "
                     "FP32-mixed, FSAL",
@@ -335,7 +350,8 @@ def adjoint_leg(r, x_pix):
         "loss": a["loss"], "grad": dict(zip(abi.ADJOINT_PARAMS, [float(v) for v in a["grad"]])),
         "events": a["events"], "checkpoints": a["checkpoints"], "scratch_GB": a["scratch_bytes"] / 1e9,
         "escape_rays": a["escape_rays"], "escape_rays_policy": "left out of the gradient",
-        "target_params": tp,
+        "target_params": tp, "n_gpus": world,
+        "sharding": "interleaved pixels, one all-reduce of loss + gradient" if world > 1 else "one GPU",
     }
 
 
@@ -417,8 +433,9 @@ def run_b200(args):
     if not args.no_batched:
         batched = batched_leg(r, world, rank, stream, lambda: barrier(world))
     adjoint = None
-    if not args.no_adjoint and rank == 0:
-        adjoint = adjoint_leg(r, args.adjoint_x_pix)
+    if not args.no_adjoint:
+        barrier(world)
+        adjoint = adjoint_leg(r, args.adjoint_x_pix, world, rank)
 
     # end to end through the public API: host pinned outputs, synchronous call
     hx = torch.empty((P, 3), dtype=torch.float32, pin_memory=True)

@@ -337,6 +337,13 @@ typedef struct rtw_adjoint_params {
                                    scales, and the FP32-stage path reaches the axis
                                    differently from the FP64 one. */
     int32_t reserved;
+    /* ray subset (for sharding one image over GPUs): pixels ray_begin + k *
+       ray_stride, k < ray_count; ray_count 0: to the end, ray_stride 0: 1.
+       The loss and gradient are the subset's; out receives its pixels (the
+       others are zero). */
+    int64_t ray_begin;
+    int64_t ray_count;
+    int64_t ray_stride;
 } rtw_adjoint_params;
 
 typedef struct rtw_adjoint_result {

@@ -120,7 +120,7 @@ class AdjointParams(C.Structure):
     _fields_ = [
         ("target", C.c_void_p), ("target_on_device", C.c_int32), ("checkpoint_every", C.c_int32),
         ("camera_delta", C.c_double), ("per_ray_grad", C.c_void_p), ("escape_rays", C.c_int32),
-        ("reserved", C.c_int32),
+        ("reserved", C.c_int32), ("ray_begin", C.c_int64), ("ray_count", C.c_int64), ("ray_stride", C.c_int64),
     ]
 
 

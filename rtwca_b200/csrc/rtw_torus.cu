@@ -201,7 +201,8 @@ constexpr uint32_t kEventCount = 0x7fffffffu;
 struct TorusKP {
     TorusModel m;
     FrameDesc frame;
-    long long total_rays;
+    long long total_rays;          // rays of this launch: pixels ray0 + k ray_stride, k < total_rays
+    long long ray0, ray_stride;
     double max_dt_scale, promote_dr, promote_theta;
     unsigned long long* counter;
     DevStats* stats;
@@ -294,8 +295,9 @@ __global__ void __launch_bounds__(128) torus_forward(const TorusKP p) {
     const int D = 8 + 2 * N;
     unsigned c_att = 0, c_rej = 0, c_pro = 0, c_esc = 0, c_rays = 0, c_nan = 0;
     for (;;) {
-        const long long id = (long long)atomicAdd(p.counter, 1ull);
-        if (id >= p.total_rays) break;
+        const long long loc = (long long)atomicAdd(p.counter, 1ull);  // index in the ray subset
+        if (loc >= p.total_rays) break;
+        const long long id = p.ray0 + loc * p.ray_stride;              // pixel
         ++c_rays;
         const int pi = (int)(id % p.frame.xp), pj = (int)(id / p.frame.xp);
         double x[9];
@@ -324,11 +326,11 @@ __global__ void __launch_bounds__(128) torus_forward(const TorusKP p) {
         long long nsteps = 0;
         uint32_t n_ev = 0;
         bool escaped = false;  // a ray with a polar escape stores its state at every step
-        const uint32_t ev_word = p.record ? p.n_events[id] : 0u;
+        const uint32_t ev_word = p.record ? p.n_events[loc] : 0u;
         const uint32_t ev_cap = ev_word & kEventCount;
         const uint32_t kc = (ev_word & kDenseCheckpoints) ? 1u : (uint32_t)p.ck_every;
-        const unsigned long long eo = p.record ? p.ev_off[id] : 0ull;
-        const unsigned long long co = p.record ? p.ck_off[id] : 0ull;
+        const unsigned long long eo = p.record ? p.ev_off[loc] : 0ull;
+        const unsigned long long co = p.record ? p.ck_off[loc] : 0ull;
         bool bad = false;
         // a checkpoint of the state before event n_ev when it starts a segment
         auto checkpoint = [&]() {
@@ -545,7 +547,7 @@ __global__ void __launch_bounds__(128) torus_forward(const TorusKP p) {
                 p.spectrum[id * N + c] = (float)((double)ihi[c] + (MIXED ? (double)ilo[c] : 0.0));
         if (p.cls) p.cls[id] = (uint8_t)cls;
         if (p.steps) p.steps[id] = (uint32_t)nsteps;
-        if (!p.record && p.n_events) p.n_events[id] = n_ev | (escaped ? kDenseCheckpoints : 0u);
+        if (!p.record && p.n_events) p.n_events[loc] = n_ev | (escaped ? kDenseCheckpoints : 0u);
         if (p.record && (bad || n_ev != ev_cap)) atomicOr(p.err_flag, 1u);
     }
     atomicAdd(&p.stats->step_attempts, (unsigned long long)c_att);
@@ -701,8 +703,9 @@ __global__ void __launch_bounds__(128) torus_reverse(const TorusRP p) {
     double lam[kTorusMaxD], mu[kTorusMaxD], tmp[kTorusMaxD];
     unsigned n_cut = 0;
     for (;;) {
-        const long long id = (long long)atomicAdd(p.counter, 1ull);
-        if (id >= p.f.total_rays) break;
+        const long long loc = (long long)atomicAdd(p.counter, 1ull);
+        if (loc >= p.f.total_rays) break;
+        const long long id = p.f.ray0 + loc * p.f.ray_stride;
         double loss = 0;
         bool fin = true;
         for (int i = 0; i < D; ++i) lam[i] = 0;
@@ -712,7 +715,7 @@ __global__ void __launch_bounds__(128) torus_reverse(const TorusRP p) {
             lam[8 + N + c] = 2 * d;
             loss += d * d;
         }
-        const bool escaped = (p.f.n_events[id] & kDenseCheckpoints) != 0;
+        const bool escaped = (p.f.n_events[loc] & kDenseCheckpoints) != 0;
         if (escaped) atomicAdd(&p.out[2 + kTorusParams], 1.0);
         if (!fin || (escaped && p.skip_escape_rays)) {
             if (fin) atomicAdd(&p.out[0], loss);
@@ -722,9 +725,9 @@ __global__ void __launch_bounds__(128) torus_reverse(const TorusRP p) {
         }
         double pb[kTorusParams] = {0, 0, 0, 0, 0};
         double pend = 0;  // d loss / d h of a step whose h was set at the previous step's start
-        const uint32_t n_ev = p.f.n_events[id] & kEventCount;
-        const int KC = (p.f.n_events[id] & kDenseCheckpoints) ? 1 : p.f.ck_every;
-        const unsigned long long eo = p.f.ev_off[id], co = p.f.ck_off[id];
+        const uint32_t n_ev = p.f.n_events[loc] & kEventCount;
+        const int KC = (p.f.n_events[loc] & kDenseCheckpoints) ? 1 : p.f.ck_every;
+        const unsigned long long eo = p.f.ev_off[loc], co = p.f.ck_off[loc];
         const int nseg = (int)((n_ev + (uint32_t)KC - 1) / (uint32_t)KC);
         for (int seg = nseg - 1; seg >= 0; --seg) {
             const int e0 = seg * KC;
@@ -932,6 +935,8 @@ rtw_status torus_setup(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* c
     if (st != RTW_OK) return fail(ctx, st, "camera parameters invalid or non-finite");
     run.P = total;
     p.total_rays = total;
+    p.ray0 = 0;
+    p.ray_stride = 1;
     p.max_dt_scale = prm->max_dt_scale;
     const double pdr = prm->promote_dr < 0 ? -1.0 : (prm->promote_dr > 0 ? prm->promote_dr : 1e-3);
     const double psn = prm->promote_sin < 0 ? 0.0 : (prm->promote_sin > 0 ? std::min(prm->promote_sin, 1.0) : 1e-2);
@@ -1037,6 +1042,15 @@ rtw_status rtw_adjoint(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* c
     TorusBuffers* b = ctx->torus;
     const int N = p.m.n, D = 8 + 2 * N;
     const long long P = run.P;
+    // the ray subset: pixels ray_begin + k ray_stride, k < ray_count
+    const long long rs = adj->ray_stride > 0 ? adj->ray_stride : 1;
+    const long long r0 = adj->ray_begin;
+    const long long Q = adj->ray_count > 0 ? adj->ray_count : (r0 < P ? (P - r0 + rs - 1) / rs : 0);
+    if (r0 < 0 || Q <= 0 || r0 + (Q - 1) * rs >= P)
+        return fail(ctx, RTW_ERR_INVALID_PARAM, "ray subset outside the image");
+    p.ray0 = r0;
+    p.ray_stride = rs;
+    p.total_rays = Q;
     const int KC = adj->checkpoint_every > 0 ? std::min(adj->checkpoint_every, kTorusMaxCk) : 16;
     p.ck_every = KC;
     const double dl = adj->camera_delta > 0 ? adj->camera_delta : 1e-6;
@@ -1074,11 +1088,11 @@ rtw_status rtw_adjoint(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* c
     float* spec = (float*)b->out;
     uint32_t* steps = (uint32_t*)((char*)b->out + spec_b);
     uint8_t* cls = (uint8_t*)((char*)b->out + spec_b + (((size_t)P * 4 + 255) & ~(size_t)255));
-    const size_t nev_b = ((size_t)P * 4 + 255) & ~(size_t)255;
-    if ((st = ensure(ctx, &b->nev, &b->nev_cap, nev_b + 2 * (size_t)P * 8)) != RTW_OK) return st;
+    const size_t nev_b = ((size_t)Q * 4 + 255) & ~(size_t)255;
+    if ((st = ensure(ctx, &b->nev, &b->nev_cap, nev_b + 2 * (size_t)Q * 8)) != RTW_OK) return st;
     uint32_t* nev = (uint32_t*)b->nev;
     unsigned long long* ev_off = (unsigned long long*)((char*)b->nev + nev_b);
-    unsigned long long* ck_off = ev_off + P;
+    unsigned long long* ck_off = ev_off + Q;
     if ((st = ensure(ctx, &b->tgt, &b->tgt_cap, (size_t)P * N * 4)) != RTW_OK) return st;
     if (adj->target_on_device)
         RTW_CUDA(cudaMemcpyAsync(b->tgt, adj->target, (size_t)P * N * 4, cudaMemcpyDeviceToDevice, s), "target");
@@ -1098,27 +1112,29 @@ rtw_status rtw_adjoint(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* c
         }
     } guard{ev};
 
-    // 1. forward: image, step counts, recorded-step counts
+    // 1. forward: image, step counts, recorded-step counts (pixels outside
+    // the subset stay zero)
     RTW_CUDA(cudaEventRecord(ev[0], s), "event");
+    RTW_CUDA(cudaMemsetAsync(b->out, 0, b->out_cap, s), "clear outputs");
     RTW_CUDA(cudaMemsetAsync(b->ctl, 0, 1024, s), "reset counters");
     p.record = 0;
     RTW_CUDA(launch_forward(p, mixed, run.grid, s), "torus forward");
     RTW_CUDA(cudaEventRecord(ev[1], s), "event");
     // offsets (host scan of the counts)
-    std::vector<uint32_t> h_nev(P);
-    RTW_CUDA(cudaMemcpyAsync(h_nev.data(), nev, 4 * P, cudaMemcpyDeviceToHost, s), "counts D2H");
+    std::vector<uint32_t> h_nev(Q);
+    RTW_CUDA(cudaMemcpyAsync(h_nev.data(), nev, 4 * Q, cudaMemcpyDeviceToHost, s), "counts D2H");
     RTW_CUDA(cudaStreamSynchronize(s), "forward");
-    std::vector<unsigned long long> h_off(2 * P);
+    std::vector<unsigned long long> h_off(2 * Q);
     unsigned long long E = 0, C = 0;
-    for (long long i = 0; i < P; ++i) {
+    for (long long i = 0; i < Q; ++i) {
         h_off[i] = E;
-        h_off[P + i] = C;
+        h_off[Q + i] = C;
         const uint32_t n = h_nev[i] & kEventCount;
         const uint32_t kc = (h_nev[i] & kDenseCheckpoints) ? 1u : (uint32_t)KC;
         E += n;
         C += (n + kc - 1) / kc;
     }
-    RTW_CUDA(cudaMemcpyAsync(ev_off, h_off.data(), 16 * P, cudaMemcpyHostToDevice, s), "offsets H2D");
+    RTW_CUDA(cudaMemcpyAsync(ev_off, h_off.data(), 16 * Q, cudaMemcpyHostToDevice, s), "offsets H2D");
     if ((st = ensure(ctx, &b->evh, &b->evh_cap, std::max<size_t>(8 * E, 256))) != RTW_OK) return st;
     if ((st = ensure(ctx, &b->evk, &b->evk_cap, std::max<size_t>(E, 256))) != RTW_OK) return st;
     if ((st = ensure(ctx, &b->ck, &b->ck_cap, std::max<size_t>(8 * C * (size_t)D, 256))) != RTW_OK) return st;
@@ -1154,6 +1170,7 @@ rtw_status rtw_adjoint(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* c
     unsigned long long* ctl = (unsigned long long*)b->ctl;
     rp.out = (double*)(ctl + 40);
     rp.counter = ctl + 39;
+    if (rp.per_ray) RTW_CUDA(cudaMemsetAsync(rp.per_ray, 0, per_ray_b, s), "clear per-ray gradients");
     RTW_CUDA(cudaEventRecord(ev[4], s), "event");
     {
         void* args[] = {(void*)&rp};
@@ -1194,7 +1211,7 @@ rtw_status rtw_adjoint(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* c
     res->checkpoints = C;
     res->escape_cuts = (uint64_t)h_out[1 + kTorusParams];
     res->escape_rays = (uint64_t)h_out[2 + kTorusParams];
-    res->scratch_bytes = 8 * E + E + 8 * C * (size_t)D + work_b + nev_b + 16 * P;
+    res->scratch_bytes = 8 * E + E + 8 * C * (size_t)D + work_b + nev_b + 16 * Q;
     ctx->have_last = false;
     return RTW_OK;
 }

@@ -139,10 +139,11 @@ class Renderer:
 
     def adjoint(self, scene: abi.Scene, cam: abi.Camera, colors_nm, target, *, precision=abi.PREC_MIXED,
                 checkpoint_every: int = 16, camera_delta: float = 0.0, want=("spectrum",), per_ray: bool = False,
-                exclude_escape_rays: bool = False, **kw) -> dict:
+                exclude_escape_rays: bool = False, rays=(0, 0, 1), **kw) -> dict:
         """Loss sum (I - target)^2 of a synchrotron-torus render and its gradient
         in (spin, inclination, n_e0, b_0, theta_e0) through rtw_adjoint.
-        target: [P, n_colors] float32 (host array or a CUDA tensor)."""
+        target: [P, n_colors] float32 (host array or a CUDA tensor).
+        rays = (begin, count, stride): the pixel subset (count 0: to the end)."""
         cam.y_pix = abi.y_pixels(cam.x_pix, cam.fov_hor, cam.fov_vert)
         P = cam.x_pix * cam.y_pix
         n = len(np.atleast_1d(colors_nm))
@@ -158,6 +159,7 @@ class Renderer:
         ap.checkpoint_every = int(checkpoint_every)
         ap.camera_delta = float(camera_delta)
         ap.escape_rays = int(bool(exclude_escape_rays))
+        ap.ray_begin, ap.ray_count, ap.ray_stride = (int(v) for v in rays)
         res = {}
         if per_ray:
             res["per_ray_grad"] = np.zeros((P, 5))
