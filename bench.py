@@ -45,6 +45,7 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=2048, help="rays in the CPU baseline sample")
     ap.add_argument("--no-batched", action="store_true", help="skip the 96-frame batched leg")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the synchrotron-torus adjoint leg")
+    ap.add_argument("--no-plain-leg", action="store_true", help="skip the plain FP64 GPU path leg")
     ap.add_argument("--adjoint-x-pix", type=int, default=512)
     ap.add_argument("--block-warps", type=int, default=0)
     ap.add_argument("--ctas-per-sm", type=int, default=0)
@@ -429,6 +430,27 @@ def run_b200(args):
         fsal = {"value": world * P * max(1, args.steps // 2) / (tf * 1e-3) / 1e6,
                 "ms_per_step": tf / max(1, args.steps // 2)}
 
+    # the plain FP64 GPU path (one thread per pixel, the reference's full state
+    # and right-hand side): one timed render of the same frame after a warm-up
+    # on a 128^2 frame; single-GPU runs only (it takes tens of seconds)
+    plain = None
+    if not args.no_plain_leg and not args.no_fp64_leg and world == 1:
+        pp = params(abi.PREC_FP64_PLAIN)
+        _, camw, _ = configs.workload(args.workload, x_pix=128)
+        r.render_raw(scene, [camw], pp, out)
+        torch.cuda.synchronize()
+        flush.fill_(1.0)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r.render_raw(scene, [cam], pp, out)
+        e1.record(stream)
+        e1.synchronize()
+        tp = e0.elapsed_time(e1)
+        plain = {"value": P / (tp * 1e-3) / 1e6, "ms_per_step": tp, "mixed_over_plain": value / (P / (tp * 1e-3) / 1e6),
+                 "what": "one FP64 thread per pixel over a grid, the reference's 8 + 2N state and per-bin right-hand "
+                         "side, no warp cooperation (RTW_PREC_FP64_PLAIN)"}
+
     batched = None
     if not args.no_batched:
         batched = batched_leg(r, world, rank, stream, lambda: barrier(world))
@@ -492,6 +514,7 @@ def run_b200(args):
                        "l2": "flushed (256 MB write) between timed renders"},
             "fp64": fp64,
             "fsal": fsal,
+            "plain_fp64": plain,
             "batched": batched,
             "adjoint": adjoint,
             "integrator": "reference step (k1 = previous sum b_i k_i)",

@@ -98,9 +98,15 @@ typedef enum rtw_term_class {
 
 typedef enum rtw_precision {
     RTW_PREC_FP64 = 0,  /* every stage, RHS and RT update in FP64             */
-    RTW_PREC_MIXED = 1  /* FP64 state + controller, FP32 stages/RHS/RT with
+    RTW_PREC_MIXED = 1, /* FP64 state + controller, FP32 stages/RHS/RT with
                            Kahan-compensated intensities, per-ray FP64 stages
                            near the horizon and the polar axis               */
+    RTW_PREC_FP64_PLAIN = 2 /* the plain FP64 GPU path, the baseline: one thread
+                           per pixel over a grid, the reference's full state of
+                           8 + 2N components with every bin's coefficients in
+                           every right-hand side (ray_kernel / integrate_ray,
+                           LttM.jl:11-80; calc_ray_derivative!,
+                           integrators_LttM.jl:9-48), no warp cooperation  */
 } rtw_precision;
 
 typedef enum rtw_integrator {

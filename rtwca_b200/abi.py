@@ -59,6 +59,7 @@ CLASS_NAMES = {0: "none", 1: "escape", 2: "horizon", 3: "thick", 4: "winding", 5
 # rtw_precision / rtw_integrator
 PREC_FP64 = 0
 PREC_MIXED = 1
+PREC_FP64_PLAIN = 2
 DP45_REF_COMPAT = 0
 DP45_FSAL = 1
 

@@ -19,7 +19,7 @@ CSRC = PKG / "csrc"
 BUILD = PKG / "_build"
 LIB = PKG / "librtw_b200.so"
 
-SOURCES = ["rtw_capi.cu", "rtw_probe.cu", "rtw_opcount.cu", "rtw_noalloc.cu", "rtw_kind0.cu", "rtw_kind1.cu", "rtw_kind2.cu", "rtw_kind3.cu", "rtw_torus.cu"]
+SOURCES = ["rtw_capi.cu", "rtw_probe.cu", "rtw_opcount.cu", "rtw_noalloc.cu", "rtw_kind0.cu", "rtw_kind1.cu", "rtw_kind2.cu", "rtw_kind3.cu", "rtw_torus.cu", "rtw_plain.cu"]
 HEADERS = ["rtw_internal.h", "rtw_scenes.cuh", "rtw_trace.cuh", "rtw_launch.cuh", "rtw_ctx.h", "rtw_dual.cuh",
            "rtw_torus.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -485,8 +485,9 @@ rtw_status rtw_render(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* ca
     if (prm->ray_bundles) return fail(ctx, RTW_ERR_UNSUPPORTED, "ray bundles are not built");
     if (scene->kind == RTW_SCENE_KERR_SYNCHRO_TORUS) return torus_render(ctx, scene, cams, n_cams, prm, out);
     if (scene->ref_precision) return fail(ctx, RTW_ERR_UNSUPPORTED, "ref_precision is an oracle-only switch");
-    if (prm->precision != RTW_PREC_FP64 && prm->precision != RTW_PREC_MIXED)
+    if (prm->precision != RTW_PREC_FP64 && prm->precision != RTW_PREC_MIXED && prm->precision != RTW_PREC_FP64_PLAIN)
         return fail(ctx, RTW_ERR_INVALID_PARAM, "precision");
+    const bool plain = prm->precision == RTW_PREC_FP64_PLAIN;
     if (prm->integrator != RTW_DP45_REF_COMPAT && prm->integrator != RTW_DP45_FSAL)
         return fail(ctx, RTW_ERR_INVALID_PARAM, "integrator");
     if (scene->kind < 0 || scene->kind > RTW_SCENE_KERR_THICK_DISK) return fail(ctx, RTW_ERR_INVALID_PARAM, "scene kind");
@@ -525,7 +526,7 @@ rtw_status rtw_render(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* ca
     // launch shape: explicit values, else the autotuner's choice, else defaults
     int warps = prm->block_warps > 0 ? std::min(prm->block_warps, 4) : 0;  // kernel launch bound: 128 threads
     int refill = prm->refill_min > 0 ? std::min(prm->refill_min, 32) : 0;
-    if (prm->autotune && (warps == 0 || refill == 0)) {
+    if (prm->autotune && !plain && (warps == 0 || refill == 0)) {
         std::array<int, 2> choice;
         const rtw_status ts = autotune(ctx, *scene, cams[0], *prm, np, choice);
         if (ts != RTW_OK) return ts;
@@ -642,7 +643,14 @@ rtw_status rtw_render(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* ca
             if ((e = cudaMemsetAsync(p.trace, 0xff, sizeof(double) * RTW_TRACE_FIELDS * (size_t)p.trace_cap, st)) != cudaSuccess)
                 return e;
         if ((e = record(ctx->ev[1])) != cudaSuccess) return e;
-        if ((e = launch_trace(p, prm->precision, grid, block, st)) != cudaSuccess) return e;
+        if (plain) {
+            // one thread per pixel over the whole image, as the reference's grid
+            const long long g = std::max<long long>(1, (total + 127) / 128);
+            e = launch_plain(p, (int)std::min<long long>(g, 1 << 30), 128, st);
+        } else {
+            e = launch_trace(p, prm->precision, grid, block, st);
+        }
+        if (e != cudaSuccess) return e;
         return record(ctx->ev[2]);
     };
     int replayed = 0;

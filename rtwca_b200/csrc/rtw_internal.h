@@ -98,6 +98,8 @@ void make_dev_scene(const rtw_scene& scene, DevScene& d);
 // Launches the trace kernel for p.sc.kind / precision on `stream`.
 // Returns cudaSuccess or the launch error.
 cudaError_t launch_trace(const KParams& p, int precision, int grid, int block, cudaStream_t stream);
+// Launches the plain FP64 one-thread-per-pixel kernel (RTW_PREC_FP64_PLAIN).
+cudaError_t launch_plain(const KParams& p, int grid, int block, cudaStream_t stream);
 // Bytes of spectral scratch per warp for a precision and padded bin count.
 size_t spec_bytes_per_warp(int precision, int np);
 // Registers / max threads of the kernel that launch_trace would run.

@@ -144,3 +144,21 @@ def test_stats(renderer):
     assert st["rays"] == 32 * 32
     assert st["step_attempts"] == int(g["steps"].sum())
     assert st["kernel_ms"] > 0
+
+
+@pytest.mark.parametrize("name", sorted(SMALL))
+def test_plain_fp64_parity(renderer, oracle, name):
+    """The plain FP64 GPU path (one thread per pixel, the reference's full
+    state and right-hand side) follows the oracle's algorithm step for step."""
+    scene, cam, _ = configs.workload(name, x_pix=SMALL[name])
+    colors = configs.log_spaced_colors(16)
+    g = _gpu(renderer, scene, cam, colors, precision=abi.PREC_FP64_PLAIN)
+    r = _ref(oracle, scene, cam, colors)
+    s = summarize(g, r)
+    print(name, s)
+    assert s["class_match"] >= 0.999, s
+    assert s["frac_within_1e-3"] >= 0.999, s
+    assert abs(float(g["steps"].sum()) / float(r["steps"].sum()) - 1.0) < 0.02
+    # the trace kernel's FP64 path gives the same image
+    t = _gpu(renderer, scene, cam, colors, precision=abi.PREC_FP64)
+    assert np.mean(t["class"] == g["class"]) >= 0.999
