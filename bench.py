@@ -137,6 +137,19 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # the CPU legs (oracle restatement of the reference's CPU integrator)
 # ---------------------------------------------------------------------------
+def steps_hist(steps):
+    """Step attempts per ray: quantiles and a log2-binned histogram."""
+    st = np.asarray(steps, dtype=np.int64)
+    q = {f"p{k}": int(np.quantile(st, k / 100)) for k in (1, 10, 50, 90, 99)}
+    q["max"] = int(st.max())
+    q["mean"] = float(st.mean())
+    edges = [0] + [2 ** k for k in range(4, 15)]
+    h, _ = np.histogram(st, bins=edges + [1 << 62])
+    q["hist_log2"] = {f"<{e2}" if e2 < (1 << 62) else f">={e1}": int(c)
+                      for e1, e2, c in zip(edges, edges[1:] + [1 << 62], h)}
+    return q
+
+
 def cpu_sample_ids(P, n):
     n = min(n, P)
     return np.unique(np.linspace(0, P - 1, n).round().astype(np.int64))
@@ -148,7 +161,7 @@ def cpu_time(scene, cam, colors, n, threads=0, keep=False):
     P = cam.x_pix * cam.y_pix
     ids = cpu_sample_ids(P, n)
     t = time.perf_counter()
-    res = O.render(scene, cam, colors, pixel_ids=ids, threads=threads, want=("xyz", "class", "steps"))
+    res = O.render(scene, cam, colors, pixel_ids=ids, threads=threads, want=("xyz", "class", "steps", "state"))
     dt = time.perf_counter() - t
     cores = threads if threads > 0 else (os.cpu_count() or 1)
     if keep:
@@ -500,9 +513,22 @@ def run_b200(args):
             y_r = ref["xyz"][:, 1]
             den = np.maximum(np.abs(y_r), 1e-6 * np.abs(y_r).max() + 1e-300)
             err = np.abs(g_y - y_r) / den
+            # photon-ring pixels: rays that wound more than once around the
+            # hole (|phi_final - phi_camera| > 2 pi in the oracle), reported apart
+            ring = np.abs(ref["state"][:, 3] - cam.position[3]) > 2 * np.pi
+
+            def part(sel):
+                if not sel.any():
+                    return {"pixels": 0}
+                ok = sel & same
+                return {"pixels": int(sel.sum()), "class_match": float(np.mean(same[sel])),
+                        "intensity_within_1e-3": float(np.mean(err[ok] <= 1e-3)) if ok.any() else None,
+                        "p99_rel_err": float(np.quantile(err[ok], 0.99)) if ok.any() else None}
             parity = {"pixels": int(ids.size), "class_match": float(np.mean(same)),
                       "intensity_within_1e-3": float(np.mean(err[same] <= 1e-3)),
                       "p99_rel_err": float(np.quantile(err[same], 0.99)),
+                      "error_denominator": "max(|ref|, 1e-6 max|ref|) on linear Y",
+                      "photon_ring": part(ring), "other": part(~ring),
                       "reference": "FP64 oracle, reference step, same pixels"}
         line = {
             "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
@@ -530,6 +556,7 @@ def run_b200(args):
             "cpu_baseline": cpu,
             "parity_sample": parity,
             "e2e": {"value": e2e_val, "unit": "Mrays/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "steps_per_ray": steps_hist(hs.numpy()),
             "gpu_launches": args.steps,
             "clocks": clk.summary(),
             "counters": {k: st[k] for k in ("step_attempts", "rejected_steps", "promoted_steps", "spectral_steps",
