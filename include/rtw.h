@@ -80,7 +80,15 @@ typedef enum rtw_scene_kind {
        Keplerian 4-velocity; thermal synchrotron j_nu from the Leung, Gammie
        & Noble (2011) fit, alpha_nu = j_nu / B_nu(T_e). Per-bin tau. Only
        the FSAL integrator. */
-    RTW_SCENE_KERR_SYNCHRO_TORUS = 4
+    RTW_SCENE_KERR_SYNCHRO_TORUS = 4,
+    /* Powehi.source, the reference's M87* model: Kerr (spin), a blackbody
+       wedge disk (r_in..r_out, theta_lo..theta_hi, a_nu, temperature) and a
+       rotating conical jet beyond r = 10 within 5 deg of the axis (Lorentz
+       factor 1.2 -> 10 over r = 10..75) radiating power-law synchrotron
+       (p = 2.5, gamma 30..1e9, anisotropy fit) in a global field B^phi = b_0,
+       electron density n_e0 (m^-3), map scale length_cm
+       (source_model.jl:7-317). Per-bin tau; both integrators. */
+    RTW_SCENE_KERR_POWEHI = 5
 } rtw_scene_kind;
 
 /* How a ray ended. The reference's calc_terminate (e.g. Kerr.source/

@@ -44,6 +44,7 @@ SCENE_SCHWARZSCHILD_DISK = 1
 SCENE_KERR_DISK = 2
 SCENE_KERR_THICK_DISK = 3
 SCENE_KERR_SYNCHRO_TORUS = 4
+SCENE_KERR_POWEHI = 5
 ADJOINT_PARAMS = ("spin", "inclination", "n_e0", "b_0", "theta_e0")
 
 # rtw_term_class

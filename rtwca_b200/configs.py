@@ -194,3 +194,18 @@ def torus_problem(x_pix: int = 512, tol: float = 1e-6, params: dict | None = Non
     scene = torus_scene(p["spin"], p["n_e0"], p["b_0"], p["theta_e0"])
     cam = torus_camera(x_pix, p["inclination_deg"], tol=tol)
     return scene, cam, torus_colors()
+
+
+# ---------------------------------------------------------------------------
+# Powehi (the reference's M87* model): its scene constants and its "m87"
+# camera (initialization.jl:100-110).
+# ---------------------------------------------------------------------------
+def powehi_scene() -> abi.Scene:
+    return abi.scene_default(abi.SCENE_KERR_POWEHI)
+
+
+def powehi_camera(x_pix: int = 256, tol: float = 1e-6, max_steps: int = 20_000) -> abi.Camera:
+    """position (0, 35, 0.3, 0), direction (pi/2, pi/6), pointing (0, 0, pi),
+    beta 0; the reference's default field of view (85 x 60 deg)."""
+    return abi.make_camera([0.0, 35.0, 0.3, 0.0], [PI / 2, PI / 6], 0.0, [0.0, 0.0, PI], x_pix, 85.0, 60.0, tol,
+                           max_steps)

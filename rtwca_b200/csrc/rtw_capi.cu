@@ -118,7 +118,8 @@ void boost(double beta, M4 out) {
 }
 
 bool is_kerr(int kind) {
-    return kind == RTW_SCENE_KERR_DISK || kind == RTW_SCENE_KERR_THICK_DISK || kind == RTW_SCENE_KERR_SYNCHRO_TORUS;
+    return kind == RTW_SCENE_KERR_DISK || kind == RTW_SCENE_KERR_THICK_DISK || kind == RTW_SCENE_KERR_SYNCHRO_TORUS ||
+           kind == RTW_SCENE_KERR_POWEHI;
 }
 
 double horizon_radius(const rtw_scene& s) {
@@ -304,6 +305,17 @@ rtw_status rtw_scene_default(int32_t kind, rtw_scene* s) {
         s->n_e0 = 1e5; s->b_0 = 10; s->theta_e0 = 10; s->length_cm = 9.62e14;
         s->escape_radius = 110;
         break;
+    case RTW_SCENE_KERR_POWEHI:
+        // Powehi.source (the reference's M87* model): a = 0.9 (source_geometry.jl:12),
+        // wedge disk r_ISCO..12, 31pi/64..33pi/64, a_nu = 1e-2, T = 5778
+        // (source_model.jl:186-190, 229-232); jet n_e0 = 1e7 m^-3, global field
+        // B^phi = 10 G (source_model.jl:13, 47-55); map_scale 9.62e12 m (:7)
+        s->spin = (double)0.9f;
+        s->r_in = reference_isco(1.0, s->spin); s->r_out = 12;
+        s->theta_lo = 31 * kPi / 64; s->theta_hi = 33 * kPi / 64;
+        s->temperature = 5778; s->a_nu = (double)1e-2f;
+        s->n_e0 = 1e7; s->b_0 = 10; s->length_cm = 9.62e14;
+        break;
     default:
         return RTW_ERR_INVALID_PARAM;
     }
@@ -483,7 +495,8 @@ rtw_status rtw_render(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* ca
     if (prm->n_colors <= 0 || prm->n_colors > RTW_MAX_BINS || !prm->colors_nm)
         return fail(ctx, RTW_ERR_INVALID_PARAM, "n_colors must be 1..128 with colors_nm set");
     if (prm->ray_bundles) return fail(ctx, RTW_ERR_UNSUPPORTED, "ray bundles are not built");
-    if (scene->kind == RTW_SCENE_KERR_SYNCHRO_TORUS) return torus_render(ctx, scene, cams, n_cams, prm, out);
+    if (scene->kind == RTW_SCENE_KERR_SYNCHRO_TORUS || scene->kind == RTW_SCENE_KERR_POWEHI)
+        return torus_render(ctx, scene, cams, n_cams, prm, out);
     if (scene->ref_precision) return fail(ctx, RTW_ERR_UNSUPPORTED, "ref_precision is an oracle-only switch");
     if (prm->precision != RTW_PREC_FP64 && prm->precision != RTW_PREC_MIXED && prm->precision != RTW_PREC_FP64_PLAIN)
         return fail(ctx, RTW_ERR_INVALID_PARAM, "precision");

@@ -28,6 +28,8 @@
 #include "rtw_trace.cuh"
 #include "rtw_torus.cuh"
 
+extern "C" rtw_status rtw_cie_weights(const double* colors_nm, int32_t n_colors, double* w_x, double* w_y,
+                                      double* w_z, double* i_lambda_factor);
 extern "C" rtw_status rtw_prepare_frames(const rtw_scene* scene, const rtw_camera* cams, int32_t n_cams,
                                          void* frames_out, int64_t* total_out);
 
@@ -67,9 +69,23 @@ RTW_HD double tE(int s) {
 struct TorusModel {
     DevScene geo;  // Kerr geodesic functor (its thin disk switched off)
     TorusDev tor;
+    PowehiDev pw;
     TorusBin bins[kTorusMaxBins];
     int n;         // bins
+    int emitter;   // 0: synchrotron torus, 1: Powehi (disk + jet)
 };
+
+// The scene's emitter at a stage point z (x^mu, k^mu) and the slopes of bin c.
+template <class R>
+RTW_HD TorusPt<R> em_point(const TorusModel& m, const R* z) {
+    if (m.emitter == 1) return powehi_point<R>(m.pw, z);
+    return torus_point<R>(m.tor, R(m.tor.a), R(m.tor.n0), R(m.tor.B0), R(m.tor.Th0), z[1], z[2], z[4], z[7]);
+}
+template <class R>
+RTW_HD void em_bin(const TorusModel& m, const TorusPt<R>& S, int c, R& ft, R& fi) {
+    if (m.emitter == 1) powehi_bin<R>(m.pw, S, m.bins[c].nu_nm, ft, fi);
+    else torus_bin<R>(S.cj, S.nus, S.th, S.g, m.bins[c], ft, fi);
+}
 
 // FP64 right-hand side on a state y[8 + 2N] = (x^mu, k^mu, tau_c, I_c).
 RTW_HD void torus_f64(const TorusModel& m, const double* y, double* f) {
@@ -81,10 +97,10 @@ RTW_HD void torus_f64(const TorusModel& m, const double* y, double* f) {
     Emit<double> em;
     KerrScene<false>::rhs<double>(m.geo, z, k, em);
     for (int i = 0; i < 8; ++i) f[i] = k[i];
-    const TorusPt<double> S = torus_point<double>(m.tor, m.tor.a, m.tor.n0, m.tor.B0, m.tor.Th0, y[1], y[2], y[4], y[7]);
+    const TorusPt<double> S = em_point<double>(m, y);
     for (int c = 0; c < N; ++c) {
         double ft = 0, fi = 0;
-        if (S.on) torus_bin<double>(S.cj, S.nus, S.th, S.g, m.bins[c], ft, fi);
+        if (S.on) em_bin<double>(m, S, c, ft, fi);
         f[8 + c] = ft;
         f[8 + N + c] = fi * exp(-y[8 + c]);
     }
@@ -207,6 +223,7 @@ struct TorusKP {
     unsigned long long* counter;
     DevStats* stats;
     float* spectrum;  // [P][N]
+    float* xyz;       // [P][3]
     uint8_t* cls;
     uint32_t* steps;
     // recording
@@ -220,6 +237,7 @@ struct TorusKP {
                                        // 1 + n: polar escape of n sub-steps
     double* ck;                        // [C][8 + 2N] states
     int ck_every;
+    int fsal;                          // 1: FSAL Dormand-Prince, 0: the reference's step
     unsigned int* err_flag;            // bit 0: record pass diverged from the count pass
 };
 
@@ -254,7 +272,7 @@ __device__ void torus_geo_stages(const TorusModel& m, const double* x, const K* 
         Emit<R> em;
         KerrScene<false>::rhs<R>(m.geo, z, kk, em);
         for (int i = 0; i < 8; ++i) Kg[s][i] = kk[i];
-        o.S[s] = torus_point<R>(m.tor, R(m.tor.a), R(m.tor.n0), R(m.tor.B0), R(m.tor.Th0), z[1], z[2], z[4], z[7]);
+        o.S[s] = em_point<R>(m, z);
         if (s == 6)
             for (int i = 0; i < 8; ++i) o.ns[i] = (double)acc[i];
     }
@@ -428,6 +446,7 @@ __global__ void __launch_bounds__(128) torus_forward(const TorusKP p) {
                         st.S[s].th = SR(sd.S[s].th);
                         st.S[s].g = SR(sd.S[s].g);
                         st.S[s].on = sd.S[s].on;
+                        st.S[s].zone = sd.S[s].zone;
                     }
                 } else {
                     torus_geo_stages<SR, SR>(p.m, x, k1, h, st);
@@ -458,15 +477,18 @@ __global__ void __launch_bounds__(128) torus_forward(const TorusKP p) {
                         for (int j = 0; j < s; ++j) a += SR(tA(s, j)) * kt[j];
                         tp = t0 + hs * a;
                         SR ft = 0, fi = 0;
-                        if (st.S[s].on) torus_bin<SR>(st.S[s].cj, st.S[s].nus, st.S[s].th, st.S[s].g, p.m.bins[c], ft, fi);
+                        if (st.S[s].on) em_bin<SR>(p.m, st.S[s], c, ft, fi);
                         kt[s] = ft;
                         ki[s] = fi * texp(-tp);
                     }
                     // tp is now the new tau (row 6 of A is b)
-                    SR nsI = 0, et = 0, ei = 0;
+                    SR nsI = 0, nsT = 0, et = 0, ei = 0;
 #pragma unroll
                     for (int j = 0; j < 7; ++j) {
-                        if (j < 6) nsI += SR(tA(6, j)) * ki[j];
+                        if (j < 6) {
+                            nsI += SR(tA(6, j)) * ki[j];
+                            nsT += SR(tA(6, j)) * kt[j];
+                        }
                         et += SR(tE(j)) * kt[j];
                         ei += SR(tE(j)) * ki[j];
                     }
@@ -484,8 +506,10 @@ __global__ void __launch_bounds__(128) torus_forward(const TorusKP p) {
                     c_t[c] = tp;
                     c_h[c] = yh;
                     c_l[c] = yl;
-                    c_kt[c] = kt[6];
-                    c_ki[c] = ki[6];
+                    // slopes carried to the next attempt: k7 (FSAL) or the
+                    // reference's sum b_i k_i
+                    c_kt[c] = p.fsal ? kt[6] : nsT;
+                    c_ki[c] = p.fsal ? ki[6] : nsI;
                 }
                 err2 += (double)ebins;
                 bool accept;
@@ -497,7 +521,7 @@ __global__ void __launch_bounds__(128) torus_forward(const TorusKP p) {
                     push(hsrc ? (uint8_t)(0x40 | hsrc) : (uint8_t)0, h);
                     for (int i = 0; i < 8; ++i) {
                         x[i] = y[i];
-                        k1[i] = st.k7[i];
+                        k1[i] = p.fsal ? st.k7[i] : SR(st.ns[i]);
                     }
                     for (int c = 0; c < N; ++c) {
                         tau[c] = c_t[c];
@@ -506,9 +530,10 @@ __global__ void __launch_bounds__(128) torus_forward(const TorusKP p) {
                         kt1[c] = c_kt[c];
                         ki1[c] = c_ki[c];
                     }
-                    if (torus_keep(x)) {
+                    if (torus_keep(x) && p.fsal) {
                         // reflected through the pole: the carried slope belongs to
-                        // the unreflected point, so take f at the new state
+                        // the unreflected point, so take f at the new state (FSAL;
+                        // the reference's step keeps its carried sum)
                         double yy[8 + 2 * kTorusMaxBins], ff[8 + 2 * kTorusMaxBins];
                         for (int i = 0; i < 8; ++i) yy[i] = x[i];
                         for (int q = 0; q < N; ++q) {
@@ -542,9 +567,21 @@ __global__ void __launch_bounds__(128) torus_forward(const TorusKP p) {
             cls = RTW_CLASS_NAN;
             ++c_nan;
         }
-        if (p.spectrum)
-            for (int c = 0; c < N; ++c)
-                p.spectrum[id * N + c] = (float)((double)ihi[c] + (MIXED ? (double)ilo[c] : 0.0));
+        if (p.spectrum || p.xyz) {
+            double X = 0, Y = 0, Z = 0;
+            for (int c = 0; c < N; ++c) {
+                const double I = (double)ihi[c] + (MIXED ? (double)ilo[c] : 0.0);
+                if (p.spectrum) p.spectrum[id * N + c] = (float)I;
+                X += I * p.m.bins[c].fx;
+                Y += I * p.m.bins[c].fy;
+                Z += I * p.m.bins[c].fz;
+            }
+            if (p.xyz) {
+                p.xyz[3 * id + 0] = (float)X;
+                p.xyz[3 * id + 1] = (float)Y;
+                p.xyz[3 * id + 2] = (float)Z;
+            }
+        }
         if (p.cls) p.cls[id] = (uint8_t)cls;
         if (p.steps) p.steps[id] = (uint32_t)nsteps;
         if (!p.record && p.n_events) p.n_events[loc] = n_ev | (escaped ? kDenseCheckpoints : 0u);
@@ -850,15 +887,59 @@ constexpr double kMe = 9.1093837015e-28;       // g
 constexpr double kHcgs = 6.62607015e-27;       // erg s
 constexpr double kMec2 = kMe * kCcgs * kCcgs;  // erg
 
+// Powehi.source constants (source_model.jl:7-35, source_geometry.jl:7-34)
+constexpr double kPowehiP = 2.5, kPowehiGmin = 30.0, kPowehiGmax = 1e9;
+constexpr double kPowehiFitC = 7.951834e-01, kPowehiFitD = 9.832989e-01, kPowehiFitE = -5.752283e-01;
+
+void powehi_model(const rtw_scene& s, const DevScene& geo, PowehiDev& w) {
+    w.M = s.mass;
+    w.a = s.spin;
+    w.rs = 2 * s.mass;
+    w.r_ev = geo.r_ev;
+    w.disk_r_in = s.r_in;
+    w.disk_r_out = s.r_out;
+    w.disk_th_lo = s.theta_lo;
+    w.disk_th_hi = s.theta_hi;
+    w.disk_a = s.a_nu;
+    w.disk_T = s.temperature;
+    w.r_nozzle = 10;
+    w.gamma_min = 1.2;
+    w.gamma_max = 10;
+    w.nozzle_acc = (10.0 - 1.2) / (75.0 - 10.0);
+    w.omega_jet = 0.5 * s.spin / (w.rs * w.r_ev);
+    w.jet_th_lo = 0.087263889;
+    w.jet_th_hi = 3.054236111;
+    w.axis_lo = 1e-3;
+    w.axis_hi = 3.1406;
+    w.b_phi = s.b_0;
+    // synch_em = 7.694e-37 map_scale 2.8e7, synch_ab = 2.8173e-24 map_scale
+    // (map_scale in metres), times the electron-distribution constants of
+    // calc_radiative_coefficients (Marszewski 2021 forms)
+    const double ms = s.length_cm / 100.0, p = kPowehiP;
+    const double gdiff = std::pow(kPowehiGmin, 1 - p) - std::pow(kPowehiGmax, 1 - p);
+    const double cj = std::pow(3.0, p / 2) * (p - 1) / (2 * (p + 1) * gdiff) * std::tgamma((3 * p - 1) / 12) *
+                      std::tgamma((3 * p + 19) / 12);
+    const double ca = std::pow(3.0, (p + 1) / 2) * (p - 1) / (4 * gdiff) * std::tgamma((3 * p + 2) / 12) *
+                      std::tgamma((3 * p + 22) / 12);
+    w.j_scale = s.n_e0 * (7.694e-37 * ms * 2.8e7) * cj;
+    w.a_scale = s.n_e0 * (2.8173e-24 * ms) * ca;
+    w.p_index = p;
+    w.inv_p_synch = 1.0 / (std::exp(kPowehiFitC + kPowehiFitE * p) * std::pow(p, kPowehiFitD * p));
+}
+
 rtw_status torus_model(const rtw_scene& s, const double* colors_nm, int N, TorusModel& m, std::string& why) {
     std::memset(&m, 0, sizeof(m));
     if (N <= 0 || N > kTorusMaxBins || !colors_nm) {
-        why = "the torus takes 1..32 bins";
+        why = "the per-bin scenes take 1..32 bins";
         return RTW_ERR_INVALID_PARAM;
     }
-    if (!(s.mass > 0) || !(std::fabs(s.spin) < s.mass) || !(s.r_in > 0) || !(s.r_out >= s.r_in) ||
-        !(s.edge_in > 0) || !(s.edge_out > 0) || !(s.n_e0 >= 0) || !(s.b_0 > 0) || !(s.theta_e0 > 0) ||
-        !(s.length_cm > 0) || !(s.rho_h > 0)) {
+    const bool powehi = s.kind == RTW_SCENE_KERR_POWEHI;
+    if (!(s.mass > 0) || !(std::fabs(s.spin) < s.mass) || !(s.b_0 > 0) || !(s.length_cm > 0) || !(s.n_e0 >= 0)) {
+        why = "scene parameters out of range";
+        return RTW_ERR_INVALID_PARAM;
+    }
+    if (!powehi && (!(s.r_in > 0) || !(s.r_out >= s.r_in) || !(s.edge_in > 0) || !(s.edge_out > 0) ||
+                    !(s.theta_e0 > 0) || !(s.rho_h > 0))) {
         why = "torus parameters out of range";
         return RTW_ERR_INVALID_PARAM;
     }
@@ -884,19 +965,26 @@ rtw_status torus_model(const rtw_scene& s, const double* colors_nm, int N, Torus
     t.Th0 = s.theta_e0;
     t.cj_unit = std::sqrt(2.0) * kPi * kE * kE / (3 * kCcgs) * s.length_cm;
     t.nuc_unit = kE / (2 * kPi * kMe * kCcgs);
+    double wx[kTorusMaxBins], wy[kTorusMaxBins], wz[kTorusMaxBins], fac[kTorusMaxBins];
+    if (rtw_cie_weights(colors_nm, N, wx, wy, wz, fac) != RTW_OK) {
+        why = "colors_nm must be positive";
+        return RTW_ERR_INVALID_PARAM;
+    }
     for (int c = 0; c < N; ++c) {
         const double lam = colors_nm[c];
-        if (!(lam > 0)) {
-            why = "colors_nm must be positive";
-            return RTW_ERR_INVALID_PARAM;
-        }
+        m.bins[c].fx = fac[c] * wx[c];
+        m.bins[c].fy = fac[c] * wy[c];
+        m.bins[c].fz = fac[c] * wz[c];
         const double nu = kLightC * 1e9 / lam;  // Hz
+        m.bins[c].nu_nm = 1.0 / lam;
         m.bins[c].nu_hz = nu;
         m.bins[c].inv_nu_nm3 = lam * lam * lam;
         m.bins[c].b0 = 2 * kHcgs * nu * nu * nu / (kCcgs * kCcgs);
         m.bins[c].hk = kHcgs * nu / kMec2;
     }
     m.n = N;
+    m.emitter = powehi ? 1 : 0;
+    if (powehi) powehi_model(s, m.geo, m.pw);
     return RTW_OK;
 }
 
@@ -920,8 +1008,8 @@ rtw_status torus_setup(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* c
     if (!scene || !cam || !prm) return fail(ctx, RTW_ERR_INVALID_PARAM, "null argument");
     if (prm->precision != RTW_PREC_FP64 && prm->precision != RTW_PREC_MIXED)
         return fail(ctx, RTW_ERR_INVALID_PARAM, "precision");
-    if (prm->integrator != RTW_DP45_FSAL)
-        return fail(ctx, RTW_ERR_UNSUPPORTED, "the synchrotron torus runs the FSAL integrator only");
+    if (prm->integrator != RTW_DP45_FSAL && prm->integrator != RTW_DP45_REF_COMPAT)
+        return fail(ctx, RTW_ERR_INVALID_PARAM, "integrator");
     if (prm->ray_bundles) return fail(ctx, RTW_ERR_UNSUPPORTED, "ray bundles are not built");
     if (!(prm->max_dt_scale > 0)) return fail(ctx, RTW_ERR_INVALID_PARAM, "max_dt_scale must be > 0");
     std::string why;
@@ -939,10 +1027,15 @@ rtw_status torus_setup(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* c
     p.ray_stride = 1;
     p.max_dt_scale = prm->max_dt_scale;
     const double pdr = prm->promote_dr < 0 ? -1.0 : (prm->promote_dr > 0 ? prm->promote_dr : 1e-3);
-    const double psn = prm->promote_sin < 0 ? 0.0 : (prm->promote_sin > 0 ? std::min(prm->promote_sin, 1.0) : 1e-2);
+    // pole promotion: default sin(theta) < 1e-2; Powehi's jet lies within 5 deg
+    // of the axis, where FP32 stages lose accuracy, so there the default covers it
+    const double psn_default = scene->kind == RTW_SCENE_KERR_POWEHI ? 0.1 : 1e-2;
+    const double psn =
+        prm->promote_sin < 0 ? 0.0 : (prm->promote_sin > 0 ? std::min(prm->promote_sin, 1.0) : psn_default);
     p.promote_dr = pdr * scene->mass;
     p.promote_theta = std::asin(psn);
     p.ck_every = 16;
+    p.fsal = prm->integrator == RTW_DP45_FSAL;
     if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, RTW_ERR_CUDA, "cudaSetDevice");
     if (!ctx->torus) ctx->torus = new TorusBuffers();
     TorusBuffers* b = ctx->torus;
@@ -979,19 +1072,22 @@ rtw_status torus_render(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* 
     float* spec = out->spectrum;
     uint8_t* cls = out->term_class;
     uint32_t* steps = out->steps;
+    float* xyz = out->xyz;
     if (!out->on_device) {
-        const size_t need = (size_t)P * (sizeof(float) * N + 1 + 4) + 1024;
+        auto up = [](size_t v) { return (v + 255) & ~(size_t)255; };
+        const size_t o_steps = up((size_t)P * N * 4), o_cls = o_steps + up((size_t)P * 4),
+                     o_xyz = o_cls + up((size_t)P), need = o_xyz + up((size_t)P * 12);
         if ((st = ensure(ctx, &b->out, &b->out_cap, need)) != RTW_OK) return st;
         char* base = (char*)b->out;
         spec = out->spectrum ? (float*)base : nullptr;
-        steps = out->steps ? (uint32_t*)(base + (((size_t)P * N * 4 + 255) & ~(size_t)255)) : nullptr;
-        cls = out->term_class ? (uint8_t*)(base + (((size_t)P * N * 4 + 255) & ~(size_t)255) +
-                                           (((size_t)P * 4 + 255) & ~(size_t)255))
-                              : nullptr;
+        steps = out->steps ? (uint32_t*)(base + o_steps) : nullptr;
+        cls = out->term_class ? (uint8_t*)(base + o_cls) : nullptr;
+        xyz = out->xyz ? (float*)(base + o_xyz) : nullptr;
     }
     p.spectrum = spec;
     p.cls = cls;
     p.steps = steps;
+    p.xyz = xyz;
     // the context's counter and stats block, so that rtw_get_stats reads them
     p.counter = ctx->d_ctl;
     p.stats = (DevStats*)(ctx->d_ctl + 1);
@@ -1006,11 +1102,8 @@ rtw_status torus_render(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* 
         if (out->steps) RTW_CUDA(cudaMemcpyAsync(out->steps, steps, 4 * P, cudaMemcpyDeviceToHost, s), "D2H");
         if (out->term_class) RTW_CUDA(cudaMemcpyAsync(out->term_class, cls, P, cudaMemcpyDeviceToHost, s), "D2H");
     }
-    // xyz of a millimetre spectrum is zero: the CIE functions vanish there
-    if (out->xyz) {
-        if (out->on_device) RTW_CUDA(cudaMemsetAsync(out->xyz, 0, sizeof(float) * 3 * P, s), "xyz");
-        else std::memset(out->xyz, 0, sizeof(float) * 3 * P);
-    }
+    if (out->xyz && !out->on_device)
+        RTW_CUDA(cudaMemcpyAsync(out->xyz, xyz, sizeof(float) * 3 * P, cudaMemcpyDeviceToHost, s), "xyz D2H");
     RTW_CUDA(cudaEventRecord(ctx->ev[3], s), "event");
     ctx->have_last = true;
     ctx->last_frames = 0;
@@ -1035,6 +1128,8 @@ rtw_status rtw_adjoint(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* c
     if (!scene || !cam || !prm || !adj || !res || !adj->target) return fail(ctx, RTW_ERR_INVALID_PARAM, "null argument");
     if (scene->kind != RTW_SCENE_KERR_SYNCHRO_TORUS)
         return fail(ctx, RTW_ERR_UNSUPPORTED, "the adjoint is built for the synchrotron torus");
+    if (prm->integrator != RTW_DP45_FSAL)
+        return fail(ctx, RTW_ERR_UNSUPPORTED, "the adjoint needs the FSAL integrator (each step a function of its start state)");
     TorusRun run;
     rtw_status st = torus_setup(ctx, scene, cam, prm, run);
     if (st != RTW_OK) return st;
@@ -1218,7 +1313,9 @@ rtw_status rtw_adjoint(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* c
 
 rtw_status rtw_torus_rhs(const rtw_scene* scene, const double* colors_nm, int32_t n_colors, int32_t form,
                          const double* state, double* slope) {
-    if (!scene || !state || !slope || scene->kind != RTW_SCENE_KERR_SYNCHRO_TORUS) return RTW_ERR_INVALID_PARAM;
+    if (!scene || !state || !slope ||
+        (scene->kind != RTW_SCENE_KERR_SYNCHRO_TORUS && scene->kind != RTW_SCENE_KERR_POWEHI))
+        return RTW_ERR_INVALID_PARAM;
     TorusModel m;
     std::string why;
     if (torus_model(*scene, colors_nm, n_colors, m, why) != RTW_OK) return RTW_ERR_INVALID_PARAM;

@@ -28,19 +28,25 @@ struct TorusDev {
 
 // Per-bin constants of the observed frequency nu_c.
 struct TorusBin {
+    double nu_nm;       // nu_c in nm^-1
     double nu_hz;       // nu_c in Hz
     double inv_nu_nm3;  // 1 / (nu_c in nm^-1)^3
     double b0;          // 2 h nu_c^3 / c^2 (cgs)
     double hk;          // h nu_c / (m_e c^2)
+    double fx, fy, fz;  // nu^3 c / lambda^2 * CIE trapezoid weights (XYZ epilogue)
 };
 
 // Emitter numbers at a point, shared by every bin: j_nu = cj nus F(nu / nus)
 // (per map unit), nus = (2/9) nu_cyc Theta^2 sin(theta_B), Theta = kT_e / m_e
 // c^2, g = -u.k. on = false outside the emitter (every slope is then 0).
+// The Powehi emitter (powehi_point) uses the same record with zone 1 (disk:
+// cj = a_nu, nus = T) or zone 2 (jet: cj = J0, nus = A0, th = 1/(nu_c sin
+// theta_B)).
 template <class T>
 struct TorusPt {
     T cj, nus, th, g;
     bool on;
+    int zone;
 };
 
 // K_2(1/theta) by the trapezoid rule on K_2(x) = int_0^inf exp(-x cosh t)
@@ -96,6 +102,7 @@ RTW_HD TorusPt<T> torus_point(const TorusDev& P, const T& a, const T& n0, const 
     typedef decltype(val(r)) B;  // float or double
     TorusPt<T> o;
     o.on = false;
+    o.zone = 0;
     o.cj = T(0.0); o.nus = T(0.0); o.th = T(1.0); o.g = T(1.0);
     const double rv = (double)val(r);
     if (!(rv >= P.cut_in && rv <= P.cut_out)) return o;
@@ -180,6 +187,136 @@ RTW_HD void torus_bin(const T& cj, const T& nus, const T& th, const T& g, const 
     // -inv(g) alpha, alpha = j expm1(h nu / k T) / (2 h nu^3 / c^2)
     const T em1 = texpm1(g * B(bn.hk) / th);
     ft = -(j * em1 / (g4 * B(bn.b0)));
+}
+
+// ---------------------------------------------------------------------------
+// The Powehi scene (Powehi.source, the reference's M87* model): Kerr a = 0.9
+// with a blackbody wedge disk (zone 1) and a rotating conical jet (zone 2)
+// radiating power-law synchrotron; source_model.jl:186-317.
+// ---------------------------------------------------------------------------
+struct PowehiDev {
+    double M, a, r_ev, rs;
+    double disk_r_in, disk_r_out, disk_th_lo, disk_th_hi, disk_a, disk_T;  // zone 1
+    double r_nozzle, gamma_min, gamma_max, nozzle_acc, omega_jet;        // zone 2 geometry
+    double jet_th_lo, jet_th_hi, axis_lo, axis_hi;                         // zone 2 polar limits
+    double b_phi;        // global field component B^phi (gauss)
+    double j_scale;      // ne_0 synch_em * (p-dependent constants): j = j_scale |b| sin Phi s^-(p-1)/2
+    double a_scale;      // ne_0 synch_ab * (p-dependent constants): a = a_scale Phi / nu s^-(p+2)/2
+    double p_index;      // electron power-law index p
+    double inv_p_synch;  // 1 / Approx_P_synch(p)
+};
+
+// Emitter numbers at a stage point z = (t, r, theta, phi, k^t, k^r, k^theta,
+// k^phi) (region_calc, get_source_velocity!, calc_freq_shift,
+// calc_fluid_params!, transform_B_b, calc_b_angle; source_model.jl:60-317).
+template <class T>
+RTW_HD TorusPt<T> powehi_point(const PowehiDev& P, const T* z) {
+    typedef decltype(val(z[1])) B;
+    TorusPt<T> o;
+    o.on = false;
+    o.zone = 0;
+    o.cj = T(0.0); o.nus = T(0.0); o.th = T(1.0); o.g = T(1.0);
+    const double rv = (double)val(z[1]), thv = (double)val(z[2]);
+    int zone = 3;
+    if (P.disk_r_in <= rv && rv <= P.disk_r_out && P.disk_th_lo <= thv && thv <= P.disk_th_hi)
+        zone = 1;
+    else if (rv >= P.r_nozzle && !(P.jet_th_lo <= thv && thv <= P.jet_th_hi) && (P.axis_lo <= thv && thv <= P.axis_hi))
+        zone = 2;
+    if (zone == 3) return o;
+    const T r = z[1], th = z[2], kt = z[4], kr = z[5], kth = z[6], kph = z[7];
+    const B a = B(P.a), M = B(P.M);
+    const T sn = tsin(th), cs = tcos(th);
+    const T r2 = r * r, s2 = sn * sn;
+    const T Sig = r2 + a * a * cs * cs;
+    const T Del = r2 - B(2.0) * M * r + a * a;
+    const T Aa = (r2 + a * a) * (r2 + a * a) - Del * a * a * s2;
+    const T gtt = -(T(B(1.0)) - B(2.0) * M * r / Sig);
+    const T gtp = -(B(2.0) * M * a * r * s2 / Sig);
+    const T gpp = Aa / Sig * s2;
+    const T grr = Sig / Del;
+    const T ghh = Sig;
+    T ut, ur = T(B(0.0)), up;
+    if (zone == 1) {
+        // prograde equatorial circular orbit
+        const T sr = tsqrt(r);
+        const T r32 = r * sr;
+        const B sM = B(sqrt(P.M));
+        const T Om = T(sM) / (r32 + a * sM);
+        const T D = r32 - B(3.0) * M * sr + B(2.0) * a * sM;
+        ut = (r32 + a * sM) / (tsqrt(r32) * tsqrt(D));
+        up = ut * Om;
+    } else {
+        // rotating conical jet accelerating through the nozzle
+        const T w = -(gtp / (gpp + B(kNoDivZero)));
+        T Om = B(0.9) / (sn * r);
+        if ((double)val(Om) > P.omega_jet) Om = T(B(P.omega_jet));
+        const T inv_lapse = tsqrt(Aa / (Sig * Del));
+        T acc = (r - B(P.r_nozzle)) * B(P.nozzle_acc);
+        if ((double)val(acc) > P.gamma_max) acc = T(B(P.gamma_max));
+        const T G = acc + B(P.gamma_min);
+        ut = G * inv_lapse;
+        const T dw = Om - w;
+        const T ur2 = (G * G - B(1.0) - gpp * ut * ut * dw * dw) / grr;
+        if (!((double)val(ur2) > 0)) return o;  // the reference's sqrt of a negative: no emitter here
+        ur = tsqrt(ur2);
+        up = ut * Om;
+    }
+    const T u_t = gtt * ut + gtp * up, u_r = grr * ur, u_p = gtp * ut + gpp * up;
+    const T g = -(u_t * kt + u_r * kr + u_p * kph);
+    o.g = g;
+    if (zone == 1) {
+        o.cj = T(B(P.disk_a));
+        o.nus = T(B(P.disk_T));
+        o.zone = 1;
+        o.on = true;
+        return o;
+    }
+    // field: global B = (0, 0, B^phi) into the fluid frame (transform_B_b),
+    // with the reference's magnitude sum_mu (sum_i g_{i mu}) b_mu^2
+    const T b1 = u_p * B(P.b_phi);
+    const T b2 = b1 * ur / ut;
+    const T b4 = (T(B(P.b_phi)) + b1 * up) / ut;
+    T bmag2 = (gtt + gtp) * b1 * b1 + grr * b2 * b2 + (gtp + gpp) * b4 * b4;
+    if ((double)val(bmag2) < 1e-12) bmag2 = T(B(1e-12));
+    // cos^2 of the field-ray angle (calc_b_angle) + no_div_zero
+    const T bk = b1 * (gtt * kt + gtp * kph) + b2 * (grr * kr) + b4 * (gtp * kt + gpp * kph);
+    T c2 = bk * bk / (bmag2 * g * g);
+    if ((double)val(c2) > 1.0) c2 = T(B(1.0));
+    c2 = c2 + B(kNoDivZero);
+    T s2b = T(B(1.0)) - c2;
+    if ((double)val(s2b) < 1e-12) s2b = T(B(1e-12));
+    const T sinb = tsqrt(s2b);
+    const T bmag = tsqrt(bmag2);
+    const T nuc = bmag * B(9.34e-11);  // cyclotron frequency, nm^-1
+    // anisotropy Phi = (1 - 0.99 cos^2)^(-p/2) / Approx_P_synch(p)
+    const T phi = texp(tlog(T(B(1.0)) - B(0.99) * c2) * B(-0.5 * P.p_index)) * B(P.inv_p_synch);
+    o.cj = bmag * sinb * phi * B(P.j_scale);  // J0
+    o.nus = phi * B(P.a_scale);               // A0
+    o.th = T(B(1.0)) / (nuc * sinb);           // 1 / (nu_c sin theta_B)
+    o.zone = 2;
+    o.on = true;
+    return o;
+}
+
+// Slopes of one bin without exp(-tau) (as torus_bin): nu = g nu_c in nm^-1.
+// Disk: a = a_nu, j = a B_nu(T); jet: j = J0 s^-(p-1)/2, a = A0 / nu s^-(p+2)/2,
+// s = nu / (nu_cyc sin theta_B) (calc_radiative_coefficients).
+template <class T>
+RTW_HD void powehi_bin(const PowehiDev& P, const TorusPt<T>& S, double nu_nm, T& ft, T& fi) {
+    typedef decltype(val(S.g)) B;
+    const T g = S.g;
+    if (S.zone == 1) {
+        const T x = g * B(kFFactor * nu_nm) / S.nus;
+        ft = -(S.cj / g);
+        fi = ft * B(kEmissionScale) / texpm1(x);
+        return;
+    }
+    const T nu = g * B(nu_nm);
+    const T ls = tlog(nu * S.th);
+    const T j = S.cj * texp(ls * B(-0.5 * (P.p_index - 1.0)));
+    const T an = S.nus / nu * texp(ls * B(-0.5 * (P.p_index + 2.0)));
+    fi = -(j / (g * nu * nu * nu));
+    ft = -(an / g);
 }
 
 // torus_bin in FP64 with its partial derivatives in (cj, nus, Theta, g), from

@@ -227,6 +227,8 @@ _WORLDS = {
     # initialization.jl:110-119
     "minkowski_t,r,θ,ϕ_sphere": (abi.SCENE_MINKOWSKI_SPHERE, [0, 4, PI / 2, 0], [PI / 2, 0],
                                  [0.0, 0.0, -PI / 2], 0.0),
+    # initialization.jl:100-109 (Powehi.source, the M87* model)
+    "m87": (abi.SCENE_KERR_POWEHI, [0, 35, 0.3, 0], [PI / 2, PI / 6], [0.0, 0.0, PI], 0.0),
 }
 
 _current: World | None = None
@@ -240,8 +242,8 @@ def available_worlds() -> list:
 def initialize_world(input_string: str):
     """Selects a scene and returns its default (position, direction, pointing, beta)
     (initialization.jl:78-172). Scenes that need the reference's missing textures
-    (wormhole, Cartesian sphere) and the M87*/synchrotron work-in-progress scenes
-    are not on this library's path and raise ValueError."""
+    (wormhole, Cartesian sphere) and the flat-space synchrotron test are not on
+    this library's path and raise ValueError."""
     global _current
     key = input_string.lower()
     if key not in _WORLDS:
@@ -283,7 +285,7 @@ def gen_image(*, camera_pos=(0, 0, 0, 0), camera_dir=(0.0, 0.0), speed=0.0, came
                           tolerance, int(max_steps))
     if print_num_pix:
         print("Number of Pixels ", cam.x_pix * cam.y_pix)
-    prec = {"fp64": abi.PREC_FP64, "mixed": abi.PREC_MIXED}[precision]
+    prec = {"fp64": abi.PREC_FP64, "mixed": abi.PREC_MIXED, "fp64_plain": abi.PREC_FP64_PLAIN}[precision]
     integ = {"ref_compat": abi.DP45_REF_COMPAT, "fsal": abi.DP45_FSAL}[integrator]
     want = ("xyz", "class", "steps") + (("spectrum", "state", "tau") if returnrays else ())
     res = r.render(_current.scene, [cam], colors, want=want, precision=prec, integrator=integ,

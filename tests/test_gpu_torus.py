@@ -62,8 +62,9 @@ def test_torus_mixed_parity(renderer, oracle):
 
 def test_torus_rejects(renderer):
     sc, cam, col = _problem(8, 1e-6)
-    with pytest.raises(abi.RTWError):  # the reference step is not built for the torus
-        renderer.render(sc, [cam], col, precision=abi.PREC_MIXED, integrator=abi.DP45_REF_COMPAT)
+    with pytest.raises(abi.RTWError):  # the adjoint needs the FSAL step
+        renderer.adjoint(sc, cam, col, np.zeros((cam.x_pix * cam.x_pix, col.size), np.float32),
+                         precision=abi.PREC_FP64, integrator=abi.DP45_REF_COMPAT)
     with pytest.raises(abi.RTWError):  # one camera per call
         renderer.render(sc, [cam, cam], col, precision=abi.PREC_MIXED, integrator=abi.DP45_FSAL)
     with pytest.raises(abi.RTWError):  # at most 32 bins
@@ -174,3 +175,30 @@ def test_adjoint_ray_subsets_sum_to_the_image(renderer, fd_problem):
         assert np.array_equal(a["spectrum"][mine], full["spectrum"][mine])
     with pytest.raises(abi.RTWError):
         renderer.adjoint(sc, cam, col, target, precision=abi.PREC_FP64, rays=(70, 0, 1))
+
+
+@pytest.mark.parametrize("integrator", [abi.DP45_REF_COMPAT, abi.DP45_FSAL])
+@pytest.mark.parametrize("precision", [abi.PREC_FP64, abi.PREC_MIXED])
+def test_powehi_parity(renderer, oracle, integrator, precision):
+    """Powehi (the reference's M87* scene, "m87" camera): disk + power-law
+    synchrotron jet through the per-bin kernel, against the oracle. FP64:
+    class >= 99.9 %, linear Y within 1e-3 on >= 99.9 %. FP32-mixed: class >=
+    99 %; Y within 1e-3 on >= 98 % with the FSAL step, on >= 95 % with the
+    reference's step, which is not convergent (its images differ from FSAL by
+    ~0.5 %), so FP32 and FP64 rounding, taking slightly different step
+    sequences, differ by that much on the optically thin jet."""
+    from tests.parity import summarize
+    sc = configs.powehi_scene()
+    cam = configs.powehi_camera(24, 1e-6)
+    col = np.array([400.0, 550.0, 700.0])
+    ref = oracle.render(sc, cam, col, integrator=integrator)
+    g = renderer.render(sc, [cam], col, want=("xyz", "class", "steps", "spectrum"), precision=precision,
+                        integrator=integrator)
+    s = summarize(g, ref)
+    print("powehi", integrator, precision, s)
+    assert np.mean(ref["xyz"][:, 1] > 0) > 0.3  # the jet and disk are in view
+    if precision == abi.PREC_FP64:
+        assert s["class_match"] >= 0.999 and s["frac_within_1e-3"] >= 0.999, s
+    else:
+        bar = 0.98 if integrator == abi.DP45_FSAL else 0.95
+        assert s["class_match"] >= 0.99 and s["frac_within_1e-3"] >= bar, s

@@ -101,3 +101,24 @@ def test_vjp_matches_central_differences():
             fd = (cot @ rhs(y, **{name: base + h}) - cot @ rhs(y, **{name: base - h})) / (2 * h)
             assert abs(fd - pb[q]) <= 1e-5 * abs(fd), (r, th, name, fd, pb[q])
         assert pb[1] == 0  # the inclination enters only the initial data
+
+
+POWEHI_POINTS = [(5.0, np.pi / 2), (8.0, 1.56), (20.0, 0.05), (40.0, 0.02), (60.0, 3.1), (15.0, 0.07), (30.0, 1.0)]
+
+
+def test_powehi_rhs_matches_oracle(oracle):
+    """Powehi (disk zone, jet zone near either pole, empty space): the
+    library's per-bin right-hand side against the oracle's restatement of
+    Powehi.source/source_model.jl."""
+    sc = configs.powehi_scene()
+    col = np.array([400.0, 550.0, 700.0])
+    rng = np.random.default_rng(1)
+    for r, th in POWEHI_POINTS:
+        y = _state(sc, 3, r, th, rng)
+        y[2] = th
+        ref = oracle.rhs(sc, col, y)
+        f = abi.torus_rhs(sc, col, y, 0)
+        scale = 1e-12 * max(np.abs(ref).max(), 1e-300)
+        err = np.abs(f - ref) / np.maximum(np.abs(ref), scale)
+        assert err.max() < 1e-11, (r, th, err.max())
+    assert abi.scene_default(abi.SCENE_KERR_POWEHI).spin == pytest.approx(0.9, rel=1e-7)
