@@ -396,6 +396,15 @@ rtw_status rtw_torus_rhs(const rtw_scene* scene, const double* colors_nm, int32_
 rtw_status rtw_torus_vjp(const rtw_scene* scene, const double* colors_nm, int32_t n_colors,
                          const double* state, const double* cot, double* mu, double* pbar);
 
+/* Host FP64 reverse of one FSAL Dormand-Prince step of size h from state of
+ * the torus (reference layout): mu = the cotangent of the start state given
+ * cot for the end state, pbar the parameter part, hbar = d loss / d h; form 0
+ * is the adjoint kernel's structured reverse, form 1 the generic one over the
+ * whole state. For tests. */
+rtw_status rtw_torus_step_vjp(const rtw_scene* scene, const double* colors_nm, int32_t n_colors,
+                              const double* state, double h, const double* cot, int32_t form, double* mu,
+                              double* pbar, double* hbar);
+
 /* Host FP64 polar escape of the torus (n_sub sub-steps z <- keep(z - temp
  * f(z)), temp from the state; Kerr source_geometry.jl:249-269 with
  * integrators_LttM.jl:62-105) and the adjoint kernel's vector-Jacobian product

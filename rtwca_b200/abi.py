@@ -161,6 +161,9 @@ SIGNATURES = {
                                 C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "rtw_torus_vjp": (C.c_int, [C.POINTER(Scene), C.POINTER(C.c_double), C.c_int32, C.POINTER(C.c_double),
                                 C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "rtw_torus_step_vjp": (C.c_int, [C.POINTER(Scene), C.POINTER(C.c_double), C.c_int32, C.POINTER(C.c_double),
+                                     C.c_double, C.POINTER(C.c_double), C.c_int32, C.POINTER(C.c_double),
+                                     C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "rtw_torus_escape_vjp": (C.c_int, [C.POINTER(Scene), C.POINTER(C.c_double), C.c_int32, C.POINTER(C.c_double),
                                        C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                        C.POINTER(C.c_double), C.POINTER(C.c_double)]),
@@ -301,3 +304,19 @@ def torus_escape_vjp(scene: Scene, colors_nm, state, n_sub: int, cot):
     if r not in (OK, ERR_NAN):
         check(r, "torus_escape_vjp")
     return end, mu, pb, r == OK
+
+
+def torus_step_vjp(scene: Scene, colors_nm, state, h: float, cot, form: int = 0):
+    """Host reverse of one torus DP45 step: (J^T cot, d/d params, d/d h)."""
+    import numpy as np
+    c = np.ascontiguousarray(colors_nm, dtype=np.float64)
+    st = np.ascontiguousarray(state, dtype=np.float64)
+    ct = np.ascontiguousarray(cot, dtype=np.float64)
+    mu = np.zeros_like(st)
+    pb = np.zeros(5)
+    hb = C.c_double(0)
+    dp = C.POINTER(C.c_double)
+    check(load().rtw_torus_step_vjp(C.byref(scene), c.ctypes.data_as(dp), int(c.size), st.ctypes.data_as(dp),
+                                    float(h), ct.ctypes.data_as(dp), int(form), mu.ctypes.data_as(dp),
+                                    pb.ctypes.data_as(dp), C.byref(hb)), "torus_step_vjp")
+    return mu, pb, hb.value

@@ -609,25 +609,33 @@ struct TorusRP {
 // One recorded step of a ray, replayed in FP64: y_out = keep(step(y_in)).
 RTW_HD bool torus_is_dp(uint8_t kind) { return kind == 0 || (kind & 0x40); }
 
+// The six stage slopes K[s][D] of one recorded FSAL step of size h from y
+// (the replay's arithmetic). Y: [D] scratch. Returns y' in y_out unless null.
+RTW_HD void torus_dp_stages(const TorusModel& m, const double* y, double h, double* K, double* Y, double* y_out) {
+    const int D = 8 + 2 * m.n;
+    torus_f64(m, y, K);
+    for (int s = 1; s < 6; ++s) {
+        for (int i = 0; i < D; ++i) {
+            double acc = 0;
+            for (int j = 0; j < s; ++j) acc += tA(s, j) * K[j * D + i];
+            Y[i] = y[i] + h * acc;
+        }
+        torus_f64(m, Y, K + s * D);
+    }
+    if (y_out)
+        for (int i = 0; i < D; ++i) {
+            double acc = 0;
+            for (int j = 0; j < 6; ++j) acc += tA(6, j) * K[j * D + i];
+            y_out[i] = y[i] + h * acc;
+        }
+}
+
 __device__ bool torus_replay(const TorusModel& m, const double* y_in, uint8_t kind, double hv, double* y_out,
                              double* K, double* Y) {
     const int N = m.n, D = 8 + 2 * N;
     if (torus_is_dp(kind)) {
         // K: [6][D] stage slopes, Y: [D] a stage point
-        torus_f64(m, y_in, K);
-        for (int s = 1; s < 6; ++s) {
-            for (int i = 0; i < D; ++i) {
-                double acc = 0;
-                for (int j = 0; j < s; ++j) acc += tA(s, j) * K[j * D + i];
-                Y[i] = y_in[i] + hv * acc;
-            }
-            torus_f64(m, Y, K + s * D);
-        }
-        for (int i = 0; i < D; ++i) {
-            double acc = 0;
-            for (int j = 0; j < 6; ++j) acc += tA(6, j) * K[j * D + i];
-            y_out[i] = y_in[i] + hv * acc;
-        }
+        torus_dp_stages(m, y_in, hv, K, Y, y_out);
         return torus_keep(y_out);
     }
     for (int i = 0; i < D; ++i) y_out[i] = y_in[i];
@@ -722,13 +730,177 @@ RTW_HD bool torus_escape_vjp(const TorusModel& m, const double* y, int nsub, dou
     return true;
 }
 
+// Reverse of one step y' = y + h sum_s b_s K_s, K_s = f(Y_s), Y_s = y + h
+// sum_{j<s} A_sj K_j, written over the whole state with the generic VJP
+// (the reference form the structured torus_dp_vjp is checked against).
+// lam: the cotangent of y' in, of y out; returns d loss / d h.
+// Scratch: Yst, kac [6][D], mu [D].
+RTW_HD double torus_dp_vjp_generic(const TorusModel& m, const double* y, const double* K, double h, double* lam,
+                                   double* pb, double* Yst, double* kac, double* mu) {
+    const int D = 8 + 2 * m.n;
+    for (int i = 0; i < D; ++i) Yst[i] = y[i];
+    for (int s = 1; s < 6; ++s)
+        for (int i = 0; i < D; ++i) {
+            double acc = 0;
+            for (int j = 0; j < s; ++j) acc += tA(s, j) * K[j * D + i];
+            Yst[s * D + i] = y[i] + h * acc;
+        }
+    double hbar = 0;
+    for (int i = 0; i < D; ++i) {
+        double bk = 0;
+        for (int s = 0; s < 6; ++s) bk += tA(6, s) * K[s * D + i];
+        hbar += lam[i] * bk;
+    }
+    for (int s = 0; s < 6; ++s)
+        for (int i = 0; i < D; ++i) kac[s * D + i] = h * tA(6, s) * lam[i];
+    for (int t = 5; t >= 0; --t) {
+        for (int i = 0; i < D; ++i) mu[i] = 0;
+        torus_vjp(m, Yst + t * D, kac + t * D, mu, pb);
+        for (int i = 0; i < D; ++i) lam[i] += mu[i];
+        for (int i = 0; i < D && t > 0; ++i) {
+            double ak = 0;
+            for (int s = 0; s < t; ++s) ak += tA(t, s) * K[s * D + i];
+            hbar += mu[i] * ak;
+        }
+        for (int s = 0; s < t; ++s) {
+            const double w = h * tA(t, s);
+            if (w != 0)
+                for (int i = 0; i < D; ++i) kac[s * D + i] += w * mu[i];
+        }
+    }
+    return hbar;
+}
+
+// The same reverse step, structured: the bins' (tau, I) cotangents never
+// depend on the geodesic ones (d f_geo / d bins = 0 and each bin's block
+// couples only to itself), so (1) the emitter numbers of the six stage points
+// and their tangents are formed once, (2) each bin runs its six-stage
+// recursion in registers from its own twelve stage slopes and adds to the
+// cotangents of the emitter numbers, (3) the eight geodesic components run
+// theirs. Same result as torus_dp_vjp_generic; far less memory traffic.
+RTW_HD double torus_dp_vjp(const TorusModel& m, const double* y, const double* K, double h, double* lam, double* pb) {
+    const int N = m.n, D = 8 + 2 * N;
+    typedef Dual<double, 8> D8;  // r, theta, k^t, k^phi, a, n0, b0, th0
+    double Yg[6][8];
+    for (int t = 0; t < 6; ++t)
+        for (int i = 0; i < 8; ++i) {
+            double acc = 0;
+            for (int s = 0; s < t; ++s) acc += tA(t, s) * K[s * D + i];
+            Yg[t][i] = y[i] + h * acc;
+        }
+    double Sv[6][4], dS[6][4][8], Sbar[6][4];
+    bool on[6];
+    for (int t = 0; t < 6; ++t) {
+        const TorusPt<D8> S = torus_point<D8>(m.tor, D8::var(m.tor.a, 4), D8::var(m.tor.n0, 5), D8::var(m.tor.B0, 6),
+                                              D8::var(m.tor.Th0, 7), D8::var(Yg[t][1], 0), D8::var(Yg[t][2], 1),
+                                              D8::var(Yg[t][4], 2), D8::var(Yg[t][7], 3));
+        on[t] = S.on;
+        const D8* comp[4] = {&S.cj, &S.nus, &S.th, &S.g};
+        for (int q = 0; q < 4; ++q) {
+            Sv[t][q] = comp[q]->v;
+            Sbar[t][q] = 0;
+            for (int u = 0; u < 8; ++u) dS[t][q][u] = comp[q]->d[u];
+        }
+    }
+    double hbar = 0;
+    // (2) bins
+    for (int c = 0; c < N; ++c) {
+        const int it = 8 + c, ii = 8 + N + c;
+        double Kt[6], Ki[6], taut[6], kt[6], ki[6];
+        const double lt = lam[it], li = lam[ii];
+        double bkt = 0, bki = 0;
+        for (int s = 0; s < 6; ++s) {
+            Kt[s] = K[s * D + it];
+            Ki[s] = K[s * D + ii];
+            bkt += tA(6, s) * Kt[s];
+            bki += tA(6, s) * Ki[s];
+            kt[s] = h * tA(6, s) * lt;
+            ki[s] = h * tA(6, s) * li;
+        }
+        hbar += lt * bkt + li * bki;
+        for (int t = 0; t < 6; ++t) {
+            double acc = 0;
+            for (int s = 0; s < t; ++s) acc += tA(t, s) * Kt[s];
+            taut[t] = y[it] + h * acc;
+        }
+        double msum = 0;
+        for (int t = 5; t >= 0; --t) {
+            if (!on[t]) continue;  // no emitter: the bin's slopes are 0 there
+            double ft, fi, dft[4], dfi[4];
+            torus_bin_grad(Sv[t][0], Sv[t][1], Sv[t][2], Sv[t][3], m.bins[c], ft, fi, dft, dfi);
+            const double e = exp(-taut[t]);
+            for (int q = 0; q < 4; ++q) Sbar[t][q] += kt[t] * dft[q] + ki[t] * e * dfi[q];
+            const double mt = -ki[t] * fi * e;  // d (fi exp(-tau)) / d tau
+            msum += mt;
+            double ak = 0;
+            for (int s = 0; s < t; ++s) {
+                ak += tA(t, s) * Kt[s];
+                kt[s] += h * tA(t, s) * mt;
+            }
+            hbar += mt * ak;
+        }
+        lam[it] = lt + msum;
+    }
+    // (3) geodesic components
+    double kg[6][8], lg[8];
+    for (int i = 0; i < 8; ++i) {
+        double bk = 0;
+        for (int s = 0; s < 6; ++s) bk += tA(6, s) * K[s * D + i];
+        hbar += lam[i] * bk;
+        lg[i] = lam[i];
+        for (int s = 0; s < 6; ++s) kg[s][i] = h * tA(6, s) * lam[i];
+    }
+    typedef Dual<double, 7> D7;  // r, theta, k^t, k^r, k^theta, k^phi, a
+    for (int t = 5; t >= 0; --t) {
+        double mu[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        for (int i = 0; i < 4; ++i) mu[4 + i] += kg[t][i];
+        {
+            const D7 r = D7::var(Yg[t][1], 0), th = D7::var(Yg[t][2], 1), a = D7::var(m.tor.a, 6);
+            D7 k[4], acc[4];
+            for (int i = 0; i < 4; ++i) k[i] = D7::var(Yg[t][4 + i], 2 + i);
+            kerr_accel<D7>(m.tor.M, a, r, th, k, acc);
+            for (int i = 0; i < 4; ++i) {
+                const double cw = kg[t][4 + i];
+                if (cw == 0) continue;
+                mu[1] += cw * acc[i].d[0];
+                mu[2] += cw * acc[i].d[1];
+                for (int q = 0; q < 4; ++q) mu[4 + q] += cw * acc[i].d[2 + q];
+                pb[0] += cw * acc[i].d[6];
+            }
+        }
+        if (on[t]) {
+            double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+            for (int q = 0; q < 4; ++q)
+                for (int u = 0; u < 8; ++u) v[u] += Sbar[t][q] * dS[t][q][u];
+            mu[1] += v[0];
+            mu[2] += v[1];
+            mu[4] += v[2];
+            mu[7] += v[3];
+            pb[0] += v[4];
+            pb[2] += v[5];
+            pb[3] += v[6];
+            pb[4] += v[7];
+        }
+        for (int i = 0; i < 8; ++i) {
+            lg[i] += mu[i];
+            double ak = 0;
+            for (int s = 0; s < t; ++s) {
+                ak += tA(t, s) * K[s * D + i];
+                kg[s][i] += h * tA(t, s) * mu[i];
+            }
+            hbar += mu[i] * ak;
+        }
+    }
+    for (int i = 0; i < 8; ++i) lam[i] = lg[i];
+    return hbar;
+}
+
 constexpr int kTorusMaxD = 8 + 2 * kTorusMaxBins;  // state components
 constexpr int kTorusMaxCk = 16;                     // recorded steps per checkpoint
 
 // Reverse kernel (FP64). Per lane work area, D = 8 + 2N doubles per row:
 //   Ys [ck_every + 1] segment states, Ks [ck_every][6] the stage slopes of
-//   each replayed step, Yst [6] stage points, kac [6] stage cotangents,
-//   Ze [4] escape evaluations, lam, mu, tmp [1] each.
+//   each replayed step, Ze [4] escape evaluations, lam, mu, tmp [1] each.
 __global__ void __launch_bounds__(128) torus_reverse(const TorusRP p) {
     const TorusModel& m = p.f.m;
     const int N = m.n, D = 8 + 2 * N;
@@ -736,7 +908,7 @@ __global__ void __launch_bounds__(128) torus_reverse(const TorusRP p) {
     // warp, so that the lanes' same-index accesses coalesce (rows of D)
     double Ys[(kTorusMaxCk + 1) * kTorusMaxD];
     double Ks[kTorusMaxCk * 6 * kTorusMaxD];
-    double Yst[6 * kTorusMaxD], kac[6 * kTorusMaxD], Ze[4 * kTorusMaxD];
+    double Ze[4 * kTorusMaxD];
     double lam[kTorusMaxD], mu[kTorusMaxD], tmp[kTorusMaxD];
     unsigned n_cut = 0;
     for (;;) {
@@ -776,7 +948,7 @@ __global__ void __launch_bounds__(128) torus_reverse(const TorusRP p) {
                 const uint8_t kind = p.f.ev_kind[eo + e];
                 const double hv = p.f.ev_h[eo + e];
                 const bool r = torus_replay(m, Ys + (long long)(e - e0) * D, kind, hv,
-                                            Ys + (long long)(e - e0 + 1) * D, Ks + (long long)(e - e0) * 6 * D, Yst);
+                                            Ys + (long long)(e - e0 + 1) * D, Ks + (long long)(e - e0) * 6 * D, tmp);
                 if (torus_is_dp(kind) && r) refl |= 1ull << (e - e0);
             }
             for (int e = e1 - 1; e >= e0; --e) {
@@ -788,41 +960,8 @@ __global__ void __launch_bounds__(128) torus_reverse(const TorusRP p) {
                         lam[2] = -lam[2];
                         lam[6] = -lam[6];
                     }
-                    // the step's stage slopes from the replay; stage points rebuilt
-                    // with the replay's own arithmetic
                     const double* Kst = Ks + (long long)(e - e0) * 6 * D;
-                    for (int i = 0; i < D; ++i) Yst[i] = y[i];
-                    for (int s = 1; s < 6; ++s)
-                        for (int i = 0; i < D; ++i) {
-                            double acc = 0;
-                            for (int j = 0; j < s; ++j) acc += tA(s, j) * Kst[j * D + i];
-                            Yst[s * D + i] = y[i] + hv * acc;
-                        }
-                    // y' = y + h sum_s b_s K_s, K_s = f(Y_s), Y_s = y + h sum_{j<s} A_sj K_j;
-                    // hbar = d loss / d h, for step sizes set by pad_max_dt
-                    double hbar = 0;
-                    for (int i = 0; i < D; ++i) {
-                        double bk = 0;
-                        for (int s = 0; s < 6; ++s) bk += tA(6, s) * Kst[s * D + i];
-                        hbar += lam[i] * bk;
-                    }
-                    for (int s = 0; s < 6; ++s)
-                        for (int i = 0; i < D; ++i) kac[s * D + i] = hv * tA(6, s) * lam[i];
-                    for (int t = 5; t >= 0; --t) {
-                        for (int i = 0; i < D; ++i) mu[i] = 0;
-                        torus_vjp(m, Yst + t * D, kac + t * D, mu, pb);
-                        for (int i = 0; i < D; ++i) lam[i] += mu[i];
-                        for (int i = 0; i < D && t > 0; ++i) {
-                            double ak = 0;
-                            for (int s = 0; s < t; ++s) ak += tA(t, s) * Kst[s * D + i];
-                            hbar += mu[i] * ak;
-                        }
-                        for (int s = 0; s < t; ++s) {
-                            const double w = hv * tA(t, s);
-                            if (w != 0)
-                                for (int i = 0; i < D; ++i) kac[s * D + i] += w * mu[i];
-                        }
-                    }
+                    const double hbar = torus_dp_vjp(m, y, Kst, hv, lam, pb);
                     // a pending step-size term of the next step lands on this state
                     if (pend != 0) torus_pad_vjp(y, p.f.max_dt_scale, pend, lam);
                     pend = 0;
@@ -1252,7 +1391,7 @@ rtw_status rtw_adjoint(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* c
     RTW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, torus_reverse, 128, 0), "occupancy");
     const int rgrid = ctx->num_sms * std::max(1, occ);
     // local-memory work area of the reverse kernel (per resident thread)
-    const size_t work_b = (size_t)rgrid * 128 * (size_t)(kTorusMaxCk + 1 + 6 * kTorusMaxCk + 6 + 6 + 4 + 3) *
+    const size_t work_b = (size_t)rgrid * 128 * (size_t)(kTorusMaxCk + 1 + 6 * kTorusMaxCk + 4 + 3) *
                           kTorusMaxD * 8;
     const size_t per_ray_b = adj->per_ray_grad ? (size_t)P * kTorusParams * 8 : 0;
     if ((st = ensure(ctx, &b->work, &b->work_cap, std::max<size_t>(per_ray_b, 256))) != RTW_OK) return st;
@@ -1378,6 +1517,39 @@ rtw_status rtw_torus_escape_vjp(const rtw_scene* scene, const double* colors_nm,
     }
     for (int q = 0; q < kTorusParams; ++q) pbar[q] = pb[q];
     return ok ? RTW_OK : RTW_ERR_NAN;
+}
+
+rtw_status rtw_torus_step_vjp(const rtw_scene* scene, const double* colors_nm, int32_t n_colors,
+                              const double* state, double h, const double* cot, int32_t form, double* mu,
+                              double* pbar, double* hbar) {
+    if (!scene || !state || !cot || !mu || !pbar || !hbar || scene->kind != RTW_SCENE_KERR_SYNCHRO_TORUS)
+        return RTW_ERR_INVALID_PARAM;
+    TorusModel m;
+    std::string why;
+    if (torus_model(*scene, colors_nm, n_colors, m, why) != RTW_OK) return RTW_ERR_INVALID_PARAM;
+    const int N = n_colors, D = 8 + 2 * N;
+    std::vector<double> y(D), lam(D), K(6 * D), Y(D), Yst(6 * D), kac(6 * D), tmp(D);
+    for (int i = 0; i < 8; ++i) {
+        y[i] = state[i];
+        lam[i] = cot[i];
+    }
+    for (int c = 0; c < N; ++c) {
+        y[8 + N + c] = state[8 + 2 * c];
+        y[8 + c] = state[9 + 2 * c];
+        lam[8 + N + c] = cot[8 + 2 * c];
+        lam[8 + c] = cot[9 + 2 * c];
+    }
+    torus_dp_stages(m, y.data(), h, K.data(), Y.data(), nullptr);
+    double pb[kTorusParams] = {0, 0, 0, 0, 0};
+    *hbar = form == 0 ? torus_dp_vjp(m, y.data(), K.data(), h, lam.data(), pb)
+                      : torus_dp_vjp_generic(m, y.data(), K.data(), h, lam.data(), pb, Yst.data(), kac.data(), tmp.data());
+    for (int i = 0; i < 8; ++i) mu[i] = lam[i];
+    for (int c = 0; c < N; ++c) {
+        mu[8 + 2 * c] = lam[8 + N + c];
+        mu[9 + 2 * c] = lam[8 + c];
+    }
+    for (int q = 0; q < kTorusParams; ++q) pbar[q] = pb[q];
+    return RTW_OK;
 }
 
 rtw_status rtw_torus_vjp(const rtw_scene* scene, const double* colors_nm, int32_t n_colors, const double* state,
