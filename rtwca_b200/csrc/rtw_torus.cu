@@ -88,8 +88,8 @@ RTW_HD void em_bin(const TorusModel& m, const TorusPt<R>& S, int c, R& ft, R& fi
 }
 
 // FP64 right-hand side on a state y[8 + 2N] = (x^mu, k^mu, tau_c, I_c).
-RTW_HD void torus_f64(const TorusModel& m, const double* y, double* f) {
-    const int N = m.n;
+// The geodesic part of the right-hand side (8 components of y).
+RTW_HD void torus_geo_rhs(const TorusModel& m, const double* y, double* f) {
     double z[10], k[9];
     for (int i = 0; i < 8; ++i) z[i] = y[i];
     z[8] = 0;
@@ -97,6 +97,11 @@ RTW_HD void torus_f64(const TorusModel& m, const double* y, double* f) {
     Emit<double> em;
     KerrScene<false>::rhs<double>(m.geo, z, k, em);
     for (int i = 0; i < 8; ++i) f[i] = k[i];
+}
+
+RTW_HD void torus_f64(const TorusModel& m, const double* y, double* f) {
+    const int N = m.n;
+    torus_geo_rhs(m, y, f);
     const TorusPt<double> S = em_point<double>(m, y);
     for (int c = 0; c < N; ++c) {
         double ft = 0, fi = 0;
@@ -584,6 +589,15 @@ __global__ void __launch_bounds__(128) torus_forward(const TorusKP p) {
         }
         if (p.cls) p.cls[id] = (uint8_t)cls;
         if (p.steps) p.steps[id] = (uint32_t)nsteps;
+        if (p.record && !bad && n_ev == ev_cap) {
+            // the final state closes the last segment (one row after the segments')
+            double* c = p.ck + (co + (ev_cap + kc - 1) / kc) * (unsigned long long)D;
+            for (int i = 0; i < 8; ++i) c[i] = x[i];
+            for (int q = 0; q < N; ++q) {
+                c[8 + q] = (double)tau[q];
+                c[8 + N + q] = (double)ihi[q] + (MIXED ? (double)ilo[q] : 0.0);
+            }
+        }
         if (!p.record && p.n_events) p.n_events[loc] = n_ev | (escaped ? kDenseCheckpoints : 0u);
         if (p.record && (bad || n_ev != ev_cap)) atomicOr(p.err_flag, 1u);
     }
@@ -730,6 +744,28 @@ RTW_HD bool torus_escape_vjp(const TorusModel& m, const double* y, int nsub, dou
     return true;
 }
 
+// The geodesic part of one recorded FSAL step alone (bit-identical to the
+// geodesic components of torus_dp_stages: the bins never enter them).
+// Kg [6][8] the stage slopes; g_out = keep(g + h sum b Kg); returns whether
+// keep reflected theta through the pole.
+RTW_HD bool torus_geo_step(const TorusModel& m, const double* g, double h, double* Kg, double* g_out) {
+    double Y[8];
+    for (int t = 0; t < 6; ++t) {
+        for (int i = 0; i < 8; ++i) {
+            double acc = 0;
+            for (int s = 0; s < t; ++s) acc += tA(t, s) * Kg[s * 8 + i];
+            Y[i] = g[i] + h * acc;
+        }
+        torus_geo_rhs(m, Y, Kg + t * 8);
+    }
+    for (int i = 0; i < 8; ++i) {
+        double acc = 0;
+        for (int s = 0; s < 6; ++s) acc += tA(6, s) * Kg[s * 8 + i];
+        g_out[i] = g[i] + h * acc;
+    }
+    return torus_keep(g_out);
+}
+
 // Reverse of one step y' = y + h sum_s b_s K_s, K_s = f(Y_s), Y_s = y + h
 // sum_{j<s} A_sj K_j, written over the whole state with the generic VJP
 // (the reference form the structured torus_dp_vjp is checked against).
@@ -774,18 +810,26 @@ RTW_HD double torus_dp_vjp_generic(const TorusModel& m, const double* y, const d
 // The same reverse step, structured: the bins' (tau, I) cotangents never
 // depend on the geodesic ones (d f_geo / d bins = 0 and each bin's block
 // couples only to itself), so (1) the emitter numbers of the six stage points
-// and their tangents are formed once, (2) each bin runs its six-stage
-// recursion in registers from its own twelve stage slopes and adds to the
-// cotangents of the emitter numbers, (3) the eight geodesic components run
-// theirs. Same result as torus_dp_vjp_generic; far less memory traffic.
-RTW_HD double torus_dp_vjp(const TorusModel& m, const double* y, const double* K, double h, double* lam, double* pb) {
-    const int N = m.n, D = 8 + 2 * N;
+// and their tangents are formed once, (2) each bin re-forms its twelve stage
+// slopes from them (the closed-form partials return the values too) and runs
+// its six-stage recursion in registers, adding to the cotangents of the
+// emitter numbers, (3) the eight geodesic components run theirs. Only the
+// step's geodesic start state yg [8], its geodesic stage slopes Kg [6][8] and
+// the bins' optical depths tau [N] are read: same result as
+// torus_dp_vjp_generic at a fraction of its memory traffic. The tau slopes
+// depend on the geodesic alone (tau' = ft(emitter numbers)), so with
+// tau_at_end the step is run backwards for tau: tau holds the depths at the
+// end of the step on entry and those at its start on return (the intensities
+// enter no slope, so the reverse sweep never needs them).
+RTW_HD double torus_dp_vjp(const TorusModel& m, const double* y, const double* Kg, double* tau, bool tau_at_end,
+                           double h, double* lam, double* pb) {
+    const int N = m.n;
     typedef Dual<double, 8> D8;  // r, theta, k^t, k^phi, a, n0, b0, th0
     double Yg[6][8];
     for (int t = 0; t < 6; ++t)
         for (int i = 0; i < 8; ++i) {
             double acc = 0;
-            for (int s = 0; s < t; ++s) acc += tA(t, s) * K[s * D + i];
+            for (int s = 0; s < t; ++s) acc += tA(t, s) * Kg[s * 8 + i];
             Yg[t][i] = y[i] + h * acc;
         }
     double Sv[6][4], dS[6][4][8], Sbar[6][4];
@@ -806,31 +850,33 @@ RTW_HD double torus_dp_vjp(const TorusModel& m, const double* y, const double* K
     // (2) bins
     for (int c = 0; c < N; ++c) {
         const int it = 8 + c, ii = 8 + N + c;
-        double Kt[6], Ki[6], taut[6], kt[6], ki[6];
+        double Kt[6], fi[6], ex[6], dft[6][4] = {}, dfi[6][4] = {}, kt[6];
         const double lt = lam[it], li = lam[ii];
         double bkt = 0, bki = 0;
-        for (int s = 0; s < 6; ++s) {
-            Kt[s] = K[s * D + it];
-            Ki[s] = K[s * D + ii];
-            bkt += tA(6, s) * Kt[s];
-            bki += tA(6, s) * Ki[s];
-            kt[s] = h * tA(6, s) * lt;
-            ki[s] = h * tA(6, s) * li;
+        for (int t = 0; t < 6; ++t) {
+            Kt[t] = fi[t] = 0;
+            if (on[t]) torus_bin_grad(Sv[t][0], Sv[t][1], Sv[t][2], Sv[t][3], m.bins[c], Kt[t], fi[t], dft[t], dfi[t]);
+            bkt += tA(6, t) * Kt[t];
         }
-        hbar += lt * bkt + li * bki;
+        double t0 = tau[c];
+        if (tau_at_end) {
+            t0 -= h * bkt;
+            tau[c] = t0;
+        }
         for (int t = 0; t < 6; ++t) {
             double acc = 0;
             for (int s = 0; s < t; ++s) acc += tA(t, s) * Kt[s];
-            taut[t] = y[it] + h * acc;
+            ex[t] = on[t] ? exp(-(t0 + h * acc)) : 0.0;
+            bki += tA(6, t) * fi[t] * ex[t];
+            kt[t] = h * tA(6, t) * lt;
         }
+        hbar += lt * bkt + li * bki;
         double msum = 0;
         for (int t = 5; t >= 0; --t) {
             if (!on[t]) continue;  // no emitter: the bin's slopes are 0 there
-            double ft, fi, dft[4], dfi[4];
-            torus_bin_grad(Sv[t][0], Sv[t][1], Sv[t][2], Sv[t][3], m.bins[c], ft, fi, dft, dfi);
-            const double e = exp(-taut[t]);
-            for (int q = 0; q < 4; ++q) Sbar[t][q] += kt[t] * dft[q] + ki[t] * e * dfi[q];
-            const double mt = -ki[t] * fi * e;  // d (fi exp(-tau)) / d tau
+            const double ki = h * tA(6, t) * li, e = ex[t];
+            for (int q = 0; q < 4; ++q) Sbar[t][q] += kt[t] * dft[t][q] + ki * e * dfi[t][q];
+            const double mt = -ki * fi[t] * e;  // d (fi exp(-tau)) / d tau
             msum += mt;
             double ak = 0;
             for (int s = 0; s < t; ++s) {
@@ -845,7 +891,7 @@ RTW_HD double torus_dp_vjp(const TorusModel& m, const double* y, const double* K
     double kg[6][8], lg[8];
     for (int i = 0; i < 8; ++i) {
         double bk = 0;
-        for (int s = 0; s < 6; ++s) bk += tA(6, s) * K[s * D + i];
+        for (int s = 0; s < 6; ++s) bk += tA(6, s) * Kg[s * 8 + i];
         hbar += lam[i] * bk;
         lg[i] = lam[i];
         for (int s = 0; s < 6; ++s) kg[s][i] = h * tA(6, s) * lam[i];
@@ -885,7 +931,7 @@ RTW_HD double torus_dp_vjp(const TorusModel& m, const double* y, const double* K
             lg[i] += mu[i];
             double ak = 0;
             for (int s = 0; s < t; ++s) {
-                ak += tA(t, s) * K[s * D + i];
+                ak += tA(t, s) * Kg[s * 8 + i];
                 kg[s][i] += h * tA(t, s) * mu[i];
             }
             hbar += mu[i] * ak;
@@ -898,17 +944,19 @@ RTW_HD double torus_dp_vjp(const TorusModel& m, const double* y, const double* K
 constexpr int kTorusMaxD = 8 + 2 * kTorusMaxBins;  // state components
 constexpr int kTorusMaxCk = 16;                     // recorded steps per checkpoint
 
-// Reverse kernel (FP64). Per lane work area, D = 8 + 2N doubles per row:
-//   Ys [ck_every + 1] segment states, Ks [ck_every][6] the stage slopes of
-//   each replayed step, Ze [4] escape evaluations, lam, mu, tmp [1] each.
-__global__ void __launch_bounds__(128) torus_reverse(const TorusRP p) {
+// Reverse kernel (FP64), one lane per ray. A ray without a polar escape
+// replays each segment's geodesic from its checkpoint (G [ck_every + 1][8]
+// states, Kgs [ck_every][6][8] stage slopes) and runs the bins' optical
+// depths backwards from the segment's end state (the next checkpoint; the
+// last segment ends at the ray's final state); a ray with a polar escape has
+// its full state checkpointed before every event (Ys [2][D], Kw [6][D] stage
+// slopes, Ze [4][D] escape evaluations). The arrays live in local memory,
+// whose layout interleaves the lanes of a warp (same-index accesses coalesce).
+__global__ void __launch_bounds__(128, 4) torus_reverse(const TorusRP p) {
     const TorusModel& m = p.f.m;
     const int N = m.n, D = 8 + 2 * N;
-    // the work area in local memory, whose layout interleaves the lanes of a
-    // warp, so that the lanes' same-index accesses coalesce (rows of D)
-    double Ys[(kTorusMaxCk + 1) * kTorusMaxD];
-    double Ks[kTorusMaxCk * 6 * kTorusMaxD];
-    double Ze[4 * kTorusMaxD];
+    double G[(kTorusMaxCk + 1) * 8], Kgs[kTorusMaxCk * 48], taus[kTorusMaxBins];
+    double Ys[2 * kTorusMaxD], Kw[6 * kTorusMaxD], Ze[4 * kTorusMaxD];
     double lam[kTorusMaxD], mu[kTorusMaxD], tmp[kTorusMaxD];
     unsigned n_cut = 0;
     for (;;) {
@@ -935,40 +983,52 @@ __global__ void __launch_bounds__(128) torus_reverse(const TorusRP p) {
         double pb[kTorusParams] = {0, 0, 0, 0, 0};
         double pend = 0;  // d loss / d h of a step whose h was set at the previous step's start
         const uint32_t n_ev = p.f.n_events[loc] & kEventCount;
-        const int KC = (p.f.n_events[loc] & kDenseCheckpoints) ? 1 : p.f.ck_every;
+        const int KC = escaped ? 1 : p.f.ck_every;
         const unsigned long long eo = p.f.ev_off[loc], co = p.f.ck_off[loc];
         const int nseg = (int)((n_ev + (uint32_t)KC - 1) / (uint32_t)KC);
-        for (int seg = nseg - 1; seg >= 0; --seg) {
-            const int e0 = seg * KC;
-            const int e1 = min(e0 + KC, (int)n_ev);
-            const double* c = p.f.ck + (co + (unsigned long long)seg) * (unsigned long long)D;
-            for (int i = 0; i < D; ++i) Ys[i] = c[i];
-            unsigned long long refl = 0;
-            for (int e = e0; e < e1; ++e) {
-                const uint8_t kind = p.f.ev_kind[eo + e];
-                const double hv = p.f.ev_h[eo + e];
-                const bool r = torus_replay(m, Ys + (long long)(e - e0) * D, kind, hv,
-                                            Ys + (long long)(e - e0 + 1) * D, Ks + (long long)(e - e0) * 6 * D, tmp);
-                if (torus_is_dp(kind) && r) refl |= 1ull << (e - e0);
+        // the reverse of one DP step from geodesic start state g
+        auto dp_step = [&](const double* g, const double* Kg, uint8_t kind, double hv, bool refl, bool tau_at_end) {
+            if (refl) {
+                lam[2] = -lam[2];
+                lam[6] = -lam[6];
             }
-            for (int e = e1 - 1; e >= e0; --e) {
-                const double* y = Ys + (long long)(e - e0) * D;
+            const double hbar = torus_dp_vjp(m, g, Kg, taus, tau_at_end, hv, lam, pb);
+            // a pending step-size term of the next step lands on this state
+            if (pend != 0) torus_pad_vjp(g, p.f.max_dt_scale, pend, lam);
+            pend = 0;
+            if (kind == 0x42) torus_pad_vjp(g, p.f.max_dt_scale, hbar, lam);
+            if (kind == 0x41) pend = hbar;
+        };
+        if (!escaped) {
+            for (int seg = nseg - 1; seg >= 0; --seg) {
+                const int e0 = seg * KC;
+                const int e1 = min(e0 + KC, (int)n_ev);
+                const double* c0 = p.f.ck + (co + (unsigned long long)seg) * (unsigned long long)D;
+                const double* c1 = c0 + D;  // the state after the segment
+                for (int i = 0; i < 8; ++i) G[i] = c0[i];
+                unsigned refl = 0;
+                for (int e = e0; e < e1; ++e)
+                    if (torus_geo_step(m, G + (e - e0) * 8, p.f.ev_h[eo + e], Kgs + (e - e0) * 48, G + (e - e0 + 1) * 8))
+                        refl |= 1u << (e - e0);
+                for (int c = 0; c < N; ++c) taus[c] = c1[8 + c];
+                for (int e = e1 - 1; e >= e0; --e)
+                    dp_step(G + (e - e0) * 8, Kgs + (e - e0) * 48, p.f.ev_kind[eo + e], p.f.ev_h[eo + e],
+                            (refl >> (e - e0)) & 1u, true);
+            }
+        } else {
+            for (int e = (int)n_ev - 1; e >= 0; --e) {
+                const double* c0 = p.f.ck + (co + (unsigned long long)e) * (unsigned long long)D;
+                for (int i = 0; i < D; ++i) Ys[i] = c0[i];
                 const uint8_t kind = p.f.ev_kind[eo + e];
                 const double hv = p.f.ev_h[eo + e];
                 if (torus_is_dp(kind)) {
-                    if (refl >> (e - e0) & 1ull) {
-                        lam[2] = -lam[2];
-                        lam[6] = -lam[6];
-                    }
-                    const double* Kst = Ks + (long long)(e - e0) * 6 * D;
-                    const double hbar = torus_dp_vjp(m, y, Kst, hv, lam, pb);
-                    // a pending step-size term of the next step lands on this state
-                    if (pend != 0) torus_pad_vjp(y, p.f.max_dt_scale, pend, lam);
-                    pend = 0;
-                    if (kind == 0x42) torus_pad_vjp(y, p.f.max_dt_scale, hbar, lam);
-                    if (kind == 0x41) pend = hbar;
+                    const bool r = torus_replay(m, Ys, kind, hv, Ys + D, Kw, tmp);
+                    for (int st = 0; st < 6; ++st)
+                        for (int i = 0; i < 8; ++i) Kgs[st * 8 + i] = Kw[st * D + i];
+                    for (int c = 0; c < N; ++c) taus[c] = Ys[8 + c];
+                    dp_step(Ys, Kgs, kind, hv, r, false);
                 } else {
-                    if (!torus_escape_vjp(m, y, (int)kind - 1, hv, lam, pb, Ze, mu, tmp)) ++n_cut;
+                    if (!torus_escape_vjp(m, Ys, (int)kind - 1, hv, lam, pb, Ze, mu, tmp)) ++n_cut;
                 }
             }
         }
@@ -1366,7 +1426,7 @@ rtw_status rtw_adjoint(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* c
         const uint32_t n = h_nev[i] & kEventCount;
         const uint32_t kc = (h_nev[i] & kDenseCheckpoints) ? 1u : (uint32_t)KC;
         E += n;
-        C += (n + kc - 1) / kc;
+        C += (n + kc - 1) / kc + 1;  // segment starts + the final state
     }
     RTW_CUDA(cudaMemcpyAsync(ev_off, h_off.data(), 16 * Q, cudaMemcpyHostToDevice, s), "offsets H2D");
     if ((st = ensure(ctx, &b->evh, &b->evh_cap, std::max<size_t>(8 * E, 256))) != RTW_OK) return st;
@@ -1391,8 +1451,8 @@ rtw_status rtw_adjoint(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* c
     RTW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, torus_reverse, 128, 0), "occupancy");
     const int rgrid = ctx->num_sms * std::max(1, occ);
     // local-memory work area of the reverse kernel (per resident thread)
-    const size_t work_b = (size_t)rgrid * 128 * (size_t)(kTorusMaxCk + 1 + 6 * kTorusMaxCk + 4 + 3) *
-                          kTorusMaxD * 8;
+    const size_t work_b = (size_t)rgrid * 128 *
+                          ((size_t)(2 + 6 + 4 + 3) * kTorusMaxD + (kTorusMaxCk + 1) * 8 + kTorusMaxCk * 48 + kTorusMaxBins) * 8;
     const size_t per_ray_b = adj->per_ray_grad ? (size_t)P * kTorusParams * 8 : 0;
     if ((st = ensure(ctx, &b->work, &b->work_cap, std::max<size_t>(per_ray_b, 256))) != RTW_OK) return st;
     rp.f = p;
@@ -1541,8 +1601,18 @@ rtw_status rtw_torus_step_vjp(const rtw_scene* scene, const double* colors_nm, i
     }
     torus_dp_stages(m, y.data(), h, K.data(), Y.data(), nullptr);
     double pb[kTorusParams] = {0, 0, 0, 0, 0};
-    *hbar = form == 0 ? torus_dp_vjp(m, y.data(), K.data(), h, lam.data(), pb)
-                      : torus_dp_vjp_generic(m, y.data(), K.data(), h, lam.data(), pb, Yst.data(), kac.data(), tmp.data());
+    double Kg[48], taus[kTorusMaxBins];
+    for (int st = 0; st < 6; ++st)
+        for (int i = 0; i < 8; ++i) Kg[st * 8 + i] = K[st * D + i];
+    if (form == 1) {
+        *hbar = torus_dp_vjp_generic(m, y.data(), K.data(), h, lam.data(), pb, Yst.data(), kac.data(), tmp.data());
+    } else {
+        // form 2 starts from the depths at the end of the step
+        std::vector<double> y1(D);
+        torus_dp_stages(m, y.data(), h, K.data(), Y.data(), y1.data());
+        for (int c = 0; c < N; ++c) taus[c] = form == 2 ? y1[8 + c] : y[8 + c];
+        *hbar = torus_dp_vjp(m, y.data(), Kg, taus, form == 2, h, lam.data(), pb);
+    }
     for (int i = 0; i < 8; ++i) mu[i] = lam[i];
     for (int c = 0; c < N; ++c) {
         mu[8 + 2 * c] = lam[8 + N + c];

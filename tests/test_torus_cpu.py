@@ -138,17 +138,18 @@ def test_structured_step_vjp_matches_generic():
             cot[8::2] /= 1e14
             a = abi.torus_step_vjp(sc, col, y, h, cot, 0)
             b = abi.torus_step_vjp(sc, col, y, h, cot, 1)
-            for u, v in zip(a[:2], b[:2]):
+            back = abi.torus_step_vjp(sc, col, y, h, cot, 2)  # depths run back from the step's end
+            for u, v, w in zip(a[:2], b[:2], back[:2]):
                 np.testing.assert_allclose(u, v, rtol=1e-11, atol=1e-13 * np.abs(v).max())
+                np.testing.assert_allclose(w, v, rtol=1e-10, atol=1e-12 * np.abs(v).max())
             assert a[2] == pytest.approx(b[2], rel=1e-11, abs=1e-13 * abs(b[2]) + 1e-300)
+            assert back[2] == pytest.approx(b[2], rel=1e-10, abs=1e-12 * abs(b[2]) + 1e-300)
             # d loss / d h against a central difference of the step
             dh = 1e-6 * abs(h)
-            zero = np.zeros_like(y)
             lp = cot @ _step(sc, col, y, h + dh)
             lm = cot @ _step(sc, col, y, h - dh)
             fd = (lp - lm) / (2 * dh)
             assert abs(fd - a[2]) <= 1e-5 * abs(fd) + 1e-9 * np.abs(cot * y).sum() / abs(h), (r, th, h, fd, a[2])
-            del zero
 
 
 def _step(sc, col, y, h):
