@@ -832,16 +832,17 @@ RTW_HD double torus_dp_vjp(const TorusModel& m, const double* y, const double* K
             for (int s = 0; s < t; ++s) acc += tA(t, s) * Kg[s * 8 + i];
             Yg[t][i] = y[i] + h * acc;
         }
-    double Sv[6][4], dS[6][4][8], Sbar[6][4];
+    double dS[6][4][8], Sbar[6][4];
+    TorusBinPre pre[6];
     bool on[6];
     for (int t = 0; t < 6; ++t) {
         const TorusPt<D8> S = torus_point<D8>(m.tor, D8::var(m.tor.a, 4), D8::var(m.tor.n0, 5), D8::var(m.tor.B0, 6),
                                               D8::var(m.tor.Th0, 7), D8::var(Yg[t][1], 0), D8::var(Yg[t][2], 1),
                                               D8::var(Yg[t][4], 2), D8::var(Yg[t][7], 3));
         on[t] = S.on;
+        if (S.on) pre[t] = torus_bin_pre(S.cj.v, S.nus.v, S.th.v, S.g.v);
         const D8* comp[4] = {&S.cj, &S.nus, &S.th, &S.g};
         for (int q = 0; q < 4; ++q) {
-            Sv[t][q] = comp[q]->v;
             Sbar[t][q] = 0;
             for (int u = 0; u < 8; ++u) dS[t][q][u] = comp[q]->d[u];
         }
@@ -855,7 +856,7 @@ RTW_HD double torus_dp_vjp(const TorusModel& m, const double* y, const double* K
         double bkt = 0, bki = 0;
         for (int t = 0; t < 6; ++t) {
             Kt[t] = fi[t] = 0;
-            if (on[t]) torus_bin_grad(Sv[t][0], Sv[t][1], Sv[t][2], Sv[t][3], m.bins[c], Kt[t], fi[t], dft[t], dfi[t]);
+            if (on[t]) torus_bin_grad_pre(pre[t], m.bins[c], Kt[t], fi[t], dft[t], dfi[t]);
             bkt += tA(6, t) * Kt[t];
         }
         double t0 = tau[c];
@@ -1180,6 +1181,8 @@ rtw_status torus_model(const rtw_scene& s, const double* colors_nm, int N, Torus
         m.bins[c].inv_nu_nm3 = lam * lam * lam;
         m.bins[c].b0 = 2 * kHcgs * nu * nu * nu / (kCcgs * kCcgs);
         m.bins[c].hk = kHcgs * nu / kMec2;
+        m.bins[c].ln_nu = std::log(nu);
+        m.bins[c].inv_b0 = 1.0 / m.bins[c].b0;
     }
     m.n = N;
     m.emitter = powehi ? 1 : 0;

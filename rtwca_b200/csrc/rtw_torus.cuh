@@ -34,6 +34,8 @@ struct TorusBin {
     double b0;          // 2 h nu_c^3 / c^2 (cgs)
     double hk;          // h nu_c / (m_e c^2)
     double fx, fy, fz;  // nu^3 c / lambda^2 * CIE trapezoid weights (XYZ epilogue)
+    double ln_nu;       // log(nu_c in Hz)
+    double inv_b0;      // 1 / b0
 };
 
 // Emitter numbers at a point, shared by every bin: j_nu = cj nus F(nu / nus)
@@ -325,6 +327,60 @@ RTW_HD void powehi_bin(const PowehiDev& P, const TorusPt<T>& S, double nu_nm, T&
 //   D_y = dln expm1(y) / dln y = y e^y / expm1(y),   y = g hk / Theta
 // ln|fi| = ln cj + ln nus + ln(P^2 e^..)(X) - 4 ln g + const,
 // ln|ft| = ln|fi| + ln expm1(y) + const.
+// The bin-independent part of torus_bin_grad at one emitter point: X = nu_c
+// r with r = g / nus, so log X = log r + log nu_c; reciprocals shared by all
+// bins.
+struct TorusBinPre {
+    double L, gt, cjnus, ig4, icj, inus, ig, ith;
+    bool ok;
+};
+
+RTW_HD TorusBinPre torus_bin_pre(double cj, double nus, double th, double g) {
+    TorusBinPre q;
+    const double r = g / nus;
+    q.ok = r > 0;
+    q.L = q.ok ? log(r) : 0.0;
+    q.gt = g / th;
+    q.cjnus = cj * nus;
+    const double g2 = g * g;
+    q.ig4 = 1.0 / (g2 * g2);
+    q.icj = 1.0 / cj;
+    q.inus = 1.0 / nus;
+    q.ig = 1.0 / g;
+    q.ith = 1.0 / th;
+    return q;
+}
+
+// torus_bin_grad from the shared part: three transcendentals per bin
+// (X^1/6; X^1/3 and X^1/2 as its square and cube) instead of six.
+RTW_HD void torus_bin_grad_pre(const TorusBinPre& q, const TorusBin& bn, double& ft, double& fi, double* dft,
+                               double* dfi) {
+    const double lx = q.L + bn.ln_nu;
+    if (!q.ok || !(lx <= 12.206072645530174)) {  // X > 2e5: exp(-X^1/3) < 1e-25, no emission
+        ft = fi = 0;
+        for (int k = 0; k < 4; ++k) dft[k] = dfi[k] = 0;
+        return;
+    }
+    const double c = 1.8877486253633868;  // 2^(11/12)
+    const double x16 = exp(lx * (1.0 / 6.0)), x13 = x16 * x16, x12 = x13 * x16;
+    const double P = x12 + c * x16;
+    const double j = q.cjnus * P * P * exp(-x13);
+    fi = -(j * bn.inv_nu_nm3 * q.ig4);
+    const double y = q.gt * bn.hk;
+    const double em1 = expm1(y);
+    ft = -(j * em1 * q.ig4 * bn.inv_b0);
+    const double DX = (x12 + c / 3.0 * x16) / P - x13 * (1.0 / 3.0);
+    const double Dy = y * (em1 + 1.0) / em1;
+    dfi[0] = fi * q.icj;
+    dfi[1] = fi * (1.0 - DX) * q.inus;
+    dfi[2] = 0;
+    dfi[3] = fi * (DX - 4.0) * q.ig;
+    dft[0] = ft * q.icj;
+    dft[1] = ft * (1.0 - DX) * q.inus;
+    dft[2] = -ft * Dy * q.ith;
+    dft[3] = ft * (DX - 4.0 + Dy) * q.ig;
+}
+
 RTW_HD void torus_bin_grad(double cj, double nus, double th, double g, const TorusBin& bn, double& ft, double& fi,
                            double* dft, double* dfi) {
     for (int q = 0; q < 4; ++q) {
