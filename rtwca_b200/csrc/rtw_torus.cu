@@ -9,13 +9,16 @@
 // The error norm is the reference's RMS over all 8 + 2N components
 // (integrators_LttM.jl:185-224).
 //
-// Adjoint: a count pass (the forward render) gives each ray's number of
-// recorded steps; an exclusive scan gives offsets; a record pass re-runs the
-// forward and stores every accepted step's size (and polar escapes) plus the
-// state every `ck_every` steps. The reverse pass, one lane per ray in FP64,
-// walks the segments backwards: it replays a segment from its checkpoint,
-// then reverses each step through its stages with vector-Jacobian products
-// of the right-hand side built from dual numbers (rtw_dual.cuh).
+// Adjoint: one recording forward pass gives the image and, per ray, a chain
+// of chunks taken from a pool by an atomic counter, each chunk one segment:
+// the state before it and the sizes and kinds of its `ck_every` accepted
+// steps (and polar escapes). Rays with a polar escape whose gradient is
+// wanted are recorded again, alone, with their state before every event.
+// The reverse pass, one lane per ray in FP64, walks the segments backwards:
+// it replays a segment's geodesic from its checkpoint, then reverses each
+// step through its stages with vector-Jacobian products of the right-hand
+// side built from dual numbers (rtw_dual.cuh), running the optical depths
+// back from the segment's end.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -87,7 +90,6 @@ RTW_HD void em_bin(const TorusModel& m, const TorusPt<R>& S, int c, R& ft, R& fi
     else torus_bin<R>(S.cj, S.nus, S.th, S.g, m.bins[c], ft, fi);
 }
 
-// FP64 right-hand side on a state y[8 + 2N] = (x^mu, k^mu, tau_c, I_c).
 // The geodesic part of the right-hand side (8 components of y).
 RTW_HD void torus_geo_rhs(const TorusModel& m, const double* y, double* f) {
     double z[10], k[9];
@@ -99,6 +101,7 @@ RTW_HD void torus_geo_rhs(const TorusModel& m, const double* y, double* f) {
     for (int i = 0; i < 8; ++i) f[i] = k[i];
 }
 
+// FP64 right-hand side on a state y[8 + 2N] = (x^mu, k^mu, tau_c, I_c).
 RTW_HD void torus_f64(const TorusModel& m, const double* y, double* f) {
     const int N = m.n;
     torus_geo_rhs(m, y, f);
@@ -213,11 +216,20 @@ RTW_HD void torus_pad_vjp(const double* y, double scale, double w, double* lam) 
     lam[7] -= w * m.d[3];
 }
 
-// n_events word: the count, and a flag for rays checkpointed at every step
-// (rays with a polar escape: near the pole the FP64 replay of FP32-stage
-// steps would drift by more than the distance to the axis)
+// n_events word: the count, a flag for rays with a polar escape (re-recorded
+// with their state before every event: near the pole the FP64 replay of
+// FP32-stage steps would drift by more than the distance to the axis), and a
+// flag for rays with more segments than their region of the pool holds
 constexpr uint32_t kDenseCheckpoints = 0x80000000u;
-constexpr uint32_t kEventCount = 0x7fffffffu;
+constexpr uint32_t kOverflow = 0x40000000u;
+constexpr uint32_t kEventCount = 0x3fffffffu;
+constexpr int kTorusMaxCk = 16;  // recorded steps per checkpoint
+
+// A recording chunk: one segment of ck_every events: the geodesic state and
+// the optical depths before it ([8 + N] doubles; the reverse sweep needs no
+// intensities), the step sizes ([ck_every] doubles) and the event kinds
+// ([ck_every] bytes). A ray's chunks are contiguous: chunk base + segment.
+RTW_HD int torus_chunk_bytes(int N, int kc) { return (8 * (8 + N) + 8 * kc + kc + 7) & ~7; }
 
 struct TorusKP {
     TorusModel m;
@@ -231,9 +243,10 @@ struct TorusKP {
     float* xyz;       // [P][3]
     uint8_t* cls;
     uint32_t* steps;
+    const uint32_t* ray_list;          // [total_rays] indices into the subset (dense re-record) or null
     // recording
-    int record;                        // 0: count events, 1: store them
-    uint32_t* n_events;                // [P] (count pass writes, record pass checks)
+    int record;                        // 0: none, 1: dense (offsets from counts), 2: chunks
+    uint32_t* n_events;                // [P] (chunk pass writes, dense pass checks)
     const unsigned long long* ev_off;  // [P] first event of a ray
     const unsigned long long* ck_off;  // [P] first checkpoint of a ray
     double* ev_h;                      // [E] step size (DP step) or escape sub-step size
@@ -244,6 +257,18 @@ struct TorusKP {
     int ck_every;
     int fsal;                          // 1: FSAL Dormand-Prince, 0: the reference's step
     unsigned int* err_flag;            // bit 0: record pass diverged from the count pass
+    // chunked recording (record 2). Chunk index i lives in pool at i < split,
+    // in pool2 at i - split above. A ray's chunks start at sub * region (first
+    // pass, at most region of them: more sets kOverflow), or at chunk_base[loc]
+    // (region 0: the pass over the overflowed rays, sized exactly). No atomics:
+    // a shared allocation counter cost this kernel a third of its speed.
+    char* pool;
+    char* pool2;
+    unsigned long long split;
+    int chunk_bytes;
+    unsigned int region;
+    const unsigned long long* chunk_base;  // [total_rays] (region 0)
+    double* fin;                           // [P][D] final states
 };
 
 template <class R>
@@ -308,6 +333,101 @@ __device__ __forceinline__ int torus_terminate(const TorusKP& p, const double* x
     return RTW_CLASS_THICK;
 }
 
+// Recording of one ray (record 1: dense offsets, 2: chunks). One kernel
+// instance serves renders and recording passes, so that both take
+// bit-identical steps; the per-segment work is out of line and the per-event
+// work is two stores into a buffer, so that a render does not pay for it.
+struct TorusRec {
+    unsigned long long eo, co;  // dense: first event and checkpoint
+    uint32_t ev_cap, kc;        // dense: event count from the first pass; segment length
+    unsigned long long base;    // chunks: the ray's first chunk
+    uint32_t seg;               // chunks: segments opened so far
+    uint32_t ovf;               // chunks: more segments than the region holds
+    uint32_t bad;               // dense: more events than the first pass
+    double hb[kTorusMaxCk];     // chunks: the current segment's events, written out whole
+    uint8_t kb[kTorusMaxCk];
+};
+
+RTW_HD char* torus_chunk(const TorusKP& p, unsigned long long i) {
+    return i < p.split ? p.pool + i * (unsigned long long)p.chunk_bytes
+                       : p.pool2 + (i - p.split) * (unsigned long long)p.chunk_bytes;
+}
+
+// write the first m buffered events of the current segment (streaming
+// stores: this kernel does not read them again)
+__device__ void torus_rec_flush(const TorusKP& p, const TorusRec* r, uint32_t m) {
+    if (r->ovf || r->seg == 0 || m == 0) return;
+    const int N = p.m.n;
+    char* chunk = torus_chunk(p, r->base + r->seg - 1);
+    double* h = (double*)(chunk + 8 * (8 + N));
+    uint8_t* k = (uint8_t*)(chunk + 8 * (8 + N) + 8 * r->kc);
+    for (uint32_t j = 0; j < m; ++j) {
+        __stcs(h + j, r->hb[j]);
+        k[j] = r->kb[j];
+    }
+}
+
+__device__ __noinline__ void torus_rec_begin(const TorusKP& p, long long loc, long long sub, TorusRec* r) {
+    r->seg = r->ovf = r->bad = 0;
+    r->kc = (uint32_t)p.ck_every;
+    r->ev_cap = 0;
+    r->eo = r->co = 0;
+    r->base = 0;
+    if (p.record == 1) {
+        const uint32_t w = p.n_events[loc];
+        r->ev_cap = w & kEventCount;
+        r->kc = (w & kDenseCheckpoints) ? 1u : (uint32_t)p.ck_every;
+        r->eo = p.ev_off[loc];
+        r->co = p.ck_off[loc];
+    } else if (p.record == 2) {
+        r->base = p.region ? (unsigned long long)sub * p.region : p.chunk_base[loc];
+    }
+}
+
+template <class SR, bool MIXED>
+__device__ void torus_save_state(int N, double* c, const double* x, const SR* tau, const SR* ihi, const SR* ilo,
+                                 bool with_i) {
+    for (int i = 0; i < 8; ++i) __stcs(c + i, x[i]);
+    for (int q = 0; q < N; ++q) __stcs(c + 8 + q, (double)tau[q]);
+    if (with_i)
+        for (int q = 0; q < N; ++q) __stcs(c + 8 + N + q, (double)ihi[q] + (MIXED ? (double)ilo[q] : 0.0));
+}
+
+// the state before event n (n a multiple of kc): a checkpoint row (dense) or
+// the ray's next chunk
+template <class SR, bool MIXED>
+__device__ __noinline__ void torus_rec_checkpoint(const TorusKP& p, TorusRec* r, uint32_t n, const double* x,
+                                                  const SR* tau, const SR* ihi, const SR* ilo) {
+    const int N = p.m.n, D = 8 + 2 * N;
+    if (p.record == 1) {
+        if (n < r->ev_cap)
+            torus_save_state<SR, MIXED>(N, p.ck + (r->co + n / r->kc) * (unsigned long long)D, x, tau, ihi, ilo, true);
+        return;
+    }
+    if (r->ovf) return;
+    if (n > 0) torus_rec_flush(p, r, r->kc);  // the previous segment is complete
+    if (p.region && r->seg >= p.region) {
+        r->ovf = 1;
+        return;
+    }
+    torus_save_state<SR, MIXED>(N, (double*)torus_chunk(p, r->base + r->seg), x, tau, ihi, ilo, false);
+    ++r->seg;
+}
+
+// the end of a ray: the last segment's events and the final state (chunks),
+// counts and flags
+template <class SR, bool MIXED>
+__device__ __noinline__ void torus_rec_end(const TorusKP& p, TorusRec* r, long long loc, long long sub, uint32_t n,
+                                           bool escaped, const double* x, const SR* tau, const SR* ihi, const SR* ilo) {
+    const int N = p.m.n, D = 8 + 2 * N;
+    if (p.record == 2) {
+        if (n > 0) torus_rec_flush(p, r, n - (n - 1) / r->kc * r->kc);
+        torus_save_state<SR, MIXED>(N, p.fin + sub * (long long)D, x, tau, ihi, ilo, true);
+        p.n_events[sub] = n | (escaped ? kDenseCheckpoints : 0u) | (r->ovf ? kOverflow : 0u);
+    }
+    if (p.record == 1 && (r->bad || n != r->ev_cap)) atomicOr(p.err_flag, 1u);
+}
+
 // Forward kernel. SR: arithmetic of the bins and of the stages (float on the
 // mixed path, with Kahan intensities and per-ray FP64 stages near the horizon
 // and the poles; double on the FP64 path).
@@ -318,9 +438,10 @@ __global__ void __launch_bounds__(128) torus_forward(const TorusKP p) {
     const int D = 8 + 2 * N;
     unsigned c_att = 0, c_rej = 0, c_pro = 0, c_esc = 0, c_rays = 0, c_nan = 0;
     for (;;) {
-        const long long loc = (long long)atomicAdd(p.counter, 1ull);  // index in the ray subset
+        const long long loc = (long long)atomicAdd(p.counter, 1ull);  // index in the ray subset (list)
         if (loc >= p.total_rays) break;
-        const long long id = p.ray0 + loc * p.ray_stride;              // pixel
+        const long long sub = p.ray_list ? (long long)p.ray_list[loc] : loc;
+        const long long id = p.ray0 + sub * p.ray_stride;              // pixel
         ++c_rays;
         const int pi = (int)(id % p.frame.xp), pj = (int)(id / p.frame.xp);
         double x[9];
@@ -349,30 +470,25 @@ __global__ void __launch_bounds__(128) torus_forward(const TorusKP p) {
         long long nsteps = 0;
         uint32_t n_ev = 0;
         bool escaped = false;  // a ray with a polar escape stores its state at every step
-        const uint32_t ev_word = p.record ? p.n_events[loc] : 0u;
-        const uint32_t ev_cap = ev_word & kEventCount;
-        const uint32_t kc = (ev_word & kDenseCheckpoints) ? 1u : (uint32_t)p.ck_every;
-        const unsigned long long eo = p.record ? p.ev_off[loc] : 0ull;
-        const unsigned long long co = p.record ? p.ck_off[loc] : 0ull;
-        bool bad = false;
-        // a checkpoint of the state before event n_ev when it starts a segment
+        TorusRec rec;
+        if (p.record) torus_rec_begin(p, loc, sub, &rec);
+        // the state before event n_ev when it starts a segment (recording)
         auto checkpoint = [&]() {
-            if (!p.record || n_ev >= ev_cap || (n_ev % kc) != 0u) return;
-            double* c = p.ck + (co + n_ev / kc) * (unsigned long long)D;
-            for (int i = 0; i < 8; ++i) c[i] = x[i];
-            for (int q = 0; q < N; ++q) {
-                c[8 + q] = (double)tau[q];
-                c[8 + N + q] = (double)ihi[q] + (MIXED ? (double)ilo[q] : 0.0);
-            }
+            if (p.record && (n_ev % rec.kc) == 0u) torus_rec_checkpoint<SR, MIXED>(p, &rec, n_ev, x, tau, ihi, ilo);
         };
+        // event n_ev: its step size (or escape sub-step size) and kind
         auto push = [&](uint8_t kind, double hv) {
-            if (p.record) {
-                if (n_ev >= ev_cap) {
-                    bad = true;
+            if (p.record == 1) {
+                if (n_ev >= rec.ev_cap) {
+                    rec.bad = 1;
                 } else {
-                    p.ev_h[eo + n_ev] = hv;
-                    p.ev_kind[eo + n_ev] = kind;
+                    p.ev_h[rec.eo + n_ev] = hv;
+                    p.ev_kind[rec.eo + n_ev] = kind;
                 }
+            } else if (p.record == 2) {
+                const uint32_t j = n_ev % rec.kc;
+                rec.hb[j] = hv;
+                rec.kb[j] = kind;
             }
             ++n_ev;
         };
@@ -589,17 +705,7 @@ __global__ void __launch_bounds__(128) torus_forward(const TorusKP p) {
         }
         if (p.cls) p.cls[id] = (uint8_t)cls;
         if (p.steps) p.steps[id] = (uint32_t)nsteps;
-        if (p.record && !bad && n_ev == ev_cap) {
-            // the final state closes the last segment (one row after the segments')
-            double* c = p.ck + (co + (ev_cap + kc - 1) / kc) * (unsigned long long)D;
-            for (int i = 0; i < 8; ++i) c[i] = x[i];
-            for (int q = 0; q < N; ++q) {
-                c[8 + q] = (double)tau[q];
-                c[8 + N + q] = (double)ihi[q] + (MIXED ? (double)ilo[q] : 0.0);
-            }
-        }
-        if (!p.record && p.n_events) p.n_events[loc] = n_ev | (escaped ? kDenseCheckpoints : 0u);
-        if (p.record && (bad || n_ev != ev_cap)) atomicOr(p.err_flag, 1u);
+        if (p.record) torus_rec_end<SR, MIXED>(p, &rec, loc, sub, n_ev, escaped, x, tau, ihi, ilo);
     }
     atomicAdd(&p.stats->step_attempts, (unsigned long long)c_att);
     atomicAdd(&p.stats->rejected_steps, (unsigned long long)c_rej);
@@ -618,6 +724,8 @@ struct TorusRP {
     double* per_ray;             // [P][5] per-ray gradients (may be null)
     int skip_escape_rays;        // 1: rays with a polar escape give no gradient
     unsigned long long* counter;
+    const uint32_t* esc_index;   // [P] a ray's index among the densely re-recorded rays
+    const unsigned long long* rbase;  // [P] a ray's first chunk
 };
 
 // One recorded step of a ray, replayed in FP64: y_out = keep(step(y_in)).
@@ -943,15 +1051,15 @@ RTW_HD double torus_dp_vjp(const TorusModel& m, const double* y, const double* K
 }
 
 constexpr int kTorusMaxD = 8 + 2 * kTorusMaxBins;  // state components
-constexpr int kTorusMaxCk = 16;                     // recorded steps per checkpoint
 
-// Reverse kernel (FP64), one lane per ray. A ray without a polar escape
-// replays each segment's geodesic from its checkpoint (G [ck_every + 1][8]
-// states, Kgs [ck_every][6][8] stage slopes) and runs the bins' optical
-// depths backwards from the segment's end state (the next checkpoint; the
-// last segment ends at the ray's final state); a ray with a polar escape has
-// its full state checkpointed before every event (Ys [2][D], Kw [6][D] stage
-// slopes, Ze [4][D] escape evaluations). The arrays live in local memory,
+// Reverse kernel (FP64), one lane per ray. A ray without a polar escape walks
+// its chunks backwards: replays each segment's geodesic from the chunk's
+// checkpoint (G [ck_every + 1][8] states, Kgs [ck_every][6][8] stage slopes)
+// and runs the bins' optical depths backwards from the segment's end state
+// (the next chunk's checkpoint; the last segment ends at the ray's final
+// state); a ray with a polar escape was re-recorded with its full state
+// before every event (Ys [2][D], Kw [6][D] stage slopes, Ze [4][D] escape
+// evaluations). The arrays live in local memory,
 // whose layout interleaves the lanes of a warp (same-index accesses coalesce).
 __global__ void __launch_bounds__(128, 4) torus_reverse(const TorusRP p) {
     const TorusModel& m = p.f.m;
@@ -985,7 +1093,6 @@ __global__ void __launch_bounds__(128, 4) torus_reverse(const TorusRP p) {
         double pend = 0;  // d loss / d h of a step whose h was set at the previous step's start
         const uint32_t n_ev = p.f.n_events[loc] & kEventCount;
         const int KC = escaped ? 1 : p.f.ck_every;
-        const unsigned long long eo = p.f.ev_off[loc], co = p.f.ck_off[loc];
         const int nseg = (int)((n_ev + (uint32_t)KC - 1) / (uint32_t)KC);
         // the reverse of one DP step from geodesic start state g
         auto dp_step = [&](const double* g, const double* Kg, uint8_t kind, double hv, bool refl, bool tau_at_end) {
@@ -1001,22 +1108,29 @@ __global__ void __launch_bounds__(128, 4) torus_reverse(const TorusRP p) {
             if (kind == 0x41) pend = hbar;
         };
         if (!escaped) {
+            const unsigned long long base = p.rbase[loc];
+            const double* c1 = p.f.fin + loc * (long long)D;  // the state after the segment
             for (int seg = nseg - 1; seg >= 0; --seg) {
                 const int e0 = seg * KC;
                 const int e1 = min(e0 + KC, (int)n_ev);
-                const double* c0 = p.f.ck + (co + (unsigned long long)seg) * (unsigned long long)D;
-                const double* c1 = c0 + D;  // the state after the segment
+                const char* ch = torus_chunk(p.f, base + (unsigned long long)seg);
+                const double* c0 = (const double*)ch;
+                const double* hs = (const double*)(ch + 8 * (8 + N));
+                const uint8_t* ks = (const uint8_t*)(ch + 8 * (8 + N) + 8 * KC);
                 for (int i = 0; i < 8; ++i) G[i] = c0[i];
                 unsigned refl = 0;
                 for (int e = e0; e < e1; ++e)
-                    if (torus_geo_step(m, G + (e - e0) * 8, p.f.ev_h[eo + e], Kgs + (e - e0) * 48, G + (e - e0 + 1) * 8))
+                    if (torus_geo_step(m, G + (e - e0) * 8, hs[e - e0], Kgs + (e - e0) * 48, G + (e - e0 + 1) * 8))
                         refl |= 1u << (e - e0);
                 for (int c = 0; c < N; ++c) taus[c] = c1[8 + c];
                 for (int e = e1 - 1; e >= e0; --e)
-                    dp_step(G + (e - e0) * 8, Kgs + (e - e0) * 48, p.f.ev_kind[eo + e], p.f.ev_h[eo + e],
-                            (refl >> (e - e0)) & 1u, true);
+                    dp_step(G + (e - e0) * 8, Kgs + (e - e0) * 48, ks[e - e0], hs[e - e0], (refl >> (e - e0)) & 1u,
+                            true);
+                c1 = c0;
             }
         } else {
+            const uint32_t j = p.esc_index[loc];
+            const unsigned long long eo = p.f.ev_off[j], co = p.f.ck_off[j];
             for (int e = (int)n_ev - 1; e >= 0; --e) {
                 const double* c0 = p.f.ck + (co + (unsigned long long)e) * (unsigned long long)D;
                 for (int i = 0; i < D; ++i) Ys[i] = c0[i];
@@ -1068,13 +1182,19 @@ struct TorusBuffers {
     size_t ck_cap = 0;
     void* work = nullptr;
     size_t work_cap = 0;
+    void* pool = nullptr;  // recording chunks (the rays' regions)
+    size_t pool_cap = 0;
+    void* pool2 = nullptr;  // recording chunks (the overflowed rays)
+    size_t pool2_cap = 0;
+    void* fin = nullptr;   // final states
+    size_t fin_cap = 0;
     void* tgt = nullptr;
     size_t tgt_cap = 0;
 };
 
 void torus_free(TorusBuffers* b) {
     if (!b) return;
-    for (void* q : {b->ctl, b->out, b->nev, b->evh, b->evk, b->ck, b->work, b->tgt})
+    for (void* q : {b->ctl, b->out, b->nev, b->evh, b->evk, b->ck, b->work, b->tgt, b->pool, b->pool2, b->fin})
         if (q) cudaFree(q);
     delete b;
 }
@@ -1385,11 +1505,21 @@ rtw_status rtw_adjoint(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* c
     float* spec = (float*)b->out;
     uint32_t* steps = (uint32_t*)((char*)b->out + spec_b);
     uint8_t* cls = (uint8_t*)((char*)b->out + spec_b + (((size_t)P * 4 + 255) & ~(size_t)255));
-    const size_t nev_b = ((size_t)Q * 4 + 255) & ~(size_t)255;
-    if ((st = ensure(ctx, &b->nev, &b->nev_cap, nev_b + 2 * (size_t)Q * 8)) != RTW_OK) return st;
+    // per-ray words: n_events, dense index, the lists of the second passes
+    // (dense re-record, overflowed rays) with their counts, offsets and chunk
+    // bases, and every ray's first chunk
+    const size_t q4 = ((size_t)Q * 4 + 255) & ~(size_t)255;
+    const size_t nev_b = 5 * q4 + 4 * (size_t)Q * 8;
+    if ((st = ensure(ctx, &b->nev, &b->nev_cap, nev_b)) != RTW_OK) return st;
     uint32_t* nev = (uint32_t*)b->nev;
-    unsigned long long* ev_off = (unsigned long long*)((char*)b->nev + nev_b);
-    unsigned long long* ck_off = ev_off + Q;
+    uint32_t* esc_index = (uint32_t*)((char*)b->nev + q4);
+    uint32_t* ray_list = (uint32_t*)((char*)b->nev + 2 * q4);
+    uint32_t* nev_d = (uint32_t*)((char*)b->nev + 3 * q4);
+    uint32_t* list2 = (uint32_t*)((char*)b->nev + 4 * q4);
+    unsigned long long* ev_off = (unsigned long long*)((char*)b->nev + 5 * q4);  // [Q] events, then [Q] rows
+    unsigned long long* base2 = ev_off + 2 * Q;
+    unsigned long long* rbase = ev_off + 3 * Q;
+    if ((st = ensure(ctx, &b->fin, &b->fin_cap, std::max<size_t>((size_t)Q * D * 8, 256))) != RTW_OK) return st;
     if ((st = ensure(ctx, &b->tgt, &b->tgt_cap, (size_t)P * N * 4)) != RTW_OK) return st;
     if (adj->target_on_device)
         RTW_CUDA(cudaMemcpyAsync(b->tgt, adj->target, (size_t)P * N * 4, cudaMemcpyDeviceToDevice, s), "target");
@@ -1409,45 +1539,119 @@ rtw_status rtw_adjoint(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* c
         }
     } guard{ev};
 
-    // 1. forward: image, step counts, recorded-step counts (pixels outside
-    // the subset stay zero)
+    // 1. forward pass, recording: image, step counts, and per ray its chunks
+    // (one per segment of KC accepted steps) in a region of R0 chunks of the
+    // pool; R0 from the memory there is (at most 256: 4096 steps at KC 16).
+    const int cb = torus_chunk_bytes(N, KC);
+    unsigned long long R0 = 256;
+    {
+        size_t fr = 0, tot = 0;
+        RTW_CUDA(cudaMemGetInfo(&fr, &tot), "memory info");
+        const double avail = 0.6 * (double)(fr + b->pool_cap);
+        R0 = std::min<unsigned long long>(R0, (unsigned long long)(avail / ((double)Q * cb)));
+        R0 = std::min<unsigned long long>(R0, (unsigned long long)(2 * p.frame.max_steps + KC - 1) / KC + 1);
+        if (R0 < 4) return fail(ctx, RTW_ERR_OOM, "not enough device memory for the adjoint's records");
+    }
+    // (allocated before the timed region, like the other buffers)
+    if ((st = ensure(ctx, &b->pool, &b->pool_cap, (size_t)Q * R0 * cb)) != RTW_OK) return st;
+    p.record = 2;
+    p.chunk_bytes = cb;
+    p.pool = (char*)b->pool;
+    p.split = (unsigned long long)Q * R0;
+    p.region = (unsigned int)R0;
+    p.fin = (double*)b->fin;
+    std::vector<uint32_t> h_nev(Q);
     RTW_CUDA(cudaEventRecord(ev[0], s), "event");
     RTW_CUDA(cudaMemsetAsync(b->out, 0, b->out_cap, s), "clear outputs");
     RTW_CUDA(cudaMemsetAsync(b->ctl, 0, 1024, s), "reset counters");
-    p.record = 0;
     RTW_CUDA(launch_forward(p, mixed, run.grid, s), "torus forward");
-    RTW_CUDA(cudaEventRecord(ev[1], s), "event");
-    // offsets (host scan of the counts)
-    std::vector<uint32_t> h_nev(Q);
     RTW_CUDA(cudaMemcpyAsync(h_nev.data(), nev, 4 * Q, cudaMemcpyDeviceToHost, s), "counts D2H");
     RTW_CUDA(cudaStreamSynchronize(s), "forward");
-    std::vector<unsigned long long> h_off(2 * Q);
-    unsigned long long E = 0, C = 0;
+    RTW_CUDA(cudaEventRecord(ev[1], s), "event");
+    // 1b. rays with more segments than R0 (and no polar escape): recorded
+    // again, alone, into pool2 at exact offsets
+    std::vector<uint32_t> h_l2;
+    std::vector<unsigned long long> h_b2, h_rb(Q);
+    unsigned long long used = p.split, extra = 0;
     for (long long i = 0; i < Q; ++i) {
-        h_off[i] = E;
-        h_off[Q + i] = C;
-        const uint32_t n = h_nev[i] & kEventCount;
-        const uint32_t kc = (h_nev[i] & kDenseCheckpoints) ? 1u : (uint32_t)KC;
-        E += n;
-        C += (n + kc - 1) / kc + 1;  // segment starts + the final state
+        h_rb[i] = (unsigned long long)i * R0;
+        if ((h_nev[i] & kOverflow) && !(h_nev[i] & kDenseCheckpoints)) {
+            const unsigned long long nseg = ((h_nev[i] & kEventCount) + KC - 1) / KC;
+            h_rb[i] = p.split + extra;
+            h_l2.push_back((uint32_t)i);
+            h_b2.push_back(h_rb[i]);
+            extra += nseg;
+        }
     }
-    RTW_CUDA(cudaMemcpyAsync(ev_off, h_off.data(), 16 * Q, cudaMemcpyHostToDevice, s), "offsets H2D");
-    if ((st = ensure(ctx, &b->evh, &b->evh_cap, std::max<size_t>(8 * E, 256))) != RTW_OK) return st;
-    if ((st = ensure(ctx, &b->evk, &b->evk_cap, std::max<size_t>(E, 256))) != RTW_OK) return st;
+    used += extra;
+    const long long n2 = (long long)h_l2.size();
+    RTW_CUDA(cudaEventRecord(ev[2], s), "event");
+    if (n2 > 0) {
+        if ((st = ensure(ctx, &b->pool2, &b->pool2_cap, (size_t)extra * cb)) != RTW_OK) return st;
+        RTW_CUDA(cudaMemcpyAsync(list2, h_l2.data(), 4 * n2, cudaMemcpyHostToDevice, s), "list H2D");
+        RTW_CUDA(cudaMemcpyAsync(base2, h_b2.data(), 8 * n2, cudaMemcpyHostToDevice, s), "bases H2D");
+        TorusKP p2 = p;
+        p2.pool2 = (char*)b->pool2;
+        p2.region = 0;
+        p2.chunk_base = base2;
+        p2.ray_list = list2;
+        p2.total_rays = n2;
+        p2.spectrum = nullptr;  // the first pass's image stays
+        p2.xyz = nullptr;
+        p2.cls = nullptr;
+        p2.steps = nullptr;
+        RTW_CUDA(cudaMemsetAsync(b->ctl, 0, 8, s), "reset queue");
+        RTW_CUDA(launch_forward(p2, mixed, run.grid, s), "torus record of long rays");
+        p.pool2 = p2.pool2;
+    }
+    RTW_CUDA(cudaMemcpyAsync(rbase, h_rb.data(), 8 * Q, cudaMemcpyHostToDevice, s), "chunk bases H2D");
+    // 2. rays with a polar escape whose gradient is wanted: a second recording
+    // pass over them alone, with the full state before every event
+    unsigned long long E = 0, C = 0;
+    std::vector<uint32_t> h_list, h_nd, h_esc(Q, 0xffffffffu);
+    for (long long i = 0; i < Q; ++i) {
+        E += h_nev[i] & kEventCount;
+        if ((h_nev[i] & kDenseCheckpoints) && adj->escape_rays != 1) {
+            h_esc[i] = (uint32_t)h_list.size();
+            h_list.push_back((uint32_t)i);
+            h_nd.push_back(h_nev[i]);
+        }
+    }
+    const long long nB = (long long)h_list.size();
+    std::vector<unsigned long long> h_off(2 * std::max<long long>(nB, 1));
+    unsigned long long Ed = 0;
+    for (long long j = 0; j < nB; ++j) {
+        h_off[j] = Ed;
+        h_off[nB + j] = C;
+        const uint32_t n = h_nd[j] & kEventCount;
+        Ed += n;
+        C += n + 1;  // one row before every event + the final state
+    }
+    if ((st = ensure(ctx, &b->evh, &b->evh_cap, std::max<size_t>(8 * Ed, 256))) != RTW_OK) return st;
+    if ((st = ensure(ctx, &b->evk, &b->evk_cap, std::max<size_t>(Ed, 256))) != RTW_OK) return st;
     if ((st = ensure(ctx, &b->ck, &b->ck_cap, std::max<size_t>(8 * C * (size_t)D, 256))) != RTW_OK) return st;
-    // 2. record pass
-    p.record = 1;
-    p.ev_off = ev_off;
-    p.ck_off = ck_off;
+    RTW_CUDA(cudaMemcpyAsync(esc_index, h_esc.data(), 4 * Q, cudaMemcpyHostToDevice, s), "dense index H2D");
     p.ev_h = (double*)b->evh;
     p.ev_kind = (uint8_t*)b->evk;
     p.ck = (double*)b->ck;
-    p.spectrum = nullptr;  // the forward pass's image stays
-    p.cls = nullptr;
-    p.steps = nullptr;
-    RTW_CUDA(cudaEventRecord(ev[2], s), "event");
-    RTW_CUDA(cudaMemsetAsync(b->ctl, 0, 8, s), "reset queue");
-    RTW_CUDA(launch_forward(p, mixed, run.grid, s), "torus record");
+    p.ev_off = ev_off;
+    p.ck_off = ev_off + nB;
+    if (nB > 0) {
+        RTW_CUDA(cudaMemcpyAsync(ray_list, h_list.data(), 4 * nB, cudaMemcpyHostToDevice, s), "list H2D");
+        RTW_CUDA(cudaMemcpyAsync(nev_d, h_nd.data(), 4 * nB, cudaMemcpyHostToDevice, s), "counts H2D");
+        RTW_CUDA(cudaMemcpyAsync(ev_off, h_off.data(), 16 * nB, cudaMemcpyHostToDevice, s), "offsets H2D");
+        TorusKP pd = p;
+        pd.record = 1;
+        pd.ray_list = ray_list;
+        pd.total_rays = nB;
+        pd.n_events = nev_d;
+        pd.spectrum = nullptr;  // the first pass's image stays
+        pd.xyz = nullptr;
+        pd.cls = nullptr;
+        pd.steps = nullptr;
+        RTW_CUDA(cudaMemsetAsync(b->ctl, 0, 8, s), "reset queue");
+        RTW_CUDA(launch_forward(pd, mixed, run.grid, s), "torus dense record");
+    }
     RTW_CUDA(cudaEventRecord(ev[3], s), "event");
     // 3. reverse pass
     int occ = 0;
@@ -1460,6 +1664,8 @@ rtw_status rtw_adjoint(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* c
     if ((st = ensure(ctx, &b->work, &b->work_cap, std::max<size_t>(per_ray_b, 256))) != RTW_OK) return st;
     rp.f = p;
     rp.f.spectrum = spec;
+    rp.esc_index = esc_index;
+    rp.rbase = rbase;
     rp.target = (const float*)b->tgt;
     rp.spectrum = spec;
     rp.per_ray = adj->per_ray_grad ? (double*)b->work : nullptr;
@@ -1505,10 +1711,10 @@ rtw_status rtw_adjoint(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* c
     res->reverse_ms = t45;
     res->total_ms = t05;
     res->events = E;
-    res->checkpoints = C;
+    res->checkpoints = used + C;  // chunk slots (the first pass's regions whole) + dense rows
     res->escape_cuts = (uint64_t)h_out[1 + kTorusParams];
     res->escape_rays = (uint64_t)h_out[2 + kTorusParams];
-    res->scratch_bytes = 8 * E + E + 8 * C * (size_t)D + work_b + nev_b + 16 * Q;
+    res->scratch_bytes = (size_t)used * cb + (size_t)Q * D * 8 + 9 * Ed + 8 * C * (size_t)D + work_b + nev_b;
     ctx->have_last = false;
     return RTW_OK;
 }
