@@ -402,7 +402,8 @@ rtw_status rtw_torus_vjp(const rtw_scene* scene, const double* colors_nm, int32_
  * cot for the end state, pbar the parameter part, hbar = d loss / d h; form 0
  * is the adjoint kernel's structured reverse, form 1 the generic one over the
  * whole state, form 2 the structured one with the optical depths run back
- * from the end of the step (the adjoint kernel's form). For tests. */
+ * from the end of the step (the adjoint kernel's form), form 3 form 2 with
+ * FP32 bin partials (the FP32-mixed adjoint's). For tests. */
 rtw_status rtw_torus_step_vjp(const rtw_scene* scene, const double* colors_nm, int32_t n_colors,
                               const double* state, double h, const double* cot, int32_t form, double* mu,
                               double* pbar, double* hbar);

@@ -25,6 +25,7 @@
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "rtw_ctx.h"
@@ -928,7 +929,10 @@ RTW_HD double torus_dp_vjp_generic(const TorusModel& m, const double* y, const d
 // depend on the geodesic alone (tau' = ft(emitter numbers)), so with
 // tau_at_end the step is run backwards for tau: tau holds the depths at the
 // end of the step on entry and those at its start on return (the intensities
-// enter no slope, so the reverse sweep never needs them).
+// enter no slope, so the reverse sweep never needs them). BT: arithmetic of
+// the bins' partials (double, or float for the FP32-mixed adjoint); the
+// cotangents accumulate in FP64 either way.
+template <class BT>
 RTW_HD double torus_dp_vjp(const TorusModel& m, const double* y, const double* Kg, double* tau, bool tau_at_end,
                            double h, double* lam, double* pb) {
     const int N = m.n;
@@ -959,12 +963,18 @@ RTW_HD double torus_dp_vjp(const TorusModel& m, const double* y, const double* K
     // (2) bins
     for (int c = 0; c < N; ++c) {
         const int it = 8 + c, ii = 8 + N + c;
-        double Kt[6], fi[6], ex[6], dft[6][4] = {}, dfi[6][4] = {}, kt[6];
+        double Kt[6], fi[6], ex[6], kt[6];
+        BT dft[6][4] = {}, dfi[6][4] = {};
         const double lt = lam[it], li = lam[ii];
         double bkt = 0, bki = 0;
         for (int t = 0; t < 6; ++t) {
             Kt[t] = fi[t] = 0;
-            if (on[t]) torus_bin_grad_pre(pre[t], m.bins[c], Kt[t], fi[t], dft[t], dfi[t]);
+            if (on[t]) {
+                BT ft_, fi_;
+                torus_bin_grad_pre<BT>(pre[t], m.bins[c], ft_, fi_, dft[t], dfi[t]);
+                Kt[t] = ft_;
+                fi[t] = fi_;
+            }
             bkt += tA(6, t) * Kt[t];
         }
         double t0 = tau[c];
@@ -975,7 +985,7 @@ RTW_HD double torus_dp_vjp(const TorusModel& m, const double* y, const double* K
         for (int t = 0; t < 6; ++t) {
             double acc = 0;
             for (int s = 0; s < t; ++s) acc += tA(t, s) * Kt[s];
-            ex[t] = on[t] ? exp(-(t0 + h * acc)) : 0.0;
+            ex[t] = on[t] ? (double)BinMath<BT>::ex(BT(-(t0 + h * acc))) : 0.0;
             bki += tA(6, t) * fi[t] * ex[t];
             kt[t] = h * tA(6, t) * lt;
         }
@@ -984,7 +994,7 @@ RTW_HD double torus_dp_vjp(const TorusModel& m, const double* y, const double* K
         for (int t = 5; t >= 0; --t) {
             if (!on[t]) continue;  // no emitter: the bin's slopes are 0 there
             const double ki = h * tA(6, t) * li, e = ex[t];
-            for (int q = 0; q < 4; ++q) Sbar[t][q] += kt[t] * dft[t][q] + ki * e * dfi[t][q];
+            for (int q = 0; q < 4; ++q) Sbar[t][q] += kt[t] * (double)dft[t][q] + ki * e * (double)dfi[t][q];
             const double mt = -ki * fi[t] * e;  // d (fi exp(-tau)) / d tau
             msum += mt;
             double ak = 0;
@@ -1061,6 +1071,7 @@ constexpr int kTorusMaxD = 8 + 2 * kTorusMaxBins;  // state components
 // before every event (Ys [2][D], Kw [6][D] stage slopes, Ze [4][D] escape
 // evaluations). The arrays live in local memory,
 // whose layout interleaves the lanes of a warp (same-index accesses coalesce).
+template <bool MIXED>
 __global__ void __launch_bounds__(128, 4) torus_reverse(const TorusRP p) {
     const TorusModel& m = p.f.m;
     const int N = m.n, D = 8 + 2 * N;
@@ -1100,7 +1111,8 @@ __global__ void __launch_bounds__(128, 4) torus_reverse(const TorusRP p) {
                 lam[2] = -lam[2];
                 lam[6] = -lam[6];
             }
-            const double hbar = torus_dp_vjp(m, g, Kg, taus, tau_at_end, hv, lam, pb);
+            const double hbar = torus_dp_vjp<typename std::conditional<MIXED, float, double>::type>(
+                m, g, Kg, taus, tau_at_end, hv, lam, pb);
             // a pending step-size term of the next step lands on this state
             if (pend != 0) torus_pad_vjp(g, p.f.max_dt_scale, pend, lam);
             pend = 0;
@@ -1655,7 +1667,8 @@ rtw_status rtw_adjoint(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* c
     RTW_CUDA(cudaEventRecord(ev[3], s), "event");
     // 3. reverse pass
     int occ = 0;
-    RTW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, torus_reverse, 128, 0), "occupancy");
+    const void* rev_fn = mixed ? (const void*)torus_reverse<true> : (const void*)torus_reverse<false>;
+    RTW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, rev_fn, 128, 0), "occupancy");
     const int rgrid = ctx->num_sms * std::max(1, occ);
     // local-memory work area of the reverse kernel (per resident thread)
     const size_t work_b = (size_t)rgrid * 128 *
@@ -1677,7 +1690,7 @@ rtw_status rtw_adjoint(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* c
     RTW_CUDA(cudaEventRecord(ev[4], s), "event");
     {
         void* args[] = {(void*)&rp};
-        RTW_CUDA(cudaLaunchKernel((const void*)torus_reverse, dim3(rgrid), dim3(128), args, 0, s), "torus reverse");
+        RTW_CUDA(cudaLaunchKernel(rev_fn, dim3(rgrid), dim3(128), args, 0, s), "torus reverse");
     }
     RTW_CUDA(cudaEventRecord(ev[5], s), "event");
     double h_out[3 + kTorusParams];
@@ -1819,8 +1832,9 @@ rtw_status rtw_torus_step_vjp(const rtw_scene* scene, const double* colors_nm, i
         // form 2 starts from the depths at the end of the step
         std::vector<double> y1(D);
         torus_dp_stages(m, y.data(), h, K.data(), Y.data(), y1.data());
-        for (int c = 0; c < N; ++c) taus[c] = form == 2 ? y1[8 + c] : y[8 + c];
-        *hbar = torus_dp_vjp(m, y.data(), Kg, taus, form == 2, h, lam.data(), pb);
+        for (int c = 0; c < N; ++c) taus[c] = form >= 2 ? y1[8 + c] : y[8 + c];
+        *hbar = form == 3 ? torus_dp_vjp<float>(m, y.data(), Kg, taus, true, h, lam.data(), pb)
+                          : torus_dp_vjp<double>(m, y.data(), Kg, taus, form == 2, h, lam.data(), pb);
     }
     for (int i = 0; i < 8; ++i) mu[i] = lam[i];
     for (int c = 0; c < N; ++c) {

@@ -351,34 +351,58 @@ RTW_HD TorusBinPre torus_bin_pre(double cj, double nus, double th, double g) {
     return q;
 }
 
+// exp and expm1 in the arithmetic of the bins' partials: FP64, or FP32 with
+// the hardware exponential (the FP32-mixed adjoint, whose forward evaluates
+// the same slopes in FP32)
+template <class T>
+struct BinMath;
+template <>
+struct BinMath<double> {
+    static RTW_HD double ex(double x) { return exp(x); }
+    static RTW_HD double em1(double x) { return expm1(x); }
+};
+template <>
+struct BinMath<float> {
+#ifdef __CUDA_ARCH__
+    static __device__ float ex(float x) { return __expf(x); }
+#else
+    static float ex(float x) { return std::exp(x); }
+#endif
+    static RTW_HD float em1(float x) { return expm1f(x); }
+};
+
 // torus_bin_grad from the shared part: three transcendentals per bin
-// (X^1/6; X^1/3 and X^1/2 as its square and cube) instead of six.
-RTW_HD void torus_bin_grad_pre(const TorusBinPre& q, const TorusBin& bn, double& ft, double& fi, double* dft,
-                               double* dfi) {
-    const double lx = q.L + bn.ln_nu;
-    if (!q.ok || !(lx <= 12.206072645530174)) {  // X > 2e5: exp(-X^1/3) < 1e-25, no emission
+// (X^1/6; X^1/3 and X^1/2 as its square and cube) instead of six, in
+// arithmetic T.
+template <class T>
+RTW_HD void torus_bin_grad_pre(const TorusBinPre& q, const TorusBin& bn, T& ft, T& fi, T* dft, T* dfi) {
+    const double lxd = q.L + bn.ln_nu;
+    if (!q.ok || !(lxd <= 12.206072645530174)) {  // X > 2e5: exp(-X^1/3) < 1e-25, no emission
         ft = fi = 0;
         for (int k = 0; k < 4; ++k) dft[k] = dfi[k] = 0;
         return;
     }
-    const double c = 1.8877486253633868;  // 2^(11/12)
-    const double x16 = exp(lx * (1.0 / 6.0)), x13 = x16 * x16, x12 = x13 * x16;
-    const double P = x12 + c * x16;
-    const double j = q.cjnus * P * P * exp(-x13);
-    fi = -(j * bn.inv_nu_nm3 * q.ig4);
-    const double y = q.gt * bn.hk;
-    const double em1 = expm1(y);
-    ft = -(j * em1 * q.ig4 * bn.inv_b0);
-    const double DX = (x12 + c / 3.0 * x16) / P - x13 * (1.0 / 3.0);
-    const double Dy = y * (em1 + 1.0) / em1;
-    dfi[0] = fi * q.icj;
-    dfi[1] = fi * (1.0 - DX) * q.inus;
+    const T lx = T(lxd);
+    const T c = T(1.8877486253633868);  // 2^(11/12)
+    const T x16 = BinMath<T>::ex(lx * T(1.0 / 6.0)), x13 = x16 * x16, x12 = x13 * x16;
+    const T P = x12 + c * x16;
+    const T j = T(q.cjnus) * P * P * BinMath<T>::ex(-x13);
+    const T ig4 = T(q.ig4);
+    fi = -(j * T(bn.inv_nu_nm3) * ig4);
+    const T y = T(q.gt * bn.hk);
+    const T em1 = BinMath<T>::em1(y);
+    ft = -(j * em1 * ig4 * T(bn.inv_b0));
+    const T DX = (x12 + c * T(1.0 / 3.0) * x16) / P - x13 * T(1.0 / 3.0);
+    const T Dy = y * (em1 + T(1)) / em1;
+    const T icj = T(q.icj), inus = T(q.inus), ig = T(q.ig);
+    dfi[0] = fi * icj;
+    dfi[1] = fi * (T(1) - DX) * inus;
     dfi[2] = 0;
-    dfi[3] = fi * (DX - 4.0) * q.ig;
-    dft[0] = ft * q.icj;
-    dft[1] = ft * (1.0 - DX) * q.inus;
-    dft[2] = -ft * Dy * q.ith;
-    dft[3] = ft * (DX - 4.0 + Dy) * q.ig;
+    dfi[3] = fi * (DX - T(4)) * ig;
+    dft[0] = ft * icj;
+    dft[1] = ft * (T(1) - DX) * inus;
+    dft[2] = -ft * Dy * T(q.ith);
+    dft[3] = ft * (DX - T(4) + Dy) * ig;
 }
 
 RTW_HD void torus_bin_grad(double cj, double nus, double th, double g, const TorusBin& bn, double& ft, double& fi,

@@ -144,6 +144,12 @@ def test_structured_step_vjp_matches_generic():
                 np.testing.assert_allclose(w, v, rtol=1e-10, atol=1e-12 * np.abs(v).max())
             assert a[2] == pytest.approx(b[2], rel=1e-11, abs=1e-13 * abs(b[2]) + 1e-300)
             assert back[2] == pytest.approx(b[2], rel=1e-10, abs=1e-12 * abs(b[2]) + 1e-300)
+            # FP32 bin partials (the FP32-mixed adjoint): FP32 rounding, which
+            # parameter components that cancel between bins amplify
+            f32 = abi.torus_step_vjp(sc, col, y, h, cot, 3)
+            np.testing.assert_allclose(f32[0], b[0], rtol=2e-5, atol=1e-5 * np.abs(b[0]).max())
+            np.testing.assert_allclose(f32[1], b[1], rtol=1e-3, atol=1e-5 * np.abs(b[1]).max())
+            assert f32[2] == pytest.approx(b[2], rel=2e-5, abs=1e-5 * abs(b[2]) + 1e-300)
             # d loss / d h against a central difference of the step
             dh = 1e-6 * abs(h)
             lp = cot @ _step(sc, col, y, h + dh)
