@@ -88,7 +88,16 @@ typedef enum rtw_scene_kind {
        (p = 2.5, gamma 30..1e9, anisotropy fit) in a global field B^phi = b_0,
        electron density n_e0 (m^-3), map scale length_cm
        (source_model.jl:7-317). Per-bin tau; both integrators. */
-    RTW_SCENE_KERR_POWEHI = 5
+    RTW_SCENE_KERR_POWEHI = 5,
+    /* Synchro_Test.source, the reference's flat-space synchrotron test:
+       Minkowski space in Cartesian coordinates (t, x, y, z) (camera
+       position and ray states are Cartesian), a static cylinder x^2 + y^2 <=
+       r_out^2 around the z axis in a uniform field B^z = b_0 (gauss),
+       radiating power-law synchrotron (p = 2.5, gamma 30..1e9, anisotropy
+       fit) with n_e0 (m^-3) and map scale length_cm; rays end beyond
+       |x| = escape_radius (source_geometry.jl:7-88, source_model.jl:7-278).
+       Per-bin tau; both integrators. */
+    RTW_SCENE_SYNCHRO_TEST = 6
 } rtw_scene_kind;
 
 /* How a ray ended. The reference's calc_terminate (e.g. Kerr.source/

@@ -25,7 +25,8 @@
 //   CIE fit, weights, I_lambda               main/color_theory.jl:11-108
 //   Heaviside                                main/my_special_functions.jl:9-15
 //   scenes: main/Minkowski_Sphere_Spherical.source/, main/Schwarzschild_Simple_
-//           Disk_Spherical.source/, main/Kerr.source/ (geometry + model files).
+//           Disk_Spherical.source/, main/Kerr.source/, main/Powehi.source/,
+//           main/Synchro_Test.source/ (geometry + model files).
 //
 // Deliberate differences from the reference, shared with the CUDA library:
 //  * Scene constants (spin, disk extent, temperature, a_nu, escape radius) are
@@ -149,6 +150,8 @@ struct OScene {
         return kind == RTW_SCENE_KERR_DISK || kind == RTW_SCENE_KERR_THICK_DISK || kind == RTW_SCENE_KERR_SYNCHRO_TORUS ||
                kind == RTW_SCENE_KERR_POWEHI;
     }
+    // Synchro_Test.source: Minkowski space in Cartesian (t, x, y, z)
+    bool is_cart() const { return kind == RTW_SCENE_SYNCHRO_TEST; }
 
     // --- geometry -----------------------------------------------------------
     // Kerr calc_metric_params, source_geometry.jl:55-60
@@ -163,7 +166,9 @@ struct OScene {
         for (int i = 0; i < 4; ++i)
             for (int j = 0; j < 4; ++j) g[i][j] = (i == j) ? 1.0 : 0.0;
         const double r = x[1], th = x[2];
-        if (is_kerr()) {
+        if (is_cart()) {  // Synchro_Test source_geometry.jl:7-16
+            g[0][0] = -1.0;
+        } else if (is_kerr()) {
             double Sig, Del, A;
             kerr_params(r, th, Sig, Del, A);
             g[0][0] = -(1.0 - rs * r / Sig);
@@ -189,6 +194,7 @@ struct OScene {
     void inv_vierbein(const double* x, double e[4][4]) const {
         for (int i = 0; i < 4; ++i)
             for (int j = 0; j < 4; ++j) e[i][j] = (i == j) ? 1.0 : 0.0;
+        if (is_cart()) return;  // Synchro_Test source_geometry.jl:44-50
         const double r = x[1], th = x[2];
         if (is_kerr()) {
             double Sig, Del, A;
@@ -258,6 +264,7 @@ struct OScene {
     // calc_christoffel_udd!: Kerr :195-243, Schwarzschild :109-128, Minkowski :93-108
     void christoffel(const double* x, double G[4][4][4]) const {
         std::memset(G, 0, sizeof(double) * 64);
+        if (is_cart()) return;  // Synchro_Test source_geometry.jl:53-66
         const double r = x[1], th = x[2];
         if (is_kerr()) {
             if (refprec)
@@ -293,6 +300,10 @@ struct OScene {
 
     // near_singularity: Kerr :249-269 (= Schwarzschild :134-154), Minkowski :114-132
     bool near_singularity(const double* x, double h, double tol, double* temp) const {
+        if (is_cart()) {  // Synchro_Test source_geometry.jl:69-73
+            *temp = h;
+            return false;
+        }
         const double th_new = x[2] + h * x[6];
         const double r_new = x[1] + h * x[5];
         if (kind == RTW_SCENE_MINKOWSKI_SPHERE) {
@@ -323,6 +334,7 @@ struct OScene {
 
     // keepinbounds!: Kerr :275-301 (= Schwarzschild :160-186), Minkowski :138-163
     void keepinbounds(double* x) const {
+        if (is_cart()) return;  // Synchro_Test source_geometry.jl:76-80
         if (kind == RTW_SCENE_MINKOWSKI_SPHERE && x[1] <= 0) {
             x[1] = -x[1] + kNoDivZero;
             x[5] = -x[5];
@@ -344,6 +356,7 @@ struct OScene {
 
     // is_singularity: Kerr :307-315 and the other scenes
     bool is_singularity(const double* pos) const {
+        if (is_cart()) return false;  // Synchro_Test source_geometry.jl:84-88
         if (std::fabs(pos[1]) <= (double)1e-32f) return true;
         if (std::fabs(pos[2]) <= (double)1e-32f || std::fabs(pos[2] - kPi) <= 1e-32) return true;
         return false;
@@ -418,6 +431,7 @@ struct OScene {
 
     // pad_max_dt: Kerr model :86-103, Schwarzschild :86-106, Minkowski :89-105
     double pad_max_dt(const double* x, double scale) const {
+        if (is_cart()) return scale * (1 + std::fabs(x[1]) + std::fabs(x[2]));  // Synchro_Test model :241-244
         double eps;
         // Kerr casts the scale to Float32 (Kerr model :92-96); the other scenes
         // keep it in Float64 except for the Float32 literal 1f-1.
@@ -446,6 +460,13 @@ struct OScene {
     // Returns the class of the first predicate that holds, or 0.
     int terminate(const double* ray, int L, double tol, long long max_steps, long long step_count) const {
         if ((double)step_count >= (double)max_steps) return RTW_CLASS_MAXSTEPS;
+        if (is_cart()) {  // Synchro_Test model :258-275
+            if (std::sqrt(ray[1] * ray[1] + ray[2] * ray[2] + ray[3] * ray[3]) > esc) return RTW_CLASS_ESCAPE;
+            const double thick = -std::log(tol);
+            for (int i = 9; i < L; i += 2)
+                if (ray[i] < thick) return 0;
+            return RTW_CLASS_THICK;
+        }
         if (ray[1] > esc) return RTW_CLASS_ESCAPE;
         if (kind != RTW_SCENE_MINKOWSKI_SPHERE && ray[1] <= (1 + 10 * tol) * r_ev) return RTW_CLASS_HORIZON;
         if (ray[3] > wind) return RTW_CLASS_WINDING;
@@ -632,6 +653,73 @@ void powehi_bins(const OScene& sc, RayWork& w, const double* R, double* slope) {
     }
 }
 
+// RT slopes of Synchro_Test.source (the reference's flat-space synchrotron
+// test, source_model.jl: is_fire :229-236, static fluid :250-256,
+// calc_B_field :47-54, transform_B_b :60-108, calc_b_angle :114-146,
+// calc_fluid_params! :152-172, calc_radiative_coefficients :186-224), with
+// the reference's constants, written over the general metric-contraction
+// forms (g = diag(-1, 1, 1, 1), u = (1, 0, 0, 0)). A ray along the field
+// (sin theta_B = 0, where the reference's j is 0 * inf) gets no emission.
+void synchro_bins(const OScene& sc, RayWork& w, const double* R, double* slope) {
+    for (int c = 0; c < w.N; ++c) {
+        slope[8 + 2 * c] = 0;
+        slope[9 + 2 * c] = 0;
+    }
+    if (!(std::sqrt(R[1] * R[1] + R[2] * R[2]) <= sc.r_out)) return;
+    sc.lower_metric(R, w.g);
+    const double (*g)[4] = w.g;
+    const double u[4] = {1, 0, 0, 0};
+    double fs = 0;  // calc_freq_shift
+    for (int j = 0; j < 4; ++j) {
+        double ps = 0;
+        for (int i = 0; i < 4; ++i) ps += g[i][j] * R[i + 4];
+        fs -= u[j] * ps;
+    }
+    const double B[4] = {0, 0, 0, sc.b0};  // (B^x, B^y, B^z) = (0, 0, 10 G)
+    double b[4];
+    b[0] = 0;
+    for (int col = 1; col < 4; ++col) {
+        double ps = 0;
+        for (int i = 0; i < 4; ++i) ps += g[i][col] * u[i];
+        b[0] += B[col] * ps;
+    }
+    for (int mu = 1; mu < 4; ++mu) b[mu] = (B[mu] + b[0] * u[mu]) / u[0];
+    double bmag2 = 0;
+    for (int mu = 0; mu < 4; ++mu) {
+        double cs = 0;
+        for (int i = 0; i < 4; ++i) cs += g[i][mu];
+        bmag2 += cs * b[mu] * b[mu];
+    }
+    double bk = 0;
+    for (int mu = 0; mu < 4; ++mu) {
+        double ps = 0;
+        for (int i = 0; i < 4; ++i) ps += g[i][mu] * R[i + 4];
+        bk += b[mu] * ps;
+    }
+    const double cos2 = bk * bk / (bmag2 * fs * fs);
+    if (!(1 - cos2 > 0)) return;
+    const double p = 2.5, gmin = 30.0, gmax = 1e9, ne0 = sc.n0, map_scale = sc.length_cm / 100.0;
+    const double synch_em = 7.694e-37 * map_scale * 2.8e7, synch_ab = 2.8173e-24 * map_scale;
+    const double nuc = 9.34e-11 * std::sqrt(bmag2);
+    const double sinth = std::sqrt(1 - cos2);
+    const double pfit = std::exp(7.951834e-01 + (-5.752283e-01) * p) * std::pow(p, 9.832989e-01 * p);
+    const double Phi = (1 / pfit) * std::pow(1 - 0.99 * cos2, -p / 2);
+    const double gd = std::pow(gmin, 1 - p) - std::pow(gmax, 1 - p);
+    for (int c = 0; c < w.N; ++c) {
+        const double nu = w.freq[c] * fs;
+        double j_nu = ne0 * synch_em * (nuc / 9.34e-11);
+        double a_nu = ne0 * synch_ab / nu;
+        j_nu *= std::pow(3.0, p / 2) * (p - 1) * sinth / (2 * (p + 1) * gd);
+        j_nu *= std::tgamma((3 * p - 1) / 12) * std::tgamma((3 * p + 19) / 12) * std::pow(nu / (nuc * sinth), -(p - 1) / 2);
+        a_nu *= std::pow(3.0, (p + 1) / 2) * (p - 1) / (4 * gd);
+        a_nu *= std::tgamma((3 * p + 2) / 12) * std::tgamma((3 * p + 22) / 12) * std::pow(nu / (nuc * sinth), -(p + 2) / 2);
+        j_nu *= Phi;
+        a_nu *= Phi;
+        slope[8 + 2 * c] = -(1 / fs) * j_nu * std::exp(-R[9 + 2 * c]) / (nu * nu * nu);
+        slope[9 + 2 * c] = -(1 / fs) * a_nu;
+    }
+}
+
 // calc_ray_derivative!, integrators_LttM.jl:9-48
 void rhs(const OScene& sc, RayWork& w, const double* R, double* slope) {
     for (int i = 0; i < 4; ++i) slope[i] = R[i + 4];
@@ -648,6 +736,10 @@ void rhs(const OScene& sc, RayWork& w, const double* R, double* slope) {
     }
     if (sc.kind == RTW_SCENE_KERR_POWEHI) {
         powehi_bins(sc, w, R, slope);
+        return;
+    }
+    if (sc.kind == RTW_SCENE_SYNCHRO_TEST) {
+        synchro_bins(sc, w, R, slope);
         return;
     }
     sc.lower_metric(R, w.g);

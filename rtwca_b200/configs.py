@@ -209,3 +209,17 @@ def powehi_camera(x_pix: int = 256, tol: float = 1e-6, max_steps: int = 20_000) 
     beta 0; the reference's default field of view (85 x 60 deg)."""
     return abi.make_camera([0.0, 35.0, 0.3, 0.0], [PI / 2, PI / 6], 0.0, [0.0, 0.0, PI], x_pix, 85.0, 60.0, tol,
                            max_steps)
+
+
+def synchro_scene() -> abi.Scene:
+    """Synchro_Test.source: flat Cartesian space, a static synchrotron cylinder
+    of radius 1 around the z axis in B^z = 10 G."""
+    return abi.scene_default(abi.SCENE_SYNCHRO_TEST)
+
+
+def synchro_camera(x_pix: int = 256, tol: float = 1e-6, max_steps: int = 20_000) -> abi.Camera:
+    """The reference's "synch" world (initialization.jl:120-128): position
+    (0, 0, 0, 0) (Cartesian t, x, y, z: inside the cylinder), direction
+    (0, 0), pointing (pi/8, 0, pi), beta 0; default field of view."""
+    return abi.make_camera([0.0, 0.0, 0.0, 0.0], [0.0, 0.0], 0.0, [PI / 8, 0.0, PI], x_pix, 85.0, 60.0, tol,
+                           max_steps)

@@ -132,6 +132,7 @@ double horizon_radius(const rtw_scene& s) {
 void inv_tetrad(const rtw_scene& s, const double* x, M4 e) {
     for (int i = 0; i < 4; ++i)
         for (int j = 0; j < 4; ++j) e[i][j] = i == j ? 1.0 : 0.0;
+    if (s.kind == RTW_SCENE_SYNCHRO_TEST) return;  // Cartesian Minkowski: the identity
     const double r = x[1], th = x[2];
     if (is_kerr(s.kind)) {
         const double a = s.spin, rs = 2 * s.mass;
@@ -316,6 +317,13 @@ rtw_status rtw_scene_default(int32_t kind, rtw_scene* s) {
         s->temperature = 5778; s->a_nu = (double)1e-2f;
         s->n_e0 = 1e7; s->b_0 = 10; s->length_cm = 9.62e14;
         break;
+    case RTW_SCENE_SYNCHRO_TEST:
+        // Synchro_Test.source: cylinder of radius 1 (source_model.jl:229-236),
+        // B^z = 10 G (:47-54), n_e0 = 1e7 m^-3 and map_scale 9.62e12 m
+        // (:7-15), rays end at |x| > 100 (:258-275)
+        s->r_out = 1; s->n_e0 = 1e7; s->b_0 = 10; s->length_cm = 9.62e14;
+        s->escape_radius = 100;
+        break;
     default:
         return RTW_ERR_INVALID_PARAM;
     }
@@ -336,7 +344,9 @@ rtw_status rtw_camera_pixels(rtw_camera* cam, int64_t* n_pix) {
 static rtw_status build_frame(const rtw_scene& s, rtw_camera& cam, FrameDesc& f) {
     rtw_status st = rtw_camera_pixels(&cam, nullptr);
     if (st != RTW_OK) return st;
-    if (on_singularity(cam.position)) return RTW_ERR_INVALID_CAMERA;
+    // (the Cartesian scene has no coordinate singularity: Synchro_Test.source/
+    // source_geometry.jl:84-88)
+    if (s.kind != RTW_SCENE_SYNCHRO_TEST && on_singularity(cam.position)) return RTW_ERR_INVALID_CAMERA;
     if (!(std::fabs(cam.speed) < 1)) return RTW_ERR_INVALID_PARAM;
     const double fh = kPi * cam.fov_hor / 180, fv = kPi * cam.fov_vert / 180;
     f.W = std::tan(fh / 2);
@@ -495,7 +505,8 @@ rtw_status rtw_render(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* ca
     if (prm->n_colors <= 0 || prm->n_colors > RTW_MAX_BINS || !prm->colors_nm)
         return fail(ctx, RTW_ERR_INVALID_PARAM, "n_colors must be 1..128 with colors_nm set");
     if (prm->ray_bundles) return fail(ctx, RTW_ERR_UNSUPPORTED, "ray bundles are not built");
-    if (scene->kind == RTW_SCENE_KERR_SYNCHRO_TORUS || scene->kind == RTW_SCENE_KERR_POWEHI)
+    if (scene->kind == RTW_SCENE_KERR_SYNCHRO_TORUS || scene->kind == RTW_SCENE_KERR_POWEHI ||
+        scene->kind == RTW_SCENE_SYNCHRO_TEST)
         return torus_render(ctx, scene, cams, n_cams, prm, out);
     if (scene->ref_precision) return fail(ctx, RTW_ERR_UNSUPPORTED, "ref_precision is an oracle-only switch");
     if (prm->precision != RTW_PREC_FP64 && prm->precision != RTW_PREC_MIXED && prm->precision != RTW_PREC_FP64_PLAIN)

@@ -74,25 +74,37 @@ struct TorusModel {
     DevScene geo;  // Kerr geodesic functor (its thin disk switched off)
     TorusDev tor;
     PowehiDev pw;
+    SynchroDev sy;
     TorusBin bins[kTorusMaxBins];
     int n;         // bins
-    int emitter;   // 0: synchrotron torus, 1: Powehi (disk + jet)
+    int emitter;   // 0: synchrotron torus, 1: Powehi (disk + jet), 2: Synchro_Test cylinder
+    int flat;      // geometry: 0 Kerr (Boyer-Lindquist), 1 Minkowski (Cartesian)
 };
 
 // The scene's emitter at a stage point z (x^mu, k^mu) and the slopes of bin c.
-template <class R>
+// (GEO: -1 the model's geometry at run time, 0 Kerr, 1 flat: the kernels
+// instantiate one geometry each, so the other's emitters stay out of them)
+template <class R, int GEO = -1>
 RTW_HD TorusPt<R> em_point(const TorusModel& m, const R* z) {
+    if (GEO == 1 || (GEO == -1 && m.emitter == 2)) return synchro_point<R>(m.sy, z);
     if (m.emitter == 1) return powehi_point<R>(m.pw, z);
     return torus_point<R>(m.tor, R(m.tor.a), R(m.tor.n0), R(m.tor.B0), R(m.tor.Th0), z[1], z[2], z[4], z[7]);
 }
 template <class R>
 RTW_HD void em_bin(const TorusModel& m, const TorusPt<R>& S, int c, R& ft, R& fi) {
-    if (m.emitter == 1) powehi_bin<R>(m.pw, S, m.bins[c].nu_nm, ft, fi);
+    if (m.emitter != 0) powehi_bin<R>(m.pw, S, m.bins[c].nu_nm, ft, fi);
     else torus_bin<R>(S.cj, S.nus, S.th, S.g, m.bins[c], ft, fi);
 }
 
 // The geodesic part of the right-hand side (8 components of y).
 RTW_HD void torus_geo_rhs(const TorusModel& m, const double* y, double* f) {
+    if (m.flat) {  // straight lines (Synchro_Test.source/source_geometry.jl:55-66)
+        for (int i = 0; i < 4; ++i) {
+            f[i] = y[4 + i];
+            f[4 + i] = 0;
+        }
+        return;
+    }
     double z[10], k[9];
     for (int i = 0; i < 8; ++i) z[i] = y[i];
     z[8] = 0;
@@ -282,7 +294,7 @@ struct TorusStages {
 
 // The seven geodesic stages of one attempt in arithmetic R from the FP64
 // state x and the carried slope k1.
-template <class R, class K>
+template <class R, class K, bool FLAT>
 __device__ void torus_geo_stages(const TorusModel& m, const double* x, const K* k1, double h, TorusStages<R>& o) {
     R Kg[7][8];
     for (int i = 0; i < 8; ++i) Kg[0][i] = R(k1[i]);
@@ -300,10 +312,17 @@ __device__ void torus_geo_stages(const TorusModel& m, const double* x, const K* 
         for (int i = 0; i < 8; ++i) z[i] = R(x[i]) + hr * acc[i];
         z[8] = R(0);
         z[9] = d0 + hr * acc[1];
-        Emit<R> em;
-        KerrScene<false>::rhs<R>(m.geo, z, kk, em);
+        if constexpr (FLAT) {
+            for (int i = 0; i < 4; ++i) {
+                kk[i] = z[4 + i];
+                kk[4 + i] = R(0);
+            }
+        } else {
+            Emit<R> em;
+            KerrScene<false>::rhs<R>(m.geo, z, kk, em);
+        }
         for (int i = 0; i < 8; ++i) Kg[s][i] = kk[i];
-        o.S[s] = em_point<R>(m, z);
+        o.S[s] = em_point<R, FLAT ? 1 : 0>(m, z);
         if (s == 6)
             for (int i = 0; i < 8; ++i) o.ns[i] = (double)acc[i];
     }
@@ -316,19 +335,34 @@ __device__ void torus_geo_stages(const TorusModel& m, const double* x, const K* 
 }
 
 // promoted (FP64-stage) geodesic part of the mixed path, out of line
-template <class K>
+template <class K, bool FLAT>
 __device__ __noinline__ void torus_geo_stages_fp64(const TorusModel& m, const double* x, const K* k1, double h,
                                                    TorusStages<double>* o) {
-    torus_geo_stages<double, K>(m, x, k1, h, *o);
+    torus_geo_stages<double, K, FLAT>(m, x, k1, h, *o);
+}
+
+// pad_max_dt of the geometry: Kerr (source_model.jl:86-103) or
+// Synchro_Test's max_dt_scale (1 + |x| + |y|) (source_model.jl:241-244)
+template <bool FLAT, class SR>
+__device__ __forceinline__ double torus_max_dt(const TorusKP& p, const double* x) {
+    if constexpr (FLAT)
+        return p.max_dt_scale * (1 + fabs(x[1]) + fabs(x[2]));
+    else
+        return pad_max_dt<RTW_SCENE_KERR_DISK, SR>(p.m.geo, x, p.max_dt_scale);
 }
 
 // calc_terminate without the step-count predicate; THICK when every bin's
 // tau has reached -log(tol)
-template <class SR>
+template <class SR, bool FLAT>
 __device__ __forceinline__ int torus_terminate(const TorusKP& p, const double* x, const SR* tau, int N) {
-    if (x[1] > p.m.geo.esc) return RTW_CLASS_ESCAPE;
-    if (x[1] <= p.frame.r_term) return RTW_CLASS_HORIZON;
-    if (x[3] > p.m.geo.wind) return RTW_CLASS_WINDING;
+    if constexpr (FLAT) {
+        // Synchro_Test.source/source_model.jl:258-275
+        if (sqrt(x[1] * x[1] + x[2] * x[2] + x[3] * x[3]) > p.m.geo.esc) return RTW_CLASS_ESCAPE;
+    } else {
+        if (x[1] > p.m.geo.esc) return RTW_CLASS_ESCAPE;
+        if (x[1] <= p.frame.r_term) return RTW_CLASS_HORIZON;
+        if (x[3] > p.m.geo.wind) return RTW_CLASS_WINDING;
+    }
     for (int c = 0; c < N; ++c)
         if ((double)tau[c] < p.frame.thick) return 0;
     return RTW_CLASS_THICK;
@@ -432,7 +466,7 @@ __device__ __noinline__ void torus_rec_end(const TorusKP& p, TorusRec* r, long l
 // Forward kernel. SR: arithmetic of the bins and of the stages (float on the
 // mixed path, with Kahan intensities and per-ray FP64 stages near the horizon
 // and the poles; double on the FP64 path).
-template <bool MIXED>
+template <bool MIXED, bool FLAT>
 __global__ void __launch_bounds__(128) torus_forward(const TorusKP p) {
     typedef typename SpecTraits<MIXED>::SR SR;
     const int N = p.m.n;
@@ -461,7 +495,7 @@ __global__ void __launch_bounds__(128) torus_forward(const TorusKP p) {
                 ki1[c] = SR(f[8 + N + c]);
             }
         }
-        double h = -pad_max_dt<RTW_SCENE_KERR_DISK, SR>(p.m.geo, x, p.max_dt_scale);
+        double h = -torus_max_dt<FLAT, SR>(p, x);
         // where h came from: 0 the controller (held fixed by the adjoint),
         // 1 -pad_max_dt of the previous accepted step's start state, 2 -pad_max_dt
         // of the current state
@@ -496,10 +530,10 @@ __global__ void __launch_bounds__(128) torus_forward(const TorusKP p) {
         int cls = 0;
         for (;;) {
             ++c_att;
-            const double max_dt = pad_max_dt<RTW_SCENE_KERR_DISK, SR>(p.m.geo, x, p.max_dt_scale);
+            const double max_dt = torus_max_dt<FLAT, SR>(p, x);
             double temp;
             bool done = false;
-            if (near_singularity<RTW_SCENE_KERR_DISK>(x, h, tol, &temp)) {
+            if (!FLAT && near_singularity<RTW_SCENE_KERR_DISK>(x, h, tol, &temp)) {
                 // polar escape (integrators_LttM.jl:62-105) in FP64 on the full state
                 checkpoint();
                 double y[8 + 2 * kTorusMaxBins], f[8 + 2 * kTorusMaxBins];
@@ -516,7 +550,7 @@ __global__ void __launch_bounds__(128) torus_forward(const TorusKP p) {
                 int nsub = 0;
                 for (int it = 0; it < 37; ++it) {
                     if (it > 0) {
-                        if (torus_terminate<double>(p, y, y + 8, N)) continue;
+                        if (torus_terminate<double, FLAT>(p, y, y + 8, N)) continue;
                         torus_f64(p.m, y, f);
                     }
                     for (int i = 0; i < D; ++i) y[i] -= temp * f[i];
@@ -532,7 +566,7 @@ __global__ void __launch_bounds__(128) torus_forward(const TorusKP p) {
                     ihi[q] = SR(y[8 + N + q]);
                     ilo[q] = MIXED ? SR(y[8 + N + q] - (double)ihi[q]) : SR(0);
                 }
-                if (torus_terminate<double>(p, y, y + 8, N)) {
+                if (torus_terminate<double, FLAT>(p, y, y + 8, N)) {
                     done = true;
                     prev_rej = false;
                 } else {
@@ -542,7 +576,7 @@ __global__ void __launch_bounds__(128) torus_forward(const TorusKP p) {
                         kt1[q] = SR(f[8 + q]);
                         ki1[q] = SR(f[8 + N + q]);
                     }
-                    h = -pad_max_dt<RTW_SCENE_KERR_DISK, SR>(p.m.geo, x, p.max_dt_scale);
+                    h = -torus_max_dt<FLAT, SR>(p, x);
                     hsrc = 2;
                 }
             }
@@ -550,13 +584,13 @@ __global__ void __launch_bounds__(128) torus_forward(const TorusKP p) {
                 // geodesic stages
                 TorusStages<SR> st;
                 bool promote = false;
-                if (MIXED)
+                if (MIXED && !FLAT)
                     promote = (x[1] - p.m.geo.r_ev < p.promote_dr) || (x[2] < p.promote_theta) ||
                               (x[2] > kPi - p.promote_theta);
                 if (promote) {
                     ++c_pro;
                     TorusStages<double> sd;
-                    torus_geo_stages_fp64<SR>(p.m, x, k1, h, &sd);
+                    torus_geo_stages_fp64<SR, FLAT>(p.m, x, k1, h, &sd);
                     for (int i = 0; i < 8; ++i) {
                         st.ns[i] = sd.ns[i];
                         st.es[i] = sd.es[i];
@@ -571,7 +605,7 @@ __global__ void __launch_bounds__(128) torus_forward(const TorusKP p) {
                         st.S[s].zone = sd.S[s].zone;
                     }
                 } else {
-                    torus_geo_stages<SR, SR>(p.m, x, k1, h, st);
+                    torus_geo_stages<SR, SR, FLAT>(p.m, x, k1, h, st);
                 }
                 double y[8];
                 double err2 = 0;
@@ -652,7 +686,7 @@ __global__ void __launch_bounds__(128) torus_forward(const TorusKP p) {
                         kt1[c] = c_kt[c];
                         ki1[c] = c_ki[c];
                     }
-                    if (torus_keep(x) && p.fsal) {
+                    if (!FLAT && torus_keep(x) && p.fsal) {
                         // reflected through the pole: the carried slope belongs to
                         // the unreflected point, so take f at the new state (FSAL;
                         // the reference's step keeps its carried sum)
@@ -671,7 +705,7 @@ __global__ void __launch_bounds__(128) torus_forward(const TorusKP p) {
                     }
                     prev_rej = false;
                 } else {
-                    torus_keep(x);
+                    if (!FLAT) torus_keep(x);
                     prev_rej = true;
                     ++c_rej;
                 }
@@ -680,7 +714,7 @@ __global__ void __launch_bounds__(128) torus_forward(const TorusKP p) {
             }
             ++nsteps;
             if (nsteps >= p.frame.max_steps) cls = RTW_CLASS_MAXSTEPS;
-            else cls = torus_terminate<SR>(p, x, tau, N);
+            else cls = torus_terminate<SR, FLAT>(p, x, tau, N);
             if (cls) break;
         }
         bool fin = true;
@@ -1265,12 +1299,16 @@ rtw_status torus_model(const rtw_scene& s, const double* colors_nm, int N, Torus
         why = "the per-bin scenes take 1..32 bins";
         return RTW_ERR_INVALID_PARAM;
     }
-    const bool powehi = s.kind == RTW_SCENE_KERR_POWEHI;
+    const bool powehi = s.kind == RTW_SCENE_KERR_POWEHI, synchro = s.kind == RTW_SCENE_SYNCHRO_TEST;
     if (!(s.mass > 0) || !(std::fabs(s.spin) < s.mass) || !(s.b_0 > 0) || !(s.length_cm > 0) || !(s.n_e0 >= 0)) {
         why = "scene parameters out of range";
         return RTW_ERR_INVALID_PARAM;
     }
-    if (!powehi && (!(s.r_in > 0) || !(s.r_out >= s.r_in) || !(s.edge_in > 0) || !(s.edge_out > 0) ||
+    if (synchro && !(s.r_out > 0 && s.escape_radius > 0)) {
+        why = "cylinder radius and escape radius must be > 0";
+        return RTW_ERR_INVALID_PARAM;
+    }
+    if (!powehi && !synchro && (!(s.r_in > 0) || !(s.r_out >= s.r_in) || !(s.edge_in > 0) || !(s.edge_out > 0) ||
                     !(s.theta_e0 > 0) || !(s.rho_h > 0))) {
         why = "torus parameters out of range";
         return RTW_ERR_INVALID_PARAM;
@@ -1317,8 +1355,17 @@ rtw_status torus_model(const rtw_scene& s, const double* colors_nm, int N, Torus
         m.bins[c].inv_b0 = 1.0 / m.bins[c].b0;
     }
     m.n = N;
-    m.emitter = powehi ? 1 : 0;
-    if (powehi) powehi_model(s, m.geo, m.pw);
+    m.emitter = powehi ? 1 : synchro ? 2 : 0;
+    m.flat = synchro ? 1 : 0;
+    if (powehi || synchro) powehi_model(s, m.geo, m.pw);  // the power-law constants
+    if (synchro) {
+        m.sy.b_z = s.b_0;
+        m.sy.r_cyl = s.r_out;
+        m.sy.j_scale = m.pw.j_scale;
+        m.sy.a_scale = m.pw.a_scale;
+        m.sy.p_index = m.pw.p_index;
+        m.sy.inv_p_synch = m.pw.inv_p_synch;
+    }
     return RTW_OK;
 }
 
@@ -1379,15 +1426,17 @@ rtw_status torus_setup(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* c
     p.counter = ctl;
     p.stats = (DevStats*)(ctl + 1);
     p.err_flag = (unsigned int*)(ctl + 32);
-    run.grid = prm->precision == RTW_PREC_MIXED ? torus_grid(ctx, torus_forward<true>)
-                                                 : torus_grid(ctx, torus_forward<false>);
+    run.grid = prm->precision == RTW_PREC_MIXED
+                   ? (p.m.flat ? torus_grid(ctx, torus_forward<true, true>) : torus_grid(ctx, torus_forward<true, false>))
+                   : (p.m.flat ? torus_grid(ctx, torus_forward<false, true>) : torus_grid(ctx, torus_forward<false, false>));
     return RTW_OK;
 }
 
 cudaError_t launch_forward(const TorusKP& p, bool mixed, int grid, cudaStream_t st) {
     void* args[] = {(void*)&p};
-    return cudaLaunchKernel(mixed ? (const void*)torus_forward<true> : (const void*)torus_forward<false>,
-                            dim3(grid), dim3(128), args, 0, st);
+    const void* fn = p.m.flat ? (mixed ? (const void*)torus_forward<true, true> : (const void*)torus_forward<false, true>)
+                              : (mixed ? (const void*)torus_forward<true, false> : (const void*)torus_forward<false, false>);
+    return cudaLaunchKernel(fn, dim3(grid), dim3(128), args, 0, st);
 }
 
 }  // namespace
@@ -1735,7 +1784,8 @@ rtw_status rtw_adjoint(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* c
 rtw_status rtw_torus_rhs(const rtw_scene* scene, const double* colors_nm, int32_t n_colors, int32_t form,
                          const double* state, double* slope) {
     if (!scene || !state || !slope ||
-        (scene->kind != RTW_SCENE_KERR_SYNCHRO_TORUS && scene->kind != RTW_SCENE_KERR_POWEHI))
+        (scene->kind != RTW_SCENE_KERR_SYNCHRO_TORUS && scene->kind != RTW_SCENE_KERR_POWEHI &&
+         scene->kind != RTW_SCENE_SYNCHRO_TEST))
         return RTW_ERR_INVALID_PARAM;
     TorusModel m;
     std::string why;

@@ -300,6 +300,52 @@ RTW_HD TorusPt<T> powehi_point(const PowehiDev& P, const T* z) {
     return o;
 }
 
+// ---------------------------------------------------------------------------
+// Synchro_Test.source, the reference's flat-space synchrotron test: Cartesian
+// Minkowski space, a static cylinder around the z axis in a uniform field
+// B^z radiating the power-law synchrotron of the Powehi jet
+// (source_model.jl:18-244). Its emitter numbers use the Powehi zone-2 record,
+// so powehi_bin gives its slopes.
+// ---------------------------------------------------------------------------
+struct SynchroDev {
+    double b_z;          // global field B^z, gauss
+    double r_cyl;        // cylinder radius (map units)
+    double j_scale, a_scale, p_index, inv_p_synch;  // as PowehiDev
+};
+
+// Emitter numbers at a stage point z = (t, x, y, z, k^t, k^x, k^y, k^z)
+// (is_fire :229-236, get_source_velocity! :250-256, calc_freq_shift,
+// calc_fluid_params! :152-172, transform_B_b :60-108, calc_b_angle :114-146).
+// With u = (1, 0, 0, 0) and g = diag(-1, 1, 1, 1): the frequency shift is
+// k^t, the fluid-frame field b = (0, 0, 0, B^z) with the reference's
+// magnitude sum_mu (sum_i g_{i mu}) b_mu^2 = B^z^2, and cos^2 of the
+// field-ray angle (k^z / k^t)^2.
+template <class T>
+RTW_HD TorusPt<T> synchro_point(const SynchroDev& Y, const T* z) {
+    typedef decltype(val(z[1])) B;
+    TorusPt<T> o;
+    o.on = false;
+    o.zone = 0;
+    o.cj = T(0.0); o.nus = T(0.0); o.th = T(1.0); o.g = T(1.0);
+    const double xv = (double)val(z[1]), yv = (double)val(z[2]);
+    if (!(sqrt(xv * xv + yv * yv) <= Y.r_cyl)) return o;
+    const T g = z[4];
+    o.g = g;
+    const T c2 = z[7] * z[7] / (g * g);
+    const T s2b = T(B(1.0)) - c2;
+    // a ray along the field: the reference's j is 0 * inf there
+    if (!((double)val(s2b) > 0)) return o;
+    const T sinb = tsqrt(s2b);
+    const B bmag = B(fabs(Y.b_z));
+    const T phi = texp(tlog(T(B(1.0)) - B(0.99) * c2) * B(-0.5 * Y.p_index)) * B(Y.inv_p_synch);
+    o.cj = sinb * phi * B(Y.j_scale * fabs(Y.b_z));   // J0
+    o.nus = phi * B(Y.a_scale);                        // A0
+    o.th = T(B(1.0)) / (sinb * B(9.34e-11) * bmag);    // 1 / (nu_c sin theta_B)
+    o.zone = 2;
+    o.on = true;
+    return o;
+}
+
 // Slopes of one bin without exp(-tau) (as torus_bin): nu = g nu_c in nm^-1.
 // Disk: a = a_nu, j = a B_nu(T); jet: j = J0 s^-(p-1)/2, a = A0 / nu s^-(p+2)/2,
 // s = nu / (nu_cyc sin theta_B) (calc_radiative_coefficients).

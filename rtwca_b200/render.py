@@ -229,6 +229,8 @@ _WORLDS = {
                                  [0.0, 0.0, -PI / 2], 0.0),
     # initialization.jl:100-109 (Powehi.source, the M87* model)
     "m87": (abi.SCENE_KERR_POWEHI, [0, 35, 0.3, 0], [PI / 2, PI / 6], [0.0, 0.0, PI], 0.0),
+    # initialization.jl:120-128 (Synchro_Test.source, Cartesian t, x, y, z)
+    "synch": (abi.SCENE_SYNCHRO_TEST, [0.0, 0.0, 0.0, 0.0], [0.0, 0.0], [PI / 8, 0.0, PI], 0.0),
 }
 
 _current: World | None = None
@@ -242,8 +244,8 @@ def available_worlds() -> list:
 def initialize_world(input_string: str):
     """Selects a scene and returns its default (position, direction, pointing, beta)
     (initialization.jl:78-172). Scenes that need the reference's missing textures
-    (wormhole, Cartesian sphere) and the flat-space synchrotron test are not on
-    this library's path and raise ValueError."""
+    (wormhole, Cartesian sphere) are not on this library's path and raise
+    ValueError."""
     global _current
     key = input_string.lower()
     if key not in _WORLDS:

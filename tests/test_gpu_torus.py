@@ -202,3 +202,37 @@ def test_powehi_parity(renderer, oracle, integrator, precision):
     else:
         bar = 0.98 if integrator == abi.DP45_FSAL else 0.95
         assert s["class_match"] >= 0.99 and s["frac_within_1e-3"] >= bar, s
+
+
+@pytest.mark.parametrize("integrator", [abi.DP45_REF_COMPAT, abi.DP45_FSAL])
+@pytest.mark.parametrize("precision", [abi.PREC_FP64, abi.PREC_MIXED])
+def test_synchro_parity(renderer, oracle, integrator, precision):
+    """Synchro_Test (the reference's "synch" world: flat Cartesian space, the
+    camera inside a synchrotron cylinder) through the per-bin kernel's flat
+    geometry, against the oracle; same bars as Powehi."""
+    from tests.parity import summarize
+    sc = configs.synchro_scene()
+    cam = configs.synchro_camera(32, 1e-6)
+    col = np.array([400.0, 475.0, 550.0, 625.0, 700.0])
+    ref = oracle.render(sc, cam, col, integrator=integrator)
+    g = renderer.render(sc, [cam], col, want=("xyz", "class", "steps", "spectrum"), precision=precision,
+                        integrator=integrator)
+    s = summarize(g, ref)
+    print("synch", integrator, precision, s)
+    assert np.all(ref["xyz"][:, 1] > 0)  # every ray leaves through the emitting cylinder
+    if precision == abi.PREC_FP64:
+        assert s["class_match"] >= 0.999 and s["frac_within_1e-3"] >= 0.999, s
+    else:
+        bar = 0.98 if integrator == abi.DP45_FSAL else 0.95
+        assert s["class_match"] >= 0.99 and s["frac_within_1e-3"] >= bar, s
+
+
+def test_synch_world_through_gen_image():
+    """initialize_world("synch") + gen_image: the reference's world defaults,
+    Cartesian camera at the origin (no coordinate singularity there)."""
+    from rtwca_b200 import render as R
+    pos, d, pt, beta = R.initialize_world("synch")
+    assert list(pos) == [0.0, 0.0, 0.0, 0.0]
+    img = R.gen_image(camera_pos=pos, camera_dir=d, speed=beta, camera_point=pt, x_pix=16, tolerance=1e-6,
+                      max_steps=1e4, colors=(400, 550, 700), precision="mixed", integrator="fsal")
+    assert img.shape[1] == 16 and np.all(np.isfinite(img)) and np.all(img[:, :, 1] > 0)

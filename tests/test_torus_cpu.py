@@ -169,3 +169,43 @@ def _step(sc, col, y, h):
         Y = y + h * sum(A[s][j] * K[j] for j in range(s)) if s else y
         K.append(abi.torus_rhs(sc, col, Y, 0))
     return y + h * sum(A[6][j] * K[j] for j in range(6))
+
+
+def test_synchro_scene_defaults():
+    s = configs.synchro_scene()
+    assert s.kind == abi.SCENE_SYNCHRO_TEST
+    assert (s.r_out, s.n_e0, s.b_0, s.escape_radius) == (1.0, 1e7, 10.0, 100.0)
+    assert s.length_cm == pytest.approx(9.62e14)
+
+
+def _cart_state(N, x, y, z, rng):
+    """A null ray at Cartesian (x, y, z) with a random direction, random tau and I."""
+    d = rng.normal(size=3)
+    d /= np.linalg.norm(d)
+    st = np.zeros(8 + 2 * N)
+    st[:8] = [0.0, x, y, z, 1.0, d[0], d[1], d[2]]
+    st[9::2] = rng.uniform(0, 2, N)
+    st[8::2] = rng.uniform(0, 1e-3, N)
+    return st
+
+
+def test_synchro_rhs_matches_oracle(oracle):
+    """Synchro_Test (flat Cartesian space, the synchrotron cylinder): the
+    library's per-bin right-hand side against the oracle's restatement of
+    Synchro_Test.source/source_model.jl, inside and outside the cylinder."""
+    sc = configs.synchro_scene()
+    col = np.array([380.0, 450.0, 550.0, 650.0, 750.0])
+    rng = np.random.default_rng(2)
+    inside = 0
+    for x, y, z in [(0.0, 0.0, 0.0), (0.5, -0.3, 4.0), (0.9, 0.1, -20.0), (-0.2, 0.7, 1.0), (1.5, 0.0, 0.0),
+                    (30.0, -40.0, 2.0)]:
+        for _ in range(3):
+            st = _cart_state(col.size, x, y, z, rng)
+            ref = oracle.rhs(sc, col, st)
+            f = abi.torus_rhs(sc, col, st, 0)
+            assert np.array_equal(f[:4], st[4:8]) and np.all(f[4:8] == 0)  # straight lines
+            scale = 1e-300 + 1e-12 * np.abs(ref[8:]).max()
+            err = np.abs(f[8:] - ref[8:]) / np.maximum(np.abs(ref[8:]), scale)
+            assert err.max() < 1e-11, (x, y, z, err.max())
+            inside += bool(np.any(ref[8:] != 0))
+    assert inside == 12  # the four points inside the cylinder emit, the two outside do not
