@@ -45,6 +45,7 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=2048, help="rays in the CPU baseline sample")
     ap.add_argument("--no-batched", action="store_true", help="skip the 96-frame batched leg")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the synchrotron-torus adjoint leg")
+    ap.add_argument("--no-scenes", action="store_true", help="skip the Powehi / Synchro_Test scene leg")
     ap.add_argument("--no-plain-leg", action="store_true", help="skip the plain FP64 GPU path leg")
     ap.add_argument("--adjoint-x-pix", type=int, default=512)
     ap.add_argument("--block-warps", type=int, default=0)
@@ -317,6 +318,49 @@ def batched_leg(r, world, rank, stream, barrier_fn):
     }
 
 
+def scenes_leg(r, rank, cpu=True):
+    """The reference's two per-bin power-law synchrotron scenes through the
+    per-bin kernels, each at 1024 px wide with the reference's default field
+    of view and colours (400/550/700 nm), tolerance 1e-6: Powehi ("m87": Kerr
+    a = 0.9, disk + jet) and Synchro_Test ("synch": flat Cartesian space,
+    camera inside the cylinder). FP32-mixed and FP64, the reference's step.
+    Device time of the kernel (1 warm-up + 3 timed renders, mean); on rank 0
+    the FP64 oracle on 4096 evenly spaced pixels on all host cores gives the
+    CPU rate and a parity sample (linear Y within 1e-3)."""
+    from rtwca_b200 import abi, configs
+
+    def rel_err(g, ref):
+        den = np.maximum(np.abs(ref), 1e-6 * np.abs(ref).max() + 1e-300)
+        return np.abs(np.asarray(g, np.float64) - ref) / den
+
+    col = np.array([400.0, 550.0, 700.0])
+    out = {}
+    for name, sc, camf in (("m87_powehi", configs.powehi_scene(), configs.powehi_camera),
+                           ("synch_synchro_test", configs.synchro_scene(), configs.synchro_camera)):
+        cam = camf(1024, 1e-6)
+        P = cam.x_pix * cam.y_pix
+        leg = {"workload": f"{name} {cam.x_pix}x{cam.y_pix}, 3 bins 400/550/700 nm, tol 1e-6, reference step"}
+        for pname, prec in (("mixed", abi.PREC_MIXED), ("fp64", abi.PREC_FP64)):
+            r.render(sc, [cam], col, want=("xyz",), precision=prec, integrator=abi.DP45_REF_COMPAT)
+            ms = []
+            for _ in range(3):
+                g = r.render(sc, [cam], col, want=("xyz",), precision=prec, integrator=abi.DP45_REF_COMPAT)
+                ms.append(r.stats()["kernel_ms"])
+            t = float(np.mean(ms))
+            leg[pname] = {"Mrays_s": P / t / 1e3, "ms": t, "step_attempts": r.stats()["step_attempts"]}
+            if pname == "mixed":
+                gx = g["xyz"]
+        if cpu and rank == 0:
+            v, n, dt, cores, ref = cpu_time(sc, cam, col, 4096, keep=True)
+            ids = cpu_sample_ids(P, 4096)
+            e = rel_err(gx[ids, 1], ref["xyz"][:, 1])
+            leg["cpu_oracle"] = {"Mrays_s": v, "pixels": n, "s": dt, "cores": cores}
+            leg["mixed_over_cpu"] = leg["mixed"]["Mrays_s"] / v
+            leg["parity_sample_within_1e-3"] = float(np.mean(e <= 1e-3))
+        out[name] = leg
+    return out
+
+
 def adjoint_leg(r, x_pix, world=1, rank=0):
     """Differentiable synchrotron torus: Kerr a = 0.94, inclination 17 deg,
     x_pix^2 rays, 32 bins over 230 GHz +- 20 %, FP32-mixed, tolerance 1e-6.
@@ -471,6 +515,9 @@ def run_b200(args):
     if not args.no_adjoint:
         barrier(world)
         adjoint = adjoint_leg(r, args.adjoint_x_pix, world, rank)
+    scenes = None
+    if not args.no_scenes:
+        scenes = scenes_leg(r, rank, cpu=not args.no_cpu_baseline)
 
     # end to end through the public API: host pinned outputs, synchronous call
     hx = torch.empty((P, 3), dtype=torch.float32, pin_memory=True)
@@ -543,6 +590,7 @@ def run_b200(args):
             "plain_fp64": plain,
             "batched": batched,
             "adjoint": adjoint,
+            "scenes": scenes,
             "integrator": "reference step (k1 = previous sum b_i k_i)",
             "roofline": {"bound": "fp32" if prec == abi.PREC_MIXED else "fp64", "achieved": achieved, "peak": peak,
                          "unit": "TFLOP/s", "frac": achieved / peak,
