@@ -82,17 +82,17 @@ struct TorusModel {
 };
 
 // The scene's emitter at a stage point z (x^mu, k^mu) and the slopes of bin c.
-// (GEO: -1 the model's geometry at run time, 0 Kerr, 1 flat: the kernels
-// instantiate one geometry each, so the other's emitters stay out of them)
-template <class R, int GEO = -1>
+// (EM: the emitter, -1 the model's at run time; the kernels instantiate one
+// emitter each, so the others' code stays out of their hot loops)
+template <class R, int EM = -1>
 RTW_HD TorusPt<R> em_point(const TorusModel& m, const R* z) {
-    if (GEO == 1 || (GEO == -1 && m.emitter == 2)) return synchro_point<R>(m.sy, z);
-    if (m.emitter == 1) return powehi_point<R>(m.pw, z);
+    if (EM == 2 || (EM == -1 && m.emitter == 2)) return synchro_point<R>(m.sy, z);
+    if (EM == 1 || (EM == -1 && m.emitter == 1)) return powehi_point<R>(m.pw, z);
     return torus_point<R>(m.tor, R(m.tor.a), R(m.tor.n0), R(m.tor.B0), R(m.tor.Th0), z[1], z[2], z[4], z[7]);
 }
-template <class R>
+template <class R, int EM = -1>
 RTW_HD void em_bin(const TorusModel& m, const TorusPt<R>& S, int c, R& ft, R& fi) {
-    if (m.emitter != 0) powehi_bin<R>(m.pw, S, m.bins[c].nu_nm, ft, fi);
+    if (EM > 0 || (EM == -1 && m.emitter != 0)) powehi_bin<R>(m.pw, S, m.bins[c].nu_nm, ft, fi);
     else torus_bin<R>(S.cj, S.nus, S.th, S.g, m.bins[c], ft, fi);
 }
 
@@ -294,8 +294,9 @@ struct TorusStages {
 
 // The seven geodesic stages of one attempt in arithmetic R from the FP64
 // state x and the carried slope k1.
-template <class R, class K, bool FLAT>
+template <class R, class K, int EM>
 __device__ void torus_geo_stages(const TorusModel& m, const double* x, const K* k1, double h, TorusStages<R>& o) {
+    constexpr bool FLAT = EM == 2;
     R Kg[7][8];
     for (int i = 0; i < 8; ++i) Kg[0][i] = R(k1[i]);
     const R hr = R(h);
@@ -322,7 +323,7 @@ __device__ void torus_geo_stages(const TorusModel& m, const double* x, const K* 
             KerrScene<false>::rhs<R>(m.geo, z, kk, em);
         }
         for (int i = 0; i < 8; ++i) Kg[s][i] = kk[i];
-        o.S[s] = em_point<R, FLAT ? 1 : 0>(m, z);
+        o.S[s] = em_point<R, EM>(m, z);
         if (s == 6)
             for (int i = 0; i < 8; ++i) o.ns[i] = (double)acc[i];
     }
@@ -335,10 +336,10 @@ __device__ void torus_geo_stages(const TorusModel& m, const double* x, const K* 
 }
 
 // promoted (FP64-stage) geodesic part of the mixed path, out of line
-template <class K, bool FLAT>
+template <class K, int EM>
 __device__ __noinline__ void torus_geo_stages_fp64(const TorusModel& m, const double* x, const K* k1, double h,
                                                    TorusStages<double>* o) {
-    torus_geo_stages<double, K, FLAT>(m, x, k1, h, *o);
+    torus_geo_stages<double, K, EM>(m, x, k1, h, *o);
 }
 
 // pad_max_dt of the geometry: Kerr (source_model.jl:86-103) or
@@ -466,8 +467,9 @@ __device__ __noinline__ void torus_rec_end(const TorusKP& p, TorusRec* r, long l
 // Forward kernel. SR: arithmetic of the bins and of the stages (float on the
 // mixed path, with Kahan intensities and per-ray FP64 stages near the horizon
 // and the poles; double on the FP64 path).
-template <bool MIXED, bool FLAT>
+template <bool MIXED, int EM>
 __global__ void __launch_bounds__(128) torus_forward(const TorusKP p) {
+    constexpr bool FLAT = EM == 2;  // Synchro_Test: flat Cartesian geometry
     typedef typename SpecTraits<MIXED>::SR SR;
     const int N = p.m.n;
     const int D = 8 + 2 * N;
@@ -590,7 +592,7 @@ __global__ void __launch_bounds__(128) torus_forward(const TorusKP p) {
                 if (promote) {
                     ++c_pro;
                     TorusStages<double> sd;
-                    torus_geo_stages_fp64<SR, FLAT>(p.m, x, k1, h, &sd);
+                    torus_geo_stages_fp64<SR, EM>(p.m, x, k1, h, &sd);
                     for (int i = 0; i < 8; ++i) {
                         st.ns[i] = sd.ns[i];
                         st.es[i] = sd.es[i];
@@ -605,7 +607,7 @@ __global__ void __launch_bounds__(128) torus_forward(const TorusKP p) {
                         st.S[s].zone = sd.S[s].zone;
                     }
                 } else {
-                    torus_geo_stages<SR, SR, FLAT>(p.m, x, k1, h, st);
+                    torus_geo_stages<SR, SR, EM>(p.m, x, k1, h, st);
                 }
                 double y[8];
                 double err2 = 0;
@@ -633,7 +635,7 @@ __global__ void __launch_bounds__(128) torus_forward(const TorusKP p) {
                         for (int j = 0; j < s; ++j) a += SR(tA(s, j)) * kt[j];
                         tp = t0 + hs * a;
                         SR ft = 0, fi = 0;
-                        if (st.S[s].on) em_bin<SR>(p.m, st.S[s], c, ft, fi);
+                        if (st.S[s].on) em_bin<SR, EM>(p.m, st.S[s], c, ft, fi);
                         kt[s] = ft;
                         ki[s] = fi * texp(-tp);
                     }
@@ -1369,6 +1371,15 @@ rtw_status torus_model(const rtw_scene& s, const double* colors_nm, int N, Torus
     return RTW_OK;
 }
 
+// the forward kernel instance: precision x emitter (0 torus, 1 Powehi, 2
+// Synchro_Test, the last in flat geometry)
+const void* forward_fn(bool mixed, int emitter) {
+    static const void* const fn[2][3] = {
+        {(const void*)torus_forward<false, 0>, (const void*)torus_forward<false, 1>, (const void*)torus_forward<false, 2>},
+        {(const void*)torus_forward<true, 0>, (const void*)torus_forward<true, 1>, (const void*)torus_forward<true, 2>}};
+    return fn[mixed ? 1 : 0][emitter >= 0 && emitter <= 2 ? emitter : 0];
+}
+
 // launch shape of the torus kernels: 128 threads, occupancy-limited CTAs
 template <class F>
 int torus_grid(rtw_ctx* ctx, F fn) {
@@ -1426,17 +1437,13 @@ rtw_status torus_setup(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* c
     p.counter = ctl;
     p.stats = (DevStats*)(ctl + 1);
     p.err_flag = (unsigned int*)(ctl + 32);
-    run.grid = prm->precision == RTW_PREC_MIXED
-                   ? (p.m.flat ? torus_grid(ctx, torus_forward<true, true>) : torus_grid(ctx, torus_forward<true, false>))
-                   : (p.m.flat ? torus_grid(ctx, torus_forward<false, true>) : torus_grid(ctx, torus_forward<false, false>));
+    run.grid = torus_grid(ctx, forward_fn(prm->precision == RTW_PREC_MIXED, p.m.emitter));
     return RTW_OK;
 }
 
 cudaError_t launch_forward(const TorusKP& p, bool mixed, int grid, cudaStream_t st) {
     void* args[] = {(void*)&p};
-    const void* fn = p.m.flat ? (mixed ? (const void*)torus_forward<true, true> : (const void*)torus_forward<false, true>)
-                              : (mixed ? (const void*)torus_forward<true, false> : (const void*)torus_forward<false, false>);
-    return cudaLaunchKernel(fn, dim3(grid), dim3(128), args, 0, st);
+    return cudaLaunchKernel(forward_fn(mixed, p.m.emitter), dim3(grid), dim3(128), args, 0, st);
 }
 
 }  // namespace
