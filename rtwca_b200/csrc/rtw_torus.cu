@@ -22,6 +22,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <functional>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -280,6 +281,7 @@ struct TorusKP {
     unsigned long long split;
     int chunk_bytes;
     unsigned int region;
+    unsigned long long region_bytes;       // a ray's region in pool: an odd number of 128-byte lines
     const unsigned long long* chunk_base;  // [total_rays] (region 0)
     double* fin;                           // [P][D] final states
 };
@@ -384,9 +386,16 @@ struct TorusRec {
     uint8_t kb[kTorusMaxCk];
 };
 
+// Chunk i: in pool (i < split), ray i / region's region, segment i % region;
+// the regions are an odd number of 128-byte lines apart, so that the lanes'
+// concurrent chunks do not alias onto the same memory channels (a stride
+// that was a multiple of 4 KB cost the reverse sweep about 10 %).
 RTW_HD char* torus_chunk(const TorusKP& p, unsigned long long i) {
-    return i < p.split ? p.pool + i * (unsigned long long)p.chunk_bytes
-                       : p.pool2 + (i - p.split) * (unsigned long long)p.chunk_bytes;
+    if (i < p.split) {
+        const unsigned long long ray = i / p.region, seg = i - ray * p.region;
+        return p.pool + ray * p.region_bytes + seg * (unsigned long long)p.chunk_bytes;
+    }
+    return p.pool2 + (i - p.split) * (unsigned long long)p.chunk_bytes;
 }
 
 // write the first m buffered events of the current segment (streaming
@@ -763,6 +772,7 @@ struct TorusRP {
     unsigned long long* counter;
     const uint32_t* esc_index;   // [P] a ray's index among the densely re-recorded rays
     const unsigned long long* rbase;  // [P] a ray's first chunk
+    const uint32_t* order;       // [P] the rays by decreasing recorded steps (the queue's order)
 };
 
 // One recorded step of a ray, replayed in FP64: y_out = keep(step(y_in)).
@@ -1116,8 +1126,10 @@ __global__ void __launch_bounds__(128, 4) torus_reverse(const TorusRP p) {
     double lam[kTorusMaxD], mu[kTorusMaxD], tmp[kTorusMaxD];
     unsigned n_cut = 0;
     for (;;) {
-        const long long loc = (long long)atomicAdd(p.counter, 1ull);
-        if (loc >= p.f.total_rays) break;
+        const long long k = (long long)atomicAdd(p.counter, 1ull);
+        if (k >= p.f.total_rays) break;
+        // longest first: the last rays taken are short, so the grid's lanes end together
+        const long long loc = p.order ? (long long)p.order[k] : k;
         const long long id = p.f.ray0 + loc * p.f.ray_stride;
         double loss = 0;
         bool fin = true;
@@ -1577,14 +1589,15 @@ rtw_status rtw_adjoint(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* c
     // (dense re-record, overflowed rays) with their counts, offsets and chunk
     // bases, and every ray's first chunk
     const size_t q4 = ((size_t)Q * 4 + 255) & ~(size_t)255;
-    const size_t nev_b = 5 * q4 + 4 * (size_t)Q * 8;
+    const size_t nev_b = 6 * q4 + 4 * (size_t)Q * 8;
     if ((st = ensure(ctx, &b->nev, &b->nev_cap, nev_b)) != RTW_OK) return st;
     uint32_t* nev = (uint32_t*)b->nev;
     uint32_t* esc_index = (uint32_t*)((char*)b->nev + q4);
     uint32_t* ray_list = (uint32_t*)((char*)b->nev + 2 * q4);
     uint32_t* nev_d = (uint32_t*)((char*)b->nev + 3 * q4);
     uint32_t* list2 = (uint32_t*)((char*)b->nev + 4 * q4);
-    unsigned long long* ev_off = (unsigned long long*)((char*)b->nev + 5 * q4);  // [Q] events, then [Q] rows
+    uint32_t* order = (uint32_t*)((char*)b->nev + 5 * q4);
+    unsigned long long* ev_off = (unsigned long long*)((char*)b->nev + 6 * q4);  // [Q] events, then [Q] rows
     unsigned long long* base2 = ev_off + 2 * Q;
     unsigned long long* rbase = ev_off + 3 * Q;
     if ((st = ensure(ctx, &b->fin, &b->fin_cap, std::max<size_t>((size_t)Q * D * 8, 256))) != RTW_OK) return st;
@@ -1621,11 +1634,14 @@ rtw_status rtw_adjoint(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* c
         if (R0 < 4) return fail(ctx, RTW_ERR_OOM, "not enough device memory for the adjoint's records");
     }
     // (allocated before the timed region, like the other buffers)
-    if ((st = ensure(ctx, &b->pool, &b->pool_cap, (size_t)Q * R0 * cb)) != RTW_OK) return st;
+    unsigned long long region_bytes = (R0 * cb + 127) / 128 * 128;
+    if ((region_bytes / 128) % 2 == 0) region_bytes += 128;
+    if ((st = ensure(ctx, &b->pool, &b->pool_cap, (size_t)Q * region_bytes)) != RTW_OK) return st;
     p.record = 2;
     p.chunk_bytes = cb;
     p.pool = (char*)b->pool;
     p.split = (unsigned long long)Q * R0;
+    p.region_bytes = region_bytes;
     p.region = (unsigned int)R0;
     p.fin = (double*)b->fin;
     std::vector<uint32_t> h_nev(Q);
@@ -1673,6 +1689,19 @@ rtw_status rtw_adjoint(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* c
         p.pool2 = p2.pool2;
     }
     RTW_CUDA(cudaMemcpyAsync(rbase, h_rb.data(), 8 * Q, cudaMemcpyHostToDevice, s), "chunk bases H2D");
+    // the reverse sweep's queue: rays by decreasing recorded steps (rays left
+    // out of the gradient cost nothing and go last)
+    std::vector<uint32_t> h_order(Q);
+    {
+        std::vector<uint64_t> key(Q);
+        for (long long i = 0; i < Q; ++i) {
+            const bool skip = (h_nev[i] & kDenseCheckpoints) && adj->escape_rays == 1;
+            key[i] = ((uint64_t)(skip ? 0u : (h_nev[i] & kEventCount)) << 32) | (uint64_t)(0xffffffffu - (uint32_t)i);
+        }
+        std::sort(key.begin(), key.end(), std::greater<uint64_t>());
+        for (long long i = 0; i < Q; ++i) h_order[i] = 0xffffffffu - (uint32_t)(key[i] & 0xffffffffu);
+    }
+    RTW_CUDA(cudaMemcpyAsync(order, h_order.data(), 4 * Q, cudaMemcpyHostToDevice, s), "order H2D");
     // 2. rays with a polar escape whose gradient is wanted: a second recording
     // pass over them alone, with the full state before every event
     unsigned long long E = 0, C = 0;
@@ -1735,6 +1764,7 @@ rtw_status rtw_adjoint(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* c
     rp.f.spectrum = spec;
     rp.esc_index = esc_index;
     rp.rbase = rbase;
+    rp.order = order;
     rp.target = (const float*)b->tgt;
     rp.spectrum = spec;
     rp.per_ray = adj->per_ray_grad ? (double*)b->work : nullptr;
