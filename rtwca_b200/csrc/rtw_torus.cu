@@ -1754,6 +1754,15 @@ rtw_status rtw_adjoint(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* c
     int occ = 0;
     const void* rev_fn = mixed ? (const void*)torus_reverse<true> : (const void*)torus_reverse<false>;
     RTW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, rev_fn, 128, 0), "occupancy");
+    {
+        // reserve the sweep's per-thread local memory now (the driver would
+        // otherwise grow the reservation, GBs, at the launch)
+        cudaFuncAttributes fa;
+        size_t cur = 0;
+        RTW_CUDA(cudaFuncGetAttributes(&fa, rev_fn), "reverse attributes");
+        RTW_CUDA(cudaDeviceGetLimit(&cur, cudaLimitStackSize), "stack limit");
+        if (fa.localSizeBytes > cur) RTW_CUDA(cudaDeviceSetLimit(cudaLimitStackSize, fa.localSizeBytes), "stack limit");
+    }
     const int rgrid = ctx->num_sms * std::max(1, occ);
     // local-memory work area of the reverse kernel (per resident thread)
     const size_t work_b = (size_t)rgrid * 128 *
