@@ -982,7 +982,8 @@ template <class BT>
 RTW_HD double torus_dp_vjp(const TorusModel& m, const double* y, const double* Kg, double* tau, bool tau_at_end,
                            double h, double* lam, double* pb) {
     const int N = m.n;
-    typedef Dual<double, 8> D8;  // r, theta, k^t, k^phi, a, n0, b0, th0
+    // the emitter numbers and their tangents in the partials' precision BT
+    typedef Dual<BT, 8> D8;  // r, theta, k^t, k^phi, a, n0, b0, th0
     double Yg[6][8];
     for (int t = 0; t < 6; ++t)
         for (int i = 0; i < 8; ++i) {
@@ -990,13 +991,15 @@ RTW_HD double torus_dp_vjp(const TorusModel& m, const double* y, const double* K
             for (int s = 0; s < t; ++s) acc += tA(t, s) * Kg[s * 8 + i];
             Yg[t][i] = y[i] + h * acc;
         }
-    double dS[6][4][8], Sbar[6][4];
+    BT dS[6][4][8];
+    double Sbar[6][4];
     TorusBinPre pre[6];
     bool on[6];
     for (int t = 0; t < 6; ++t) {
-        const TorusPt<D8> S = torus_point<D8>(m.tor, D8::var(m.tor.a, 4), D8::var(m.tor.n0, 5), D8::var(m.tor.B0, 6),
-                                              D8::var(m.tor.Th0, 7), D8::var(Yg[t][1], 0), D8::var(Yg[t][2], 1),
-                                              D8::var(Yg[t][4], 2), D8::var(Yg[t][7], 3));
+        const TorusPt<D8> S = torus_point<D8>(m.tor, D8::var(BT(m.tor.a), 4), D8::var(BT(m.tor.n0), 5),
+                                              D8::var(BT(m.tor.B0), 6), D8::var(BT(m.tor.Th0), 7),
+                                              D8::var(BT(Yg[t][1]), 0), D8::var(BT(Yg[t][2]), 1),
+                                              D8::var(BT(Yg[t][4]), 2), D8::var(BT(Yg[t][7]), 3));
         on[t] = S.on;
         if (S.on) pre[t] = torus_bin_pre(S.cj.v, S.nus.v, S.th.v, S.g.v);
         const D8* comp[4] = {&S.cj, &S.nus, &S.th, &S.g};
@@ -1082,7 +1085,7 @@ RTW_HD double torus_dp_vjp(const TorusModel& m, const double* y, const double* K
         if (on[t]) {
             double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
             for (int q = 0; q < 4; ++q)
-                for (int u = 0; u < 8; ++u) v[u] += Sbar[t][q] * dS[t][q][u];
+                for (int u = 0; u < 8; ++u) v[u] += Sbar[t][q] * (double)dS[t][q][u];
             mu[1] += v[0];
             mu[2] += v[1];
             mu[4] += v[2];

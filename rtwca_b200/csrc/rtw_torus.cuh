@@ -79,20 +79,22 @@ RTW_HD T bessel_k2_inv(const T& theta) {
 // chain-rule step (dK_2(x)/dx = -int cosh t cosh 2t exp(-x cosh t) dt).
 template <class T, int K>
 RTW_HD Dual<T, K> bessel_k2_inv(const Dual<T, K>& theta) {
-    const double x = 1.0 / (double)theta.v;
-    double s = 0, ds = 0;
+    // (in the tangents' precision T: FP32 for the FP32-mixed adjoint's
+    // emitter tangents, FP64 otherwise)
+    const T x = T(1.0) / theta.v;
+    T s = T(0), ds = T(0);
     for (int i = 0; i < 33; ++i) {
 #ifdef __CUDA_ARCH__
         const double ch = c_k2_cosh[i], ch2 = c_k2_cosh2[i];
 #else
         const double ch = h_k2_cosh[i], ch2 = h_k2_cosh2[i];
 #endif
-        const double w = (i == 0 ? 0.125 : 0.25) * ch2 * exp(-x * ch);
+        const T w = T((i == 0 ? 0.125 : 0.25) * ch2) * texp(-x * T(ch));
         s += w;
-        ds -= w * ch;
+        ds -= w * T(ch);
     }
     // d/dtheta = dK/dx * (-1 / theta^2)
-    return chain(theta, T(s), T(ds * (-x * x)));
+    return chain(theta, s, ds * (-x * x));
 }
 
 // Emitter numbers at (r, theta) for a ray with k^t, k^phi (the Keplerian
