@@ -1640,6 +1640,16 @@ rtw_status rtw_adjoint(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* c
     unsigned long long region_bytes = (R0 * cb + 127) / 128 * 128;
     if ((region_bytes / 128) % 2 == 0) region_bytes += 128;
     if ((st = ensure(ctx, &b->pool, &b->pool_cap, (size_t)Q * region_bytes)) != RTW_OK) return st;
+    {
+        // and the reverse sweep's per-thread local memory (the driver would
+        // otherwise grow its reservation, GBs, at the sweep's first launch)
+        const void* rfn = mixed ? (const void*)torus_reverse<true> : (const void*)torus_reverse<false>;
+        cudaFuncAttributes fa;
+        size_t cur = 0;
+        RTW_CUDA(cudaFuncGetAttributes(&fa, rfn), "reverse attributes");
+        RTW_CUDA(cudaDeviceGetLimit(&cur, cudaLimitStackSize), "stack limit");
+        if (fa.localSizeBytes > cur) RTW_CUDA(cudaDeviceSetLimit(cudaLimitStackSize, fa.localSizeBytes), "stack limit");
+    }
     p.record = 2;
     p.chunk_bytes = cb;
     p.pool = (char*)b->pool;
@@ -1757,15 +1767,6 @@ rtw_status rtw_adjoint(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* c
     int occ = 0;
     const void* rev_fn = mixed ? (const void*)torus_reverse<true> : (const void*)torus_reverse<false>;
     RTW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, rev_fn, 128, 0), "occupancy");
-    {
-        // reserve the sweep's per-thread local memory now (the driver would
-        // otherwise grow the reservation, GBs, at the launch)
-        cudaFuncAttributes fa;
-        size_t cur = 0;
-        RTW_CUDA(cudaFuncGetAttributes(&fa, rev_fn), "reverse attributes");
-        RTW_CUDA(cudaDeviceGetLimit(&cur, cudaLimitStackSize), "stack limit");
-        if (fa.localSizeBytes > cur) RTW_CUDA(cudaDeviceSetLimit(cudaLimitStackSize, fa.localSizeBytes), "stack limit");
-    }
     const int rgrid = ctx->num_sms * std::max(1, occ);
     // local-memory work area of the reverse kernel (per resident thread)
     const size_t work_b = (size_t)rgrid * 128 *
