@@ -49,3 +49,50 @@ def test_gpu_matches_golden(renderer, name, integ, tag, prec):
     assert s["frac_within_1e-3"] >= 0.99, s
     if prec == abi.PREC_FP64:
         assert s["max_rel"] < 1e-5, s
+
+
+# ---- the per-bin scenes (Powehi, Synchro_Test, the synchrotron torus) ----
+from tests.golden.make_golden import PERBIN, perbin_case  # noqa: E402
+
+PERBIN_CASES = [(n, t) for n, tags in sorted(PERBIN.items()) for t in tags]
+
+
+@pytest.mark.parametrize("name,tag", PERBIN_CASES)
+def test_oracle_reproduces_perbin_golden(oracle, name, tag):
+    g = load(name, tag)
+    scene, cam, colors = perbin_case(name)
+    integ = abi.DP45_REF_COMPAT if tag == "ref" else abi.DP45_FSAL
+    assert np.array_equal(colors, g["colors"])
+    r = oracle.render(scene, cam, colors, integrator=integ)
+    assert np.array_equal(r["class"], g["class"])
+    assert np.array_equal(r["steps"], g["steps"])
+    assert np.allclose(r["spectrum"], g["spectrum"], rtol=1e-12, atol=0)
+    assert np.allclose(r["state"], g["state"], rtol=1e-12, atol=1e-300)
+
+
+# (the torus fixture is at tolerance 1e-8, below what FP32 stages resolve; the
+# FP32-mixed torus is checked at 1e-6 in test_gpu_torus)
+PERBIN_GPU = [(n, t, p) for n, t in PERBIN_CASES for p in (abi.PREC_FP64, abi.PREC_MIXED)
+              if not (n == "synchrotron_torus" and p == abi.PREC_MIXED)]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,tag,prec", PERBIN_GPU)
+def test_gpu_matches_perbin_golden(renderer, name, tag, prec):
+    """The per-bin kernels against the committed oracle fixtures, on the
+    spectrum (the synchrotron torus's 1.3 mm bins have no XYZ): FP64 within
+    1e-3 on >= 98 % of pixel-bins (the 8 x 8 torus has a ray that grazes the
+    spin axis and takes the polar escape, where rounding differences grow to
+    ~2e-3); FP32-mixed on >= 95 % (the reference step on Powehi's thin jet
+    takes FP32-sensitive step sequences)."""
+    g = load(name, tag)
+    scene, cam, colors = perbin_case(name)
+    integ = abi.DP45_REF_COMPAT if tag == "ref" else abi.DP45_FSAL
+    out = renderer.render(scene, [cam], colors, want=("class", "spectrum"), precision=prec, integrator=integ)
+    same = out["class"] == g["class"]
+    ref = g["spectrum"].astype(np.float64)
+    den = np.maximum(np.abs(ref), 1e-6 * np.abs(ref).max() + 1e-300)
+    err = (np.abs(out["spectrum"].astype(np.float64) - ref) / den)[same]
+    bar = 0.98 if prec == abi.PREC_FP64 else 0.95
+    assert np.mean(same) >= 0.97, (name, tag, np.mean(same))
+    assert np.mean(err <= 1e-3) >= bar, (name, tag, np.mean(err <= 1e-3), np.quantile(err, 0.99))
