@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define RTW_ABI_VERSION 3
+#define RTW_ABI_VERSION 4
 /* Largest number of spectral bins (reference `colors`) one render takes. */
 #define RTW_MAX_BINS 128
 /* Largest number of frames (cameras) one batched render takes. */
@@ -181,6 +181,12 @@ typedef struct rtw_camera {
     double fov_vert;        /* degrees */
     double tolerance;       /* abs_tol = rel_tol for every state component */
     int64_t max_steps;      /* step-attempt cap per ray */
+    /* window: render only pixels [win_x0, win_x0 + win_w) x [win_y0, win_y0 +
+       win_h) of the x_pix x y_pix image (win_w = win_h = 0: the whole image).
+       The window's rays are those of the whole image; its outputs are its own
+       pixels, row-major. Used to split one frame over GPUs in interleaved
+       tiles. No counterpart in the reference (one image per call). */
+    int32_t win_x0, win_y0, win_w, win_h;
 } rtw_camera;
 
 typedef struct rtw_render_params {

@@ -15,7 +15,7 @@ PKG = Path(__file__).resolve().parent
 # RTW_LIB_PATH selects another build of the same library (e.g. a tuning variant)
 LIB_PATH = Path(os.environ.get("RTW_LIB_PATH", PKG / "librtw_b200.so"))
 
-ABI_VERSION = 3
+ABI_VERSION = 4
 MAX_BINS = 128
 MAX_FRAMES = 4096
 TRACE_FIELDS = 15
@@ -87,6 +87,7 @@ class Camera(C.Structure):
         ("pointing", C.c_double * 3), ("x_pix", C.c_int32), ("y_pix", C.c_int32),
         ("fov_hor", C.c_double), ("fov_vert", C.c_double),
         ("tolerance", C.c_double), ("max_steps", C.c_int64),
+        ("win_x0", C.c_int32), ("win_y0", C.c_int32), ("win_w", C.c_int32), ("win_h", C.c_int32),
     ]
 
 
@@ -235,6 +236,22 @@ def scene_default(kind: int) -> Scene:
     s = Scene()
     check(load().rtw_scene_default(kind, C.byref(s)), "scene_default")
     return s
+
+
+def camera_pixels(c: "Camera") -> int:
+    """Pixels a camera renders: its window (win_w x win_h) or the whole image
+    (sets c.y_pix)."""
+    c.y_pix = y_pixels(c.x_pix, c.fov_hor, c.fov_vert)
+    if c.win_w or c.win_h:
+        return int(c.win_w) * int(c.win_h)
+    return c.x_pix * c.y_pix
+
+
+def window(c: "Camera", x0: int, y0: int, w: int, h: int) -> "Camera":
+    """A copy of camera c that renders pixels [x0, x0 + w) x [y0, y0 + h) of its image."""
+    d = Camera.from_buffer_copy(c)
+    d.win_x0, d.win_y0, d.win_w, d.win_h = int(x0), int(y0), int(w), int(h)
+    return d
 
 
 def make_camera(position, direction=(0.0, 0.0), speed=0.0, pointing=(0.0, 0.0, 0.0), x_pix=100,

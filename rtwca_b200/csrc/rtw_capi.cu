@@ -351,10 +351,21 @@ static rtw_status build_frame(const rtw_scene& s, rtw_camera& cam, FrameDesc& f)
     const double fh = kPi * cam.fov_hor / 180, fv = kPi * cam.fov_vert / 180;
     f.W = std::tan(fh / 2);
     f.H = std::tan(fv / 2);
-    f.xp = cam.x_pix;
-    f.yp = cam.y_pix;
-    f.rh = 2 * f.W / (f.xp + 1);
-    f.rv = 2 * f.H / (f.yp + 1);
+    f.rh = 2 * f.W / (cam.x_pix + 1);
+    f.rv = 2 * f.H / (cam.y_pix + 1);
+    if (cam.win_w == 0 && cam.win_h == 0 && cam.win_x0 == 0 && cam.win_y0 == 0) {
+        f.xp = cam.x_pix;
+        f.yp = cam.y_pix;
+        f.i0 = f.j0 = 0;
+    } else {
+        if (cam.win_x0 < 0 || cam.win_y0 < 0 || cam.win_w < 1 || cam.win_h < 1 ||
+            (int64_t)cam.win_x0 + cam.win_w > cam.x_pix || (int64_t)cam.win_y0 + cam.win_h > cam.y_pix)
+            return RTW_ERR_INVALID_PARAM;
+        f.xp = cam.win_w;
+        f.yp = cam.win_h;
+        f.i0 = cam.win_x0;
+        f.j0 = cam.win_y0;
+    }
     M4 R, L, R2, e, t1, t2, M;
     rot_intrinsic(cam.pointing, R);
     boost(-cam.speed, L);
@@ -404,8 +415,8 @@ rtw_status rtw_camera_rays(const rtw_scene* scene, const rtw_camera* camin, doub
     for (int j = 0; j < f.yp; ++j)
         for (int i = 0; i < f.xp; ++i) {
             double* S = rays + 8 * ((int64_t)i + (int64_t)f.xp * j);
-            const double w = f.rh * ((i + 1) - 0.5) - f.W;
-            const double hh = f.rv * ((j + 1) - 0.5) - f.H;
+            const double w = f.rh * ((f.i0 + i + 1) - 0.5) - f.W;
+            const double hh = f.rv * ((f.j0 + j + 1) - 0.5) - f.H;
             const double th = std::atan(std::sqrt(w * w + hh * hh));
             double ph;
             if (w > 0) ph = std::atan(hh / w);

@@ -21,7 +21,8 @@ struct FrameDesc {
     double thick;        // -log(tol): optically thick threshold
     long long ray_begin; // first global ray id of this frame
     long long max_steps;
-    int xp, yp;
+    int xp, yp;          // the frame's (window's) pixels
+    int i0, j0;          // the window's origin in the whole image
 };
 
 // Scene constants in the form the device functors use.

@@ -299,8 +299,10 @@ __device__ __noinline__ void rhs_fp64(const DevScene& s, const double* x9, doubl
 
 // Camera ray of pixel (i, j) of a frame (initialization.jl:213-240,327), FP64.
 __device__ __forceinline__ void camera_ray(const FrameDesc& f, int i, int j, double* x) {
-    const double w = f.rh * ((i + 1) - 0.5) - f.W;
-    const double hh = f.rv * ((j + 1) - 0.5) - f.H;
+    // (i, j): the pixel in the frame's window; the direction is that of pixel
+    // (i0 + i, j0 + j) of the whole image
+    const double w = f.rh * ((f.i0 + i + 1) - 0.5) - f.W;
+    const double hh = f.rv * ((f.j0 + j + 1) - 0.5) - f.H;
     const double th = atan(sqrt(w * w + hh * hh));
     double ph;
     if (w > 0) ph = atan(hh / w);

@@ -93,12 +93,12 @@ class Renderer:
 
     def render(self, scene: abi.Scene, cams, colors_nm, *, want=("xyz", "class", "steps"), **kw) -> dict:
         """Renders frames into new host numpy arrays; returns a dict of arrays
-        indexed by global pixel (frames concatenated, pixel i + x_pix * j)."""
+        indexed by global pixel (frames concatenated, pixel i + x_pix * j; a
+        windowed camera contributes its window's pixels, i + win_w * j)."""
         cams = list(cams)
         total = 0
         for c in cams:
-            c.y_pix = abi.y_pixels(c.x_pix, c.fov_hor, c.fov_vert)
-            total += c.x_pix * c.y_pix
+            total += abi.camera_pixels(c)
         n = len(np.atleast_1d(colors_nm))
         res = {}
         out = abi.Outputs()
@@ -144,8 +144,7 @@ class Renderer:
         in (spin, inclination, n_e0, b_0, theta_e0) through rtw_adjoint.
         target: [P, n_colors] float32 (host array or a CUDA tensor).
         rays = (begin, count, stride): the pixel subset (count 0: to the end)."""
-        cam.y_pix = abi.y_pixels(cam.x_pix, cam.fov_hor, cam.fov_vert)
-        P = cam.x_pix * cam.y_pix
+        P = abi.camera_pixels(cam)
         n = len(np.atleast_1d(colors_nm))
         ap = abi.AdjointParams()
         on_dev = hasattr(target, "data_ptr")

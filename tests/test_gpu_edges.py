@@ -84,3 +84,32 @@ def test_rejected_inputs(renderer):
     bundles = renderer.params(colors, ray_bundles=True)
     assert _call(renderer, scene, [cam], bundles) == abi.ERR_UNSUPPORTED            # not built
     assert renderer.last_error() != ""
+
+
+def test_frame_in_tiles_equals_whole_frame(renderer):
+    """One frame rendered as interleaved 16 x 16 tiles (windowed cameras, the
+    multi-GPU split of a frame; here both halves on this GPU) reassembles to
+    the whole-frame render exactly: each ray's arithmetic does not depend on
+    its batch."""
+    from rtwca_b200 import shard
+    scene, cam, colors = configs.workload("kerr_thin_disk", x_pix=72)
+    whole = renderer.render(scene, [cam], colors, want=("xyz", "class", "steps"), precision=abi.PREC_MIXED)
+    wins = shard.tile_windows(cam.x_pix, cam.y_pix, 16)
+    tiles = {}
+    for rank in range(2):  # the two ranks' shares, rendered one after the other
+        mine = shard.tiles_of_rank(len(wins), 2, rank)
+        res = renderer.render(scene, [abi.window(cam, *wins[t]) for t in mine], colors,
+                              want=("xyz", "class", "steps"), precision=abi.PREC_MIXED)
+        off = 0
+        for t in mine:
+            n = wins[t][2] * wins[t][3]
+            tiles[t] = {k: res[k][off:off + n] for k in ("xyz", "class", "steps")}
+            off += n
+    got = shard.assemble_tiles(wins, tiles, cam.x_pix, cam.y_pix)
+    for k in ("xyz", "class", "steps"):
+        assert np.array_equal(got[k], whole[k]), k
+    one = shard.render_frame_tiles(renderer, scene, cam, colors, precision=abi.PREC_MIXED)
+    assert np.array_equal(one["xyz"], whole["xyz"])
+    bad = abi.window(cam, cam.x_pix - 4, 0, 8, 8)  # past the image's edge
+    with pytest.raises(abi.RTWError):
+        renderer.render(scene, [bad], colors, want=("class",), precision=abi.PREC_MIXED)
