@@ -303,7 +303,8 @@ int32_t rtw_abi_version(void);
 rtw_status rtw_scene_default(int32_t kind, rtw_scene* out);
 
 /* Sets cam->y_pix = round(x_pix tan(fov_vert/2) / tan(fov_hor/2)) with ties to
- * even (initialization.jl:197-200) and returns the pixel count in *n_pix. */
+ * even (initialization.jl:197-200) and returns the count of pixels the camera
+ * renders in *n_pix (the image's, or its window's). */
 rtw_status rtw_camera_pixels(rtw_camera* cam, int64_t* n_pix);
 
 /* Host FP64 initial data of one camera, the reference's initialize_camera

@@ -337,7 +337,10 @@ rtw_status rtw_camera_pixels(rtw_camera* cam, int64_t* n_pix) {
     const double yp = std::nearbyint(cam->x_pix * H / W);
     if (!(yp >= 1 && yp < 1e9)) return RTW_ERR_INVALID_PARAM;
     cam->y_pix = (int32_t)yp;
-    if (n_pix) *n_pix = (int64_t)cam->x_pix * cam->y_pix;
+    if (n_pix) {
+        const bool win = cam->win_w || cam->win_h || cam->win_x0 || cam->win_y0;
+        *n_pix = win ? (int64_t)cam->win_w * cam->win_h : (int64_t)cam->x_pix * cam->y_pix;
+    }
     return RTW_OK;
 }
 
