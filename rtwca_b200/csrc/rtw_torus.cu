@@ -980,9 +980,28 @@ RTW_HD double torus_dp_vjp_generic(const TorusModel& m, const double* y, const d
 // enter no slope, so the reverse sweep never needs them). BT: arithmetic of
 // the bins' partials (double, or float for the FP32-mixed adjoint); the
 // cotangents accumulate in FP64 either way.
+// mu += (d accel / d(r, theta, k))^T cw and pb[0] += (d accel / d a)^T cw at
+// the stage point Yt, the acceleration's Jacobian from 7-tangent duals in T
+template <class T>
+RTW_HD void torus_accel_vjp(const TorusModel& m, const double* Yt, const double* cw4, double* mu, double* pb) {
+    typedef Dual<T, 7> D7;  // r, theta, k^t, k^r, k^theta, k^phi, a
+    const D7 r = D7::var(T(Yt[1]), 0), th = D7::var(T(Yt[2]), 1), a = D7::var(T(m.tor.a), 6);
+    D7 k[4], acc[4];
+    for (int i = 0; i < 4; ++i) k[i] = D7::var(T(Yt[4 + i]), 2 + i);
+    kerr_accel<D7>(m.tor.M, a, r, th, k, acc);
+    for (int i = 0; i < 4; ++i) {
+        const double cw = cw4[i];
+        if (cw == 0) continue;
+        mu[1] += cw * (double)acc[i].d[0];
+        mu[2] += cw * (double)acc[i].d[1];
+        for (int q = 0; q < 4; ++q) mu[4 + q] += cw * (double)acc[i].d[2 + q];
+        pb[0] += cw * (double)acc[i].d[6];
+    }
+}
+
 template <class BT>
 RTW_HD double torus_dp_vjp(const TorusModel& m, const double* y, const double* Kg, double* tau, bool tau_at_end,
-                           double h, double* lam, double* pb) {
+                           double h, double* lam, double* pb, bool geo64 = true) {
     const int N = m.n;
     // the emitter numbers and their tangents in the partials' precision BT
     typedef Dual<BT, 8> D8;  // r, theta, k^t, k^phi, a, n0, b0, th0
@@ -1066,24 +1085,15 @@ RTW_HD double torus_dp_vjp(const TorusModel& m, const double* y, const double* K
         lg[i] = lam[i];
         for (int s = 0; s < 6; ++s) kg[s][i] = h * tA(6, s) * lam[i];
     }
-    typedef Dual<double, 7> D7;  // r, theta, k^t, k^r, k^theta, k^phi, a
     for (int t = 5; t >= 0; --t) {
         double mu[8] = {0, 0, 0, 0, 0, 0, 0, 0};
         for (int i = 0; i < 4; ++i) mu[4 + i] += kg[t][i];
-        {
-            const D7 r = D7::var(Yg[t][1], 0), th = D7::var(Yg[t][2], 1), a = D7::var(m.tor.a, 6);
-            D7 k[4], acc[4];
-            for (int i = 0; i < 4; ++i) k[i] = D7::var(Yg[t][4 + i], 2 + i);
-            kerr_accel<D7>(m.tor.M, a, r, th, k, acc);
-            for (int i = 0; i < 4; ++i) {
-                const double cw = kg[t][4 + i];
-                if (cw == 0) continue;
-                mu[1] += cw * acc[i].d[0];
-                mu[2] += cw * acc[i].d[1];
-                for (int q = 0; q < 4; ++q) mu[4 + q] += cw * acc[i].d[2 + q];
-                pb[0] += cw * acc[i].d[6];
-            }
-        }
+        // the geodesic Jacobian: FP32 where the FP32-mixed forward ran FP32
+        // stages (away from the horizon and the poles), FP64 elsewhere
+        if (sizeof(BT) == 4 && !geo64)
+            torus_accel_vjp<float>(m, Yg[t], kg[t] + 4, mu, pb);
+        else
+            torus_accel_vjp<double>(m, Yg[t], kg[t] + 4, mu, pb);
         if (on[t]) {
             double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
             for (int q = 0; q < 4; ++q)
@@ -1164,8 +1174,10 @@ __global__ void __launch_bounds__(128, 4) torus_reverse(const TorusRP p) {
                 lam[2] = -lam[2];
                 lam[6] = -lam[6];
             }
+            const bool geo64 = !MIXED || (g[1] - m.geo.r_ev < p.f.promote_dr) || (g[2] < p.f.promote_theta) ||
+                               (g[2] > kPi - p.f.promote_theta);
             const double hbar = torus_dp_vjp<typename std::conditional<MIXED, float, double>::type>(
-                m, g, Kg, taus, tau_at_end, hv, lam, pb);
+                m, g, Kg, taus, tau_at_end, hv, lam, pb, geo64);
             // a pending step-size term of the next step lands on this state
             if (pend != 0) torus_pad_vjp(g, p.f.max_dt_scale, pend, lam);
             pend = 0;
@@ -1935,7 +1947,7 @@ rtw_status rtw_torus_step_vjp(const rtw_scene* scene, const double* colors_nm, i
         std::vector<double> y1(D);
         torus_dp_stages(m, y.data(), h, K.data(), Y.data(), y1.data());
         for (int c = 0; c < N; ++c) taus[c] = form >= 2 ? y1[8 + c] : y[8 + c];
-        *hbar = form == 3 ? torus_dp_vjp<float>(m, y.data(), Kg, taus, true, h, lam.data(), pb)
+        *hbar = form == 3 ? torus_dp_vjp<float>(m, y.data(), Kg, taus, true, h, lam.data(), pb, false)
                           : torus_dp_vjp<double>(m, y.data(), Kg, taus, form == 2, h, lam.data(), pb);
     }
     for (int i = 0; i < 8; ++i) mu[i] = lam[i];
