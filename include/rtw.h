@@ -97,7 +97,14 @@ typedef enum rtw_scene_kind {
        fit) with n_e0 (m^-3) and map scale length_cm; rays end beyond
        |x| = escape_radius (source_geometry.jl:7-88, source_model.jl:7-278).
        Per-bin tau; both integrators. */
-    RTW_SCENE_SYNCHRO_TEST = 6
+    RTW_SCENE_SYNCHRO_TEST = 6,
+    /* Wormhole.source, the reference's Dneg wormhole: coordinates (t, l,
+       theta, phi), metric -dt^2 + dl^2 + r(l)^2 dOmega^2 with throat radius
+       r_in, half-length edge_in and lensing width edge_out (Interstellar's:
+       1, 0.005, 0.05); empty space; rays end beyond r(l) = escape_radius or
+       phi > winding_limit (source_geometry.jl:7-205, source_model.jl:54-147).
+       Both integrators. */
+    RTW_SCENE_WORMHOLE = 7
 } rtw_scene_kind;
 
 /* How a ray ended. The reference's calc_terminate (e.g. Kerr.source/

@@ -152,6 +152,25 @@ struct OScene {
     }
     // Synchro_Test.source: Minkowski space in Cartesian (t, x, y, z)
     bool is_cart() const { return kind == RTW_SCENE_SYNCHRO_TEST; }
+    // Wormhole.source: the Dneg wormhole in (t, l, theta, phi)
+    bool is_wh() const { return kind == RTW_SCENE_WORMHOLE; }
+    // source_geometry.jl:7-41: M = W / W_over_M, r(l), and dr/dl as the
+    // reference writes it (with its extra (x - 1) / (1 + x^2) term)
+    double wh_M() const {
+        const double c = kPi / (2 * std::sqrt(2.0));
+        return edge_out / (-std::log(1 / std::cos(c)) + c * std::tan(c));
+    }
+    double wh_r(double l) const {
+        if (!(std::fabs(l) > edge_in)) return r_in;
+        const double M = wh_M(), x = 2 * (std::fabs(l) - edge_in) / (kPi * M);
+        return r_in + M * (x * std::atan(x) - std::log(1 + x * x) / 2);
+    }
+    double wh_drdl(double l) const {
+        if (!(std::fabs(l) > edge_in)) return 0.0;
+        const double M = wh_M(), x = 2 * (std::fabs(l) - edge_in) / (kPi * M);
+        const double d = 2 * (std::atan(x) + (x - 1) / (1 + x * x)) / kPi;
+        return l < 0 ? -d : d;
+    }
 
     // --- geometry -----------------------------------------------------------
     // Kerr calc_metric_params, source_geometry.jl:55-60
@@ -168,6 +187,10 @@ struct OScene {
         const double r = x[1], th = x[2];
         if (is_cart()) {  // Synchro_Test source_geometry.jl:7-16
             g[0][0] = -1.0;
+        } else if (is_wh()) {  // Wormhole source_geometry.jl:44-51
+            g[0][0] = -1.0;
+            g[2][2] = sq(wh_r(r));
+            g[3][3] = sq(wh_r(r) * std::sin(th));
         } else if (is_kerr()) {
             double Sig, Del, A;
             kerr_params(r, th, Sig, Del, A);
@@ -196,6 +219,11 @@ struct OScene {
             for (int j = 0; j < 4; ++j) e[i][j] = (i == j) ? 1.0 : 0.0;
         if (is_cart()) return;  // Synchro_Test source_geometry.jl:44-50
         const double r = x[1], th = x[2];
+        if (is_wh()) {  // Wormhole source_geometry.jl:83-90
+            e[2][2] = 1.0 / wh_r(r);
+            e[3][3] = 1.0 / (wh_r(r) * std::sin(th) + kNoDivZero);
+            return;
+        }
         if (is_kerr()) {
             double Sig, Del, A;
             kerr_params(r, th, Sig, Del, A);
@@ -266,6 +294,19 @@ struct OScene {
         std::memset(G, 0, sizeof(double) * 64);
         if (is_cart()) return;  // Synchro_Test source_geometry.jl:53-66
         const double r = x[1], th = x[2];
+        if (is_wh()) {  // Wormhole source_geometry.jl:131-150
+            const double rl = wh_r(r), drdl = wh_drdl(r);
+            G[1][2][2] = -rl * drdl;
+            G[1][3][3] = -rl * drdl * sq(std::sin(th));
+            G[2][1][2] = drdl / rl;
+            G[2][2][1] = G[2][1][2];
+            G[2][3][3] = -std::sin(th) * std::cos(th);
+            G[3][1][3] = drdl / rl;
+            G[3][3][1] = G[3][1][3];
+            G[3][2][3] = std::cos(th) / std::sin(th);
+            G[3][3][2] = G[3][2][3];
+            return;
+        }
         if (is_kerr()) {
             if (refprec)
                 kerr_christoffel<float>((float)r, (float)th, (float)a, (float)rs, G);
@@ -301,6 +342,18 @@ struct OScene {
     // near_singularity: Kerr :249-269 (= Schwarzschild :134-154), Minkowski :114-132
     bool near_singularity(const double* x, double h, double tol, double* temp) const {
         if (is_cart()) {  // Synchro_Test source_geometry.jl:69-73
+            *temp = h;
+            return false;
+        }
+        if (is_wh()) {  // Wormhole source_geometry.jl:156-171: within 5 tol of a pole
+            const double th_w = x[2] + h * x[6];
+            if (std::fabs(th_w) <= 5 * tol) {
+                *temp = 2 * std::fabs(x[2]) / (std::fabs(x[6] * 37) + kNoDivZero);
+                return true;
+            } else if (std::fabs(th_w - kPi) <= 5 * tol) {
+                *temp = 2 * std::fabs((x[2] - kPi) / (std::fabs(x[6] * 37) + kNoDivZero));
+                return true;
+            }
             *temp = h;
             return false;
         }
@@ -357,6 +410,8 @@ struct OScene {
     // is_singularity: Kerr :307-315 and the other scenes
     bool is_singularity(const double* pos) const {
         if (is_cart()) return false;  // Synchro_Test source_geometry.jl:84-88
+        if (is_wh())  // Wormhole source_geometry.jl:197-205: the poles only
+            return std::fabs(pos[2]) <= (double)1e-32f || std::fabs(pos[2] - kPi) <= (double)1e-32f;
         if (std::fabs(pos[1]) <= (double)1e-32f) return true;
         if (std::fabs(pos[2]) <= (double)1e-32f || std::fabs(pos[2] - kPi) <= 1e-32) return true;
         return false;
@@ -432,6 +487,14 @@ struct OScene {
     // pad_max_dt: Kerr model :86-103, Schwarzschild :86-106, Minkowski :89-105
     double pad_max_dt(const double* x, double scale) const {
         if (is_cart()) return scale * (1 + std::fabs(x[1]) + std::fabs(x[2]));  // Synchro_Test model :241-244
+        if (is_wh()) {  // Wormhole model :88-110
+            double e = (x[2] < kPi / 8 || x[2] > 7 * kPi / 8) ? std::min(scale, (double)1e-1f) : scale;
+            if (std::fabs(x[1]) < 100 * edge_in) e = e / 10;
+            const double a = std::fabs(1.0 / (e / (std::fabs(x[5]) + kNoDivZero)) + kNoDivZero);
+            const double b = std::fabs(1.0 / (e * std::min(x[2], kPi - x[2]) / (std::fabs(x[6]) + kNoDivZero) + kNoDivZero));
+            const double c = std::fabs(1.0 / (e / (std::fabs(x[7]) + kNoDivZero) + kNoDivZero));
+            return std::max(std::min(1.0 / (a + b + c + kNoDivZero), 0.5), (double)1e-12f);
+        }
         double eps;
         // Kerr casts the scale to Float32 (Kerr model :92-96); the other scenes
         // keep it in Float64 except for the Float32 literal 1f-1.
@@ -460,6 +523,14 @@ struct OScene {
     // Returns the class of the first predicate that holds, or 0.
     int terminate(const double* ray, int L, double tol, long long max_steps, long long step_count) const {
         if ((double)step_count >= (double)max_steps) return RTW_CLASS_MAXSTEPS;
+        if (is_wh()) {  // Wormhole model :134-147
+            if (wh_r(ray[1]) > esc) return RTW_CLASS_ESCAPE;
+            if (ray[3] > wind) return RTW_CLASS_WINDING;
+            const double thick = -std::log(tol);
+            for (int i = 9; i < L; i += 2)
+                if (ray[i] < thick) return 0;
+            return RTW_CLASS_THICK;
+        }
         if (is_cart()) {  // Synchro_Test model :258-275
             if (std::sqrt(ray[1] * ray[1] + ray[2] * ray[2] + ray[3] * ray[3]) > esc) return RTW_CLASS_ESCAPE;
             const double thick = -std::log(tol);

@@ -46,6 +46,7 @@ SCENE_KERR_THICK_DISK = 3
 SCENE_KERR_SYNCHRO_TORUS = 4
 SCENE_KERR_POWEHI = 5
 SCENE_SYNCHRO_TEST = 6
+SCENE_WORMHOLE = 7
 ADJOINT_PARAMS = ("spin", "inclination", "n_e0", "b_0", "theta_e0")
 
 # rtw_term_class

@@ -217,6 +217,20 @@ def synchro_scene() -> abi.Scene:
     return abi.scene_default(abi.SCENE_SYNCHRO_TEST)
 
 
+def wormhole_scene() -> abi.Scene:
+    """Wormhole.source: Interstellar's Dneg wormhole (throat radius 1,
+    half-length 0.005, lensing width 0.05)."""
+    return abi.scene_default(abi.SCENE_WORMHOLE)
+
+
+def wormhole_camera(x_pix: int = 256, tol: float = 1e-6, max_steps: int = 20_000) -> abi.Camera:
+    """The reference's "wormhole" world (initialization.jl:140-148): position
+    (0, l = 5, pi/2, 0), direction (pi/2, 0), pointing (0, 0, -pi/2), beta 0;
+    default field of view."""
+    return abi.make_camera([0.0, 5.0, PI / 2, 0.0], [PI / 2, 0.0], 0.0, [0.0, 0.0, -PI / 2], x_pix, 85.0, 60.0, tol,
+                           max_steps)
+
+
 def synchro_camera(x_pix: int = 256, tol: float = 1e-6, max_steps: int = 20_000) -> abi.Camera:
     """The reference's "synch" world (initialization.jl:120-128): position
     (0, 0, 0, 0) (Cartesian t, x, y, z: inside the cylinder), direction

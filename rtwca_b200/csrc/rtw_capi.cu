@@ -128,11 +128,27 @@ double horizon_radius(const rtw_scene& s) {
     return 0.0;
 }
 
+// Wormhole.source r(l) (source_geometry.jl:7-31) for the camera's tetrad
+double wormhole_r_host(const rtw_scene& s, double l) {
+    const double c = kPi / (2 * std::sqrt(2.0));
+    const double w_over_m = -std::log(1 / std::cos(c)) + c * std::tan(c);
+    const double M = s.edge_out / w_over_m;
+    if (!(std::fabs(l) > s.edge_in)) return s.r_in;
+    const double x = 2 * (std::fabs(l) - s.edge_in) / (kPi * M);
+    return s.r_in + M * (x * std::atan(x) - std::log(1 + x * x) / 2);
+}
+
 // inverse tetrad at the camera (calc_inv_vierbein of each scene)
 void inv_tetrad(const rtw_scene& s, const double* x, M4 e) {
     for (int i = 0; i < 4; ++i)
         for (int j = 0; j < 4; ++j) e[i][j] = i == j ? 1.0 : 0.0;
     if (s.kind == RTW_SCENE_SYNCHRO_TEST) return;  // Cartesian Minkowski: the identity
+    if (s.kind == RTW_SCENE_WORMHOLE) {            // Wormhole.source/source_geometry.jl:83-90
+        const double rl = wormhole_r_host(s, x[1]);
+        e[2][2] = 1 / rl;
+        e[3][3] = 1 / (rl * std::sin(x[2]) + kNoDivZero);
+        return;
+    }
     const double r = x[1], th = x[2];
     if (is_kerr(s.kind)) {
         const double a = s.spin, rs = 2 * s.mass;
@@ -324,6 +340,11 @@ rtw_status rtw_scene_default(int32_t kind, rtw_scene* s) {
         s->r_out = 1; s->n_e0 = 1e7; s->b_0 = 10; s->length_cm = 9.62e14;
         s->escape_radius = 100;
         break;
+    case RTW_SCENE_WORMHOLE:
+        // Interstellar's Dneg wormhole (Wormhole.source/source_geometry.jl:7-15):
+        // rho = 1, a = 0.005 rho, W = 0.05 rho; escape at r(l) > 100, phi > 8 pi
+        s->r_in = 1; s->edge_in = 0.005; s->edge_out = 0.05; s->escape_radius = 100;
+        break;
     default:
         return RTW_ERR_INVALID_PARAM;
     }
@@ -349,7 +370,12 @@ static rtw_status build_frame(const rtw_scene& s, rtw_camera& cam, FrameDesc& f)
     if (st != RTW_OK) return st;
     // (the Cartesian scene has no coordinate singularity: Synchro_Test.source/
     // source_geometry.jl:84-88)
-    if (s.kind != RTW_SCENE_SYNCHRO_TEST && on_singularity(cam.position)) return RTW_ERR_INVALID_CAMERA;
+    if (s.kind == RTW_SCENE_WORMHOLE) {  // the poles only (Wormhole.source/source_geometry.jl:197-205)
+        if (std::fabs(cam.position[2]) <= (double)1e-32f || std::fabs(cam.position[2] - kPi) <= (double)1e-32f)
+            return RTW_ERR_INVALID_CAMERA;
+    } else if (s.kind != RTW_SCENE_SYNCHRO_TEST && on_singularity(cam.position)) {
+        return RTW_ERR_INVALID_CAMERA;
+    }
     if (!(std::fabs(cam.speed) < 1)) return RTW_ERR_INVALID_PARAM;
     const double fh = kPi * cam.fov_hor / 180, fv = kPi * cam.fov_vert / 180;
     f.W = std::tan(fh / 2);
@@ -520,7 +546,7 @@ rtw_status rtw_render(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* ca
         return fail(ctx, RTW_ERR_INVALID_PARAM, "n_colors must be 1..128 with colors_nm set");
     if (prm->ray_bundles) return fail(ctx, RTW_ERR_UNSUPPORTED, "ray bundles are not built");
     if (scene->kind == RTW_SCENE_KERR_SYNCHRO_TORUS || scene->kind == RTW_SCENE_KERR_POWEHI ||
-        scene->kind == RTW_SCENE_SYNCHRO_TEST)
+        scene->kind == RTW_SCENE_SYNCHRO_TEST || scene->kind == RTW_SCENE_WORMHOLE)
         return torus_render(ctx, scene, cams, n_cams, prm, out);
     if (scene->ref_precision) return fail(ctx, RTW_ERR_UNSUPPORTED, "ref_precision is an oracle-only switch");
     if (prm->precision != RTW_PREC_FP64 && prm->precision != RTW_PREC_MIXED && prm->precision != RTW_PREC_FP64_PLAIN)

@@ -135,6 +135,8 @@ RTW_HD float tcos(float x) { return cosf(x); }
 RTW_HD double tcos(double x) { return cos(x); }
 RTW_HD float texpm1(float x) { return expm1f(x); }
 RTW_HD double texpm1(double x) { return expm1(x); }
+RTW_HD float tatan(float x) { return atanf(x); }
+RTW_HD double tatan(double x) { return atan(x); }
 
 template <class T, int K>
 RTW_HD Dual<T, K> tsqrt(const Dual<T, K>& u) {
@@ -156,6 +158,8 @@ template <class T, int K>
 RTW_HD Dual<T, K> tsin(const Dual<T, K>& u) { return chain(u, tsin(u.v), tcos(u.v)); }
 template <class T, int K>
 RTW_HD Dual<T, K> tcos(const Dual<T, K>& u) { return chain(u, tcos(u.v), -tsin(u.v)); }
+template <class T, int K>
+RTW_HD Dual<T, K> tatan(const Dual<T, K>& u) { return chain(u, tatan(u.v), T(1) / (T(1) + u.v * u.v)); }
 
 // u^p for u > 0 and a constant exponent
 template <class S>

@@ -76,10 +76,11 @@ struct TorusModel {
     TorusDev tor;
     PowehiDev pw;
     SynchroDev sy;
+    WormholeDev wh;
     TorusBin bins[kTorusMaxBins];
     int n;         // bins
-    int emitter;   // 0: synchrotron torus, 1: Powehi (disk + jet), 2: Synchro_Test cylinder
-    int flat;      // geometry: 0 Kerr (Boyer-Lindquist), 1 Minkowski (Cartesian)
+    int emitter;   // 0: synchrotron torus, 1: Powehi (disk + jet), 2: Synchro_Test cylinder, 3: none (wormhole)
+    int geom;      // geometry: 0 Kerr (Boyer-Lindquist), 1 Minkowski (Cartesian), 2 Dneg wormhole
 };
 
 // The scene's emitter at a stage point z (x^mu, k^mu) and the slopes of bin c.
@@ -87,6 +88,13 @@ struct TorusModel {
 // emitter each, so the others' code stays out of their hot loops)
 template <class R, int EM = -1>
 RTW_HD TorusPt<R> em_point(const TorusModel& m, const R* z) {
+    if (EM == 3 || (EM == -1 && m.emitter == 3)) {  // the wormhole: empty space everywhere
+        TorusPt<R> o;
+        o.on = false;
+        o.zone = 0;
+        o.cj = R(0.0); o.nus = R(0.0); o.th = R(1.0); o.g = R(1.0);
+        return o;
+    }
     if (EM == 2 || (EM == -1 && m.emitter == 2)) return synchro_point<R>(m.sy, z);
     if (EM == 1 || (EM == -1 && m.emitter == 1)) return powehi_point<R>(m.pw, z);
     return torus_point<R>(m.tor, R(m.tor.a), R(m.tor.n0), R(m.tor.B0), R(m.tor.Th0), z[1], z[2], z[4], z[7]);
@@ -99,7 +107,11 @@ RTW_HD void em_bin(const TorusModel& m, const TorusPt<R>& S, int c, R& ft, R& fi
 
 // The geodesic part of the right-hand side (8 components of y).
 RTW_HD void torus_geo_rhs(const TorusModel& m, const double* y, double* f) {
-    if (m.flat) {  // straight lines (Synchro_Test.source/source_geometry.jl:55-66)
+    if (m.geom == 2) {
+        wormhole_rhs<double>(m.wh, y, f);
+        return;
+    }
+    if (m.geom == 1) {  // straight lines (Synchro_Test.source/source_geometry.jl:55-66)
         for (int i = 0; i < 4; ++i) {
             f[i] = y[4 + i];
             f[4 + i] = 0;
@@ -255,6 +267,7 @@ struct TorusKP {
     DevStats* stats;
     float* spectrum;  // [P][N]
     float* xyz;       // [P][3]
+    double* final_state;  // [P][8] (may be null)
     uint8_t* cls;
     uint32_t* steps;
     const uint32_t* ray_list;          // [total_rays] indices into the subset (dense re-record) or null
@@ -320,6 +333,8 @@ __device__ void torus_geo_stages(const TorusModel& m, const double* x, const K* 
                 kk[i] = z[4 + i];
                 kk[4 + i] = R(0);
             }
+        } else if constexpr (EM == 3) {
+            wormhole_rhs<R>(m.wh, z, kk);
         } else {
             Emit<R> em;
             KerrScene<false>::rhs<R>(m.geo, z, kk, em);
@@ -344,23 +359,67 @@ __device__ __noinline__ void torus_geo_stages_fp64(const TorusModel& m, const do
     torus_geo_stages<double, K, EM>(m, x, k1, h, *o);
 }
 
-// pad_max_dt of the geometry: Kerr (source_model.jl:86-103) or
-// Synchro_Test's max_dt_scale (1 + |x| + |y|) (source_model.jl:241-244)
-template <bool FLAT, class SR>
+// pad_max_dt of the wormhole (Wormhole.source/source_model.jl:88-110): the
+// Kerr form with |k^l| for |k^r|, a tenfold smaller epsilon within 100 a of
+// the throat, and the reference's Float32 literals
+RTW_HD double wormhole_max_dt(const WormholeDev& W, const double* x, double scale) {
+    const double th = x[2];
+    double eps = (th < kPi / 8 || th > 7 * kPi / 8) ? fmin(scale, (double)1e-1f) : scale;
+    if (fabs(x[1]) < 100 * W.a_wh) eps = eps / 10;
+    const double a = fabs(1.0 / (eps / (fabs(x[5]) + kNoDivZero)) + kNoDivZero);
+    const double b = fabs(1.0 / (eps * fmin(th, kPi - th) / (fabs(x[6]) + kNoDivZero) + kNoDivZero));
+    const double c = fabs(1.0 / (eps / (fabs(x[7]) + kNoDivZero) + kNoDivZero));
+    double m = fmin(1.0 / (a + b + c + kNoDivZero), 0.5);
+    return fmax(m, (double)1e-12f);
+}
+
+// pad_max_dt of the geometry: Kerr (source_model.jl:86-103), Synchro_Test's
+// max_dt_scale (1 + |x| + |y|) (source_model.jl:241-244) or the wormhole's
+template <int EM, class SR>
 __device__ __forceinline__ double torus_max_dt(const TorusKP& p, const double* x) {
-    if constexpr (FLAT)
+    if constexpr (EM == 2)
         return p.max_dt_scale * (1 + fabs(x[1]) + fabs(x[2]));
+    else if constexpr (EM == 3)
+        return wormhole_max_dt(p.m.wh, x, p.max_dt_scale);
     else
         return pad_max_dt<RTW_SCENE_KERR_DISK, SR>(p.m.geo, x, p.max_dt_scale);
 }
 
+// near_singularity of the geometry: Kerr (source_geometry.jl:249-269), none
+// in flat Cartesian space, the wormhole's within 5 tol of a pole
+// (Wormhole.source/source_geometry.jl:156-171)
+template <int EM>
+__device__ __forceinline__ bool torus_near_singularity(const double* x, double h, double tol, double* temp) {
+    if constexpr (EM == 2) {
+        return false;
+    } else if constexpr (EM == 3) {
+        const double th_new = x[2] + h * x[6];
+        if (fabs(th_new) <= 5 * tol) {
+            *temp = 2 * fabs(x[2]) / (fabs(x[6] * 37) + kNoDivZero);
+            return true;
+        }
+        if (fabs(th_new - kPi) <= 5 * tol) {
+            *temp = 2 * fabs((x[2] - kPi) / (fabs(x[6] * 37) + kNoDivZero));
+            return true;
+        }
+        *temp = h;
+        return false;
+    } else {
+        return near_singularity<RTW_SCENE_KERR_DISK>(x, h, tol, temp);
+    }
+}
+
 // calc_terminate without the step-count predicate; THICK when every bin's
 // tau has reached -log(tol)
-template <class SR, bool FLAT>
+template <class SR, int EM>
 __device__ __forceinline__ int torus_terminate(const TorusKP& p, const double* x, const SR* tau, int N) {
-    if constexpr (FLAT) {
+    if constexpr (EM == 2) {
         // Synchro_Test.source/source_model.jl:258-275
         if (sqrt(x[1] * x[1] + x[2] * x[2] + x[3] * x[3]) > p.m.geo.esc) return RTW_CLASS_ESCAPE;
+    } else if constexpr (EM == 3) {
+        // Wormhole.source/source_model.jl:134-147: r(l) beyond the escape radius, phi winding
+        if (wormhole_r<double>(p.m.wh, x[1]) > p.m.geo.esc) return RTW_CLASS_ESCAPE;
+        if (x[3] > p.m.geo.wind) return RTW_CLASS_WINDING;
     } else {
         if (x[1] > p.m.geo.esc) return RTW_CLASS_ESCAPE;
         if (x[1] <= p.frame.r_term) return RTW_CLASS_HORIZON;
@@ -508,7 +567,7 @@ __global__ void __launch_bounds__(128, MIXED ? 3 : 2) torus_forward(const TorusK
                 ki1[c] = SR(f[8 + N + c]);
             }
         }
-        double h = -torus_max_dt<FLAT, SR>(p, x);
+        double h = -torus_max_dt<EM, SR>(p, x);
         // where h came from: 0 the controller (held fixed by the adjoint),
         // 1 -pad_max_dt of the previous accepted step's start state, 2 -pad_max_dt
         // of the current state
@@ -543,10 +602,10 @@ __global__ void __launch_bounds__(128, MIXED ? 3 : 2) torus_forward(const TorusK
         int cls = 0;
         for (;;) {
             ++c_att;
-            const double max_dt = torus_max_dt<FLAT, SR>(p, x);
+            const double max_dt = torus_max_dt<EM, SR>(p, x);
             double temp;
             bool done = false;
-            if (!FLAT && near_singularity<RTW_SCENE_KERR_DISK>(x, h, tol, &temp)) {
+            if (torus_near_singularity<EM>(x, h, tol, &temp)) {
                 // polar escape (integrators_LttM.jl:62-105) in FP64 on the full state
                 checkpoint();
                 double y[8 + 2 * kTorusMaxBins], f[8 + 2 * kTorusMaxBins];
@@ -563,7 +622,7 @@ __global__ void __launch_bounds__(128, MIXED ? 3 : 2) torus_forward(const TorusK
                 int nsub = 0;
                 for (int it = 0; it < 37; ++it) {
                     if (it > 0) {
-                        if (torus_terminate<double, FLAT>(p, y, y + 8, N)) continue;
+                        if (torus_terminate<double, EM>(p, y, y + 8, N)) continue;
                         torus_f64(p.m, y, f);
                     }
                     for (int i = 0; i < D; ++i) y[i] -= temp * f[i];
@@ -579,7 +638,7 @@ __global__ void __launch_bounds__(128, MIXED ? 3 : 2) torus_forward(const TorusK
                     ihi[q] = SR(y[8 + N + q]);
                     ilo[q] = MIXED ? SR(y[8 + N + q] - (double)ihi[q]) : SR(0);
                 }
-                if (torus_terminate<double, FLAT>(p, y, y + 8, N)) {
+                if (torus_terminate<double, EM>(p, y, y + 8, N)) {
                     done = true;
                     prev_rej = false;
                 } else {
@@ -589,7 +648,7 @@ __global__ void __launch_bounds__(128, MIXED ? 3 : 2) torus_forward(const TorusK
                         kt1[q] = SR(f[8 + q]);
                         ki1[q] = SR(f[8 + N + q]);
                     }
-                    h = -torus_max_dt<FLAT, SR>(p, x);
+                    h = -torus_max_dt<EM, SR>(p, x);
                     hsrc = 2;
                 }
             }
@@ -597,7 +656,9 @@ __global__ void __launch_bounds__(128, MIXED ? 3 : 2) torus_forward(const TorusK
                 // geodesic stages
                 TorusStages<SR> st;
                 bool promote = false;
-                if (MIXED && !FLAT)
+                if (MIXED && EM == 3)  // the wormhole: the poles only (no horizon)
+                    promote = (x[2] < p.promote_theta) || (x[2] > kPi - p.promote_theta);
+                else if (MIXED && !FLAT)
                     promote = (x[1] - p.m.geo.r_ev < p.promote_dr) || (x[2] < p.promote_theta) ||
                               (x[2] > kPi - p.promote_theta);
                 if (promote) {
@@ -727,7 +788,7 @@ __global__ void __launch_bounds__(128, MIXED ? 3 : 2) torus_forward(const TorusK
             }
             ++nsteps;
             if (nsteps >= p.frame.max_steps) cls = RTW_CLASS_MAXSTEPS;
-            else cls = torus_terminate<SR, FLAT>(p, x, tau, N);
+            else cls = torus_terminate<SR, EM>(p, x, tau, N);
             if (cls) break;
         }
         bool fin = true;
@@ -753,6 +814,8 @@ __global__ void __launch_bounds__(128, MIXED ? 3 : 2) torus_forward(const TorusK
         }
         if (p.cls) p.cls[id] = (uint8_t)cls;
         if (p.steps) p.steps[id] = (uint32_t)nsteps;
+        if (p.final_state)
+            for (int i = 0; i < 8; ++i) p.final_state[8 * id + i] = x[i];
         if (p.record) torus_rec_end<SR, MIXED>(p, &rec, loc, sub, n_ev, escaped, x, tau, ihi, ilo);
     }
     atomicAdd(&p.stats->step_attempts, (unsigned long long)c_att);
@@ -1330,8 +1393,15 @@ rtw_status torus_model(const rtw_scene& s, const double* colors_nm, int N, Torus
         why = "the per-bin scenes take 1..32 bins";
         return RTW_ERR_INVALID_PARAM;
     }
-    const bool powehi = s.kind == RTW_SCENE_KERR_POWEHI, synchro = s.kind == RTW_SCENE_SYNCHRO_TEST;
-    if (!(s.mass > 0) || !(std::fabs(s.spin) < s.mass) || !(s.b_0 > 0) || !(s.length_cm > 0) || !(s.n_e0 >= 0)) {
+    const bool powehi = s.kind == RTW_SCENE_KERR_POWEHI, synchro = s.kind == RTW_SCENE_SYNCHRO_TEST,
+               wormhole = s.kind == RTW_SCENE_WORMHOLE;
+    if (wormhole) {
+        if (!(s.r_in > 0) || !(s.edge_in >= 0) || !(s.edge_out > 0) || !(s.escape_radius > s.r_in)) {
+            why = "wormhole parameters out of range";
+            return RTW_ERR_INVALID_PARAM;
+        }
+    } else if (!(s.mass > 0) || !(std::fabs(s.spin) < s.mass) || !(s.b_0 > 0) || !(s.length_cm > 0) ||
+               !(s.n_e0 >= 0)) {
         why = "scene parameters out of range";
         return RTW_ERR_INVALID_PARAM;
     }
@@ -1339,7 +1409,7 @@ rtw_status torus_model(const rtw_scene& s, const double* colors_nm, int N, Torus
         why = "cylinder radius and escape radius must be > 0";
         return RTW_ERR_INVALID_PARAM;
     }
-    if (!powehi && !synchro && (!(s.r_in > 0) || !(s.r_out >= s.r_in) || !(s.edge_in > 0) || !(s.edge_out > 0) ||
+    if (!powehi && !synchro && !wormhole && (!(s.r_in > 0) || !(s.r_out >= s.r_in) || !(s.edge_in > 0) || !(s.edge_out > 0) ||
                     !(s.theta_e0 > 0) || !(s.rho_h > 0))) {
         why = "torus parameters out of range";
         return RTW_ERR_INVALID_PARAM;
@@ -1386,8 +1456,15 @@ rtw_status torus_model(const rtw_scene& s, const double* colors_nm, int N, Torus
         m.bins[c].inv_b0 = 1.0 / m.bins[c].b0;
     }
     m.n = N;
-    m.emitter = powehi ? 1 : synchro ? 2 : 0;
-    m.flat = synchro ? 1 : 0;
+    m.emitter = powehi ? 1 : synchro ? 2 : wormhole ? 3 : 0;
+    m.geom = synchro ? 1 : wormhole ? 2 : 0;
+    if (wormhole) {
+        // Wormhole.source/source_geometry.jl:7-15: M = W / W_over_M
+        const double c = kPi / (2 * std::sqrt(2.0));
+        m.wh.rho = s.r_in;
+        m.wh.a_wh = s.edge_in;
+        m.wh.M = s.edge_out / (-std::log(1 / std::cos(c)) + c * std::tan(c));
+    }
     if (powehi || synchro) powehi_model(s, m.geo, m.pw);  // the power-law constants
     if (synchro) {
         m.sy.b_z = s.b_0;
@@ -1401,12 +1478,14 @@ rtw_status torus_model(const rtw_scene& s, const double* colors_nm, int N, Torus
 }
 
 // the forward kernel instance: precision x emitter (0 torus, 1 Powehi, 2
-// Synchro_Test, the last in flat geometry)
+// Synchro_Test in flat Cartesian geometry, 3 none in the wormhole's geometry)
 const void* forward_fn(bool mixed, int emitter) {
-    static const void* const fn[2][3] = {
-        {(const void*)torus_forward<false, 0>, (const void*)torus_forward<false, 1>, (const void*)torus_forward<false, 2>},
-        {(const void*)torus_forward<true, 0>, (const void*)torus_forward<true, 1>, (const void*)torus_forward<true, 2>}};
-    return fn[mixed ? 1 : 0][emitter >= 0 && emitter <= 2 ? emitter : 0];
+    static const void* const fn[2][4] = {
+        {(const void*)torus_forward<false, 0>, (const void*)torus_forward<false, 1>, (const void*)torus_forward<false, 2>,
+         (const void*)torus_forward<false, 3>},
+        {(const void*)torus_forward<true, 0>, (const void*)torus_forward<true, 1>, (const void*)torus_forward<true, 2>,
+         (const void*)torus_forward<true, 3>}};
+    return fn[mixed ? 1 : 0][emitter >= 0 && emitter <= 3 ? emitter : 0];
 }
 
 // launch shape of the torus kernels: 128 threads, occupancy-limited CTAs
@@ -1492,17 +1571,21 @@ rtw_status torus_render(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* 
     uint8_t* cls = out->term_class;
     uint32_t* steps = out->steps;
     float* xyz = out->xyz;
+    double* fst = out->final_state;
     if (!out->on_device) {
         auto up = [](size_t v) { return (v + 255) & ~(size_t)255; };
         const size_t o_steps = up((size_t)P * N * 4), o_cls = o_steps + up((size_t)P * 4),
-                     o_xyz = o_cls + up((size_t)P), need = o_xyz + up((size_t)P * 12);
+                     o_xyz = o_cls + up((size_t)P), o_fst = o_xyz + up((size_t)P * 12),
+                     need = o_fst + up((size_t)P * 64);
         if ((st = ensure(ctx, &b->out, &b->out_cap, need)) != RTW_OK) return st;
         char* base = (char*)b->out;
         spec = out->spectrum ? (float*)base : nullptr;
         steps = out->steps ? (uint32_t*)(base + o_steps) : nullptr;
         cls = out->term_class ? (uint8_t*)(base + o_cls) : nullptr;
         xyz = out->xyz ? (float*)(base + o_xyz) : nullptr;
+        fst = out->final_state ? (double*)(base + o_fst) : nullptr;
     }
+    p.final_state = fst;
     p.spectrum = spec;
     p.cls = cls;
     p.steps = steps;
@@ -1523,6 +1606,9 @@ rtw_status torus_render(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* 
     }
     if (out->xyz && !out->on_device)
         RTW_CUDA(cudaMemcpyAsync(out->xyz, xyz, sizeof(float) * 3 * P, cudaMemcpyDeviceToHost, s), "xyz D2H");
+    if (out->final_state && !out->on_device)
+        RTW_CUDA(cudaMemcpyAsync(out->final_state, fst, sizeof(double) * 8 * P, cudaMemcpyDeviceToHost, s),
+                 "state D2H");
     RTW_CUDA(cudaEventRecord(ctx->ev[3], s), "event");
     ctx->have_last = true;
     ctx->last_frames = 0;
@@ -1849,7 +1935,7 @@ rtw_status rtw_torus_rhs(const rtw_scene* scene, const double* colors_nm, int32_
                          const double* state, double* slope) {
     if (!scene || !state || !slope ||
         (scene->kind != RTW_SCENE_KERR_SYNCHRO_TORUS && scene->kind != RTW_SCENE_KERR_POWEHI &&
-         scene->kind != RTW_SCENE_SYNCHRO_TEST))
+         scene->kind != RTW_SCENE_SYNCHRO_TEST && scene->kind != RTW_SCENE_WORMHOLE))
         return RTW_ERR_INVALID_PARAM;
     TorusModel m;
     std::string why;

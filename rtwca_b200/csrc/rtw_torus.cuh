@@ -348,6 +348,58 @@ RTW_HD TorusPt<T> synchro_point(const SynchroDev& Y, const T* z) {
     return o;
 }
 
+// ---------------------------------------------------------------------------
+// Wormhole.source, the reference's Dneg wormhole (Interstellar's): coordinates
+// (t, l, theta, phi), metric -dt^2 + dl^2 + r(l)^2 dOmega^2, throat radius rho,
+// half-length a, lensing width W = M W_over_M (source_geometry.jl:7-150). No
+// emitter anywhere (source_model.jl:54-86).
+// ---------------------------------------------------------------------------
+struct WormholeDev {
+    double rho, a_wh, M;  // throat radius, half-length, lensing mass parameter
+};
+
+// r(l) (source_geometry.jl:22-31)
+template <class T>
+RTW_HD T wormhole_r(const WormholeDev& W, const T& l) {
+    typedef decltype(val(l)) B;
+    const double lv = (double)val(l);
+    if (!(fabs(lv) > W.a_wh)) return T(B(W.rho));
+    const T al = lv < 0 ? T(B(0)) - l : l;
+    const T x = (al - B(W.a_wh)) * B(2.0 / (kPi * W.M));
+    return T(B(W.rho)) + B(W.M) * (x * tatan(x) - tlog(T(B(1)) + x * x) * B(0.5));
+}
+
+// dr/dl as the reference writes it (source_geometry.jl:34-41): 2 sign(l)
+// (atan x + (x - 1) / (1 + x^2)) / pi. (The derivative of its r(l) is
+// 2 sign(l) atan(x) / pi; the extra term is the reference's, kept for parity.)
+template <class T>
+RTW_HD T wormhole_drdl(const WormholeDev& W, const T& l) {
+    typedef decltype(val(l)) B;
+    const double lv = (double)val(l);
+    if (!(fabs(lv) > W.a_wh)) return T(B(0));
+    const T al = lv < 0 ? T(B(0)) - l : l;
+    const T x = (al - B(W.a_wh)) * B(2.0 / (kPi * W.M));
+    const T d = (tatan(x) + (x - B(1)) / (T(B(1)) + x * x)) * B(2.0 / kPi);
+    return lv < 0 ? T(B(0)) - d : d;
+}
+
+// the geodesic right-hand side from the Christoffel symbols of
+// calc_christoffel_udd! (source_geometry.jl:131-150): z = (t, l, theta, phi,
+// k^t, k^l, k^theta, k^phi)
+template <class T>
+RTW_HD void wormhole_rhs(const WormholeDev& W, const T* z, T* k) {
+    typedef decltype(val(z[1])) B;
+    const T r = wormhole_r<T>(W, z[1]), rp = wormhole_drdl<T>(W, z[1]);
+    const T sn = tsin(z[2]), cs = tcos(z[2]);
+    const T kl = z[5], kth = z[6], kph = z[7];
+    const T rpr = rp / r;
+    for (int i = 0; i < 4; ++i) k[i] = z[4 + i];
+    k[4] = T(B(0));
+    k[5] = r * rp * kth * kth + r * rp * sn * sn * kph * kph;
+    k[6] = B(-2) * rpr * kl * kth + sn * cs * kph * kph;
+    k[7] = B(-2) * rpr * kl * kph - B(2) * (cs / sn) * kth * kph;
+}
+
 // Slopes of one bin without exp(-tau) (as torus_bin): nu = g nu_c in nm^-1.
 // Disk: a = a_nu, j = a B_nu(T); jet: j = J0 s^-(p-1)/2, a = A0 / nu s^-(p+2)/2,
 // s = nu / (nu_cyc sin theta_B) (calc_radiative_coefficients).

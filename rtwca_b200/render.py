@@ -230,6 +230,8 @@ _WORLDS = {
     "m87": (abi.SCENE_KERR_POWEHI, [0, 35, 0.3, 0], [PI / 2, PI / 6], [0.0, 0.0, PI], 0.0),
     # initialization.jl:120-128 (Synchro_Test.source, Cartesian t, x, y, z)
     "synch": (abi.SCENE_SYNCHRO_TEST, [0.0, 0.0, 0.0, 0.0], [0.0, 0.0], [PI / 8, 0.0, PI], 0.0),
+    # initialization.jl:140-148 (Wormhole.source, coordinates t, l, theta, phi)
+    "wormhole": (abi.SCENE_WORMHOLE, [0, 5, PI / 2, 0], [PI / 2, 0], [0.0, 0.0, -PI / 2], 0.0),
 }
 
 _current: World | None = None
@@ -242,8 +244,8 @@ def available_worlds() -> list:
 
 def initialize_world(input_string: str):
     """Selects a scene and returns its default (position, direction, pointing, beta)
-    (initialization.jl:78-172). Scenes that need the reference's missing textures
-    (wormhole, Cartesian sphere) are not on this library's path and raise
+    (initialization.jl:78-172). The Cartesian sphere (its image is a skybox of
+    the reference's missing textures) is not on this library's path and raises
     ValueError."""
     global _current
     key = input_string.lower()

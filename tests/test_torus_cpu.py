@@ -209,3 +209,21 @@ def test_synchro_rhs_matches_oracle(oracle):
             assert err.max() < 1e-11, (x, y, z, err.max())
             inside += bool(np.any(ref[8:] != 0))
     assert inside == 12  # the four points inside the cylinder emit, the two outside do not
+
+
+def test_wormhole_rhs_matches_oracle(oracle):
+    """The Dneg wormhole (Wormhole.source): the library's geodesic right-hand
+    side against the oracle's Christoffel contraction, in the throat, near it
+    and far out on both sides; no emission anywhere."""
+    sc = configs.wormhole_scene()
+    assert sc.kind == abi.SCENE_WORMHOLE and (sc.r_in, sc.edge_in, sc.edge_out) == (1.0, 0.005, 0.05)
+    col = np.array([400.0, 550.0, 700.0])
+    rng = np.random.default_rng(7)
+    for l, th in [(0.0, 1.2), (0.003, 0.7), (0.2, 1.5), (-0.4, 2.0), (5.0, 1.571), (-30.0, 0.3), (80.0, 2.9)]:
+        st = np.zeros(8 + 2 * col.size)
+        st[:8] = [0.0, l, th, 0.4, 1.0, *rng.normal(size=3)]
+        ref = oracle.rhs(sc, col, st)
+        f = abi.torus_rhs(sc, col, st, 0)
+        err = np.abs(f[:8] - ref[:8]) / np.maximum(np.abs(ref[:8]), 1e-12 * np.abs(ref[:8]).max() + 1e-300)
+        assert err.max() < 1e-12, (l, th, err.max())
+        assert np.all(f[8:] == 0) and np.all(ref[8:] == 0)
