@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define RTW_ABI_VERSION 4
+#define RTW_ABI_VERSION 5
 /* Largest number of spectral bins (reference `colors`) one render takes. */
 #define RTW_MAX_BINS 128
 /* Largest number of frames (cameras) one batched render takes. */
@@ -228,6 +228,16 @@ typedef struct rtw_render_params {
                                    counter reset, kernel) is captured once in a
                                    CUDA graph and replayed while the launch
                                    parameters match; cameras may change */
+    /* RTW_SCENE_WORMHOLE: the two skyboxes (skybox[0] beyond the throat's
+       positive-l side, skybox[1] beyond its negative side), each a cube map in
+       the reference's cross layout: skybox_h[k] pixels per face edge, 3 h rows
+       x 4 h columns of (R, G, B) float32 in [0, 1], row 0 at the top (the
+       PNGs the reference loads in load_textures; NULL: no skybox). Host
+       memory. A ray that ends beyond r(l) = 50 adds the texel it points at,
+       as the reference's skybox_handling! without ray bundles does
+       (Wormhole.source/source_model.jl:150-443). */
+    const float* skybox[2];
+    int32_t skybox_h[2];
 } rtw_render_params;
 
 /* Output buffers, owned by the caller. Pixel p of frame f is at

@@ -53,6 +53,8 @@ def load() -> C.CDLL:
                                       D, C.POINTER(C.c_ubyte), C.POINTER(C.c_uint), D, D, D,
                                       C.POINTER(C.c_longlong), C.c_int]
         lib.oracle_render.restype = C.c_int
+        lib.oracle_set_skybox.argtypes = [C.c_int, C.POINTER(C.c_float), C.c_int]
+        lib.oracle_set_skybox.restype = C.c_int
         _lib = lib
     return _lib
 
@@ -112,7 +114,7 @@ def pad_max_dt(scene, x, scale):
 
 
 def render(scene, cam, colors_nm, *, max_dt_scale=0.1, integrator=0, pixel_ids=None, threads=0,
-           want=("xyz", "class", "steps", "spectrum", "tau", "state")):
+           want=("xyz", "class", "steps", "spectrum", "tau", "state"), skybox=(None, None)):
     """Traces one camera (or the pixel subset `pixel_ids`) with the FP64 oracle.
     Returns a dict of arrays indexed like the pixel list, plus 'counters'
     (step attempts, rejected attempts, polar Euler sub-steps)."""
@@ -139,12 +141,21 @@ def render(scene, cam, colors_nm, *, max_dt_scale=0.1, integrator=0, pixel_ids=N
     def ptr(a, t):
         return a.ctypes.data_as(C.POINTER(t)) if a is not None else None
 
-    st = load().oracle_render(
-        C.byref(scene), C.byref(cam), _dp(c), N, float(max_dt_scale), int(integrator),
-        ids.ctypes.data_as(C.POINTER(C.c_longlong)) if ids is not None else None, n,
-        ptr(res["xyz"], C.c_double), ptr(res["class"], C.c_ubyte), ptr(res["steps"], C.c_uint),
-        ptr(res["spectrum"], C.c_double), ptr(res["tau"], C.c_double), ptr(res["state"], C.c_double),
-        counters.ctypes.data_as(C.POINTER(C.c_longlong)), int(threads))
+    # the wormhole's skyboxes (float32 [3 h, 4 h, 3] cross layout), set for this call
+    texs = [None if t is None else np.ascontiguousarray(t, dtype=np.float32) for t in skybox]
+    for k, t in enumerate(texs):
+        load().oracle_set_skybox(k, t.ctypes.data_as(C.POINTER(C.c_float)) if t is not None else None,
+                                 t.shape[0] // 3 if t is not None else 0)
+    try:
+        st = load().oracle_render(
+            C.byref(scene), C.byref(cam), _dp(c), N, float(max_dt_scale), int(integrator),
+            ids.ctypes.data_as(C.POINTER(C.c_longlong)) if ids is not None else None, n,
+            ptr(res["xyz"], C.c_double), ptr(res["class"], C.c_ubyte), ptr(res["steps"], C.c_uint),
+            ptr(res["spectrum"], C.c_double), ptr(res["tau"], C.c_double), ptr(res["state"], C.c_double),
+            counters.ctypes.data_as(C.POINTER(C.c_longlong)), int(threads))
+    finally:
+        for k in range(2):
+            load().oracle_set_skybox(k, None, 0)
     if st != 0:
         raise RuntimeError(f"oracle_render failed with status {st}")
     res = {k: v for k, v in res.items() if v is not None}

@@ -1091,7 +1091,81 @@ void cie_weights(const double* colors, int n, double* wx, double* wy, double* wz
 // ----------------------------------------------------------------------------
 // C API for tests (ctypes). Outputs are double precision.
 // ----------------------------------------------------------------------------
+// Skyboxes of the wormhole (set by oracle_set_skybox): cube maps in the
+// reference's cross layout, 3h rows x 4h columns x RGB, row 0 at the top.
+static const float* g_sky[2] = {nullptr, nullptr};
+static int g_sky_h[2] = {0, 0};
+
+inline double normal_gauss(double x, double s, double m) {  // my_special_functions.jl:20-22
+    return std::exp(-(x - m) * (x - m) / (2 * s * s)) / (s * std::sqrt(2 * kPi));
+}
+
+// skybox_handling! without ray bundles (Wormhole.source/source_model.jl:393-
+// 443): calc_skybox_coord (:175-263, R_sph_to_cart gen_geometry.jl:110-122),
+// cubemap_coord_calc (gen_geometry.jl:347-370), skybox_I_nu_calc (:150-172)
+void wormhole_skybox(const OScene& sc, double* ray, int N, const double* freq) {
+    const double rl = sc.wh_r(ray[1]);
+    if (!(rl > 50) || ray[1] == 0) return;
+    const int k = ray[1] > 0 ? 0 : 1;
+    if (!g_sky[k]) return;
+    const int H = g_sky_h[k];
+    const double th = ray[2], ph = ray[3];
+    const double e[4] = {ray[4], ray[5], rl * ray[6], rl * std::sin(th) * ray[7]};
+    double R[4][4] = {};
+    R[0][0] = 1;
+    R[1][1] = std::sin(th) * std::cos(ph); R[1][2] = std::cos(th) * std::cos(ph); R[1][3] = -std::sin(ph);
+    R[2][1] = std::sin(th) * std::sin(ph); R[2][2] = std::cos(th) * std::sin(ph); R[2][3] = std::cos(ph);
+    R[3][1] = std::cos(th); R[3][2] = -std::sin(th);
+    double v[4] = {0, 0, 0, 0};
+    for (int a = 0; a < 4; ++a)
+        for (int b = 0; b < 4; ++b) v[a] += R[a][b] * e[b];
+    const double nv = std::sqrt(v[1] * v[1] + v[2] * v[2] + v[3] * v[3]);
+    const double x = v[1] / nv, y = v[2] / nv, z = v[3] / nv;
+    int face;
+    if (std::fabs(x) >= std::fabs(y) && std::fabs(x) >= std::fabs(z)) face = x > 0 ? 1 : 3;
+    else if (std::fabs(y) >= std::fabs(x) && std::fabs(y) >= std::fabs(z)) face = y > 0 ? 4 : 2;
+    else face = z > 0 ? 6 : 5;
+    double u, w;
+    switch (face) {
+    case 1: u = -y / std::fabs(x); w = z / std::fabs(x); break;
+    case 2: u = -x / std::fabs(y); w = z / std::fabs(y); break;
+    case 3: u = y / std::fabs(x); w = z / std::fabs(x); break;
+    case 4: u = x / std::fabs(y); w = z / std::fabs(y); break;
+    case 5: u = -x / std::fabs(z); w = -y / std::fabs(z); break;
+    default: u = -x / std::fabs(z); w = y / std::fabs(z); break;
+    }
+    long long i = std::min((long long)std::floor(H * (u + 1) / 2) + 1, (long long)H);
+    long long j = std::min((long long)std::floor(H * (w + 1) / 2) + 1, (long long)H);
+    switch (face) {
+    case 1: j += H; break;
+    case 2: i += H; j += H; break;
+    case 3: i += 2 * H; j += H; break;
+    case 4: i += 3 * H; j += H; break;
+    case 5: i += H; break;
+    default: i += H; j += 2 * H; break;
+    }
+    const float* t = g_sky[k] + ((3LL * H - j) * 4LL * H + (i - 1)) * 3;
+    const double Rc = 1.0 * t[0], Gc = 0.843 * t[1], Bc = 0.914 * t[2];
+    const double fs = ray[4];  // -g(u, k) with u = (1, 0, 0, 0), g_tt = -1
+    for (int c = 0; c < N; ++c) {
+        const double f = freq[c] * fs;
+        const double I = 1e-12 * (Rc * normal_gauss(f, 5e-5, 0.001587) + Gc * normal_gauss(f, 7e-5, 0.001879) +
+                                  Bc * normal_gauss(f, 9e-5, 0.002141));
+        ray[8 + 2 * c] += I * std::exp(-ray[9 + 2 * c]) / (f * f * f);
+    }
+}
+
 extern "C" {
+
+// the wormhole's skybox k (0: positive-l side, 1: negative), h pixels per
+// face edge (tex NULL: none); kept until changed
+int oracle_set_skybox(int k, const float* tex, int h) {
+    if (k < 0 || k > 1 || (tex && h < 1)) return RTW_ERR_INVALID_PARAM;
+    g_sky[k] = tex;
+    g_sky_h[k] = tex ? h : 0;
+    return RTW_OK;
+}
+
 
 int oracle_abi_version(void) { return RTW_ABI_VERSION; }
 
@@ -1206,6 +1280,7 @@ int oracle_render(const rtw_scene* scene, rtw_camera* cam, const double* colors_
             }
             for (int k = 0; k < 8; ++k)
                 if (!std::isfinite(ray[k])) klass = RTW_CLASS_NAN;
+            if (sc.is_wh()) wormhole_skybox(sc, ray.data(), N, freq.data());
             tot_steps += step_count;
             tot_esc += esc;
             if (cls) cls[q] = (unsigned char)klass;

@@ -15,7 +15,7 @@ PKG = Path(__file__).resolve().parent
 # RTW_LIB_PATH selects another build of the same library (e.g. a tuning variant)
 LIB_PATH = Path(os.environ.get("RTW_LIB_PATH", PKG / "librtw_b200.so"))
 
-ABI_VERSION = 4
+ABI_VERSION = 5
 MAX_BINS = 128
 MAX_FRAMES = 4096
 TRACE_FIELDS = 15
@@ -100,6 +100,7 @@ class RenderParams(C.Structure):
         ("block_warps", C.c_int32), ("ctas_per_sm", C.c_int32),
         ("stream", C.c_void_p), ("pixel_order", C.c_int32), ("refill_min", C.c_int32),
         ("trace_ray", C.c_int64), ("autotune", C.c_int32), ("graph", C.c_int32),
+        ("skybox", C.POINTER(C.c_float) * 2), ("skybox_h", C.c_int32 * 2),
     ]
 
 

@@ -268,6 +268,8 @@ struct TorusKP {
     float* spectrum;  // [P][N]
     float* xyz;       // [P][3]
     double* final_state;  // [P][8] (may be null)
+    const float* sky[2];  // the wormhole's skyboxes (cross-layout cube maps) or null
+    int sky_h[2];         // pixels per face edge
     uint8_t* cls;
     uint32_t* steps;
     const uint32_t* ray_list;          // [total_rays] indices into the subset (dense re-record) or null
@@ -357,6 +359,69 @@ template <class K, int EM>
 __device__ __noinline__ void torus_geo_stages_fp64(const TorusModel& m, const double* x, const K* k1, double h,
                                                    TorusStages<double>* o) {
     torus_geo_stages<double, K, EM>(m, x, k1, h, *o);
+}
+
+// skybox_handling! without ray bundles (Wormhole.source/source_model.jl:393-
+// 443) at a ray's end x: beyond r(l) = 50 the ray takes the texel of the
+// skybox on its side of the throat that its direction points at
+// (calc_skybox_coord :175-263 with R_sph_to_cart, gen_geometry.jl:110-122;
+// cubemap_coord_calc, gen_geometry.jl:347-370) and adds, per bin, the
+// texel's spectrum (skybox_I_nu_calc :150-172: three Gaussian lines for R, G,
+// B) x exp(-tau) / f^3 at f = nu_c k^t.
+__device__ void wormhole_skybox(const TorusKP& p, const double* x, int N, double* I, const double* tau) {
+    const WormholeDev& W = p.m.wh;
+    const double rl = wormhole_r<double>(W, x[1]);
+    if (!(rl > 50) || x[1] == 0) return;
+    const int k = x[1] > 0 ? 0 : 1;
+    if (!p.sky[k]) return;
+    const long long H = p.sky_h[k];
+    double st, ct, sp, cp;
+    sincos(x[2], &st, &ct);
+    sincos(x[3], &sp, &cp);
+    const double e1 = x[5], e2 = rl * x[6], e3 = rl * st * x[7];
+    const double vx = st * cp * e1 + ct * cp * e2 - sp * e3;
+    const double vy = st * sp * e1 + ct * sp * e2 + cp * e3;
+    const double vz = ct * e1 - st * e2;
+    const double nv = sqrt(vx * vx + vy * vy + vz * vz);
+    const double X = vx / nv, Y = vy / nv, Z = vz / nv;
+    const double ax = fabs(X), ay = fabs(Y), az = fabs(Z);
+    int face;
+    if (ax >= ay && ax >= az) face = X > 0 ? 1 : 3;
+    else if (ay >= ax && ay >= az) face = Y > 0 ? 4 : 2;
+    else face = Z > 0 ? 6 : 5;
+    double u, v;
+    switch (face) {
+    case 1: u = -Y / ax; v = Z / ax; break;
+    case 2: u = -X / ay; v = Z / ay; break;
+    case 3: u = Y / ax; v = Z / ax; break;
+    case 4: u = X / ay; v = Z / ay; break;
+    case 5: u = -X / az; v = -Y / az; break;
+    default: u = -X / az; v = Y / az; break;
+    }
+    long long i = (long long)floor(H * (u + 1) / 2) + 1, j = (long long)floor(H * (v + 1) / 2) + 1;
+    if (i > H) i = H;
+    if (j > H) j = H;
+    if (i < 1) i = 1;  // (u, v) in [-1, 1]: rounding only
+    if (j < 1) j = 1;
+    switch (face) {
+    case 1: j += H; break;
+    case 2: i += H; j += H; break;
+    case 3: i += 2 * H; j += H; break;
+    case 4: i += 3 * H; j += H; break;
+    case 5: i += H; break;
+    default: i += H; j += 2 * H; break;
+    }
+    const float* t = p.sky[k] + ((3 * H - j) * 4 * H + (i - 1)) * 3;
+    const double R = 1.0 * (double)t[0], G = 0.843 * (double)t[1], B = 0.914 * (double)t[2];
+    const double inv = 1.0 / sqrt(2 * kPi);
+    for (int c = 0; c < N; ++c) {
+        const double f = p.m.bins[c].nu_nm * x[4];
+        const double d1 = f - 0.001587, d2 = f - 0.001879, d3 = f - 0.002141;
+        const double s = 1e-12 * inv *
+                         (R * exp(-d1 * d1 / (2 * 5e-5 * 5e-5)) / 5e-5 + G * exp(-d2 * d2 / (2 * 7e-5 * 7e-5)) / 7e-5 +
+                          B * exp(-d3 * d3 / (2 * 9e-5 * 9e-5)) / 9e-5);
+        I[c] += s * exp(-tau[c]) / (f * f * f);
+    }
 }
 
 // pad_max_dt of the wormhole (Wormhole.source/source_model.jl:88-110): the
@@ -796,6 +861,20 @@ __global__ void __launch_bounds__(128, MIXED ? 3 : 2) torus_forward(const TorusK
         if (!fin) {
             cls = RTW_CLASS_NAN;
             ++c_nan;
+        }
+        if constexpr (EM == 3) {
+            if (fin && (p.sky[0] || p.sky[1])) {
+                double I[kTorusMaxBins], tv[kTorusMaxBins];
+                for (int c = 0; c < N; ++c) {
+                    I[c] = (double)ihi[c] + (MIXED ? (double)ilo[c] : 0.0);
+                    tv[c] = (double)tau[c];
+                }
+                wormhole_skybox(p, x, N, I, tv);
+                for (int c = 0; c < N; ++c) {
+                    ihi[c] = SR(I[c]);
+                    ilo[c] = MIXED ? SR(I[c] - (double)ihi[c]) : SR(0);
+                }
+            }
         }
         if (p.spectrum || p.xyz) {
             double X = 0, Y = 0, Z = 0;
@@ -1326,6 +1405,8 @@ struct TorusBuffers {
     size_t pool_cap = 0;
     void* pool2 = nullptr;  // recording chunks (the overflowed rays)
     size_t pool2_cap = 0;
+    void* sky = nullptr;    // the wormhole's skyboxes
+    size_t sky_cap = 0;
     void* fin = nullptr;   // final states
     size_t fin_cap = 0;
     void* tgt = nullptr;
@@ -1334,7 +1415,7 @@ struct TorusBuffers {
 
 void torus_free(TorusBuffers* b) {
     if (!b) return;
-    for (void* q : {b->ctl, b->out, b->nev, b->evh, b->evk, b->ck, b->work, b->tgt, b->pool, b->pool2, b->fin})
+    for (void* q : {b->ctl, b->out, b->nev, b->evh, b->evk, b->ck, b->work, b->tgt, b->pool, b->pool2, b->fin, b->sky})
         if (q) cudaFree(q);
     delete b;
 }
@@ -1587,6 +1668,27 @@ rtw_status torus_render(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* 
     }
     p.final_state = fst;
     p.spectrum = spec;
+    // the wormhole's skyboxes: host cube maps uploaded for this render
+    if (scene->kind == RTW_SCENE_WORMHOLE) {
+        size_t off[2] = {0, 0}, need = 0;
+        for (int k = 0; k < 2; ++k)
+            if (prm->skybox[k]) {
+                if (prm->skybox_h[k] < 1) return fail(ctx, RTW_ERR_INVALID_PARAM, "skybox_h must be >= 1");
+                off[k] = need;
+                need += ((size_t)12 * prm->skybox_h[k] * prm->skybox_h[k] * 3 * sizeof(float) + 255) & ~(size_t)255;
+            }
+        if (need) {
+            if ((st = ensure(ctx, &b->sky, &b->sky_cap, need)) != RTW_OK) return st;
+            for (int k = 0; k < 2; ++k)
+                if (prm->skybox[k]) {
+                    const size_t bytes = (size_t)12 * prm->skybox_h[k] * prm->skybox_h[k] * 3 * sizeof(float);
+                    RTW_CUDA(cudaMemcpyAsync((char*)b->sky + off[k], prm->skybox[k], bytes, cudaMemcpyHostToDevice, s),
+                             "skybox H2D");
+                    p.sky[k] = (const float*)((char*)b->sky + off[k]);
+                    p.sky_h[k] = prm->skybox_h[k];
+                }
+        }
+    }
     p.cls = cls;
     p.steps = steps;
     p.xyz = xyz;

@@ -62,7 +62,10 @@ class Renderer:
     @staticmethod
     def params(colors_nm, precision=abi.PREC_FP64, integrator=abi.DP45_REF_COMPAT, max_dt_scale=0.1,
                block_warps=0, ctas_per_sm=0, promote_dr=0.0, promote_sin=0.0, stream=None,
-               pixel_order=0, ray_bundles=False, trace_ray=-1, refill_min=0, autotune=False, graph=False):
+               pixel_order=0, ray_bundles=False, trace_ray=-1, refill_min=0, autotune=False, graph=False,
+               skybox=(None, None)):
+        """skybox: the wormhole's two cube maps, each None or a float32 array
+        [3 h, 4 h, 3] in the reference's cross layout (RGB in [0, 1])."""
         colors = np.ascontiguousarray(np.asarray(colors_nm, dtype=np.float64))
         p = abi.RenderParams()
         p.n_colors = int(colors.size)
@@ -81,7 +84,18 @@ class Renderer:
         p.refill_min = int(refill_min)
         p.autotune = int(bool(autotune))
         p.graph = int(bool(graph))
-        p._keep = colors  # keep the array alive with the struct
+        keep = [colors]
+        for k, tex in enumerate(skybox):
+            if tex is None:
+                continue
+            t = np.ascontiguousarray(np.asarray(tex, dtype=np.float32))
+            h = t.shape[0] // 3
+            if t.ndim != 3 or t.shape != (3 * h, 4 * h, 3) or h < 1:
+                raise ValueError("a skybox is a float32 array [3 h, 4 h, 3]")
+            p.skybox[k] = t.ctypes.data_as(C.POINTER(C.c_float))
+            p.skybox_h[k] = h
+            keep.append(t)
+        p._keep = keep  # keep the arrays alive with the struct
         return p
 
     def render_raw(self, scene: abi.Scene, cams, params: abi.RenderParams, outputs: abi.Outputs) -> None:

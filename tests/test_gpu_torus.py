@@ -262,3 +262,33 @@ def test_wormhole_parity(renderer, oracle, integrator, precision):
         assert abs(g["steps"].sum() / ref["steps"].sum() - 1) < 1e-3
     else:
         assert np.mean(d < 1e-3) >= 0.99, (np.mean(d < 1e-3), d.max())
+
+
+@pytest.mark.parametrize("precision", [abi.PREC_FP64, abi.PREC_MIXED])
+def test_wormhole_skybox_matches_oracle(renderer, oracle, precision):
+    """The wormhole's skybox lookup as a device epilogue (skybox_handling!
+    without ray bundles) with two synthetic cross-layout cube maps (the
+    reference's PNG textures are not in its repository): spectra against the
+    oracle's lookup of the same maps. FP64: every pixel within 1e-6; FP32-
+    mixed: >= 95 % within 1e-3 (the FP32-stage geodesics end up to ~1e-3 rad
+    from the FP64 directions, so with 16-texel faces (~0.1 rad texels) a few %
+    of the rays take a neighbouring texel: 3.1 % here)."""
+    rng = np.random.default_rng(3)
+    H = 16
+    sky = tuple(rng.uniform(0, 1, (3 * H, 4 * H, 3)).astype(np.float32) for _ in range(2))
+    sc = configs.wormhole_scene()
+    cam = configs.wormhole_camera(32, 1e-6)
+    col = np.array([467.0, 532.0, 630.0])  # the lines of the RGB -> spectrum scheme
+    ref = oracle.render(sc, cam, col, integrator=abi.DP45_FSAL, skybox=sky)
+    g = renderer.render(sc, [cam], col, want=("class", "spectrum", "xyz"), precision=precision,
+                        integrator=abi.DP45_FSAL, skybox=sky)
+    assert np.all(ref["spectrum"] > 0)
+    e = np.abs(g["spectrum"].astype(np.float64) - ref["spectrum"]) / ref["spectrum"]
+    if precision == abi.PREC_FP64:
+        assert e.max() < 1e-6, e.max()
+    else:
+        assert np.mean(np.all(e <= 1e-3, axis=1)) >= 0.95, np.mean(np.all(e <= 1e-3, axis=1))
+    assert np.all(g["xyz"][:, 1] > 0)
+    # without the maps the wormhole is dark
+    dark = renderer.render(sc, [cam], col, want=("spectrum",), precision=precision, integrator=abi.DP45_FSAL)
+    assert np.all(dark["spectrum"] == 0)
