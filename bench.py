@@ -156,13 +156,14 @@ def cpu_sample_ids(P, n):
     return np.unique(np.linspace(0, P - 1, n).round().astype(np.int64))
 
 
-def cpu_time(scene, cam, colors, n, threads=0, keep=False):
+def cpu_time(scene, cam, colors, n, threads=0, keep=False, skybox=(None, None)):
     from oracle import oracle as O
     O.build()
     P = cam.x_pix * cam.y_pix
     ids = cpu_sample_ids(P, n)
     t = time.perf_counter()
-    res = O.render(scene, cam, colors, pixel_ids=ids, threads=threads, want=("xyz", "class", "steps", "state"))
+    res = O.render(scene, cam, colors, pixel_ids=ids, threads=threads, want=("xyz", "class", "steps", "state"),
+                   skybox=skybox)
     dt = time.perf_counter() - t
     cores = threads if threads > 0 else (os.cpu_count() or 1)
     if keep:
@@ -323,7 +324,9 @@ def scenes_leg(r, rank, cpu=True):
     per-bin kernels, each at 1024 px wide with the reference's default field
     of view and colours (400/550/700 nm), tolerance 1e-6: Powehi ("m87": Kerr
     a = 0.9, disk + jet) and Synchro_Test ("synch": flat Cartesian space,
-    camera inside the cylinder). FP32-mixed and FP64, the reference's step.
+    camera inside the cylinder), and the Dneg wormhole ("wormhole", two
+    synthetic 64-texel cube maps from numpy default_rng(0) standing in for the
+    reference's missing skybox PNGs). FP32-mixed and FP64, the reference's step.
     Device time of the kernel (1 warm-up + 3 timed renders, mean); on rank 0
     the FP64 oracle on 4096 evenly spaced pixels on all host cores gives the
     CPU rate and a parity sample (linear Y within 1e-3)."""
@@ -335,23 +338,26 @@ def scenes_leg(r, rank, cpu=True):
 
     col = np.array([400.0, 550.0, 700.0])
     out = {}
-    for name, sc, camf in (("m87_powehi", configs.powehi_scene(), configs.powehi_camera),
-                           ("synch_synchro_test", configs.synchro_scene(), configs.synchro_camera)):
+    rng = np.random.default_rng(0)
+    sky = tuple(rng.uniform(0, 1, (3 * 64, 4 * 64, 3)).astype(np.float32) for _ in range(2))
+    for name, sc, camf, kw in (("m87_powehi", configs.powehi_scene(), configs.powehi_camera, {}),
+                               ("synch_synchro_test", configs.synchro_scene(), configs.synchro_camera, {}),
+                               ("wormhole", configs.wormhole_scene(), configs.wormhole_camera, {"skybox": sky})):
         cam = camf(1024, 1e-6)
         P = cam.x_pix * cam.y_pix
         leg = {"workload": f"{name} {cam.x_pix}x{cam.y_pix}, 3 bins 400/550/700 nm, tol 1e-6, reference step"}
         for pname, prec in (("mixed", abi.PREC_MIXED), ("fp64", abi.PREC_FP64)):
-            r.render(sc, [cam], col, want=("xyz",), precision=prec, integrator=abi.DP45_REF_COMPAT)
+            r.render(sc, [cam], col, want=("xyz",), precision=prec, integrator=abi.DP45_REF_COMPAT, **kw)
             ms = []
             for _ in range(3):
-                g = r.render(sc, [cam], col, want=("xyz",), precision=prec, integrator=abi.DP45_REF_COMPAT)
+                g = r.render(sc, [cam], col, want=("xyz",), precision=prec, integrator=abi.DP45_REF_COMPAT, **kw)
                 ms.append(r.stats()["kernel_ms"])
             t = float(np.mean(ms))
             leg[pname] = {"Mrays_s": P / t / 1e3, "ms": t, "step_attempts": r.stats()["step_attempts"]}
             if pname == "mixed":
                 gx = g["xyz"]
         if cpu and rank == 0:
-            v, n, dt, cores, ref = cpu_time(sc, cam, col, 4096, keep=True)
+            v, n, dt, cores, ref = cpu_time(sc, cam, col, 4096, keep=True, skybox=kw.get("skybox", (None, None)))
             ids = cpu_sample_ids(P, 4096)
             e = rel_err(gx[ids, 1], ref["xyz"][:, 1])
             leg["cpu_oracle"] = {"Mrays_s": v, "pixels": n, "s": dt, "cores": cores}
