@@ -397,8 +397,11 @@ typedef struct rtw_adjoint_result {
     double loss;
     double grad[RTW_ADJOINT_PARAMS];  /* dL/d(a, inclination, n_e0, b_0, theta_e0) */
     double forward_ms;          /* recording forward pass (image, step sizes, checkpoints) */
-    double record_ms;           /* second recording pass of the rays with a polar escape whose
-                                   gradient is wanted (state before every event); 0 if none */
+    double record_ms;           /* between the first recording pass and the reverse sweep: the
+                                   pass of rays that outgrew their region, the host scan and
+                                   queue order, and the second recording pass of the rays with
+                                   a polar escape whose gradient is wanted (state before every
+                                   event) */
     double reverse_ms;          /* reverse sweep */
     double total_ms;            /* the whole call, device time */
     uint64_t events;            /* recorded steps: accepted DP45 steps + polar escapes */
