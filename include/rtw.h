@@ -203,7 +203,9 @@ typedef struct rtw_render_params {
                                    `colors`); host memory */
     double max_dt_scale;        /* reference max_dt_scale (default 0.1) */
     int32_t integrator;         /* rtw_integrator */
-    int32_t ray_bundles;        /* must be 0 (bundles are not built) */
+    int32_t ray_bundles;        /* 1: Gaussian ray-bundle lookup of the wormhole's
+                                   skyboxes (RTW_SCENE_WORMHOLE only; other scenes
+                                   return RTW_ERR_UNSUPPORTED) */
     double promote_dr;          /* MIXED: FP64 stages while r - r_horizon < promote_dr M
                                    (0: default 1e-3; < 0: never) */
     double promote_sin;         /* MIXED: FP64 stages while sin(theta) < promote_sin
@@ -234,8 +236,10 @@ typedef struct rtw_render_params {
        x 4 h columns of (R, G, B) float32 in [0, 1], row 0 at the top (the
        PNGs the reference loads in load_textures; NULL: no skybox). Host
        memory. A ray that ends beyond r(l) = 50 adds the texel it points at,
-       as the reference's skybox_handling! without ray bundles does
-       (Wormhole.source/source_model.jl:150-443). */
+       as the reference's skybox_handling! without ray bundles does, or, with
+       ray_bundles = 1, the texels within a Gaussian footprint of the pixel's
+       ray bundle (up to 21 x 21 texels, across face edges), as its
+       calc_skybox_I_nu_beam! does (Wormhole.source/source_model.jl:150-443). */
     const float* skybox[2];
     int32_t skybox_h[2];
 } rtw_render_params;
@@ -432,6 +436,12 @@ rtw_status rtw_torus_rhs(const rtw_scene* scene, const double* colors_nm, int32_
  * pbar[5] = (d slope / d(a, -, n_e0, b_0, theta_e0))^T cot (pbar[1] = 0). */
 rtw_status rtw_torus_vjp(const rtw_scene* scene, const double* colors_nm, int32_t n_colors,
                          const double* state, const double* cot, double* mu, double* pbar);
+
+/* Host evaluation of the wormhole skybox's cube-map neighbour rule (cube_wrap,
+ * gen_geometry.jl:128-344), the one the ray-bundle lookup uses: texel (i, j)
+ * of face `face` (1-based, n texels per face edge) moved by x along i and y
+ * along j; out[3] = (i, j, face) after the move. For tests. */
+rtw_status rtw_skybox_wrap(int32_t i, int32_t j, int32_t face, int32_t x, int32_t y, int32_t n, int32_t* out);
 
 /* Host FP64 reverse of one FSAL Dormand-Prince step of size h from state of
  * the torus (reference layout): mu = the cotangent of the start state given

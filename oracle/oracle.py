@@ -55,6 +55,10 @@ def load() -> C.CDLL:
         lib.oracle_render.restype = C.c_int
         lib.oracle_set_skybox.argtypes = [C.c_int, C.POINTER(C.c_float), C.c_int]
         lib.oracle_set_skybox.restype = C.c_int
+        lib.oracle_set_ray_bundles.argtypes = [C.c_int]
+        lib.oracle_set_ray_bundles.restype = C.c_int
+        lib.oracle_cube_wrap.argtypes = [C.c_int] * 6 + [C.POINTER(C.c_int)]
+        lib.oracle_cube_wrap.restype = C.c_int
         _lib = lib
     return _lib
 
@@ -114,10 +118,11 @@ def pad_max_dt(scene, x, scale):
 
 
 def render(scene, cam, colors_nm, *, max_dt_scale=0.1, integrator=0, pixel_ids=None, threads=0,
-           want=("xyz", "class", "steps", "spectrum", "tau", "state"), skybox=(None, None)):
+           want=("xyz", "class", "steps", "spectrum", "tau", "state"), skybox=(None, None), ray_bundles=False):
     """Traces one camera (or the pixel subset `pixel_ids`) with the FP64 oracle.
     Returns a dict of arrays indexed like the pixel list, plus 'counters'
-    (step attempts, rejected attempts, polar Euler sub-steps)."""
+    (step attempts, rejected attempts, polar Euler sub-steps). ray_bundles:
+    the Gaussian ray-bundle lookup of the wormhole's skyboxes."""
     from rtwca_b200 import abi
     cam = abi.Camera.from_buffer_copy(cam)
     cam.y_pix = abi.y_pixels(cam.x_pix, cam.fov_hor, cam.fov_vert)
@@ -146,6 +151,7 @@ def render(scene, cam, colors_nm, *, max_dt_scale=0.1, integrator=0, pixel_ids=N
     for k, t in enumerate(texs):
         load().oracle_set_skybox(k, t.ctypes.data_as(C.POINTER(C.c_float)) if t is not None else None,
                                  t.shape[0] // 3 if t is not None else 0)
+    load().oracle_set_ray_bundles(int(bool(ray_bundles)))
     try:
         st = load().oracle_render(
             C.byref(scene), C.byref(cam), _dp(c), N, float(max_dt_scale), int(integrator),
@@ -156,9 +162,20 @@ def render(scene, cam, colors_nm, *, max_dt_scale=0.1, integrator=0, pixel_ids=N
     finally:
         for k in range(2):
             load().oracle_set_skybox(k, None, 0)
+        load().oracle_set_ray_bundles(0)
     if st != 0:
         raise RuntimeError(f"oracle_render failed with status {st}")
     res = {k: v for k, v in res.items() if v is not None}
     res["counters"] = counters
     res["y_pix"] = cam.y_pix
     return res
+
+
+def cube_wrap(i, j, face, x, y, n):
+    """The oracle's cube_wrap (gen_geometry.jl:128-344): (i, j, face) after
+    moving texel (i, j) of `face` by x along i and y along j, n texels a face."""
+    out = (C.c_int * 3)()
+    st = load().oracle_cube_wrap(int(i), int(j), int(face), int(x), int(y), int(n), out)
+    if st != 0:
+        raise RuntimeError(f"oracle_cube_wrap failed with status {st}")
+    return tuple(out)

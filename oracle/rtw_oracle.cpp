@@ -55,6 +55,7 @@
 #include "../include/rtw.h"
 
 #include <cmath>
+#include <complex>
 #include <cstdint>
 #include <cstring>
 #include <vector>
@@ -1009,6 +1010,7 @@ struct CameraGeom {
     int xp = 0, yp = 0;
     double W = 0, H = 0, rh = 0, rv = 0;
     Mat4 M;  // e * R2 * L * R
+    double B3[3][3];  // R2[2:4,2:4] * L[2:4,2:4] * R[2:4,2:4] (ray bundles)
 };
 
 bool camera_geom(const OScene& sc, const rtw_camera& cam, CameraGeom& cg) {
@@ -1027,7 +1029,79 @@ bool camera_geom(const OScene& sc, const rtw_camera& cam, CameraGeom& cg) {
     matmul(e, R2, t1);
     matmul(t1, L, t2);
     matmul(t2, R, cg.M);
+    double RL[3][3];
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) {
+            RL[a][b] = 0;
+            for (int c = 0; c < 3; ++c) RL[a][b] += R2[1 + a][1 + c] * L[1 + c][1 + b];
+        }
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) {
+            cg.B3[a][b] = 0;
+            for (int c = 0; c < 3; ++c) cg.B3[a][b] += RL[a][c] * R[1 + c][1 + b];
+        }
     return true;
+}
+
+// The ray-bundle components of pixel (i, j), 0-based, as initialize_camera
+// sets them (initialization.jl:198-204, 244-249, 262-324), in the order
+// b = (chi, du, dv, dg, dh, size): the shape parameters u, v, g, h, chi and
+// dchi start at 0, the rates of u, v, g, h come from the bundle's major axis
+// J = n x d (d = (0, 0, -1); (0, -1, 0) if |J|^2 < 1e-3) and the basis (a, b)
+// normal to the ray, both after R2 L R, and the size is |beamscale n_z| with
+// beamscale = atan(rho_hor) / 2. Their slopes are zero (integrators_LttM.jl:
+// 43-46), so these are also their values at the ray's end.
+void camera_bundle(const CameraGeom& cg, int i, int j, double* bo) {
+    const double w = cg.rh * ((i + 1) - 0.5) - cg.W;
+    const double h = cg.rv * ((j + 1) - 0.5) - cg.H;
+    const double th = std::atan(std::sqrt(w * w + h * h));
+    double ph;
+    if (w > 0) ph = std::atan(h / w);
+    else if (w < 0 && h >= 0) ph = std::atan(h / w) + kPi;
+    else if (w < 0 && h < 0) ph = std::atan(h / w) - kPi;
+    else if (w == 0 && h > 0) ph = kPi / 2;
+    else if (w == 0 && h < 0) ph = -kPi / 2;
+    else ph = 0;
+    double n[3] = {-std::sin(th) * std::cos(ph), -std::sin(th) * std::sin(ph), -std::cos(th)};
+    const double beamscale = std::atan(cg.rh) / 2;
+    const double size = std::fabs(beamscale * n[2]);
+    const double d[3] = {0.0, 0.0, -1.0};
+    const double E = 1.0 / (std::fabs(n[2]) + kNoDivZero);
+    double J[3] = {n[1] * d[2] - n[2] * d[1], n[2] * d[0] - n[0] * d[2], n[0] * d[1] - n[1] * d[0]};
+    if (J[0] * J[0] + J[1] * J[1] + J[2] * J[2] < 1e-3) {
+        J[0] = 0.0; J[1] = -1.0; J[2] = 0.0;
+    }
+    double J2[3], n2[3];
+    for (int a = 0; a < 3; ++a) {
+        J2[a] = cg.B3[a][0] * J[0] + cg.B3[a][1] * J[1] + cg.B3[a][2] * J[2];
+        n2[a] = cg.B3[a][0] * n[0] + cg.B3[a][1] * n[1] + cg.B3[a][2] * n[2];
+    }
+    const double jj = std::sqrt(J2[0] * J2[0] + J2[1] * J2[1] + J2[2] * J2[2]);
+    const double nn = std::sqrt(n2[0] * n2[0] + n2[1] * n2[1] + n2[2] * n2[2]);
+    for (int a = 0; a < 3; ++a) {
+        J2[a] = J2[a] / jj;
+        n2[a] = n2[a] / nn;
+    }
+    double av[3], bv[3];
+    if (!(std::fabs(1 - n2[0]) < 1e-3)) {
+        av[0] = n2[1]; av[1] = 1 - n2[1] * n2[1] / (1 - n2[0]); av[2] = -n2[1] * n2[2] / (1 - n2[0]);
+        const double aa = av[0] * av[0] + av[1] * av[1] + av[2] * av[2];
+        for (double& v : av) v = v / aa;
+        bv[0] = n2[2]; bv[1] = -n2[1] * n2[2] / (1 - n2[0]); bv[2] = 1 - n2[2] * n2[2] / (1 - n2[0]);
+        const double bb = bv[0] * bv[0] + bv[1] * bv[1] + bv[2] * bv[2];
+        for (double& v : bv) v = v / bb;
+    } else {
+        av[0] = 0.0; av[1] = -1.0; av[2] = 0.0;
+        bv[0] = 0.0; bv[1] = 0.0; bv[2] = -1.0;
+    }
+    const double aJ = av[0] * J2[0] + av[1] * J2[1] + av[2] * J2[2];
+    const double bJ = bv[0] * J2[0] + bv[1] * J2[1] + bv[2] * J2[2];
+    bo[0] = 0;
+    bo[1] = aJ * (1 + E) / 2;
+    bo[2] = bJ * (1 + E) / 2;
+    bo[3] = aJ * (1 - E) / 2;
+    bo[4] = bJ * (1 - E) / 2;
+    bo[5] = size;
 }
 
 // Initial state of pixel (i, j), 0-based (initialization.jl:213-240,327).
@@ -1095,15 +1169,124 @@ void cie_weights(const double* colors, int n, double* wx, double* wy, double* wz
 // reference's cross layout, 3h rows x 4h columns x RGB, row 0 at the top.
 static const float* g_sky[2] = {nullptr, nullptr};
 static int g_sky_h[2] = {0, 0};
+static int g_bundles = 0;
 
 inline double normal_gauss(double x, double s, double m) {  // my_special_functions.jl:20-22
     return std::exp(-(x - m) * (x - m) / (2 * s * s)) / (s * std::sqrt(2 * kPi));
 }
 
-// skybox_handling! without ray bundles (Wormhole.source/source_model.jl:393-
-// 443): calc_skybox_coord (:175-263, R_sph_to_cart gen_geometry.jl:110-122),
-// cubemap_coord_calc (gen_geometry.jl:347-370), skybox_I_nu_calc (:150-172)
-void wormhole_skybox(const OScene& sc, double* ray, int N, const double* freq) {
+// cube_wrap (gen_geometry.jl:128-344), branch by branch: face, then the
+// axis of a one-axis move, then the side it leaves by; a diagonal move is two
+// one-axis moves in the reference's order.
+void cube_wrap(int i1, int j1, int F1, int x, int y, int N, int& i2, int& j2, int& F2) {
+    auto m1 = [N](int v) { return ((v - 1) % N + N) % N + 1; };  // mod1
+    i2 = i1; j2 = j1; F2 = F1;
+    if (!(x != 0 && y != 0)) {
+        if (x != 0) {
+            const int s = i1 + x;
+            if (s >= 1 && s <= N) { i2 = s; return; }
+            const bool hi = s > N;
+            switch (F1) {
+            case 1: i2 = m1(s); F2 = hi ? 2 : 4; break;
+            case 2: i2 = m1(s); F2 = hi ? 3 : 1; break;
+            case 3: i2 = m1(s); F2 = hi ? 4 : 2; break;
+            case 4: i2 = m1(s); F2 = hi ? 1 : 3; break;
+            case 5:
+                if (hi) { i2 = N - j1 + 1; j2 = m1(s); F2 = 3; }
+                else { i2 = j1; j2 = 1 - i1 - x; F2 = 1; }
+                break;
+            case 6:
+                if (hi) { i2 = j1; j2 = N - m1(s) + 1; F2 = 3; }
+                else { i2 = N - j1 + 1; j2 = N - i1 - x; F2 = 1; }
+                break;
+            }
+        } else {
+            const int t = j1 + y;
+            if (t >= 1 && t <= N) { j2 = t; return; }
+            const bool hi = t > N;
+            switch (F1) {
+            case 1:
+                if (hi) { i2 = m1(t); j2 = N + 1 - i1; F2 = 6; }
+                else { i2 = 1 - j1 - y; j2 = i1; F2 = 5; }
+                break;
+            case 2: j2 = m1(t); F2 = hi ? 6 : 5; break;
+            case 3:
+                if (hi) { i2 = N - m1(t) + 1; j2 = i1; F2 = 6; }
+                else { i2 = N + j1 + y; j2 = N - i1 + 1; F2 = 5; }
+                break;
+            case 4:
+                if (hi) { i2 = N - i1 + 1; j2 = N - m1(t) + 1; F2 = 6; }
+                else { i2 = N - i1 + 1; j2 = 1 - j1 - y; F2 = 5; }
+                break;
+            case 5:
+                if (hi) { j2 = m1(t); F2 = 2; }
+                else { i2 = N - i1 + 1; j2 = 1 - j1 - y; F2 = 4; }
+                break;
+            case 6:
+                if (hi) { i2 = N - i1 + 1; j2 = N - m1(t) + 1; F2 = 4; }
+                else { j2 = m1(t); F2 = 2; }
+                break;
+            }
+        }
+        return;
+    }
+    int ia, ja, Fa;
+    cube_wrap(i1, j1, F1, x, 0, N, ia, ja, Fa);
+    const bool lo = i1 + x < 1, hi = i1 + x > N;
+    if (F1 == 6 && lo) cube_wrap(ia, ja, Fa, -y, 0, N, i2, j2, F2);
+    else if (F1 == 6 && hi) cube_wrap(ia, ja, Fa, y, 0, N, i2, j2, F2);
+    else if (F1 == 5 && hi) cube_wrap(ia, ja, Fa, -y, 0, N, i2, j2, F2);
+    else if (F1 == 5 && lo) cube_wrap(ia, ja, Fa, y, 0, N, i2, j2, F2);
+    else cube_wrap(ia, ja, Fa, 0, y, N, i2, j2, F2);
+}
+
+void cubemap_coord(int i, int j, int F, int N, int& ia, int& ja) {  // cubemap_coord_calc
+    ia = i; ja = j;
+    if (F == 1) ja += N;
+    else if (F == 2) { ia += N; ja += N; }
+    else if (F == 3) { ia += 2 * N; ja += N; }
+    else if (F == 4) { ia += 3 * N; ja += N; }
+    else if (F == 5) ia += N;
+    else { ia += N; ja += 2 * N; }
+}
+
+// skybox_I_nu_calc (Wormhole.source/source_model.jl:150-172) at
+// cross-layout texel (i, j) of map k
+double skybox_I(int k, int i, int j, double f) {
+    const int H = g_sky_h[k];
+    const float* t = g_sky[k] + ((3LL * H - j) * 4LL * H + (i - 1)) * 3;
+    const double Rc = 1.0 * t[0], Gc = 0.843 * t[1], Bc = 0.914 * t[2];
+    return 1e-12 * (Rc * normal_gauss(f, 5e-5, 0.001587) + Gc * normal_gauss(f, 7e-5, 0.001879) +
+                    Bc * normal_gauss(f, 9e-5, 0.002141));
+}
+
+// D2_Gauss and distort_gauss (my_special_functions.jl:28-52)
+double d2_gauss(double x, double y, double sx, double sy, double t) {
+    const double c = std::cos(t), s = std::sin(t);
+    const double a = c * c / (2 * sx * sx) + s * s / (2 * sy * sy);
+    const double b = -s * c / (2 * sx * sx) + s * c / (2 * sy * sy);
+    const double cc = s * s / (2 * sx * sx) + c * c / (2 * sy * sy);
+    return 1.0 / (2 * kPi * sx * sy) * std::exp(-(a * x * x + 2 * b * x * y + cc * y * y));
+}
+
+void distort_gauss(double sx, double sy, double t, double a, double b, double& sxo, double& syo, double& to) {
+    const double c = std::cos(t), s = std::sin(t);
+    const double xx = a * a * (sx * sx * c * c + sy * sy * s * s);
+    const double yy = b * b * (sx * sx * s * s + sy * sy * c * c);
+    const double xy = a * b * (sx * sx - sy * sy) * std::sin(2 * t) / 2;
+    const double r = std::sqrt((xx - yy) * (xx - yy) + 4 * xy * xy);
+    sxo = std::sqrt((xx + yy + r) / 2);
+    syo = std::sqrt((xx + yy - r) / 2);
+    to = std::atan2(2 * xy, xx - yy) / 2;
+}
+
+// skybox_handling! (Wormhole.source/source_model.jl:393-443):
+// calc_skybox_coord (:175-263, R_sph_to_cart gen_geometry.jl:110-122),
+// cubemap_coord_calc (gen_geometry.jl:347-370), skybox_I_nu_calc (:150-172);
+// with a bundle b (camera_bundle's layout), calc_skybox_I_nu_beam! (:266-358).
+// Texels that wrap off the map (faces under 10 texels; the reference stops
+// with an index error) and a footprint with a NaN width add nothing.
+void wormhole_skybox(const OScene& sc, double* ray, int N, const double* freq, const double* bund) {
     const double rl = sc.wh_r(ray[1]);
     if (!(rl > 50) || ray[1] == 0) return;
     const int k = ray[1] > 0 ? 0 : 1;
@@ -1144,14 +1327,49 @@ void wormhole_skybox(const OScene& sc, double* ray, int N, const double* freq) {
     case 5: i += H; break;
     default: i += H; j += 2 * H; break;
     }
-    const float* t = g_sky[k] + ((3LL * H - j) * 4LL * H + (i - 1)) * 3;
-    const double Rc = 1.0 * t[0], Gc = 0.843 * t[1], Bc = 0.914 * t[2];
     const double fs = ray[4];  // -g(u, k) with u = (1, 0, 0, 0), g_tt = -1
+    if (bund) {
+        // face-local (i, j): undo the cross offsets taken above
+        int il = (int)i, jl = (int)j;
+        switch (face) {
+        case 1: jl -= H; break;
+        case 2: il -= H; jl -= H; break;
+        case 3: il -= 2 * H; jl -= H; break;
+        case 4: il -= 3 * H; jl -= H; break;
+        case 5: il -= H; break;
+        default: il -= H; jl -= 2 * H; break;
+        }
+        const double dprime = bund[5] * fs;
+        const double A = std::sqrt(bund[1] * bund[1] + bund[2] * bund[2]);
+        const double B = std::sqrt(bund[3] * bund[3] + bund[4] * bund[4]);
+        const double dmaj = dprime * (A + B), dmin = dprime * (A - B);
+        const double mu = bund[0] + std::arg(std::complex<double>(bund[1], bund[2]) *
+                                             std::complex<double>(bund[3], bund[4])) / 2;
+        const double sky_beamscale = std::atan(2.0 / (H + 1)) / 2;
+        double sx, sy, tn;
+        distort_gauss(dmaj, dmin, mu, 1.0 / (sky_beamscale + kNoDivZero), 1.0 / (sky_beamscale + kNoDivZero), sx, sy,
+                      tn);
+        if (!(sx > 0 && sy > 0 && std::isfinite(sx) && std::isfinite(sy))) return;
+        const int hw = (int)std::min(std::ceil(std::max(sx, sy)), 10.0);
+        std::vector<double> In(N, 0.0);
+        for (int kk = -hw; kk <= hw; ++kk)
+            for (int ll = -hw; ll <= hw; ++ll) {
+                int iw, jw, Fw, ia, ja;
+                cube_wrap(il, jl, face, kk, ll, H, iw, jw, Fw);
+                cubemap_coord(iw, jw, Fw, H, ia, ja);
+                if (ia < 1 || ia > 4 * H || ja < 1 || ja > 3 * H) continue;
+                for (int c = 0; c < N; ++c) {
+                    const double f = freq[c] * fs;
+                    In[c] += d2_gauss(kk, ll, sx, sy, tn) * skybox_I(k, ia, ja, f) * std::exp(-ray[9 + 2 * c]) /
+                             (f * f * f);
+                }
+            }
+        for (int c = 0; c < N; ++c) ray[8 + 2 * c] += In[c];
+        return;
+    }
     for (int c = 0; c < N; ++c) {
         const double f = freq[c] * fs;
-        const double I = 1e-12 * (Rc * normal_gauss(f, 5e-5, 0.001587) + Gc * normal_gauss(f, 7e-5, 0.001879) +
-                                  Bc * normal_gauss(f, 9e-5, 0.002141));
-        ray[8 + 2 * c] += I * std::exp(-ray[9 + 2 * c]) / (f * f * f);
+        ray[8 + 2 * c] += skybox_I(k, (int)i, (int)j, f) * std::exp(-ray[9 + 2 * c]) / (f * f * f);
     }
 }
 
@@ -1159,6 +1377,17 @@ extern "C" {
 
 // the wormhole's skybox k (0: positive-l side, 1: negative), h pixels per
 // face edge (tex NULL: none); kept until changed
+int oracle_set_ray_bundles(int on) {  // gen_image's ray_bundles; kept until changed
+    g_bundles = on ? 1 : 0;
+    return RTW_OK;
+}
+
+int oracle_cube_wrap(int i, int j, int face, int x, int y, int n, int* out) {
+    if (!out || n < 1 || face < 1 || face > 6) return RTW_ERR_INVALID_PARAM;
+    cube_wrap(i, j, face, x, y, n, out[0], out[1], out[2]);
+    return RTW_OK;
+}
+
 int oracle_set_skybox(int k, const float* tex, int h) {
     if (k < 0 || k > 1 || (tex && h < 1)) return RTW_ERR_INVALID_PARAM;
     g_sky[k] = tex;
@@ -1280,7 +1509,11 @@ int oracle_render(const rtw_scene* scene, rtw_camera* cam, const double* colors_
             }
             for (int k = 0; k < 8; ++k)
                 if (!std::isfinite(ray[k])) klass = RTW_CLASS_NAN;
-            if (sc.is_wh()) wormhole_skybox(sc, ray.data(), N, freq.data());
+            if (sc.is_wh()) {
+                double bund[6];
+                if (g_bundles) camera_bundle(cg, i, j, bund);
+                wormhole_skybox(sc, ray.data(), N, freq.data(), g_bundles ? bund : nullptr);
+            }
             tot_steps += step_count;
             tot_esc += esc;
             if (cls) cls[q] = (unsigned char)klass;

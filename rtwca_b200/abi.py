@@ -165,6 +165,7 @@ SIGNATURES = {
                                 C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "rtw_torus_vjp": (C.c_int, [C.POINTER(Scene), C.POINTER(C.c_double), C.c_int32, C.POINTER(C.c_double),
                                 C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "rtw_skybox_wrap": (C.c_int, [C.c_int32] * 6 + [C.POINTER(C.c_int32)]),
     "rtw_torus_step_vjp": (C.c_int, [C.POINTER(Scene), C.POINTER(C.c_double), C.c_int32, C.POINTER(C.c_double),
                                      C.c_double, C.POINTER(C.c_double), C.c_int32, C.POINTER(C.c_double),
                                      C.POINTER(C.c_double), C.POINTER(C.c_double)]),

@@ -220,6 +220,28 @@ void make_dev_scene(const rtw_scene& scene, DevScene& d) {
     d.r_pm = is_kerr(scene.kind) ? 2 * std::sqrt(scene.mass * scene.mass - scene.spin * scene.spin) : 0.0;
 }
 
+// Spatial blocks of the camera's R2, L and R multiplied, R2[2:4,2:4] *
+// L[2:4,2:4] * R[2:4,2:4] (initialization.jl:273-275): what takes a ray
+// bundle's axis and direction from the canvas to the observer's frame.
+void bundle_basis(const rtw_camera& cam, double m3[9]) {
+    M4 R, L, R2;
+    rot_intrinsic(cam.pointing, R);
+    boost(-cam.speed, L);
+    rot_final(cam.direction, R2);
+    double t[3][3];
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) {
+            t[a][b] = 0;
+            for (int c = 0; c < 3; ++c) t[a][b] += R2[1 + a][1 + c] * L[1 + c][1 + b];
+        }
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) {
+            double v = 0;
+            for (int c = 0; c < 3; ++c) v += t[a][c] * R[1 + c][1 + b];
+            m3[3 * a + b] = v;
+        }
+}
+
 }  // namespace rtw
 
 using namespace rtw;
@@ -544,7 +566,8 @@ rtw_status rtw_render(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* ca
     if (n_cams <= 0 || n_cams > RTW_MAX_FRAMES) return fail(ctx, RTW_ERR_INVALID_PARAM, "n_cams out of range");
     if (prm->n_colors <= 0 || prm->n_colors > RTW_MAX_BINS || !prm->colors_nm)
         return fail(ctx, RTW_ERR_INVALID_PARAM, "n_colors must be 1..128 with colors_nm set");
-    if (prm->ray_bundles) return fail(ctx, RTW_ERR_UNSUPPORTED, "ray bundles are not built");
+    if (prm->ray_bundles && scene->kind != RTW_SCENE_WORMHOLE)
+        return fail(ctx, RTW_ERR_UNSUPPORTED, "ray bundles are built for the wormhole scene only");
     if (scene->kind == RTW_SCENE_KERR_SYNCHRO_TORUS || scene->kind == RTW_SCENE_KERR_POWEHI ||
         scene->kind == RTW_SCENE_SYNCHRO_TEST || scene->kind == RTW_SCENE_WORMHOLE)
         return torus_render(ctx, scene, cams, n_cams, prm, out);

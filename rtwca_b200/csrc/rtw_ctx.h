@@ -83,6 +83,9 @@ inline rtw_status ensure(rtw_ctx* ctx, void** ptr, size_t* cap, size_t need) {
 }
 
 
+// Spatial R2 L R of a camera, row-major (rtw_capi.cu).
+void bundle_basis(const rtw_camera& cam, double m3[9]);
+
 // rtw_render of a RTW_SCENE_KERR_SYNCHRO_TORUS scene (rtw_torus.cu).
 rtw_status torus_render(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* cams, int32_t n_cams,
                         const rtw_render_params* prm, rtw_outputs* out);

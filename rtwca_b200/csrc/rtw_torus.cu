@@ -270,6 +270,8 @@ struct TorusKP {
     double* final_state;  // [P][8] (may be null)
     const float* sky[2];  // the wormhole's skyboxes (cross-layout cube maps) or null
     int sky_h[2];         // pixels per face edge
+    int bundles;          // 1: Gaussian ray-bundle lookup of the skyboxes
+    double bundle_m[9];   // row-major R2 L R of the camera, spatial blocks (initialization.jl:273-275)
     uint8_t* cls;
     uint32_t* steps;
     const uint32_t* ray_list;          // [total_rays] indices into the subset (dense re-record) or null
@@ -361,20 +363,98 @@ __device__ __noinline__ void torus_geo_stages_fp64(const TorusModel& m, const do
     torus_geo_stages<double, K, EM>(m, x, k1, h, *o);
 }
 
-// skybox_handling! without ray bundles (Wormhole.source/source_model.jl:393-
-// 443) at a ray's end x: beyond r(l) = 50 the ray takes the texel of the
-// skybox on its side of the throat that its direction points at
-// (calc_skybox_coord :175-263 with R_sph_to_cart, gen_geometry.jl:110-122;
-// cubemap_coord_calc, gen_geometry.jl:347-370) and adds, per bin, the
-// texel's spectrum (skybox_I_nu_calc :150-172: three Gaussian lines for R, G,
-// B) x exp(-tau) / f^3 at f = nu_c k^t.
-__device__ void wormhole_skybox(const TorusKP& p, const double* x, int N, double* I, const double* tau) {
+// The ray bundle of pixel (pi, pj) of the frame's window (initialization.jl:
+// 198-204, 241-249, 262-325): its size |beamscale cos theta| (beamscale =
+// atan(rho_hor) / 2) and the rates (du, dv, dg, dh) = (a.J (1 + E), b.J (1 +
+// E), a.J (1 - E), b.J (1 - E)) / 2 of its shape, with E = 1 / (|n_z| +
+// no_div_zero), J = n x (0, 0, -1) (or (0, -1, 0) when that is short) and n
+// the ray's direction on the canvas, both taken through R2 L R (spatial blocks)
+// and normalised, and (a, b) the basis normal to n of the reference (each
+// divided by its squared length). The reference gives the 11 bundle components
+// zero slope (integrators_LttM.jl:43-46) and leaves them out of the step's
+// error norm (:180-185), so they reach the skybox as the camera set them: the
+// bundle is a function of the pixel. Out: d[0..3] = du, dv, dg, dh; d[4] = size.
+__device__ void bundle_shape(const TorusKP& p, int pi, int pj, double* d) {
+    const FrameDesc& f = p.frame;
+    const double w = f.rh * ((f.i0 + pi + 1) - 0.5) - f.W;
+    const double hh = f.rv * ((f.j0 + pj + 1) - 0.5) - f.H;
+    const double th = atan(sqrt(w * w + hh * hh));
+    double ph;
+    if (w > 0) ph = atan(hh / w);
+    else if (w < 0 && hh >= 0) ph = atan(hh / w) + kPi;
+    else if (w < 0 && hh < 0) ph = atan(hh / w) - kPi;
+    else if (w == 0 && hh > 0) ph = kPi / 2;
+    else if (w == 0 && hh < 0) ph = -kPi / 2;
+    else ph = 0;
+    double st, ct, sp, cp;
+    sincos(th, &st, &ct);
+    sincos(ph, &sp, &cp);
+    double n[3] = {-st * cp, -st * sp, -ct};
+    d[4] = fabs(atan(f.rh) / 2 * n[2]);
+    const double E = 1.0 / (fabs(n[2]) + 1e-24);
+    double J[3] = {-n[1], n[0], 0.0};
+    if (J[0] * J[0] + J[1] * J[1] + J[2] * J[2] < 1e-3) {
+        J[0] = 0;
+        J[1] = -1;
+        J[2] = 0;
+    }
+    double Jr[3], nr[3];
+    for (int r = 0; r < 3; ++r) {
+        Jr[r] = p.bundle_m[3 * r] * J[0] + p.bundle_m[3 * r + 1] * J[1] + p.bundle_m[3 * r + 2] * J[2];
+        nr[r] = p.bundle_m[3 * r] * n[0] + p.bundle_m[3 * r + 1] * n[1] + p.bundle_m[3 * r + 2] * n[2];
+    }
+    const double jn = sqrt(Jr[0] * Jr[0] + Jr[1] * Jr[1] + Jr[2] * Jr[2]);
+    const double nn = sqrt(nr[0] * nr[0] + nr[1] * nr[1] + nr[2] * nr[2]);
+    for (int r = 0; r < 3; ++r) {
+        Jr[r] /= jn;
+        nr[r] /= nn;
+    }
+    double A[3], B[3];
+    if (!(fabs(1 - nr[0]) < 1e-3)) {
+        const double q = 1 - nr[0];
+        A[0] = nr[1]; A[1] = 1 - nr[1] * nr[1] / q; A[2] = -nr[1] * nr[2] / q;
+        B[0] = nr[2]; B[1] = -nr[1] * nr[2] / q; B[2] = 1 - nr[2] * nr[2] / q;
+        const double aa = A[0] * A[0] + A[1] * A[1] + A[2] * A[2], bb = B[0] * B[0] + B[1] * B[1] + B[2] * B[2];
+        for (int r = 0; r < 3; ++r) {
+            A[r] /= aa;
+            B[r] /= bb;
+        }
+    } else {
+        A[0] = 0; A[1] = -1; A[2] = 0;
+        B[0] = 0; B[1] = 0; B[2] = -1;
+    }
+    const double aJ = A[0] * Jr[0] + A[1] * Jr[1] + A[2] * Jr[2];
+    const double bJ = B[0] * Jr[0] + B[1] * Jr[1] + B[2] * Jr[2];
+    d[0] = aJ * (1 + E) / 2;
+    d[1] = bJ * (1 + E) / 2;
+    d[2] = aJ * (1 - E) / 2;
+    d[3] = bJ * (1 - E) / 2;
+}
+
+// skybox_handling! (Wormhole.source/source_model.jl:393-443) at a ray's end
+// x: beyond r(l) = 50 the ray looks up the skybox on its side of the throat
+// in the direction it points (calc_skybox_coord :175-263 with R_sph_to_cart,
+// gen_geometry.jl:110-122) and adds, per bin, the spectrum of the texel
+// colours (skybox_I_nu_calc :150-172: three Gaussian lines for R, G, B) x
+// exp(-tau) / f^3 at f = nu_c k^t. Without ray bundles the colours are those
+// of the texel hit (cubemap_coord_calc); with them (calc_skybox_I_nu_beam!
+// :266-358) a Gaussian footprint weighs the texels within h <= 10 of it
+// across face edges: the pixel's bundle, scaled by k^t, as major/minor axes
+// and orientation (distort_gauss, my_special_functions.jl:40-52, by the
+// inverse texel size atan(2 / (h_sky + 1)) / 2 on both axes), D2_Gauss
+// (:28-34) as the weight of texel offset (k, l). The spectrum is linear in
+// the colours, so the weighted colours are summed first and the bins take one
+// spectrum: the reference's sum, reassociated. Texels whose wrapped
+// coordinates fall off the map (maps under 10 texels a face: the reference
+// stops with an index error there) are skipped.
+__device__ void wormhole_skybox(const TorusKP& p, const double* x, int N, double* I, const double* tau, int pi,
+                                int pj) {
     const WormholeDev& W = p.m.wh;
     const double rl = wormhole_r<double>(W, x[1]);
     if (!(rl > 50) || x[1] == 0) return;
     const int k = x[1] > 0 ? 0 : 1;
     if (!p.sky[k]) return;
-    const long long H = p.sky_h[k];
+    const int H = p.sky_h[k];
     double st, ct, sp, cp;
     sincos(x[2], &st, &ct);
     sincos(x[3], &sp, &cp);
@@ -398,21 +478,59 @@ __device__ void wormhole_skybox(const TorusKP& p, const double* x, int N, double
     case 5: u = -X / az; v = -Y / az; break;
     default: u = -X / az; v = Y / az; break;
     }
-    long long i = (long long)floor(H * (u + 1) / 2) + 1, j = (long long)floor(H * (v + 1) / 2) + 1;
-    if (i > H) i = H;
-    if (j > H) j = H;
+    int i = (int)min((double)H, floor(H * (u + 1) / 2) + 1), j = (int)min((double)H, floor(H * (v + 1) / 2) + 1);
     if (i < 1) i = 1;  // (u, v) in [-1, 1]: rounding only
     if (j < 1) j = 1;
-    switch (face) {
-    case 1: j += H; break;
-    case 2: i += H; j += H; break;
-    case 3: i += 2 * H; j += H; break;
-    case 4: i += 3 * H; j += H; break;
-    case 5: i += H; break;
-    default: i += H; j += 2 * H; break;
+    const float* map = p.sky[k];
+    const long long H4 = 4LL * H;
+    double cr, cg, cb;  // weighted texel colours
+    if (!p.bundles) {
+        sky_cross(face, H, i, j);
+        const float* t = map + ((3LL * H - j) * H4 + (i - 1)) * 3;
+        cr = (double)t[0];
+        cg = (double)t[1];
+        cb = (double)t[2];
+    } else {
+        double d[5];
+        bundle_shape(p, pi, pj, d);
+        const double dp = d[4] * x[4];
+        const double ra = sqrt(d[0] * d[0] + d[1] * d[1]), rb = sqrt(d[2] * d[2] + d[3] * d[3]);
+        const double dmaj = dp * (ra + rb), dmin = dp * (ra - rb);
+        const double mu = atan2(d[0] * d[3] + d[1] * d[2], d[0] * d[2] - d[1] * d[3]) / 2;
+        const double sc = 1.0 / (atan(2.0 / (H + 1)) / 2 + 1e-24);
+        double sm, cm;
+        sincos(mu, &sm, &cm);
+        const double sxx = sc * sc * (dmaj * dmaj * cm * cm + dmin * dmin * sm * sm);
+        const double syy = sc * sc * (dmaj * dmaj * sm * sm + dmin * dmin * cm * cm);
+        const double sxy = sc * sc * (dmaj * dmaj - dmin * dmin) * sin(2 * mu) / 2;
+        const double root = sqrt((sxx - syy) * (sxx - syy) + 4 * sxy * sxy);
+        const double sx = sqrt((sxx + syy + root) / 2), sy = sqrt((sxx + syy - root) / 2);
+        const double tn = atan2(2 * sxy, sxx - syy) / 2;
+        // a footprint the reference cannot form (a NaN width, where it stops
+        // with an error) adds nothing
+        if (!(sx > 0 && sy > 0 && isfinite(sx) && isfinite(sy))) return;
+        const int hw = (int)min(10.0, ceil(fmax(sx, sy)));
+        double stn, ctn;
+        sincos(tn, &stn, &ctn);
+        const double ga = ctn * ctn / (2 * sx * sx) + stn * stn / (2 * sy * sy);
+        const double gb = -stn * ctn / (2 * sx * sx) + stn * ctn / (2 * sy * sy);
+        const double gc = stn * stn / (2 * sx * sx) + ctn * ctn / (2 * sy * sy);
+        const double gn = 1.0 / (2 * kPi * sx * sy);
+        cr = cg = cb = 0;
+        for (int kk = -hw; kk <= hw; ++kk)
+            for (int ll = -hw; ll <= hw; ++ll) {
+                int i2 = i, j2 = j, F2 = face;
+                sky_wrap(i2, j2, F2, kk, ll, H);
+                sky_cross(F2, H, i2, j2);
+                if (i2 < 1 || i2 > 4 * H || j2 < 1 || j2 > 3 * H) continue;
+                const double wgt = gn * exp(-(ga * kk * kk + 2 * gb * kk * ll + gc * ll * ll));
+                const float* t = map + ((3LL * H - j2) * H4 + (i2 - 1)) * 3;
+                cr += wgt * (double)t[0];
+                cg += wgt * (double)t[1];
+                cb += wgt * (double)t[2];
+            }
     }
-    const float* t = p.sky[k] + ((3 * H - j) * 4 * H + (i - 1)) * 3;
-    const double R = 1.0 * (double)t[0], G = 0.843 * (double)t[1], B = 0.914 * (double)t[2];
+    const double R = 1.0 * cr, G = 0.843 * cg, B = 0.914 * cb;
     const double inv = 1.0 / sqrt(2 * kPi);
     for (int c = 0; c < N; ++c) {
         const double f = p.m.bins[c].nu_nm * x[4];
@@ -869,7 +987,7 @@ __global__ void __launch_bounds__(128, MIXED ? 3 : 2) torus_forward(const TorusK
                     I[c] = (double)ihi[c] + (MIXED ? (double)ilo[c] : 0.0);
                     tv[c] = (double)tau[c];
                 }
-                wormhole_skybox(p, x, N, I, tv);
+                wormhole_skybox(p, x, N, I, tv, pi, pj);
                 for (int c = 0; c < N; ++c) {
                     ihi[c] = SR(I[c]);
                     ilo[c] = MIXED ? SR(I[c] - (double)ihi[c]) : SR(0);
@@ -1591,7 +1709,11 @@ rtw_status torus_setup(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* c
         return fail(ctx, RTW_ERR_INVALID_PARAM, "precision");
     if (prm->integrator != RTW_DP45_FSAL && prm->integrator != RTW_DP45_REF_COMPAT)
         return fail(ctx, RTW_ERR_INVALID_PARAM, "integrator");
-    if (prm->ray_bundles) return fail(ctx, RTW_ERR_UNSUPPORTED, "ray bundles are not built");
+    // the bundle enters only the wormhole's skybox lookup; in every other
+    // scene the reference's bundle slots would also hold off its opacity stop
+    // (the all-slots tau test of calc_terminate), which is not built
+    if (prm->ray_bundles && scene->kind != RTW_SCENE_WORMHOLE)
+        return fail(ctx, RTW_ERR_UNSUPPORTED, "ray bundles are built for the wormhole scene only");
     if (!(prm->max_dt_scale > 0)) return fail(ctx, RTW_ERR_INVALID_PARAM, "max_dt_scale must be > 0");
     std::string why;
     TorusKP& p = run.kp;
@@ -1603,6 +1725,10 @@ rtw_status torus_setup(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* c
     if (st == RTW_ERR_INVALID_CAMERA) return fail(ctx, st, "camera is on a coordinate singularity");
     if (st != RTW_OK) return fail(ctx, st, "camera parameters invalid or non-finite");
     run.P = total;
+    if (prm->ray_bundles) {
+        p.bundles = 1;
+        bundle_basis(*cam, p.bundle_m);
+    }
     p.total_rays = total;
     p.ray0 = 0;
     p.ray_stride = 1;
@@ -2101,6 +2227,16 @@ rtw_status rtw_torus_escape_vjp(const rtw_scene* scene, const double* colors_nm,
     }
     for (int q = 0; q < kTorusParams; ++q) pbar[q] = pb[q];
     return ok ? RTW_OK : RTW_ERR_NAN;
+}
+
+rtw_status rtw_skybox_wrap(int32_t i, int32_t j, int32_t face, int32_t x, int32_t y, int32_t n, int32_t* out) {
+    if (!out || n < 1 || face < 1 || face > 6) return RTW_ERR_INVALID_PARAM;
+    int a = i, b = j, F = face;
+    sky_wrap(a, b, F, x, y, n);
+    out[0] = a;
+    out[1] = b;
+    out[2] = F;
+    return RTW_OK;
 }
 
 rtw_status rtw_torus_step_vjp(const rtw_scene* scene, const double* colors_nm, int32_t n_colors,

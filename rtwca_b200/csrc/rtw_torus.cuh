@@ -400,6 +400,109 @@ RTW_HD void wormhole_rhs(const WormholeDev& W, const T* z, T* k) {
     k[7] = B(-2) * rpr * kl * kph - B(2) * (cs / sn) * kth * kph;
 }
 
+// Cube-map neighbours (cube_wrap, gen_geometry.jl:128-344). Texel (i, j) of
+// face F, 1-based with n texels per face edge, moved by x texels along i and
+// y along j. A move that leaves the face enters the face across that edge,
+// re-oriented as the reference's table says; its formulas are kept as they
+// are, so some moves land outside [1, n] (face 6's low i edge gives j = n - s)
+// and, in cross-layout coordinates, on another region of the map, as there.
+RTW_HD int sky_mod1(int s, int n) {
+    int r = (s - 1) % n;
+    if (r < 0) r += n;
+    return r + 1;
+}
+
+RTW_HD void sky_move_i(int& i, int& j, int& F, int x, int n) {
+    const int s = i + x;
+    if (s >= 1 && s <= n) {
+        i = s;
+        return;
+    }
+    const bool hi = s > n;
+    const int m = sky_mod1(s, n);
+    switch (F) {
+    case 1: i = m; F = hi ? 2 : 4; break;
+    case 2: i = m; F = hi ? 3 : 1; break;
+    case 3: i = m; F = hi ? 4 : 2; break;
+    case 4: i = m; F = hi ? 1 : 3; break;
+    case 5:
+        if (hi) { i = n - j + 1; j = m; F = 3; }
+        else { i = j; j = 1 - s; F = 1; }
+        break;
+    case 6:
+        if (hi) { i = j; j = n - m + 1; F = 3; }
+        else { i = n - j + 1; j = n - s; F = 1; }
+        break;
+    default: break;
+    }
+}
+
+RTW_HD void sky_move_j(int& i, int& j, int& F, int y, int n) {
+    const int t = j + y;
+    if (t >= 1 && t <= n) {
+        j = t;
+        return;
+    }
+    const bool hi = t > n;
+    const int m = sky_mod1(t, n);
+    switch (F) {
+    case 1:
+        if (hi) { j = n + 1 - i; i = m; F = 6; }
+        else { j = i; i = 1 - t; F = 5; }
+        break;
+    case 2: j = m; F = hi ? 6 : 5; break;
+    case 3:
+        if (hi) { j = i; i = n - m + 1; F = 6; }
+        else { j = n - i + 1; i = n + t; F = 5; }
+        break;
+    case 4:
+        i = n - i + 1;
+        if (hi) { j = n - m + 1; F = 6; }
+        else { j = 1 - t; F = 5; }
+        break;
+    case 5:
+        if (hi) { j = m; F = 2; }
+        else { i = n - i + 1; j = 1 - t; F = 4; }
+        break;
+    case 6:
+        if (hi) { i = n - i + 1; j = n - m + 1; F = 4; }
+        else { j = m; F = 2; }
+        break;
+    default: break;
+    }
+}
+
+// A diagonal move is an i move, then a j move; on faces 5 and 6 an i move
+// that leaves the face continues as an i move on the new face (by -y or +y).
+RTW_HD void sky_wrap(int& i, int& j, int& F, int x, int y, int n) {
+    if (x == 0 || y == 0) {
+        if (x != 0) sky_move_i(i, j, F, x, n);
+        else sky_move_j(i, j, F, y, n);
+        return;
+    }
+    const int s = i + x, F0 = F;
+    sky_move_i(i, j, F, x, n);
+    if (F0 == 6 && s < 1) sky_move_i(i, j, F, -y, n);
+    else if (F0 == 6 && s > n) sky_move_i(i, j, F, y, n);
+    else if (F0 == 5 && s > n) sky_move_i(i, j, F, -y, n);
+    else if (F0 == 5 && s < 1) sky_move_i(i, j, F, y, n);
+    else sky_move_j(i, j, F, y, n);
+}
+
+// Face-local texel (i, j) of face F to cross-layout coordinates
+// (cubemap_coord_calc, gen_geometry.jl:347-370): faces 1-4 in the middle row
+// of four squares, 5 below face 2, 6 above it.
+RTW_HD void sky_cross(int F, int n, int& i, int& j) {
+    switch (F) {
+    case 1: j += n; break;
+    case 2: i += n; j += n; break;
+    case 3: i += 2 * n; j += n; break;
+    case 4: i += 3 * n; j += n; break;
+    case 5: i += n; break;
+    default: i += n; j += 2 * n; break;
+    }
+}
+
 // Slopes of one bin without exp(-tau) (as torus_bin): nu = g nu_c in nm^-1.
 // Disk: a = a_nu, j = a B_nu(T); jet: j = J0 s^-(p-1)/2, a = A0 / nu s^-(p+2)/2,
 // s = nu / (nu_cyc sin theta_B) (calc_radiative_coefficients).

@@ -10,8 +10,11 @@ same meaning and defaults, and calls librtw_b200.so through its C ABI.
 Differences, by design of the library: gen_image returns linear CIE XYZ
 [y_pix, x_pix, 3] in the reference's image orientation (the reference converts
 to xyY, normalises brightness and converts to RGB{N0f16}; ``xyz_to_srgb`` gives
-that last step as an informational helper), and ``ray_bundles=True`` raises
-RTW_ERR_UNSUPPORTED.
+that last step as an informational helper); the wormhole's skybox textures,
+which the reference loads from PNG files that its repository does not hold,
+are arrays the caller hands to ``load_textures``; and ``ray_bundles=True`` (the
+Gaussian footprint lookup of those skyboxes) is built for the wormhole, the
+one scene whose image depends on it, and raises RTW_ERR_UNSUPPORTED elsewhere.
 """
 from __future__ import annotations
 
@@ -250,6 +253,17 @@ _WORLDS = {
 
 _current: World | None = None
 _renderer: Renderer | None = None
+_textures = (None, None)
+
+
+def load_textures(skybox1=None, skybox2=None):
+    """The wormhole's two skyboxes (load_textures, Wormhole.source/
+    source_model.jl): cube maps in the reference's cross layout, float32
+    [3 h, 4 h, 3] RGB in [0, 1], row 0 at the top; skybox1 lies beyond the
+    throat's positive-l side. gen_image uses them until they are replaced."""
+    global _textures
+    _textures = (skybox1, skybox2)
+    return _textures
 
 
 def available_worlds() -> list:
@@ -305,8 +319,9 @@ def gen_image(*, camera_pos=(0, 0, 0, 0), camera_dir=(0.0, 0.0), speed=0.0, came
     prec = {"fp64": abi.PREC_FP64, "mixed": abi.PREC_MIXED, "fp64_plain": abi.PREC_FP64_PLAIN}[precision]
     integ = {"ref_compat": abi.DP45_REF_COMPAT, "fsal": abi.DP45_FSAL}[integrator]
     want = ("xyz", "class", "steps") + (("spectrum", "state", "tau") if returnrays else ())
+    sky = _textures if _current.scene.kind == abi.SCENE_WORMHOLE else (None, None)
     res = r.render(_current.scene, [cam], colors, want=want, precision=prec, integrator=integ,
-                   max_dt_scale=max_dt_scale, ray_bundles=ray_bundles)
+                   max_dt_scale=max_dt_scale, ray_bundles=ray_bundles, skybox=sky)
     xp, yp = cam.x_pix, cam.y_pix
     img = res["xyz"].reshape(yp, xp, 3)[::-1].copy()
     if not returnrays:

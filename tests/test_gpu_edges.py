@@ -82,7 +82,7 @@ def test_rejected_inputs(renderer):
     pole.position[2] = 0.0
     assert _call(renderer, scene, [pole], ok) == abi.ERR_INVALID_CAMERA             # on the axis
     bundles = renderer.params(colors, ray_bundles=True)
-    assert _call(renderer, scene, [cam], bundles) == abi.ERR_UNSUPPORTED            # not built
+    assert _call(renderer, scene, [cam], bundles) == abi.ERR_UNSUPPORTED            # wormhole only
     assert renderer.last_error() != ""
 
 

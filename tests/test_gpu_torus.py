@@ -292,3 +292,56 @@ def test_wormhole_skybox_matches_oracle(renderer, oracle, precision):
     # without the maps the wormhole is dark
     dark = renderer.render(sc, [cam], col, want=("spectrum",), precision=precision, integrator=abi.DP45_FSAL)
     assert np.all(dark["spectrum"] == 0)
+
+
+@pytest.mark.parametrize("precision", [abi.PREC_FP64, abi.PREC_MIXED])
+def test_wormhole_ray_bundles_match_oracle(renderer, oracle, precision):
+    """gen_image's ray_bundles for the wormhole: the device's Gaussian
+    footprint lookup (calc_skybox_I_nu_beam!: the pixel's bundle from the
+    camera, footprint widths, texels within it across face edges) against the
+    oracle's, with synthetic 16-texel cube maps. FP64: every pixel within 1e-6;
+    FP32-mixed: >= 95 % within 1e-3, the plain lookup's bar (the footprint
+    moves with the FP32-stage direction error as the single texel does). The
+    footprint changes the image, and a frame rendered as two windows (whose
+    bundles come from whole-image pixel indices) equals the whole frame."""
+    rng = np.random.default_rng(5)
+    H = 16
+    sky = tuple(rng.uniform(0, 1, (3 * H, 4 * H, 3)).astype(np.float32) for _ in range(2))
+    sc = configs.wormhole_scene()
+    cam = configs.wormhole_camera(32, 1e-6)
+    col = np.array([467.0, 532.0, 630.0])
+    ref = oracle.render(sc, cam, col, integrator=abi.DP45_FSAL, skybox=sky, ray_bundles=True, want=("spectrum",))
+    plain = oracle.render(sc, cam, col, integrator=abi.DP45_FSAL, skybox=sky, want=("spectrum",))
+    kw = dict(precision=precision, integrator=abi.DP45_FSAL, skybox=sky, ray_bundles=True)
+    g = renderer.render(sc, [cam], col, want=("class", "spectrum", "xyz"), **kw)
+    assert np.all(ref["spectrum"] > 0)
+    assert np.median(np.abs(ref["spectrum"] / plain["spectrum"] - 1)) > 1e-2
+    e = np.abs(g["spectrum"].astype(np.float64) - ref["spectrum"]) / ref["spectrum"]
+    if precision == abi.PREC_FP64:
+        assert e.max() < 1e-6, e.max()
+    else:
+        assert np.mean(np.all(e <= 1e-3, axis=1)) >= 0.95, np.mean(np.all(e <= 1e-3, axis=1))
+    yp = abi.y_pixels(cam.x_pix, cam.fov_hor, cam.fov_vert)
+    top = renderer.render(sc, [abi.window(cam, 0, 0, 32, 8)], col, want=("spectrum",), **kw)
+    bot = renderer.render(sc, [abi.window(cam, 0, 8, 32, yp - 8)], col, want=("spectrum",), **kw)
+    assert np.array_equal(np.concatenate([top["spectrum"], bot["spectrum"]]), g["spectrum"])
+
+
+def test_wormhole_world_through_gen_image_with_bundles():
+    """initialize_world("wormhole") + load_textures + gen_image(ray_bundles=True):
+    the reference's keyword path; other scenes refuse the bundles."""
+    from rtwca_b200 import render as R
+    rng = np.random.default_rng(2)
+    sky = tuple(rng.uniform(0, 1, (48, 64, 3)).astype(np.float32) for _ in range(2))
+    pos, d, pt, beta = R.initialize_world("wormhole")
+    R.load_textures(*sky)
+    try:
+        img = R.gen_image(camera_pos=pos, camera_dir=d, speed=beta, camera_point=pt, x_pix=16, tolerance=1e-6,
+                          max_steps=2e4, colors=(467, 532, 630), ray_bundles=True, integrator="fsal")
+        assert img.shape[1] == 16 and np.all(np.isfinite(img)) and np.all(img[:, :, 1] > 0)
+    finally:
+        R.load_textures(None, None)
+    pos, d, pt, beta = R.initialize_world("synch")
+    with pytest.raises(abi.RTWError) as ei:
+        R.gen_image(camera_pos=pos, camera_dir=d, speed=beta, camera_point=pt, x_pix=8, ray_bundles=True)
+    assert ei.value.status == abi.ERR_UNSUPPORTED

@@ -1,0 +1,105 @@
+"""The wormhole's skybox lookup on the CPU: the library's cube-map neighbour
+rule (the function the device's ray-bundle footprint runs, evaluated on the
+host) against the oracle's separately written restatement of cube_wrap
+(gen_geometry.jl:128-344) over every texel, face and footprint offset, and
+properties of the oracle's ray-bundle lookup (calc_skybox_I_nu_beam!,
+Wormhole.source/source_model.jl:266-358).
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from rtwca_b200 import abi, configs
+
+
+def _lib_wrap(lib):
+    f = lib.rtw_skybox_wrap
+    f.argtypes = [C.c_int32] * 6 + [C.POINTER(C.c_int32)]
+    f.restype = C.c_int
+    out = (C.c_int32 * 3)()
+
+    def wrap(i, j, face, x, y, n):
+        assert f(i, j, face, x, y, n, out) == abi.OK
+        return tuple(out)
+
+    return wrap
+
+
+def test_cube_wrap_library_matches_oracle(rtwlib, oracle):
+    """Every texel of an 11-texel face, every face, every offset of the
+    largest footprint (|x|, |y| <= 10): both restatements agree exactly."""
+    wrap = _lib_wrap(rtwlib)
+    n = 11
+    bad = []
+    for face in range(1, 7):
+        for i in range(1, n + 1):
+            for j in range(1, n + 1):
+                for x in range(-10, 11):
+                    for y in range(-10, 11):
+                        a = wrap(i, j, face, x, y, n)
+                        b = oracle.cube_wrap(i, j, face, x, y, n)
+                        if a != b:
+                            bad.append(((i, j, face, x, y), a, b))
+    assert not bad, bad[:5]
+
+
+def test_cube_wrap_properties(rtwlib):
+    """Moves inside a face stay there; the ring of faces 1-4 along i is a
+    cycle (a move and its reverse return to the start); crossing the top edge
+    of face 2 enters face 6 and its bottom edge face 5."""
+    wrap = _lib_wrap(rtwlib)
+    n = 16
+    assert wrap(5, 7, 3, 4, -3, n) == (9, 4, 3)
+    for face in range(1, 5):
+        for i in (1, 8, 16):
+            for x in (-10, -1, 1, 10):
+                i2, j2, f2 = wrap(i, 5, face, x, 0, n)
+                assert f2 in (1, 2, 3, 4) and j2 == 5
+                assert wrap(i2, j2, f2, -x, 0, n) == (i, 5, face)
+    assert wrap(4, 16, 2, 0, 1, n)[2] == 6
+    assert wrap(4, 1, 2, 0, -1, n)[2] == 5
+
+
+def _wormhole_case(H, seed):
+    rng = np.random.default_rng(seed)
+    sky = tuple(rng.uniform(0, 1, (3 * H, 4 * H, 3)).astype(np.float32) for _ in range(2))
+    sc = configs.wormhole_scene()
+    cam = configs.wormhole_camera(12, 1e-6)
+    col = np.array([467.0, 532.0, 630.0])
+    return sc, cam, col, sky
+
+
+def test_oracle_bundle_lookup_properties(oracle):
+    """With a uniform map the footprint only rescales the texel's spectrum:
+    bundle / plain is the same in every bin of a pixel (the summed weights);
+    with a random map the footprint changes the image; either way the
+    geodesics and the step counts do not depend on the bundle (its components
+    have zero slope and stay out of the error norm)."""
+    sc, cam, col, sky = _wormhole_case(16, 7)
+    ids = np.arange(0, 12 * 8, 5)
+    flat = tuple(np.full_like(s, 0.5) for s in sky)
+    kw = dict(integrator=abi.DP45_FSAL, pixel_ids=ids, want=("spectrum", "steps", "state"))
+    p = oracle.render(sc, cam, col, skybox=flat, **kw)
+    b = oracle.render(sc, cam, col, skybox=flat, ray_bundles=True, **kw)
+    assert np.array_equal(p["steps"], b["steps"]) and np.array_equal(p["state"], b["state"])
+    ratio = b["spectrum"] / p["spectrum"]
+    assert np.all(ratio > 0.05) and np.all(ratio < 2)
+    np.testing.assert_allclose(ratio, ratio[:, :1] * np.ones_like(ratio), rtol=1e-12)
+    p = oracle.render(sc, cam, col, skybox=sky, **kw)
+    b = oracle.render(sc, cam, col, skybox=sky, ray_bundles=True, **kw)
+    assert np.median(np.abs(b["spectrum"] / p["spectrum"] - 1)) > 1e-2
+    # the bundle flag is reset after each call
+    again = oracle.render(sc, cam, col, skybox=sky, **kw)
+    assert np.array_equal(again["spectrum"], p["spectrum"])
+
+
+@pytest.mark.parametrize("H", [3, 16])
+def test_oracle_bundle_lookup_small_maps(oracle, H):
+    """Faces smaller than the footprint (3 texels: offsets wrap past a whole
+    face, where the reference stops with an index error) give finite, positive
+    spectra: texels whose coordinates leave the map are skipped."""
+    sc, cam, col, sky = _wormhole_case(H, 11)
+    r = oracle.render(sc, cam, col, integrator=abi.DP45_FSAL, skybox=sky, ray_bundles=True,
+                      pixel_ids=np.arange(0, 96, 7), want=("spectrum",))
+    assert np.all(np.isfinite(r["spectrum"])) and np.all(r["spectrum"] > 0)
