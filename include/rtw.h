@@ -104,7 +104,14 @@ typedef enum rtw_scene_kind {
        1, 0.005, 0.05); empty space; rays end beyond r(l) = escape_radius or
        phi > winding_limit (source_geometry.jl:7-205, source_model.jl:54-147).
        Both integrators. */
-    RTW_SCENE_WORMHOLE = 7
+    RTW_SCENE_WORMHOLE = 7,
+    /* Minkowski_Sphere_Cartesian.source ("minkowski_t,x,y,z_sphere"): flat
+       space in Cartesian (t, x, y, z), a static blackbody sphere of radius
+       r_out at temperature (5778 K) with a_nu = a_nu (1 per map unit, so
+       optically thin: tau <= 2) in front of skybox[0], which every ray adds at
+       its end; rays end beyond |x| = escape_radius (source_geometry.jl:7-82,
+       source_model.jl:8-431). Both integrators. */
+    RTW_SCENE_MINKOWSKI_CART_SPHERE = 8
 } rtw_scene_kind;
 
 /* How a ray ended. The reference's calc_terminate (e.g. Kerr.source/
@@ -203,9 +210,10 @@ typedef struct rtw_render_params {
                                    `colors`); host memory */
     double max_dt_scale;        /* reference max_dt_scale (default 0.1) */
     int32_t integrator;         /* rtw_integrator */
-    int32_t ray_bundles;        /* 1: Gaussian ray-bundle lookup of the wormhole's
-                                   skyboxes (RTW_SCENE_WORMHOLE only; other scenes
-                                   return RTW_ERR_UNSUPPORTED) */
+    int32_t ray_bundles;        /* 1: Gaussian ray-bundle lookup of the skyboxes
+                                   (RTW_SCENE_WORMHOLE, RTW_SCENE_MINKOWSKI_CART_SPHERE;
+                                   other scenes return RTW_ERR_UNSUPPORTED); as in
+                                   the reference, no opacity stop then */
     double promote_dr;          /* MIXED: FP64 stages while r - r_horizon < promote_dr M
                                    (0: default 1e-3; < 0: never) */
     double promote_sin;         /* MIXED: FP64 stages while sin(theta) < promote_sin
@@ -239,7 +247,9 @@ typedef struct rtw_render_params {
        as the reference's skybox_handling! without ray bundles does, or, with
        ray_bundles = 1, the texels within a Gaussian footprint of the pixel's
        ray bundle (up to 21 x 21 texels, across face edges), as its
-       calc_skybox_I_nu_beam! does (Wormhole.source/source_model.jl:150-443). */
+       calc_skybox_I_nu_beam! does (Wormhole.source/source_model.jl:150-443).
+       RTW_SCENE_MINKOWSKI_CART_SPHERE: skybox[0] only, added at the end of
+       every ray (Minkowski_Sphere_Cartesian.source/source_model.jl:175-431). */
     const float* skybox[2];
     int32_t skybox_h[2];
 } rtw_render_params;

@@ -114,6 +114,9 @@ struct OScene {
     double T = 5778, anu = 1, esc = 100, wind = 8 * kPi;
     double rho_r0 = 6, rho_h = 0.1, rho_idx = -2, t_idx = -0.75;
     double n0 = 0, b0 = 0, th0 = 0, b_idx = 0, edge_in = 1, edge_out = 1, length_cm = 1;
+    // gen_image's ray_bundles: 11 more ray components, which calc_terminate's
+    // all-slots opacity test also reads (they are 0 or small: it never holds)
+    bool bundles = false;
 
     explicit OScene(const rtw_scene& s) {
         kind = s.kind;
@@ -151,8 +154,10 @@ struct OScene {
         return kind == RTW_SCENE_KERR_DISK || kind == RTW_SCENE_KERR_THICK_DISK || kind == RTW_SCENE_KERR_SYNCHRO_TORUS ||
                kind == RTW_SCENE_KERR_POWEHI;
     }
-    // Synchro_Test.source: Minkowski space in Cartesian (t, x, y, z)
-    bool is_cart() const { return kind == RTW_SCENE_SYNCHRO_TEST; }
+    // Synchro_Test.source and Minkowski_Sphere_Cartesian.source: Minkowski
+    // space in Cartesian (t, x, y, z) (the two geometry files differ in
+    // whitespace only)
+    bool is_cart() const { return kind == RTW_SCENE_SYNCHRO_TEST || kind == RTW_SCENE_MINKOWSKI_CART_SPHERE; }
     // Wormhole.source: the Dneg wormhole in (t, l, theta, phi)
     bool is_wh() const { return kind == RTW_SCENE_WORMHOLE; }
     // source_geometry.jl:7-41: M = W / W_over_M, r(l), and dr/dl as the
@@ -424,6 +429,8 @@ struct OScene {
         const double r = x[1], th = x[2];
         switch (kind) {
         case RTW_SCENE_MINKOWSKI_SPHERE: return r <= r_out;
+        case RTW_SCENE_MINKOWSKI_CART_SPHERE:  // Minkowski_Sphere_Cartesian model :82-90
+            return std::sqrt(x[1] * x[1] + x[2] * x[2] + x[3] * x[3]) <= r_out;
         case RTW_SCENE_SCHWARZSCHILD_DISK:
         case RTW_SCENE_KERR_DISK:
             return r_in <= r && r <= r_out && th_lo <= th && th <= th_hi;
@@ -436,7 +443,7 @@ struct OScene {
     void source_velocity(const double* x, double u[4]) const {
         const double r = x[1], th = x[2];
         u[0] = 1; u[1] = 0; u[2] = 0; u[3] = 0;
-        if (kind == RTW_SCENE_MINKOWSKI_SPHERE) return;
+        if (kind == RTW_SCENE_MINKOWSKI_SPHERE || kind == RTW_SCENE_MINKOWSKI_CART_SPHERE) return;
         if (kind == RTW_SCENE_SCHWARZSCHILD_DISK) {
             if (is_fire(x)) {
                 u[0] = 1.0 / std::sqrt(1 - 3 * M / r);
@@ -487,6 +494,8 @@ struct OScene {
 
     // pad_max_dt: Kerr model :86-103, Schwarzschild :86-106, Minkowski :89-105
     double pad_max_dt(const double* x, double scale) const {
+        if (kind == RTW_SCENE_MINKOWSKI_CART_SPHERE)  // Minkowski_Sphere_Cartesian model :130-132
+            return scale * (1 + std::fabs(x[1]) + std::fabs(x[2]) + std::fabs(x[3]));
         if (is_cart()) return scale * (1 + std::fabs(x[1]) + std::fabs(x[2]));  // Synchro_Test model :241-244
         if (is_wh()) {  // Wormhole model :88-110
             double e = (x[2] < kPi / 8 || x[2] > 7 * kPi / 8) ? std::min(scale, (double)1e-1f) : scale;
@@ -527,13 +536,15 @@ struct OScene {
         if (is_wh()) {  // Wormhole model :134-147
             if (wh_r(ray[1]) > esc) return RTW_CLASS_ESCAPE;
             if (ray[3] > wind) return RTW_CLASS_WINDING;
+            if (bundles) return 0;  // the bundle slots are in the opacity test too
             const double thick = -std::log(tol);
             for (int i = 9; i < L; i += 2)
                 if (ray[i] < thick) return 0;
             return RTW_CLASS_THICK;
         }
-        if (is_cart()) {  // Synchro_Test model :258-275
+        if (is_cart()) {  // Synchro_Test model :258-275, Minkowski_Sphere_Cartesian :158-172
             if (std::sqrt(ray[1] * ray[1] + ray[2] * ray[2] + ray[3] * ray[3]) > esc) return RTW_CLASS_ESCAPE;
+            if (bundles) return 0;
             const double thick = -std::log(tol);
             for (int i = 9; i < L; i += 2)
                 if (ray[i] < thick) return 0;
@@ -1286,22 +1297,31 @@ void distort_gauss(double sx, double sy, double t, double a, double b, double& s
 // with a bundle b (camera_bundle's layout), calc_skybox_I_nu_beam! (:266-358).
 // Texels that wrap off the map (faces under 10 texels; the reference stops
 // with an index error) and a footprint with a NaN width add nothing.
+// Minkowski_Sphere_Cartesian.source/source_model.jl:175-431: the same lookup
+// at every ray's end, skybox 1, the velocity already Cartesian.
 void wormhole_skybox(const OScene& sc, double* ray, int N, const double* freq, const double* bund) {
-    const double rl = sc.wh_r(ray[1]);
-    if (!(rl > 50) || ray[1] == 0) return;
-    const int k = ray[1] > 0 ? 0 : 1;
-    if (!g_sky[k]) return;
-    const int H = g_sky_h[k];
-    const double th = ray[2], ph = ray[3];
-    const double e[4] = {ray[4], ray[5], rl * ray[6], rl * std::sin(th) * ray[7]};
-    double R[4][4] = {};
-    R[0][0] = 1;
-    R[1][1] = std::sin(th) * std::cos(ph); R[1][2] = std::cos(th) * std::cos(ph); R[1][3] = -std::sin(ph);
-    R[2][1] = std::sin(th) * std::sin(ph); R[2][2] = std::cos(th) * std::sin(ph); R[2][3] = std::cos(ph);
-    R[3][1] = std::cos(th); R[3][2] = -std::sin(th);
+    int k = 0;
     double v[4] = {0, 0, 0, 0};
+    if (sc.kind == RTW_SCENE_MINKOWSKI_CART_SPHERE) {
+        for (int a = 0; a < 4; ++a) v[a] = ray[4 + a];
+    } else {
+        const double rl = sc.wh_r(ray[1]);
+        if (!(rl > 50) || ray[1] == 0) return;
+        k = ray[1] > 0 ? 0 : 1;
+        const double th = ray[2], ph = ray[3];
+        const double e[4] = {ray[4], ray[5], rl * ray[6], rl * std::sin(th) * ray[7]};
+        double R[4][4] = {};
+        R[0][0] = 1;
+        R[1][1] = std::sin(th) * std::cos(ph); R[1][2] = std::cos(th) * std::cos(ph); R[1][3] = -std::sin(ph);
+        R[2][1] = std::sin(th) * std::sin(ph); R[2][2] = std::cos(th) * std::sin(ph); R[2][3] = std::cos(ph);
+        R[3][1] = std::cos(th); R[3][2] = -std::sin(th);
+        for (int a = 0; a < 4; ++a)
+            for (int b = 0; b < 4; ++b) v[a] += R[a][b] * e[b];
+    }
+    if (!g_sky[k]) return;
     for (int a = 0; a < 4; ++a)
-        for (int b = 0; b < 4; ++b) v[a] += R[a][b] * e[b];
+        if (!std::isfinite(v[a])) return;  // a NaN ray (the reference stops with an error)
+    const int H = g_sky_h[k];
     const double nv = std::sqrt(v[1] * v[1] + v[2] * v[2] + v[3] * v[3]);
     const double x = v[1] / nv, y = v[2] / nv, z = v[3] / nv;
     int face;
@@ -1464,6 +1484,7 @@ int oracle_render(const rtw_scene* scene, rtw_camera* cam, const double* colors_
                   long long* counters, int n_threads) {
     if (!scene || !cam || !colors_nm || n_colors <= 0 || n_colors > RTW_MAX_BINS) return RTW_ERR_INVALID_PARAM;
     OScene sc(*scene);
+    sc.bundles = g_bundles != 0;
     if (sc.is_singularity(cam->position)) return RTW_ERR_INVALID_CAMERA;
     CameraGeom cg;
     camera_geom(sc, *cam, cg);
@@ -1509,7 +1530,7 @@ int oracle_render(const rtw_scene* scene, rtw_camera* cam, const double* colors_
             }
             for (int k = 0; k < 8; ++k)
                 if (!std::isfinite(ray[k])) klass = RTW_CLASS_NAN;
-            if (sc.is_wh()) {
+            if (sc.is_wh() || sc.kind == RTW_SCENE_MINKOWSKI_CART_SPHERE) {
                 double bund[6];
                 if (g_bundles) camera_bundle(cg, i, j, bund);
                 wormhole_skybox(sc, ray.data(), N, freq.data(), g_bundles ? bund : nullptr);

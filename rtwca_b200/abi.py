@@ -47,6 +47,7 @@ SCENE_KERR_SYNCHRO_TORUS = 4
 SCENE_KERR_POWEHI = 5
 SCENE_SYNCHRO_TEST = 6
 SCENE_WORMHOLE = 7
+SCENE_MINKOWSKI_CART_SPHERE = 8
 ADJOINT_PARAMS = ("spin", "inclination", "n_e0", "b_0", "theta_e0")
 
 # rtw_term_class

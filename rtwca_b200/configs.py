@@ -223,6 +223,21 @@ def wormhole_scene() -> abi.Scene:
     return abi.scene_default(abi.SCENE_WORMHOLE)
 
 
+def cart_sphere_scene() -> abi.Scene:
+    """Minkowski_Sphere_Cartesian.source: flat Cartesian space, a blackbody
+    sphere of radius 1 at 5778 K with a_nu = 1 (optically thin) in front of a
+    skybox."""
+    return abi.scene_default(abi.SCENE_MINKOWSKI_CART_SPHERE)
+
+
+def cart_sphere_camera(x_pix: int = 256, tol: float = 1e-6, max_steps: int = 20_000) -> abi.Camera:
+    """The reference's "minkowski_t,x,y,z_sphere" world (initialization.jl:
+    130-138): position (0, 0, 0, -4) (Cartesian t, x, y, z), direction (0, 0),
+    pointing (0, 0, 0), beta 0; default field of view."""
+    return abi.make_camera([0.0, 0.0, 0.0, -4.0], [0.0, 0.0], 0.0, [0.0, 0.0, 0.0], x_pix, 85.0, 60.0, tol,
+                           max_steps)
+
+
 def wormhole_camera(x_pix: int = 256, tol: float = 1e-6, max_steps: int = 20_000) -> abi.Camera:
     """The reference's "wormhole" world (initialization.jl:140-148): position
     (0, l = 5, pi/2, 0), direction (pi/2, 0), pointing (0, 0, -pi/2), beta 0;

@@ -142,7 +142,8 @@ double wormhole_r_host(const rtw_scene& s, double l) {
 void inv_tetrad(const rtw_scene& s, const double* x, M4 e) {
     for (int i = 0; i < 4; ++i)
         for (int j = 0; j < 4; ++j) e[i][j] = i == j ? 1.0 : 0.0;
-    if (s.kind == RTW_SCENE_SYNCHRO_TEST) return;  // Cartesian Minkowski: the identity
+    if (s.kind == RTW_SCENE_SYNCHRO_TEST || s.kind == RTW_SCENE_MINKOWSKI_CART_SPHERE)
+        return;  // Cartesian Minkowski: the identity
     if (s.kind == RTW_SCENE_WORMHOLE) {            // Wormhole.source/source_geometry.jl:83-90
         const double rl = wormhole_r_host(s, x[1]);
         e[2][2] = 1 / rl;
@@ -367,6 +368,12 @@ rtw_status rtw_scene_default(int32_t kind, rtw_scene* s) {
         // rho = 1, a = 0.005 rho, W = 0.05 rho; escape at r(l) > 100, phi > 8 pi
         s->r_in = 1; s->edge_in = 0.005; s->edge_out = 0.05; s->escape_radius = 100;
         break;
+    case RTW_SCENE_MINKOWSKI_CART_SPHERE:
+        // Minkowski_Sphere_Cartesian.source: sphere of radius 1 (is_fire
+        // :82-90), T = 5.778f3 K (:51-55), a_nu = 1f0 / map_scale (:66-77),
+        // rays end at |x| > 100 (:158-172)
+        s->r_out = 1; s->temperature = 5778; s->a_nu = 1; s->escape_radius = 100;
+        break;
     default:
         return RTW_ERR_INVALID_PARAM;
     }
@@ -390,12 +397,13 @@ rtw_status rtw_camera_pixels(rtw_camera* cam, int64_t* n_pix) {
 static rtw_status build_frame(const rtw_scene& s, rtw_camera& cam, FrameDesc& f) {
     rtw_status st = rtw_camera_pixels(&cam, nullptr);
     if (st != RTW_OK) return st;
-    // (the Cartesian scene has no coordinate singularity: Synchro_Test.source/
-    // source_geometry.jl:84-88)
+    // (the Cartesian scenes have no coordinate singularity: Synchro_Test.source/
+    // source_geometry.jl:84-88, Minkowski_Sphere_Cartesian.source/source_geometry.jl:80-82)
     if (s.kind == RTW_SCENE_WORMHOLE) {  // the poles only (Wormhole.source/source_geometry.jl:197-205)
         if (std::fabs(cam.position[2]) <= (double)1e-32f || std::fabs(cam.position[2] - kPi) <= (double)1e-32f)
             return RTW_ERR_INVALID_CAMERA;
-    } else if (s.kind != RTW_SCENE_SYNCHRO_TEST && on_singularity(cam.position)) {
+    } else if (s.kind != RTW_SCENE_SYNCHRO_TEST && s.kind != RTW_SCENE_MINKOWSKI_CART_SPHERE &&
+               on_singularity(cam.position)) {
         return RTW_ERR_INVALID_CAMERA;
     }
     if (!(std::fabs(cam.speed) < 1)) return RTW_ERR_INVALID_PARAM;
@@ -566,10 +574,11 @@ rtw_status rtw_render(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* ca
     if (n_cams <= 0 || n_cams > RTW_MAX_FRAMES) return fail(ctx, RTW_ERR_INVALID_PARAM, "n_cams out of range");
     if (prm->n_colors <= 0 || prm->n_colors > RTW_MAX_BINS || !prm->colors_nm)
         return fail(ctx, RTW_ERR_INVALID_PARAM, "n_colors must be 1..128 with colors_nm set");
-    if (prm->ray_bundles && scene->kind != RTW_SCENE_WORMHOLE)
-        return fail(ctx, RTW_ERR_UNSUPPORTED, "ray bundles are built for the wormhole scene only");
+    if (prm->ray_bundles && scene->kind != RTW_SCENE_WORMHOLE && scene->kind != RTW_SCENE_MINKOWSKI_CART_SPHERE)
+        return fail(ctx, RTW_ERR_UNSUPPORTED, "ray bundles are built for the skybox scenes only");
     if (scene->kind == RTW_SCENE_KERR_SYNCHRO_TORUS || scene->kind == RTW_SCENE_KERR_POWEHI ||
-        scene->kind == RTW_SCENE_SYNCHRO_TEST || scene->kind == RTW_SCENE_WORMHOLE)
+        scene->kind == RTW_SCENE_SYNCHRO_TEST || scene->kind == RTW_SCENE_WORMHOLE ||
+        scene->kind == RTW_SCENE_MINKOWSKI_CART_SPHERE)
         return torus_render(ctx, scene, cams, n_cams, prm, out);
     if (scene->ref_precision) return fail(ctx, RTW_ERR_UNSUPPORTED, "ref_precision is an oracle-only switch");
     if (prm->precision != RTW_PREC_FP64 && prm->precision != RTW_PREC_MIXED && prm->precision != RTW_PREC_FP64_PLAIN)

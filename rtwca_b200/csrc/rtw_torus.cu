@@ -77,9 +77,11 @@ struct TorusModel {
     PowehiDev pw;
     SynchroDev sy;
     WormholeDev wh;
+    SphereDev sp;
     TorusBin bins[kTorusMaxBins];
     int n;         // bins
-    int emitter;   // 0: synchrotron torus, 1: Powehi (disk + jet), 2: Synchro_Test cylinder, 3: none (wormhole)
+    int emitter;   // 0: synchrotron torus, 1: Powehi (disk + jet), 2: Synchro_Test cylinder, 3: none (wormhole),
+                   // 4: the Cartesian blackbody sphere
     int geom;      // geometry: 0 Kerr (Boyer-Lindquist), 1 Minkowski (Cartesian), 2 Dneg wormhole
 };
 
@@ -95,13 +97,15 @@ RTW_HD TorusPt<R> em_point(const TorusModel& m, const R* z) {
         o.cj = R(0.0); o.nus = R(0.0); o.th = R(1.0); o.g = R(1.0);
         return o;
     }
+    if (EM == 4 || (EM == -1 && m.emitter == 4)) return sphere_point<R>(m.sp, z);
     if (EM == 2 || (EM == -1 && m.emitter == 2)) return synchro_point<R>(m.sy, z);
     if (EM == 1 || (EM == -1 && m.emitter == 1)) return powehi_point<R>(m.pw, z);
     return torus_point<R>(m.tor, R(m.tor.a), R(m.tor.n0), R(m.tor.B0), R(m.tor.Th0), z[1], z[2], z[4], z[7]);
 }
 template <class R, int EM = -1>
 RTW_HD void em_bin(const TorusModel& m, const TorusPt<R>& S, int c, R& ft, R& fi) {
-    if (EM > 0 || (EM == -1 && m.emitter != 0)) powehi_bin<R>(m.pw, S, m.bins[c].nu_nm, ft, fi);
+    if (EM == 4 || (EM == -1 && m.emitter == 4)) sphere_bin<R>(m.sp, S, m.bins[c].nu_nm, ft, fi);
+    else if (EM > 0 || (EM == -1 && m.emitter != 0)) powehi_bin<R>(m.pw, S, m.bins[c].nu_nm, ft, fi);
     else torus_bin<R>(S.cj, S.nus, S.th, S.g, m.bins[c], ft, fi);
 }
 
@@ -111,7 +115,7 @@ RTW_HD void torus_geo_rhs(const TorusModel& m, const double* y, double* f) {
         wormhole_rhs<double>(m.wh, y, f);
         return;
     }
-    if (m.geom == 1) {  // straight lines (Synchro_Test.source/source_geometry.jl:55-66)
+    if (m.geom == 1) {  // straight lines (Synchro_Test.source/source_geometry.jl:55-66 and the Cartesian sphere's)
         for (int i = 0; i < 4; ++i) {
             f[i] = y[4 + i];
             f[4 + i] = 0;
@@ -315,7 +319,7 @@ struct TorusStages {
 // state x and the carried slope k1.
 template <class R, class K, int EM>
 __device__ void torus_geo_stages(const TorusModel& m, const double* x, const K* k1, double h, TorusStages<R>& o) {
-    constexpr bool FLAT = EM == 2;
+    constexpr bool FLAT = EM == 2 || EM == 4;
     R Kg[7][8];
     for (int i = 0; i < 8; ++i) Kg[0][i] = R(k1[i]);
     const R hr = R(h);
@@ -447,21 +451,33 @@ __device__ void bundle_shape(const TorusKP& p, int pi, int pj, double* d) {
 // spectrum: the reference's sum, reassociated. Texels whose wrapped
 // coordinates fall off the map (maps under 10 texels a face: the reference
 // stops with an index error there) are skipped.
+// The Cartesian sphere (EM 4; Minkowski_Sphere_Cartesian.source/
+// source_model.jl:175-431) runs the same lookup at every ray's end, in skybox
+// 1, with the direction (k^x, k^y, k^z) as it is.
+template <int EM>
 __device__ void wormhole_skybox(const TorusKP& p, const double* x, int N, double* I, const double* tau, int pi,
                                 int pj) {
-    const WormholeDev& W = p.m.wh;
-    const double rl = wormhole_r<double>(W, x[1]);
-    if (!(rl > 50) || x[1] == 0) return;
-    const int k = x[1] > 0 ? 0 : 1;
+    int k = 0;
+    double vx, vy, vz;
+    if constexpr (EM == 4) {
+        vx = x[5];
+        vy = x[6];
+        vz = x[7];
+    } else {
+        const WormholeDev& W = p.m.wh;
+        const double rl = wormhole_r<double>(W, x[1]);
+        if (!(rl > 50) || x[1] == 0) return;
+        k = x[1] > 0 ? 0 : 1;
+        double st, ct, sp, cp;
+        sincos(x[2], &st, &ct);
+        sincos(x[3], &sp, &cp);
+        const double e1 = x[5], e2 = rl * x[6], e3 = rl * st * x[7];
+        vx = st * cp * e1 + ct * cp * e2 - sp * e3;
+        vy = st * sp * e1 + ct * sp * e2 + cp * e3;
+        vz = ct * e1 - st * e2;
+    }
     if (!p.sky[k]) return;
     const int H = p.sky_h[k];
-    double st, ct, sp, cp;
-    sincos(x[2], &st, &ct);
-    sincos(x[3], &sp, &cp);
-    const double e1 = x[5], e2 = rl * x[6], e3 = rl * st * x[7];
-    const double vx = st * cp * e1 + ct * cp * e2 - sp * e3;
-    const double vy = st * sp * e1 + ct * sp * e2 + cp * e3;
-    const double vz = ct * e1 - st * e2;
     const double nv = sqrt(vx * vx + vy * vy + vz * vz);
     const double X = vx / nv, Y = vy / nv, Z = vz / nv;
     const double ax = fabs(X), ay = fabs(Y), az = fabs(Z);
@@ -557,11 +573,15 @@ RTW_HD double wormhole_max_dt(const WormholeDev& W, const double* x, double scal
 }
 
 // pad_max_dt of the geometry: Kerr (source_model.jl:86-103), Synchro_Test's
-// max_dt_scale (1 + |x| + |y|) (source_model.jl:241-244) or the wormhole's
+// max_dt_scale (1 + |x| + |y|) (source_model.jl:241-244), the Cartesian
+// sphere's max_dt_scale (1 + |x| + |y| + |z|) (source_model.jl:130-132) or the
+// wormhole's
 template <int EM, class SR>
 __device__ __forceinline__ double torus_max_dt(const TorusKP& p, const double* x) {
     if constexpr (EM == 2)
         return p.max_dt_scale * (1 + fabs(x[1]) + fabs(x[2]));
+    else if constexpr (EM == 4)
+        return p.max_dt_scale * (1 + fabs(x[1]) + fabs(x[2]) + fabs(x[3]));
     else if constexpr (EM == 3)
         return wormhole_max_dt(p.m.wh, x, p.max_dt_scale);
     else
@@ -573,7 +593,7 @@ __device__ __forceinline__ double torus_max_dt(const TorusKP& p, const double* x
 // (Wormhole.source/source_geometry.jl:156-171)
 template <int EM>
 __device__ __forceinline__ bool torus_near_singularity(const double* x, double h, double tol, double* temp) {
-    if constexpr (EM == 2) {
+    if constexpr (EM == 2 || EM == 4) {
         return false;
     } else if constexpr (EM == 3) {
         const double th_new = x[2] + h * x[6];
@@ -593,11 +613,12 @@ __device__ __forceinline__ bool torus_near_singularity(const double* x, double h
 }
 
 // calc_terminate without the step-count predicate; THICK when every bin's
-// tau has reached -log(tol)
+// tau has reached -log(tol). With ray bundles the reference's test also sees
+// the bundle slots, which are 0 or small and keep it from firing: no THICK.
 template <class SR, int EM>
 __device__ __forceinline__ int torus_terminate(const TorusKP& p, const double* x, const SR* tau, int N) {
-    if constexpr (EM == 2) {
-        // Synchro_Test.source/source_model.jl:258-275
+    if constexpr (EM == 2 || EM == 4) {
+        // Synchro_Test.source/source_model.jl:258-275, the sphere's :158-172
         if (sqrt(x[1] * x[1] + x[2] * x[2] + x[3] * x[3]) > p.m.geo.esc) return RTW_CLASS_ESCAPE;
     } else if constexpr (EM == 3) {
         // Wormhole.source/source_model.jl:134-147: r(l) beyond the escape radius, phi winding
@@ -608,6 +629,8 @@ __device__ __forceinline__ int torus_terminate(const TorusKP& p, const double* x
         if (x[1] <= p.frame.r_term) return RTW_CLASS_HORIZON;
         if (x[3] > p.m.geo.wind) return RTW_CLASS_WINDING;
     }
+    if constexpr (EM >= 3)
+        if (p.bundles) return 0;
     for (int c = 0; c < N; ++c)
         if ((double)tau[c] < p.frame.thick) return 0;
     return RTW_CLASS_THICK;
@@ -722,7 +745,7 @@ __device__ __noinline__ void torus_rec_end(const TorusKP& p, TorusRec* r, long l
 // 255; FP64 stays at 2, where 3 was 8-20 % slower)
 template <bool MIXED, int EM>
 __global__ void __launch_bounds__(128, MIXED ? 3 : 2) torus_forward(const TorusKP p) {
-    constexpr bool FLAT = EM == 2;  // Synchro_Test: flat Cartesian geometry
+    constexpr bool FLAT = EM == 2 || EM == 4;  // Synchro_Test, the sphere: flat Cartesian geometry
     typedef typename SpecTraits<MIXED>::SR SR;
     const int N = p.m.n;
     const int D = 8 + 2 * N;
@@ -980,14 +1003,14 @@ __global__ void __launch_bounds__(128, MIXED ? 3 : 2) torus_forward(const TorusK
             cls = RTW_CLASS_NAN;
             ++c_nan;
         }
-        if constexpr (EM == 3) {
+        if constexpr (EM == 3 || EM == 4) {
             if (fin && (p.sky[0] || p.sky[1])) {
                 double I[kTorusMaxBins], tv[kTorusMaxBins];
                 for (int c = 0; c < N; ++c) {
                     I[c] = (double)ihi[c] + (MIXED ? (double)ilo[c] : 0.0);
                     tv[c] = (double)tau[c];
                 }
-                wormhole_skybox(p, x, N, I, tv, pi, pj);
+                wormhole_skybox<EM>(p, x, N, I, tv, pi, pj);
                 for (int c = 0; c < N; ++c) {
                     ihi[c] = SR(I[c]);
                     ilo[c] = MIXED ? SR(I[c] - (double)ihi[c]) : SR(0);
@@ -1593,8 +1616,13 @@ rtw_status torus_model(const rtw_scene& s, const double* colors_nm, int N, Torus
         return RTW_ERR_INVALID_PARAM;
     }
     const bool powehi = s.kind == RTW_SCENE_KERR_POWEHI, synchro = s.kind == RTW_SCENE_SYNCHRO_TEST,
-               wormhole = s.kind == RTW_SCENE_WORMHOLE;
-    if (wormhole) {
+               wormhole = s.kind == RTW_SCENE_WORMHOLE, sphere = s.kind == RTW_SCENE_MINKOWSKI_CART_SPHERE;
+    if (sphere) {
+        if (!(s.r_out > 0) || !(s.temperature > 0) || !(s.a_nu >= 0) || !(s.escape_radius > 0)) {
+            why = "sphere radius, temperature and escape radius must be > 0, a_nu >= 0";
+            return RTW_ERR_INVALID_PARAM;
+        }
+    } else if (wormhole) {
         if (!(s.r_in > 0) || !(s.edge_in >= 0) || !(s.edge_out > 0) || !(s.escape_radius > s.r_in)) {
             why = "wormhole parameters out of range";
             return RTW_ERR_INVALID_PARAM;
@@ -1608,7 +1636,7 @@ rtw_status torus_model(const rtw_scene& s, const double* colors_nm, int N, Torus
         why = "cylinder radius and escape radius must be > 0";
         return RTW_ERR_INVALID_PARAM;
     }
-    if (!powehi && !synchro && !wormhole && (!(s.r_in > 0) || !(s.r_out >= s.r_in) || !(s.edge_in > 0) || !(s.edge_out > 0) ||
+    if (!powehi && !synchro && !wormhole && !sphere && (!(s.r_in > 0) || !(s.r_out >= s.r_in) || !(s.edge_in > 0) || !(s.edge_out > 0) ||
                     !(s.theta_e0 > 0) || !(s.rho_h > 0))) {
         why = "torus parameters out of range";
         return RTW_ERR_INVALID_PARAM;
@@ -1655,8 +1683,14 @@ rtw_status torus_model(const rtw_scene& s, const double* colors_nm, int N, Torus
         m.bins[c].inv_b0 = 1.0 / m.bins[c].b0;
     }
     m.n = N;
-    m.emitter = powehi ? 1 : synchro ? 2 : wormhole ? 3 : 0;
-    m.geom = synchro ? 1 : wormhole ? 2 : 0;
+    m.emitter = powehi ? 1 : synchro ? 2 : wormhole ? 3 : sphere ? 4 : 0;
+    m.geom = synchro || sphere ? 1 : wormhole ? 2 : 0;
+    if (sphere) {
+        m.sp.r_sph = s.r_out;
+        m.sp.a_nu = s.a_nu;
+        m.sp.es = kEmissionScale;
+        m.sp.ff_T = kFFactor / s.temperature;
+    }
     if (wormhole) {
         // Wormhole.source/source_geometry.jl:7-15: M = W / W_over_M
         const double c = kPi / (2 * std::sqrt(2.0));
@@ -1677,14 +1711,15 @@ rtw_status torus_model(const rtw_scene& s, const double* colors_nm, int N, Torus
 }
 
 // the forward kernel instance: precision x emitter (0 torus, 1 Powehi, 2
-// Synchro_Test in flat Cartesian geometry, 3 none in the wormhole's geometry)
+// Synchro_Test in flat Cartesian geometry, 3 none in the wormhole's geometry,
+// 4 the blackbody sphere in flat Cartesian geometry)
 const void* forward_fn(bool mixed, int emitter) {
-    static const void* const fn[2][4] = {
+    static const void* const fn[2][5] = {
         {(const void*)torus_forward<false, 0>, (const void*)torus_forward<false, 1>, (const void*)torus_forward<false, 2>,
-         (const void*)torus_forward<false, 3>},
+         (const void*)torus_forward<false, 3>, (const void*)torus_forward<false, 4>},
         {(const void*)torus_forward<true, 0>, (const void*)torus_forward<true, 1>, (const void*)torus_forward<true, 2>,
-         (const void*)torus_forward<true, 3>}};
-    return fn[mixed ? 1 : 0][emitter >= 0 && emitter <= 3 ? emitter : 0];
+         (const void*)torus_forward<true, 3>, (const void*)torus_forward<true, 4>}};
+    return fn[mixed ? 1 : 0][emitter >= 0 && emitter <= 4 ? emitter : 0];
 }
 
 // launch shape of the torus kernels: 128 threads, occupancy-limited CTAs
@@ -1709,11 +1744,11 @@ rtw_status torus_setup(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* c
         return fail(ctx, RTW_ERR_INVALID_PARAM, "precision");
     if (prm->integrator != RTW_DP45_FSAL && prm->integrator != RTW_DP45_REF_COMPAT)
         return fail(ctx, RTW_ERR_INVALID_PARAM, "integrator");
-    // the bundle enters only the wormhole's skybox lookup; in every other
-    // scene the reference's bundle slots would also hold off its opacity stop
-    // (the all-slots tau test of calc_terminate), which is not built
-    if (prm->ray_bundles && scene->kind != RTW_SCENE_WORMHOLE)
-        return fail(ctx, RTW_ERR_UNSUPPORTED, "ray bundles are built for the wormhole scene only");
+    // the bundle enters only the skybox lookups; in the reference its slots
+    // also hold off the opacity stop (the all-slots tau test of
+    // calc_terminate), which the skybox scenes follow and the others do not
+    if (prm->ray_bundles && scene->kind != RTW_SCENE_WORMHOLE && scene->kind != RTW_SCENE_MINKOWSKI_CART_SPHERE)
+        return fail(ctx, RTW_ERR_UNSUPPORTED, "ray bundles are built for the skybox scenes only");
     if (!(prm->max_dt_scale > 0)) return fail(ctx, RTW_ERR_INVALID_PARAM, "max_dt_scale must be > 0");
     std::string why;
     TorusKP& p = run.kp;
@@ -1794,8 +1829,8 @@ rtw_status torus_render(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* 
     }
     p.final_state = fst;
     p.spectrum = spec;
-    // the wormhole's skyboxes: host cube maps uploaded for this render
-    if (scene->kind == RTW_SCENE_WORMHOLE) {
+    // the skyboxes: host cube maps uploaded for this render
+    if (scene->kind == RTW_SCENE_WORMHOLE || scene->kind == RTW_SCENE_MINKOWSKI_CART_SPHERE) {
         size_t off[2] = {0, 0}, need = 0;
         for (int k = 0; k < 2; ++k)
             if (prm->skybox[k]) {
@@ -2163,7 +2198,8 @@ rtw_status rtw_torus_rhs(const rtw_scene* scene, const double* colors_nm, int32_
                          const double* state, double* slope) {
     if (!scene || !state || !slope ||
         (scene->kind != RTW_SCENE_KERR_SYNCHRO_TORUS && scene->kind != RTW_SCENE_KERR_POWEHI &&
-         scene->kind != RTW_SCENE_SYNCHRO_TEST && scene->kind != RTW_SCENE_WORMHOLE))
+         scene->kind != RTW_SCENE_SYNCHRO_TEST && scene->kind != RTW_SCENE_WORMHOLE &&
+         scene->kind != RTW_SCENE_MINKOWSKI_CART_SPHERE))
         return RTW_ERR_INVALID_PARAM;
     TorusModel m;
     std::string why;

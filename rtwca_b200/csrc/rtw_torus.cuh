@@ -400,6 +400,45 @@ RTW_HD void wormhole_rhs(const WormholeDev& W, const T* z, T* k) {
     k[7] = B(-2) * rpr * kl * kph - B(2) * (cs / sn) * kth * kph;
 }
 
+// ---------------------------------------------------------------------------
+// Minkowski_Sphere_Cartesian.source: flat space in Cartesian (t, x, y, z) and
+// a static blackbody sphere of radius 1 centred on the origin (is_fire
+// :82-90), T = 5778 K (calc_fluid_params! :51-55), a_nu = 1 / map_scale and
+// j_nu = a_nu calc_planck(T, nu) (calc_radiative_coefficients :66-77), at
+// rest (get_source_velocity! :138-145): the frequency shift is k^t.
+// ---------------------------------------------------------------------------
+struct SphereDev {
+    double r_sph;   // radius (map units)
+    double a_nu;    // absorption coefficient (1 / map unit)
+    double es;      // emission_scale
+    double ff_T;    // f_factor / T (nm)
+};
+
+template <class T>
+RTW_HD TorusPt<T> sphere_point(const SphereDev& S, const T* z) {
+    TorusPt<T> o;
+    o.on = false;
+    o.zone = 0;
+    o.cj = T(0.0); o.nus = T(0.0); o.th = T(1.0); o.g = T(1.0);
+    const double xv = (double)val(z[1]), yv = (double)val(z[2]), zv = (double)val(z[3]);
+    if (!(sqrt(xv * xv + yv * yv + zv * zv) <= S.r_sph)) return o;
+    o.g = z[4];
+    o.zone = 1;
+    o.on = true;
+    return o;
+}
+
+// Slopes of bin c without exp(-tau), nu = g nu_c (nm^-1): tau' = -a / g and
+// I' = -(a / g) emission_scale / (exp(f_factor nu / T) - 1) (calc_planck :26-29
+// over nu^3, calc_ray_derivative! integrators_LttM.jl:37-42)
+template <class T>
+RTW_HD void sphere_bin(const SphereDev& S, const TorusPt<T>& P, double nu_nm, T& ft, T& fi) {
+    typedef decltype(val(P.g)) B;
+    const T ag = T(B(S.a_nu)) / P.g;
+    ft = -ag;
+    fi = -(ag * B(S.es)) / (texp(P.g * B(S.ff_T * nu_nm)) - B(1.0));
+}
+
 // Cube-map neighbours (cube_wrap, gen_geometry.jl:128-344). Texel (i, j) of
 // face F, 1-based with n texels per face edge, moved by x texels along i and
 // y along j. A move that leaves the face enters the face across that edge,

@@ -13,8 +13,9 @@ to xyY, normalises brightness and converts to RGB{N0f16}; ``xyz_to_srgb`` gives
 that last step as an informational helper); the wormhole's skybox textures,
 which the reference loads from PNG files that its repository does not hold,
 are arrays the caller hands to ``load_textures``; and ``ray_bundles=True`` (the
-Gaussian footprint lookup of those skyboxes) is built for the wormhole, the
-one scene whose image depends on it, and raises RTW_ERR_UNSUPPORTED elsewhere.
+Gaussian footprint lookup of those skyboxes) is built for the two skybox
+scenes (the wormhole and the Cartesian sphere), whose images depend on it, and
+raises RTW_ERR_UNSUPPORTED elsewhere.
 """
 from __future__ import annotations
 
@@ -249,6 +250,9 @@ _WORLDS = {
     "synch": (abi.SCENE_SYNCHRO_TEST, [0.0, 0.0, 0.0, 0.0], [0.0, 0.0], [PI / 8, 0.0, PI], 0.0),
     # initialization.jl:140-148 (Wormhole.source, coordinates t, l, theta, phi)
     "wormhole": (abi.SCENE_WORMHOLE, [0, 5, PI / 2, 0], [PI / 2, 0], [0.0, 0.0, -PI / 2], 0.0),
+    # initialization.jl:130-138 (Minkowski_Sphere_Cartesian.source, Cartesian t, x, y, z)
+    "minkowski_t,x,y,z_sphere": (abi.SCENE_MINKOWSKI_CART_SPHERE, [0.0, 0.0, 0.0, -4.0], [0.0, 0.0],
+                                 [0.0, 0.0, 0.0], 0.0),
 }
 
 _current: World | None = None
@@ -257,10 +261,12 @@ _textures = (None, None)
 
 
 def load_textures(skybox1=None, skybox2=None):
-    """The wormhole's two skyboxes (load_textures, Wormhole.source/
-    source_model.jl): cube maps in the reference's cross layout, float32
-    [3 h, 4 h, 3] RGB in [0, 1], row 0 at the top; skybox1 lies beyond the
-    throat's positive-l side. gen_image uses them until they are replaced."""
+    """The skybox worlds' textures (load_textures, Wormhole.source/ and
+    Minkowski_Sphere_Cartesian.source/source_model.jl): cube maps in the
+    reference's cross layout, float32 [3 h, 4 h, 3] RGB in [0, 1], row 0 at the
+    top. The wormhole's skybox1 lies beyond the throat's positive-l side; the
+    Cartesian sphere uses skybox1 only. gen_image uses them until they are
+    replaced."""
     global _textures
     _textures = (skybox1, skybox2)
     return _textures
@@ -272,9 +278,8 @@ def available_worlds() -> list:
 
 def initialize_world(input_string: str):
     """Selects a scene and returns its default (position, direction, pointing, beta)
-    (initialization.jl:78-172). The Cartesian sphere (its image is a skybox of
-    the reference's missing textures) is not on this library's path and raises
-    ValueError."""
+    (initialization.jl:78-172). The skybox worlds ("wormhole",
+    "minkowski_t,x,y,z_sphere") take their textures from load_textures."""
     global _current
     key = input_string.lower()
     if key not in _WORLDS:
@@ -319,7 +324,7 @@ def gen_image(*, camera_pos=(0, 0, 0, 0), camera_dir=(0.0, 0.0), speed=0.0, came
     prec = {"fp64": abi.PREC_FP64, "mixed": abi.PREC_MIXED, "fp64_plain": abi.PREC_FP64_PLAIN}[precision]
     integ = {"ref_compat": abi.DP45_REF_COMPAT, "fsal": abi.DP45_FSAL}[integrator]
     want = ("xyz", "class", "steps") + (("spectrum", "state", "tau") if returnrays else ())
-    sky = _textures if _current.scene.kind == abi.SCENE_WORMHOLE else (None, None)
+    sky = _textures if _current.scene.kind in (abi.SCENE_WORMHOLE, abi.SCENE_MINKOWSKI_CART_SPHERE) else (None, None)
     res = r.render(_current.scene, [cam], colors, want=want, precision=prec, integrator=integ,
                    max_dt_scale=max_dt_scale, ray_bundles=ray_bundles, skybox=sky)
     xp, yp = cam.x_pix, cam.y_pix

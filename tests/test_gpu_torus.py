@@ -227,6 +227,70 @@ def test_synchro_parity(renderer, oracle, integrator, precision):
         assert s["class_match"] >= 0.99 and s["frac_within_1e-3"] >= bar, s
 
 
+@pytest.mark.parametrize("integrator", [abi.DP45_REF_COMPAT, abi.DP45_FSAL])
+@pytest.mark.parametrize("precision", [abi.PREC_FP64, abi.PREC_MIXED])
+def test_cart_sphere_parity(renderer, oracle, integrator, precision):
+    """The reference's "minkowski_t,x,y,z_sphere" world (a blackbody sphere in
+    flat Cartesian space) through the per-bin kernel's flat geometry and its
+    sphere emitter, against the oracle; Synchro_Test's bars."""
+    from tests.parity import summarize
+    sc = configs.cart_sphere_scene()
+    cam = configs.cart_sphere_camera(32, 1e-6)
+    col = np.array([450.0, 550.0, 650.0])
+    ref = oracle.render(sc, cam, col, integrator=integrator)
+    g = renderer.render(sc, [cam], col, want=("xyz", "class", "steps", "spectrum"), precision=precision,
+                        integrator=integrator)
+    s = summarize(g, ref)
+    print("cart sphere", integrator, precision, s)
+    assert np.any(ref["xyz"][:, 1] > 0) and np.any(ref["xyz"][:, 1] == 0)  # the sphere and empty space
+    if precision == abi.PREC_FP64:
+        assert s["class_match"] >= 0.999 and s["frac_within_1e-3"] >= 0.999, s
+    else:
+        bar = 0.98 if integrator == abi.DP45_FSAL else 0.95
+        assert s["class_match"] >= 0.99 and s["frac_within_1e-3"] >= bar, s
+
+
+@pytest.mark.parametrize("precision", [abi.PREC_FP64, abi.PREC_MIXED])
+def test_cart_sphere_skybox_and_bundles(renderer, oracle, precision):
+    """The Cartesian sphere in front of its skybox (skybox 1, added at every
+    ray's end, attenuated by the sphere), with and without ray bundles, against
+    the oracle with a synthetic 16-texel cube map: >= 99.9 % of the pixels
+    within 1e-3 in every bin (FP64), >= 95 % (FP32-mixed)."""
+    rng = np.random.default_rng(9)
+    H = 16
+    sky1 = rng.uniform(0, 1, (3 * H, 4 * H, 3)).astype(np.float32)
+    sc = configs.cart_sphere_scene()
+    cam = configs.cart_sphere_camera(32, 1e-6)
+    col = np.array([467.0, 532.0, 630.0])
+    for bundles in (False, True):
+        ref = oracle.render(sc, cam, col, integrator=abi.DP45_FSAL, skybox=(sky1, None), ray_bundles=bundles,
+                            want=("spectrum",))
+        g = renderer.render(sc, [cam], col, want=("spectrum",), precision=precision, integrator=abi.DP45_FSAL,
+                            skybox=(sky1, None), ray_bundles=bundles)
+        assert np.all(ref["spectrum"] > 0)
+        e = np.abs(g["spectrum"].astype(np.float64) - ref["spectrum"]) / ref["spectrum"]
+        ok = np.mean(np.all(e <= 1e-3, axis=1))
+        print("cart sphere skybox", precision, bundles, ok, e.max())
+        assert ok >= (0.999 if precision == abi.PREC_FP64 else 0.95), (bundles, ok, e.max())
+
+
+def test_cart_sphere_world_through_gen_image():
+    """initialize_world("minkowski_t,x,y,z_sphere") + load_textures +
+    gen_image(ray_bundles=True): the reference's keyword path."""
+    from rtwca_b200 import render as R
+    rng = np.random.default_rng(4)
+    sky1 = rng.uniform(0, 1, (48, 64, 3)).astype(np.float32)
+    pos, d, pt, beta = R.initialize_world("minkowski_t,x,y,z_sphere")
+    assert list(pos) == [0.0, 0.0, 0.0, -4.0]
+    R.load_textures(sky1, None)
+    try:
+        img = R.gen_image(camera_pos=pos, camera_dir=d, speed=beta, camera_point=pt, x_pix=16, tolerance=1e-6,
+                          max_steps=2e4, colors=(467, 532, 630), ray_bundles=True, integrator="fsal")
+        assert img.shape[1] == 16 and np.all(np.isfinite(img)) and np.all(img[:, :, 1] > 0)
+    finally:
+        R.load_textures(None, None)
+
+
 def test_synch_world_through_gen_image():
     """initialize_world("synch") + gen_image: the reference's world defaults,
     Cartesian camera at the origin (no coordinate singularity there)."""

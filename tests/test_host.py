@@ -40,11 +40,10 @@ def test_workloads_shapes():
 
 def test_worlds_table():
     worlds = render.available_worlds()
-    for w in ("kerr_boyer_lindquist", "m87", "synch", "wormhole"):
+    for w in ("kerr_boyer_lindquist", "m87", "synch", "wormhole", "minkowski_t,x,y,z_sphere"):
         assert w in worlds
-    # the Cartesian sphere's image is a skybox of the reference's missing textures
     with pytest.raises(ValueError):
-        render.initialize_world("minkowski_t,x,y,z_sphere")
+        render.initialize_world("no such world")
 
 
 class FakeRenderer:

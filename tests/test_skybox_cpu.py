@@ -3,7 +3,9 @@ rule (the function the device's ray-bundle footprint runs, evaluated on the
 host) against the oracle's separately written restatement of cube_wrap
 (gen_geometry.jl:128-344) over every texel, face and footprint offset, and
 properties of the oracle's ray-bundle lookup (calc_skybox_I_nu_beam!,
-Wormhole.source/source_model.jl:266-358).
+Wormhole.source/source_model.jl:266-358), and the oracle's Cartesian
+blackbody sphere (Minkowski_Sphere_Cartesian.source) against the closed form
+of a straight ray through it.
 """
 import ctypes as C
 
@@ -103,3 +105,35 @@ def test_oracle_bundle_lookup_small_maps(oracle, H):
     r = oracle.render(sc, cam, col, integrator=abi.DP45_FSAL, skybox=sky, ray_bundles=True,
                       pixel_ids=np.arange(0, 96, 7), want=("spectrum",))
     assert np.all(np.isfinite(r["spectrum"])) and np.all(r["spectrum"] > 0)
+
+
+def test_oracle_cart_sphere_closed_form(oracle):
+    """The Cartesian blackbody sphere in the oracle against the closed form of
+    a straight ray through a uniform, optically thin sphere at rest: tau is the
+    chord 2 sqrt(r^2 - b^2) (a_nu = 1, k^t = 1) and I_c = B_c (1 - exp(-tau)),
+    B_c = emission_scale / (exp(f_factor nu_c / T) - 1); rays that miss it stay
+    dark without a skybox; with one, every ray adds the skybox texel it points
+    at, attenuated by exp(-tau)."""
+    sc = configs.cart_sphere_scene()
+    cam = configs.cart_sphere_camera(24, 1e-8)
+    col = np.array([450.0, 550.0, 650.0])
+    x0 = oracle.camera_rays(sc, cam)
+    p0, d = x0[:, 1:4], x0[:, 5:8] / x0[:, 4:5]
+    d = d / np.linalg.norm(d, axis=1, keepdims=True)
+    b2 = np.sum(p0 * p0, axis=1) - np.sum(p0 * d, axis=1) ** 2  # squared impact parameter
+    chord = 2 * np.sqrt(np.maximum(0.0, 1.0 - b2))
+    r = oracle.render(sc, cam, col, integrator=abi.DP45_FSAL, want=("spectrum", "tau", "class"))
+    assert np.all(r["class"] == abi.CLASS_ESCAPE)
+    es, ff = oracle.constants()
+    B = es / np.expm1(ff / col / 5778.0)
+    hit = chord > 0.05
+    assert hit.sum() > 20 and (~hit).sum() > 20
+    np.testing.assert_allclose(r["tau"][hit], np.repeat(chord[hit, None], 3, 1), rtol=2e-3, atol=2e-4)
+    np.testing.assert_allclose(r["spectrum"][hit], B * -np.expm1(-r["tau"][hit]), rtol=1e-5)
+    assert np.all(r["spectrum"][chord == 0] == 0) and np.all(r["tau"][chord == 0] == 0)
+    H = 8
+    flat = np.full((3 * H, 4 * H, 3), 0.5, np.float32)
+    s = oracle.render(sc, cam, col, integrator=abi.DP45_FSAL, skybox=(flat, None), want=("spectrum", "tau"))
+    sky = (s["spectrum"] - r["spectrum"]) / np.exp(-r["tau"])
+    np.testing.assert_allclose(sky, np.repeat(sky[:1], len(sky), 0), rtol=1e-9)  # one colour, k^t = 1
+    assert np.all(sky > 0)

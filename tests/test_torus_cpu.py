@@ -211,6 +211,34 @@ def test_synchro_rhs_matches_oracle(oracle):
     assert inside == 12  # the four points inside the cylinder emit, the two outside do not
 
 
+def test_cart_sphere_rhs_matches_oracle(oracle):
+    """The Cartesian blackbody sphere (Minkowski_Sphere_Cartesian.source):
+    defaults, and the library's per-bin right-hand side against the oracle's
+    generic calc_ray_derivative! with its is_fire and calc_planck, inside and
+    outside the sphere; tau' = -a_nu / k^t exactly."""
+    sc = configs.cart_sphere_scene()
+    assert sc.kind == abi.SCENE_MINKOWSKI_CART_SPHERE
+    assert (sc.r_out, sc.temperature, sc.a_nu, sc.escape_radius) == (1.0, 5778.0, 1.0, 100.0)
+    col = np.array([380.0, 450.0, 550.0, 650.0, 750.0])
+    rng = np.random.default_rng(4)
+    inside = 0
+    for x, y, z in [(0.0, 0.0, 0.0), (0.5, -0.3, 0.6), (-0.1, 0.2, -0.95), (0.9, 0.5, 0.0), (0.0, 0.0, -4.0),
+                    (30.0, -40.0, 2.0)]:
+        for _ in range(3):
+            st = _cart_state(col.size, x, y, z, rng)
+            st[4] = rng.uniform(0.5, 2.0)  # k^t: the frequency shift
+            ref = oracle.rhs(sc, col, st)
+            f = abi.torus_rhs(sc, col, st, 0)
+            assert np.array_equal(f[:4], st[4:8]) and np.all(f[4:8] == 0)  # straight lines
+            scale = 1e-300 + 1e-12 * np.abs(ref[8:]).max()
+            err = np.abs(f[8:] - ref[8:]) / np.maximum(np.abs(ref[8:]), scale)
+            assert err.max() < 1e-11, (x, y, z, err.max())
+            if np.any(ref[8:] != 0):
+                inside += 1
+                assert np.array_equal(f[9::2], np.full(col.size, -1.0 / st[4]))
+    assert inside == 9  # the three points inside the sphere emit, (0.9, 0.5, 0) and the others do not
+
+
 def test_wormhole_rhs_matches_oracle(oracle):
     """The Dneg wormhole (Wormhole.source): the library's geodesic right-hand
     side against the oracle's Christoffel contraction, in the throat, near it
