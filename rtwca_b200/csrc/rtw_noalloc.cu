@@ -119,7 +119,7 @@ extern "C" rtw_status rtw_render_noalloc(const rtw_scene* scene, const rtw_camer
         return fail(RTW_ERR_INVALID_PARAM, "n_cams must be 1..RTW_NOALLOC_MAX_FRAMES");
     if (prm->n_colors <= 0 || prm->n_colors > RTW_MAX_BINS || !prm->colors_nm)
         return fail(RTW_ERR_INVALID_PARAM, "n_colors must be 1..128 with colors_nm set");
-    if (prm->ray_bundles) return fail(RTW_ERR_UNSUPPORTED, "ray bundles are not built");
+    if (prm->ray_bundles) return fail(RTW_ERR_UNSUPPORTED, "ray bundles are built for the skybox scenes only");
     if (scene->ref_precision) return fail(RTW_ERR_UNSUPPORTED, "ref_precision is an oracle-only switch");
     if (prm->precision != RTW_PREC_FP64 && prm->precision != RTW_PREC_MIXED) return fail(RTW_ERR_INVALID_PARAM, "precision");
     if (prm->integrator != RTW_DP45_REF_COMPAT && prm->integrator != RTW_DP45_FSAL)
