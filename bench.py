@@ -523,7 +523,12 @@ def run_b200(args):
         adjoint = adjoint_leg(r, args.adjoint_x_pix, world, rank)
     scenes = None
     if not args.no_scenes:
-        scenes = scenes_leg(r, rank, cpu=not args.no_cpu_baseline)
+        # no collectives in this leg: a failure in it is reported in the line
+        # instead of ending the run before the headline's end-to-end leg
+        try:
+            scenes = scenes_leg(r, rank, cpu=not args.no_cpu_baseline)
+        except Exception as exc:
+            scenes = {"error": f"{type(exc).__name__}: {exc}"[:400]}
 
     # end to end through the public API: host pinned outputs, synchronous call
     hx = torch.empty((P, 3), dtype=torch.float32, pin_memory=True)
