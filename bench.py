@@ -45,7 +45,7 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=2048, help="rays in the CPU baseline sample")
     ap.add_argument("--no-batched", action="store_true", help="skip the 96-frame batched leg")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the synchrotron-torus adjoint leg")
-    ap.add_argument("--no-scenes", action="store_true", help="skip the Powehi / Synchro_Test scene leg")
+    ap.add_argument("--no-scenes", action="store_true", help="skip the Powehi / Synchro_Test / wormhole scene leg")
     ap.add_argument("--no-plain-leg", action="store_true", help="skip the plain FP64 GPU path leg")
     ap.add_argument("--adjoint-x-pix", type=int, default=512)
     ap.add_argument("--block-warps", type=int, default=0)
@@ -320,8 +320,8 @@ def batched_leg(r, world, rank, stream, barrier_fn):
 
 
 def scenes_leg(r, rank, cpu=True):
-    """The reference's two per-bin power-law synchrotron scenes through the
-    per-bin kernels, each at 1024 px wide with the reference's default field
+    """Three of the reference's per-bin scenes through the per-bin kernels,
+    each at 1024 px wide with the reference's default field
     of view and colours (400/550/700 nm), tolerance 1e-6: Powehi ("m87": Kerr
     a = 0.9, disk + jet) and Synchro_Test ("synch": flat Cartesian space,
     camera inside the cylinder), and the Dneg wormhole ("wormhole", two
