@@ -63,6 +63,19 @@ def test_cube_wrap_properties(rtwlib):
     assert wrap(4, 1, 2, 0, -1, n)[2] == 5
 
 
+def test_cube_wrap_rejects_bad_arguments(rtwlib, oracle):
+    """A face outside 1..6, a face edge under 1 texel or no output buffer is
+    RTW_ERR_INVALID_PARAM from the library's hook and the oracle's."""
+    f = rtwlib.rtw_skybox_wrap
+    out = (C.c_int32 * 3)()
+    assert f(1, 1, 0, 0, 0, 4, out) == abi.ERR_INVALID_PARAM
+    assert f(1, 1, 7, 0, 0, 4, out) == abi.ERR_INVALID_PARAM
+    assert f(1, 1, 1, 0, 0, 0, out) == abi.ERR_INVALID_PARAM
+    assert f(1, 1, 1, 0, 0, 4, None) == abi.ERR_INVALID_PARAM
+    with pytest.raises(RuntimeError):
+        oracle.cube_wrap(1, 1, 9, 0, 0, 4)
+
+
 def _wormhole_case(H, seed):
     rng = np.random.default_rng(seed)
     sky = tuple(rng.uniform(0, 1, (3 * H, 4 * H, 3)).astype(np.float32) for _ in range(2))
