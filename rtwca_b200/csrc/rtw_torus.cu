@@ -77,12 +77,12 @@ struct TorusModel {
     PowehiDev pw;
     SynchroDev sy;
     WormholeDev wh;
-    SphereDev sp;
     TorusBin bins[kTorusMaxBins];
     int n;         // bins
     int emitter;   // 0: synchrotron torus, 1: Powehi (disk + jet), 2: Synchro_Test cylinder, 3: none (wormhole),
                    // 4: the Cartesian blackbody sphere
     int geom;      // geometry: 0 Kerr (Boyer-Lindquist), 1 Minkowski (Cartesian), 2 Dneg wormhole
+    SphereDev sp;
 };
 
 // The scene's emitter at a stage point z (x^mu, k^mu) and the slopes of bin c.
@@ -131,14 +131,16 @@ RTW_HD void torus_geo_rhs(const TorusModel& m, const double* y, double* f) {
     for (int i = 0; i < 8; ++i) f[i] = k[i];
 }
 
-// FP64 right-hand side on a state y[8 + 2N] = (x^mu, k^mu, tau_c, I_c).
+// FP64 right-hand side on a state y[8 + 2N] = (x^mu, k^mu, tau_c, I_c)
+// (EM: the emitter as in em_point; the forward kernels pass their own).
+template <int EM = -1>
 RTW_HD void torus_f64(const TorusModel& m, const double* y, double* f) {
     const int N = m.n;
     torus_geo_rhs(m, y, f);
-    const TorusPt<double> S = em_point<double>(m, y);
+    const TorusPt<double> S = em_point<double, EM>(m, y);
     for (int c = 0; c < N; ++c) {
         double ft = 0, fi = 0;
-        if (S.on) em_bin<double>(m, S, c, ft, fi);
+        if (S.on) em_bin<double, EM>(m, S, c, ft, fi);
         f[8 + c] = ft;
         f[8 + N + c] = fi * exp(-y[8 + c]);
     }
@@ -746,6 +748,12 @@ __device__ __noinline__ void torus_rec_end(const TorusKP& p, TorusRec* r, long l
 template <bool MIXED, int EM>
 __global__ void __launch_bounds__(128, MIXED ? 3 : 2) torus_forward(const TorusKP p) {
     constexpr bool FLAT = EM == 2 || EM == 4;  // Synchro_Test, the sphere: flat Cartesian geometry
+    // the FP64 slope at a ray's start and after escapes: the instance's own
+    // emitter on the mixed path (ptxas: the torus, Powehi and wormhole
+    // instances then spill 32-124 B per thread instead of 318-326 with the
+    // run-time dispatch), the run-time dispatch on the FP64 path (where the
+    // instance's own emitter raised Synchro_Test's spills from 132 B to 496 B)
+    constexpr int KEM = MIXED ? EM : -1;
     typedef typename SpecTraits<MIXED>::SR SR;
     const int N = p.m.n;
     const int D = 8 + 2 * N;
@@ -765,7 +773,7 @@ __global__ void __launch_bounds__(128, MIXED ? 3 : 2) torus_forward(const TorusK
             double y[8 + 2 * kTorusMaxBins], f[8 + 2 * kTorusMaxBins];
             for (int i = 0; i < 8; ++i) y[i] = x[i];
             for (int i = 8; i < D; ++i) y[i] = 0;
-            torus_f64(p.m, y, f);
+            torus_f64<KEM>(p.m, y, f);
             for (int i = 0; i < 8; ++i) k1[i] = SR(f[i]);
             for (int c = 0; c < N; ++c) {
                 tau[c] = 0; ihi[c] = 0; ilo[c] = 0;
@@ -829,7 +837,7 @@ __global__ void __launch_bounds__(128, MIXED ? 3 : 2) torus_forward(const TorusK
                 for (int it = 0; it < 37; ++it) {
                     if (it > 0) {
                         if (torus_terminate<double, EM>(p, y, y + 8, N)) continue;
-                        torus_f64(p.m, y, f);
+                        torus_f64<KEM>(p.m, y, f);
                     }
                     for (int i = 0; i < D; ++i) y[i] -= temp * f[i];
                     torus_keep(y);
@@ -848,7 +856,7 @@ __global__ void __launch_bounds__(128, MIXED ? 3 : 2) torus_forward(const TorusK
                     done = true;
                     prev_rej = false;
                 } else {
-                    torus_f64(p.m, y, f);
+                    torus_f64<KEM>(p.m, y, f);
                     for (int i = 0; i < 8; ++i) k1[i] = SR(f[i]);
                     for (int q = 0; q < N; ++q) {
                         kt1[q] = SR(f[8 + q]);
@@ -976,7 +984,7 @@ __global__ void __launch_bounds__(128, MIXED ? 3 : 2) torus_forward(const TorusK
                             yy[8 + q] = (double)tau[q];
                             yy[8 + N + q] = (double)ihi[q] + (MIXED ? (double)ilo[q] : 0.0);
                         }
-                        torus_f64(p.m, yy, ff);
+                        torus_f64<KEM>(p.m, yy, ff);
                         for (int i = 0; i < 8; ++i) k1[i] = SR(ff[i]);
                         for (int q = 0; q < N; ++q) {
                             kt1[q] = SR(ff[8 + q]);
