@@ -45,7 +45,7 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=2048, help="rays in the CPU baseline sample")
     ap.add_argument("--no-batched", action="store_true", help="skip the 96-frame batched leg")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the synchrotron-torus adjoint leg")
-    ap.add_argument("--no-scenes", action="store_true", help="skip the Powehi / Synchro_Test / wormhole scene leg")
+    ap.add_argument("--no-scenes", action="store_true", help="skip the per-bin scene leg (Powehi, Synchro_Test, wormhole, Cartesian sphere)")
     ap.add_argument("--no-plain-leg", action="store_true", help="skip the plain FP64 GPU path leg")
     ap.add_argument("--adjoint-x-pix", type=int, default=512)
     ap.add_argument("--block-warps", type=int, default=0)
@@ -320,13 +320,14 @@ def batched_leg(r, world, rank, stream, barrier_fn):
 
 
 def scenes_leg(r, rank, cpu=True):
-    """Three of the reference's per-bin scenes through the per-bin kernels,
+    """Four of the reference's per-bin scenes through the per-bin kernels,
     each at 1024 px wide with the reference's default field
     of view and colours (400/550/700 nm), tolerance 1e-6: Powehi ("m87": Kerr
     a = 0.9, disk + jet) and Synchro_Test ("synch": flat Cartesian space,
-    camera inside the cylinder), and the Dneg wormhole ("wormhole", two
+    camera inside the cylinder), the Dneg wormhole ("wormhole", two
     synthetic 64-texel cube maps from numpy default_rng(0) standing in for the
-    reference's missing skybox PNGs). FP32-mixed and FP64, the reference's step.
+    reference's missing skybox PNGs) and the Cartesian blackbody sphere
+    ("minkowski_t,x,y,z_sphere", the first of those maps as its skybox). FP32-mixed and FP64, the reference's step.
     Device time of the kernel (1 warm-up + 3 timed renders, mean); on rank 0
     the FP64 oracle on 4096 evenly spaced pixels on all host cores gives the
     CPU rate and a parity sample (linear Y within 1e-3)."""
@@ -342,7 +343,9 @@ def scenes_leg(r, rank, cpu=True):
     sky = tuple(rng.uniform(0, 1, (3 * 64, 4 * 64, 3)).astype(np.float32) for _ in range(2))
     for name, sc, camf, kw in (("m87_powehi", configs.powehi_scene(), configs.powehi_camera, {}),
                                ("synch_synchro_test", configs.synchro_scene(), configs.synchro_camera, {}),
-                               ("wormhole", configs.wormhole_scene(), configs.wormhole_camera, {"skybox": sky})):
+                               ("wormhole", configs.wormhole_scene(), configs.wormhole_camera, {"skybox": sky}),
+                               ("minkowski_cart_sphere", configs.cart_sphere_scene(), configs.cart_sphere_camera,
+                                {"skybox": (sky[0], None)})):
         cam = camf(1024, 1e-6)
         P = cam.x_pix * cam.y_pix
         leg = {"workload": f"{name} {cam.x_pix}x{cam.y_pix}, 3 bins 400/550/700 nm, tol 1e-6, reference step"}
