@@ -5,7 +5,8 @@ tests pin no numerical results, so the fixtures come from the oracle (the
 FP64 restatement of the reference's CPU integrator), pinned itself by
 tests/test_oracle_physics.py and tests/test_ref_integrator.py. Small cases:
 10x10 pixels (flat sphere 16x16, thick disk 8x8), 8 spectral bins, tolerance 1e-8, both step
-modes; and the per-bin scenes (PERBIN below). Run: python tests/golden/make_golden.py
+modes; the per-bin scenes (PERBIN below); the skybox scenes (SKYBOX below).
+Run: python tests/golden/make_golden.py (all), or with --skybox (the skybox scenes).
 """
 import sys
 from pathlib import Path
@@ -25,6 +26,22 @@ N_COLORS = 8
 # ("synch" camera, 16 px wide, 3 bins), both steps, tolerance 1e-6; the
 # synchrotron torus (8 x 8, 4 bins, tolerance 1e-8, FSAL only)
 PERBIN = {"powehi": ("ref", "fsal"), "synchro_test": ("ref", "fsal"), "synchrotron_torus": ("fsal",)}
+
+
+# the skybox scenes, with synthetic 8-texel cube maps (the reference's PNGs are
+# not in its repository); the oracle side only for now
+SKYBOX = {"wormhole_bundles": ("fsal",), "cart_sphere": ("ref", "fsal"), "cart_sphere_bundles": ("fsal",)}
+
+
+def skybox_case(name):
+    """(scene, camera, colours, skyboxes, ray_bundles) of a skybox fixture."""
+    rng = np.random.default_rng(12)
+    sky = tuple(rng.uniform(0, 1, (24, 32, 3)).astype(np.float32) for _ in range(2))
+    col = np.array([467.0, 532.0, 630.0])
+    if name == "wormhole_bundles":
+        return configs.wormhole_scene(), configs.wormhole_camera(12, 1e-6), col, sky, True
+    return (configs.cart_sphere_scene(), configs.cart_sphere_camera(12, 1e-6), col, (sky[0], None),
+            name == "cart_sphere_bundles")
 
 
 def perbin_case(name):
@@ -61,7 +78,21 @@ def main():
                                 steps=res["steps"], spectrum=res["spectrum"], tau=res["tau"][:, 0],
                                 state=res["state"])
             print(name, tag, np.bincount(res["class"], minlength=7).tolist())
+    skybox_main()
+
+
+def skybox_main():
+    O.build()
+    for name, tags in SKYBOX.items():
+        for tag in tags:
+            integ = abi.DP45_REF_COMPAT if tag == "ref" else abi.DP45_FSAL
+            scene, cam, colors, sky, bundles = skybox_case(name)
+            res = O.render(scene, cam, colors, integrator=integ, skybox=sky, ray_bundles=bundles)
+            np.savez_compressed(HERE / f"{name}_{tag}.npz", colors=colors, xyz=res["xyz"], term_class=res["class"],
+                                steps=res["steps"], spectrum=res["spectrum"], tau=res["tau"][:, 0],
+                                state=res["state"])
+            print(name, tag, np.bincount(res["class"], minlength=7).tolist())
 
 
 if __name__ == "__main__":
-    main()
+    skybox_main() if sys.argv[1:] == ["--skybox"] else main()

@@ -70,6 +70,29 @@ def test_oracle_reproduces_perbin_golden(oracle, name, tag):
     assert np.allclose(r["state"], g["state"], rtol=1e-12, atol=1e-300)
 
 
+from tests.golden.make_golden import SKYBOX, skybox_case  # noqa: E402
+
+SKYBOX_CASES = [(n, t) for n, tags in sorted(SKYBOX.items()) for t in tags]
+
+
+@pytest.mark.parametrize("name,tag", SKYBOX_CASES)
+def test_oracle_reproduces_skybox_golden(oracle, name, tag):
+    """The skybox scenes (the wormhole with ray bundles, the Cartesian sphere
+    with and without) with their synthetic cube maps: the oracle against its
+    committed fixtures. The GPU is held to the oracle on these scenes directly
+    (tests/test_gpu_torus.py)."""
+    g = load(name, tag)
+    scene, cam, colors, sky, bundles = skybox_case(name)
+    integ = abi.DP45_REF_COMPAT if tag == "ref" else abi.DP45_FSAL
+    assert np.array_equal(colors, g["colors"])
+    r = oracle.render(scene, cam, colors, integrator=integ, skybox=sky, ray_bundles=bundles)
+    assert np.array_equal(r["class"], g["class"])
+    assert np.array_equal(r["steps"], g["steps"])
+    assert np.all(g["spectrum"] > 0)
+    assert np.allclose(r["spectrum"], g["spectrum"], rtol=1e-12, atol=0)
+    assert np.allclose(r["state"], g["state"], rtol=1e-12, atol=1e-300)
+
+
 # (the torus fixture is at tolerance 1e-8, below what FP32 stages resolve; the
 # FP32-mixed torus is checked at 1e-6 in test_gpu_torus)
 PERBIN_GPU = [(n, t, p) for n, t in PERBIN_CASES for p in (abi.PREC_FP64, abi.PREC_MIXED)
