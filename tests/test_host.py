@@ -84,3 +84,29 @@ def test_bench_cpu_sample_ids():
     ids = bench.cpu_sample_ids(1024 * 1024, 2048)
     assert ids.size == 2048 and ids[0] == 0 and ids[-1] == 1024 * 1024 - 1
     assert np.all(np.diff(ids) > 0)
+
+
+def test_gen_image_passes_textures_to_skybox_worlds():
+    """load_textures' maps reach the render call for the two skybox worlds,
+    with ray_bundles, and no other world gets them."""
+    seen = {}
+
+    class Spy(FakeRenderer):
+        def render(self, scene, cams, colors, want, **kw):
+            seen["skybox"], seen["bundles"] = kw.get("skybox"), kw.get("ray_bundles")
+            return super().render(scene, cams, colors, want, **kw)
+
+    maps = (np.zeros((6, 8, 3), np.float32), np.ones((6, 8, 3), np.float32))
+    render.load_textures(*maps)
+    try:
+        for world in ("wormhole", "minkowski_t,x,y,z_sphere", "synch"):
+            pos, d, pt, beta = render.initialize_world(world)
+            render.gen_image(camera_pos=pos, camera_dir=d, speed=beta, camera_point=pt, x_pix=4, ray_bundles=True,
+                             renderer=Spy())
+            if world == "synch":
+                assert seen["skybox"] == (None, None)
+            else:
+                assert seen["skybox"][0] is maps[0] and seen["skybox"][1] is maps[1]
+            assert seen["bundles"] is True
+    finally:
+        render.load_textures(None, None)
