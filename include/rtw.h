@@ -504,9 +504,15 @@ rtw_status rtw_scene_rhs(const rtw_scene* scene, int32_t fp32, const double* sta
  * resident warps, so it runs slower than rtw_render. Larger requests return
  * RTW_ERR_INVALID_PARAM (text in rtw_noalloc_last_error). Runs on the current
  * device and on params->stream (NULL: default stream, returns when done).
+ * block_warps, ctas_per_sm and refill_min are honoured as rtw_render takes
+ * them; graph, autotune and trace_ray >= 0 need a context and return
+ * RTW_ERR_UNSUPPORTED. The frame and bin tables travel as kernel parameters,
+ * so the call reads no host memory after it returns.
  * Calls share the arrays: calls that overlap on the GPU race; serialise them.
  * The first call on a device looks up the arrays' addresses
- * (cudaGetSymbolAddress); make it before any stream capture. */
+ * (cudaGetSymbolAddress) and caches them; make it before any stream capture.
+ * The cache does not survive cudaDeviceReset: do not call this entry point
+ * again in a process after a reset of its device. */
 rtw_status rtw_render_noalloc(const rtw_scene* scene, const rtw_camera* cams, int32_t n_cams,
                               const rtw_render_params* params, rtw_outputs* out);
 /* Text of the calling thread's last rtw_render_noalloc error ("" if none). */

@@ -18,12 +18,20 @@
 //
 // Every call shares the arrays: calls that overlap on the GPU (two streams,
 // two host threads) race and corrupt each other; serialise them. Each call
-// zeroes the work counter and rewrites the frame and bin tables before its
-// launch; the kernel initialises a ray's spectral row when it starts the ray.
+// zeroes the work counter and the counters and rewrites the frame and bin
+// tables before its trace launch; the kernel initialises a ray's spectral row
+// when it starts the ray.
+//
+// The tables reach the device as the by-value parameters of a one-CTA upload
+// kernel (a launch copies its parameters when it is enqueued), so the call
+// reads no host memory after it returns.
 //
 // The first call on a device looks up the device addresses of the arrays
 // (cudaGetSymbolAddress, with that device current) and caches them; make that
-// first call before any stream capture.
+// first call before any stream capture. The cached addresses belong to the
+// device's primary context as it was then: after cudaDeviceReset the module
+// may load elsewhere, so this entry point must not be used again in that
+// process.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -51,6 +59,24 @@ static __device__ __align__(256) FrameDesc g_noalloc_frames[RTW_NOALLOC_MAX_FRAM
 static __device__ __align__(256) double g_noalloc_bins[4 * RTW_MAX_BINS];
 // [0] work counter, [1..] DevStats
 static __device__ __align__(256) unsigned long long g_noalloc_ctl[32];
+
+// What one call uploads: the frame table (first n_frames entries used) and
+// the bin table. About 20 KB, within the 32 KB kernel-parameter limit.
+struct NoallocTables {
+    FrameDesc frames[RTW_NOALLOC_MAX_FRAMES];
+    double bins[4 * RTW_MAX_BINS];
+    int n_frames;
+};
+static_assert(sizeof(NoallocTables) <= 32000, "upload tables exceed the kernel-parameter limit");
+
+// One CTA: copies the tables into the arrays and zeroes the work counter and
+// the counters.
+__global__ void __launch_bounds__(256) noalloc_upload(const NoallocTables t) {
+    const int i = threadIdx.x;
+    if (i < t.n_frames) g_noalloc_frames[i] = t.frames[i];
+    for (int k = i; k < 4 * RTW_MAX_BINS; k += blockDim.x) g_noalloc_bins[k] = t.bins[k];
+    if (i < 32) g_noalloc_ctl[i] = 0ull;
+}
 
 namespace {
 
@@ -121,6 +147,8 @@ extern "C" rtw_status rtw_render_noalloc(const rtw_scene* scene, const rtw_camer
         return fail(RTW_ERR_INVALID_PARAM, "n_colors must be 1..128 with colors_nm set");
     if (prm->ray_bundles) return fail(RTW_ERR_UNSUPPORTED, "ray bundles are built for the skybox scenes only");
     if (scene->ref_precision) return fail(RTW_ERR_UNSUPPORTED, "ref_precision is an oracle-only switch");
+    if (prm->graph || prm->autotune || prm->trace_ray >= 0)
+        return fail(RTW_ERR_UNSUPPORTED, "graph, autotune and trace_ray need an rtw_ctx (use rtw_render)");
     if (prm->precision != RTW_PREC_FP64 && prm->precision != RTW_PREC_MIXED) return fail(RTW_ERR_INVALID_PARAM, "precision");
     if (prm->integrator != RTW_DP45_REF_COMPAT && prm->integrator != RTW_DP45_FSAL)
         return fail(RTW_ERR_INVALID_PARAM, "integrator");
@@ -136,15 +164,16 @@ extern "C" rtw_status rtw_render_noalloc(const rtw_scene* scene, const rtw_camer
     rtw_status st = symbols(dev, sym);
     if (st != RTW_OK) return st;
 
-    // host-side tables (stack / host heap only; no device allocation)
-    FrameDesc frames[RTW_NOALLOC_MAX_FRAMES];
+    // host-side tables (on the stack; they travel as the upload kernel's parameters)
+    NoallocTables tab;
+    std::memset(&tab, 0, sizeof(tab));
+    tab.n_frames = n_cams;
     int64_t total = 0;
-    st = rtw_prepare_frames(scene, cams, n_cams, frames, &total);
+    st = rtw_prepare_frames(scene, cams, n_cams, tab.frames, &total);
     if (st == RTW_ERR_INVALID_CAMERA) return fail(st, "a camera is on a coordinate singularity");
     if (st != RTW_OK) return fail(st, "camera parameters invalid or non-finite");
     const int N = prm->n_colors;
-    double bins[4 * RTW_MAX_BINS];
-    std::memset(bins, 0, sizeof(bins));
+    double* bins = tab.bins;
     double wx[RTW_MAX_BINS], wy[RTW_MAX_BINS], wz[RTW_MAX_BINS], fac[RTW_MAX_BINS];
     if (rtw_cie_weights(prm->colors_nm, N, wx, wy, wz, fac) != RTW_OK)
         return fail(RTW_ERR_INVALID_PARAM, "colors_nm must be positive");
@@ -156,12 +185,14 @@ extern "C" rtw_status rtw_render_noalloc(const rtw_scene* scene, const rtw_camer
     }
     const int np = N <= 32 ? 32 : (N <= 64 ? 64 : 128);
 
-    // launch shape: as many warps as the kernel keeps resident, capped by the scratch
+    // launch shape: as many warps as the kernel keeps resident (or ctas_per_sm
+    // CTAs per SM when given), capped by the scratch
     const int warps = prm->block_warps > 0 ? (prm->block_warps < 4 ? prm->block_warps : 4) : 4;
     const int block = 32 * warps;
-    int occ = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, noalloc_kernel(scene->kind, prm->precision, np), block, 0) !=
-        cudaSuccess)
+    int occ = prm->ctas_per_sm;
+    if (occ <= 0 &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, noalloc_kernel(scene->kind, prm->precision, np), block, 0) !=
+            cudaSuccess)
         return fail(RTW_ERR_CUDA, "occupancy query failed");
     const size_t per_warp = spec_bytes_per_warp(prm->precision, np);
     const long long fit = (long long)(RTW_NOALLOC_SCRATCH_BYTES / (per_warp * warps));
@@ -202,17 +233,15 @@ extern "C" rtw_status rtw_render_noalloc(const rtw_scene* scene, const rtw_camer
     p.trace = nullptr;
     p.trace_gid = -1;
     p.trace_cap = 0;
+    // compaction interval as rtw_render takes it (0: 1)
+    p.refill_min = prm->refill_min > 0 ? (prm->refill_min < 32 ? prm->refill_min : 32) : 1;
 
     cudaStream_t stream = static_cast<cudaStream_t>(prm->stream);
-    if (cudaMemcpyAsync(sym->frames, frames, sizeof(FrameDesc) * n_cams, cudaMemcpyHostToDevice, stream) != cudaSuccess ||
-        cudaMemcpyAsync(sym->bins, bins, sizeof(bins), cudaMemcpyHostToDevice, stream) != cudaSuccess ||
-        cudaMemsetAsync(sym->ctl, 0, sizeof(unsigned long long) * 32, stream) != cudaSuccess)
-        return fail(RTW_ERR_CUDA, "upload of the frame / bin tables failed");
+    noalloc_upload<<<1, 256, 0, stream>>>(tab);
+    if (cudaGetLastError() != cudaSuccess) return fail(RTW_ERR_CUDA, "upload of the frame / bin tables failed");
     if (launch_trace(p, prm->precision, (int)grid, block, stream) != cudaSuccess)
         return fail(RTW_ERR_CUDA, "trace kernel launch failed");
-    // the host tables above are copied out of pageable memory before the
-    // copies return, so they may go out of scope; wait only when the caller
-    // gave no stream
+    // wait only when the caller gave no stream
     if (!prm->stream && cudaStreamSynchronize(stream) != cudaSuccess) return fail(RTW_ERR_CUDA, "trace kernel failed");
     return RTW_OK;
 }
