@@ -42,11 +42,13 @@ def parse():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--no-fp64-leg", action="store_true", help="skip the FP64 comparison leg")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-sample", type=int, default=2048, help="rays in the CPU baseline sample")
+    ap.add_argument("--cpu-sample", type=int, default=8192, help="rays in the CPU baseline sample")
     ap.add_argument("--no-batched", action="store_true", help="skip the 96-frame batched leg")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the synchrotron-torus adjoint leg")
     ap.add_argument("--no-scenes", action="store_true", help="skip the per-bin scene leg (Powehi, Synchro_Test, wormhole, Cartesian sphere)")
     ap.add_argument("--no-plain-leg", action="store_true", help="skip the plain FP64 GPU path leg")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the cfg1-cfg3 legs (Minkowski sphere 256^2, Schwarzschild 1024^2, Kerr thick 2048^2)")
     ap.add_argument("--adjoint-x-pix", type=int, default=512)
     ap.add_argument("--block-warps", type=int, default=0)
     ap.add_argument("--ctas-per-sm", type=int, default=0)
@@ -154,6 +156,60 @@ def steps_hist(steps):
 def cpu_sample_ids(P, n):
     n = min(n, P)
     return np.unique(np.linspace(0, P - 1, n).round().astype(np.int64))
+
+
+def rel_err_y(g_xyz, ref_xyz):
+    """Relative error of linear Y against the oracle, denominator
+    max(|ref|, 1e-6 max|ref|)."""
+    y_r = np.asarray(ref_xyz)[:, 1]
+    y_g = np.asarray(g_xyz)[:, 1].astype(np.float64)
+    den = np.maximum(np.abs(y_r), 1e-6 * np.abs(y_r).max() + 1e-300)
+    return np.abs(y_g - y_r) / den
+
+
+def parity_block(g_cls, g_xyz, ref, sel=None):
+    """Class match and intensity error of GPU pixels against the FP64 oracle on
+    the same pixels (sel: a boolean subset of them)."""
+    same = np.asarray(g_cls) == ref["class"]
+    err = rel_err_y(g_xyz, ref["xyz"])
+    if sel is None:
+        sel = np.ones(same.size, bool)
+    if not sel.any():
+        return {"px": 0}
+    ok = sel & same
+    out = {"px": int(sel.sum()), "class_match": float(np.mean(same[sel]))}
+    if ok.any():
+        e = err[ok]
+        out.update({"within_1e-3": float(np.mean(e <= 1e-3)), "p99_rel_err": float(np.quantile(e, 0.99)),
+                    "max_rel_err": float(e.max())})
+    return out
+
+
+def _short(block, with_px=True):
+    """A parity block rounded for the summary line."""
+    if not block:
+        return {}
+    keys = (("px", "px"), ("class_match", "class"), ("within_1e-3", "in_1e-3"), ("p99_rel_err", "p99"))
+    out = {}
+    for k, o in keys:
+        if k in block and (with_px or k != "px"):
+            v = block[k]
+            out[o] = v if isinstance(v, int) else float(f"{v:.4g}")
+    return out
+
+
+def shadow_annulus(cls_img, x_pix, y_pix, width=3):
+    """Pixels within `width` of the shadow edge: horizon-class pixels with a
+    non-horizon 4-neighbour, dilated by width pixels. This band holds the
+    critical curve and the photon-ring images around it."""
+    hz = np.asarray(cls_img).reshape(y_pix, x_pix) == 2  # RTW_CLASS_HORIZON
+    pad = np.pad(hz, 1, mode="edge")
+    inner = pad[:-2, 1:-1] & pad[2:, 1:-1] & pad[1:-1, :-2] & pad[1:-1, 2:]
+    band = hz & ~inner
+    for _ in range(width):
+        pb = np.pad(band, 1)
+        band = band | pb[:-2, 1:-1] | pb[2:, 1:-1] | pb[1:-1, :-2] | pb[1:-1, 2:]
+    return np.flatnonzero(band.ravel())
 
 
 def cpu_time(scene, cam, colors, n, threads=0, keep=False, skybox=(None, None)):
@@ -370,6 +426,75 @@ def scenes_leg(r, rank, cpu=True):
     return out
 
 
+def render_timed(r, scene, cam, colors, prec, reps, integrator=None, want=("xyz", "class")):
+    """One warm-up and `reps` timed renders (device time of the kernel); the
+    last render's host outputs and counters."""
+    from rtwca_b200 import abi
+    integ = abi.DP45_REF_COMPAT if integrator is None else integrator
+    r.render(scene, [cam], colors, want=("class",), precision=prec, integrator=integ)
+    ms = []
+    g = None
+    for _ in range(reps):
+        g = r.render(scene, [cam], colors, want=want, precision=prec, integrator=integ)
+        ms.append(r.stats()["kernel_ms"])
+    return g, float(np.mean(ms)), r.stats()
+
+
+def config_legs(r, rank, cpu=True, sample=2048):
+    """The workload configs besides the headline, each at its stated size,
+    FP32-mixed and FP64 (device time of the kernel), each precision's error
+    stated against the FP64 oracle:
+      cfg1 minkowski_sphere 256^2 (64 bins, tol 1e-8): the whole frame;
+      cfg2 schwarzschild_disk 1024^2 (64 bins, tol 1e-8): `sample` evenly
+           spaced pixels;
+      cfg3 kerr_thick_disk 2048^2 (64 bins, tol 1e-7, orbiting camera at
+           r = 5 M): `sample` evenly spaced pixels."""
+    from rtwca_b200 import abi, configs
+    out = {}
+    for key, name, reps in (("cfg1_minkowski_sphere_256", "minkowski_sphere", 3),
+                            ("cfg2_schwarzschild_1024", "schwarzschild_disk", 2),
+                            ("cfg3_kerr_thick_2048", "kerr_thick_disk", 1)):
+        scene, cam, colors = configs.workload(name)
+        P = cam.x_pix * cam.y_pix
+        leg = {"workload": f"{name} {cam.x_pix}x{cam.y_pix}, 64 bins, tol {cam.tolerance:g}"}
+        gs = {}
+        for pname, prec in (("mixed", abi.PREC_MIXED), ("fp64", abi.PREC_FP64)):
+            g, ms, st = render_timed(r, scene, cam, colors, prec, reps)
+            gs[pname] = g
+            leg[pname] = {"Mrays_s": P / ms / 1e3, "ms": ms, "step_attempts": st["step_attempts"],
+                          "promoted_steps": st["promoted_steps"]}
+        leg["mixed_over_fp64"] = leg["mixed"]["Mrays_s"] / leg["fp64"]["Mrays_s"]
+        if cpu and rank == 0:
+            ids = np.arange(P) if name == "minkowski_sphere" else cpu_sample_ids(P, sample)
+            v, n, dt, cores, ref = cpu_time(scene, cam, colors, ids.size, keep=True)
+            leg["oracle"] = {"Mrays_s": v, "pixels": n, "s": dt, "cores": cores}
+            for pname in ("mixed", "fp64"):
+                leg[pname]["parity"] = parity_block(gs[pname]["class"][ids], gs[pname]["xyz"][ids], ref)
+        out[key] = leg
+    return out
+
+
+def photon_ring_leg(scene, cam, colors, g_cls, g_xyz, n_max=4096):
+    """The headline frame's shadow-edge annulus (3 px either side of the
+    shadow boundary of the GPU render, at most n_max evenly spaced pixels)
+    against the FP64 oracle. Photon-ring pixels are those whose oracle ray
+    wound more than once around the hole (|phi_end - phi_camera| > 2 pi) or
+    crossed the equatorial plane at least twice; they are reported apart from
+    the rest of the band."""
+    from oracle import oracle as O
+    ids = shadow_annulus(g_cls, cam.x_pix, cam.y_pix)
+    if ids.size > n_max:
+        ids = ids[np.unique(np.linspace(0, ids.size - 1, n_max).round().astype(np.int64))]
+    t = time.perf_counter()
+    ref = O.render(scene, cam, colors, pixel_ids=ids, want=("xyz", "class", "state", "crossings"))
+    dt = time.perf_counter() - t
+    ring = (np.abs(ref["state"][:, 3] - cam.position[3]) > 2 * np.pi) | (ref["crossings"] >= 2)
+    return {"band_px": int(ids.size), "oracle_s": dt,
+            "criterion": "oracle |dphi| > 2 pi or >= 2 equatorial crossings",
+            "ring": parity_block(g_cls[ids], g_xyz[ids], ref, ring),
+            "rest_of_band": parity_block(g_cls[ids], g_xyz[ids], ref, ~ring)}
+
+
 def adjoint_leg(r, x_pix, world=1, rank=0):
     """Differentiable synchrotron torus: Kerr a = 0.94, inclination 17 deg,
     x_pix^2 rays, 32 bins over 230 GHz +- 20 %, FP32-mixed, tolerance 1e-6.
@@ -533,7 +658,14 @@ def run_b200(args):
         except Exception as exc:
             scenes = {"error": f"{type(exc).__name__}: {exc}"[:400]}
 
-    # end to end through the public API: host pinned outputs, synchronous call
+    configs_leg = None
+    if not args.no_configs and world == 1:
+        configs_leg = config_legs(r, rank, cpu=not args.no_cpu_baseline)
+
+    # end to end through the public API: the synchronous rtw_render call with
+    # pinned host outputs, timed by the host clock around the call (frame
+    # set-up, table uploads, kernel, device-to-host copies of XYZ, class and
+    # step counts)
     hx = torch.empty((P, 3), dtype=torch.float32, pin_memory=True)
     hc = torch.empty(P, dtype=torch.uint8, pin_memory=True)
     hs = torch.empty(P, dtype=torch.int32, pin_memory=True)
@@ -542,14 +674,15 @@ def run_b200(args):
     prm = r.params(colors, precision=prec, block_warps=args.block_warps, ctas_per_sm=args.ctas_per_sm)
     r.render_raw(scene, [cam], prm, hout)
     barrier(world)
-    e2e_ms = 0.0
+    e2e_s = 0.0
     ke = max(1, args.steps // 2)
     for _ in range(ke):
         flush.fill_(1.0)
         torch.cuda.synchronize()
-        r.render_raw(scene, [cam], prm, hout)   # synchronous: H2D frames/bins, kernel, D2H outputs
-        e2e_ms += r.stats()["total_ms"]
-    e2e_ms = all_max(e2e_ms, world)
+        t0 = time.perf_counter()
+        r.render_raw(scene, [cam], prm, hout)   # synchronous: returns with the outputs on the host
+        e2e_s += time.perf_counter() - t0
+    e2e_ms = all_max(e2e_s * 1e3, world)
     e2e_val = world * P * ke / (e2e_ms * 1e-3) / 1e6
     h2d = 8 * 4 * 128 + 256  # bins table + one frame descriptor
     d2h = P * (12 + 1 + 4)
@@ -561,6 +694,8 @@ def run_b200(args):
         peak = peaks["fp32_flops"] / 1e12 if prec == abi.PREC_MIXED else peaks["fp64_flops"] / 1e12
         cpu = None
         parity = None
+        ring = None
+        g_cls, g_xyz = hc.numpy(), hx.numpy()
         if not args.no_cpu_baseline:
             v, n, dt, cores, ref = cpu_time(scene, cam, colors, args.cpu_sample, keep=True)
             cpu = {"value": v, "unit": "Mrays/s", "cores": cores, "kind": "port",
@@ -568,62 +703,65 @@ def run_b200(args):
                              "restatement of the reference's CPU integrator, OpenMP"}
             # the same pixels of the (end-to-end) render against the FP64 oracle
             ids = cpu_sample_ids(P, args.cpu_sample)
-            g_cls = hc.numpy()[ids]
-            g_y = hx.numpy()[ids, 1].astype(np.float64)
-            same = g_cls == ref["class"]
-            y_r = ref["xyz"][:, 1]
-            den = np.maximum(np.abs(y_r), 1e-6 * np.abs(y_r).max() + 1e-300)
-            err = np.abs(g_y - y_r) / den
-            # photon-ring pixels: rays that wound more than once around the
-            # hole (|phi_final - phi_camera| > 2 pi in the oracle), reported apart
-            ring = np.abs(ref["state"][:, 3] - cam.position[3]) > 2 * np.pi
-
-            def part(sel):
-                if not sel.any():
-                    return {"pixels": 0}
-                ok = sel & same
-                return {"pixels": int(sel.sum()), "class_match": float(np.mean(same[sel])),
-                        "intensity_within_1e-3": float(np.mean(err[ok] <= 1e-3)) if ok.any() else None,
-                        "p99_rel_err": float(np.quantile(err[ok], 0.99)) if ok.any() else None}
-            parity = {"pixels": int(ids.size), "class_match": float(np.mean(same)),
-                      "intensity_within_1e-3": float(np.mean(err[same] <= 1e-3)),
-                      "p99_rel_err": float(np.quantile(err[same], 0.99)),
-                      "error_denominator": "max(|ref|, 1e-6 max|ref|) on linear Y",
-                      "photon_ring": part(ring), "other": part(~ring),
-                      "reference": "FP64 oracle, reference step, same pixels"}
+            parity = parity_block(g_cls[ids], g_xyz[ids], ref)
+            parity["of"] = "evenly spaced pixels vs the FP64 oracle, reference step; error on linear Y"
+            if args.workload in ("kerr_thin_disk", "schwarzschild_disk"):
+                ring = photon_ring_leg(scene, cam, colors, g_cls, g_xyz)
+        fp64_v = fp64["value"] if fp64 else None
+        summary = {
+            "mixed_Mrays_s": value if prec == abi.PREC_MIXED else None,
+            "fp64_Mrays_s": fp64_v,
+            "mixed_over_fp64": value / fp64_v if fp64_v else None,
+            "plain_fp64_Mrays_s": plain["value"] if plain else None,
+            "mixed_over_plain_fp64": plain["mixed_over_plain"] if plain else None,
+            "fsal_Mrays_s": fsal["value"] if fsal else None,
+            "batched_Mrays_s": batched["value"] if batched else None,
+            "batched_frame_done_ms_p50_p99": ([round(batched["frame_done_ms"]["p50"]), round(batched["frame_done_ms"]["p99"])]
+                                              if batched else None),
+            "adjoint_grad_per_s": adjoint["value"] if adjoint else None,
+            "adjoint_over_forward": adjoint["adjoint_over_forward"] if adjoint else None,
+            "parity": _short(parity),
+            "photon_ring": ({"band_px": ring["band_px"], "ring": _short(ring["ring"]),
+                             "rest": _short(ring["rest_of_band"])} if ring else None),
+        }
+        if configs_leg:
+            for k, leg in configs_leg.items():
+                summary[k] = {pn: {"Mrays_s": round(leg[pn]["Mrays_s"], 4), **_short(leg[pn].get("parity"), False)}
+                              for pn in ("mixed", "fp64")}
         line = {
             "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32+f64" if prec == abi.PREC_MIXED else "f64", "data": "synthetic",
+            "gpu_launches": args.steps,
             "config": {"workload": f"{args.workload} {cam.x_pix}x{cam.y_pix}, 64 bins, tol {cam.tolerance:g}, "
-                                   f"{'FP32-mixed' if prec == abi.PREC_MIXED else 'FP64'}",
+                                   f"{'FP32-mixed' if prec == abi.PREC_MIXED else 'FP64'}, reference step",
                        "rays_per_gpu": P, "parallelism": f"weak x{world} (one frame per GPU)",
                        "l2": "flushed (256 MB write) between timed renders"},
-            "fp64": fp64,
-            "fsal": fsal,
-            "plain_fp64": plain,
-            "batched": batched,
-            "adjoint": adjoint,
-            "scenes": scenes,
-            "integrator": "reference step (k1 = previous sum b_i k_i)",
+            "summary": summary,
             "roofline": {"bound": "fp32" if prec == abi.PREC_MIXED else "fp64", "achieved": achieved, "peak": peak,
                          "unit": "TFLOP/s", "frac": achieved / peak,
                          "traffic": (st["step_attempts"] * TRAFFIC_B_PER_ATTEMPT
                                      if prec == abi.PREC_MIXED and args.workload == "kerr_thin_disk" else None),
-                         "traffic_source": "ncu dram__bytes_read+write of one capture of this kernel at 512^2, "
-                                           "3.21 GB over 357.2 M step attempts, scaled by this launch's attempts",
-                         "peak_source": "measured in-run FMA microbenchmark (rtw_measure_peaks)",
-                         "mufu_gops": mufu / (kms * 1e-3) / 1e9,
-                         "mufu_peak_gops": peaks["mufu_ops"] / 1e9},
+                         "peak_source": "measured in-run FMA probe (rtw_measure_peaks)",
+                         "mufu_gops": mufu / (kms * 1e-3) / 1e9, "mufu_peak_gops": peaks["mufu_ops"] / 1e9},
             "cpu_baseline": cpu,
-            "parity_sample": parity,
-            "e2e": {"value": e2e_val, "unit": "Mrays/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-            "steps_per_ray": steps_hist(hs.numpy()),
-            "gpu_launches": args.steps,
+            "e2e": {"value": e2e_val, "unit": "Mrays/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "timer": "host clock around the synchronous rtw_render call"},
             "clocks": clk.summary(),
+        }
+        details = {
+            "fp64": fp64, "fsal": fsal, "plain_fp64": plain, "batched": batched, "adjoint": adjoint,
+            "scenes": scenes, "configs": configs_leg, "photon_ring": ring, "parity_sample": parity,
+            "integrator": "reference step (k1 = previous sum b_i k_i)",
+            "traffic_source": "ncu dram__bytes_read+write of one capture of this kernel at 512^2, scaled by step "
+                              "attempts",
+            "op_counts": oc, "steps_per_ray": steps_hist(hs.numpy()),
             "counters": {k: st[k] for k in ("step_attempts", "rejected_steps", "promoted_steps", "spectral_steps",
                                             "emitting_steps", "escape_substeps", "nan_rays")},
         }
+        # every leg in full on stderr (one JSON line), the summary on stdout
+        sys.stderr.write("BENCH_DETAILS " + json.dumps(details) + "\n")
+        sys.stderr.flush()
         print(json.dumps(line), flush=True)
     r.close()
     if world > 1:

@@ -55,6 +55,8 @@ def load() -> C.CDLL:
         lib.oracle_render.restype = C.c_int
         lib.oracle_set_skybox.argtypes = [C.c_int, C.POINTER(C.c_float), C.c_int]
         lib.oracle_set_skybox.restype = C.c_int
+        lib.oracle_set_diagnostics.argtypes = [C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        lib.oracle_set_diagnostics.restype = C.c_int
         lib.oracle_set_ray_bundles.argtypes = [C.c_int]
         lib.oracle_set_ray_bundles.restype = C.c_int
         lib.oracle_cube_wrap.argtypes = [C.c_int] * 6 + [C.POINTER(C.c_int)]
@@ -122,7 +124,9 @@ def render(scene, cam, colors_nm, *, max_dt_scale=0.1, integrator=0, pixel_ids=N
     """Traces one camera (or the pixel subset `pixel_ids`) with the FP64 oracle.
     Returns a dict of arrays indexed like the pixel list, plus 'counters'
     (step attempts, rejected attempts, polar Euler sub-steps). ray_bundles:
-    the Gaussian ray-bundle lookup of the wormhole's skyboxes."""
+    the Gaussian ray-bundle lookup of the wormhole's skyboxes. want may add
+    "crossings" (steps that cross the equatorial plane, per pixel) and
+    "escapes" (polar Euler sub-steps, per pixel)."""
     from rtwca_b200 import abi
     cam = abi.Camera.from_buffer_copy(cam)
     cam.y_pix = abi.y_pixels(cam.x_pix, cam.fov_hor, cam.fov_vert)
@@ -141,6 +145,8 @@ def render(scene, cam, colors_nm, *, max_dt_scale=0.1, integrator=0, pixel_ids=N
     res["spectrum"] = np.zeros((n, N)) if "spectrum" in want else None
     res["tau"] = np.zeros((n, N)) if "tau" in want else None
     res["state"] = np.zeros((n, 8)) if "state" in want else None
+    res["crossings"] = np.zeros(n, np.int32) if "crossings" in want else None
+    res["escapes"] = np.zeros(n, np.int32) if "escapes" in want else None
     counters = np.zeros(3, np.int64)
 
     def ptr(a, t):
@@ -152,6 +158,7 @@ def render(scene, cam, colors_nm, *, max_dt_scale=0.1, integrator=0, pixel_ids=N
         load().oracle_set_skybox(k, t.ctypes.data_as(C.POINTER(C.c_float)) if t is not None else None,
                                  t.shape[0] // 3 if t is not None else 0)
     load().oracle_set_ray_bundles(int(bool(ray_bundles)))
+    load().oracle_set_diagnostics(ptr(res["crossings"], C.c_int), ptr(res["escapes"], C.c_int))
     try:
         st = load().oracle_render(
             C.byref(scene), C.byref(cam), _dp(c), N, float(max_dt_scale), int(integrator),
@@ -163,6 +170,7 @@ def render(scene, cam, colors_nm, *, max_dt_scale=0.1, integrator=0, pixel_ids=N
         for k in range(2):
             load().oracle_set_skybox(k, None, 0)
         load().oracle_set_ray_bundles(0)
+        load().oracle_set_diagnostics(None, None)
     if st != 0:
         raise RuntimeError(f"oracle_render failed with status {st}")
     res = {k: v for k, v in res.items() if v is not None}

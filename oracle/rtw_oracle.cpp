@@ -1181,6 +1181,11 @@ void cie_weights(const double* colors, int n, double* wx, double* wy, double* wz
 static const float* g_sky[2] = {nullptr, nullptr};
 static int g_sky_h[2] = {0, 0};
 static int g_bundles = 0;
+// per-pixel diagnostics of the next oracle_render (NULL: not recorded): the
+// number of accepted steps and polar escapes that carry the ray across the
+// equatorial plane theta = pi/2, and the polar Euler sub-steps it took
+static int* g_diag_cross = nullptr;
+static int* g_diag_escape = nullptr;
 
 inline double normal_gauss(double x, double s, double m) {  // my_special_functions.jl:20-22
     return std::exp(-(x - m) * (x - m) / (2 * s * s)) / (s * std::sqrt(2 * kPi));
@@ -1408,6 +1413,13 @@ int oracle_cube_wrap(int i, int j, int face, int x, int y, int n, int* out) {
     return RTW_OK;
 }
 
+// per-pixel diagnostics of the next renders (NULL: off); kept until changed
+int oracle_set_diagnostics(int* crossings, int* escape_substeps) {
+    g_diag_cross = crossings;
+    g_diag_escape = escape_substeps;
+    return RTW_OK;
+}
+
 int oracle_set_skybox(int k, const float* tex, int h) {
     if (k < 0 || k > 1 || (tex && h < 1)) return RTW_ERR_INVALID_PARAM;
     g_sky[k] = tex;
@@ -1519,9 +1531,12 @@ int oracle_render(const rtw_scene* scene, rtw_camera* cam, const double* colors_
             long long step_count = 0;
             long long esc = 0;
             int klass = 0;
+            int crossings = 0;
             while (true) {
                 bool rj = false;
+                const double side = ray[2] - kPi / 2;
                 dt = dp45_step(sc, w, ray.data(), dt, rejected, &rj, &esc);
+                if ((side < 0) != (ray[2] - kPi / 2 < 0)) ++crossings;
                 rejected = rj;
                 tot_rej += rj ? 1 : 0;
                 ++step_count;
@@ -1537,6 +1552,8 @@ int oracle_render(const rtw_scene* scene, rtw_camera* cam, const double* colors_
             }
             tot_steps += step_count;
             tot_esc += esc;
+            if (g_diag_cross) g_diag_cross[q] = crossings;
+            if (g_diag_escape) g_diag_escape[q] = (int)esc;
             if (cls) cls[q] = (unsigned char)klass;
             if (steps) steps[q] = (unsigned int)step_count;
             if (xyz) {

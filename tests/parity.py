@@ -31,3 +31,20 @@ def summarize(gpu, ref, mask=None):
         "max_rel": float(e.max()) if e.size else 0.0,
         "p99_rel": float(np.quantile(e, 0.99)) if e.size else 0.0,
     }
+
+
+def min_sin_theta(oracle, scene, cam):
+    """Per pixel, the smallest sin(theta) its camera ray's geodesic can reach:
+    from the constants of motion at the camera (E = -k_t, L_z = k_phi and the
+    Carter constant Q = k_theta^2 + cos^2 theta (L_z^2 / sin^2 theta - a^2 E^2)),
+    the turning point of the theta motion, sin^2 theta_min ~ L_z^2 / (Q + a^2 E^2
+    + L_z^2). Rays with a small value pass close to the spin axis, where
+    Boyer-Lindquist coordinates are ill-conditioned."""
+    rays = oracle.camera_rays(scene, cam)
+    g = oracle.metric(scene, rays[0, :4])
+    k = rays[:, 4:8] @ g.T  # lower-index momenta (g is symmetric)
+    E, Lz, kth = -k[:, 0], k[:, 3], k[:, 2]
+    th = rays[0, 2]
+    a = scene.spin if scene.kind in (2, 3, 4, 5) else 0.0
+    Q = kth ** 2 + np.cos(th) ** 2 * (Lz ** 2 / np.sin(th) ** 2 - a * a * E ** 2)
+    return np.sqrt(Lz ** 2 / np.maximum(Q + a * a * E ** 2 + Lz ** 2, 1e-300))

@@ -45,8 +45,8 @@ def test_gpu_matches_golden(renderer, name, integ, tag, prec):
     out = renderer.render(scene, [cam], colors, want=("xyz", "class", "steps", "spectrum"), precision=prec,
                           integrator=integ)
     s = summarize(out, g)
-    assert s["class_match"] >= 0.99, s
-    assert s["frac_within_1e-3"] >= 0.99, s
+    assert s["class_match"] >= 0.999, s
+    assert s["frac_within_1e-3"] >= 0.999, s
     if prec == abi.PREC_FP64:
         assert s["max_rel"] < 1e-5, s
 

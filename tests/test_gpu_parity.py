@@ -2,8 +2,10 @@
 
 Sizes are small enough for the oracle to finish in seconds. Bars: termination
 class identical on >= 99.9% of pixels; linear intensity (CIE Y) within 1e-3
-relative error on >= 99.9% of the pixels whose class agrees (FP64 path), with
-the looser bars of the FP32-mixed path written next to each test.
+relative error on >= 99.9% of the pixels whose class agrees, for both the FP64
+and the FP32-mixed path with the reference's step. The one looser bar (FSAL
+with FP32 stages) applies only to the rays that pass close to the spin axis;
+they are named and counted apart in that test.
 """
 import math
 
@@ -11,7 +13,7 @@ import numpy as np
 import pytest
 
 from rtwca_b200 import abi, configs
-from tests.parity import summarize
+from tests.parity import min_sin_theta, summarize
 
 pytestmark = pytest.mark.gpu
 
@@ -60,8 +62,24 @@ def test_mixed_parity(renderer, oracle, name):
     r = _ref(oracle, scene, cam, colors)
     s = summarize(g, r)
     print(name, s)
-    assert s["class_match"] >= 0.995, s
-    assert s["frac_within_1e-3"] >= 0.99, s
+    assert s["class_match"] >= 0.999, s
+    assert s["frac_within_1e-3"] >= 0.999, s
+
+
+def test_mixed_parity_headline_128(renderer, oracle):
+    """The headline scene (Kerr a = 0.9 thin disk, camera at r = 50 M and 80
+    deg, tol 1e-8, the reference's step) at 128^2 with its 64 bins: the
+    FP32-mixed path against the FP64 oracle, at the parity bar itself (class
+    on >= 99.9% of pixels, linear Y within 1e-3 on >= 99.9%)."""
+    scene, cam, colors = configs.workload("kerr_thin_disk", x_pix=128)
+    g = renderer.render(scene, [cam], colors, want=("xyz", "class", "steps"), precision=abi.PREC_MIXED)
+    r = oracle.render(scene, cam, colors, want=("xyz", "class", "steps"))
+    s = summarize(g, r)
+    print(s)
+    assert g["class"].size == 128 * 128
+    assert s["class_match"] >= 0.999, s
+    assert s["frac_within_1e-3"] >= 0.999, s
+    assert s["p99_rel"] < 1e-4, s
 
 
 def test_fsal_parity(renderer, oracle):
@@ -79,15 +97,23 @@ def test_fsal_mixed_parity(renderer, oracle, name):
     """FSAL with FP32 stages. Rays that cross within ~1e-3 of the spin axis
     with near-zero L_z are ill-conditioned in Boyer-Lindquist coordinates (an
     error in k^phi at theta grows like (theta/theta')^2 on the way in, traced
-    on the GPU); on these grids they are <= 1.5% of the pixels."""
+    on the GPU). Those rays (sin theta_min < 2e-3 from their constants of
+    motion) are counted apart with a looser bar; every other pixel is held to
+    the parity bar."""
     scene, cam, _ = configs.workload(name, x_pix=SMALL[name])
     colors = configs.log_spaced_colors(16)
     g = _gpu(renderer, scene, cam, colors, precision=abi.PREC_MIXED, integrator=abi.DP45_FSAL)
     r = _ref(oracle, scene, cam, colors, integrator=abi.DP45_FSAL)
-    s = summarize(g, r)
-    print(name, s)
-    assert s["class_match"] >= 0.98, s
-    assert s["frac_within_1e-3"] >= 0.99, s
+    graze = min_sin_theta(oracle, scene, cam) < 2e-3
+    rest = summarize(g, r, mask=~graze)
+    near = summarize(g, r, mask=graze)
+    rest_class = float(np.mean(g["class"][~graze] == r["class"][~graze]))
+    print(name, "grazing", int(graze.sum()), near, "rest", rest_class, rest)
+    assert graze.mean() <= 0.1
+    assert rest_class >= 0.999, rest
+    assert rest["frac_within_1e-3"] >= 0.999, rest
+    if graze.any():
+        assert float(np.mean(g["class"][graze] == r["class"][graze])) >= 0.5, near
 
 
 @pytest.mark.parametrize("n_colors", [1, 33, 64, 100])
@@ -127,6 +153,34 @@ def test_batch_equals_single(renderer):
         for k in ("xyz", "class", "steps"):
             assert np.array_equal(batch[k][off:off + n], one[k]), k
         off += n
+
+
+@pytest.mark.parametrize("prec", [abi.PREC_FP64, abi.PREC_MIXED])
+def test_polar_escape_trace_kernel(renderer, oracle, prec):
+    """The reference's polar escape (37 explicit Euler sub-steps across the
+    axis, integrators_LttM.jl:62-105, triggered by near_singularity,
+    Kerr.source/source_geometry.jl:249-269) in the trace kernel. The pixel
+    column whose rays have L_z = 0 passes over the pole; at tol 1e-5 those rays
+    come within tol of the axis (at the headline's 1e-8 they turn round at
+    theta ~ 1e-5 first). The kernel must take escapes, and the escaping rays
+    must match the oracle's class and intensity."""
+    scene, cam, _ = configs.workload("kerr_thin_disk", x_pix=64, tol=1e-5)
+    colors = configs.log_spaced_colors(16)
+    g = _gpu(renderer, scene, cam, colors, precision=prec)
+    st = renderer.stats()
+    r = oracle.render(scene, cam, colors, want=("xyz", "class", "steps", "escapes"))
+    esc = r["escapes"] > 0
+    print("oracle escape rays", int(esc.sum()), "substeps", int(r["escapes"].sum()),
+          "gpu substeps", st["escape_substeps"])
+    assert esc.sum() >= 8
+    assert st["escape_substeps"] >= 37 * 8
+    s_esc = summarize(g, r, mask=esc)
+    cm = float(np.mean(g["class"][esc] == r["class"][esc]))
+    print("escape pixels: class", cm, s_esc, "all:", summarize(g, r))
+    assert cm >= 0.99, s_esc
+    assert s_esc["frac_within_1e-3"] >= 0.99, s_esc
+    s_all = summarize(g, r)
+    assert s_all["class_match"] >= 0.999 and s_all["frac_within_1e-3"] >= 0.999, s_all
 
 
 def test_invalid_camera(renderer):
