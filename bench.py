@@ -50,6 +50,9 @@ def parse():
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the cfg1-cfg3 legs (Minkowski sphere 256^2, Schwarzschild 1024^2, Kerr thick 2048^2)")
     ap.add_argument("--adjoint-x-pix", type=int, default=512)
+    ap.add_argument("--strong", action="store_true",
+                    help="N>1: report the strong-scaling leg (one frame over N GPUs in interleaved tiles) as the "
+                         "headline value")
     ap.add_argument("--block-warps", type=int, default=0)
     ap.add_argument("--ctas-per-sm", type=int, default=0)
     return ap.parse_args()
@@ -495,6 +498,36 @@ def photon_ring_leg(scene, cam, colors, g_cls, g_xyz, n_max=4096):
             "rest_of_band": parity_block(g_cls[ids], g_xyz[ids], ref, ~ring)}
 
 
+def strong_leg(r, world, rank, scene, cam, colors, barrier_fn, reps=2):
+    """One frame over `world` GPUs (strong scaling): interleaved 16 x 16 pixel
+    tiles (tile t -> rank t mod world), each rank's tiles in one batched
+    launch, one gather of the tiles to rank 0, which assembles the image.
+    Device time (CUDA events around the whole call, gather included), max
+    over ranks."""
+    import torch
+    from rtwca_b200 import abi, shard
+    P = cam.x_pix * cam.y_pix
+    shard.render_frame_tiles(r, scene, cam, colors, world, rank, precision=abi.PREC_MIXED)  # warm-up
+    ms = []
+    for _ in range(reps):
+        barrier_fn()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        img = shard.render_frame_tiles(r, scene, cam, colors, world, rank, precision=abi.PREC_MIXED)
+        e1.record()
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    t = all_max(float(np.mean(ms)), world)
+    out = {"value": P / (t * 1e-3) / 1e6, "unit": "Mrays/s", "ms": t, "tile": 16,
+           "tiles_per_rank": -(-len(shard.tile_windows(cam.x_pix, cam.y_pix)) // world),
+           "exchange": "one gather of the tiles to rank 0"}
+    if rank == 0 and img is not None:
+        out["pixels_assembled"] = int(img["class"].size)
+    return out
+
+
 def adjoint_leg(r, x_pix, world=1, rank=0):
     """Differentiable synchrotron torus: Kerr a = 0.94, inclination 17 deg,
     x_pix^2 rays, 32 bins over 230 GHz +- 20 %, FP32-mixed, tolerance 1e-6.
@@ -642,6 +675,13 @@ def run_b200(args):
                  "what": "one FP64 thread per pixel over a grid, the reference's 8 + 2N state and per-bin right-hand "
                          "side, no warp cooperation (RTW_PREC_FP64_PLAIN)"}
 
+    strong = None
+    if world > 1 or args.strong:
+        strong = strong_leg(r, world, rank, scene, cam, colors, lambda: barrier(world))
+        if args.strong:
+            value = strong["value"]
+            ms_per_step = strong["ms"]
+
     batched = None
     if not args.no_batched:
         batched = batched_leg(r, world, rank, stream, lambda: barrier(world))
@@ -716,6 +756,7 @@ def run_b200(args):
             "mixed_over_plain_fp64": plain["mixed_over_plain"] if plain else None,
             "fsal_Mrays_s": fsal["value"] if fsal else None,
             "batched_Mrays_s": batched["value"] if batched else None,
+            "strong_Mrays_s": strong["value"] if strong else None,
             "batched_frame_done_ms_p50_p99": ([round(batched["frame_done_ms"]["p50"]), round(batched["frame_done_ms"]["p99"])]
                                               if batched else None),
             "adjoint_grad_per_s": adjoint["value"] if adjoint else None,
@@ -730,12 +771,15 @@ def run_b200(args):
                               for pn in ("mixed", "fp64")}
         line = {
             "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+            "scaling": "strong" if args.strong else "weak",
             "vs_baseline": None, "dtype": "f32+f64" if prec == abi.PREC_MIXED else "f64", "data": "synthetic",
             "gpu_launches": args.steps,
             "config": {"workload": f"{args.workload} {cam.x_pix}x{cam.y_pix}, 64 bins, tol {cam.tolerance:g}, "
                                    f"{'FP32-mixed' if prec == abi.PREC_MIXED else 'FP64'}, reference step",
-                       "rays_per_gpu": P, "parallelism": f"weak x{world} (one frame per GPU)",
+                       "rays_per_gpu": P // world if args.strong else P,
+                       "parallelism": (f"strong x{world} (one frame in interleaved 16x16 tiles)" if args.strong
+                                       else f"weak x{world} (one frame per GPU)"),
                        "l2": "flushed (256 MB write) between timed renders"},
             "summary": summary,
             "roofline": {"bound": "fp32" if prec == abi.PREC_MIXED else "fp64", "achieved": achieved, "peak": peak,
@@ -750,7 +794,7 @@ def run_b200(args):
             "clocks": clk.summary(),
         }
         details = {
-            "fp64": fp64, "fsal": fsal, "plain_fp64": plain, "batched": batched, "adjoint": adjoint,
+            "fp64": fp64, "fsal": fsal, "plain_fp64": plain, "batched": batched, "adjoint": adjoint, "strong": strong,
             "scenes": scenes, "configs": configs_leg, "photon_ring": ring, "parity_sample": parity,
             "integrator": "reference step (k1 = previous sum b_i k_i)",
             "traffic_source": "ncu dram__bytes_read+write of one capture of this kernel at 512^2, scaled by step "

@@ -55,6 +55,10 @@ def load() -> C.CDLL:
         lib.oracle_render.restype = C.c_int
         lib.oracle_set_skybox.argtypes = [C.c_int, C.POINTER(C.c_float), C.c_int]
         lib.oracle_set_skybox.restype = C.c_int
+        lib.oracle_torus_forward.argtypes = [P, P, D, C.c_int, C.c_double, C.c_int, C.POINTER(C.c_longlong),
+                                             C.c_longlong, D, D, C.POINTER(C.c_ubyte), C.POINTER(C.c_uint),
+                                             C.POINTER(C.c_int), C.c_int]
+        lib.oracle_torus_forward.restype = C.c_int
         lib.oracle_set_diagnostics.argtypes = [C.POINTER(C.c_int), C.POINTER(C.c_int)]
         lib.oracle_set_diagnostics.restype = C.c_int
         lib.oracle_set_ray_bundles.argtypes = [C.c_int]
@@ -176,6 +180,34 @@ def render(scene, cam, colors_nm, *, max_dt_scale=0.1, integrator=0, pixel_ids=N
     res = {k: v for k, v in res.items() if v is not None}
     res["counters"] = counters
     res["y_pix"] = cam.y_pix
+    return res
+
+
+def torus_forward(scene, cam, colors_nm, *, mode=0, max_dt_scale=0.1, pixel_ids=None, threads=0):
+    """Forward-mode derivatives of the synchrotron torus's FSAL render: dict of
+    'spectrum' [n, N], 'tangents' [n, N, 5] = dI/d(spin, inclination (rad),
+    n_e0, b_0, theta_e0), 'class', 'steps', 'escapes' (polar Euler sub-steps).
+    mode 0 holds the controller's step sizes fixed and differentiates those
+    set by pad_max_dt (the discrete adjoint's convention); mode 1 carries the
+    tangents through every step size."""
+    from rtwca_b200 import abi
+    cam = abi.Camera.from_buffer_copy(cam)
+    cam.y_pix = abi.y_pixels(cam.x_pix, cam.fov_hor, cam.fov_vert)
+    P = cam.x_pix * cam.y_pix
+    c = np.ascontiguousarray(colors_nm, dtype=np.float64)
+    N = c.size
+    ids = None if pixel_ids is None else np.ascontiguousarray(pixel_ids, dtype=np.int64)
+    n = P if ids is None else ids.size
+    res = {"spectrum": np.zeros((n, N)), "tangents": np.zeros((n, N, 5)), "class": np.zeros(n, np.uint8),
+           "steps": np.zeros(n, np.uint32), "escapes": np.zeros(n, np.int32)}
+    st = load().oracle_torus_forward(
+        C.byref(scene), C.byref(cam), _dp(c), N, float(max_dt_scale), int(mode),
+        ids.ctypes.data_as(C.POINTER(C.c_longlong)) if ids is not None else None, n,
+        _dp(res["spectrum"]), _dp(res["tangents"]), res["class"].ctypes.data_as(C.POINTER(C.c_ubyte)),
+        res["steps"].ctypes.data_as(C.POINTER(C.c_uint)), res["escapes"].ctypes.data_as(C.POINTER(C.c_int)),
+        int(threads))
+    if st != 0:
+        raise RuntimeError(f"oracle_torus_forward failed with status {st}")
     return res
 
 

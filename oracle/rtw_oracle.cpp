@@ -105,6 +105,77 @@ inline double jl_mod(double x, double y) {
 inline double sq(double x) { return x * x; }
 
 // ----------------------------------------------------------------------------
+// Forward-mode derivatives: a dual number with five tangents (spin,
+// inclination, n_e0, b_0, theta_e0 of the synchrotron torus). The oracle's
+// torus path below is written once over the scalar type and instantiated
+// with double (the oracle itself) and with D5 (its forward-mode derivative,
+// in the role ForwardDiff plays for the reference's CPU integrator).
+// Comparisons and branches use the value, as ForwardDiff's do.
+// ----------------------------------------------------------------------------
+constexpr int kTan = 5;
+struct D5 {
+    double v = 0;
+    double d[kTan] = {0, 0, 0, 0, 0};
+    D5() = default;
+    D5(double x) : v(x) {}  // NOLINT: constants enter with zero tangents
+};
+inline double val(double x) { return x; }
+inline double val(const D5& x) { return x.v; }
+template <class F>
+inline D5 chain(const D5& a, double f, double df) {  // f(a), f'(a)
+    D5 r(f);
+    for (int i = 0; i < kTan; ++i) r.d[i] = df * a.d[i];
+    return r;
+}
+inline D5 operator-(const D5& a) { D5 r(-a.v); for (int i = 0; i < kTan; ++i) r.d[i] = -a.d[i]; return r; }
+inline D5 operator+(const D5& a, const D5& b) { D5 r(a.v + b.v); for (int i = 0; i < kTan; ++i) r.d[i] = a.d[i] + b.d[i]; return r; }
+inline D5 operator-(const D5& a, const D5& b) { D5 r(a.v - b.v); for (int i = 0; i < kTan; ++i) r.d[i] = a.d[i] - b.d[i]; return r; }
+inline D5 operator*(const D5& a, const D5& b) {
+    D5 r(a.v * b.v);
+    for (int i = 0; i < kTan; ++i) r.d[i] = a.d[i] * b.v + a.v * b.d[i];
+    return r;
+}
+inline D5 operator/(const D5& a, const D5& b) {
+    D5 r(a.v / b.v);
+    for (int i = 0; i < kTan; ++i) r.d[i] = (a.d[i] - r.v * b.d[i]) / b.v;
+    return r;
+}
+inline D5 operator+(const D5& a, double b) { D5 r = a; r.v += b; return r; }
+inline D5 operator+(double a, const D5& b) { return b + a; }
+inline D5 operator-(const D5& a, double b) { D5 r = a; r.v -= b; return r; }
+inline D5 operator-(double a, const D5& b) { return -(b - a); }
+inline D5 operator*(const D5& a, double b) { D5 r(a.v * b); for (int i = 0; i < kTan; ++i) r.d[i] = a.d[i] * b; return r; }
+inline D5 operator*(double a, const D5& b) { return b * a; }
+inline D5 operator/(const D5& a, double b) { D5 r(a.v / b); for (int i = 0; i < kTan; ++i) r.d[i] = a.d[i] / b; return r; }
+inline D5 operator/(double a, const D5& b) { return D5(a) / b; }
+inline D5& operator+=(D5& a, const D5& b) { a = a + b; return a; }
+inline D5& operator-=(D5& a, const D5& b) { a = a - b; return a; }
+inline bool operator<(const D5& a, const D5& b) { return a.v < b.v; }
+inline bool operator>(const D5& a, const D5& b) { return a.v > b.v; }
+inline bool operator<=(const D5& a, const D5& b) { return a.v <= b.v; }
+inline bool operator>=(const D5& a, const D5& b) { return a.v >= b.v; }
+inline bool operator==(const D5& a, const D5& b) { return a.v == b.v; }
+inline bool operator!=(const D5& a, const D5& b) { return a.v != b.v; }
+inline D5 sin(const D5& a) { return chain<D5>(a, std::sin(a.v), std::cos(a.v)); }
+inline D5 cos(const D5& a) { return chain<D5>(a, std::cos(a.v), -std::sin(a.v)); }
+inline D5 tan(const D5& a) { const double t = std::tan(a.v); return chain<D5>(a, t, 1 + t * t); }
+inline D5 atan(const D5& a) { return chain<D5>(a, std::atan(a.v), 1 / (1 + a.v * a.v)); }
+inline D5 sqrt(const D5& a) { const double s = std::sqrt(a.v); return chain<D5>(a, s, 0.5 / s); }
+inline D5 exp(const D5& a) { const double e = std::exp(a.v); return chain<D5>(a, e, e); }
+inline D5 expm1(const D5& a) { return chain<D5>(a, std::expm1(a.v), std::exp(a.v)); }
+inline D5 log(const D5& a) { return chain<D5>(a, std::log(a.v), 1 / a.v); }
+inline D5 pow(const D5& a, double e) { return chain<D5>(a, std::pow(a.v, e), e * std::pow(a.v, e - 1)); }
+inline D5 fabs(const D5& a) { return a.v < 0 ? -a : a; }
+inline bool isfinite(const D5& a) { return std::isfinite(a.v); }
+// K_nu(x) and dK_nu/dx = -(K_{nu-1}(x) + K_{nu+1}(x)) / 2
+inline D5 cyl_bessel_k(double nu, const D5& x) {
+    return chain<D5>(x, std::cyl_bessel_k(nu, x.v),
+                     -0.5 * (std::cyl_bessel_k(nu - 1, x.v) + std::cyl_bessel_k(nu + 1, x.v)));
+}
+template <class T>
+inline T sqT(const T& x) { return x * x; }
+
+// ----------------------------------------------------------------------------
 // Scenes (".source" plugins), restated with runtime constants.
 // ----------------------------------------------------------------------------
 struct OScene {
@@ -186,6 +257,23 @@ struct OScene {
         A = (r * r + a * a) * Sig + rs * r * sq(a * std::sin(th));
     }
 
+    // Kerr calc_lower_metric! (source_geometry.jl:66-75) over the scalar type,
+    // spin al (the metric entries not written are left as they are)
+    template <class T>
+    void kerr_metric_t(const T& r, const T& th, const T& al, T g[4][4]) const {
+        using std::cos;
+        using std::sin;
+        const T Sig = r * r + sqT(al * cos(th));
+        const T Del = r * r - r * rs + al * al;
+        const T A = (r * r + al * al) * Sig + rs * r * sqT(al * sin(th));
+        g[0][0] = -(1.0 - rs * r / Sig);
+        g[0][3] = -rs * al * r * sqT(sin(th)) / Sig;
+        g[3][0] = g[0][3];
+        g[1][1] = Sig / Del;
+        g[2][2] = Sig;
+        g[3][3] = (A / Sig) * sqT(sin(th));
+    }
+
     // calc_lower_metric!: Kerr :66-75, Schwarzschild :15-21, Minkowski :10-16
     void lower_metric(const double* x, double g[4][4]) const {
         for (int i = 0; i < 4; ++i)
@@ -198,14 +286,7 @@ struct OScene {
             g[2][2] = sq(wh_r(r));
             g[3][3] = sq(wh_r(r) * std::sin(th));
         } else if (is_kerr()) {
-            double Sig, Del, A;
-            kerr_params(r, th, Sig, Del, A);
-            g[0][0] = -(1.0 - rs * r / Sig);
-            g[0][3] = -rs * a * r * sq(std::sin(th)) / Sig;
-            g[3][0] = g[0][3];
-            g[1][1] = Sig / Del;
-            g[2][2] = Sig;
-            g[3][3] = (A / Sig) * sq(std::sin(th));
+            kerr_metric_t<double>(r, th, a, g);
         } else if (kind == RTW_SCENE_SCHWARZSCHILD_DISK) {
             g[0][0] = -(1.0 - rs / r);
             g[1][1] = 1.0 / (1.0 - rs / r);
@@ -249,13 +330,15 @@ struct OScene {
         }
     }
 
-    template <class F>
-    void kerr_christoffel(F r, F th, F al, F rsv, double G[4][4][4]) const {
+    template <class F, class GT>
+    void kerr_christoffel(F r, F th, F al, F rsv, GT G[4][4][4]) const {
+        using std::cos;
+        using std::sin;
         const F two = 2;
-        const F Sig = r * r + (al * std::cos(th)) * (al * std::cos(th));
+        const F Sig = r * r + (al * cos(th)) * (al * cos(th));
         const F Del = r * r - r * rsv + al * al;
-        const F A = (r * r + al * al) * Sig + rsv * r * (al * std::sin(th)) * (al * std::sin(th));
-        const F s = std::sin(th), c = std::cos(th), s2t = std::sin(two * th);
+        const F A = (r * r + al * al) * Sig + rsv * r * (al * sin(th)) * (al * sin(th));
+        const F s = sin(th), c = cos(th), s2t = sin(two * th);
         const F cot = c / s;  // cot(theta)
         const F ac2 = (al * c) * (al * c), as2 = (al * s) * (al * s);
         const F Sig2 = Sig * Sig, Sig3 = Sig * Sig * Sig;
@@ -315,9 +398,9 @@ struct OScene {
         }
         if (is_kerr()) {
             if (refprec)
-                kerr_christoffel<float>((float)r, (float)th, (float)a, (float)rs, G);
+                kerr_christoffel<float, double>((float)r, (float)th, (float)a, (float)rs, G);
             else
-                kerr_christoffel<double>(r, th, a, rs, G);
+                kerr_christoffel<double, double>(r, th, a, rs, G);
         } else if (kind == RTW_SCENE_SCHWARZSCHILD_DISK) {
             G[0][0][1] = rs / (2 * r * (r - rs));
             G[0][1][0] = G[0][0][1];
@@ -585,55 +668,69 @@ struct RayWork {
 };
 
 // RT slopes of the synchrotron torus (no reference counterpart; the formulas
-// are listed in the file header). slope[8 + 2c] = dI_c, slope[9 + 2c] = dtau_c.
-void torus_bins(const OScene& sc, RayWork& w, const double* R, double* slope) {
-    for (int c = 0; c < w.N; ++c) {
+// are listed in the file header), over the scalar type: spin al and the
+// emission parameters n0, b0, th0 are arguments so that forward-mode tangents
+// can enter through them. slope[8 + 2c] = dI_c, slope[9 + 2c] = dtau_c.
+template <class T>
+void torus_bins_t(const OScene& sc, const T& al, const T& n0, const T& b0, const T& th0, const double* freq, int N,
+                  const T* R, T* slope) {
+    using std::cos;
+    using std::cyl_bessel_k;
+    using std::exp;
+    using std::expm1;
+    using std::pow;
+    using std::sqrt;
+    for (int c = 0; c < N; ++c) {
         slope[8 + 2 * c] = 0;
         slope[9 + 2 * c] = 0;
     }
-    const double r = R[1], th = R[2];
+    const T r = R[1], th = R[2];
     const double cut_in = std::max(sc.r_in - 4 * sc.edge_in, 1.01 * sc.r_ev);
     const double cut_out = sc.r_out + 4 * sc.edge_out;
-    if (!(r >= cut_in && r <= cut_out)) return;
-    double taper = 1;
-    if (r < sc.r_in) taper = std::exp(-sq((sc.r_in - r) / sc.edge_in));
-    else if (r > sc.r_out) taper = std::exp(-sq((r - sc.r_out) / sc.edge_out));
-    const double x = r / sc.r_in;
-    const double z = r * std::cos(th), hz = sc.rho_h * r;
-    const double ne = sc.n0 * std::pow(x, sc.rho_idx) * std::exp(-z * z / (2 * hz * hz)) * taper;
-    const double B = sc.b0 * std::pow(x, sc.b_idx);
-    const double Th = sc.th0 * std::pow(x, sc.t_idx);
-    sc.lower_metric(R, w.g);
-    const double Om = std::sqrt(sc.M) / (std::pow(r, 1.5) + sc.a * std::sqrt(sc.M));
-    const double n2 = -(w.g[0][0] + 2 * Om * w.g[0][3] + Om * Om * w.g[3][3]);
-    if (!(n2 > 0)) return;
-    const double ut = 1 / std::sqrt(n2);
-    const double u_t = ut * (w.g[0][0] + Om * w.g[0][3]);
-    const double u_p = ut * (w.g[0][3] + Om * w.g[3][3]);
-    const double gs = -(u_t * R[4] + u_p * R[7]);
-    const double kph_low = w.g[0][3] * R[4] + w.g[3][3] * R[7];
-    const double bb = w.g[3][3] + u_p * u_p;
-    const double bk = kph_low - u_p * gs;
-    if (!(bb > 0) || !(gs > 0)) return;
-    const double c2 = bk * bk / (bb * gs * gs);
-    if (!(1 - c2 > 1e-12)) return;
-    const double sinb = std::sqrt(1 - c2);
+    if (!(val(r) >= cut_in && val(r) <= cut_out)) return;
+    T taper = 1;
+    if (r < sc.r_in) taper = exp(-sqT((sc.r_in - r) / sc.edge_in));
+    else if (r > sc.r_out) taper = exp(-sqT((r - sc.r_out) / sc.edge_out));
+    const T x = r / sc.r_in;
+    const T z = r * cos(th), hz = sc.rho_h * r;
+    const T ne = n0 * pow(x, sc.rho_idx) * exp(-z * z / (2 * hz * hz)) * taper;
+    const T B = b0 * pow(x, sc.b_idx);
+    const T Th = th0 * pow(x, sc.t_idx);
+    T g[4][4];
+    sc.kerr_metric_t<T>(r, th, al, g);
+    const T Om = std::sqrt(sc.M) / (pow(r, 1.5) + al * std::sqrt(sc.M));
+    const T n2 = -(g[0][0] + 2 * Om * g[0][3] + Om * Om * g[3][3]);
+    if (!(val(n2) > 0)) return;
+    const T ut = 1 / sqrt(n2);
+    const T u_t = ut * (g[0][0] + Om * g[0][3]);
+    const T u_p = ut * (g[0][3] + Om * g[3][3]);
+    const T gs = -(u_t * R[4] + u_p * R[7]);
+    const T kph_low = g[0][3] * R[4] + g[3][3] * R[7];
+    const T bb = g[3][3] + u_p * u_p;
+    const T bk = kph_low - u_p * gs;
+    if (!(val(bb) > 0) || !(val(gs) > 0)) return;
+    const T c2 = bk * bk / (bb * gs * gs);
+    if (!(val(1 - c2) > 1e-12)) return;
+    const T sinb = sqrt(1 - c2);
     constexpr double e = 4.80320425e-10, cc = 2.99792458e10, me = 9.1093837015e-28, h = 6.62607015e-27;
-    const double nus = 2.0 / 9.0 * (e * B / (2 * kPi * me * cc)) * Th * Th * sinb;
-    const double k2 = std::cyl_bessel_k(2.0, 1 / Th);
-    for (int c = 0; c < w.N; ++c) {
-        const double nu = gs * kLightC * 1e9 * w.freq[c];  // Hz in the fluid frame
-        const double X = nu / nus;
-        if (!(X > 0) || X > 2.0e5) continue;
-        const double j = ne * std::sqrt(2.0) * kPi * e * e * nus / (3 * cc * k2) *
-                         sq(std::sqrt(X) + std::pow(2.0, 11.0 / 12) * std::pow(X, 1.0 / 6)) *
-                         std::exp(-std::pow(X, 1.0 / 3));
-        const double bnu = 2 * h * nu * nu * nu / (cc * cc) / std::expm1(h * nu / (Th * me * cc * cc));
-        const double j_u = j * sc.length_cm, a_u = j / bnu * sc.length_cm;
-        const double nu_nm = gs * w.freq[c];
-        slope[8 + 2 * c] = -(1 / gs) * j_u * std::exp(-R[9 + 2 * c]) / (nu_nm * nu_nm * nu_nm);
+    const T nus = 2.0 / 9.0 * (e * B / (2 * kPi * me * cc)) * Th * Th * sinb;
+    const T k2 = cyl_bessel_k(2.0, 1 / Th);
+    for (int c = 0; c < N; ++c) {
+        const T nu = gs * kLightC * 1e9 * freq[c];  // Hz in the fluid frame
+        const T X = nu / nus;
+        if (!(val(X) > 0) || val(X) > 2.0e5) continue;
+        const T j = ne * std::sqrt(2.0) * kPi * e * e * nus / (3 * cc * k2) *
+                    sqT(sqrt(X) + std::pow(2.0, 11.0 / 12) * pow(X, 1.0 / 6)) * exp(-pow(X, 1.0 / 3));
+        const T bnu = 2 * h * nu * nu * nu / (cc * cc) / expm1(h * nu / (Th * me * cc * cc));
+        const T j_u = j * sc.length_cm, a_u = j / bnu * sc.length_cm;
+        const T nu_nm = gs * freq[c];
+        slope[8 + 2 * c] = -(1 / gs) * j_u * exp(-R[9 + 2 * c]) / (nu_nm * nu_nm * nu_nm);
         slope[9 + 2 * c] = -(1 / gs) * a_u;
     }
+}
+
+void torus_bins(const OScene& sc, RayWork& w, const double* R, double* slope) {
+    torus_bins_t<double>(sc, sc.a, sc.n0, sc.b0, sc.th0, w.freq, w.N, R, slope);
 }
 
 // RT slopes of Powehi.source (the reference's M87* model, source_model.jl:
@@ -1137,6 +1234,196 @@ void camera_ray(const CameraGeom& cg, const rtw_camera& cam, int i, int j, doubl
 }
 
 // ----------------------------------------------------------------------------
+// The synchrotron torus's render over the scalar type T (double: the same
+// arithmetic as the render loop above; D5: forward-mode tangents). Restates,
+// for the Kerr torus only: calc_ray_derivative! (integrators_LttM.jl:9-48),
+// RKDP_Step_w_buffer! with the FSAL step (integrators_LttM.jl:54-224),
+// pad_max_dt (Kerr model :86-103), near_singularity (Kerr geometry :249-269),
+// keepinbounds! (:275-301) and the camera (initialization.jl:190-331) with
+// the Kerr inverse vierbein (:112-121).
+//
+// Step sizes: mode 1 carries tangents through every step size, the
+// controller's err^(-1/5) included (what forward-mode differentiation of the
+// whole program gives). Mode 0 keeps a step size's tangent only where it is
+// -pad_max_dt (the first step, after a polar escape, and where the
+// controller's proposal is capped by max_dt) and holds the controller's own
+// choices fixed: the convention of the discrete adjoint.
+// ----------------------------------------------------------------------------
+template <class T>
+struct TorusFwd {
+    const OScene& sc;
+    T al, n0, b0, th0;  // spin and the emission parameters, with their tangents
+    const double* freq;
+    int N, L;
+    double tol, scale;
+    int mode;
+    std::vector<T> k1, buf, y, k2, k3, k4, k5, k6, k7, ns;
+
+    TorusFwd(const OScene& s, int n, const double* f, double tol_, double scale_, int mode_)
+        : sc(s), freq(f), N(n), L(8 + 2 * n), tol(tol_), scale(scale_), mode(mode_) {
+        for (auto* v : {&k1, &buf, &y, &k2, &k3, &k4, &k5, &k6, &k7, &ns}) v->assign(L, T(0));
+    }
+
+    void rhs(const T* R, T* slope) const {
+        for (int i = 0; i < 4; ++i) slope[i] = R[i + 4];
+        T G[4][4][4];
+        for (auto& a : G)
+            for (auto& b : a)
+                for (auto& c : b) c = 0;
+        sc.kerr_christoffel<T, T>(R[1], R[2], al, T(sc.rs), G);
+        for (int i = 0; i < 4; ++i) {
+            T acc = 0;
+            for (int j = 0; j < 4; ++j)
+                for (int k = 0; k < 4; ++k) acc -= G[i][j][k] * R[4 + j] * R[4 + k];
+            slope[4 + i] = acc;
+        }
+        torus_bins_t<T>(sc, al, n0, b0, th0, freq, N, R, slope);
+    }
+
+    static T tmin(const T& a, const T& b) { return val(b) < val(a) ? b : a; }
+    static T tmax(const T& a, const T& b) { return val(a) < val(b) ? b : a; }
+
+    T pad_max_dt(const T* x) const {
+        using std::fabs;
+        const double sc32 = (double)(float)scale;
+        double eps;
+        if (val(x[2]) < kPi / 8 || val(x[2]) > 7 * kPi / 8) eps = std::min(sc32, (double)1e-1f);
+        else eps = sc32;
+        const T first = fabs(1.0 / (eps / fabs(x[5]))) + kNoDivZero;
+        const T second = fabs(1.0 / (eps * tmin(x[2], kPi - x[2]) / (fabs(x[6]) + kNoDivZero) + kNoDivZero));
+        const T third = fabs(1.0 / (eps / (fabs(x[7]) + kNoDivZero) + kNoDivZero));
+        T m = tmin(1.0 / (first + second + third + kNoDivZero), T(0.5));
+        return tmax(m, T((double)1e-12f));
+    }
+
+    bool near_singularity(const T* x, const T& h, T* temp) const {
+        using std::fabs;
+        const T th_new = x[2] + h * x[6];
+        if (val(fabs(th_new)) <= tol) {
+            *temp = 2 * fabs(x[2]) / (fabs(x[6] * 37) + kNoDivZero);
+            return true;
+        } else if (val(fabs(th_new - kPi)) <= tol) {
+            *temp = 2 * fabs((x[2] - kPi) / (fabs(x[6] * 37) + kNoDivZero));
+            return true;
+        }
+        *temp = h;
+        return false;
+    }
+
+    void keepinbounds(T* x) const {
+        if (val(x[2]) < 0) {
+            x[2] = -x[2];
+            x[3] = x[3] - kPi;
+            x[6] = -x[6];
+        }
+        const double m = jl_mod(val(x[2]), 2 * kPi);
+        x[2] = x[2] + (m - val(x[2]));  // mod(theta, 2 pi): the shift carries no tangent
+        if (val(x[2]) >= kPi) {
+            x[2] = 2 * kPi - x[2];
+            x[3] = x[3] + kPi;
+            x[6] = -x[6];
+        }
+    }
+
+    int terminate(const T* R, long long max_steps, long long step_count) const {
+        std::vector<double> v(L);
+        for (int i = 0; i < L; ++i) v[i] = val(R[i]);
+        return sc.terminate(v.data(), L, tol, max_steps, step_count);
+    }
+
+    // a step size the controller chose: mode 0 keeps the tangent of -max_dt only
+    T held(const T& hn, const T& max_dt) const {
+        if (mode == 1) return hn;
+        if (val(hn) == val(-max_dt)) return -max_dt;
+        return T(val(hn));
+    }
+
+    // one call of RKDP_Step_w_buffer! with the FSAL step (the torus's)
+    T step(T* R, T h, bool prev_rejected, bool* rejected, long long* esc) {
+        using std::fabs;
+        using std::pow;
+        using std::sqrt;
+        const T max_dt = pad_max_dt(R);
+        T temp;
+        if (near_singularity(R, h, &temp)) {
+            for (int i = 0; i < L; ++i) R[i] = R[i] - temp * k1[i];
+            keepinbounds(R);
+            ++*esc;
+            for (int it = 0; it < 36; ++it) {
+                if (!terminate(R, 2, 1)) {
+                    rhs(R, k1.data());
+                    for (int j = 0; j < L; ++j) R[j] = R[j] - temp * k1[j];
+                    keepinbounds(R);
+                    ++*esc;
+                }
+            }
+            if (terminate(R, 2, 1)) {
+                *rejected = false;
+                return h;
+            }
+            rhs(R, k1.data());
+            h = -pad_max_dt(R);
+        }
+        const auto& A = kDP.a;
+        for (int i = 0; i < L; ++i) buf[i] = R[i] + h * k1[i] * A[2][2];
+        rhs(buf.data(), k2.data());
+        for (int i = 0; i < L; ++i) buf[i] = R[i] + h * (k1[i] * A[3][2] + k2[i] * A[3][3]);
+        rhs(buf.data(), k3.data());
+        for (int i = 0; i < L; ++i) buf[i] = R[i] + h * (k1[i] * A[4][2] + k2[i] * A[4][3] + k3[i] * A[4][4]);
+        rhs(buf.data(), k4.data());
+        for (int i = 0; i < L; ++i)
+            buf[i] = R[i] + h * (k1[i] * A[5][2] + k2[i] * A[5][3] + k3[i] * A[5][4] + k4[i] * A[5][5]);
+        rhs(buf.data(), k5.data());
+        for (int i = 0; i < L; ++i)
+            buf[i] = R[i] + h * (k1[i] * A[6][2] + k2[i] * A[6][3] + k3[i] * A[6][4] + k4[i] * A[6][5] +
+                                 k5[i] * A[6][6]);
+        rhs(buf.data(), k6.data());
+        for (int i = 0; i < L; ++i)
+            ns[i] = k1[i] * A[7][2] + k3[i] * A[7][4] + k4[i] * A[7][5] + k5[i] * A[7][6] + k6[i] * A[7][7];
+        for (int i = 0; i < L; ++i) buf[i] = R[i] + h * ns[i];
+        rhs(buf.data(), k7.data());
+        for (int i = 0; i < L; ++i) y[i] = R[i] + h * ns[i];
+        T err = 0;
+        for (int i = 0; i < L; ++i) {
+            const T d = y[i] - R[i] -
+                        h * (k1[i] * A[9][2] + k3[i] * A[9][4] + k4[i] * A[9][5] + k5[i] * A[9][6] +
+                             k6[i] * A[9][7] + k7[i] * A[9][8]);
+            const T tl = tol + tmax(fabs(R[i]), fabs(y[i])) * tol;
+            err = err + sqT(d / tl);
+        }
+        err = sqrt(err / L);
+        T hn = 0.9 * h * pow(1.0 / err, 1.0 / 5);
+        if (val(fabs(hn)) > val(max_dt)) hn = -max_dt;
+        if (val(err) == 0 || !isfinite(val(hn))) {
+            const double th_before = val(y[2]);
+            keepinbounds(y.data());
+            for (int i = 0; i < L; ++i) {
+                k1[i] = k7[i];
+                R[i] = y[i];
+            }
+            if (val(y[2]) != th_before) rhs(R, k1.data());
+            *rejected = false;
+            return held(h, max_dt);
+        } else if (val(err) > 1) {
+            if (prev_rejected && val(fabs(hn)) >= val(fabs(h))) hn = h / 2;
+            keepinbounds(R);
+            *rejected = true;
+            return held(hn, max_dt);
+        }
+        if (val(fabs(hn)) > 5 * val(fabs(h))) hn = 5 * h;
+        const double th_before = val(y[2]);
+        keepinbounds(y.data());
+        for (int i = 0; i < L; ++i) {
+            k1[i] = k7[i];
+            R[i] = y[i];
+        }
+        if (val(y[2]) != th_before) rhs(R, k1.data());
+        *rejected = false;
+        return held(hn, max_dt);
+    }
+};
+
+// ----------------------------------------------------------------------------
 // CIE (color_theory.jl)
 // ----------------------------------------------------------------------------
 const double kCie[4][7] = {
@@ -1427,6 +1714,127 @@ int oracle_set_skybox(int k, const float* tex, int h) {
     return RTW_OK;
 }
 
+
+// Forward-mode tangents of the synchrotron torus's render (FSAL step): per
+// pixel the spectrum (I per bin) and dI/d(spin, inclination, n_e0, b_0,
+// theta_e0) [n][n_colors][5], inclination in radians (the camera's theta).
+// mode 0: the discrete adjoint's convention for step sizes, 1: tangents
+// through every step size (see TorusFwd). Optional class, step counts and
+// polar Euler sub-steps per pixel.
+int oracle_torus_forward(const rtw_scene* scene, rtw_camera* cam, const double* colors_nm, int n_colors,
+                         double max_dt_scale, int mode, const long long* pixel_ids, long long n_ids,
+                         double* spectrum, double* tangents, unsigned char* cls, unsigned int* steps, int* escapes,
+                         int n_threads) {
+    if (!scene || !cam || !colors_nm || n_colors <= 0 || n_colors > RTW_MAX_BINS) return RTW_ERR_INVALID_PARAM;
+    if (scene->kind != RTW_SCENE_KERR_SYNCHRO_TORUS || (mode != 0 && mode != 1)) return RTW_ERR_UNSUPPORTED;
+    if (cam->speed != 0) return RTW_ERR_UNSUPPORTED;  // a static camera: theta is the inclination
+    OScene sc(*scene);
+    if (sc.is_singularity(cam->position)) return RTW_ERR_INVALID_CAMERA;
+    CameraGeom cg;
+    camera_geom(sc, *cam, cg);
+    cam->y_pix = cg.yp;
+    const long long P = (long long)cg.xp * cg.yp;
+    const long long n = pixel_ids ? n_ids : P;
+    // e R2 L R as camera_geom forms it; only the inverse vierbein carries tangents
+    Mat4 Rm, Lm, R2;
+    intrinsic_rotation(cam->pointing, Rm);
+    boost_z(-cam->speed, Lm);
+    final_rotation(cam->direction, R2);
+    D5 al(sc.a), thc(cam->position[2]), n0(sc.n0), b0(sc.b0), th0(sc.th0);
+    al.d[0] = 1;
+    thc.d[1] = 1;
+    n0.d[2] = 1;
+    b0.d[3] = 1;
+    th0.d[4] = 1;
+    D5 e[4][4];
+    {
+        using std::cos;
+        using std::sin;
+        using std::sqrt;
+        const D5 r(cam->position[1]);
+        const D5 Sig = r * r + sqT(al * cos(thc));
+        const D5 Del = r * r - r * sc.rs + al * al;
+        const D5 A = (r * r + al * al) * Sig + sc.rs * r * sqT(al * sin(thc));
+        e[0][0] = sqrt(A / (Sig * Del));
+        e[3][0] = (sc.rs * al * r / A) * e[0][0];
+        e[1][1] = sqrt(Del / Sig);
+        e[2][2] = 1.0 / sqrt(Sig);
+        e[3][3] = sqrt(Sig / A) / sin(thc);
+    }
+    auto mul = [](const D5 a[4][4], const Mat4 b, D5 c[4][4]) {
+        for (int i = 0; i < 4; ++i)
+            for (int j = 0; j < 4; ++j) {
+                D5 acc = 0;
+                for (int k = 0; k < 4; ++k) acc += a[i][k] * b[k][j];
+                c[i][j] = acc;
+            }
+    };
+    D5 t1[4][4], t2[4][4], M[4][4];
+    mul(e, R2, t1);
+    mul(t1, Lm, t2);
+    mul(t2, Rm, M);
+    std::vector<double> freq(n_colors);
+    for (int c = 0; c < n_colors; ++c) freq[c] = 1.0 / colors_nm[c];
+    const int N = n_colors, L = 8 + 2 * N;
+    const double tol = cam->tolerance;
+    const long long max_steps = cam->max_steps;
+    const int nt = n_threads > 0 ? n_threads : omp_get_max_threads();
+#pragma omp parallel for num_threads(nt) schedule(dynamic, 1)
+    for (long long q = 0; q < n; ++q) {
+        TorusFwd<D5> w(sc, N, freq.data(), tol, max_dt_scale, mode);
+        w.al = al;
+        w.n0 = n0;
+        w.b0 = b0;
+        w.th0 = th0;
+        const long long p = pixel_ids ? pixel_ids[q] : q;
+        const int i = (int)(p % cg.xp), j = (int)(p / cg.xp);
+        const double wq = cg.rh * ((i + 1) - 0.5) - cg.W;
+        const double hq = cg.rv * ((j + 1) - 0.5) - cg.H;
+        const double th = std::atan(std::sqrt(wq * wq + hq * hq));
+        double ph;
+        if (wq > 0) ph = std::atan(hq / wq);
+        else if (wq < 0 && hq >= 0) ph = std::atan(hq / wq) + kPi;
+        else if (wq < 0 && hq < 0) ph = std::atan(hq / wq) - kPi;
+        else if (wq == 0 && hq > 0) ph = kPi / 2;
+        else if (wq == 0 && hq < 0) ph = -kPi / 2;
+        else ph = 0;
+        const double v[4] = {1, -std::sin(th) * std::cos(ph), -std::sin(th) * std::sin(ph), -std::cos(th)};
+        std::vector<D5> ray(L, D5(0.0));
+        ray[0] = cam->position[0];
+        ray[1] = cam->position[1];
+        ray[2] = thc;
+        ray[3] = cam->position[3];
+        for (int rr = 0; rr < 4; ++rr) {
+            D5 acc = 0;
+            for (int k = 0; k < 4; ++k) acc += M[rr][k] * v[k];
+            ray[4 + rr] = acc;
+        }
+        D5 dt = -w.pad_max_dt(ray.data());
+        w.rhs(ray.data(), w.k1.data());
+        bool rejected = false;
+        long long step_count = 0, esc = 0;
+        int klass = 0;
+        while (true) {
+            bool rj = false;
+            dt = w.step(ray.data(), dt, rejected, &rj, &esc);
+            rejected = rj;
+            ++step_count;
+            klass = w.terminate(ray.data(), max_steps, step_count);
+            if (klass) break;
+        }
+        for (int k = 0; k < 8; ++k)
+            if (!std::isfinite(ray[k].v)) klass = RTW_CLASS_NAN;
+        if (cls) cls[q] = (unsigned char)klass;
+        if (steps) steps[q] = (unsigned int)step_count;
+        if (escapes) escapes[q] = (int)esc;
+        for (int c = 0; c < N; ++c) {
+            if (spectrum) spectrum[(long long)N * q + c] = ray[8 + 2 * c].v;
+            if (tangents)
+                for (int t = 0; t < kTan; ++t) tangents[((long long)N * q + c) * kTan + t] = ray[8 + 2 * c].d[t];
+        }
+    }
+    return RTW_OK;
+}
 
 int oracle_abi_version(void) { return RTW_ABI_VERSION; }
 

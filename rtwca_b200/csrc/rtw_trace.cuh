@@ -35,13 +35,20 @@ namespace rtw {
 
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kMaxWarps = 4;  // warps per CTA (launch bound 128 threads)
-// rays whose spectral bins one pass of the spectral phase updates (1
-// measured fastest: wider passes grow the hot loop's code more than their
-// overlapped chains save)
-#ifndef RTW_SPEC_RAYS
-#define RTW_SPEC_RAYS 1
+// Lanes that share one ray's bins in a pass of the spectral phase (32, 16 or
+// 8): a pass serves 32 / RTW_SPEC_LANES rays at once, each lane taking
+// BPL * 32 / RTW_SPEC_LANES of its ray's bins. 32 serves one ray per pass.
+// Measured on the Kerr disk at 1024^2 (64 bins, FP32-mixed, reference step):
+// 32 lanes 385 ms, 16 lanes 376 ms, 8 lanes 405 ms (fewer passes, but each
+// pass's chain is longer and the register demand spills into the geodesic
+// phase); the spectral pass is bound by its dependency chain, not by the
+// number of passes.
+#ifndef RTW_SPEC_LANES
+#define RTW_SPEC_LANES 16
 #endif
-constexpr int kSpecRays = RTW_SPEC_RAYS;
+constexpr int kSpecLanes = RTW_SPEC_LANES;
+static_assert(kSpecLanes == 32 || kSpecLanes == 16 || kSpecLanes == 8 || kSpecLanes == 4, "RTW_SPEC_LANES");
+constexpr int kSpecGroups = 32 / kSpecLanes;
 
 // Dormand-Prince coefficients (64BitConstants.jl:28-37): a_sl, b_l (= a_7l), b*_l.
 constexpr double a21 = 1.0 / 5;
@@ -535,6 +542,15 @@ __global__ void __launch_bounds__(128, MIXED ? RTW_MIXED_MIN_CTAS : 2) trace_ker
         const int c = lane + 32 * b;
         nub[b] = c < N ? SR(p.bin_nu[c]) : SR(0);
     }
+    // the lane's bins in a spectral pass (c = sub + kSpecLanes * b)
+    constexpr int kBL = BPL * kSpecGroups;
+    const int grp = lane / kSpecLanes, sub = lane % kSpecLanes;
+    SR nus[kBL];
+#pragma unroll
+    for (int b = 0; b < kBL; ++b) {
+        const int c = sub + kSpecLanes * b;
+        nus[b] = c < N ? SR(p.bin_nu[c]) : SR(0);
+    }
 
     // lane ray state
     bool active = false, dry = false;
@@ -698,113 +714,106 @@ __global__ void __launch_bounds__(128, MIXED ? RTW_MIXED_MIN_CTAS : 2) trace_ker
         RTW_PHASE(cy_geo);
 
         // ---------------- spectral phase (warp-cooperative) --------------
-        // kSpecRays rays per pass: their bin chains (scratch loads, stage
-        // slopes, error reduction, decision, write-back) are independent, so
-        // they overlap. Each ray's arithmetic and reduction order do not
-        // depend on which rays share its pass.
+        // Each pass serves the next kSpecGroups rays of the warp that need
+        // bin work; kSpecLanes consecutive lanes split one ray's bins (bin
+        // c = sub + kSpecLanes * b). A ray's arithmetic and the association
+        // order of its error sum depend on kSpecLanes only, not on which
+        // rays share its pass or which lane traces it.
         const bool need = active && !esc_done && (emit || spec_live);
         unsigned nm = __ballot_sync(kFull, need);
         if (need) ++c_spec;
         while (nm) {
-            int rg[kSpecRays];
-            bool vg[kSpecRays];
+            const unsigned pass_rays = nm;
+            // this group's ray: the (grp+1)-th set bit of nm
+            unsigned mg = nm;
 #pragma unroll
-            for (int g = 0; g < kSpecRays; ++g) {
-                vg[g] = nm != 0u;
-                rg[g] = vg[g] ? __ffs(nm) - 1 : rg[0];  // an empty slot repeats ray 0, discarded
-                nm &= nm - 1u;
+            for (int g = 0; g < kSpecGroups - 1; ++g)
+                if (g < grp) mg &= mg - 1u;
+            const bool vg = mg != 0u;
+            const int r = vg ? __ffs(mg) - 1 : __ffs(nm) - 1;  // an empty group repeats the first ray, discarded
+#pragma unroll
+            for (int g = 0; g < kSpecGroups; ++g) nm &= nm - 1u;
+            SR Ar[5], Xr[5];
+#pragma unroll
+            for (int j = 0; j < 5; ++j) {  // stages 3..7
+                Ar[j] = s_ax[wib][0][j + 1][r];
+                Xr[j] = x_for_bins(s_ax[wib][1][j + 1][r]);
             }
-            SR yv[kSpecRays][BPL], yl[kSpecRays][BPL], nk[kSpecRays][BPL];
-            SR acc[kSpecRays];
-            bool nz[kSpecRays];
+            const SR hs = SR(__shfl_sync(kFull, h, r));
+            const SR ts = SR(__shfl_sync(kFull, tol, r));
+            SR yv[kBL], yl[kBL], nk[kBL];
+            SR acc = 0;
+            bool nz = false;
+            // Branch-free over the lane's bins: a row holds np >= N slots, so
+            // every load is in bounds; slots past N only feed discarded values.
 #pragma unroll
-            for (int g = 0; g < kSpecRays; ++g) {
-                const int r = rg[g];
-                SR Ar[5], Xr[5];
-#pragma unroll
-                for (int j = 0; j < 5; ++j) {  // stages 3..7
-                    Ar[j] = s_ax[wib][0][j + 1][r];
-                    Xr[j] = x_for_bins(s_ax[wib][1][j + 1][r]);
+            for (int b = 0; b < kBL; ++b) {
+                const int c = sub + kSpecLanes * b;
+                const bool ok = c < N;
+                const SR I = sI[r * np + c];
+                const SR kk1 = sK[r * np + c];
+                const SR nuc = nus[b];
+                const SR kk3 = bin_slope(Ar[0], Xr[0], nuc);
+                const SR kk4 = bin_slope(Ar[1], Xr[1], nuc);
+                const SR kk5 = bin_slope(Ar[2], Xr[2], nuc);
+                const SR kk6 = bin_slope(Ar[3], Xr[3], nuc);
+                const SR kk7 = bin_slope(Ar[4], Xr[4], nuc);
+                // (k2 has zero weight in both the 5th-order update and the
+                // error estimate, and the intensity slopes do not depend on
+                // the intensity, so stage 2 needs no bin work.)
+                const SR ns = kk1 * SR(b1) + kk3 * SR(b3) + kk4 * SR(b4) + kk5 * SR(b5) + kk6 * SR(b6);
+                const SR es = kk1 * SR(e1) + kk3 * SR(e3) + kk4 * SR(e4) + kk5 * SR(e5) + kk6 * SR(e6) +
+                              kk7 * SR(e7);
+                SR yy, ylo = 0;
+                if constexpr (MIXED) {
+                    float hi = I, lo = sL[r * np + c];
+                    kahan_add(hi, lo, hs * ns);
+                    yy = hi;
+                    ylo = lo;
+                } else {
+                    yy = I + hs * ns;
                 }
-                const SR hs = SR(__shfl_sync(kFull, h, r));
-                const SR ts = SR(__shfl_sync(kFull, tol, r));
-                acc[g] = 0;
-                nz[g] = false;
-                // Branch-free over the lane's bins: a row holds np >= N slots, so
-                // every load is in bounds; slots past N only feed discarded values.
-#pragma unroll
-                for (int b = 0; b < BPL; ++b) {
-                    const int c = lane + 32 * b;
-                    const bool ok = c < N;
-                    const SR I = sI[r * np + c];
-                    const SR kk1 = sK[r * np + c];
-                    const SR kk3 = bin_slope(Ar[0], Xr[0], nub[b]);
-                    const SR kk4 = bin_slope(Ar[1], Xr[1], nub[b]);
-                    const SR kk5 = bin_slope(Ar[2], Xr[2], nub[b]);
-                    const SR kk6 = bin_slope(Ar[3], Xr[3], nub[b]);
-                    const SR kk7 = bin_slope(Ar[4], Xr[4], nub[b]);
-                    // (k2 has zero weight in both the 5th-order update and the
-                    // error estimate, and the intensity slopes do not depend on
-                    // the intensity, so stage 2 needs no bin work.)
-                    const SR ns = kk1 * SR(b1) + kk3 * SR(b3) + kk4 * SR(b4) + kk5 * SR(b5) + kk6 * SR(b6);
-                    const SR es = kk1 * SR(e1) + kk3 * SR(e3) + kk4 * SR(e4) + kk5 * SR(e5) + kk6 * SR(e6) +
-                                  kk7 * SR(e7);
-                    SR yy, ylo = 0;
-                    if constexpr (MIXED) {
-                        float hi = I, lo = sL[r * np + c];
-                        kahan_add(hi, lo, hs * ns);
-                        yy = hi;
-                        ylo = lo;
-                    } else {
-                        yy = I + hs * ns;
-                    }
-                    const SR d = hs * es;
-                    const SR tl = ts + rmax(rabs(I), rabs(yy)) * ts;
-                    const SR q = cdiv(d, tl);
-                    acc[g] += ok ? q * q : SR(0);
-                    yv[g][b] = yy;
-                    yl[g][b] = ylo;
-                    nk[g][b] = p.fsal ? kk7 : ns;
-                    nz[g] |= ok && nk[g][b] != SR(0);
-                }
+                const SR d = hs * es;
+                const SR tl = ts + rmax(rabs(I), rabs(yy)) * ts;
+                const SR q = cdiv(d, tl);
+                acc += ok ? q * q : SR(0);
+                yv[b] = yy;
+                yl[b] = ylo;
+                nk[b] = p.fsal ? kk7 : ns;
+                nz |= ok && nk[b] != SR(0);
             }
+            // the group's sum, in one association order, in every lane of the group
 #pragma unroll
-            for (int g = 0; g < kSpecRays; ++g) acc[g] = warp_sum(acc[g]);
+            for (int o = kSpecLanes / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(kFull, acc, o);
+            acc = __shfl_sync(kFull, acc, grp * kSpecLanes);
             // the lane that owns a ray of this pass decides its attempt
-            int gown = -1;
-#pragma unroll
-            for (int g = 0; g < kSpecRays; ++g)
-                if (vg[g] && lane == rg[g] && gown < 0) gown = g;
-            SR aown = acc[0];
-#pragma unroll
-            for (int g = 1; g < kSpecRays; ++g)
-                if (gown == g) aown = acc[g];
+            const int rank = __popc(pass_rays & ((1u << lane) - 1u));
+            const bool own = ((pass_rays >> lane) & 1u) && rank < kSpecGroups;
+            const SR aown = __shfl_sync(kFull, acc, own ? rank * kSpecLanes : 0);
             int dec = 0;
-            if (gown >= 0) {
+            if (own) {
                 decide<CT>(err2 + CT(aown), L, h, max_dt, prev_rej, accept, hnext);
                 decided = true;
                 dec = accept ? 1 : 0;
             }
-            bool nzown = false;
+            // every lane takes part in each collective (a full-mask shuffle
+            // skipped by some lanes is undefined)
+            const int dsrc = __shfl_sync(kFull, dec, r);
+            const bool dg = vg && dsrc != 0;
+            if (dg) {
 #pragma unroll
-            for (int g = 0; g < kSpecRays; ++g) {
-                const int r = rg[g];
-                const bool dg = vg[g] && __shfl_sync(kFull, dec, r) != 0;
-                if (dg) {
-#pragma unroll
-                    for (int b = 0; b < BPL; ++b) {
-                        const int c = lane + 32 * b;
-                        if (c < N) {
-                            sI[r * np + c] = yv[g][b];
-                            sK[r * np + c] = nk[g][b];
-                            if constexpr (MIXED) sL[r * np + c] = yl[g][b];
-                        }
+                for (int b = 0; b < kBL; ++b) {
+                    const int c = sub + kSpecLanes * b;
+                    if (c < N) {
+                        sI[r * np + c] = yv[b];
+                        sK[r * np + c] = nk[b];
+                        if constexpr (MIXED) sL[r * np + c] = yl[b];
                     }
                 }
-                const bool nzg = __any_sync(kFull, nz[g]);
-                if (gown == g) nzown = nzg;
             }
-            if (gown >= 0 && dec) spec_live = nzown;
+            const unsigned nzb = __ballot_sync(kFull, vg && nz);
+            constexpr unsigned kGroupMask = kSpecLanes == 32 ? kFull : ((1u << kSpecLanes) - 1u);
+            if (own && dec) spec_live = ((nzb >> (rank * kSpecLanes)) & kGroupMask) != 0u;
         }
         __syncwarp();
         RTW_PHASE(cy_spec);

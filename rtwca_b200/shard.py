@@ -39,9 +39,10 @@ def frames_of_rank(cams, world: int, rank: int) -> list:
 
 def gather_frames(per_frame: dict, n_frames: int, world: int, group=None) -> list | None:
     """All ranks pass {frame index: 1-D float32 array}; rank 0 receives the list
-    of every frame's array in frame order (other ranks get None). Uses
-    all_gather_object for the (small) index/size metadata and one
-    all_gather of a padded float32 tensor for the data."""
+    of every frame's array in frame order (other ranks get None). One
+    all-reduce (max) of the per-rank sizes, gather_object of the (small)
+    index/size metadata to rank 0, and one gather of a padded float32 tensor
+    to rank 0: the data crosses the links once, to the rank that assembles it."""
     import torch
     import torch.distributed as dist
 
@@ -49,17 +50,18 @@ def gather_frames(per_frame: dict, n_frames: int, world: int, group=None) -> lis
         return [per_frame[i] for i in range(n_frames)]
     rank = dist.get_rank(group)
     meta = [(i, int(a.size)) for i, a in sorted(per_frame.items())]
-    metas = [None] * world
-    dist.all_gather_object(metas, meta, group=group)
     backend = dist.get_backend(group)
     dev = torch.device("cuda", torch.cuda.current_device()) if backend == "nccl" else torch.device("cpu")
-    sizes = [sum(s for _, s in m) for m in metas]
-    cap = max(max(sizes), 1)
+    size = torch.tensor([sum(s for _, s in meta)], dtype=torch.int64, device=dev)
+    dist.all_reduce(size, op=dist.ReduceOp.MAX, group=group)
+    cap = max(int(size.item()), 1)
+    metas = [None] * world if rank == 0 else None
+    dist.gather_object(meta, metas, dst=0, group=group)
     buf = torch.zeros(cap, dtype=torch.float32, device=dev)
     flat = np.concatenate([per_frame[i] for i, _ in meta]).astype(np.float32) if meta else np.zeros(0, np.float32)
     buf[: flat.size] = torch.from_numpy(flat).to(dev)
-    bufs = [torch.empty(cap, dtype=torch.float32, device=dev) for _ in range(world)]
-    dist.all_gather(bufs, buf, group=group)
+    bufs = [torch.empty(cap, dtype=torch.float32, device=dev) for _ in range(world)] if rank == 0 else None
+    dist.gather(buf, bufs, dst=0, group=group)
     if rank != 0:
         return None
     out = [None] * n_frames

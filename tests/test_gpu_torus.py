@@ -409,3 +409,92 @@ def test_wormhole_world_through_gen_image_with_bundles():
     with pytest.raises(abi.RTWError) as ei:
         R.gen_image(camera_pos=pos, camera_dir=d, speed=beta, camera_point=pt, x_pix=8, ray_bundles=True)
     assert ei.value.status == abi.ERR_UNSUPPORTED
+
+
+@pytest.fixture(scope="module")
+def fwd_problem(oracle):
+    """16x16 pixels, 8 bins, tolerance 1e-6: the oracle's target (parameters
+    perturbed with numpy default_rng(1)); the per-pixel loss gradient by
+    forward-mode (dual-number) differentiation of the oracle's FP64 integrator,
+    in the discrete adjoint's step-size convention (mode 0) and with tangents
+    through every step size (mode 1); the oracle's per-pixel central
+    differences at relative step 1e-4; the rays with a polar escape."""
+    xp, tol, nb = 16, 1e-6, 8
+    sct, camt, col = _problem(xp, tol, configs.torus_target_params(1), nb)
+    target = oracle.render(sct, camt, col, integrator=abi.DP45_FSAL)["spectrum"].astype(np.float32)
+    sc, cam, col = _problem(xp, tol, None, nb)
+    t64 = target.astype(np.float64)
+
+    def grad(fw):
+        return np.einsum("pc,pct->pt", 2 * (fw["spectrum"] - t64), fw["tangents"])
+
+    fw0 = oracle.torus_forward(sc, cam, col, mode=0)
+    fw1 = oracle.torus_forward(sc, cam, col, mode=1)
+    base = dict(configs.TORUS_DEFAULTS)
+
+    def px_loss(params):
+        s, c, cl = _problem(xp, tol, params, nb)
+        sp = oracle.render(s, c, cl, integrator=abi.DP45_FSAL, want=("spectrum",))["spectrum"]
+        return np.sum((sp - t64) ** 2, axis=1)
+
+    fd = np.zeros((xp * xp, 5))
+    for q, k in enumerate(NAMES):
+        h = 1e-4 * base[k]
+        pp, pm = dict(base), dict(base)
+        pp[k] += h
+        pm[k] -= h
+        fd[:, q] = (px_loss(pp) - px_loss(pm)) / (2 * h) * (180 / np.pi if k == "inclination_deg" else 1)
+    return sc, cam, col, target, grad(fw0), grad(fw1), fd, fw0["escapes"] > 0
+
+
+def _rel_rows(a, b):
+    """Per-pixel, per-parameter |a - b| / (|b| + 1e-3 max |b| of the parameter)."""
+    return np.abs(a - b) / (np.abs(b) + 1e-3 * np.abs(b).max(axis=0) + 1e-300)
+
+
+def test_adjoint_mixed_matches_forward_mode_and_differences(renderer, fwd_problem):
+    """The benchmarked adjoint (FP32-mixed forward, tolerance 1e-6) against
+    two independent derivatives of the FP64 oracle's loss: forward-mode
+    dual numbers through its integrator, and central differences with
+    relative step 1e-4. Per parameter, the gradient summed over the pixels
+    and the 99th percentile of the per-pixel error are within 1e-3. Rays with
+    a polar escape (in the oracle, or in the mixed forward) are left out: their
+    FP32-stage paths reach the axis differently from FP64."""
+    sc, cam, col, target, g0, g1, fd, esc = fwd_problem
+    a = renderer.adjoint(sc, cam, col, target, precision=abi.PREC_MIXED, per_ray=True, exclude_escape_rays=True)
+    g = a["per_ray_grad"]
+    cut = np.all(g == 0, axis=1) & np.any(g0 != 0, axis=1)
+    keep = ~esc & ~cut
+    print("pixels", keep.size, "oracle escape rays", int(esc.sum()), "mixed escape rays", a["escape_rays"])
+    assert keep.sum() >= 0.9 * keep.size
+    for name, ref in (("forward mode", g0), ("central differences", fd)):
+        gs, rs = g[keep].sum(0), ref[keep].sum(0)
+        rel_sum = np.abs(gs - rs) / np.abs(rs)
+        p99 = np.quantile(_rel_rows(g[keep], ref[keep]), 0.99, axis=0)
+        print(name, "summed rel err", rel_sum, "per-pixel p99", p99)
+        assert np.all(rel_sum <= 1e-3), (name, rel_sum)
+        assert np.all(p99 <= 1e-3), (name, p99)
+    # the step-size convention: tangents through every step size (what
+    # differentiating the whole program gives) differ at truncation level
+    d01 = np.abs(g0[keep].sum(0) - g1[keep].sum(0)) / np.abs(g1[keep].sum(0))
+    print("forward mode, controller steps held vs differentiated:", d01)
+    assert np.all(d01 <= 1e-3)
+
+
+def test_adjoint_fp64_matches_forward_mode_on_every_ray(renderer, fwd_problem):
+    """The FP64 adjoint against the dual-number gradient on every pixel,
+    the rays with a polar escape included: there central differences of the
+    loss break down (the discrete loss is not smooth at finite-difference
+    scales near the axis), while forward mode differentiates the same
+    discrete escape the adjoint reverses."""
+    sc, cam, col, target, g0, g1, fd, esc = fwd_problem
+    a = renderer.adjoint(sc, cam, col, target, precision=abi.PREC_FP64, per_ray=True)
+    g = a["per_ray_grad"]
+    rel = _rel_rows(g, g0)
+    print("escape rays", int(esc.sum()), "max rel err: others", rel[~esc].max(axis=0),
+          "escape rays", rel[esc].max(axis=0) if esc.any() else None)
+    assert np.quantile(rel[~esc], 0.99, axis=0).max() <= 1e-6
+    gs, rs = g.sum(0), g0.sum(0)
+    assert np.all(np.abs(gs - rs) <= 1e-6 * np.abs(rs)), (gs, rs)
+    if esc.any():
+        assert np.quantile(rel[esc], 0.5, axis=0).max() <= 1e-3
