@@ -1,0 +1,122 @@
+"""Physics pins of the GPU trace kernel that do not go through the oracle.
+
+1. Constants of motion. Along a Kerr null geodesic E = -k_t, L_z = k_phi, the
+   Carter constant Q = k_theta^2 + cos^2 theta (L_z^2 / sin^2 theta - a^2 E^2)
+   and the null norm g_mn k^m k^n = 0 are conserved. The final states of the
+   GPU rays (textbook FSAL step; the reference's own step is not convergent and
+   drifts the null norm by ~1e-3 by design) must keep them to the level the
+   tolerance allows over ~1300 steps (the FP64 oracle: Q and the null norm
+   to ~7e-6, E and L_z to ~1e-8).
+2. The Kerr shadow (Bardeen 1973). With xi = L_z / E and eta = Q / E^2 fixed by
+   the camera ray, the radial potential R(r) = (r^2 + a^2 - a xi)^2 -
+   Delta (eta + (xi - a)^2) decides the ray's fate: a ray heading inwards
+   with R > 0 everywhere between the horizon and the camera falls in; one whose
+   R has a root there turns round. In vacuum Kerr the GPU classes (horizon /
+   escape) must agree, except for rays on the critical curve itself.
+"""
+import numpy as np
+import pytest
+
+from rtwca_b200 import abi, configs
+from tests.parity import min_sin_theta
+
+pytestmark = pytest.mark.gpu
+
+
+def _lower(oracle, scene, states):
+    """Lower-index momenta k_m at each state's position."""
+    out = np.zeros((states.shape[0], 4))
+    for q, s in enumerate(states):
+        out[q] = oracle.metric(scene, s[:4]) @ s[4:8]
+    return out
+
+
+def _constants(scene, states, k):
+    th = states[:, 2]
+    a = scene.spin
+    E, L, kth = -k[:, 0], k[:, 3], k[:, 2]
+    Q = kth ** 2 + np.cos(th) ** 2 * (L ** 2 / np.sin(th) ** 2 - a * a * E ** 2)
+    null = np.einsum("pm,pm->p", k, states[:, 4:8])
+    return E, L, Q, null
+
+
+def _vacuum_kerr(a=0.9):
+    """The headline's Kerr metric with no emitter (an empty disk range)."""
+    return configs._scene(abi.SCENE_KERR_DISK, spin=a, r_in=30.0, r_out=29.0, theta_lo=0.0, theta_hi=np.pi,
+                          temperature=1e4, a_nu=0.0)
+
+
+@pytest.mark.parametrize("prec,bar", [(abi.PREC_FP64, 3e-5), (abi.PREC_MIXED, 1e-3)])
+def test_constants_of_motion_conserved(renderer, oracle, prec, bar):
+    scene = _vacuum_kerr()
+    cam = configs.look_at_camera(50.0, np.radians(60.0), 45.0, 48, 1e-8)
+    colors = configs.log_spaced_colors(4)
+    g = renderer.render(scene, [cam], colors, want=("class", "state"), precision=prec, integrator=abi.DP45_FSAL)
+    start = oracle.camera_rays(scene, cam)
+    esc = g["class"] == abi.CLASS_ESCAPE
+    assert esc.mean() > 0.5
+    s0, s1 = start[esc], g["state"][esc]
+    E0, L0, Q0, n0 = _constants(scene, s0, _lower(oracle, scene, s0))
+    E1, L1, Q1, n1 = _constants(scene, s1, _lower(oracle, scene, s1))
+    scale = E0 ** 2
+    dE = np.abs(E1 - E0) / np.abs(E0)
+    dL = np.abs(L1 - L0) / (np.abs(L0) + np.abs(E0))
+    dQ = np.abs(Q1 - Q0) / (np.abs(Q0) + scale)
+    dn = np.abs(n1) / scale
+    print("rays", int(esc.sum()), "p99: E", np.quantile(dE, 0.99), "L", np.quantile(dL, 0.99), "Q",
+          np.quantile(dQ, 0.99), "null", np.quantile(dn, 0.99))
+    for d in (dE, dL, dQ, dn):
+        assert np.quantile(d, 0.99) < bar
+
+
+def _radial_potential_fate(xi, eta, a, r_h, r_cam, band, n=20000):
+    """Per ray: +1 if R(r) > 0 on (r_h, r_cam) (no turning point: it falls in),
+    -1 if R has a root there, 0 if the minimum of R / r^4 is within `band` of 0
+    (the critical curve)."""
+    r = np.linspace(r_h * (1 + 1e-6), r_cam, n)
+    out = np.zeros(xi.size, int)
+    for q in range(xi.size):
+        Del = r * r - 2 * r + a * a
+        R = ((r * r + a * a - a * xi[q]) ** 2 - Del * (eta[q] + (xi[q] - a) ** 2)) / r ** 4
+        m = R.min()
+        out[q] = 0 if abs(m) < band else (1 if m > 0 else -1)
+    return out
+
+
+# (precision, step, band): the textbook FSAL step keeps the constants to ~1e-8;
+# the reference's own step drifts them by ~1e-3, which moves rays within a
+# few 1e-3 of the critical curve across it, so its band is wider
+SHADOW_CASES = [(abi.PREC_FP64, abi.DP45_FSAL, 2e-3), (abi.PREC_MIXED, abi.DP45_FSAL, 2e-3),
+                (abi.PREC_MIXED, abi.DP45_REF_COMPAT, 3e-2)]
+
+
+@pytest.mark.parametrize("prec,integ,band", SHADOW_CASES)
+def test_kerr_shadow_matches_bardeen(renderer, oracle, prec, integ, band):
+    """Rays heading inwards (the integration runs backwards along k, so the
+    ray moves in r as -k^r) are captured exactly when the Kerr radial
+    potential has no root between the horizon and the camera."""
+    a = 0.9
+    scene = _vacuum_kerr(a)
+    cam = configs.look_at_camera(50.0, np.radians(75.0), 30.0, 64, 1e-8)
+    colors = configs.log_spaced_colors(4)
+    g = renderer.render(scene, [cam], colors, want=("class",), precision=prec, integrator=integ)
+    start = oracle.camera_rays(scene, cam)
+    k = _lower(oracle, scene, start)
+    E, L, Q, _ = _constants(scene, start, k)
+    xi, eta = L / E, Q / E ** 2
+    r_h = 1 + np.sqrt(1 - a * a)
+    fate = _radial_potential_fate(xi, eta, a, r_h, 50.0, band)
+    inward = -start[:, 5] < 0
+    fate[~inward] = -1  # outward rays meet no turning point before escaping
+    # rays that pass within ~1e-2 of the spin axis (L_z ~ 0) cross the
+    # coordinate singularity of Boyer-Lindquist coordinates: left out
+    axis = min_sin_theta(oracle, scene, cam) < 1e-2
+    sure = (fate != 0) & ~axis
+    pred = np.where(fate > 0, abi.CLASS_HORIZON, abi.CLASS_ESCAPE)
+    got = g["class"]
+    agree = np.mean(pred[sure] == got[sure])
+    print("captured (predicted)", int((pred[sure] == abi.CLASS_HORIZON).sum()), "critical-curve rays",
+          int((fate == 0).sum()), "axis rays", int(axis.sum()), "agreement", agree)
+    assert (pred[sure] == abi.CLASS_HORIZON).sum() > 200
+    assert (~sure).sum() < 0.1 * sure.size
+    assert agree == 1.0

@@ -493,8 +493,11 @@ def test_adjoint_fp64_matches_forward_mode_on_every_ray(renderer, fwd_problem):
     rel = _rel_rows(g, g0)
     print("escape rays", int(esc.sum()), "max rel err: others", rel[~esc].max(axis=0),
           "escape rays", rel[esc].max(axis=0) if esc.any() else None)
-    assert np.quantile(rel[~esc], 0.99, axis=0).max() <= 1e-6
+    # The library's loss is that of the image it outputs, a float32 spectrum:
+    # its residual I - target carries the float32 rounding of I (~6e-8 |I|),
+    # i.e. ~1e-6 of the residual here, which the FP64 dual numbers do not have.
+    assert np.quantile(rel[~esc], 0.99, axis=0).max() <= 1e-5
     gs, rs = g.sum(0), g0.sum(0)
-    assert np.all(np.abs(gs - rs) <= 1e-6 * np.abs(rs)), (gs, rs)
+    assert np.all(np.abs(gs - rs) <= 1e-5 * np.abs(rs)), (gs, rs)
     if esc.any():
         assert np.quantile(rel[esc], 0.5, axis=0).max() <= 1e-3
