@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define RTW_ABI_VERSION 5
+#define RTW_ABI_VERSION 6
 /* Largest number of spectral bins (reference `colors`) one render takes. */
 #define RTW_MAX_BINS 128
 /* Largest number of frames (cameras) one batched render takes. */
@@ -111,7 +111,20 @@ typedef enum rtw_scene_kind {
        optically thin: tau <= 2) in front of skybox[0], which every ray adds at
        its end; rays end beyond |x| = escape_radius (source_geometry.jl:7-82,
        source_model.jl:8-431). Both integrators. */
-    RTW_SCENE_MINKOWSKI_CART_SPHERE = 8
+    RTW_SCENE_MINKOWSKI_CART_SPHERE = 8,
+    /* Kerr with a thermal bremsstrahlung torus: the fluid of
+       RTW_SCENE_KERR_SYNCHRO_TORUS (n_e, Theta_e, tapers, Keplerian
+       4-velocity; no field), radiating free-free emission
+         j_nu = C n_e^2 Theta_e^(-1/2) exp(-u) g_ff(gamma^2, u),
+         u = h nu / (Theta_e m_e c^2), gamma^2 = Ry / (Theta_e m_e c^2),
+       C = 7.089314638783696e-44 erg cm^3 s^-1 Hz^-1 sr^-1 (C_Yar_cgs,
+       emission_functions.jl:19), alpha_nu = j_nu / B_nu(T_e). g_ff is the
+       reference's gaunt_ei_therm_van_Hoof (emission_functions.jl:54-78): a
+       bilinear lookup in the van Hoof (2014) merged Gaunt-factor table that
+       the caller passes as rtw_render_params.gaunt_lut, in Float32 with its
+       index offsets and its fallback 1.2 outside the table. No scene of the
+       reference calls that function. Per-bin tau; both integrators. */
+    RTW_SCENE_KERR_BREMS_TORUS = 9
 } rtw_scene_kind;
 
 /* How a ray ended. The reference's calc_terminate (e.g. Kerr.source/
@@ -252,7 +265,17 @@ typedef struct rtw_render_params {
        every ray (Minkowski_Sphere_Cartesian.source/source_model.jl:175-431). */
     const float* skybox[2];
     int32_t skybox_h[2];
+    /* RTW_SCENE_KERR_BREMS_TORUS: the van Hoof merged Gaunt-factor table
+       (Main/Gaunt_Factors/gauntff_merged_Z01.dat without its 42 header lines):
+       RTW_GAUNT_ROWS rows of constant log10 u (-16, -15.8, ...) by
+       RTW_GAUNT_COLS columns of constant log10 gamma^2 (-6, -5.8, ...),
+       row-major float32, host memory (the reference's Gaunt_LUT[i, j] is
+       gaunt_lut[(i - 1) * RTW_GAUNT_COLS + (j - 1)]). Required for that scene. */
+    const float* gaunt_lut;
 } rtw_render_params;
+
+#define RTW_GAUNT_ROWS 146
+#define RTW_GAUNT_COLS 81
 
 /* Output buffers, owned by the caller. Pixel p of frame f is at
  * frame_offset(f) + i + x_pix * j, with i the horizontal index (reference
@@ -489,6 +512,19 @@ rtw_status rtw_measure_peaks(rtw_ctx* ctx, double* fp32_flops, double* fp64_flop
  * ktau = -a_nu / g, from which the intensity slope of bin c is
  * -A / (exp(X nu_c) - 1). */
 rtw_status rtw_scene_rhs(const rtw_scene* scene, int32_t fp32, const double* state, double* slope, double* emit);
+
+/* The reference's gaunt_ei_therm_van_Hoof (emission_functions.jl:54-78) as
+ * the bremsstrahlung kernels evaluate it: the Gaunt factor at gam2 and u from
+ * the table lut (layout of rtw_render_params.gaunt_lut), in Float32 with the
+ * reference's index offsets and its 1.2 outside the table. For tests. */
+float rtw_gaunt_lookup(const float* lut, double gam2, double u);
+
+/* Right-hand side of a RTW_SCENE_KERR_BREMS_TORUS scene on the host with the
+ * kernels' own functions in FP64 (the layout of rtw_torus_rhs: state[8 + 2N]
+ * = (x^mu, k^mu, I_1, tau_1, ..., I_N, tau_N)), with the Gaunt table gaunt_lut
+ * (layout of rtw_render_params.gaunt_lut). For tests. */
+rtw_status rtw_brems_rhs(const rtw_scene* scene, const double* colors_nm, int32_t n_colors,
+                         const float* gaunt_lut, const double* state, double* slope);
 
 /* Limits of rtw_render_noalloc. */
 #define RTW_NOALLOC_MAX_FRAMES 64

@@ -59,6 +59,10 @@ def load() -> C.CDLL:
                                              C.c_longlong, D, D, C.POINTER(C.c_ubyte), C.POINTER(C.c_uint),
                                              C.POINTER(C.c_int), C.c_int]
         lib.oracle_torus_forward.restype = C.c_int
+        lib.oracle_set_gaunt.argtypes = [C.POINTER(C.c_float)]
+        lib.oracle_set_gaunt.restype = C.c_int
+        lib.oracle_gaunt.argtypes = [C.c_double, C.c_double]
+        lib.oracle_gaunt.restype = C.c_float
         lib.oracle_set_diagnostics.argtypes = [C.POINTER(C.c_int), C.POINTER(C.c_int)]
         lib.oracle_set_diagnostics.restype = C.c_int
         lib.oracle_set_ray_bundles.argtypes = [C.c_int]
@@ -103,11 +107,16 @@ def camera_rays(scene, cam):
     return rays
 
 
-def rhs(scene, colors_nm, state):
+def rhs(scene, colors_nm, state, gaunt_lut=None):
     c = np.ascontiguousarray(colors_nm, dtype=np.float64)
     s = np.ascontiguousarray(state, dtype=np.float64)
     out = np.zeros_like(s)
-    load().oracle_rhs(C.byref(scene), _dp(c), c.size, _dp(s), _dp(out))
+    lut = None if gaunt_lut is None else np.ascontiguousarray(gaunt_lut, dtype=np.float32)
+    load().oracle_set_gaunt(lut.ctypes.data_as(C.POINTER(C.c_float)) if lut is not None else None)
+    try:
+        load().oracle_rhs(C.byref(scene), _dp(c), c.size, _dp(s), _dp(out))
+    finally:
+        load().oracle_set_gaunt(None)
     return out
 
 
@@ -124,7 +133,8 @@ def pad_max_dt(scene, x, scale):
 
 
 def render(scene, cam, colors_nm, *, max_dt_scale=0.1, integrator=0, pixel_ids=None, threads=0,
-           want=("xyz", "class", "steps", "spectrum", "tau", "state"), skybox=(None, None), ray_bundles=False):
+           want=("xyz", "class", "steps", "spectrum", "tau", "state"), skybox=(None, None), ray_bundles=False,
+           gaunt_lut=None):
     """Traces one camera (or the pixel subset `pixel_ids`) with the FP64 oracle.
     Returns a dict of arrays indexed like the pixel list, plus 'counters'
     (step attempts, rejected attempts, polar Euler sub-steps). ray_bundles:
@@ -163,6 +173,8 @@ def render(scene, cam, colors_nm, *, max_dt_scale=0.1, integrator=0, pixel_ids=N
                                  t.shape[0] // 3 if t is not None else 0)
     load().oracle_set_ray_bundles(int(bool(ray_bundles)))
     load().oracle_set_diagnostics(ptr(res["crossings"], C.c_int), ptr(res["escapes"], C.c_int))
+    lut = None if gaunt_lut is None else np.ascontiguousarray(gaunt_lut, dtype=np.float32)
+    load().oracle_set_gaunt(lut.ctypes.data_as(C.POINTER(C.c_float)) if lut is not None else None)
     try:
         st = load().oracle_render(
             C.byref(scene), C.byref(cam), _dp(c), N, float(max_dt_scale), int(integrator),
@@ -175,6 +187,7 @@ def render(scene, cam, colors_nm, *, max_dt_scale=0.1, integrator=0, pixel_ids=N
             load().oracle_set_skybox(k, None, 0)
         load().oracle_set_ray_bundles(0)
         load().oracle_set_diagnostics(None, None)
+        load().oracle_set_gaunt(None)
     if st != 0:
         raise RuntimeError(f"oracle_render failed with status {st}")
     res = {k: v for k, v in res.items() if v is not None}
@@ -209,6 +222,16 @@ def torus_forward(scene, cam, colors_nm, *, mode=0, max_dt_scale=0.1, pixel_ids=
     if st != 0:
         raise RuntimeError(f"oracle_torus_forward failed with status {st}")
     return res
+
+
+def gaunt(lut, gam2, u):
+    """The oracle's own gaunt_ei_therm_van_Hoof from a [146, 81] float32 table."""
+    t = np.ascontiguousarray(lut, dtype=np.float32)
+    load().oracle_set_gaunt(t.ctypes.data_as(C.POINTER(C.c_float)))
+    try:
+        return float(load().oracle_gaunt(float(gam2), float(u)))
+    finally:
+        load().oracle_set_gaunt(None)
 
 
 def cube_wrap(i, j, face, x, y, n):

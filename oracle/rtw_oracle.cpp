@@ -223,6 +223,7 @@ struct OScene {
 
     bool is_kerr() const {
         return kind == RTW_SCENE_KERR_DISK || kind == RTW_SCENE_KERR_THICK_DISK || kind == RTW_SCENE_KERR_SYNCHRO_TORUS ||
+               kind == RTW_SCENE_KERR_BREMS_TORUS ||
                kind == RTW_SCENE_KERR_POWEHI;
     }
     // Synchro_Test.source and Minkowski_Sphere_Cartesian.source: Minkowski
@@ -733,6 +734,76 @@ void torus_bins(const OScene& sc, RayWork& w, const double* R, double* slope) {
     torus_bins_t<double>(sc, sc.a, sc.n0, sc.b0, sc.th0, w.freq, w.N, R, slope);
 }
 
+// The van Hoof merged Gaunt-factor table of the bremsstrahlung torus
+// ([146][81] float32 row-major: rows of constant log10 u from -16, columns of
+// constant log10 gamma^2 from -6, 0.2 dex apart), set by oracle_set_gaunt.
+static const float* g_gaunt = nullptr;
+
+// gaunt_ei_therm_van_Hoof (emission_functions.jl:54-78), Float32 as there:
+// loggam, logu rounded to Float32; frac = (log + offset) / 0.2f0 used as the
+// 1-based index; floor / ceil(frac + 1f-3) neighbours; bilinear weights
+// (ceil - frac), (frac - floor); 1.2 outside [1, 146] x [1, 81]. A non-finite
+// argument (floor(Int32, .) would throw there) also gives 1.2.
+float gaunt_van_hoof_oracle(double gam2, double u) {
+    if (!g_gaunt) return 1.2f;
+    const float loggam = (float)std::log10(gam2);
+    const float logu = (float)std::log10(u);
+    const float frac_i = (logu + 16.0f) / 0.2f;
+    const float frac_j = (loggam + 6.0f) / 0.2f;
+    if (!std::isfinite(frac_i) || !std::isfinite(frac_j)) return 1.2f;
+    const double floor_i = std::floor((double)frac_i), floor_j = std::floor((double)frac_j);
+    const double ceil_i = std::ceil((double)(frac_i + 1e-3f)), ceil_j = std::ceil((double)(frac_j + 1e-3f));
+    if (!(1 <= floor_i && 1 <= floor_j && ceil_i <= 146 && ceil_j <= 81)) return 1.2f;
+    auto L = [](double i, double j) { return g_gaunt[((long)i - 1) * 81 + ((long)j - 1)]; };
+    const float a_i = (float)ceil_i - frac_i, b_i = frac_i - (float)floor_i;
+    const float gaunt1 = a_i * L(floor_i, floor_j) + b_i * L(ceil_i, floor_j);
+    const float gaunt2 = a_i * L(floor_i, ceil_j) + b_i * L(ceil_i, ceil_j);
+    return ((float)ceil_j - frac_j) * gaunt1 + (frac_j - (float)floor_j) * gaunt2;
+}
+
+// RT slopes of the bremsstrahlung torus (RTW_SCENE_KERR_BREMS_TORUS; no
+// reference scene, the reference's parts are C_Yar_cgs (emission_functions.jl:
+// 19) and the Gaunt factor): the synchrotron torus's n_e, Theta_e, tapers and
+// Keplerian velocity; j_nu = C_Yar n_e^2 Theta_e^(-1/2) exp(-u) g_ff,
+// u = h nu / (Theta_e m_e c^2), gamma^2 = Ry / (Theta_e m_e c^2),
+// alpha_nu = j_nu / B_nu(T_e).
+void brems_bins(const OScene& sc, RayWork& w, const double* R, double* slope) {
+    for (int c = 0; c < w.N; ++c) {
+        slope[8 + 2 * c] = 0;
+        slope[9 + 2 * c] = 0;
+    }
+    const double r = R[1], th = R[2];
+    if (!(r >= std::max(sc.r_in - 4 * sc.edge_in, 1.01 * sc.r_ev) && r <= sc.r_out + 4 * sc.edge_out)) return;
+    double taper = 1;
+    if (r < sc.r_in) taper = std::exp(-sq((sc.r_in - r) / sc.edge_in));
+    else if (r > sc.r_out) taper = std::exp(-sq((r - sc.r_out) / sc.edge_out));
+    const double x = r / sc.r_in;
+    const double zz = r * std::cos(th), hz = sc.rho_h * r;
+    const double ne = sc.n0 * std::pow(x, sc.rho_idx) * std::exp(-zz * zz / (2 * hz * hz)) * taper;
+    const double Th = sc.th0 * std::pow(x, sc.t_idx);
+    sc.lower_metric(R, w.g);
+    const double Om = std::sqrt(sc.M) / (std::pow(r, 1.5) + sc.a * std::sqrt(sc.M));
+    const double n2 = -(w.g[0][0] + 2 * Om * w.g[0][3] + Om * Om * w.g[3][3]);
+    if (!(n2 > 0)) return;
+    const double ut = 1 / std::sqrt(n2);
+    const double gs = -(ut * (w.g[0][0] + Om * w.g[0][3]) * R[4] + ut * (w.g[0][3] + Om * w.g[3][3]) * R[7]);
+    if (!(gs > 0)) return;
+    constexpr double cc = 2.99792458e10, me = 9.1093837015e-28, h = 6.62607015e-27;
+    constexpr double ry = 2.1798723611035e-11, c_yar = 7.089314638783696e-44;
+    const double kT = Th * me * cc * cc;
+    for (int c = 0; c < w.N; ++c) {
+        const double nu = gs * kLightC * 1e9 * w.freq[c];  // Hz in the fluid frame
+        const double u = h * nu / kT;
+        if (!(u > 0)) continue;
+        const double gff = (double)gaunt_van_hoof_oracle(ry / kT, u);
+        const double j = c_yar * ne * ne / std::sqrt(Th) * std::exp(-u) * gff;
+        const double bnu = 2 * h * nu * nu * nu / (cc * cc) / std::expm1(u);
+        const double nu_nm = gs * w.freq[c];
+        slope[8 + 2 * c] = -(1 / gs) * j * sc.length_cm * std::exp(-R[9 + 2 * c]) / (nu_nm * nu_nm * nu_nm);
+        slope[9 + 2 * c] = -(1 / gs) * j / bnu * sc.length_cm;
+    }
+}
+
 // RT slopes of Powehi.source (the reference's M87* model, source_model.jl:
 // region_calc :229-241, get_source_velocity! :269-317, transform_B_b :60-113,
 // calc_b_angle :115-146, calc_fluid_params! :152-176,
@@ -914,6 +985,10 @@ void rhs(const OScene& sc, RayWork& w, const double* R, double* slope) {
         torus_bins(sc, w, R, slope);
         return;
     }
+    if (sc.kind == RTW_SCENE_KERR_BREMS_TORUS) {
+        brems_bins(sc, w, R, slope);
+        return;
+    }
     if (sc.kind == RTW_SCENE_KERR_POWEHI) {
         powehi_bins(sc, w, R, slope);
         return;
@@ -1015,7 +1090,8 @@ double dp45_step(const OScene& sc, RayWork& w, double* R, double h, bool prev_re
             k1[i] = newk1[i];
             R[i] = y[i];
         }
-        if ((sc.kind == RTW_SCENE_KERR_SYNCHRO_TORUS || sc.kind == RTW_SCENE_KERR_POWEHI) && w.fsal && y[2] != th_before)
+        if ((sc.kind == RTW_SCENE_KERR_SYNCHRO_TORUS || sc.kind == RTW_SCENE_KERR_POWEHI ||
+             sc.kind == RTW_SCENE_KERR_BREMS_TORUS) && w.fsal && y[2] != th_before)
         rhs(sc, w, R, k1);
         *rejected = false;
         return h;
@@ -1036,7 +1112,8 @@ double dp45_step(const OScene& sc, RayWork& w, double* R, double h, bool prev_re
     // through the pole re-evaluates the carried slope at the new state, so that
     // each step depends on its start state alone, as the library's per-bin
     // kernels do (the reference's own step keeps its carried slope)
-    if ((sc.kind == RTW_SCENE_KERR_SYNCHRO_TORUS || sc.kind == RTW_SCENE_KERR_POWEHI) && w.fsal && y[2] != th_before)
+    if ((sc.kind == RTW_SCENE_KERR_SYNCHRO_TORUS || sc.kind == RTW_SCENE_KERR_POWEHI ||
+             sc.kind == RTW_SCENE_KERR_BREMS_TORUS) && w.fsal && y[2] != th_before)
         rhs(sc, w, R, k1);
     *rejected = false;
     return hn;
@@ -1706,6 +1783,15 @@ int oracle_set_diagnostics(int* crossings, int* escape_substeps) {
     g_diag_escape = escape_substeps;
     return RTW_OK;
 }
+
+// the bremsstrahlung torus's Gaunt-factor table ([146][81] float32; NULL: none); kept until changed
+int oracle_set_gaunt(const float* lut) {
+    g_gaunt = lut;
+    return RTW_OK;
+}
+
+// the oracle's own Gaunt factor at gam2 and u (the table set by oracle_set_gaunt)
+float oracle_gaunt(double gam2, double u) { return gaunt_van_hoof_oracle(gam2, u); }
 
 int oracle_set_skybox(int k, const float* tex, int h) {
     if (k < 0 || k > 1 || (tex && h < 1)) return RTW_ERR_INVALID_PARAM;

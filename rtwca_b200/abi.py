@@ -15,7 +15,7 @@ PKG = Path(__file__).resolve().parent
 # RTW_LIB_PATH selects another build of the same library (e.g. a tuning variant)
 LIB_PATH = Path(os.environ.get("RTW_LIB_PATH", PKG / "librtw_b200.so"))
 
-ABI_VERSION = 5
+ABI_VERSION = 6
 MAX_BINS = 128
 MAX_FRAMES = 4096
 TRACE_FIELDS = 15
@@ -48,6 +48,9 @@ SCENE_KERR_POWEHI = 5
 SCENE_SYNCHRO_TEST = 6
 SCENE_WORMHOLE = 7
 SCENE_MINKOWSKI_CART_SPHERE = 8
+SCENE_KERR_BREMS_TORUS = 9
+GAUNT_ROWS = 146
+GAUNT_COLS = 81
 ADJOINT_PARAMS = ("spin", "inclination", "n_e0", "b_0", "theta_e0")
 
 # rtw_term_class
@@ -102,6 +105,7 @@ class RenderParams(C.Structure):
         ("stream", C.c_void_p), ("pixel_order", C.c_int32), ("refill_min", C.c_int32),
         ("trace_ray", C.c_int64), ("autotune", C.c_int32), ("graph", C.c_int32),
         ("skybox", C.POINTER(C.c_float) * 2), ("skybox_h", C.c_int32 * 2),
+        ("gaunt_lut", C.POINTER(C.c_float)),
     ]
 
 
@@ -180,6 +184,9 @@ SIGNATURES = {
     "rtw_noalloc_last_error": (C.c_char_p, []),
     "rtw_scene_rhs": (C.c_int, [C.POINTER(Scene), C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                 C.POINTER(C.c_double)]),
+    "rtw_gaunt_lookup": (C.c_float, [C.POINTER(C.c_float), C.c_double, C.c_double]),
+    "rtw_brems_rhs": (C.c_int, [C.POINTER(Scene), C.POINTER(C.c_double), C.c_int32, C.POINTER(C.c_float),
+                                C.POINTER(C.c_double), C.POINTER(C.c_double)]),
 }
 
 _lib = None
@@ -293,6 +300,29 @@ def torus_rhs(scene: Scene, colors_nm, state, form: int = 0):
     dp = C.POINTER(C.c_double)
     check(load().rtw_torus_rhs(C.byref(scene), c.ctypes.data_as(dp), int(c.size), int(form), st.ctypes.data_as(dp),
                                out.ctypes.data_as(dp)), "torus_rhs")
+    return out
+
+
+def gaunt_lookup(lut, gam2: float, u: float) -> float:
+    """The library's Gaunt factor (gaunt_ei_therm_van_Hoof) from a
+    [GAUNT_ROWS, GAUNT_COLS] float32 table."""
+    import numpy as np
+    t = np.ascontiguousarray(lut, dtype=np.float32)
+    assert t.shape == (GAUNT_ROWS, GAUNT_COLS)
+    return float(load().rtw_gaunt_lookup(t.ctypes.data_as(C.POINTER(C.c_float)), float(gam2), float(u)))
+
+
+def brems_rhs(scene: Scene, colors_nm, lut, state):
+    """Host FP64 right-hand side of the bremsstrahlung torus (layout of torus_rhs)."""
+    import numpy as np
+    c = np.ascontiguousarray(colors_nm, dtype=np.float64)
+    t = np.ascontiguousarray(lut, dtype=np.float32)
+    st = np.ascontiguousarray(state, dtype=np.float64)
+    out = np.zeros_like(st)
+    dp = C.POINTER(C.c_double)
+    check(load().rtw_brems_rhs(C.byref(scene), c.ctypes.data_as(dp), int(c.size),
+                               t.ctypes.data_as(C.POINTER(C.c_float)), st.ctypes.data_as(dp),
+                               out.ctypes.data_as(dp)), "brems_rhs")
     return out
 
 

@@ -252,3 +252,24 @@ def synchro_camera(x_pix: int = 256, tol: float = 1e-6, max_steps: int = 20_000)
     (0, 0), pointing (pi/8, 0, pi), beta 0; default field of view."""
     return abi.make_camera([0.0, 0.0, 0.0, 0.0], [0.0, 0.0], 0.0, [PI / 8, 0.0, PI], x_pix, 85.0, 60.0, tol,
                            max_steps)
+
+
+# ---------------------------------------------------------------------------
+# Thermal bremsstrahlung torus (the van Hoof Gaunt-factor lookup of the
+# reference's emission_functions.jl:54-78 on the synchrotron torus's fluid).
+# ---------------------------------------------------------------------------
+def brems_scene(spin: float = 0.94, n_e0: float = 1e8, theta_e0: float = 10.0) -> abi.Scene:
+    s = abi.scene_default(abi.SCENE_KERR_BREMS_TORUS)
+    s.spin, s.n_e0, s.theta_e0 = float(spin), float(n_e0), float(theta_e0)
+    return s
+
+
+def smooth_gaunt_table() -> np.ndarray:
+    """A smooth stand-in for the van Hoof table (the real one is data the
+    caller supplies): on the table's grid (log10 u = -16 + 0.2 i, log10
+    gamma^2 = -6 + 0.2 j), g = 1 + 0.55 ln(1 + 10^(-0.9 log10 u)) / (1 + 0.05
+    |log10 gamma^2|), float32 [146, 81]. It rises towards small u as the
+    real factor does; its values are not physical Gaunt factors."""
+    lu = -16.0 + 0.2 * np.arange(abi.GAUNT_ROWS)[:, None]
+    lg = -6.0 + 0.2 * np.arange(abi.GAUNT_COLS)[None, :]
+    return (1.0 + 0.55 * np.log1p(10.0 ** (-0.9 * lu)) / (1.0 + 0.05 * np.abs(lg))).astype(np.float32)

@@ -119,7 +119,7 @@ void boost(double beta, M4 out) {
 
 bool is_kerr(int kind) {
     return kind == RTW_SCENE_KERR_DISK || kind == RTW_SCENE_KERR_THICK_DISK || kind == RTW_SCENE_KERR_SYNCHRO_TORUS ||
-           kind == RTW_SCENE_KERR_POWEHI;
+           kind == RTW_SCENE_KERR_POWEHI || kind == RTW_SCENE_KERR_BREMS_TORUS;
 }
 
 double horizon_radius(const rtw_scene& s) {
@@ -343,6 +343,15 @@ rtw_status rtw_scene_default(int32_t kind, rtw_scene* s) {
         s->r_in = 6; s->r_out = 40; s->edge_in = 0.5; s->edge_out = 5;
         s->rho_h = 0.3; s->rho_index = -1.5; s->t_index = -1.0; s->b_index = -1.0;
         s->n_e0 = 1e5; s->b_0 = 10; s->theta_e0 = 10; s->length_cm = 9.62e14;
+        s->escape_radius = 110;
+        break;
+    case RTW_SCENE_KERR_BREMS_TORUS:
+        // no reference counterpart: the synchrotron torus's fluid (n_e, Theta_e,
+        // tapers) radiating thermal bremsstrahlung, denser (n_e0 = 1e8 cm^-3)
+        s->spin = 0.94;
+        s->r_in = 6; s->r_out = 40; s->edge_in = 0.5; s->edge_out = 5;
+        s->rho_h = 0.3; s->rho_index = -1.5; s->t_index = -1.0; s->b_index = -1.0;
+        s->n_e0 = 1e8; s->b_0 = 0; s->theta_e0 = 10; s->length_cm = 9.62e14;
         s->escape_radius = 110;
         break;
     case RTW_SCENE_KERR_POWEHI:
@@ -578,7 +587,7 @@ rtw_status rtw_render(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* ca
         return fail(ctx, RTW_ERR_UNSUPPORTED, "ray bundles are built for the skybox scenes only");
     if (scene->kind == RTW_SCENE_KERR_SYNCHRO_TORUS || scene->kind == RTW_SCENE_KERR_POWEHI ||
         scene->kind == RTW_SCENE_SYNCHRO_TEST || scene->kind == RTW_SCENE_WORMHOLE ||
-        scene->kind == RTW_SCENE_MINKOWSKI_CART_SPHERE)
+        scene->kind == RTW_SCENE_MINKOWSKI_CART_SPHERE || scene->kind == RTW_SCENE_KERR_BREMS_TORUS)
         return torus_render(ctx, scene, cams, n_cams, prm, out);
     if (scene->ref_precision) return fail(ctx, RTW_ERR_UNSUPPORTED, "ref_precision is an oracle-only switch");
     if (prm->precision != RTW_PREC_FP64 && prm->precision != RTW_PREC_MIXED && prm->precision != RTW_PREC_FP64_PLAIN)

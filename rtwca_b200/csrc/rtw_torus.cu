@@ -80,9 +80,10 @@ struct TorusModel {
     TorusBin bins[kTorusMaxBins];
     int n;         // bins
     int emitter;   // 0: synchrotron torus, 1: Powehi (disk + jet), 2: Synchro_Test cylinder, 3: none (wormhole),
-                   // 4: the Cartesian blackbody sphere
+                   // 4: the Cartesian blackbody sphere, 5: the bremsstrahlung torus
     int geom;      // geometry: 0 Kerr (Boyer-Lindquist), 1 Minkowski (Cartesian), 2 Dneg wormhole
     SphereDev sp;
+    BremsDev br;
 };
 
 // The scene's emitter at a stage point z (x^mu, k^mu) and the slopes of bin c.
@@ -98,6 +99,8 @@ RTW_HD TorusPt<R> em_point(const TorusModel& m, const R* z) {
         return o;
     }
     if (EM == 4 || (EM == -1 && m.emitter == 4)) return sphere_point<R>(m.sp, z);
+    if (EM == 5 || (EM == -1 && m.emitter == 5))
+        return brems_point<R>(m.tor, m.br, R(m.tor.a), R(m.tor.n0), R(m.tor.Th0), z[1], z[2], z[4], z[7]);
     if (EM == 2 || (EM == -1 && m.emitter == 2)) return synchro_point<R>(m.sy, z);
     if (EM == 1 || (EM == -1 && m.emitter == 1)) return powehi_point<R>(m.pw, z);
     return torus_point<R>(m.tor, R(m.tor.a), R(m.tor.n0), R(m.tor.B0), R(m.tor.Th0), z[1], z[2], z[4], z[7]);
@@ -105,6 +108,7 @@ RTW_HD TorusPt<R> em_point(const TorusModel& m, const R* z) {
 template <class R, int EM = -1>
 RTW_HD void em_bin(const TorusModel& m, const TorusPt<R>& S, int c, R& ft, R& fi) {
     if (EM == 4 || (EM == -1 && m.emitter == 4)) sphere_bin<R>(m.sp, S, m.bins[c].nu_nm, ft, fi);
+    else if (EM == 5 || (EM == -1 && m.emitter == 5)) brems_bin<R>(m.br, S, m.bins[c], ft, fi);
     else if (EM > 0 || (EM == -1 && m.emitter != 0)) powehi_bin<R>(m.pw, S, m.bins[c].nu_nm, ft, fi);
     else torus_bin<R>(S.cj, S.nus, S.th, S.g, m.bins[c], ft, fi);
 }
@@ -1556,6 +1560,8 @@ struct TorusBuffers {
     size_t pool2_cap = 0;
     void* sky = nullptr;    // the wormhole's skyboxes
     size_t sky_cap = 0;
+    void* gaunt = nullptr;  // the bremsstrahlung torus's Gaunt-factor table
+    size_t gaunt_cap = 0;
     void* fin = nullptr;   // final states
     size_t fin_cap = 0;
     void* tgt = nullptr;
@@ -1564,7 +1570,8 @@ struct TorusBuffers {
 
 void torus_free(TorusBuffers* b) {
     if (!b) return;
-    for (void* q : {b->ctl, b->out, b->nev, b->evh, b->evk, b->ck, b->work, b->tgt, b->pool, b->pool2, b->fin, b->sky})
+    for (void* q : {b->ctl, b->out, b->nev, b->evh, b->evk, b->ck, b->work, b->tgt, b->pool, b->pool2, b->fin, b->sky,
+                    b->gaunt})
         if (q) cudaFree(q);
     delete b;
 }
@@ -1576,6 +1583,7 @@ constexpr double kCcgs = 2.99792458e10;        // cm/s
 constexpr double kMe = 9.1093837015e-28;       // g
 constexpr double kHcgs = 6.62607015e-27;       // erg s
 constexpr double kMec2 = kMe * kCcgs * kCcgs;  // erg
+constexpr double kRydbergErg = 2.1798723611035e-11;  // Rydberg energy (CODATA 2018), erg
 
 // Powehi.source constants (source_model.jl:7-35, source_geometry.jl:7-34)
 constexpr double kPowehiP = 2.5, kPowehiGmin = 30.0, kPowehiGmax = 1e9;
@@ -1624,8 +1632,14 @@ rtw_status torus_model(const rtw_scene& s, const double* colors_nm, int N, Torus
         return RTW_ERR_INVALID_PARAM;
     }
     const bool powehi = s.kind == RTW_SCENE_KERR_POWEHI, synchro = s.kind == RTW_SCENE_SYNCHRO_TEST,
-               wormhole = s.kind == RTW_SCENE_WORMHOLE, sphere = s.kind == RTW_SCENE_MINKOWSKI_CART_SPHERE;
-    if (sphere) {
+               wormhole = s.kind == RTW_SCENE_WORMHOLE, sphere = s.kind == RTW_SCENE_MINKOWSKI_CART_SPHERE,
+               brems = s.kind == RTW_SCENE_KERR_BREMS_TORUS;
+    if (brems) {
+        if (!(s.mass > 0) || !(std::fabs(s.spin) < s.mass) || !(s.length_cm > 0) || !(s.n_e0 >= 0)) {
+            why = "scene parameters out of range";
+            return RTW_ERR_INVALID_PARAM;
+        }
+    } else if (sphere) {
         if (!(s.r_out > 0) || !(s.temperature > 0) || !(s.a_nu >= 0) || !(s.escape_radius > 0)) {
             why = "sphere radius, temperature and escape radius must be > 0, a_nu >= 0";
             return RTW_ERR_INVALID_PARAM;
@@ -1691,7 +1705,12 @@ rtw_status torus_model(const rtw_scene& s, const double* colors_nm, int N, Torus
         m.bins[c].inv_b0 = 1.0 / m.bins[c].b0;
     }
     m.n = N;
-    m.emitter = powehi ? 1 : synchro ? 2 : wormhole ? 3 : sphere ? 4 : 0;
+    m.emitter = powehi ? 1 : synchro ? 2 : wormhole ? 3 : sphere ? 4 : brems ? 5 : 0;
+    if (brems) {
+        m.br.lut = nullptr;  // set where the table is placed (device or host)
+        m.br.cj_unit = kCYarCgs * s.length_cm;
+        m.br.ry_mec2 = kRydbergErg / kMec2;
+    }
     m.geom = synchro || sphere ? 1 : wormhole ? 2 : 0;
     if (sphere) {
         m.sp.r_sph = s.r_out;
@@ -1720,14 +1739,15 @@ rtw_status torus_model(const rtw_scene& s, const double* colors_nm, int N, Torus
 
 // the forward kernel instance: precision x emitter (0 torus, 1 Powehi, 2
 // Synchro_Test in flat Cartesian geometry, 3 none in the wormhole's geometry,
-// 4 the blackbody sphere in flat Cartesian geometry)
+// 4 the blackbody sphere in flat Cartesian geometry, 5 the bremsstrahlung
+// torus)
 const void* forward_fn(bool mixed, int emitter) {
-    static const void* const fn[2][5] = {
+    static const void* const fn[2][6] = {
         {(const void*)torus_forward<false, 0>, (const void*)torus_forward<false, 1>, (const void*)torus_forward<false, 2>,
-         (const void*)torus_forward<false, 3>, (const void*)torus_forward<false, 4>},
+         (const void*)torus_forward<false, 3>, (const void*)torus_forward<false, 4>, (const void*)torus_forward<false, 5>},
         {(const void*)torus_forward<true, 0>, (const void*)torus_forward<true, 1>, (const void*)torus_forward<true, 2>,
-         (const void*)torus_forward<true, 3>, (const void*)torus_forward<true, 4>}};
-    return fn[mixed ? 1 : 0][emitter >= 0 && emitter <= 4 ? emitter : 0];
+         (const void*)torus_forward<true, 3>, (const void*)torus_forward<true, 4>, (const void*)torus_forward<true, 5>}};
+    return fn[mixed ? 1 : 0][emitter >= 0 && emitter <= 5 ? emitter : 0];
 }
 
 // launch shape of the torus kernels: 128 threads, occupancy-limited CTAs
@@ -1857,6 +1877,14 @@ rtw_status torus_render(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* 
                     p.sky_h[k] = prm->skybox_h[k];
                 }
         }
+    }
+    // the bremsstrahlung torus's Gaunt-factor table, uploaded for this render
+    if (scene->kind == RTW_SCENE_KERR_BREMS_TORUS) {
+        if (!prm->gaunt_lut) return fail(ctx, RTW_ERR_INVALID_PARAM, "the bremsstrahlung torus needs gaunt_lut");
+        const size_t bytes = sizeof(float) * kGauntRows * kGauntCols;
+        if ((st = ensure(ctx, &b->gaunt, &b->gaunt_cap, bytes)) != RTW_OK) return st;
+        RTW_CUDA(cudaMemcpyAsync(b->gaunt, prm->gaunt_lut, bytes, cudaMemcpyHostToDevice, s), "Gaunt table H2D");
+        p.m.br.lut = (const float*)b->gaunt;
     }
     p.cls = cls;
     p.steps = steps;
@@ -2202,16 +2230,12 @@ rtw_status rtw_adjoint(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* c
     return RTW_OK;
 }
 
-rtw_status rtw_torus_rhs(const rtw_scene* scene, const double* colors_nm, int32_t n_colors, int32_t form,
-                         const double* state, double* slope) {
-    if (!scene || !state || !slope ||
-        (scene->kind != RTW_SCENE_KERR_SYNCHRO_TORUS && scene->kind != RTW_SCENE_KERR_POWEHI &&
-         scene->kind != RTW_SCENE_SYNCHRO_TEST && scene->kind != RTW_SCENE_WORMHOLE &&
-         scene->kind != RTW_SCENE_MINKOWSKI_CART_SPHERE))
-        return RTW_ERR_INVALID_PARAM;
+static rtw_status torus_rhs_host(const rtw_scene* scene, const double* colors_nm, int32_t n_colors, int32_t form,
+                                 const float* gaunt_lut, const double* state, double* slope) {
     TorusModel m;
     std::string why;
     if (torus_model(*scene, colors_nm, n_colors, m, why) != RTW_OK) return RTW_ERR_INVALID_PARAM;
+    m.br.lut = gaunt_lut;
     const int N = n_colors, D = 8 + 2 * N;
     std::vector<double> y(D), f(D);
     for (int i = 0; i < 8; ++i) y[i] = state[i];
@@ -2232,6 +2256,28 @@ rtw_status rtw_torus_rhs(const rtw_scene* scene, const double* colors_nm, int32_
         slope[9 + 2 * c] = f[8 + c];
     }
     return RTW_OK;
+}
+
+rtw_status rtw_torus_rhs(const rtw_scene* scene, const double* colors_nm, int32_t n_colors, int32_t form,
+                         const double* state, double* slope) {
+    if (!scene || !state || !slope ||
+        (scene->kind != RTW_SCENE_KERR_SYNCHRO_TORUS && scene->kind != RTW_SCENE_KERR_POWEHI &&
+         scene->kind != RTW_SCENE_SYNCHRO_TEST && scene->kind != RTW_SCENE_WORMHOLE &&
+         scene->kind != RTW_SCENE_MINKOWSKI_CART_SPHERE))
+        return RTW_ERR_INVALID_PARAM;
+    return torus_rhs_host(scene, colors_nm, n_colors, form, nullptr, state, slope);
+}
+
+rtw_status rtw_brems_rhs(const rtw_scene* scene, const double* colors_nm, int32_t n_colors, const float* gaunt_lut,
+                         const double* state, double* slope) {
+    if (!scene || !state || !slope || !gaunt_lut || scene->kind != RTW_SCENE_KERR_BREMS_TORUS)
+        return RTW_ERR_INVALID_PARAM;
+    return torus_rhs_host(scene, colors_nm, n_colors, 0, gaunt_lut, state, slope);
+}
+
+float rtw_gaunt_lookup(const float* lut, double gam2, double u) {
+    if (!lut) return 1.2f;
+    return gaunt_van_hoof(lut, rlog10f_(gam2), rlog10f_(u));
 }
 
 rtw_status rtw_torus_escape_vjp(const rtw_scene* scene, const double* colors_nm, int32_t n_colors,

@@ -439,6 +439,139 @@ RTW_HD void sphere_bin(const SphereDev& S, const TorusPt<T>& P, double nu_nm, T&
     fi = -(ag * B(S.es)) / (texp(P.g * B(S.ff_T * nu_nm)) - B(1.0));
 }
 
+// ---------------------------------------------------------------------------
+// Thermal bremsstrahlung torus (RTW_SCENE_KERR_BREMS_TORUS): the synchrotron
+// torus's fluid (n_e, Theta_e, tapers, Keplerian 4-velocity) radiating
+// free-free emission with the van Hoof Gaunt factor of the reference's
+// gaunt_ei_therm_van_Hoof (emission_functions.jl:54-78).
+// ---------------------------------------------------------------------------
+constexpr int kGauntRows = 146;  // constant log10 u: -16, -15.8, ...
+constexpr int kGauntCols = 81;   // constant log10 gamma^2: -6, -5.8, ...
+constexpr double kCYarCgs = 7.089314638783696e-44;  // emission_functions.jl:19
+
+struct BremsDev {
+    const float* lut;  // [kGauntRows][kGauntCols] row-major (device memory in the kernels)
+    double cj_unit;    // C_Yar_cgs * length_cm
+    double ry_mec2;    // Ry / (m_e c^2)
+};
+
+// IEEE single-precision steps without contraction (the reference's Float32
+// arithmetic, which does not fuse a multiply and an add)
+RTW_HD float f32_add(float a, float b) {
+#ifdef __CUDA_ARCH__
+    return __fadd_rn(a, b);
+#else
+    return a + b;
+#endif
+}
+RTW_HD float f32_mul(float a, float b) {
+#ifdef __CUDA_ARCH__
+    return __fmul_rn(a, b);
+#else
+    return a * b;
+#endif
+}
+RTW_HD float f32_div(float a, float b) {
+#ifdef __CUDA_ARCH__
+    return __fdiv_rn(a, b);
+#else
+    return a / b;
+#endif
+}
+
+// gaunt_ei_therm_van_Hoof (emission_functions.jl:54-78) at log10 gamma^2 and
+// log10 u (each already rounded to Float32, as Float32(log10(.)) there).
+// Kept as the reference writes it: the fractional indices (log + 16) / 0.2 and
+// (log + 6) / 0.2 address the 1-based table directly, so the lookup sits one
+// grid step (0.2 dex) away from the table's own abscissae, and the upper
+// index is ceil(frac + 1e-3), so just below an integer the two weights add up
+// to 2. Outside the table, and for a non-finite argument (where the
+// reference's floor(Int32, .) throws), the Gaunt factor is 1.2.
+RTW_HD float gaunt_van_hoof(const float* lut, float loggam, float logu) {
+    const float frac_i = f32_div(f32_add(logu, 16.0f), 0.2f);
+    const float frac_j = f32_div(f32_add(loggam, 6.0f), 0.2f);
+    if (!(frac_i >= 1.0f && frac_i < 200.0f && frac_j >= 1.0f && frac_j < 200.0f)) return 1.2f;
+    const float fi = floorf(frac_i), ci = ceilf(f32_add(frac_i, 1e-3f));
+    const float fj = floorf(frac_j), cj = ceilf(f32_add(frac_j, 1e-3f));
+    if (!(ci <= (float)kGauntRows && cj <= (float)kGauntCols)) return 1.2f;
+    const int i0 = (int)fi - 1, i1 = (int)ci - 1, j0 = (int)fj - 1, j1 = (int)cj - 1;
+    const float wi0 = ci - frac_i, wi1 = frac_i - fi;  // exact: integers and frac_i are Float32
+    const float g1 = f32_add(f32_mul(wi0, lut[i0 * kGauntCols + j0]), f32_mul(wi1, lut[i1 * kGauntCols + j0]));
+    const float g2 = f32_add(f32_mul(wi0, lut[i0 * kGauntCols + j1]), f32_mul(wi1, lut[i1 * kGauntCols + j1]));
+    return f32_add(f32_mul(cj - frac_j, g1), f32_mul(frac_j - fj, g2));
+}
+RTW_HD float rlog10f_(float x) { return log10f(x); }
+RTW_HD float rlog10f_(double x) { return (float)log10(x); }
+
+// The fluid at (r, theta) for a ray with k^t, k^phi: cj = C n_e^2 length_cm,
+// th = Theta_e, g = -u.k (the synchrotron torus's profiles and 4-velocity).
+template <class T>
+RTW_HD TorusPt<T> brems_point(const TorusDev& P, const BremsDev& Bd, const T& a, const T& n0, const T& th0,
+                              const T& r, const T& th, const T& kt, const T& kph) {
+    typedef decltype(val(r)) B;
+    TorusPt<T> o;
+    o.on = false;
+    o.zone = 0;
+    o.cj = T(0.0); o.nus = T(1.0); o.th = T(1.0); o.g = T(1.0);
+    const double rv = (double)val(r);
+    if (!(rv >= P.cut_in && rv <= P.cut_out)) return o;
+    const T x = r * B(1.0 / P.r_in);
+    T taper = T(1.0);
+    if (rv < P.r_in) {
+        const T q = (T(B(P.r_in)) - r) * B(1.0 / P.edge_in);
+        taper = texp(-(q * q));
+    } else if (rv > P.r_out) {
+        const T q = (r - B(P.r_out)) * B(1.0 / P.edge_out);
+        taper = texp(-(q * q));
+    }
+    const T sn = tsin(th), cs = tcos(th);
+    const T lx = tlog(x);
+    const T gz = cs * cs * B(-0.5 / (P.h_ratio * P.h_ratio));
+    const T ne = n0 * texp(lx * B(P.ne_idx) + gz) * taper;
+    const T tht = th0 * texp(lx * B(P.t_idx));
+    const B M = B(P.M);
+    const T r2 = r * r, a2 = a * a, s2 = sn * sn;
+    const T Sig = r2 + a2 * cs * cs;
+    const T f = B(2.0) * M * r / Sig;
+    const T gtt = f - B(1.0);
+    const T gtp = -(f * a * s2);
+    const T gpp = (r2 + a2 + f * a2 * s2) * s2;
+    const B sM = B(sqrt(P.M));
+    const T Om = T(sM) / (r * tsqrt(r) + a * sM);
+    const T n2 = -(gtt + B(2.0) * Om * gtp + Om * Om * gpp);
+    if (!(val(n2) > 0)) return o;
+    const T ut = T(1.0) / tsqrt(n2);
+    const T g = -(ut * (gtt + Om * gtp) * kt + ut * (gtp + Om * gpp) * kph);
+    if (!(val(g) > 0)) return o;
+    o.cj = ne * ne * B(Bd.cj_unit);
+    o.th = tht;
+    o.g = g;
+    o.on = true;
+    return o;
+}
+
+// Slopes of one bin without the exp(-tau) factor (slope[tau] = ft,
+// slope[I] = fi exp(-tau)): j_nu = cj Theta^-1/2 exp(-u) g_ff(gamma^2, u),
+// u = h nu / (Theta m_e c^2) with nu = g nu_c, gamma^2 = Ry / (Theta m_e c^2),
+// alpha_nu = j_nu / B_nu(T_e) = j_nu expm1(u) / (2 h nu^3 / c^2).
+template <class T>
+RTW_HD void brems_bin(const BremsDev& Bd, const TorusPt<T>& S, const TorusBin& bn, T& ft, T& fi) {
+    typedef decltype(val(S.g)) B;
+    const T u = S.g * B(bn.hk) / S.th;
+    if (!(val(u) > 0)) {
+        ft = T(0.0);
+        fi = T(0.0);
+        return;
+    }
+    const T gam2 = T(B(Bd.ry_mec2)) / S.th;
+    const float gff = gaunt_van_hoof(Bd.lut, rlog10f_(val(gam2)), rlog10f_(val(u)));
+    const T j = S.cj / tsqrt(S.th) * texp(-u) * B(gff);
+    const T g2 = S.g * S.g;
+    const T g4 = g2 * g2;
+    fi = -(j * B(bn.inv_nu_nm3) / g4);
+    ft = -(j * texpm1(u) / (g4 * B(bn.b0)));
+}
+
 // Cube-map neighbours (cube_wrap, gen_geometry.jl:128-344). Texel (i, j) of
 // face F, 1-based with n texels per face edge, moved by x texels along i and
 // y along j. A move that leaves the face enters the face across that edge,

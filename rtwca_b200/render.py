@@ -67,7 +67,7 @@ class Renderer:
     def params(colors_nm, precision=abi.PREC_FP64, integrator=abi.DP45_REF_COMPAT, max_dt_scale=0.1,
                block_warps=0, ctas_per_sm=0, promote_dr=0.0, promote_sin=0.0, stream=None,
                pixel_order=0, ray_bundles=False, trace_ray=-1, refill_min=0, autotune=False, graph=False,
-               skybox=(None, None)):
+               skybox=(None, None), gaunt_lut=None):
         """skybox: the wormhole's two cube maps, each None or a float32 array
         [3 h, 4 h, 3] in the reference's cross layout (RGB in [0, 1])."""
         colors = np.ascontiguousarray(np.asarray(colors_nm, dtype=np.float64))
@@ -98,6 +98,12 @@ class Renderer:
                 raise ValueError("a skybox is a float32 array [3 h, 4 h, 3]")
             p.skybox[k] = t.ctypes.data_as(C.POINTER(C.c_float))
             p.skybox_h[k] = h
+            keep.append(t)
+        if gaunt_lut is not None:  # the bremsstrahlung torus's Gaunt-factor table
+            t = np.ascontiguousarray(np.asarray(gaunt_lut, dtype=np.float32))
+            if t.shape != (abi.GAUNT_ROWS, abi.GAUNT_COLS):
+                raise ValueError(f"gaunt_lut is a float32 array [{abi.GAUNT_ROWS}, {abi.GAUNT_COLS}]")
+            p.gaunt_lut = t.ctypes.data_as(C.POINTER(C.c_float))
             keep.append(t)
         p._keep = keep  # keep the arrays alive with the struct
         return p
