@@ -272,6 +272,12 @@ typedef struct rtw_render_params {
        row-major float32, host memory (the reference's Gaunt_LUT[i, j] is
        gaunt_lut[(i - 1) * RTW_GAUNT_COLS + (j - 1)]). Required for that scene. */
     const float* gaunt_lut;
+    /* FP32-mixed trace kernel (kinds 0-3): 0 (default) hands each ray that
+       comes within promote_dr of the horizon or promote_sin of a pole to a
+       second pass of the kernel that traces such rays, all in FP64 stages,
+       in whole warps (the results are the same bit for bit); -1 keeps every
+       ray in its lane, with FP64 stages there. */
+    int32_t tail_pass;
 } rtw_render_params;
 
 #define RTW_GAUNT_ROWS 146
@@ -321,6 +327,8 @@ typedef struct rtw_stats {
     int32_t block_warps;        /*   warps per CTA */
     int32_t refill_min;         /*   compaction interval */
     int32_t graph_replayed;     /* 1: the render replayed a captured graph */
+    uint64_t tail_rays;         /* FP32-mixed trace kernel: rays finished by the
+                                   FP64 tail pass */
 } rtw_stats;
 
 /* Algorithmic operation counts of the trace kernel's arithmetic for one scene

@@ -105,7 +105,7 @@ class RenderParams(C.Structure):
         ("stream", C.c_void_p), ("pixel_order", C.c_int32), ("refill_min", C.c_int32),
         ("trace_ray", C.c_int64), ("autotune", C.c_int32), ("graph", C.c_int32),
         ("skybox", C.POINTER(C.c_float) * 2), ("skybox_h", C.c_int32 * 2),
-        ("gaunt_lut", C.POINTER(C.c_float)),
+        ("gaunt_lut", C.POINTER(C.c_float)), ("tail_pass", C.c_int32),
     ]
 
 
@@ -124,6 +124,7 @@ class Stats(C.Structure):
         ("escape_substeps", C.c_uint64), ("nan_rays", C.c_uint64),
         ("kernel_ms", C.c_double), ("total_ms", C.c_double), ("phase_cycles", C.c_uint64 * 4),
         ("grid", C.c_int32), ("block_warps", C.c_int32), ("refill_min", C.c_int32), ("graph_replayed", C.c_int32),
+        ("tail_rays", C.c_uint64),
     ]
 
 

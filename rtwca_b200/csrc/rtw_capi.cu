@@ -31,13 +31,23 @@ static const void* kernel_ptr(int kind, int precision, int np) {
     }
 }
 
-cudaError_t launch_trace(const KParams& p, int precision, int grid, int block, cudaStream_t stream) {
+static cudaError_t launch_one(const KParams& p, int precision, int grid, int block, cudaStream_t stream) {
     switch (p.sc.kind) {
     case 0: return launch_kind_0(p, precision, grid, block, stream);
     case 1: return launch_kind_1(p, precision, grid, block, stream);
     case 2: return launch_kind_2(p, precision, grid, block, stream);
     default: return launch_kind_3(p, precision, grid, block, stream);
     }
+}
+
+// The trace kernel; with a tail queue (FP32-mixed), the main pass and then,
+// on the same stream, the tail pass over the rays the main pass queued.
+cudaError_t launch_trace(const KParams& p, int precision, int grid, int block, cudaStream_t stream) {
+    const cudaError_t e = launch_one(p, precision, grid, block, stream);
+    if (e != cudaSuccess || !p.tail || precision != RTW_PREC_MIXED) return e;
+    KParams q = p;
+    q.tail_mode = 1;
+    return launch_one(q, precision, grid, block, stream);
 }
 
 size_t spec_bytes_per_warp(int precision, int np) {
@@ -289,6 +299,7 @@ void rtw_destroy(rtw_ctx* ctx) {
     cudaFree(ctx->d_bins);
     cudaFree(ctx->d_ctl);
     cudaFree(ctx->d_spec);
+    cudaFree(ctx->d_tail);
     cudaFree(ctx->d_out);
     cudaFree(ctx->d_sink);
     cudaFree(ctx->d_fclock);
@@ -655,6 +666,16 @@ rtw_status rtw_render(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* ca
     rtw_status s;
     if ((s = ensure(ctx, &ctx->d_frames, &ctx->frames_cap, sizeof(FrameDesc) * n_cams)) != RTW_OK) return s;
     if ((s = ensure(ctx, &ctx->d_spec, &ctx->spec_cap, spec_need)) != RTW_OK) return s;
+    // the FP32-mixed tail queue: room for a quarter of the rays (at least
+    // 65536); rays past it stay in their lanes
+    const bool use_tail = prm->precision == RTW_PREC_MIXED && prm->tail_pass >= 0 && !plain;
+    long long tail_cap = 0;
+    if (use_tail) {
+        tail_cap = std::min<long long>(total, std::max<long long>(65536, total / 4));
+        const size_t rec = ((sizeof(TailRec) * (size_t)tail_cap + 255) & ~(size_t)255);
+        if ((s = ensure(ctx, &ctx->d_tail, &ctx->tail_bytes, rec + sizeof(float) * 3 * np * (size_t)tail_cap)) != RTW_OK)
+            return s;
+    }
     if ((s = ensure(ctx, (void**)&ctx->d_fclock, &ctx->fclock_cap, sizeof(unsigned long long) * 3 * n_cams)) != RTW_OK)
         return s;
 
@@ -726,6 +747,12 @@ rtw_status rtw_render(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* ca
     p.trace_cap = tracing ? out->trace_capacity : 0;
     p.refill_min = refill;
     p.frame_clock = ctx->d_fclock;
+    if (use_tail) {
+        p.tail = (TailRec*)ctx->d_tail;
+        p.tail_spec = (float*)((char*)ctx->d_tail + ((sizeof(TailRec) * (size_t)tail_cap + 255) & ~(size_t)255));
+        p.tail_cap = tail_cap;
+    }
+    ctx->last_tail_cap = use_tail ? tail_cap : 0;
 
     const size_t frames_bytes = sizeof(FrameDesc) * n_cams;
     const size_t bins_bytes = sizeof(double) * 4 * RTW_MAX_BINS;
@@ -863,6 +890,7 @@ rtw_status rtw_get_stats(rtw_ctx* ctx, rtw_stats* out) {
     out->block_warps = ctx->last_warps;
     out->refill_min = ctx->last_refill;
     out->graph_replayed = ctx->last_replayed;
+    out->tail_rays = std::min<unsigned long long>(ds.tail_rays, (unsigned long long)ctx->last_tail_cap);
     return RTW_OK;
 }
 

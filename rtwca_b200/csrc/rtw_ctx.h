@@ -29,6 +29,9 @@ struct rtw_ctx {
     unsigned long long* d_ctl = nullptr;  // [0] work counter, then DevStats
     void* d_spec = nullptr;
     size_t spec_cap = 0;
+    void* d_tail = nullptr;  // FP32-mixed tail queue: records, then spectral rows
+    size_t tail_bytes = 0;
+    long long last_tail_cap = 0;
     void* d_out = nullptr;
     size_t out_cap = 0;
     float* d_sink = nullptr;

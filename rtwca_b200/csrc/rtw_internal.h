@@ -49,6 +49,20 @@ struct DevStats {
     unsigned long long rays;
     // RTW_PHASE_CLOCKS builds only: SM cycles per phase, summed over warps
     unsigned long long cyc_refill, cyc_geo, cyc_spec, cyc_commit;
+    // rays handed to the FP64 tail pass (slots asked for; the pass takes at
+    // most the queue's capacity), and the tail pass's work counter
+    unsigned long long tail_rays, tail_counter;
+};
+
+// A ray handed from the main pass of the FP32-mixed trace kernel to its tail
+// pass, at the start of an attempt: the lane state, exactly. Its spectral row
+// (intensity, carried slope, Kahan low part, np values each) is stored apart.
+struct TailRec {
+    double x[9];
+    double h, tol, r_term, thick;
+    long long gid, nsteps, max_steps;
+    float k1[9];
+    int fi, prev_rej, spec_live;
 };
 
 struct KParams {
@@ -91,6 +105,15 @@ struct KParams {
     // [n_frames] global-timer ns when the frame's first ray started, then
     // [n_frames] when its last ray finished
     unsigned long long* frame_clock;
+    // FP32-mixed kernel: rays that need FP64 stages (within promote_dr of the
+    // horizon or promote_theta of a pole) at the start of an attempt leave the
+    // main pass (tail_mode 0) for the queue `tail` (tail_cap records, spectral
+    // rows in tail_spec [tail_cap][3][np]); the tail pass (tail_mode 1) traces
+    // them with whole warps of such rays. tail NULL: every ray stays in its lane.
+    TailRec* tail;
+    float* tail_spec;
+    long long tail_cap;
+    int tail_mode;
 };
 
 // Scene constants of the device functors from the public scene struct.

@@ -503,6 +503,31 @@ __device__ __noinline__ FreshRay<K> fresh_ray(const KParams& p, long long id) {
     return o;
 }
 
+// The tail queue's record of a ray, written and read out of line (both run
+// once per queued ray; inline, their state copies raised the hot loop's
+// spills).
+template <class K>
+__device__ __noinline__ void tail_store(TailRec* t, const double* x, const K* k1, double h, double tol, double r_term,
+                                        double thick, long long gid, long long nsteps, long long max_steps, int fi,
+                                        bool prev_rej, bool spec_live) {
+    for (int i = 0; i < 9; ++i) {
+        t->x[i] = x[i];
+        t->k1[i] = float(k1[i]);
+    }
+    t->h = h;
+    t->tol = tol;
+    t->r_term = r_term;
+    t->thick = thick;
+    t->gid = gid;
+    t->nsteps = nsteps;
+    t->max_steps = max_steps;
+    t->fi = fi;
+    t->prev_rej = prev_rej ? 1 : 0;
+    t->spec_live = spec_live ? 1 : 0;
+}
+template <class T>
+__device__ __noinline__ T tail_load(const T* t) { return *t; }
+
 // Launch bounds: 128 threads per CTA; RTW_MIXED_MIN_CTAS resident CTAs per SM
 // for the mixed kernel (3: 168 registers per thread, measured faster than 4
 // with spills or 2), 2 for the FP64 kernel.
@@ -578,6 +603,13 @@ __global__ void __launch_bounds__(128, MIXED ? RTW_MIXED_MIN_CTAS : 2) trace_ker
 #else
 #define RTW_PHASE(acc) do {} while (0)
 #endif
+    // the tail pass takes the queued rays (at most tail_cap), with its own counter
+    const bool tail_pass = MIXED && p.tail_mode;
+    const long long total_rays =
+        tail_pass ? (long long)min(*(volatile unsigned long long*)&p.stats->tail_rays, (unsigned long long)p.tail_cap)
+                  : p.total_rays;
+    unsigned long long* const work_counter = tail_pass ? &p.stats->tail_counter : p.counter;
+    long long tail_id = -1;  // tail pass: the queue record of the lane's ray
     for (;;) {
         // ---------------- refill -----------------------------------------
         const unsigned empty = __ballot_sync(kFull, !active);
@@ -587,12 +619,35 @@ __global__ void __launch_bounds__(128, MIXED ? RTW_MIXED_MIN_CTAS : 2) trace_ker
         if (empty && !dry && (__popc(empty) >= p.refill_min || empty == kFull)) {
             unsigned long long base = 0;
             const unsigned n = __popc(empty);
-            if (lane == 0) base = atomicAdd(p.counter, (unsigned long long)n);
+            if (lane == 0) base = atomicAdd(work_counter, (unsigned long long)n);
             base = __shfl_sync(kFull, base, 0);
-            if ((long long)(base + n) >= p.total_rays) dry = true;
-            if (!active) {
+            if ((long long)(base + n) >= total_rays) dry = true;
+            if (!active && tail_pass) {
                 const long long id = (long long)base + __popc(empty & ((1u << lane) - 1u));
-                if (id < p.total_rays) {
+                if (id < total_rays) {
+                    const TailRec t = tail_load(p.tail + id);
+#pragma unroll
+                    for (int i = 0; i < 9; ++i) {
+                        x[i] = t.x[i];
+                        k1[i] = K(t.k1[i]);
+                    }
+                    gid = t.gid;
+                    fi = t.fi;
+                    tol = t.tol;
+                    r_term = t.r_term;
+                    thick = t.thick;
+                    max_steps = t.max_steps;
+                    h = t.h;
+                    nsteps = t.nsteps;
+                    prev_rej = t.prev_rej != 0;
+                    spec_live = t.spec_live != 0;
+                    tail_id = id;
+                    active = true;
+                    fresh = true;
+                }
+            } else if (!active) {
+                const long long id = (long long)base + __popc(empty & ((1u << lane) - 1u));
+                if (id < total_rays) {
                     const FreshRay<K> fr = fresh_ray<KIND, K, CT>(p, id);
 #pragma unroll
                     for (int i = 0; i < 9; ++i) {
@@ -617,8 +672,25 @@ __global__ void __launch_bounds__(128, MIXED ? RTW_MIXED_MIN_CTAS : 2) trace_ker
                 }
             }
         }
-        // spectral init of fresh rays: I = 0, k1 = slope at the camera
-        {
+        // spectral init of fresh rays: I = 0, k1 = slope at the camera (tail
+        // pass: the row the ray left the main pass with)
+        if (tail_pass) {
+            unsigned fm = __ballot_sync(kFull, fresh);
+            while (fm) {
+                const int r = __ffs(fm) - 1;
+                fm &= fm - 1;
+                const float* row = p.tail_spec + __shfl_sync(kFull, tail_id, r) * (long long)ST::kFields * np;
+#pragma unroll
+                for (int b = 0; b < BPL; ++b) {
+                    const int c = lane + 32 * b;
+                    if (c < N) {
+                        sI[r * np + c] = row[c];
+                        sK[r * np + c] = row[np + c];
+                        if constexpr (MIXED) sL[r * np + c] = row[2 * np + c];
+                    }
+                }
+            }
+        } else {
             unsigned fm = __ballot_sync(kFull, fresh);
             while (fm) {
                 const int r = __ffs(fm) - 1;
@@ -640,6 +712,56 @@ __global__ void __launch_bounds__(128, MIXED ? RTW_MIXED_MIN_CTAS : 2) trace_ker
         if (!act) break;
         __syncwarp();
         RTW_PHASE(cy_ref);
+
+        // ---------------- hand-off to the tail pass (FP32-mixed) ---------
+        // A ray that needs FP64 stages leaves the lane here, at the start of
+        // an attempt, with its whole state; the tail pass resumes this attempt.
+        // Rays within promote_dr of the horizon fall in from there, so they
+        // would run FP64 attempts for the rest of their path in a lane of an
+        // otherwise FP32 warp. Slots past the queue's capacity keep their ray.
+        if constexpr (MIXED) {
+            if (p.tail && !tail_pass) {
+                const bool want = active && ((x[1] - s.r_ev < p.promote_dr) || (x[2] < p.promote_theta) ||
+                                             (x[2] > kPi - p.promote_theta));
+                const unsigned hm = __ballot_sync(kFull, want);
+                if (hm) {
+                    unsigned long long base = 0;
+                    if (lane == 0) base = atomicAdd(&p.stats->tail_rays, (unsigned long long)__popc(hm));
+                    base = __shfl_sync(kFull, base, 0);
+                    const long long slot = (long long)base + __popc(hm & ((1u << lane) - 1u));
+                    const bool go = want && slot < p.tail_cap;
+                    if (go) {
+                        // out of line on copies, so that x and k1 stay in registers
+                        double xe[9];
+                        K ke[9];
+#pragma unroll
+                        for (int i = 0; i < 9; ++i) {
+                            xe[i] = x[i];
+                            ke[i] = k1[i];
+                        }
+                        tail_store<K>(p.tail + slot, xe, ke, h, tol, r_term, thick, gid, nsteps, max_steps, fi,
+                                      prev_rej, spec_live);
+                    }
+                    unsigned gm = __ballot_sync(kFull, go);
+                    while (gm) {
+                        const int r = __ffs(gm) - 1;
+                        gm &= gm - 1;
+                        float* row = p.tail_spec + __shfl_sync(kFull, slot, r) * (long long)ST::kFields * np;
+#pragma unroll
+                        for (int b = 0; b < BPL; ++b) {
+                            const int c = lane + 32 * b;
+                            if (c < N) {
+                                row[c] = sI[r * np + c];
+                                row[np + c] = sK[r * np + c];
+                                row[2 * np + c] = sL[r * np + c];
+                            }
+                        }
+                    }
+                    if (go) active = false;
+                    __syncwarp();
+                }
+            }
+        }
 
         // ---------------- geodesic phase ---------------------------------
         K ns[9];   // 5th-order slope: the new state is x + h ns

@@ -67,7 +67,7 @@ class Renderer:
     def params(colors_nm, precision=abi.PREC_FP64, integrator=abi.DP45_REF_COMPAT, max_dt_scale=0.1,
                block_warps=0, ctas_per_sm=0, promote_dr=0.0, promote_sin=0.0, stream=None,
                pixel_order=0, ray_bundles=False, trace_ray=-1, refill_min=0, autotune=False, graph=False,
-               skybox=(None, None), gaunt_lut=None):
+               skybox=(None, None), gaunt_lut=None, tail_pass=True):
         """skybox: the wormhole's two cube maps, each None or a float32 array
         [3 h, 4 h, 3] in the reference's cross layout (RGB in [0, 1])."""
         colors = np.ascontiguousarray(np.asarray(colors_nm, dtype=np.float64))
@@ -88,6 +88,7 @@ class Renderer:
         p.refill_min = int(refill_min)
         p.autotune = int(bool(autotune))
         p.graph = int(bool(graph))
+        p.tail_pass = 0 if tail_pass else -1
         keep = [colors]
         for k, tex in enumerate(skybox):
             if tex is None:

@@ -216,3 +216,48 @@ def test_plain_fp64_parity(renderer, oracle, name):
     # the trace kernel's FP64 path gives the same image
     t = _gpu(renderer, scene, cam, colors, precision=abi.PREC_FP64)
     assert np.mean(t["class"] == g["class"]) >= 0.999
+
+
+@pytest.mark.parametrize("name,integ", [("kerr_thin_disk", abi.DP45_REF_COMPAT), ("kerr_thin_disk", abi.DP45_FSAL),
+                                        ("schwarzschild_disk", abi.DP45_REF_COMPAT),
+                                        ("kerr_thick_disk", abi.DP45_REF_COMPAT)])
+def test_tail_pass_is_bit_identical(renderer, name, integ):
+    """FP32-mixed: rays that need FP64 stages (near the horizon or a pole)
+    leave the main pass for the tail pass with their whole state at the start
+    of an attempt; every output is the same bit for bit as when they stay in
+    their lanes, and some rays do take the tail pass."""
+    scene, cam, _ = configs.workload(name, x_pix=48)
+    colors = configs.log_spaced_colors(16)
+    a = _gpu(renderer, scene, cam, colors, precision=abi.PREC_MIXED, integrator=integ, tail_pass=True)
+    sa = renderer.stats()
+    b = _gpu(renderer, scene, cam, colors, precision=abi.PREC_MIXED, integrator=integ, tail_pass=False)
+    sb = renderer.stats()
+    print(name, "tail rays", sa["tail_rays"], "of", sa["rays"])
+    assert sa["tail_rays"] > 0 and sb["tail_rays"] == 0
+    for k in ("xyz", "class", "steps", "spectrum", "state", "tau"):
+        assert np.array_equal(a[k], b[k]), k
+    for k in ("step_attempts", "rejected_steps", "promoted_steps", "spectral_steps", "rays"):
+        assert sa[k] == sb[k], k
+
+
+def test_tail_pass_batched_and_traced(renderer):
+    """Several cameras in one launch, the step trace of a ray that takes the
+    tail pass, and the per-frame clocks, with and without the tail pass."""
+    scene = configs.kerr_disk_scene()
+    colors = configs.log_spaced_colors(16)
+    cams = [configs.look_at_camera(30.0, math.radians(60.0), 45.0, 24, 1e-6),
+            configs.look_at_camera(12.0, math.radians(85.0), 45.0, 16, 1e-8)]
+    a = renderer.render(scene, cams, colors, want=("xyz", "class", "steps"), precision=abi.PREC_MIXED)
+    b = renderer.render(scene, cams, colors, want=("xyz", "class", "steps"), precision=abi.PREC_MIXED,
+                        tail_pass=False)
+    for k in ("xyz", "class", "steps"):
+        assert np.array_equal(a[k], b[k]), k
+    ft = renderer.frame_times(2) if hasattr(renderer, "frame_times") else None
+    if ft is not None:
+        assert np.all(np.isfinite(ft["done"]))
+    # a horizon ray of the first camera: its trace is the same either way
+    q = int(np.flatnonzero(a["class"][: 24 * 24] == abi.CLASS_HORIZON)[0])
+    ta = renderer.render(scene, [cams[0]], colors, want=("class",), precision=abi.PREC_MIXED, trace_ray=q)["trace"]
+    tb = renderer.render(scene, [cams[0]], colors, want=("class",), precision=abi.PREC_MIXED, trace_ray=q,
+                         tail_pass=False)["trace"]
+    assert np.array_equal(ta, tb, equal_nan=True)
