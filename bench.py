@@ -215,14 +215,14 @@ def shadow_annulus(cls_img, x_pix, y_pix, width=3):
     return np.flatnonzero(band.ravel())
 
 
-def cpu_time(scene, cam, colors, n, threads=0, keep=False, skybox=(None, None)):
+def cpu_time(scene, cam, colors, n, threads=0, keep=False, skybox=(None, None), gaunt_lut=None):
     from oracle import oracle as O
     O.build()
     P = cam.x_pix * cam.y_pix
     ids = cpu_sample_ids(P, n)
     t = time.perf_counter()
-    res = O.render(scene, cam, colors, pixel_ids=ids, threads=threads, want=("xyz", "class", "steps", "state"),
-                   skybox=skybox)
+    want = ("xyz", "class", "steps", "state") + (("spectrum",) if gaunt_lut is not None else ())
+    res = O.render(scene, cam, colors, pixel_ids=ids, threads=threads, want=want, skybox=skybox, gaunt_lut=gaunt_lut)
     dt = time.perf_counter() - t
     cores = threads if threads > 0 else (os.cpu_count() or 1)
     if keep:
@@ -386,7 +386,11 @@ def scenes_leg(r, rank, cpu=True):
     camera inside the cylinder), the Dneg wormhole ("wormhole", two
     synthetic 64-texel cube maps from numpy default_rng(0) standing in for the
     reference's missing skybox PNGs) and the Cartesian blackbody sphere
-    ("minkowski_t,x,y,z_sphere", the first of those maps as its skybox). FP32-mixed and FP64, the reference's step.
+    ("minkowski_t,x,y,z_sphere", the first of those maps as its skybox), and the
+    bremsstrahlung torus (the Gaunt-factor lookup of emission_functions.jl:54-78
+    on a smooth stand-in table on the van Hoof grid; 512^2, 230 GHz +- 20 %,
+    8 bins, the torus camera; its parity on the spectra). FP32-mixed and FP64,
+    the reference's step.
     Device time of the kernel (1 warm-up + 3 timed renders, mean); on rank 0
     the FP64 oracle on 4096 evenly spaced pixels on all host cores gives the
     CPU rate and a parity sample (linear Y within 1e-3)."""
@@ -404,24 +408,32 @@ def scenes_leg(r, rank, cpu=True):
                                ("synch_synchro_test", configs.synchro_scene(), configs.synchro_camera, {}),
                                ("wormhole", configs.wormhole_scene(), configs.wormhole_camera, {"skybox": sky}),
                                ("minkowski_cart_sphere", configs.cart_sphere_scene(), configs.cart_sphere_camera,
-                                {"skybox": (sky[0], None)})):
-        cam = camf(1024, 1e-6)
+                                {"skybox": (sky[0], None)}),
+                               ("brems_torus", configs.brems_scene(), configs.torus_camera,
+                                {"gaunt_lut": configs.smooth_gaunt_table()})):
+        cam = camf(1024 if name != "brems_torus" else 512, tol=1e-6)
         P = cam.x_pix * cam.y_pix
-        leg = {"workload": f"{name} {cam.x_pix}x{cam.y_pix}, 3 bins 400/550/700 nm, tol 1e-6, reference step"}
+        colv = configs.torus_colors(8) if name == "brems_torus" else col
+        leg = {"workload": f"{name} {cam.x_pix}x{cam.y_pix}, {colv.size} bins, tol 1e-6, reference step"}
         for pname, prec in (("mixed", abi.PREC_MIXED), ("fp64", abi.PREC_FP64)):
-            r.render(sc, [cam], col, want=("xyz",), precision=prec, integrator=abi.DP45_REF_COMPAT, **kw)
+            wv = ("spectrum",) if name == "brems_torus" else ("xyz",)
+            r.render(sc, [cam], colv, want=wv, precision=prec, integrator=abi.DP45_REF_COMPAT, **kw)
             ms = []
             for _ in range(3):
-                g = r.render(sc, [cam], col, want=("xyz",), precision=prec, integrator=abi.DP45_REF_COMPAT, **kw)
+                g = r.render(sc, [cam], colv, want=wv, precision=prec, integrator=abi.DP45_REF_COMPAT, **kw)
                 ms.append(r.stats()["kernel_ms"])
             t = float(np.mean(ms))
             leg[pname] = {"Mrays_s": P / t / 1e3, "ms": t, "step_attempts": r.stats()["step_attempts"]}
             if pname == "mixed":
-                gx = g["xyz"]
+                gx = g["spectrum"] if name == "brems_torus" else g["xyz"]
         if cpu and rank == 0:
-            v, n, dt, cores, ref = cpu_time(sc, cam, col, 4096, keep=True, skybox=kw.get("skybox", (None, None)))
+            v, n, dt, cores, ref = cpu_time(sc, cam, colv, 4096, keep=True, skybox=kw.get("skybox", (None, None)),
+                                            gaunt_lut=kw.get("gaunt_lut"))
             ids = cpu_sample_ids(P, 4096)
-            e = rel_err(gx[ids, 1], ref["xyz"][:, 1])
+            if name == "brems_torus":  # mm-wave bins: the spectra (the CIE weights vanish there)
+                e = rel_err(gx[ids].ravel(), ref["spectrum"].ravel())
+            else:
+                e = rel_err(gx[ids, 1], ref["xyz"][:, 1])
             leg["cpu_oracle"] = {"Mrays_s": v, "pixels": n, "s": dt, "cores": cores}
             leg["mixed_over_cpu"] = leg["mixed"]["Mrays_s"] / v
             leg["parity_sample_within_1e-3"] = float(np.mean(e <= 1e-3))
@@ -801,7 +813,7 @@ def run_b200(args):
                               "attempts",
             "op_counts": oc, "steps_per_ray": steps_hist(hs.numpy()),
             "counters": {k: st[k] for k in ("step_attempts", "rejected_steps", "promoted_steps", "spectral_steps",
-                                            "emitting_steps", "escape_substeps", "nan_rays")},
+                                            "emitting_steps", "escape_substeps", "nan_rays", "tail_rays")},
         }
         # every leg in full on stderr (one JSON line), the summary on stdout
         sys.stderr.write("BENCH_DETAILS " + json.dumps(details) + "\n")

@@ -273,10 +273,10 @@ typedef struct rtw_render_params {
        gaunt_lut[(i - 1) * RTW_GAUNT_COLS + (j - 1)]). Required for that scene. */
     const float* gaunt_lut;
     /* FP32-mixed trace kernel (kinds 0-3): 0 (default) hands each ray that
-       comes within promote_dr of the horizon or promote_sin of a pole to a
-       second pass of the kernel that traces such rays, all in FP64 stages,
-       in whole warps (the results are the same bit for bit); -1 keeps every
-       ray in its lane, with FP64 stages there. */
+       comes within promote_dr of the horizon (from where it falls in, with
+       FP64 stages) to a second pass of the kernel that traces such rays in
+       whole warps (the results are the same bit for bit); -1 keeps every ray
+       in its lane, with FP64 stages there. */
     int32_t tail_pass;
 } rtw_render_params;
 

@@ -54,6 +54,22 @@ size_t spec_bytes_per_warp(int precision, int np) {
     return precision == RTW_PREC_MIXED ? (size_t)3 * 32 * np * sizeof(float) : (size_t)2 * 32 * np * sizeof(double);
 }
 
+size_t trace_dyn_smem(int precision, int np, int warps) {
+#if RTW_SPEC_SHARED
+    if (precision == RTW_PREC_MIXED && np <= 64) return (size_t)warps * 2 * 32 * np * sizeof(float);
+#endif
+    return 0;
+}
+
+cudaError_t trace_allow_smem(int kind, int precision, int np) {
+    const size_t bytes = trace_dyn_smem(precision, np, 4);  // the largest CTA: 4 warps
+    if (!bytes) return cudaSuccess;
+    const void* fn = kernel_ptr(kind, precision, np);
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+}
+
 cudaError_t trace_attributes(int kind, int precision, int np, cudaFuncAttributes* attr) {
     return cudaFuncGetAttributes(attr, kernel_ptr(kind, precision, np));
 }
@@ -653,10 +669,12 @@ rtw_status rtw_render(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* ca
     if (warps == 0) warps = 4;
     if (refill == 0) refill = 1;
     const int block = 32 * warps;
+    if (!plain) RTW_CUDA(trace_allow_smem(scene->kind, prm->precision, np), "kernel shared-memory attribute");
     int per_sm = prm->ctas_per_sm;
     if (per_sm <= 0) {
         int occ = 0;
-        RTW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel_ptr(scene->kind, prm->precision, np), block, 0),
+        RTW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel_ptr(scene->kind, prm->precision, np), block,
+                                                               trace_dyn_smem(prm->precision, np, warps)),
                  "occupancy query");
         per_sm = std::max(1, occ);
     }

@@ -7,6 +7,12 @@
 
 #include "../../include/rtw.h"
 
+// FP32-mixed trace kernel with up to 64 bins: the spectral phase's intensity
+// and carried-slope rows in shared memory (1), or in the global scratch (0).
+#ifndef RTW_SPEC_SHARED
+#define RTW_SPEC_SHARED 1
+#endif
+
 namespace rtw {
 
 // One frame (camera) of a batched render: the FP64 camera transform of
@@ -105,11 +111,11 @@ struct KParams {
     // [n_frames] global-timer ns when the frame's first ray started, then
     // [n_frames] when its last ray finished
     unsigned long long* frame_clock;
-    // FP32-mixed kernel: rays that need FP64 stages (within promote_dr of the
-    // horizon or promote_theta of a pole) at the start of an attempt leave the
-    // main pass (tail_mode 0) for the queue `tail` (tail_cap records, spectral
-    // rows in tail_spec [tail_cap][3][np]); the tail pass (tail_mode 1) traces
-    // them with whole warps of such rays. tail NULL: every ray stays in its lane.
+    // FP32-mixed kernel: rays within promote_dr of the horizon at the start
+    // of an attempt leave the main pass (tail_mode 0) for the queue `tail`
+    // (tail_cap records, spectral rows in tail_spec [tail_cap][3][np]); the
+    // tail pass (tail_mode 1) traces them with whole warps of such rays.
+    // tail NULL: every ray stays in its lane.
     TailRec* tail;
     float* tail_spec;
     long long tail_cap;
@@ -126,6 +132,11 @@ cudaError_t launch_trace(const KParams& p, int precision, int grid, int block, c
 cudaError_t launch_plain(const KParams& p, int grid, int block, cudaStream_t stream);
 // Bytes of spectral scratch per warp for a precision and padded bin count.
 size_t spec_bytes_per_warp(int precision, int np);
+// Dynamic shared memory of a trace-kernel CTA of `warps` warps (the spectral
+// rows kept in shared memory: FP32-mixed, np <= 64), and the kernel attribute
+// that allows it (call before a launch or an occupancy query).
+size_t trace_dyn_smem(int precision, int np, int warps);
+cudaError_t trace_allow_smem(int kind, int precision, int np);
 // Registers / max threads of the kernel that launch_trace would run.
 cudaError_t trace_attributes(int kind, int precision, int np, cudaFuncAttributes* attr);
 

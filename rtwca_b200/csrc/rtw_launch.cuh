@@ -25,7 +25,7 @@ template <int KIND>
 cudaError_t launch_kind(const KParams& p, int precision, int grid, int block, cudaStream_t stream) {
     const void* fn = trace_kernel_ptr<KIND>(precision, p.np);
     void* args[] = {(void*)&p};
-    return cudaLaunchKernel(fn, dim3(grid), dim3(block), args, 0, stream);
+    return cudaLaunchKernel(fn, dim3(grid), dim3(block), args, trace_dyn_smem(precision, p.np, block / 32), stream);
 }
 
 }  // namespace rtw

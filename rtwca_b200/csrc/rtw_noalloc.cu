@@ -189,10 +189,12 @@ extern "C" rtw_status rtw_render_noalloc(const rtw_scene* scene, const rtw_camer
     // CTAs per SM when given), capped by the scratch
     const int warps = prm->block_warps > 0 ? (prm->block_warps < 4 ? prm->block_warps : 4) : 4;
     const int block = 32 * warps;
+    if (trace_allow_smem(scene->kind, prm->precision, np) != cudaSuccess)
+        return fail(RTW_ERR_CUDA, "kernel shared-memory attribute failed");
     int occ = prm->ctas_per_sm;
     if (occ <= 0 &&
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, noalloc_kernel(scene->kind, prm->precision, np), block, 0) !=
-            cudaSuccess)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, noalloc_kernel(scene->kind, prm->precision, np), block,
+                                                      trace_dyn_smem(prm->precision, np, warps)) != cudaSuccess)
         return fail(RTW_ERR_CUDA, "occupancy query failed");
     const size_t per_warp = spec_bytes_per_warp(prm->precision, np);
     const long long fit = (long long)(RTW_NOALLOC_SCRATCH_BYTES / (per_warp * warps));

@@ -50,6 +50,14 @@ constexpr int kSpecLanes = RTW_SPEC_LANES;
 static_assert(kSpecLanes == 32 || kSpecLanes == 16 || kSpecLanes == 8 || kSpecLanes == 4, "RTW_SPEC_LANES");
 constexpr int kSpecGroups = 32 / kSpecLanes;
 
+// FP32-mixed with up to 64 bins: the intensity and carried-slope rows of the
+// spectral phase live in shared memory (2 x 32 x np floats per warp, dynamic);
+// the Kahan low parts, which the error reduction does not wait for, stay in the
+// global scratch. RTW_SPEC_SHARED (rtw_internal.h) 0 keeps every row in global
+// memory.
+template <bool MIXED, int BPL>
+RTW_HD constexpr bool spec_in_shared() { return RTW_SPEC_SHARED && MIXED && BPL <= 2; }
+
 // Dormand-Prince coefficients (64BitConstants.jl:28-37): a_sl, b_l (= a_7l), b*_l.
 constexpr double a21 = 1.0 / 5;
 constexpr double a31 = 3.0 / 40, a32 = 9.0 / 40;
@@ -554,8 +562,10 @@ __global__ void __launch_bounds__(128, MIXED ? RTW_MIXED_MIN_CTAS : 2) trace_ker
     const int L = 8 + 2 * N;
     const DevScene& s = p.sc;
     SR* spec = reinterpret_cast<SR*>(p.spec) + warp_id * (long long)ST::kFields * 32 * np;
-    SR* sI = spec;                  // [32][np]
-    SR* sK = spec + 32 * np;        // [32][np]
+    extern __shared__ __align__(16) unsigned char s_rows[];
+    constexpr bool kShRows = spec_in_shared<MIXED, BPL>();
+    SR* sI = kShRows ? reinterpret_cast<SR*>(s_rows) + wib * 2 * 32 * np : spec;  // [32][np]
+    SR* sK = sI + 32 * np;                                                       // [32][np]
     SR* sL = spec + 2 * 32 * np;    // [32][np] (MIXED only)
     SR* myA = &s_ax[wib][0][0][lane];
     SR* myX = &s_ax[wib][1][0][lane];
@@ -714,15 +724,17 @@ __global__ void __launch_bounds__(128, MIXED ? RTW_MIXED_MIN_CTAS : 2) trace_ker
         RTW_PHASE(cy_ref);
 
         // ---------------- hand-off to the tail pass (FP32-mixed) ---------
-        // A ray that needs FP64 stages leaves the lane here, at the start of
-        // an attempt, with its whole state; the tail pass resumes this attempt.
-        // Rays within promote_dr of the horizon fall in from there, so they
-        // would run FP64 attempts for the rest of their path in a lane of an
-        // otherwise FP32 warp. Slots past the queue's capacity keep their ray.
+        // A ray within promote_dr of the horizon leaves the lane here, at the
+        // start of an attempt, with its whole state; the tail pass resumes
+        // this attempt. Such a ray is inside the photon sphere moving inwards
+        // and falls in from there, so it would run FP64 attempts (about 400)
+        // for the rest of its path in a lane of an otherwise FP32 warp. Rays
+        // near a pole stay: they leave the pole's FP64 zone again, and their
+        // remaining paths (thousands of steps along the axis) would set the
+        // length of the tail pass. Slots past the queue's capacity keep their ray.
         if constexpr (MIXED) {
             if (p.tail && !tail_pass) {
-                const bool want = active && ((x[1] - s.r_ev < p.promote_dr) || (x[2] < p.promote_theta) ||
-                                             (x[2] > kPi - p.promote_theta));
+                const bool want = active && (x[1] - s.r_ev < p.promote_dr);
                 const unsigned hm = __ballot_sync(kFull, want);
                 if (hm) {
                     unsigned long long base = 0;
