@@ -50,6 +50,9 @@ def parse():
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the cfg1-cfg3 legs (Minkowski sphere 256^2, Schwarzschild 1024^2, Kerr thick 2048^2)")
     ap.add_argument("--adjoint-x-pix", type=int, default=512)
+    ap.add_argument("--torus-forward-only", action="store_true",
+                    help="time only the synchrotron torus's forward render (FP32-mixed, FSAL) at --adjoint-x-pix "
+                         "(one warm-up, --steps timed) and print one JSON line")
     ap.add_argument("--strong", action="store_true",
                     help="N>1: report the strong-scaling leg (one frame over N GPUs in interleaved tiles) as the "
                          "headline value")
@@ -825,8 +828,30 @@ def run_b200(args):
         dist.destroy_process_group()
 
 
+def torus_forward_only(args):
+    """The per-bin forward kernel alone on the synchrotron torus (the forward
+    render of the adjoint leg, without the adjoint's record pool)."""
+    from rtwca_b200 import Renderer, abi, configs
+    sc, cam, col = configs.torus_problem(x_pix=args.adjoint_x_pix, tol=1e-6)
+    r = Renderer(0)
+    r.render(sc, [cam], col, want=("spectrum",), precision=abi.PREC_MIXED, integrator=abi.DP45_FSAL)
+    ms = []
+    for _ in range(max(1, args.steps)):
+        r.render(sc, [cam], col, want=("spectrum",), precision=abi.PREC_MIXED, integrator=abi.DP45_FSAL)
+        ms.append(r.stats()["kernel_ms"])
+    P = cam.x_pix * cam.y_pix
+    st = r.stats()
+    print(json.dumps({"metric": "torus forward Mrays/s", "value": P / float(np.mean(ms)) / 1e3, "unit": "Mrays/s",
+                      "ms": ms, "step_attempts": st["step_attempts"],
+                      "workload": f"synchrotron torus {cam.x_pix}x{cam.y_pix}, 32 bins, tol 1e-6, FP32-mixed, FSAL"}))
+    r.close()
+
+
 def main():
     args = parse()
+    if args.torus_forward_only:
+        torus_forward_only(args)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -155,6 +155,9 @@ __device__ __forceinline__ float rabs(float v) { return fabsf(v); }
 __device__ __forceinline__ double rabs(double v) { return fabs(v); }
 __device__ __forceinline__ float rmax(float a, float b) { return fmaxf(a, b); }
 __device__ __forceinline__ double rmax(double a, double b) { return fmax(a, b); }
+// the smaller of two values; a NaN argument gives the other
+__device__ __forceinline__ float rmin_(float a, float b) { return fminf(a, b); }
+__device__ __forceinline__ double rmin_(double a, double b) { return fmin(a, b); }
 
 // Compensated (TwoSum) add into hi/lo.
 __device__ __forceinline__ void kahan_add(float& hi, float& lo, float t) {
