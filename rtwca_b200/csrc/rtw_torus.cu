@@ -1,14 +1,13 @@
 // rtw_torus.cu - the synchrotron torus: forward render (FP32-mixed or FP64,
 // FSAL Dormand-Prince, per-bin optical depth) and its discrete adjoint.
 //
-// Forward: each lane owns one ray's geodesic (rays taken from a global queue
-// by warp-aggregated refill). Per attempt the seven geodesic stages run first
-// (scene functor of rtw_scenes.cuh) and leave six emitter-number sets (cj,
-// nus, Theta, g) in shared memory; then the warp's lanes split the bins of
-// the rays that need bin work (a group of lanes per ray, one bin per lane),
-// each bin running its own seven tau / I stages from those numbers, with the
-// bins' state in per-warp scratch rows. The error norm is the reference's RMS
-// over all 8 + 2N components (integrators_LttM.jl:185-224).
+// Forward: one lane per ray, rays taken from a global queue one at a time
+// (per-lane refill; the lanes of a warp do not cooperate here). Per attempt
+// the seven geodesic stages run first (scene functor of rtw_scenes.cuh) and
+// leave six emitter-number sets (cj, nus, Theta, g) in local memory; then
+// each bin runs its own seven tau / I stages from those numbers in registers.
+// The error norm is the reference's RMS over all 8 + 2N components
+// (integrators_LttM.jl:185-224).
 //
 // Adjoint: one recording forward pass gives the image and, per ray, a chain
 // of chunks taken from a pool by an atomic counter, each chunk one segment:
@@ -276,7 +275,6 @@ struct TorusKP {
     double max_dt_scale, promote_dr, promote_theta;
     unsigned long long* counter;
     DevStats* stats;
-    void* spec;       // per-warp bin rows of the forward kernel ([fields][32 rays][32 bins] of its SR)
     float* spectrum;  // [P][N]
     float* xyz;       // [P][3]
     double* final_state;  // [P][8] (may be null)
@@ -644,27 +642,6 @@ __device__ __forceinline__ int torus_terminate(const TorusKP& p, const double* x
     return RTW_CLASS_THICK;
 }
 
-// calc_terminate with the least optical depth of the ray's bins in place of
-// the all-bins test (the same predicate: THICK when even the least has reached
-// -log(tol); NaN bins are passed over by the minimum as they are by the test)
-template <class SR, int EM>
-__device__ __forceinline__ int torus_terminate_min(const TorusKP& p, const double* x, SR tau_min) {
-    if constexpr (EM == 2 || EM == 4) {
-        if (sqrt(x[1] * x[1] + x[2] * x[2] + x[3] * x[3]) > p.m.geo.esc) return RTW_CLASS_ESCAPE;
-    } else if constexpr (EM == 3) {
-        if (wormhole_r<double>(p.m.wh, x[1]) > p.m.geo.esc) return RTW_CLASS_ESCAPE;
-        if (x[3] > p.m.geo.wind) return RTW_CLASS_WINDING;
-    } else {
-        if (x[1] > p.m.geo.esc) return RTW_CLASS_ESCAPE;
-        if (x[1] <= p.frame.r_term) return RTW_CLASS_HORIZON;
-        if (x[3] > p.m.geo.wind) return RTW_CLASS_WINDING;
-    }
-    if constexpr (EM >= 3)
-        if (p.bundles) return 0;
-    if ((double)tau_min < p.frame.thick) return 0;
-    return RTW_CLASS_THICK;
-}
-
 // Recording of one ray (record 1: dense offsets, 2: chunks). One kernel
 // instance serves renders and recording passes, so that both take
 // bit-identical steps; the per-segment work is out of line and the per-event
@@ -770,214 +747,132 @@ __device__ __noinline__ void torus_rec_end(const TorusKP& p, TorusRec* r, long l
 // Forward kernel. SR: arithmetic of the bins and of the stages (float on the
 // mixed path, with Kahan intensities and per-ray FP64 stages near the horizon
 // and the poles; double on the FP64 path).
-// (FP32-mixed: 3 CTAs/SM, 168 registers; FP64 stays at 2)
-//
-// Work decomposition: each lane owns one ray's geodesic (its FP64 state, the
-// stages, the controller); a ray's bins live in the warp's scratch rows
-// ([field][32 rays][32 bins], coalesced along the bins). In each attempt the
-// geodesic stages leave their emitter numbers in shared memory; then a
-// spectral pass serves 32 / L rays at once, L = the power of two >= N lanes
-// per ray, one bin per lane: each lane runs its bin's seven tau / I stages,
-// the group reduces the bins' error, the ray's lane decides the attempt (with
-// the geodesic error), and the lanes write the accepted bins back. A ray
-// whose stages do not emit and whose carried bin slopes are all zero leaves
-// its bins unchanged (every bin slope is 0), so it takes no pass.
+// (FP32-mixed: 3 CTAs/SM, 168 registers, measured 7-13 % faster than 2 CTAs at
+// 255; FP64 stays at 2, where 3 was 8-20 % slower)
 template <bool MIXED, int EM>
 __global__ void __launch_bounds__(128, MIXED ? 3 : 2) torus_forward(const TorusKP p) {
     constexpr bool FLAT = EM == 2 || EM == 4;  // Synchro_Test, the sphere: flat Cartesian geometry
     // the FP64 slope at a ray's start and after escapes: the instance's own
-    // emitter on the mixed path, the run-time dispatch on the FP64 path (where
-    // the instance's own emitter raised Synchro_Test's spills)
+    // emitter on the mixed path (ptxas: the torus, Powehi and wormhole
+    // instances then spill 32-124 B per thread instead of 318-326 with the
+    // run-time dispatch), the run-time dispatch on the FP64 path (where the
+    // instance's own emitter raised Synchro_Test's spills from 132 B to 496 B)
     constexpr int KEM = MIXED ? EM : -1;
     typedef typename SpecTraits<MIXED>::SR SR;
-    constexpr int kF = MIXED ? 5 : 4;  // row fields: tau, I (high part), carried tau slope, carried I slope, I low part
-    constexpr int kR = kTorusMaxBins;  // row length
-    // per-lane emitter numbers of stage points 1..6, read by the spectral pass
-    __shared__ SR s_pt[kMaxWarps][6][4][32];
-    __shared__ unsigned char s_on[kMaxWarps][6][32];  // bit 0: on, bits 1..: zone
-
     const int N = p.m.n;
     const int D = 8 + 2 * N;
-    const int lane = threadIdx.x & 31;
-    const int wib = threadIdx.x >> 5;
-    const long long warp_id = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    SR* rows = reinterpret_cast<SR*>(p.spec) + warp_id * (long long)kF * 32 * kR;
-    SR* rT = rows;                 // [32][kR] optical depths
-    SR* rH = rows + 32 * kR;       // intensities (high part)
-    SR* rKT = rows + 2 * 32 * kR;  // carried tau slopes
-    SR* rKI = rows + 3 * 32 * kR;  // carried I slopes
-    SR* rL = rows + 4 * 32 * kR;   // intensity low parts (MIXED)
-    SR* myT = rT + lane * kR;
-    SR* myH = rH + lane * kR;
-    SR* myKT = rKT + lane * kR;
-    SR* myKI = rKI + lane * kR;
-    SR* myL = rL + lane * kR;
-    // lanes per ray in a spectral pass and rays per pass
-    int L = 1;
-    while (L < N) L <<= 1;
-    const int G = 32 / L;
-    const int grp = lane / L, sub = lane % L;
-    const bool bin_ok = sub < N;
-
     unsigned c_att = 0, c_rej = 0, c_pro = 0, c_esc = 0, c_rays = 0, c_nan = 0;
-    // lane ray state
-    bool active = false, dry = false;
-    long long loc = 0, sub_id = 0, id = 0;
-    int pi = 0, pj = 0;
-    double x[9];
-    SR k1[8];
-    double h = 0;
-    uint8_t hsrc = 2;
-    bool prev_rej = false, escaped = false, spec_live = false;
-    long long nsteps = 0;
-    uint32_t n_ev = 0;
-    SR tau_min = SR(0);
-    TorusRec rec;
-    const double tol = p.frame.tol;
-
-    // the state before event n_ev when it starts a segment (recording)
-    auto checkpoint = [&]() {
-        if (p.record && (n_ev % rec.kc) == 0u) torus_rec_checkpoint<SR, MIXED>(p, &rec, n_ev, x, myT, myH, myL);
-    };
-    // event n_ev: its step size (or escape sub-step size) and kind
-    auto push = [&](uint8_t kind, double hv) {
-        if (p.record == 1) {
-            if (n_ev >= rec.ev_cap) {
-                rec.bad = 1;
-            } else {
-                p.ev_h[rec.eo + n_ev] = hv;
-                p.ev_kind[rec.eo + n_ev] = kind;
-            }
-        } else if (p.record == 2) {
-            const uint32_t j = n_ev % rec.kc;
-            rec.hb[j] = hv;
-            rec.kb[j] = kind;
-        }
-        ++n_ev;
-    };
-    // this lane's whole state in FP64 (x, then tau and I per bin), and back
-    auto gather = [&](double* y) {
-        for (int i = 0; i < 8; ++i) y[i] = x[i];
-        for (int q = 0; q < N; ++q) {
-            y[8 + q] = (double)myT[q];
-            y[8 + N + q] = (double)myH[q] + (MIXED ? (double)myL[q] : 0.0);
-        }
-    };
-    // the carried slopes from an FP64 right-hand side f, and what they imply
-    auto take_slopes = [&](const double* f) {
-        for (int i = 0; i < 8; ++i) k1[i] = SR(f[i]);
-        bool nz = false;
-        for (int q = 0; q < N; ++q) {
-            myKT[q] = SR(f[8 + q]);
-            myKI[q] = SR(f[8 + N + q]);
-            nz |= myKT[q] != SR(0) || myKI[q] != SR(0);
-        }
-        spec_live = nz;
-    };
-
     for (;;) {
-        // ---------------- refill -----------------------------------------
-        const unsigned empty = __ballot_sync(kFull, !active);
-        if (empty && !dry) {
-            unsigned long long base = 0;
-            const unsigned n = __popc(empty);
-            if (lane == 0) base = atomicAdd(p.counter, (unsigned long long)n);
-            base = __shfl_sync(kFull, base, 0);
-            if ((long long)(base + n) >= p.total_rays) dry = true;
-            if (!active) {
-                loc = (long long)base + __popc(empty & ((1u << lane) - 1u));  // index in the ray subset (list)
-                if (loc < p.total_rays) {
-                    sub_id = p.ray_list ? (long long)p.ray_list[loc] : loc;
-                    id = p.ray0 + sub_id * p.ray_stride;  // pixel
-                    ++c_rays;
-                    pi = (int)(id % p.frame.xp);
-                    pj = (int)(id / p.frame.xp);
-                    camera_ray(p.frame, pi, pj, x);
-                    {
-                        double y[8 + 2 * kTorusMaxBins], f[8 + 2 * kTorusMaxBins];
-                        for (int i = 0; i < 8; ++i) y[i] = x[i];
-                        for (int i = 8; i < D; ++i) y[i] = 0;
-                        torus_f64<KEM>(p.m, y, f);
-                        for (int q = 0; q < N; ++q) {
-                            myT[q] = SR(0);
-                            myH[q] = SR(0);
-                            if constexpr (MIXED) myL[q] = SR(0);
-                        }
-                        take_slopes(f);
-                    }
-                    h = -torus_max_dt<EM, SR>(p, x);
-                    // where h came from: 0 the controller (held fixed by the adjoint),
-                    // 1 -pad_max_dt of the previous accepted step's start state, 2
-                    // -pad_max_dt of the current state
-                    hsrc = 2;
-                    prev_rej = false;
-                    nsteps = 0;
-                    n_ev = 0;
-                    escaped = false;  // a ray with a polar escape stores its state at every step
-                    tau_min = SR(0);
-                    if (p.record) torus_rec_begin(p, loc, sub_id, &rec);
-                    active = true;
-                }
+        const long long loc = (long long)atomicAdd(p.counter, 1ull);  // index in the ray subset (list)
+        if (loc >= p.total_rays) break;
+        const long long sub = p.ray_list ? (long long)p.ray_list[loc] : loc;
+        const long long id = p.ray0 + sub * p.ray_stride;              // pixel
+        ++c_rays;
+        const int pi = (int)(id % p.frame.xp), pj = (int)(id / p.frame.xp);
+        double x[9];
+        camera_ray(p.frame, pi, pj, x);
+        SR tau[kTorusMaxBins], ihi[kTorusMaxBins], ilo[kTorusMaxBins], kt1[kTorusMaxBins], ki1[kTorusMaxBins];
+        SR k1[8];
+        {
+            double y[8 + 2 * kTorusMaxBins], f[8 + 2 * kTorusMaxBins];
+            for (int i = 0; i < 8; ++i) y[i] = x[i];
+            for (int i = 8; i < D; ++i) y[i] = 0;
+            torus_f64<KEM>(p.m, y, f);
+            for (int i = 0; i < 8; ++i) k1[i] = SR(f[i]);
+            for (int c = 0; c < N; ++c) {
+                tau[c] = 0; ihi[c] = 0; ilo[c] = 0;
+                kt1[c] = SR(f[8 + c]);
+                ki1[c] = SR(f[8 + N + c]);
             }
         }
-        if (!__ballot_sync(kFull, active)) break;
-        __syncwarp();
-
-        // ---------------- escape and geodesic stages (one lane per ray) ---
-        bool done = false, decided = false, accept = false, need = false;
-        double max_dt = 0, hnext = h, err2 = 0;
-        double y[8];
-        TorusStages<SR> st;
-        if (active) {
+        double h = -torus_max_dt<EM, SR>(p, x);
+        // where h came from: 0 the controller (held fixed by the adjoint),
+        // 1 -pad_max_dt of the previous accepted step's start state, 2 -pad_max_dt
+        // of the current state
+        uint8_t hsrc = 2;
+        const double tol = p.frame.tol;
+        bool prev_rej = false;
+        long long nsteps = 0;
+        uint32_t n_ev = 0;
+        bool escaped = false;  // a ray with a polar escape stores its state at every step
+        TorusRec rec;
+        if (p.record) torus_rec_begin(p, loc, sub, &rec);
+        // the state before event n_ev when it starts a segment (recording)
+        auto checkpoint = [&]() {
+            if (p.record && (n_ev % rec.kc) == 0u) torus_rec_checkpoint<SR, MIXED>(p, &rec, n_ev, x, tau, ihi, ilo);
+        };
+        // event n_ev: its step size (or escape sub-step size) and kind
+        auto push = [&](uint8_t kind, double hv) {
+            if (p.record == 1) {
+                if (n_ev >= rec.ev_cap) {
+                    rec.bad = 1;
+                } else {
+                    p.ev_h[rec.eo + n_ev] = hv;
+                    p.ev_kind[rec.eo + n_ev] = kind;
+                }
+            } else if (p.record == 2) {
+                const uint32_t j = n_ev % rec.kc;
+                rec.hb[j] = hv;
+                rec.kb[j] = kind;
+            }
+            ++n_ev;
+        };
+        int cls = 0;
+        for (;;) {
             ++c_att;
-            max_dt = torus_max_dt<EM, SR>(p, x);
+            const double max_dt = torus_max_dt<EM, SR>(p, x);
             double temp;
+            bool done = false;
             if (torus_near_singularity<EM>(x, h, tol, &temp)) {
                 // polar escape (integrators_LttM.jl:62-105) in FP64 on the full state
                 checkpoint();
-                double yy[8 + 2 * kTorusMaxBins], f[8 + 2 * kTorusMaxBins];
-                gather(yy);
-                for (int i = 0; i < 8; ++i) f[i] = (double)k1[i];
+                double y[8 + 2 * kTorusMaxBins], f[8 + 2 * kTorusMaxBins];
+                for (int i = 0; i < 8; ++i) {
+                    y[i] = x[i];
+                    f[i] = (double)k1[i];
+                }
                 for (int q = 0; q < N; ++q) {
-                    f[8 + q] = (double)myKT[q];
-                    f[8 + N + q] = (double)myKI[q];
+                    y[8 + q] = (double)tau[q];
+                    y[8 + N + q] = (double)ihi[q] + (MIXED ? (double)ilo[q] : 0.0);
+                    f[8 + q] = (double)kt1[q];
+                    f[8 + N + q] = (double)ki1[q];
                 }
                 int nsub = 0;
                 for (int it = 0; it < 37; ++it) {
                     if (it > 0) {
-                        if (torus_terminate<double, EM>(p, yy, yy + 8, N)) continue;
-                        torus_f64<KEM>(p.m, yy, f);
+                        if (torus_terminate<double, EM>(p, y, y + 8, N)) continue;
+                        torus_f64<KEM>(p.m, y, f);
                     }
-                    for (int i = 0; i < D; ++i) yy[i] -= temp * f[i];
-                    torus_keep(yy);
+                    for (int i = 0; i < D; ++i) y[i] -= temp * f[i];
+                    torus_keep(y);
                     ++nsub;
                 }
                 c_esc += nsub;
                 escaped = true;
                 push((uint8_t)(1 + nsub), temp);
-                for (int i = 0; i < 8; ++i) x[i] = yy[i];
-                SR tm = SR(0);
+                for (int i = 0; i < 8; ++i) x[i] = y[i];
                 for (int q = 0; q < N; ++q) {
-                    myT[q] = SR(yy[8 + q]);
-                    myH[q] = SR(yy[8 + N + q]);
-                    if constexpr (MIXED) myL[q] = SR(yy[8 + N + q] - (double)myH[q]);
-                    tm = q == 0 ? myT[q] : rmin_(tm, myT[q]);
+                    tau[q] = SR(y[8 + q]);
+                    ihi[q] = SR(y[8 + N + q]);
+                    ilo[q] = MIXED ? SR(y[8 + N + q] - (double)ihi[q]) : SR(0);
                 }
-                tau_min = tm;
-                if (torus_terminate<double, EM>(p, yy, yy + 8, N)) {
+                if (torus_terminate<double, EM>(p, y, y + 8, N)) {
                     done = true;
-                    decided = true;
-                    accept = true;
-                    hnext = h;
+                    prev_rej = false;
                 } else {
-                    torus_f64<KEM>(p.m, yy, f);
-                    take_slopes(f);
+                    torus_f64<KEM>(p.m, y, f);
+                    for (int i = 0; i < 8; ++i) k1[i] = SR(f[i]);
+                    for (int q = 0; q < N; ++q) {
+                        kt1[q] = SR(f[8 + q]);
+                        ki1[q] = SR(f[8 + N + q]);
+                    }
                     h = -torus_max_dt<EM, SR>(p, x);
                     hsrc = 2;
-                    hnext = h;
                 }
             }
             if (!done) {
+                // geodesic stages
+                TorusStages<SR> st;
                 bool promote = false;
                 if (MIXED && EM == 3)  // the wormhole: the poles only (no horizon)
                     promote = (x[2] < p.promote_theta) || (x[2] > kPi - p.promote_theta);
@@ -1004,160 +899,101 @@ __global__ void __launch_bounds__(128, MIXED ? 3 : 2) torus_forward(const TorusK
                 } else {
                     torus_geo_stages<SR, SR, EM>(p.m, x, k1, h, st);
                 }
+                double y[8];
+                double err2 = 0;
                 for (int i = 0; i < 8; ++i) {
                     y[i] = x[i] + h * st.ns[i];
                     const double d = h * st.es[i];
                     const double tl = tol + fmax(fabs(x[i]), fabs(y[i])) * tol;
                     err2 += (d / tl) * (d / tl);
                 }
-                bool any_on = false;
-                for (int s = 1; s < 7; ++s) {
-                    s_pt[wib][s - 1][0][lane] = st.S[s].cj;
-                    s_pt[wib][s - 1][1][lane] = st.S[s].nus;
-                    s_pt[wib][s - 1][2][lane] = st.S[s].th;
-                    s_pt[wib][s - 1][3][lane] = st.S[s].g;
-                    s_on[wib][s - 1][lane] = (unsigned char)((st.S[s].on ? 1 : 0) | (st.S[s].zone << 1));
-                    any_on |= st.S[s].on;
-                }
-                need = any_on || spec_live;
-            }
-        }
-        __syncwarp();
-
-        // ---------------- spectral passes (warp-cooperative) -------------
-        unsigned nm = __ballot_sync(kFull, need);
-        while (nm) {
-            const unsigned pass_rays = nm;
-            // this group's ray: the (grp+1)-th set bit of nm
-            unsigned mg = nm;
-            for (int g = 0; g < grp; ++g) mg &= mg - 1u;
-            const bool vg = mg != 0u;
-            const int r = vg ? __ffs(mg) - 1 : __ffs(nm) - 1;  // an empty group repeats the first ray, discarded
-            for (int g = 0; g < G && nm; ++g) nm &= nm - 1u;
-            const SR hs = SR(__shfl_sync(kFull, h, r));
-            const SR ts = SR(tol);
-            const int c = bin_ok ? sub : 0;
-            SR c_t = 0, c_h = 0, c_l = 0, c_kt = 0, c_ki = 0, e_c = 0;
-            {
-                SR kt[7], ki[7];
-                kt[0] = rKT[r * kR + c];
-                ki[0] = rKI[r * kR + c];
-                const SR t0 = rT[r * kR + c];
-                const SR i0 = rH[r * kR + c];
-                SR tp = t0;
+                // bins: seven tau / I stages each
+                SR c_t[kTorusMaxBins], c_h[kTorusMaxBins], c_l[kTorusMaxBins], c_kt[kTorusMaxBins],
+                    c_ki[kTorusMaxBins];
+                const SR hs = SR(h), ts = SR(tol);
+                SR ebins = 0;
+                for (int c = 0; c < N; ++c) {
+                    SR kt[7], ki[7];
+                    kt[0] = kt1[c];
+                    ki[0] = ki1[c];
+                    const SR t0 = tau[c];
+                    SR tp = t0;
 #pragma unroll
-                for (int s = 1; s < 7; ++s) {
-                    SR a = 0;
+                    for (int s = 1; s < 7; ++s) {
+                        SR a = 0;
 #pragma unroll
-                    for (int j = 0; j < s; ++j) a += SR(tA(s, j)) * kt[j];
-                    tp = t0 + hs * a;
-                    SR ft = 0, fi = 0;
-                    const unsigned char on = s_on[wib][s - 1][r];
-                    if (on & 1) {
-                        TorusPt<SR> P;
-                        P.cj = s_pt[wib][s - 1][0][r];
-                        P.nus = s_pt[wib][s - 1][1][r];
-                        P.th = s_pt[wib][s - 1][2][r];
-                        P.g = s_pt[wib][s - 1][3][r];
-                        P.on = true;
-                        P.zone = on >> 1;
-                        em_bin<SR, EM>(p.m, P, c, ft, fi);
+                        for (int j = 0; j < s; ++j) a += SR(tA(s, j)) * kt[j];
+                        tp = t0 + hs * a;
+                        SR ft = 0, fi = 0;
+                        if (st.S[s].on) em_bin<SR, EM>(p.m, st.S[s], c, ft, fi);
+                        kt[s] = ft;
+                        ki[s] = fi * texp(-tp);
                     }
-                    kt[s] = ft;
-                    ki[s] = fi * texp(-tp);
-                }
-                // tp is now the new tau (row 6 of A is b)
-                SR nsI = 0, nsT = 0, et = 0, ei = 0;
+                    // tp is now the new tau (row 6 of A is b)
+                    SR nsI = 0, nsT = 0, et = 0, ei = 0;
 #pragma unroll
-                for (int j = 0; j < 7; ++j) {
-                    if (j < 6) {
-                        nsI += SR(tA(6, j)) * ki[j];
-                        nsT += SR(tA(6, j)) * kt[j];
+                    for (int j = 0; j < 7; ++j) {
+                        if (j < 6) {
+                            nsI += SR(tA(6, j)) * ki[j];
+                            nsT += SR(tA(6, j)) * kt[j];
+                        }
+                        et += SR(tE(j)) * kt[j];
+                        ei += SR(tE(j)) * ki[j];
                     }
-                    et += SR(tE(j)) * kt[j];
-                    ei += SR(tE(j)) * ki[j];
+                    SR yh = ihi[c], yl = MIXED ? ilo[c] : SR(0);
+                    if constexpr (MIXED) {
+                        kahan_add(yh, yl, hs * nsI);
+                    } else {
+                        yh = yh + hs * nsI;
+                    }
+                    const SR i0 = ihi[c];
+                    const SR dt_ = hs * et, di = hs * ei;
+                    const SR tlt = ts + rmax(rabs(t0), rabs(tp)) * ts;
+                    const SR tli = ts + rmax(rabs(i0), rabs(yh)) * ts;
+                    ebins += (dt_ / tlt) * (dt_ / tlt) + (di / tli) * (di / tli);
+                    c_t[c] = tp;
+                    c_h[c] = yh;
+                    c_l[c] = yl;
+                    // slopes carried to the next attempt: k7 (FSAL) or the
+                    // reference's sum b_i k_i
+                    c_kt[c] = p.fsal ? kt[6] : nsT;
+                    c_ki[c] = p.fsal ? ki[6] : nsI;
                 }
-                SR yh = i0, yl = MIXED ? rL[r * kR + c] : SR(0);
-                if constexpr (MIXED) {
-                    kahan_add(yh, yl, hs * nsI);
-                } else {
-                    yh = yh + hs * nsI;
-                }
-                const SR dt_ = hs * et, di = hs * ei;
-                const SR tlt = ts + rmax(rabs(t0), rabs(tp)) * ts;
-                const SR tli = ts + rmax(rabs(i0), rabs(yh)) * ts;
-                e_c = bin_ok ? (dt_ / tlt) * (dt_ / tlt) + (di / tli) * (di / tli) : SR(0);
-                c_t = tp;
-                c_h = yh;
-                c_l = yl;
-                // slopes carried to the next attempt: k7 (FSAL) or the
-                // reference's sum b_i k_i
-                c_kt = p.fsal ? kt[6] : nsT;
-                c_ki = p.fsal ? ki[6] : nsI;
-            }
-            // the group's error sum and least optical depth, in one
-            // association order, in every lane of the group
-            SR esum = e_c, tmin = bin_ok ? c_t : SR(3.0e38);
-            for (int o = L / 2; o > 0; o >>= 1) {
-                esum += __shfl_xor_sync(kFull, esum, o);
-                tmin = rmin_(tmin, __shfl_xor_sync(kFull, tmin, o));
-            }
-            esum = __shfl_sync(kFull, esum, grp * L);
-            tmin = __shfl_sync(kFull, tmin, grp * L);
-            // the lane that owns a ray of this pass decides its attempt
-            const int rank = __popc(pass_rays & ((1u << lane) - 1u));
-            const bool own = ((pass_rays >> lane) & 1u) && rank < G;
-            const SR e_own = __shfl_sync(kFull, esum, own ? rank * L : 0);
-            const SR t_own = __shfl_sync(kFull, tmin, own ? rank * L : 0);
-            int dec = 0;
-            if (own) {
-                decide<double>(err2 + (double)e_own, D, h, max_dt, prev_rej, accept, hnext);
-                decided = true;
-                dec = accept ? 1 : 0;
-                if (accept) {
-                    checkpoint();  // the state before the step: the rows are written below
-                    tau_min = t_own;
-                }
-            }
-            __syncwarp();
-            const int dsrc = __shfl_sync(kFull, dec, r);
-            if (vg && dsrc && bin_ok) {
-                rT[r * kR + c] = c_t;
-                rH[r * kR + c] = c_h;
-                if constexpr (MIXED) rL[r * kR + c] = c_l;
-                rKT[r * kR + c] = c_kt;
-                rKI[r * kR + c] = c_ki;
-            }
-            const unsigned nzb = __ballot_sync(kFull, vg && bin_ok && (c_kt != SR(0) || c_ki != SR(0)));
-            const unsigned gmask = L == 32 ? kFull : ((1u << L) - 1u);
-            if (own && dec) spec_live = ((nzb >> (rank * L)) & gmask) != 0u;
-            __syncwarp();
-        }
-
-        // ---------------- controller, commit, termination ----------------
-        int cls = 0;
-        if (active) {
-            if (!done) {
-                if (!decided) {
-                    // no bin work: the bins' error is 0 and they stay as they are
-                    decide<double>(err2, D, h, max_dt, prev_rej, accept, hnext);
-                    if (accept) checkpoint();
-                }
+                err2 += (double)ebins;
+                bool accept;
+                double hnext;
+                decide<double>(err2, D, h, max_dt, prev_rej, accept, hnext);
                 const uint8_t next_src = hnext == -max_dt ? (accept ? 1 : 2) : 0;
                 if (accept) {
+                    checkpoint();
                     push(hsrc ? (uint8_t)(0x40 | hsrc) : (uint8_t)0, h);
                     for (int i = 0; i < 8; ++i) {
                         x[i] = y[i];
                         k1[i] = p.fsal ? st.k7[i] : SR(st.ns[i]);
+                    }
+                    for (int c = 0; c < N; ++c) {
+                        tau[c] = c_t[c];
+                        ihi[c] = c_h[c];
+                        ilo[c] = c_l[c];
+                        kt1[c] = c_kt[c];
+                        ki1[c] = c_ki[c];
                     }
                     if (!FLAT && torus_keep(x) && p.fsal) {
                         // reflected through the pole: the carried slope belongs to
                         // the unreflected point, so take f at the new state (FSAL;
                         // the reference's step keeps its carried sum)
                         double yy[8 + 2 * kTorusMaxBins], ff[8 + 2 * kTorusMaxBins];
-                        gather(yy);
+                        for (int i = 0; i < 8; ++i) yy[i] = x[i];
+                        for (int q = 0; q < N; ++q) {
+                            yy[8 + q] = (double)tau[q];
+                            yy[8 + N + q] = (double)ihi[q] + (MIXED ? (double)ilo[q] : 0.0);
+                        }
                         torus_f64<KEM>(p.m, yy, ff);
-                        take_slopes(ff);
+                        for (int i = 0; i < 8; ++i) k1[i] = SR(ff[i]);
+                        for (int q = 0; q < N; ++q) {
+                            kt1[q] = SR(ff[8 + q]);
+                            ki1[q] = SR(ff[8 + N + q]);
+                        }
                     }
                     prev_rej = false;
                 } else {
@@ -1167,59 +1003,52 @@ __global__ void __launch_bounds__(128, MIXED ? 3 : 2) torus_forward(const TorusK
                 }
                 h = hnext;
                 hsrc = next_src;
-            } else {
-                prev_rej = false;
             }
             ++nsteps;
             if (nsteps >= p.frame.max_steps) cls = RTW_CLASS_MAXSTEPS;
-            else cls = torus_terminate_min<SR, EM>(p, x, tau_min);
+            else cls = torus_terminate<SR, EM>(p, x, tau, N);
+            if (cls) break;
         }
-
-        // ---------------- a finished ray: epilogue, outputs --------------
-        if (active && cls) {
-            bool fin = true;
-            for (int i = 0; i < 8; ++i) fin &= isfinite(x[i]);
-            if (!fin) {
-                cls = RTW_CLASS_NAN;
-                ++c_nan;
-            }
-            if constexpr (EM == 3 || EM == 4) {
-                if (fin && (p.sky[0] || p.sky[1])) {
-                    double I[kTorusMaxBins], tv[kTorusMaxBins];
-                    for (int q = 0; q < N; ++q) {
-                        I[q] = (double)myH[q] + (MIXED ? (double)myL[q] : 0.0);
-                        tv[q] = (double)myT[q];
-                    }
-                    wormhole_skybox<EM>(p, x, N, I, tv, pi, pj);
-                    for (int q = 0; q < N; ++q) {
-                        myH[q] = SR(I[q]);
-                        if constexpr (MIXED) myL[q] = SR(I[q] - (double)myH[q]);
-                    }
-                }
-            }
-            if (p.spectrum || p.xyz) {
-                double X = 0, Y = 0, Z = 0;
-                for (int q = 0; q < N; ++q) {
-                    const double I = (double)myH[q] + (MIXED ? (double)myL[q] : 0.0);
-                    if (p.spectrum) p.spectrum[id * N + q] = (float)I;
-                    X += I * p.m.bins[q].fx;
-                    Y += I * p.m.bins[q].fy;
-                    Z += I * p.m.bins[q].fz;
-                }
-                if (p.xyz) {
-                    p.xyz[3 * id + 0] = (float)X;
-                    p.xyz[3 * id + 1] = (float)Y;
-                    p.xyz[3 * id + 2] = (float)Z;
-                }
-            }
-            if (p.cls) p.cls[id] = (uint8_t)cls;
-            if (p.steps) p.steps[id] = (uint32_t)nsteps;
-            if (p.final_state)
-                for (int i = 0; i < 8; ++i) p.final_state[8 * id + i] = x[i];
-            if (p.record) torus_rec_end<SR, MIXED>(p, &rec, loc, sub_id, n_ev, escaped, x, myT, myH, myL);
-            active = false;
+        bool fin = true;
+        for (int i = 0; i < 8; ++i) fin &= isfinite(x[i]);
+        if (!fin) {
+            cls = RTW_CLASS_NAN;
+            ++c_nan;
         }
-        __syncwarp();
+        if constexpr (EM == 3 || EM == 4) {
+            if (fin && (p.sky[0] || p.sky[1])) {
+                double I[kTorusMaxBins], tv[kTorusMaxBins];
+                for (int c = 0; c < N; ++c) {
+                    I[c] = (double)ihi[c] + (MIXED ? (double)ilo[c] : 0.0);
+                    tv[c] = (double)tau[c];
+                }
+                wormhole_skybox<EM>(p, x, N, I, tv, pi, pj);
+                for (int c = 0; c < N; ++c) {
+                    ihi[c] = SR(I[c]);
+                    ilo[c] = MIXED ? SR(I[c] - (double)ihi[c]) : SR(0);
+                }
+            }
+        }
+        if (p.spectrum || p.xyz) {
+            double X = 0, Y = 0, Z = 0;
+            for (int c = 0; c < N; ++c) {
+                const double I = (double)ihi[c] + (MIXED ? (double)ilo[c] : 0.0);
+                if (p.spectrum) p.spectrum[id * N + c] = (float)I;
+                X += I * p.m.bins[c].fx;
+                Y += I * p.m.bins[c].fy;
+                Z += I * p.m.bins[c].fz;
+            }
+            if (p.xyz) {
+                p.xyz[3 * id + 0] = (float)X;
+                p.xyz[3 * id + 1] = (float)Y;
+                p.xyz[3 * id + 2] = (float)Z;
+            }
+        }
+        if (p.cls) p.cls[id] = (uint8_t)cls;
+        if (p.steps) p.steps[id] = (uint32_t)nsteps;
+        if (p.final_state)
+            for (int i = 0; i < 8; ++i) p.final_state[8 * id + i] = x[i];
+        if (p.record) torus_rec_end<SR, MIXED>(p, &rec, loc, sub, n_ev, escaped, x, tau, ihi, ilo);
     }
     atomicAdd(&p.stats->step_attempts, (unsigned long long)c_att);
     atomicAdd(&p.stats->rejected_steps, (unsigned long long)c_rej);
@@ -1733,8 +1562,6 @@ struct TorusBuffers {
     size_t sky_cap = 0;
     void* gaunt = nullptr;  // the bremsstrahlung torus's Gaunt-factor table
     size_t gaunt_cap = 0;
-    void* spec = nullptr;   // the forward kernel's per-warp bin rows
-    size_t spec_cap = 0;
     void* fin = nullptr;   // final states
     size_t fin_cap = 0;
     void* tgt = nullptr;
@@ -1744,7 +1571,7 @@ struct TorusBuffers {
 void torus_free(TorusBuffers* b) {
     if (!b) return;
     for (void* q : {b->ctl, b->out, b->nev, b->evh, b->evk, b->ck, b->work, b->tgt, b->pool, b->pool2, b->fin, b->sky,
-                    b->gaunt, b->spec})
+                    b->gaunt})
         if (q) cudaFree(q);
     delete b;
 }
@@ -1989,11 +1816,6 @@ rtw_status torus_setup(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* c
     p.stats = (DevStats*)(ctl + 1);
     p.err_flag = (unsigned int*)(ctl + 32);
     run.grid = torus_grid(ctx, forward_fn(prm->precision == RTW_PREC_MIXED, p.m.emitter));
-    // the forward kernel's bin rows: per warp 5 (FP32-mixed) or 4 (FP64) fields of 32 x 32
-    const size_t row_bytes = prm->precision == RTW_PREC_MIXED ? 5 * 32 * kTorusMaxBins * sizeof(float)
-                                                              : 4 * 32 * kTorusMaxBins * sizeof(double);
-    if ((st = ensure(ctx, &b->spec, &b->spec_cap, (size_t)run.grid * 4 * row_bytes)) != RTW_OK) return st;
-    p.spec = b->spec;
     return RTW_OK;
 }
 

@@ -53,8 +53,8 @@ constexpr int kSpecGroups = 32 / kSpecLanes;
 // FP32-mixed with up to 64 bins: the intensity and carried-slope rows of the
 // spectral phase live in shared memory (2 x 32 x np floats per warp, dynamic);
 // the Kahan low parts, which the error reduction does not wait for, stay in the
-// global scratch. RTW_SPEC_SHARED (rtw_internal.h) 0 keeps every row in global
-// memory.
+// global scratch. RTW_SPEC_SHARED (rtw_internal.h, 0 by default: measured
+// slower) 0 keeps every row in global memory.
 template <bool MIXED, int BPL>
 RTW_HD constexpr bool spec_in_shared() { return RTW_SPEC_SHARED && MIXED && BPL <= 2; }
 
@@ -155,9 +155,6 @@ __device__ __forceinline__ float rabs(float v) { return fabsf(v); }
 __device__ __forceinline__ double rabs(double v) { return fabs(v); }
 __device__ __forceinline__ float rmax(float a, float b) { return fmaxf(a, b); }
 __device__ __forceinline__ double rmax(double a, double b) { return fmax(a, b); }
-// the smaller of two values; a NaN argument gives the other
-__device__ __forceinline__ float rmin_(float a, float b) { return fminf(a, b); }
-__device__ __forceinline__ double rmin_(double a, double b) { return fmin(a, b); }
 
 // Compensated (TwoSum) add into hi/lo.
 __device__ __forceinline__ void kahan_add(float& hi, float& lo, float t) {

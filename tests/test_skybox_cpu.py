@@ -150,3 +150,66 @@ def test_oracle_cart_sphere_closed_form(oracle):
     sky = (s["spectrum"] - r["spectrum"]) / np.exp(-r["tau"])
     np.testing.assert_allclose(sky, np.repeat(sky[:1], len(sky), 0), rtol=1e-9)  # one colour, k^t = 1
     assert np.all(sky > 0)
+
+
+def _hand_skybox(sky, h, state, freq_nm, tau):
+    """The skybox term of a ray of the Cartesian sphere, written from the
+    reference's functions by hand (Minkowski_Sphere_Cartesian.source/
+    source_model.jl:175-188, 191-280, 406-424; gen_geometry.jl:347-370;
+    my_special_functions.jl:20-22): face of the largest |direction|
+    component, (u, v) on it, the texel (i, j), its place in the cross layout,
+    the map's row 3h + 1 - j, and three Gaussian lines per texel colour."""
+    v = np.asarray(state[4:8], dtype=np.float64)
+    n = np.sqrt(v[1] ** 2 + v[2] ** 2 + v[3] ** 2)
+    x, y, z = v[1] / n, v[2] / n, v[3] / n
+    if abs(x) >= abs(y) and abs(x) >= abs(z):
+        face = 1 if x > 0 else 3
+    elif abs(y) >= abs(x) and abs(y) >= abs(z):
+        face = 4 if y > 0 else 2
+    else:
+        face = 6 if z > 0 else 5
+    if face == 1:
+        u, w = -y / abs(x), z / abs(x)
+    elif face == 2:
+        u, w = -x / abs(y), z / abs(y)
+    elif face == 3:
+        u, w = y / abs(x), z / abs(x)
+    elif face == 4:
+        u, w = x / abs(y), z / abs(y)
+    elif face == 5:
+        u, w = -x / abs(z), -y / abs(z)
+    else:
+        u, w = -x / abs(z), y / abs(z)
+    i = min(int(np.floor(h * (u + 1) / 2)) + 1, h)
+    j = min(int(np.floor(h * (w + 1) / 2)) + 1, h)
+    di, dj = {1: (0, h), 2: (h, h), 3: (2 * h, h), 4: (3 * h, h), 5: (h, 0), 6: (h, 2 * h)}[face]
+    ia, ja = i + di, j + dj
+    rgb = sky[3 * h + 1 - ja - 1, ia - 1].astype(np.float64)
+
+    def ng(f, s, m):
+        return np.exp(-(f - m) ** 2 / (2 * s * s)) / (s * np.sqrt(2 * np.pi))
+
+    f = np.asarray(freq_nm) * v[0]  # freq_shift = -[1,0,0,0] g v = v^t in flat space
+    I = 1e-12 * (1.0 * rgb[0] * ng(f, 5e-5, 0.001587) + 0.843 * rgb[1] * ng(f, 7e-5, 0.001879)
+                 + 0.914 * rgb[2] * ng(f, 9e-5, 0.002141))
+    return I * np.exp(-np.asarray(tau)) / f ** 3
+
+
+def test_cart_sphere_skybox_against_hand_computation(oracle):
+    """Pins the skybox lookup independently of the oracle's code (the skybox
+    golden fixtures pin it only against itself): for every ray of the
+    Cartesian sphere that misses the sphere (a straight line, tau = 0), the
+    oracle's spectrum equals the hand computation of the texel its final
+    direction points at, on a map whose every texel has its own colour."""
+    h = 8
+    rng = np.random.default_rng(21)
+    sky = rng.uniform(0.05, 1.0, (3 * h, 4 * h, 3)).astype(np.float32)
+    col = np.array([467.0, 532.0, 630.0])
+    cam = configs.cart_sphere_camera(24, 1e-6)
+    r = oracle.render(configs.cart_sphere_scene(), cam, col, integrator=abi.DP45_FSAL, skybox=(sky, None),
+                      want=("spectrum", "state", "tau", "class"))
+    miss = np.all(r["tau"] == 0, axis=1) & (r["class"] == abi.CLASS_ESCAPE)
+    assert miss.sum() > 100
+    for q in np.flatnonzero(miss):
+        want = _hand_skybox(sky, h, r["state"][q], 1.0 / col, r["tau"][q])
+        assert np.allclose(r["spectrum"][q], want, rtol=1e-12, atol=0), (q, r["spectrum"][q], want)
