@@ -283,8 +283,10 @@ def op_model(renderer, scene_kind, stats, n_bins):
 
 
 # DRAM bytes per step attempt of the FP32-mixed Kerr trace kernel (local-memory
-# spill traffic; the outputs are 17 B per ray), from one ncu capture at 512^2
-TRAFFIC_B_PER_ATTEMPT = 3.2103e9 / 357226998
+# write-back; the outputs are 17 B per ray), from one ncu capture at 512^2: the
+# main launch's dram__bytes_read+write (0.0516 + 0.7491 GB) over the render's
+# step attempts (the tail launch, 9 % of that render's time, returned no counters)
+TRAFFIC_B_PER_ATTEMPT = 0.8007e9 / 357227612
 
 
 def batched_leg(r, world, rank, stream, barrier_fn):
@@ -629,6 +631,7 @@ def run_b200(args):
         torch.cuda.synchronize()
         total = 0.0
         kernel = 0.0
+        launches = 0
         st = None
         for _ in range(k):
             flush.fill_(1.0)  # evict L2 between timed renders
@@ -641,8 +644,10 @@ def run_b200(args):
             total += e0.elapsed_time(e1)
             st = r.stats()
             kernel += st["kernel_ms"]
+            launches += st["launches"]
         torch.cuda.synchronize()
         barrier(world)
+        st = dict(st, launches_total=launches)
         return total, kernel, st
 
     peaks = r.measure_peaks() if rank == 0 else None
@@ -789,7 +794,7 @@ def run_b200(args):
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
             "scaling": "strong" if args.strong else "weak",
             "vs_baseline": None, "dtype": "f32+f64" if prec == abi.PREC_MIXED else "f64", "data": "synthetic",
-            "gpu_launches": args.steps,
+            "gpu_launches": st["launches_total"],
             "config": {"workload": f"{args.workload} {cam.x_pix}x{cam.y_pix}, 64 bins, tol {cam.tolerance:g}, "
                                    f"{'FP32-mixed' if prec == abi.PREC_MIXED else 'FP64'}, reference step",
                        "rays_per_gpu": P // world if args.strong else P,

@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define RTW_ABI_VERSION 6
+#define RTW_ABI_VERSION 7
 /* Largest number of spectral bins (reference `colors`) one render takes. */
 #define RTW_MAX_BINS 128
 /* Largest number of frames (cameras) one batched render takes. */
@@ -329,6 +329,10 @@ typedef struct rtw_stats {
     int32_t graph_replayed;     /* 1: the render replayed a captured graph */
     uint64_t tail_rays;         /* FP32-mixed trace kernel: rays finished by the
                                    FP64 tail pass */
+    int32_t launches;           /* this library's kernel launches in the last
+                                   render call (2 for an FP32-mixed trace render
+                                   with its tail pass) */
+    int32_t reserved0;
 } rtw_stats;
 
 /* Algorithmic operation counts of the trace kernel's arithmetic for one scene

@@ -15,7 +15,7 @@ PKG = Path(__file__).resolve().parent
 # RTW_LIB_PATH selects another build of the same library (e.g. a tuning variant)
 LIB_PATH = Path(os.environ.get("RTW_LIB_PATH", PKG / "librtw_b200.so"))
 
-ABI_VERSION = 6
+ABI_VERSION = 7
 MAX_BINS = 128
 MAX_FRAMES = 4096
 TRACE_FIELDS = 15
@@ -124,7 +124,7 @@ class Stats(C.Structure):
         ("escape_substeps", C.c_uint64), ("nan_rays", C.c_uint64),
         ("kernel_ms", C.c_double), ("total_ms", C.c_double), ("phase_cycles", C.c_uint64 * 4),
         ("grid", C.c_int32), ("block_warps", C.c_int32), ("refill_min", C.c_int32), ("graph_replayed", C.c_int32),
-        ("tail_rays", C.c_uint64),
+        ("tail_rays", C.c_uint64), ("launches", C.c_int32), ("reserved0", C.c_int32),
     ]
 
 

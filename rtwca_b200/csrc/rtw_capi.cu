@@ -874,6 +874,7 @@ rtw_status rtw_render(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* ca
     ctx->last_warps = warps;
     ctx->last_refill = refill;
     ctx->last_replayed = replayed;
+    ctx->last_launches = use_tail ? 2 : 1;
     if (!prm->stream) {
         RTW_CUDA(cudaStreamSynchronize(st), "trace kernel");
     }
@@ -909,6 +910,8 @@ rtw_status rtw_get_stats(rtw_ctx* ctx, rtw_stats* out) {
     out->refill_min = ctx->last_refill;
     out->graph_replayed = ctx->last_replayed;
     out->tail_rays = std::min<unsigned long long>(ds.tail_rays, (unsigned long long)ctx->last_tail_cap);
+    out->launches = ctx->last_launches;
+    out->reserved0 = 0;
     return RTW_OK;
 }
 

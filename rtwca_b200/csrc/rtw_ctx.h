@@ -46,7 +46,7 @@ struct rtw_ctx {
     std::vector<unsigned char> gkey;
     void* h_stage = nullptr;
     size_t stage_cap = 0;
-    int last_grid = 0, last_warps = 0, last_refill = 0, last_replayed = 0;
+    int last_grid = 0, last_warps = 0, last_refill = 0, last_replayed = 0, last_launches = 0;
     // synchrotron torus renders and adjoints (rtw_torus.cu)
     TorusBuffers* torus = nullptr;
     std::string err;

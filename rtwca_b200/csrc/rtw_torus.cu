@@ -1915,6 +1915,8 @@ rtw_status torus_render(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* 
     ctx->last_warps = 4;
     ctx->last_refill = 1;
     ctx->last_replayed = 0;
+    ctx->last_launches = 1;
+    ctx->last_tail_cap = 0;
     if (!prm->stream) RTW_CUDA(cudaStreamSynchronize(s), "torus kernel");
     return RTW_OK;
 }

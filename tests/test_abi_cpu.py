@@ -32,7 +32,7 @@ def test_every_declared_symbol_is_exported(rtwlib):
 
 
 def test_abi_version(rtwlib):
-    assert rtwlib.rtw_abi_version() == abi.ABI_VERSION == 6
+    assert rtwlib.rtw_abi_version() == abi.ABI_VERSION == 7
 
 
 STRUCTS = {

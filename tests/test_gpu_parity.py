@@ -234,6 +234,7 @@ def test_tail_pass_is_bit_identical(renderer, name, integ):
     sb = renderer.stats()
     print(name, "tail rays", sa["tail_rays"], "of", sa["rays"])
     assert sa["tail_rays"] > 0 and sb["tail_rays"] == 0
+    assert sa["launches"] == 2 and sb["launches"] == 1  # main pass + tail pass
     for k in ("xyz", "class", "steps", "spectrum", "state", "tau"):
         assert np.array_equal(a[k], b[k]), k
     for k in ("step_attempts", "rejected_steps", "promoted_steps", "spectral_steps", "rays"):
