@@ -71,7 +71,7 @@ static_assert(sizeof(NoallocTables) <= 32000, "upload tables exceed the kernel-p
 
 // One CTA: copies the tables into the arrays and zeroes the work counter and
 // the counters.
-__global__ void __launch_bounds__(256) noalloc_upload(const NoallocTables t) {
+__global__ void __launch_bounds__(256) noalloc_upload(__grid_constant__ const NoallocTables t) {
     const int i = threadIdx.x;
     if (i < t.n_frames) g_noalloc_frames[i] = t.frames[i];
     for (int k = i; k < 4 * RTW_MAX_BINS; k += blockDim.x) g_noalloc_bins[k] = t.bins[k];

@@ -750,7 +750,7 @@ __device__ __noinline__ void torus_rec_end(const TorusKP& p, TorusRec* r, long l
 // (FP32-mixed: 3 CTAs/SM, 168 registers, measured 7-13 % faster than 2 CTAs at
 // 255; FP64 stays at 2, where 3 was 8-20 % slower)
 template <bool MIXED, int EM>
-__global__ void __launch_bounds__(128, MIXED ? 3 : 2) torus_forward(const TorusKP p) {
+__global__ void __launch_bounds__(128, MIXED ? 3 : 2) torus_forward(__grid_constant__ const TorusKP p) {
     constexpr bool FLAT = EM == 2 || EM == 4;  // Synchro_Test, the sphere: flat Cartesian geometry
     // the FP64 slope at a ray's start and after escapes: the instance's own
     // emitter on the mixed path (ptxas: the torus, Powehi and wormhole
@@ -899,6 +899,9 @@ __global__ void __launch_bounds__(128, MIXED ? 3 : 2) torus_forward(const TorusK
                 } else {
                     torus_geo_stages<SR, SR, EM>(p.m, x, k1, h, st);
                 }
+                if constexpr (MIXED && EM == 0)
+                    for (int s = 1; s < 7; ++s)
+                        if (st.S[s].on) torus_bin_stage<SR>(st.S[s]);
                 double y[8];
                 double err2 = 0;
                 for (int i = 0; i < 8; ++i) {
@@ -925,7 +928,12 @@ __global__ void __launch_bounds__(128, MIXED ? 3 : 2) torus_forward(const TorusK
                         for (int j = 0; j < s; ++j) a += SR(tA(s, j)) * kt[j];
                         tp = t0 + hs * a;
                         SR ft = 0, fi = 0;
-                        if (st.S[s].on) em_bin<SR, EM>(p.m, st.S[s], c, ft, fi);
+                        if (st.S[s].on) {
+                            if constexpr (MIXED && EM == 0)
+                                torus_bin_fast<SR>(st.S[s], p.m.bins[c], ft, fi);
+                            else
+                                em_bin<SR, EM>(p.m, st.S[s], c, ft, fi);
+                        }
                         kt[s] = ft;
                         ki[s] = fi * texp(-tp);
                     }
@@ -1427,8 +1435,11 @@ constexpr int kTorusMaxD = 8 + 2 * kTorusMaxBins;  // state components
 // before every event (Ys [2][D], Kw [6][D] stage slopes, Ze [4][D] escape
 // evaluations). The arrays live in local memory,
 // whose layout interleaves the lanes of a warp (same-index accesses coalesce).
+#ifndef RTW_REV_MIN_CTAS
+#define RTW_REV_MIN_CTAS 4  // CTAs per SM the reverse kernel is compiled for (128 registers)
+#endif
 template <bool MIXED>
-__global__ void __launch_bounds__(128, 4) torus_reverse(const TorusRP p) {
+__global__ void __launch_bounds__(128, RTW_REV_MIN_CTAS) torus_reverse(__grid_constant__ const TorusRP p) {
     const TorusModel& m = p.f.m;
     const int N = m.n, D = 8 + 2 * N;
     double G[(kTorusMaxCk + 1) * 8], Kgs[kTorusMaxCk * 48], taus[kTorusMaxBins];
@@ -1703,6 +1714,7 @@ rtw_status torus_model(const rtw_scene& s, const double* colors_nm, int N, Torus
         m.bins[c].hk = kHcgs * nu / kMec2;
         m.bins[c].ln_nu = std::log(nu);
         m.bins[c].inv_b0 = 1.0 / m.bins[c].b0;
+        m.bins[c].nu16 = std::pow(nu, 1.0 / 6.0);
     }
     m.n = N;
     m.emitter = powehi ? 1 : synchro ? 2 : wormhole ? 3 : sphere ? 4 : brems ? 5 : 0;
