@@ -1333,51 +1333,69 @@ RTW_HD double torus_dp_vjp(const TorusModel& m, const double* y, const double* K
         }
     }
     double hbar = 0;
-    // (2) bins
+    // (2) bins. The partials of a bin's slopes are linear in (DX, Dy) with
+    // per-stage factors (torus_bin_core), so each stage's cotangent of the
+    // emitter numbers is formed from three sums over the bins, with
+    // U = kappa_tau ft and V = kappa_I e fi:
+    //   W0 = sum (U + V), WX = sum (U + V) DX, WY = sum U Dy;
+    //   Sbar = (W0 / cj, (W0 - WX) / nus, -WY / th, (WX - 4 W0 + WY) / g).
+    // The per-stage arrays of a bin are kept in BT (their values' own
+    // precision), so that the loop's live set stays in registers.
+    double W0[6] = {0, 0, 0, 0, 0, 0}, WX[6] = {0, 0, 0, 0, 0, 0}, WY[6] = {0, 0, 0, 0, 0, 0};
     for (int c = 0; c < N; ++c) {
         const int it = 8 + c, ii = 8 + N + c;
-        double Kt[6], fi[6], ex[6], kt[6];
-        BT dft[6][4] = {}, dfi[6][4] = {};
+        BT Kt[6], fi[6], ex[6], DX[6], Dy[6];
+        double kt[6];
         const double lt = lam[it], li = lam[ii];
         double bkt = 0, bki = 0;
+#pragma unroll
         for (int t = 0; t < 6; ++t) {
-            Kt[t] = fi[t] = 0;
-            if (on[t]) {
-                BT ft_, fi_;
-                torus_bin_grad_pre<BT>(pre[t], m.bins[c], ft_, fi_, dft[t], dfi[t]);
-                Kt[t] = ft_;
-                fi[t] = fi_;
-            }
-            bkt += tA(6, t) * Kt[t];
+            Kt[t] = fi[t] = DX[t] = Dy[t] = BT(0);
+            if (on[t]) torus_bin_core<BT>(pre[t], m.bins[c], Kt[t], fi[t], DX[t], Dy[t]);
+            bkt += tA(6, t) * (double)Kt[t];
         }
         double t0 = tau[c];
         if (tau_at_end) {
             t0 -= h * bkt;
             tau[c] = t0;
         }
+#pragma unroll
         for (int t = 0; t < 6; ++t) {
             double acc = 0;
-            for (int s = 0; s < t; ++s) acc += tA(t, s) * Kt[s];
-            ex[t] = on[t] ? (double)BinMath<BT>::ex(BT(-(t0 + h * acc))) : 0.0;
-            bki += tA(6, t) * fi[t] * ex[t];
+#pragma unroll
+            for (int s = 0; s < t; ++s) acc += tA(t, s) * (double)Kt[s];
+            ex[t] = on[t] ? BinMath<BT>::ex(BT(-(t0 + h * acc))) : BT(0);
+            bki += tA(6, t) * (double)fi[t] * (double)ex[t];
             kt[t] = h * tA(6, t) * lt;
         }
         hbar += lt * bkt + li * bki;
         double msum = 0;
+#pragma unroll
         for (int t = 5; t >= 0; --t) {
             if (!on[t]) continue;  // no emitter: the bin's slopes are 0 there
-            const double ki = h * tA(6, t) * li, e = ex[t];
-            for (int q = 0; q < 4; ++q) Sbar[t][q] += kt[t] * (double)dft[t][q] + ki * e * (double)dfi[t][q];
-            const double mt = -ki * fi[t] * e;  // d (fi exp(-tau)) / d tau
+            const double ki = h * tA(6, t) * li, e = (double)ex[t];
+            const double U = kt[t] * (double)Kt[t], V = ki * e * (double)fi[t];
+            W0[t] += U + V;
+            WX[t] += (U + V) * (double)DX[t];
+            WY[t] += U * (double)Dy[t];
+            const double mt = -ki * (double)fi[t] * e;  // d (fi exp(-tau)) / d tau
             msum += mt;
             double ak = 0;
+#pragma unroll
             for (int s = 0; s < t; ++s) {
-                ak += tA(t, s) * Kt[s];
+                ak += tA(t, s) * (double)Kt[s];
                 kt[s] += h * tA(t, s) * mt;
             }
             hbar += mt * ak;
         }
         lam[it] = lt + msum;
+    }
+    for (int t = 0; t < 6; ++t) {
+        if (!on[t]) continue;
+        Sbar[t][0] = W0[t] * pre[t].icj;
+        Sbar[t][1] = (W0[t] - WX[t]) * pre[t].inus;
+        Sbar[t][2] = -WY[t] * pre[t].ith;
+        Sbar[t][3] = (WX[t] - 4 * W0[t] + WY[t]) * pre[t].ig;
     }
     // (3) geodesic components
     double kg[6][8], lg[8];

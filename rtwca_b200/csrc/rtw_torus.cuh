@@ -60,8 +60,30 @@ __device__ __constant__ double c_k2_cosh2[33] = {1.0, 1.1276259652063807, 1.5430
 static const double h_k2_cosh[33] = {1.0, 1.0314130998795732, 1.1276259652063807, 1.2946832846768448, 1.5430806348152437, 1.8884238771610158, 2.352409615243247, 2.9641883097280877, 3.7621956910836314, 4.796567530460195, 6.132289479663686, 7.853279872697439, 10.067661995777765, 12.914557062512392, 16.572824671057315, 21.272299872959398, 27.308232836016487, 35.05983829029843, 45.014120148530026, 57.79646811119539, 74.20994852478785, 95.28575798851459, 122.34800951782942, 157.09692153324536, 201.7156361224559, 259.00737756123914, 332.5715682417774, 427.02996670288616, 548.3170351552121, 704.0527791895422, 904.0214837702167, 1160.7864226767986, 1490.479161252178};
 static const double h_k2_cosh2[33] = {1.0, 1.1276259652063807, 1.5430806348152437, 2.352409615243247, 3.7621956910836314, 6.132289479663686, 10.067661995777765, 16.572824671057315, 27.308232836016487, 45.014120148530026, 74.20994852478785, 122.34800951782942, 201.7156361224559, 332.5715682417774, 548.3170351552121, 904.0214837702167, 1490.479161252178, 2457.384521883752, 4051.542025492594, 6679.863452256851, 11013.232920103323, 18157.751350891544, 29937.07086594976, 49357.885510445296, 81377.39571257407, 134168.64326230055, 221206.6960055904, 364708.18492453615, 601302.1420828041, 991379.6317690365, 1634508.6862362083, 2694849.238141599, 4443055.260253993};
 
+// The FP32 paths' rule: step 0.4 up to t = 7.6 (20 points; relative error
+// below 2e-8 for x in [0.02, 3], under FP32's rounding), cosh(0.4 i) and
+// cosh(0.8 i).
+__device__ __constant__ double c_k2f_cosh[20] = {1.0, 1.0810723718384547, 1.3374349463048447, 1.8106555673243752, 2.5774644711948853, 3.7621956910836314, 5.556947166965509, 8.252728416861135, 12.28664620054386, 18.31277908306264, 27.308232836016487, 40.73157300243561, 60.75932363289199, 90.63887921978599, 135.21505264493462, 201.7156361224559, 300.9233497146777, 448.9242027127831, 669.7157554901132, 999.0981977777762};
+__device__ __constant__ double c_k2f_cosh2[20] = {1.0, 1.3374349463048447, 2.5774644711948853, 5.556947166965509, 12.28664620054386, 27.308232836016487, 60.75932363289199, 135.21505264493462, 300.9233497146777, 669.7157554901132, 1490.479161252178, 3317.1220785054825, 7382.3908166530155, 16429.812852437903, 36565.22092354488, 81377.39571257407, 181108.72480700444, 403064.87956261594, 897037.3863033862, 1996393.417605601};
+static const double h_k2f_cosh[20] = {1.0, 1.0810723718384547, 1.3374349463048447, 1.8106555673243752, 2.5774644711948853, 3.7621956910836314, 5.556947166965509, 8.252728416861135, 12.28664620054386, 18.31277908306264, 27.308232836016487, 40.73157300243561, 60.75932363289199, 90.63887921978599, 135.21505264493462, 201.7156361224559, 300.9233497146777, 448.9242027127831, 669.7157554901132, 999.0981977777762};
+static const double h_k2f_cosh2[20] = {1.0, 1.3374349463048447, 2.5774644711948853, 5.556947166965509, 12.28664620054386, 27.308232836016487, 60.75932363289199, 135.21505264493462, 300.9233497146777, 669.7157554901132, 1490.479161252178, 3317.1220785054825, 7382.3908166530155, 16429.812852437903, 36565.22092354488, 81377.39571257407, 181108.72480700444, 403064.87956261594, 897037.3863033862, 1996393.417605601};
+
 template <class T>
 RTW_HD T bessel_k2_inv(const T& theta) {
+    if constexpr (sizeof(decltype(val(theta))) == 4) {
+        const T x = T(1.0) / theta;
+        T s = T(0.0);
+        for (int i = 0; i < 20; ++i) {
+#ifdef __CUDA_ARCH__
+            const double ch = c_k2f_cosh[i], ch2 = c_k2f_cosh2[i];
+#else
+            const double ch = h_k2f_cosh[i], ch2 = h_k2f_cosh2[i];
+#endif
+            const double w = i == 0 ? 0.2 : 0.4;
+            s = s + texp(x * decltype(val(x))(-ch)) * decltype(val(x))(w * ch2);
+        }
+        return s;
+    }
     const T x = T(1.0) / theta;
     T s = T(0.0);
     for (int i = 0; i < 33; ++i) {
@@ -84,6 +106,19 @@ RTW_HD Dual<T, K> bessel_k2_inv(const Dual<T, K>& theta) {
     // emitter tangents, FP64 otherwise)
     const T x = T(1.0) / theta.v;
     T s = T(0), ds = T(0);
+    if constexpr (sizeof(T) == 4) {
+        for (int i = 0; i < 20; ++i) {
+#ifdef __CUDA_ARCH__
+            const double ch = c_k2f_cosh[i], ch2 = c_k2f_cosh2[i];
+#else
+            const double ch = h_k2f_cosh[i], ch2 = h_k2f_cosh2[i];
+#endif
+            const T w = T((i == 0 ? 0.2 : 0.4) * ch2) * texp(-x * T(ch));
+            s += w;
+            ds -= w * T(ch);
+        }
+        return chain(theta, s, ds * (-x * x));
+    }
     for (int i = 0; i < 33; ++i) {
 #ifdef __CUDA_ARCH__
         const double ch = c_k2_cosh[i], ch2 = c_k2_cosh2[i];
@@ -749,6 +784,7 @@ RTW_HD void powehi_bin(const PowehiDev& P, const TorusPt<T>& S, double nu_nm, T&
 // bins.
 struct TorusBinPre {
     double L, gt, cjnus, ig4, icj, inus, ig, ith;
+    double e6;  // (g / nus)^(1/6) = exp(L / 6)
     bool ok;
 };
 
@@ -757,6 +793,7 @@ RTW_HD TorusBinPre torus_bin_pre(double cj, double nus, double th, double g) {
     const double r = g / nus;
     q.ok = r > 0;
     q.L = q.ok ? log(r) : 0.0;
+    q.e6 = q.ok ? exp(q.L * (1.0 / 6.0)) : 0.0;
     q.gt = g / th;
     q.cjnus = cj * nus;
     const double g2 = g * g;
@@ -788,29 +825,63 @@ struct BinMath<float> {
     static RTW_HD float em1(float x) { return expm1f(x); }
 };
 
-// torus_bin_grad from the shared part: three transcendentals per bin
-// (X^1/6; X^1/3 and X^1/2 as its square and cube) instead of six, in
-// arithmetic T.
+// torus_bin_grad from the shared part, in arithmetic T: the bin's slopes
+// (ft, fi) and the two numbers their partials are linear in,
+//   d ft / d(cj, nus, th, g) = ft (1/cj, (1 - DX)/nus, -Dy/th, (DX - 4 + Dy)/g),
+//   d fi / d(cj, nus, th, g) = fi (1/cj, (1 - DX)/nus, 0, (DX - 4)/g),
+// with DX = d log(P^2 exp(-X^1/3)) / d log X (P = X^1/2 + 2^(11/12) X^1/6, the
+// emissivity's X dependence) and Dy = y e^y / expm1(y). FP64: X^1/6 by one
+// exponential, X^1/3 and X^1/2 as its square and cube. FP32: the factorized
+// form of torus_bin_fast (X^(1/6) = (g / nus)^(1/6) nu_c^(1/6); expm1(y) and
+// y e^y / expm1(y) as Taylor polynomials below 1e-2, relative error < 2e-11).
 template <class T>
-RTW_HD void torus_bin_grad_pre(const TorusBinPre& q, const TorusBin& bn, T& ft, T& fi, T* dft, T* dfi) {
-    const double lxd = q.L + bn.ln_nu;
-    if (!q.ok || !(lxd <= 12.206072645530174)) {  // X > 2e5: exp(-X^1/3) < 1e-25, no emission
-        ft = fi = 0;
-        for (int k = 0; k < 4; ++k) dft[k] = dfi[k] = 0;
-        return;
-    }
-    const T lx = T(lxd);
+RTW_HD void torus_bin_core(const TorusBinPre& q, const TorusBin& bn, T& ft, T& fi, T& DX, T& Dy) {
     const T c = T(1.8877486253633868);  // 2^(11/12)
-    const T x16 = BinMath<T>::ex(lx * T(1.0 / 6.0)), x13 = x16 * x16, x12 = x13 * x16;
+    T x16;
+    if constexpr (sizeof(T) == 4) {
+        x16 = T(q.e6) * T(bn.nu16);
+        if (!q.ok || !(x16 <= T(7.647244913317299))) {  // X > 2e5 ((2e5)^(1/6)): no emission
+            ft = fi = DX = Dy = T(0);
+            return;
+        }
+    } else {
+        const double lxd = q.L + bn.ln_nu;
+        if (!q.ok || !(lxd <= 12.206072645530174)) {  // X > 2e5: exp(-X^1/3) < 1e-25, no emission
+            ft = fi = DX = Dy = T(0);
+            return;
+        }
+        x16 = BinMath<T>::ex(T(lxd) * T(1.0 / 6.0));
+    }
+    const T x13 = x16 * x16, x12 = x13 * x16;
     const T P = x12 + c * x16;
     const T j = T(q.cjnus) * P * P * BinMath<T>::ex(-x13);
     const T ig4 = T(q.ig4);
     fi = -(j * T(bn.inv_nu_nm3) * ig4);
-    const T y = T(q.gt * bn.hk);
-    const T em1 = BinMath<T>::em1(y);
-    ft = -(j * em1 * ig4 * T(bn.inv_b0));
-    const T DX = (x12 + c * T(1.0 / 3.0) * x16) / P - x13 * T(1.0 / 3.0);
-    const T Dy = y * (em1 + T(1)) / em1;
+    T em1;
+    if constexpr (sizeof(T) == 4) {
+        const T y = T(q.gt) * T(bn.hk);
+        if (y < T(1e-2)) {
+            em1 = y * (T(1) + y * (T(0.5) + y * (T(1.0 / 6.0) + y * (T(1.0 / 24.0) + y * T(1.0 / 120.0)))));
+            Dy = T(1) + y * (T(0.5) + y * (T(1.0 / 12.0) - y * y * T(1.0 / 720.0)));
+        } else {
+            em1 = BinMath<T>::em1(y);
+            Dy = y * (em1 + T(1)) / em1;
+        }
+        ft = -(j * (em1 * T(bn.inv_b0)) * ig4);  // em1 / b0 first: j em1 alone can fall below FP32's normal range
+    } else {
+        const T y = T(q.gt * bn.hk);
+        em1 = BinMath<T>::em1(y);
+        Dy = y * (em1 + T(1)) / em1;
+        ft = -(j * em1 * ig4 * T(bn.inv_b0));
+    }
+    DX = (x12 + c * T(1.0 / 3.0) * x16) / P - x13 * T(1.0 / 3.0);
+}
+
+// The bin's slopes and their partials d(ft, fi) / d(cj, nus, th, g).
+template <class T>
+RTW_HD void torus_bin_grad_pre(const TorusBinPre& q, const TorusBin& bn, T& ft, T& fi, T* dft, T* dfi) {
+    T DX, Dy;
+    torus_bin_core<T>(q, bn, ft, fi, DX, Dy);
     const T icj = T(q.icj), inus = T(q.inus), ig = T(q.ig);
     dfi[0] = fi * icj;
     dfi[1] = fi * (T(1) - DX) * inus;
