@@ -1284,22 +1284,18 @@ RTW_HD double torus_dp_vjp_generic(const TorusModel& m, const double* y, const d
 // the bins' partials (double, or float for the FP32-mixed adjoint); the
 // cotangents accumulate in FP64 either way.
 // mu += (d accel / d(r, theta, k))^T cw and pb[0] += (d accel / d a)^T cw at
-// the stage point Yt, the acceleration's Jacobian from 7-tangent duals in T
+// the stage point Yt, by the acceleration's reverse mode (kerr_accel_vjp) in T
 template <class T>
 RTW_HD void torus_accel_vjp(const TorusModel& m, const double* Yt, const double* cw4, double* mu, double* pb) {
-    typedef Dual<T, 7> D7;  // r, theta, k^t, k^r, k^theta, k^phi, a
-    const D7 r = D7::var(T(Yt[1]), 0), th = D7::var(T(Yt[2]), 1), a = D7::var(T(m.tor.a), 6);
-    D7 k[4], acc[4];
-    for (int i = 0; i < 4; ++i) k[i] = D7::var(T(Yt[4 + i]), 2 + i);
-    kerr_accel<D7>(m.tor.M, a, r, th, k, acc);
-    for (int i = 0; i < 4; ++i) {
-        const double cw = cw4[i];
-        if (cw == 0) continue;
-        mu[1] += cw * (double)acc[i].d[0];
-        mu[2] += cw * (double)acc[i].d[1];
-        for (int q = 0; q < 4; ++q) mu[4 + q] += cw * (double)acc[i].d[2 + q];
-        pb[0] += cw * (double)acc[i].d[6];
-    }
+    if (cw4[0] == 0 && cw4[1] == 0 && cw4[2] == 0 && cw4[3] == 0) return;
+    const T k[4] = {T(Yt[4]), T(Yt[5]), T(Yt[6]), T(Yt[7])};
+    const T cw[4] = {T(cw4[0]), T(cw4[1]), T(cw4[2]), T(cw4[3])};
+    T br, bth, ba, bk[4];
+    kerr_accel_vjp<T>(m.tor.M, T(m.tor.a), T(Yt[1]), T(Yt[2]), k, cw, br, bth, ba, bk);
+    mu[1] += (double)br;
+    mu[2] += (double)bth;
+    for (int q = 0; q < 4; ++q) mu[4 + q] += (double)bk[q];
+    pb[0] += (double)ba;
 }
 
 template <class BT>
