@@ -755,6 +755,7 @@ def run_b200(args):
         cpu = None
         parity = None
         ring = None
+        ref_form = None
         g_cls, g_xyz = hc.numpy(), hx.numpy()
         if not args.no_cpu_baseline:
             v, n, dt, cores, ref = cpu_time(scene, cam, colors, args.cpu_sample, keep=True)
@@ -767,6 +768,17 @@ def run_b200(args):
             parity["of"] = "evenly spaced pixels vs the FP64 oracle, reference step; error on linear Y"
             if args.workload in ("kerr_thin_disk", "schwarzschild_disk"):
                 ring = photon_ring_leg(scene, cam, colors, g_cls, g_xyz)
+            # the work of the reference's form: the oracle's own integration of
+            # the same pixels over a counting scalar (its own step counts),
+            # scaled to the frame
+            from oracle import oracle as O
+            wk = O.work(scene, cam, colors, pixel_ids=ids)
+            fw = wk["flops"] * P / ids.size
+            ref_form = {"achieved": round(fw / (kms * 1e-3) / 1e12, 3),
+                        "frac": round(fw / (kms * 1e-3) / 1e12 / peak, 4),
+                        "flops_per_attempt": round(wk["flops"] / wk["attempts"]),
+                        "kernel_flops_per_attempt": round(flops / st["step_attempts"]),
+                        "source": "oracle counting-scalar run of the cpu sample, scaled to the frame"}
         fp64_v = fp64["value"] if fp64 else None
         summary = {
             "mixed_Mrays_s": value if prec == abi.PREC_MIXED else None,
@@ -807,7 +819,8 @@ def run_b200(args):
                          "traffic": (st["step_attempts"] * TRAFFIC_B_PER_ATTEMPT
                                      if prec == abi.PREC_MIXED and args.workload == "kerr_thin_disk" else None),
                          "peak_source": "measured in-run FMA probe (rtw_measure_peaks)",
-                         "mufu_gops": mufu / (kms * 1e-3) / 1e9, "mufu_peak_gops": peaks["mufu_ops"] / 1e9},
+                         "mufu_gops": mufu / (kms * 1e-3) / 1e9, "mufu_peak_gops": peaks["mufu_ops"] / 1e9,
+                         "reference_form": ref_form},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_val, "unit": "Mrays/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "timer": "host clock around the synchronous rtw_render call"},

@@ -53,6 +53,9 @@ def load() -> C.CDLL:
                                       D, C.POINTER(C.c_ubyte), C.POINTER(C.c_uint), D, D, D,
                                       C.POINTER(C.c_longlong), C.c_int]
         lib.oracle_render.restype = C.c_int
+        lib.oracle_work.argtypes = [P, P, D, C.c_int, C.c_double, C.c_int, C.POINTER(C.c_longlong), C.c_longlong,
+                                    C.POINTER(C.c_longlong), C.c_int]
+        lib.oracle_work.restype = C.c_int
         lib.oracle_set_skybox.argtypes = [C.c_int, C.POINTER(C.c_float), C.c_int]
         lib.oracle_set_skybox.restype = C.c_int
         lib.oracle_torus_forward.argtypes = [P, P, D, C.c_int, C.c_double, C.c_int, C.POINTER(C.c_longlong),
@@ -194,6 +197,31 @@ def render(scene, cam, colors_nm, *, max_dt_scale=0.1, integrator=0, pixel_ids=N
     res["counters"] = counters
     res["y_pix"] = cam.y_pix
     return res
+
+
+def work(scene, cam, colors_nm, *, max_dt_scale=0.1, integrator=0, pixel_ids=None, threads=0):
+    """Algorithmic work of the reference's form over one camera's pixels (or
+    `pixel_ids`): the oracle's own integration of those rays run over a
+    counting scalar (same path and step counts as render()). Thin-disk scenes
+    only. Returns {"flops", "transcendentals", "attempts", "rays"}:
+    add/sub/mul 1 flop; div/sqrt/exp/log/sin/cos 1 flop + 1 transcendental;
+    pow 2 + 2."""
+    from rtwca_b200 import abi
+    cam = abi.Camera.from_buffer_copy(cam)
+    cam.y_pix = abi.y_pixels(cam.x_pix, cam.fov_hor, cam.fov_vert)
+    c = np.ascontiguousarray(colors_nm, dtype=np.float64)
+    ids = None
+    n = cam.x_pix * cam.y_pix
+    if pixel_ids is not None:
+        ids = np.ascontiguousarray(pixel_ids, dtype=np.int64)
+        n = ids.size
+    out = np.zeros(4, np.int64)
+    st = load().oracle_work(C.byref(scene), C.byref(cam), _dp(c), c.size, float(max_dt_scale), int(integrator),
+                            ids.ctypes.data_as(C.POINTER(C.c_longlong)) if ids is not None else None, n,
+                            out.ctypes.data_as(C.POINTER(C.c_longlong)), int(threads))
+    if st != 0:
+        raise RuntimeError(f"oracle_work failed with status {st}")
+    return {"flops": int(out[0]), "transcendentals": int(out[1]), "attempts": int(out[2]), "rays": int(out[3])}
 
 
 def torus_forward(scene, cam, colors_nm, *, mode=0, max_dt_scale=0.1, pixel_ids=None, threads=0):

@@ -176,6 +176,85 @@ template <class T>
 inline T sqT(const T& x) { return x * x; }
 
 // ----------------------------------------------------------------------------
+// Counting scalar: a double value and, per thread, the operations the
+// oracle's arithmetic performs on it, so that the algorithmic work of the
+// reference's form is counted by running the oracle itself: add/sub/mul = 1
+// flop; div/sqrt/exp/log/sin/cos = 1 flop + 1 transcendental; pow = 2 + 2
+// (the convention of the library's rtw_get_op_counts). Sign flips and
+// fabs/min/max are not counted. Comparisons and branches use the value, so a
+// counting run takes the double run's path exactly.
+// ----------------------------------------------------------------------------
+struct OpTally {
+    long long flops = 0, special = 0;
+};
+inline OpTally& tally() {
+    static thread_local OpTally t;
+    return t;
+}
+struct Cnt {
+    double v = 0;
+    Cnt() = default;
+    Cnt(double x) : v(x) {}  // NOLINT: constants enter uncounted
+};
+inline double val(const Cnt& x) { return x.v; }
+inline Cnt cnt_op(double r, int f, int sp) {
+    OpTally& t = tally();
+    t.flops += f;
+    t.special += sp;
+    return Cnt(r);
+}
+inline Cnt operator-(const Cnt& a) { return Cnt(-a.v); }
+inline Cnt operator+(const Cnt& a, const Cnt& b) { return cnt_op(a.v + b.v, 1, 0); }
+inline Cnt operator-(const Cnt& a, const Cnt& b) { return cnt_op(a.v - b.v, 1, 0); }
+inline Cnt operator*(const Cnt& a, const Cnt& b) { return cnt_op(a.v * b.v, 1, 0); }
+inline Cnt operator/(const Cnt& a, const Cnt& b) { return cnt_op(a.v / b.v, 1, 1); }
+inline Cnt operator+(const Cnt& a, double b) { return cnt_op(a.v + b, 1, 0); }
+inline Cnt operator+(double a, const Cnt& b) { return cnt_op(a + b.v, 1, 0); }
+inline Cnt operator-(const Cnt& a, double b) { return cnt_op(a.v - b, 1, 0); }
+inline Cnt operator-(double a, const Cnt& b) { return cnt_op(a - b.v, 1, 0); }
+inline Cnt operator*(const Cnt& a, double b) { return cnt_op(a.v * b, 1, 0); }
+inline Cnt operator*(double a, const Cnt& b) { return cnt_op(a * b.v, 1, 0); }
+inline Cnt operator/(const Cnt& a, double b) { return cnt_op(a.v / b, 1, 1); }
+inline Cnt operator/(double a, const Cnt& b) { return cnt_op(a / b.v, 1, 1); }
+inline Cnt& operator+=(Cnt& a, const Cnt& b) { return a = a + b; }
+inline Cnt& operator-=(Cnt& a, const Cnt& b) { return a = a - b; }
+inline Cnt& operator*=(Cnt& a, const Cnt& b) { return a = a * b; }
+inline bool operator<(const Cnt& a, const Cnt& b) { return a.v < b.v; }
+inline bool operator>(const Cnt& a, const Cnt& b) { return a.v > b.v; }
+inline bool operator<=(const Cnt& a, const Cnt& b) { return a.v <= b.v; }
+inline bool operator>=(const Cnt& a, const Cnt& b) { return a.v >= b.v; }
+inline bool operator==(const Cnt& a, const Cnt& b) { return a.v == b.v; }
+inline bool operator!=(const Cnt& a, const Cnt& b) { return a.v != b.v; }
+inline bool operator<(const Cnt& a, double b) { return a.v < b; }
+inline bool operator>(const Cnt& a, double b) { return a.v > b; }
+inline bool operator<=(const Cnt& a, double b) { return a.v <= b; }
+inline bool operator>=(const Cnt& a, double b) { return a.v >= b; }
+inline bool operator==(const Cnt& a, double b) { return a.v == b; }
+inline bool operator!=(const Cnt& a, double b) { return a.v != b; }
+inline bool operator<(double a, const Cnt& b) { return a < b.v; }
+inline bool operator>(double a, const Cnt& b) { return a > b.v; }
+inline bool operator<=(double a, const Cnt& b) { return a <= b.v; }
+inline bool operator>=(double a, const Cnt& b) { return a >= b.v; }
+inline Cnt sin(const Cnt& a) { return cnt_op(std::sin(a.v), 1, 1); }
+inline Cnt cos(const Cnt& a) { return cnt_op(std::cos(a.v), 1, 1); }
+inline Cnt tan(const Cnt& a) { return cnt_op(std::tan(a.v), 1, 1); }
+inline Cnt atan(const Cnt& a) { return cnt_op(std::atan(a.v), 1, 1); }
+inline Cnt sqrt(const Cnt& a) { return cnt_op(std::sqrt(a.v), 1, 1); }
+inline Cnt exp(const Cnt& a) { return cnt_op(std::exp(a.v), 1, 1); }
+inline Cnt expm1(const Cnt& a) { return cnt_op(std::expm1(a.v), 1, 1); }
+inline Cnt log(const Cnt& a) { return cnt_op(std::log(a.v), 1, 1); }
+inline Cnt pow(const Cnt& a, double e) { return cnt_op(std::pow(a.v, e), 2, 2); }
+inline Cnt pow(const Cnt& a, const Cnt& e) { return cnt_op(std::pow(a.v, e.v), 2, 2); }
+inline Cnt fabs(const Cnt& a) { return Cnt(std::fabs(a.v)); }
+inline bool isfinite(const Cnt& a) { return std::isfinite(a.v); }
+inline Cnt jl_mod(const Cnt& x, double y) { return cnt_op(jl_mod(x.v, y), 1, 0); }
+inline Cnt max(const Cnt& a, const Cnt& b) { return a.v < b.v ? b : a; }
+inline Cnt min(const Cnt& a, const Cnt& b) { return b.v < a.v ? b : a; }
+inline Cnt max(const Cnt& a, double b) { return a.v < b ? Cnt(b) : a; }
+inline Cnt min(const Cnt& a, double b) { return b < a.v ? Cnt(b) : a; }
+
+
+// ----------------------------------------------------------------------------
 // Scenes (".source" plugins), restated with runtime constants.
 // ----------------------------------------------------------------------------
 struct OScene {
@@ -276,28 +355,33 @@ struct OScene {
     }
 
     // calc_lower_metric!: Kerr :66-75, Schwarzschild :15-21, Minkowski :10-16
-    void lower_metric(const double* x, double g[4][4]) const {
+    // (over the scalar F: double, or Cnt for the thin-disk scenes' op counts)
+    template <class F>
+    void lower_metric(const F* x, F g[4][4]) const {
+        using std::sin;
         for (int i = 0; i < 4; ++i)
             for (int j = 0; j < 4; ++j) g[i][j] = (i == j) ? 1.0 : 0.0;
-        const double r = x[1], th = x[2];
+        const F r = x[1], th = x[2];
         if (is_cart()) {  // Synchro_Test source_geometry.jl:7-16
             g[0][0] = -1.0;
         } else if (is_wh()) {  // Wormhole source_geometry.jl:44-51
-            g[0][0] = -1.0;
-            g[2][2] = sq(wh_r(r));
-            g[3][3] = sq(wh_r(r) * std::sin(th));
+            if constexpr (std::is_same<F, double>::value) {
+                g[0][0] = -1.0;
+                g[2][2] = sq(wh_r(r));
+                g[3][3] = sq(wh_r(r) * std::sin(th));
+            }
         } else if (is_kerr()) {
-            kerr_metric_t<double>(r, th, a, g);
+            kerr_metric_t<F>(r, th, F(a), g);
         } else if (kind == RTW_SCENE_SCHWARZSCHILD_DISK) {
             g[0][0] = -(1.0 - rs / r);
             g[1][1] = 1.0 / (1.0 - rs / r);
             g[2][2] = r * r;
-            g[3][3] = sq(r * std::sin(th));
+            g[3][3] = sqT(r * sin(th));
         } else {
             g[0][0] = -1.0;
             g[1][1] = 1.0;
             g[2][2] = r * r;
-            g[3][3] = sq(r * std::sin(th));
+            g[3][3] = sqT(r * sin(th));
         }
     }
 
@@ -380,11 +464,22 @@ struct OScene {
     }
 
     // calc_christoffel_udd!: Kerr :195-243, Schwarzschild :109-128, Minkowski :93-108
-    void christoffel(const double* x, double G[4][4][4]) const {
-        std::memset(G, 0, sizeof(double) * 64);
+    template <class F>
+    void christoffel(const F* x, F G[4][4][4]) const {
+        using std::cos;
+        using std::sin;
+        for (int i = 0; i < 4; ++i)
+            for (int j = 0; j < 4; ++j)
+                for (int k = 0; k < 4; ++k) G[i][j][k] = 0.0;
         if (is_cart()) return;  // Synchro_Test source_geometry.jl:53-66
-        const double r = x[1], th = x[2];
-        if (is_wh()) {  // Wormhole source_geometry.jl:131-150
+        const F r = x[1], th = x[2];
+        if constexpr (!std::is_same<F, double>::value) {
+            // the counting run: the thin-disk scenes (FP64 Christoffel symbols)
+            if (is_kerr()) {
+                kerr_christoffel<F, F>(r, th, F(a), F(rs), G);
+                return;
+            }
+        } else if (is_wh()) {  // Wormhole source_geometry.jl:131-150
             const double rl = wh_r(r), drdl = wh_drdl(r);
             G[1][2][2] = -rl * drdl;
             G[1][3][3] = -rl * drdl * sq(std::sin(th));
@@ -397,34 +492,38 @@ struct OScene {
             G[3][3][2] = G[3][2][3];
             return;
         }
-        if (is_kerr()) {
-            if (refprec)
-                kerr_christoffel<float, double>((float)r, (float)th, (float)a, (float)rs, G);
-            else
-                kerr_christoffel<double, double>(r, th, a, rs, G);
-        } else if (kind == RTW_SCENE_SCHWARZSCHILD_DISK) {
+        if constexpr (std::is_same<F, double>::value) {
+            if (is_kerr()) {
+                if (refprec)
+                    kerr_christoffel<float, double>((float)r, (float)th, (float)a, (float)rs, G);
+                else
+                    kerr_christoffel<double, double>(r, th, a, rs, G);
+                return;
+            }
+        }
+        if (kind == RTW_SCENE_SCHWARZSCHILD_DISK) {
             G[0][0][1] = rs / (2 * r * (r - rs));
             G[0][1][0] = G[0][0][1];
             G[1][0][0] = rs * (r - rs) / (2 * r * r * r);
             G[1][1][1] = -rs / (2 * r * (r - rs));
             G[1][2][2] = -(r - rs);
-            G[1][3][3] = -(r - rs) * sq(std::sin(th));
+            G[1][3][3] = -(r - rs) * sqT(sin(th));
             G[2][1][2] = 1.0 / r;
             G[2][2][1] = G[2][1][2];
-            G[2][3][3] = -std::sin(th) * std::cos(th);
+            G[2][3][3] = -sin(th) * cos(th);
             G[3][1][3] = 1.0 / r;
             G[3][3][1] = G[3][1][3];
-            G[3][2][3] = std::cos(th) / std::sin(th);
+            G[3][2][3] = cos(th) / sin(th);
             G[3][3][2] = G[3][2][3];
         } else {
             G[1][2][2] = -r;
-            G[1][3][3] = -r * sq(std::sin(th));
+            G[1][3][3] = -r * sqT(sin(th));
             G[2][1][2] = 1.0 / (r + kNoDivZero);
             G[2][2][1] = G[2][1][2];
-            G[2][3][3] = -std::sin(th) * std::cos(th);
+            G[2][3][3] = -sin(th) * cos(th);
             G[3][1][3] = 1.0 / (r + kNoDivZero);
             G[3][3][1] = G[3][1][3];
-            G[3][2][3] = std::cos(th) / std::sin(th);
+            G[3][2][3] = cos(th) / sin(th);
             G[3][3][2] = G[3][2][3];
         }
     }
@@ -476,7 +575,8 @@ struct OScene {
     }
 
     // keepinbounds!: Kerr :275-301 (= Schwarzschild :160-186), Minkowski :138-163
-    void keepinbounds(double* x) const {
+    template <class F>
+    void keepinbounds(F* x) const {
         if (is_cart()) return;  // Synchro_Test source_geometry.jl:76-80
         if (kind == RTW_SCENE_MINKOWSKI_SPHERE && x[1] <= 0) {
             x[1] = -x[1] + kNoDivZero;
@@ -509,12 +609,14 @@ struct OScene {
 
     // --- model --------------------------------------------------------------
     // is_fire: Kerr model :73-80, Schwarzschild :73-80, Minkowski :76-83
-    bool is_fire(const double* x) const {
-        const double r = x[1], th = x[2];
+    template <class F>
+    bool is_fire(const F* x) const {
+        using std::sqrt;
+        const F r = x[1], th = x[2];
         switch (kind) {
         case RTW_SCENE_MINKOWSKI_SPHERE: return r <= r_out;
         case RTW_SCENE_MINKOWSKI_CART_SPHERE:  // Minkowski_Sphere_Cartesian model :82-90
-            return std::sqrt(x[1] * x[1] + x[2] * x[2] + x[3] * x[3]) <= r_out;
+            return sqrt(x[1] * x[1] + x[2] * x[2] + x[3] * x[3]) <= r_out;
         case RTW_SCENE_SCHWARZSCHILD_DISK:
         case RTW_SCENE_KERR_DISK:
             return r_in <= r && r <= r_out && th_lo <= th && th <= th_hi;
@@ -524,32 +626,37 @@ struct OScene {
     }
 
     // get_source_velocity!: Kerr model :109-137, Schwarzschild :112-133, Minkowski :111-117
-    void source_velocity(const double* x, double u[4]) const {
-        const double r = x[1], th = x[2];
+    template <class F>
+    void source_velocity(const F* x, F u[4]) const {
+        using std::cos;
+        using std::pow;
+        using std::sin;
+        using std::sqrt;
+        const F r = x[1], th = x[2];
         u[0] = 1; u[1] = 0; u[2] = 0; u[3] = 0;
         if (kind == RTW_SCENE_MINKOWSKI_SPHERE || kind == RTW_SCENE_MINKOWSKI_CART_SPHERE) return;
         if (kind == RTW_SCENE_SCHWARZSCHILD_DISK) {
             if (is_fire(x)) {
-                u[0] = 1.0 / std::sqrt(1 - 3 * M / r);
-                u[3] = (1.0 / std::sqrt(1 - 3 * M / r)) * std::sqrt(M / (r * r * r));
+                u[0] = 1.0 / sqrt(1 - 3 * M / r);
+                u[3] = (1.0 / sqrt(1 - 3 * M / r)) * sqrt(M / (r * r * r));
             } else {
-                u[0] = 1.0 / std::sqrt(1 - 2 * M / r);
+                u[0] = 1.0 / sqrt(1 - 2 * M / r);
             }
             return;
         }
         if (is_fire(x)) {
-            const double r32 = std::pow(r, 1.5);
-            const double Om = std::sqrt(M) / (r32 + a * std::sqrt(M));
-            const double D = r32 - 3 * M * std::sqrt(r) + 2 * a * std::sqrt(M);
-            const double ut = (r32 + a * std::sqrt(M)) / (std::pow(r, 0.75) * std::sqrt(D));
+            const F r32 = pow(r, 1.5);
+            const F Om = sqrt(F(M)) / (r32 + a * sqrt(F(M)));
+            const F D = r32 - 3 * M * sqrt(r) + 2 * a * sqrt(F(M));
+            const F ut = (r32 + a * sqrt(F(M))) / (pow(r, 0.75) * sqrt(D));
             u[0] = ut;
             u[3] = ut * Om;
         } else {
-            const double Aa = std::sqrt(r * r + sq(a * std::cos(th)));
-            const double B = r * r + a * a - 2 * M * r;
-            const double C = sq(r * r + a * a) - B * sq(a * std::sin(th));
-            const double ut = std::sqrt(C) / (Aa * std::sqrt(B));
-            const double Om = 2 * a * M * r / C;
+            const F Aa = sqrt(r * r + sqT(a * cos(th)));
+            const F B = r * r + a * a - 2 * M * r;
+            const F C = sqT(r * r + a * a) - B * sqT(a * sin(th));
+            const F ut = sqrt(C) / (Aa * sqrt(B));
+            const F Om = 2 * a * M * r / C;
             u[0] = ut;
             u[3] = ut * Om;
         }
@@ -557,23 +664,27 @@ struct OScene {
 
     // calc_radiative_coefficients + calc_planck (Kerr model :18-21,57-67 and
     // the other scenes). fluid: temperature (and density for the thick disk).
-    void radiative(const double* x, double nu, double* a_nu, double* j_nu) const {
+    template <class F>
+    void radiative(const F* x, F nu, F* a_nu, F* j_nu) const {
+        using std::cos;
+        using std::exp;
+        using std::pow;
         if (!is_fire(x)) {
             *a_nu = 0;
             *j_nu = 0;
             return;
         }
-        double Tl = T, al = anu;
+        F Tl = T, al = anu;
         if (kind == RTW_SCENE_KERR_THICK_DISK) {
-            const double r = x[1];
-            const double z = r * std::cos(x[2]);
-            const double hz = rho_h * r;
-            const double rho = std::pow(r / rho_r0, rho_idx) * std::exp(-(z * z) / (2 * hz * hz));
-            Tl = T * std::pow(r / rho_r0, t_idx);
+            const F r = x[1];
+            const F z = r * cos(x[2]);
+            const F hz = rho_h * r;
+            const F rho = pow(r / rho_r0, rho_idx) * exp(-(z * z) / (2 * hz * hz));
+            Tl = T * pow(r / rho_r0, t_idx);
             al = anu * rho;
         }
         *a_nu = al;
-        *j_nu = al * (kEmissionScale * (nu * nu * nu) / (std::exp(kFFactor * nu / Tl) - 1));
+        *j_nu = al * (kEmissionScale * (nu * nu * nu) / (exp(kFFactor * nu / Tl) - 1));
     }
 
     // pad_max_dt: Kerr model :86-103, Schwarzschild :86-106, Minkowski :89-105
@@ -647,16 +758,19 @@ struct OScene {
 // ----------------------------------------------------------------------------
 // Integrator (integrators_LttM.jl), one ray's buffers.
 // ----------------------------------------------------------------------------
-struct RayWork {
+// (over the scalar F: double, or Cnt for the thin-disk scenes' op counts)
+template <class F>
+struct RayWorkT {
     int L = 0, N = 0;
     const double* freq = nullptr;  // colors_freq, nm^-1
     double tol = 1e-4;
     double scale = 0.1;
     bool fsal = false;
-    std::vector<double> last_slope, next_slope, buffer, y, k2, k3, k4, k5, k6, k7;
-    double G[4][4][4];
-    double g[4][4];
-    double u[4];
+    std::vector<F> last_slope, next_slope, buffer, y, k2, k3, k4, k5, k6, k7;
+    std::vector<double> plain;  // the state as doubles, for the scene's control functions
+    F G[4][4][4];
+    F g[4][4];
+    F u[4];
     void init(int N_, const double* f, double tol_, double scale_, bool fsal_) {
         N = N_;
         L = 8 + 2 * N;
@@ -664,9 +778,20 @@ struct RayWork {
         tol = tol_;
         scale = scale_;
         fsal = fsal_;
-        for (auto* v : {&last_slope, &next_slope, &buffer, &y, &k2, &k3, &k4, &k5, &k6, &k7}) v->assign(L, 0.0);
+        for (auto* v : {&last_slope, &next_slope, &buffer, &y, &k2, &k3, &k4, &k5, &k6, &k7}) v->assign(L, F(0.0));
+        plain.assign(L, 0.0);
     }
 };
+using RayWork = RayWorkT<double>;
+
+// The state's values as doubles (the scene's step-size cap, polar-escape
+// test and termination test read values only): R itself for double.
+inline const double* plain_state(RayWork&, const double* R) { return R; }
+template <class F>
+const double* plain_state(RayWorkT<F>& w, const F* R) {
+    for (int i = 0; i < w.L; ++i) w.plain[i] = val(R[i]);
+    return w.plain.data();
+}
 
 // RT slopes of the synchrotron torus (no reference counterpart; the formulas
 // are listed in the file header), over the scalar type: spin al and the
@@ -972,49 +1097,54 @@ void synchro_bins(const OScene& sc, RayWork& w, const double* R, double* slope) 
 }
 
 // calc_ray_derivative!, integrators_LttM.jl:9-48
-void rhs(const OScene& sc, RayWork& w, const double* R, double* slope) {
+// (over the scalar F: double; Cnt runs the thin-disk scenes only)
+template <class F>
+void rhs(const OScene& sc, RayWorkT<F>& w, const F* R, F* slope) {
+    using std::exp;
     for (int i = 0; i < 4; ++i) slope[i] = R[i + 4];
     sc.christoffel(R, w.G);
     for (int i = 0; i < 4; ++i) {
-        double acc = 0;
+        F acc = 0;
         for (int j = 0; j < 4; ++j)
             for (int k = 0; k < 4; ++k) acc -= w.G[i][j][k] * R[4 + j] * R[4 + k];
         slope[4 + i] = acc;
     }
-    if (sc.kind == RTW_SCENE_KERR_SYNCHRO_TORUS) {
-        torus_bins(sc, w, R, slope);
-        return;
-    }
-    if (sc.kind == RTW_SCENE_KERR_BREMS_TORUS) {
-        brems_bins(sc, w, R, slope);
-        return;
-    }
-    if (sc.kind == RTW_SCENE_KERR_POWEHI) {
-        powehi_bins(sc, w, R, slope);
-        return;
-    }
-    if (sc.kind == RTW_SCENE_SYNCHRO_TEST) {
-        synchro_bins(sc, w, R, slope);
-        return;
+    if constexpr (std::is_same<F, double>::value) {
+        if (sc.kind == RTW_SCENE_KERR_SYNCHRO_TORUS) {
+            torus_bins(sc, w, R, slope);
+            return;
+        }
+        if (sc.kind == RTW_SCENE_KERR_BREMS_TORUS) {
+            brems_bins(sc, w, R, slope);
+            return;
+        }
+        if (sc.kind == RTW_SCENE_KERR_POWEHI) {
+            powehi_bins(sc, w, R, slope);
+            return;
+        }
+        if (sc.kind == RTW_SCENE_SYNCHRO_TEST) {
+            synchro_bins(sc, w, R, slope);
+            return;
+        }
     }
     sc.lower_metric(R, w.g);
     sc.source_velocity(R, w.u);
     // calc_freq_shift, gen_geometry.jl:373-390
-    double fs = 0;
+    F fs = 0;
     for (int j = 0; j < 4; ++j) {
-        double ps = 0;
+        F ps = 0;
         for (int i = 0; i < 4; ++i) ps += w.g[i][j] * R[i + 4];
         fs -= w.u[j] * ps;
     }
     for (int c = 0; c < w.N; ++c) {
-        const double nu = w.freq[c] * fs;
-        double a_nu, j_nu;
+        const F nu = w.freq[c] * fs;
+        F a_nu, j_nu;
         sc.radiative(R, nu, &a_nu, &j_nu);
         if (a_nu == 0 && j_nu == 0) {
             slope[8 + 2 * c] = 0;
             slope[9 + 2 * c] = 0;
         } else {
-            slope[8 + 2 * c] = -(1.0 / fs) * j_nu * std::exp(-R[9 + 2 * c]) / (nu * nu * nu);
+            slope[8 + 2 * c] = -(1.0 / fs) * j_nu * exp(-R[9 + 2 * c]) / (nu * nu * nu);
             slope[9 + 2 * c] = -(1.0 / fs) * a_nu;
         }
     }
@@ -1022,35 +1152,42 @@ void rhs(const OScene& sc, RayWork& w, const double* R, double* slope) {
 
 // RKDP_Step_w_buffer!, integrators_LttM.jl:54-224. Returns the new step size;
 // *rejected is the reject flag. counters[0] counts polar Euler sub-steps.
-double dp45_step(const OScene& sc, RayWork& w, double* R, double h, bool prev_rejected, bool* rejected,
-                 long long* escape_substeps) {
+// (over the scalar F: double, or Cnt for the thin-disk scenes' op counts)
+template <class F>
+F dp45_step(const OScene& sc, RayWorkT<F>& w, F* R, F h, bool prev_rejected, bool* rejected,
+            long long* escape_substeps) {
+    using std::fabs;
+    using std::isfinite;
+    using std::max;
+    using std::pow;
+    using std::sqrt;
     const int L = w.L;
-    double* k1 = w.last_slope.data();
-    const double max_dt = sc.pad_max_dt(R, w.scale);
+    F* k1 = w.last_slope.data();
+    const double max_dt = sc.pad_max_dt(plain_state(w, R), w.scale);
     double temp;
-    if (sc.near_singularity(R, h, w.tol, &temp)) {
+    if (sc.near_singularity(plain_state(w, R), val(h), w.tol, &temp)) {
         for (int i = 0; i < L; ++i) R[i] -= temp * k1[i];
         sc.keepinbounds(R);
         if (escape_substeps) ++*escape_substeps;
         for (int it = 0; it < 36; ++it) {
-            if (!sc.terminate(R, L, w.tol, 2, 1)) {
+            if (!sc.terminate(plain_state(w, R), L, w.tol, 2, 1)) {
                 rhs(sc, w, R, k1);
                 for (int j = 0; j < L; ++j) R[j] -= temp * k1[j];
                 sc.keepinbounds(R);
                 if (escape_substeps) ++*escape_substeps;
             }
         }
-        if (sc.terminate(R, L, w.tol, 2, 1)) {
+        if (sc.terminate(plain_state(w, R), L, w.tol, 2, 1)) {
             *rejected = false;
             return h;
         }
         rhs(sc, w, R, k1);
-        h = -sc.pad_max_dt(R, w.scale);
+        h = -sc.pad_max_dt(plain_state(w, R), w.scale);
     }
     const auto& A = kDP.a;
-    double* buf = w.buffer.data();
-    double *k2 = w.k2.data(), *k3 = w.k3.data(), *k4 = w.k4.data(), *k5 = w.k5.data(), *k6 = w.k6.data(),
-           *k7 = w.k7.data();
+    F* buf = w.buffer.data();
+    F *k2 = w.k2.data(), *k3 = w.k3.data(), *k4 = w.k4.data(), *k5 = w.k5.data(), *k6 = w.k6.data(),
+      *k7 = w.k7.data();
     for (int i = 0; i < L; ++i) buf[i] = R[i] + h * k1[i] * A[2][2];
     rhs(sc, w, buf, k2);
     for (int i = 0; i < L; ++i) buf[i] = R[i] + h * (k1[i] * A[3][2] + k2[i] * A[3][3]);
@@ -1063,46 +1200,46 @@ double dp45_step(const OScene& sc, RayWork& w, double* R, double h, bool prev_re
     for (int i = 0; i < L; ++i)
         buf[i] = R[i] + h * (k1[i] * A[6][2] + k2[i] * A[6][3] + k3[i] * A[6][4] + k4[i] * A[6][5] + k5[i] * A[6][6]);
     rhs(sc, w, buf, k6);
-    double* ns = w.next_slope.data();
+    F* ns = w.next_slope.data();
     for (int i = 0; i < L; ++i)
         ns[i] = k1[i] * A[7][2] + k3[i] * A[7][4] + k4[i] * A[7][5] + k5[i] * A[7][6] + k6[i] * A[7][7];
     for (int i = 0; i < L; ++i) buf[i] = R[i] + h * ns[i];
     rhs(sc, w, buf, k7);
-    double* y = w.y.data();
+    F* y = w.y.data();
     for (int i = 0; i < L; ++i) y[i] = R[i] + h * ns[i];
     for (int i = 0; i < L; ++i)
         buf[i] = y[i] - R[i] -
                  h * (k1[i] * A[9][2] + k3[i] * A[9][4] + k4[i] * A[9][5] + k5[i] * A[9][6] + k6[i] * A[9][7] +
                       k7[i] * A[9][8]);
-    double err = 0;
+    F err = 0;
     for (int i = 0; i < L; ++i) {
-        const double tol = w.tol + std::max(std::fabs(R[i]), std::fabs(y[i])) * w.tol;
-        err += sq(buf[i] / tol);
+        const F tol = w.tol + max(fabs(R[i]), fabs(y[i])) * w.tol;
+        err += sqT(buf[i] / tol);
     }
-    err = std::sqrt(err / L);
-    double hn = 0.9 * h * std::pow(1.0 / err, 1.0 / 5);
-    if (std::fabs(hn) > max_dt) hn = -max_dt;
-    const double* newk1 = w.fsal ? k7 : ns;
-    if (err == 0 || !std::isfinite(hn)) {
-        const double th_before = y[2];
+    err = sqrt(err / L);
+    F hn = 0.9 * h * pow(1.0 / err, 1.0 / 5);
+    if (fabs(hn) > max_dt) hn = -max_dt;
+    const F* newk1 = w.fsal ? k7 : ns;
+    if (err == 0 || !isfinite(hn)) {
+        const double th_before = val(y[2]);
         sc.keepinbounds(y);
         for (int i = 0; i < L; ++i) {
             k1[i] = newk1[i];
             R[i] = y[i];
         }
         if ((sc.kind == RTW_SCENE_KERR_SYNCHRO_TORUS || sc.kind == RTW_SCENE_KERR_POWEHI ||
-             sc.kind == RTW_SCENE_KERR_BREMS_TORUS) && w.fsal && y[2] != th_before)
+             sc.kind == RTW_SCENE_KERR_BREMS_TORUS) && w.fsal && val(y[2]) != th_before)
         rhs(sc, w, R, k1);
         *rejected = false;
         return h;
     } else if (err > 1) {
-        if (prev_rejected && std::fabs(hn) >= std::fabs(h)) hn = h / 2;
+        if (prev_rejected && fabs(hn) >= fabs(h)) hn = h / 2;
         sc.keepinbounds(R);
         *rejected = true;
         return hn;
     }
-    if (std::fabs(hn) > 5 * std::fabs(h)) hn = 5 * h;
-    const double th_before = y[2];
+    if (fabs(hn) > 5 * fabs(h)) hn = 5 * h;
+    const double th_before = val(y[2]);
     sc.keepinbounds(y);
     for (int i = 0; i < L; ++i) {
         k1[i] = newk1[i];
@@ -1113,10 +1250,34 @@ double dp45_step(const OScene& sc, RayWork& w, double* R, double h, bool prev_re
     // each step depends on its start state alone, as the library's per-bin
     // kernels do (the reference's own step keeps its carried slope)
     if ((sc.kind == RTW_SCENE_KERR_SYNCHRO_TORUS || sc.kind == RTW_SCENE_KERR_POWEHI ||
-             sc.kind == RTW_SCENE_KERR_BREMS_TORUS) && w.fsal && y[2] != th_before)
+             sc.kind == RTW_SCENE_KERR_BREMS_TORUS) && w.fsal && val(y[2]) != th_before)
         rhs(sc, w, R, k1);
     *rejected = false;
     return hn;
+}
+
+// integrate_ray, LttM.jl:11-59: one ray from its initial state to its
+// termination class (over the scalar F, as dp45_step); counts its step
+// attempts, rejections, polar sub-steps and equatorial crossings.
+template <class F>
+int integrate_ray(const OScene& sc, RayWorkT<F>& w, F* ray, double max_dt_scale, double tol, long long max_steps,
+                  long long* step_count, long long* rej, long long* esc, int* crossings) {
+    const int L = w.L;
+    F dt = -sc.pad_max_dt(plain_state(w, ray), max_dt_scale);
+    rhs(sc, w, ray, w.last_slope.data());
+    w.next_slope = w.last_slope;
+    bool rejected = false;
+    while (true) {
+        bool rj = false;
+        const double side = val(ray[2]) - kPi / 2;
+        dt = dp45_step(sc, w, ray, dt, rejected, &rj, esc);
+        if ((side < 0) != (val(ray[2]) - kPi / 2 < 0)) ++*crossings;
+        rejected = rj;
+        *rej += rj ? 1 : 0;
+        ++*step_count;
+        const int klass = sc.terminate(plain_state(w, ray), L, tol, max_steps, *step_count);
+        if (klass) return klass;
+    }
 }
 
 // ----------------------------------------------------------------------------
@@ -1471,7 +1632,7 @@ struct TorusFwd {
         err = sqrt(err / L);
         T hn = 0.9 * h * pow(1.0 / err, 1.0 / 5);
         if (val(fabs(hn)) > val(max_dt)) hn = -max_dt;
-        if (val(err) == 0 || !isfinite(val(hn))) {
+        if (val(err) == 0 || !std::isfinite(val(hn))) {
             const double th_before = val(y[2]);
             keepinbounds(y.data());
             for (int i = 0; i < L; ++i) {
@@ -2017,26 +2178,11 @@ int oracle_render(const rtw_scene* scene, rtw_camera* cam, const double* colors_
             const int i = (int)(p % cg.xp), j = (int)(p / cg.xp);
             std::fill(ray.begin(), ray.end(), 0.0);
             camera_ray(cg, *cam, i, j, ray.data());
-            // integrate_ray, LttM.jl:11-59
-            double dt = -sc.pad_max_dt(ray.data(), max_dt_scale);
-            rhs(sc, w, ray.data(), w.last_slope.data());
-            w.next_slope = w.last_slope;
-            bool rejected = false;
-            long long step_count = 0;
-            long long esc = 0;
-            int klass = 0;
+            long long step_count = 0, esc = 0, rej = 0;
             int crossings = 0;
-            while (true) {
-                bool rj = false;
-                const double side = ray[2] - kPi / 2;
-                dt = dp45_step(sc, w, ray.data(), dt, rejected, &rj, &esc);
-                if ((side < 0) != (ray[2] - kPi / 2 < 0)) ++crossings;
-                rejected = rj;
-                tot_rej += rj ? 1 : 0;
-                ++step_count;
-                klass = sc.terminate(ray.data(), L, tol, max_steps, step_count);
-                if (klass) break;
-            }
+            int klass = integrate_ray(sc, w, ray.data(), max_dt_scale, tol, max_steps, &step_count, &rej, &esc,
+                                      &crossings);
+            tot_rej += rej;
             for (int k = 0; k < 8; ++k)
                 if (!std::isfinite(ray[k])) klass = RTW_CLASS_NAN;
             if (sc.is_wh() || sc.kind == RTW_SCENE_MINKOWSKI_CART_SPHERE) {
@@ -2075,6 +2221,66 @@ int oracle_render(const rtw_scene* scene, rtw_camera* cam, const double* colors_
         counters[1] = tot_rej;
         counters[2] = tot_esc;
     }
+    return RTW_OK;
+}
+
+// Algorithmic work of the reference's form over the given pixels (all when
+// pixel_ids is null): the oracle's own integration of those rays (the same
+// arithmetic, hence the same path and step counts as oracle_render) run over
+// the counting scalar Cnt. The scene's step-size cap, polar-escape and
+// termination tests and the camera set-up are not counted. Thin-disk scenes
+// (Minkowski sphere, Schwarzschild disk, Kerr thin and thick disk) only.
+// out[0] flops, out[1] transcendentals (div/sqrt/exp/log/sin/cos 1, pow 2),
+// out[2] step attempts, out[3] rays.
+int oracle_work(const rtw_scene* scene, rtw_camera* cam, const double* colors_nm, int n_colors,
+                double max_dt_scale, int integrator, const long long* pixel_ids, long long n_ids, long long* out,
+                int n_threads) {
+    if (!scene || !cam || !colors_nm || !out || n_colors <= 0 || n_colors > RTW_MAX_BINS) return RTW_ERR_INVALID_PARAM;
+    if (scene->kind != RTW_SCENE_MINKOWSKI_SPHERE && scene->kind != RTW_SCENE_SCHWARZSCHILD_DISK &&
+        scene->kind != RTW_SCENE_KERR_DISK && scene->kind != RTW_SCENE_KERR_THICK_DISK)
+        return RTW_ERR_UNSUPPORTED;
+    OScene sc(*scene);
+    if (sc.is_singularity(cam->position)) return RTW_ERR_INVALID_CAMERA;
+    CameraGeom cg;
+    camera_geom(sc, *cam, cg);
+    cam->y_pix = cg.yp;
+    const long long P = (long long)cg.xp * cg.yp;
+    const long long n = pixel_ids ? n_ids : P;
+    std::vector<double> freq(n_colors);
+    for (int c = 0; c < n_colors; ++c) freq[c] = 1.0 / colors_nm[c];
+    const int N = n_colors, L = 8 + 2 * N;
+    const double tol = cam->tolerance;
+    const long long max_steps = cam->max_steps;
+    int nt = n_threads > 0 ? n_threads : omp_get_max_threads();
+    const long long chunk = std::max(1LL, (n + 100LL * nt - 1) / (100LL * nt));
+    long long flops = 0, special = 0, attempts = 0, rays = 0;
+#pragma omp parallel num_threads(nt) reduction(+ : flops, special, attempts, rays)
+    {
+        RayWorkT<Cnt> w;
+        w.init(N, freq.data(), tol, max_dt_scale, integrator == RTW_DP45_FSAL);
+        std::vector<double> ray0(L);
+        std::vector<Cnt> ray(L);
+        tally() = OpTally{};
+#pragma omp for schedule(dynamic, chunk)
+        for (long long q = 0; q < n; ++q) {
+            const long long p = pixel_ids ? pixel_ids[q] : q;
+            const int i = (int)(p % cg.xp), j = (int)(p / cg.xp);
+            std::fill(ray0.begin(), ray0.end(), 0.0);
+            camera_ray(cg, *cam, i, j, ray0.data());
+            for (int k = 0; k < L; ++k) ray[k] = Cnt(ray0[k]);
+            long long step_count = 0, esc = 0, rej = 0;
+            int crossings = 0;
+            integrate_ray(sc, w, ray.data(), max_dt_scale, tol, max_steps, &step_count, &rej, &esc, &crossings);
+            attempts += step_count;
+            ++rays;
+        }
+        flops += tally().flops;
+        special += tally().special;
+    }
+    out[0] = flops;
+    out[1] = special;
+    out[2] = attempts;
+    out[3] = rays;
     return RTW_OK;
 }
 
