@@ -785,6 +785,15 @@ __global__ void __launch_bounds__(128, MIXED ? 3 : 2) torus_forward(__grid_const
                 ki1[c] = SR(f[8 + N + c]);
             }
         }
+        // some carried bin slope is nonzero: with no emitting stage point and
+        // every carried slope zero, an attempt leaves every bin exactly as it
+        // is (all its tau / I slopes are 0), so the bins' loop is skipped
+        auto slopes_live = [&]() {
+            bool nz = false;
+            for (int c = 0; c < N; ++c) nz |= kt1[c] != SR(0) || ki1[c] != SR(0);
+            return nz;
+        };
+        bool live = slopes_live();
         double h = -torus_max_dt<EM, SR>(p, x);
         // where h came from: 0 the controller (held fixed by the adjoint),
         // 1 -pad_max_dt of the previous accepted step's start state, 2 -pad_max_dt
@@ -866,6 +875,7 @@ __global__ void __launch_bounds__(128, MIXED ? 3 : 2) torus_forward(__grid_const
                         kt1[q] = SR(f[8 + q]);
                         ki1[q] = SR(f[8 + N + q]);
                     }
+                    live = slopes_live();
                     h = -torus_max_dt<EM, SR>(p, x);
                     hsrc = 2;
                 }
@@ -915,7 +925,9 @@ __global__ void __launch_bounds__(128, MIXED ? 3 : 2) torus_forward(__grid_const
                     c_ki[kTorusMaxBins];
                 const SR hs = SR(h), ts = SR(tol);
                 SR ebins = 0;
-                for (int c = 0; c < N; ++c) {
+                bool run_bins = live, nz = false;
+                for (int s = 1; s < 7; ++s) run_bins |= st.S[s].on;
+                for (int c = 0; c < (run_bins ? N : 0); ++c) {
                     SR kt[7], ki[7];
                     kt[0] = kt1[c];
                     ki[0] = ki1[c];
@@ -935,7 +947,7 @@ __global__ void __launch_bounds__(128, MIXED ? 3 : 2) torus_forward(__grid_const
                                 em_bin<SR, EM>(p.m, st.S[s], c, ft, fi);
                         }
                         kt[s] = ft;
-                        ki[s] = fi * texp(-tp);
+                        ki[s] = fi * (MIXED && EM == 0 ? BinMath<SR>::ex(-tp) : texp(-tp));
                     }
                     // tp is now the new tau (row 6 of A is b)
                     SR nsI = 0, nsT = 0, et = 0, ei = 0;
@@ -958,7 +970,9 @@ __global__ void __launch_bounds__(128, MIXED ? 3 : 2) torus_forward(__grid_const
                     const SR dt_ = hs * et, di = hs * ei;
                     const SR tlt = ts + rmax(rabs(t0), rabs(tp)) * ts;
                     const SR tli = ts + rmax(rabs(i0), rabs(yh)) * ts;
-                    ebins += (dt_ / tlt) * (dt_ / tlt) + (di / tli) * (di / tli);
+                    // (FP32-mixed: the hardware reciprocal, 2 ulp, for the error norm)
+                    const SR qt = MIXED ? dt_ * rinv(tlt) : dt_ / tlt, qi = MIXED ? di * rinv(tli) : di / tli;
+                    ebins += qt * qt + qi * qi;
                     c_t[c] = tp;
                     c_h[c] = yh;
                     c_l[c] = yl;
@@ -966,6 +980,7 @@ __global__ void __launch_bounds__(128, MIXED ? 3 : 2) torus_forward(__grid_const
                     // reference's sum b_i k_i
                     c_kt[c] = p.fsal ? kt[6] : nsT;
                     c_ki[c] = p.fsal ? ki[6] : nsI;
+                    nz |= c_kt[c] != SR(0) || c_ki[c] != SR(0);
                 }
                 err2 += (double)ebins;
                 bool accept;
@@ -979,12 +994,15 @@ __global__ void __launch_bounds__(128, MIXED ? 3 : 2) torus_forward(__grid_const
                         x[i] = y[i];
                         k1[i] = p.fsal ? st.k7[i] : SR(st.ns[i]);
                     }
-                    for (int c = 0; c < N; ++c) {
-                        tau[c] = c_t[c];
-                        ihi[c] = c_h[c];
-                        ilo[c] = c_l[c];
-                        kt1[c] = c_kt[c];
-                        ki1[c] = c_ki[c];
+                    if (run_bins) {
+                        for (int c = 0; c < N; ++c) {
+                            tau[c] = c_t[c];
+                            ihi[c] = c_h[c];
+                            ilo[c] = c_l[c];
+                            kt1[c] = c_kt[c];
+                            ki1[c] = c_ki[c];
+                        }
+                        live = nz;
                     }
                     if (!FLAT && torus_keep(x) && p.fsal) {
                         // reflected through the pole: the carried slope belongs to
@@ -1002,6 +1020,7 @@ __global__ void __launch_bounds__(128, MIXED ? 3 : 2) torus_forward(__grid_const
                             kt1[q] = SR(ff[8 + q]);
                             ki1[q] = SR(ff[8 + N + q]);
                         }
+                        live = slopes_live();
                     }
                     prev_rej = false;
                 } else {
@@ -1450,7 +1469,7 @@ constexpr int kTorusMaxD = 8 + 2 * kTorusMaxBins;  // state components
 // evaluations). The arrays live in local memory,
 // whose layout interleaves the lanes of a warp (same-index accesses coalesce).
 #ifndef RTW_REV_MIN_CTAS
-#define RTW_REV_MIN_CTAS 4  // CTAs per SM the reverse kernel is compiled for (128 registers)
+#define RTW_REV_MIN_CTAS 2  // CTAs per SM the reverse kernel is compiled for (255 registers)
 #endif
 template <bool MIXED>
 __global__ void __launch_bounds__(128, RTW_REV_MIN_CTAS) torus_reverse(__grid_constant__ const TorusRP p) {

@@ -229,6 +229,25 @@ RTW_HD void torus_bin(const T& cj, const T& nus, const T& th, const T& g, const 
     ft = -(j * em1 / (g4 * B(bn.b0)));
 }
 
+// exp and expm1 in the arithmetic of the bins' slopes and partials: FP64, or
+// FP32 with the hardware exponential (the FP32-mixed forward and adjoint)
+template <class T>
+struct BinMath;
+template <>
+struct BinMath<double> {
+    static RTW_HD double ex(double x) { return exp(x); }
+    static RTW_HD double em1(double x) { return expm1(x); }
+};
+template <>
+struct BinMath<float> {
+#ifdef __CUDA_ARCH__
+    static __device__ float ex(float x) { return __expf(x); }
+#else
+    static float ex(float x) { return std::exp(x); }
+#endif
+    static RTW_HD float em1(float x) { return expm1f(x); }
+};
+
 // torus_bin in two parts, for the FP32-mixed forward. Per stage point, the
 // bin-independent factors replace the emitter numbers in place:
 //   (cj, nus, th, g) -> (cj nus, (g / nus)^(1/6), g / th, 1 / g^4),
@@ -262,7 +281,7 @@ RTW_HD void torus_bin_fast(const TorusPt<R>& S, const TorusBin& bn, R& ft, R& fi
     }
     const R x13 = x16 * x16, x12 = x13 * x16;
     const R p = x12 + x16 * R(1.8877486253633868);  // 2^(11/12)
-    const R j = S.cj * p * p * texp(-x13);
+    const R j = S.cj * p * p * BinMath<R>::ex(-x13);
     fi = -(j * R(bn.inv_nu_nm3) * S.g);
     const R y = S.th * R(bn.hk);
     const R em1 = y < R(1e-2) ? y * (R(1) + y * (R(0.5) + y * (R(1.0 / 6.0) + y * (R(1.0 / 24.0) + y * R(1.0 / 120.0)))))
@@ -805,25 +824,6 @@ RTW_HD TorusBinPre torus_bin_pre(double cj, double nus, double th, double g) {
     return q;
 }
 
-// exp and expm1 in the arithmetic of the bins' partials: FP64, or FP32 with
-// the hardware exponential (the FP32-mixed adjoint, whose forward evaluates
-// the same slopes in FP32)
-template <class T>
-struct BinMath;
-template <>
-struct BinMath<double> {
-    static RTW_HD double ex(double x) { return exp(x); }
-    static RTW_HD double em1(double x) { return expm1(x); }
-};
-template <>
-struct BinMath<float> {
-#ifdef __CUDA_ARCH__
-    static __device__ float ex(float x) { return __expf(x); }
-#else
-    static float ex(float x) { return std::exp(x); }
-#endif
-    static RTW_HD float em1(float x) { return expm1f(x); }
-};
 
 // torus_bin_grad from the shared part, in arithmetic T: the bin's slopes
 // (ft, fi) and the two numbers their partials are linear in,
