@@ -1357,7 +1357,11 @@ RTW_HD double torus_dp_vjp(const TorusModel& m, const double* y, const double* K
     // The per-stage arrays of a bin are kept in BT (their values' own
     // precision), so that the loop's live set stays in registers.
     double W0[6] = {0, 0, 0, 0, 0, 0}, WX[6] = {0, 0, 0, 0, 0, 0}, WY[6] = {0, 0, 0, 0, 0, 0};
-    for (int c = 0; c < N; ++c) {
+    // no emitting stage point: every bin's slopes are 0 in this step, so it
+    // adds nothing to any cotangent and leaves the optical depths as they are
+    bool any_on = false;
+    for (int t = 0; t < 6; ++t) any_on |= on[t];
+    for (int c = 0; c < (any_on ? N : 0); ++c) {
         const int it = 8 + c, ii = 8 + N + c;
         BT Kt[6], fi[6], ex[6], DX[6], Dy[6];
         double kt[6];
