@@ -749,6 +749,14 @@ __device__ __noinline__ void torus_rec_end(const TorusKP& p, TorusRec* r, long l
 // and the poles; double on the FP64 path).
 // (FP32-mixed: 3 CTAs/SM, 168 registers, measured 7-13 % faster than 2 CTAs at
 // 255; FP64 stays at 2, where 3 was 8-20 % slower)
+// The FP64 right-hand side at the forward kernel's rare sites (a ray's start,
+// polar escapes, pole reflections), kept out of line so that its per-bin loop
+// stays out of the hot loop's code.
+template <int KEM>
+__device__ __noinline__ void torus_f64_cold(const TorusModel& m, const double* y, double* f) {
+    torus_f64<KEM>(m, y, f);
+}
+
 template <bool MIXED, int EM>
 __global__ void __launch_bounds__(128, MIXED ? 3 : 2) torus_forward(__grid_constant__ const TorusKP p) {
     constexpr bool FLAT = EM == 2 || EM == 4;  // Synchro_Test, the sphere: flat Cartesian geometry
@@ -777,7 +785,7 @@ __global__ void __launch_bounds__(128, MIXED ? 3 : 2) torus_forward(__grid_const
             double y[8 + 2 * kTorusMaxBins], f[8 + 2 * kTorusMaxBins];
             for (int i = 0; i < 8; ++i) y[i] = x[i];
             for (int i = 8; i < D; ++i) y[i] = 0;
-            torus_f64<KEM>(p.m, y, f);
+            torus_f64_cold<KEM>(p.m, y, f);
             for (int i = 0; i < 8; ++i) k1[i] = SR(f[i]);
             for (int c = 0; c < N; ++c) {
                 tau[c] = 0; ihi[c] = 0; ilo[c] = 0;
@@ -850,7 +858,7 @@ __global__ void __launch_bounds__(128, MIXED ? 3 : 2) torus_forward(__grid_const
                 for (int it = 0; it < 37; ++it) {
                     if (it > 0) {
                         if (torus_terminate<double, EM>(p, y, y + 8, N)) continue;
-                        torus_f64<KEM>(p.m, y, f);
+                        torus_f64_cold<KEM>(p.m, y, f);
                     }
                     for (int i = 0; i < D; ++i) y[i] -= temp * f[i];
                     torus_keep(y);
@@ -869,7 +877,7 @@ __global__ void __launch_bounds__(128, MIXED ? 3 : 2) torus_forward(__grid_const
                     done = true;
                     prev_rej = false;
                 } else {
-                    torus_f64<KEM>(p.m, y, f);
+                    torus_f64_cold<KEM>(p.m, y, f);
                     for (int i = 0; i < 8; ++i) k1[i] = SR(f[i]);
                     for (int q = 0; q < N; ++q) {
                         kt1[q] = SR(f[8 + q]);
@@ -1014,7 +1022,7 @@ __global__ void __launch_bounds__(128, MIXED ? 3 : 2) torus_forward(__grid_const
                             yy[8 + q] = (double)tau[q];
                             yy[8 + N + q] = (double)ihi[q] + (MIXED ? (double)ilo[q] : 0.0);
                         }
-                        torus_f64<KEM>(p.m, yy, ff);
+                        torus_f64_cold<KEM>(p.m, yy, ff);
                         for (int i = 0; i < 8; ++i) k1[i] = SR(ff[i]);
                         for (int q = 0; q < N; ++q) {
                             kt1[q] = SR(ff[8 + q]);
@@ -1472,6 +1480,17 @@ constexpr int kTorusMaxD = 8 + 2 * kTorusMaxBins;  // state components
 // before every event (Ys [2][D], Kw [6][D] stage slopes, Ze [4][D] escape
 // evaluations). The arrays live in local memory,
 // whose layout interleaves the lanes of a warp (same-index accesses coalesce).
+// The reverse kernel's path for rays with a polar escape (re-recorded with
+// their full state before every event; rare), kept out of line.
+__device__ __noinline__ bool torus_replay_cold(const TorusModel& m, const double* y_in, uint8_t kind, double hv,
+                                               double* y_out, double* K, double* Y) {
+    return torus_replay(m, y_in, kind, hv, y_out, K, Y);
+}
+__device__ __noinline__ bool torus_escape_vjp_cold(const TorusModel& m, const double* y, int nsub, double temp,
+                                                   double* lam, double* pb, double* W, double* mu, double* tmp) {
+    return torus_escape_vjp(m, y, nsub, temp, lam, pb, W, mu, tmp);
+}
+
 #ifndef RTW_REV_MIN_CTAS
 #define RTW_REV_MIN_CTAS 2  // CTAs per SM the reverse kernel is compiled for (255 registers)
 #endif
@@ -1557,13 +1576,13 @@ __global__ void __launch_bounds__(128, RTW_REV_MIN_CTAS) torus_reverse(__grid_co
                 const uint8_t kind = p.f.ev_kind[eo + e];
                 const double hv = p.f.ev_h[eo + e];
                 if (torus_is_dp(kind)) {
-                    const bool r = torus_replay(m, Ys, kind, hv, Ys + D, Kw, tmp);
+                    const bool r = torus_replay_cold(m, Ys, kind, hv, Ys + D, Kw, tmp);
                     for (int st = 0; st < 6; ++st)
                         for (int i = 0; i < 8; ++i) Kgs[st * 8 + i] = Kw[st * D + i];
                     for (int c = 0; c < N; ++c) taus[c] = Ys[8 + c];
                     dp_step(Ys, Kgs, kind, hv, r, false);
                 } else {
-                    if (!torus_escape_vjp(m, Ys, (int)kind - 1, hv, lam, pb, Ze, mu, tmp)) ++n_cut;
+                    if (!torus_escape_vjp_cold(m, Ys, (int)kind - 1, hv, lam, pb, Ze, mu, tmp)) ++n_cut;
                 }
             }
         }
