@@ -1348,7 +1348,7 @@ RTW_HD double torus_dp_vjp(const TorusModel& m, const double* y, const double* K
                                               D8::var(BT(Yg[t][1]), 0), D8::var(BT(Yg[t][2]), 1),
                                               D8::var(BT(Yg[t][4]), 2), D8::var(BT(Yg[t][7]), 3));
         on[t] = S.on;
-        if (S.on) pre[t] = torus_bin_pre(S.cj.v, S.nus.v, S.th.v, S.g.v);
+        if (S.on) pre[t] = torus_bin_pre_t<BT>(S.cj.v, S.nus.v, S.th.v, S.g.v);
         const D8* comp[4] = {&S.cj, &S.nus, &S.th, &S.g};
         for (int q = 0; q < 4; ++q) {
             Sbar[t][q] = 0;
@@ -1371,7 +1371,7 @@ RTW_HD double torus_dp_vjp(const TorusModel& m, const double* y, const double* K
     for (int t = 0; t < 6; ++t) any_on |= on[t];
     for (int c = 0; c < (any_on ? N : 0); ++c) {
         const int it = 8 + c, ii = 8 + N + c;
-        BT Kt[6], fi[6], ex[6], DX[6], Dy[6];
+        BT Kt[6], fi[6], ex[6], DX[6], Dy[6], av[6];
         double kt[6];
         const double lt = lam[it], li = lam[ii];
         double bkt = 0, bki = 0;
@@ -1386,12 +1386,16 @@ RTW_HD double torus_dp_vjp(const TorusModel& m, const double* y, const double* K
             t0 -= h * bkt;
             tau[c] = t0;
         }
+        // the stage depth offsets sum_s a_ts Kt_s in BT (the FP32-mixed
+        // forward forms its stage depths so), kept for the step-size term below
+        const BT t0b = BT(t0), hb = BT(h);
 #pragma unroll
         for (int t = 0; t < 6; ++t) {
-            double acc = 0;
+            BT acc = 0;
 #pragma unroll
-            for (int s = 0; s < t; ++s) acc += tA(t, s) * (double)Kt[s];
-            ex[t] = on[t] ? BinMath<BT>::ex(BT(-(t0 + h * acc))) : BT(0);
+            for (int s = 0; s < t; ++s) acc += BT(tA(t, s)) * Kt[s];
+            av[t] = acc;
+            ex[t] = on[t] ? BinMath<BT>::ex(-(t0b + hb * acc)) : BT(0);
             bki += tA(6, t) * (double)fi[t] * (double)ex[t];
             kt[t] = h * tA(6, t) * lt;
         }
@@ -1407,13 +1411,9 @@ RTW_HD double torus_dp_vjp(const TorusModel& m, const double* y, const double* K
             WY[t] += U * (double)Dy[t];
             const double mt = -ki * (double)fi[t] * e;  // d (fi exp(-tau)) / d tau
             msum += mt;
-            double ak = 0;
 #pragma unroll
-            for (int s = 0; s < t; ++s) {
-                ak += tA(t, s) * (double)Kt[s];
-                kt[s] += h * tA(t, s) * mt;
-            }
-            hbar += mt * ak;
+            for (int s = 0; s < t; ++s) kt[s] += h * tA(t, s) * mt;
+            hbar += mt * (double)av[t];
         }
         lam[it] = lt + msum;
     }

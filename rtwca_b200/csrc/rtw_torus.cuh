@@ -824,6 +824,32 @@ RTW_HD TorusBinPre torus_bin_pre(double cj, double nus, double th, double g) {
     return q;
 }
 
+// The same in the bins' arithmetic BT: FP64 as above, or FP32 for the
+// FP32-mixed adjoint, whose partials read these factors in FP32 (X^(1/6)'s
+// stage factor then comes out as the forward's torus_bin_stage forms it).
+template <class BT>
+RTW_HD TorusBinPre torus_bin_pre_t(BT cj, BT nus, BT th, BT g) {
+    if constexpr (sizeof(BT) == 8) {
+        return torus_bin_pre(cj, nus, th, g);
+    } else {
+        TorusBinPre q;
+        const BT r = g / nus;
+        q.ok = r > BT(0);
+        const BT L = q.ok ? tlog(r) : BT(0);
+        q.L = L;
+        q.e6 = q.ok ? (double)texp(L * BT(1.0 / 6.0)) : 0.0;
+        q.gt = g / th;
+        q.cjnus = cj * nus;
+        const BT g2 = g * g;
+        q.ig4 = BT(1) / (g2 * g2);
+        q.icj = BT(1) / cj;
+        q.inus = BT(1) / nus;
+        q.ig = BT(1) / g;
+        q.ith = BT(1) / th;
+        return q;
+    }
+}
+
 
 // torus_bin_grad from the shared part, in arithmetic T: the bin's slopes
 // (ft, fi) and the two numbers their partials are linear in,
