@@ -282,11 +282,11 @@ def op_model(renderer, scene_kind, stats, n_bins):
     return flops, mufu, oc
 
 
-# DRAM bytes per step attempt of the FP32-mixed Kerr trace kernel (local-memory
-# write-back; the outputs are 17 B per ray), from one ncu capture at 512^2: the
-# main launch's dram__bytes_read+write (0.0516 + 0.7491 GB) over the render's
-# step attempts (the tail launch, 9 % of that render's time, returned no counters)
-TRAFFIC_B_PER_ATTEMPT = 0.8007e9 / 357227612
+# DRAM bytes per step attempt of the FP32-mixed Kerr trace kernel, from one ncu
+# capture at 512^2: the main launch's dram__bytes_read+write (23.4 + 1.1 MB; the
+# outputs, 17 B per ray, are still in L2 when the launch ends) over the render's
+# step attempts (the tail launch, 10 % of that render's time, returned no counters)
+TRAFFIC_B_PER_ATTEMPT = 24.49e6 / 357227515
 
 
 def batched_leg(r, world, rank, stream, barrier_fn):
