@@ -1325,6 +1325,15 @@ RTW_HD void torus_accel_vjp(const TorusModel& m, const double* Yt, const double*
     pb[0] += (double)ba;
 }
 
+#ifdef __CUDA_ARCH__
+// the FP64 Jacobian of the FP32-mixed sweep (near the horizon and the poles;
+// rare), out of line
+__device__ __noinline__ void torus_accel_vjp_f64_cold(const TorusModel& m, const double* Yt, const double* cw4,
+                                                      double* mu, double* pb) {
+    torus_accel_vjp<double>(m, Yt, cw4, mu, pb);
+}
+#endif
+
 template <class BT>
 RTW_HD double torus_dp_vjp(const TorusModel& m, const double* y, const double* Kg, double* tau, bool tau_at_end,
                            double h, double* lam, double* pb, bool geo64 = true) {
@@ -1440,6 +1449,10 @@ RTW_HD double torus_dp_vjp(const TorusModel& m, const double* y, const double* K
         // stages (away from the horizon and the poles), FP64 elsewhere
         if (sizeof(BT) == 4 && !geo64)
             torus_accel_vjp<float>(m, Yg[t], kg[t] + 4, mu, pb);
+#ifdef __CUDA_ARCH__
+        else if (sizeof(BT) == 4)
+            torus_accel_vjp_f64_cold(m, Yg[t], kg[t] + 4, mu, pb);
+#endif
         else
             torus_accel_vjp<double>(m, Yg[t], kg[t] + 4, mu, pb);
         if (on[t]) {
