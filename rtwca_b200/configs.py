@@ -149,7 +149,7 @@ def batched_frames(n_frames: int = 96, seed: int = 0, sizes=(256, 512, 1024), to
 
 # ---------------------------------------------------------------------------
 # Differentiable synchrotron torus (Kerr a = 0.94, inclination 17 deg, 512^2,
-# 32 bins over 230 GHz +- 20 %). BASELINE-level parameters; the camera
+# 32 bins over 230 GHz +- 20 %), the differentiable-render workload; the camera
 # distance, field of view and torus extent are choices of this library.
 # ---------------------------------------------------------------------------
 TORUS_DEFAULTS = {"spin": 0.94, "inclination_deg": 17.0, "n_e0": 1e5, "b_0": 10.0, "theta_e0": 10.0}

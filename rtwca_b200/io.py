@@ -4,7 +4,7 @@ LttM.jl:176) as a cube [y_pix, x_pix, n_bins], written as NPY (with a JSON
 sidecar) or as a FITS primary image. The reference returns only the colour
 image after the xyY / RGB conversion (gen_image, LttM.jl:182-208); raw
 spectral output ("something like FITS files") is one of its planned
-features (README.md:21).
+features (the reference's README.md:21).
 """
 from __future__ import annotations
 
