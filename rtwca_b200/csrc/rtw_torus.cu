@@ -757,8 +757,17 @@ __device__ __noinline__ void torus_f64_cold(const TorusModel& m, const double* y
     torus_f64<KEM>(m, y, f);
 }
 
+// CTAs per SM the FP32-mixed per-bin forward is compiled for, per emitter
+// (measured at 512^2 / 1024 x 645): the thermal tori (synchrotron, brems) at 4
+// (128 registers: 478 against 500 ms, 0.501 against 0.489 Mrays/s), the others
+// at 3 (168 registers: Powehi 4.56 against 4.32, the wormhole 3.48 against
+// 3.11 Mrays/s at 4)
+#ifndef RTW_FWD_MIN_CTAS
+#define RTW_FWD_MIN_CTAS 4
+#endif
 template <bool MIXED, int EM>
-__global__ void __launch_bounds__(128, MIXED ? 3 : 2) torus_forward(__grid_constant__ const TorusKP p) {
+__global__ void __launch_bounds__(128, MIXED ? ((EM == 0 || EM == 5) ? RTW_FWD_MIN_CTAS : 3) : 2)
+    torus_forward(__grid_constant__ const TorusKP p) {
     constexpr bool FLAT = EM == 2 || EM == 4;  // Synchro_Test, the sphere: flat Cartesian geometry
     // the FP64 slope at a ray's start and after escapes: the instance's own
     // emitter on the mixed path (ptxas: the torus, Powehi and wormhole
