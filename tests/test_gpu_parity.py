@@ -38,6 +38,7 @@ def test_fp64_parity(renderer, oracle, name):
     scene, cam, _ = configs.workload(name, x_pix=SMALL[name])
     colors = configs.log_spaced_colors(16)
     g = _gpu(renderer, scene, cam, colors, precision=abi.PREC_FP64)
+    assert renderer.stats()["launches"] == 1  # no tail pass in FP64
     r = _ref(oracle, scene, cam, colors)
     s = summarize(g, r)
     print(name, s)
@@ -207,6 +208,7 @@ def test_plain_fp64_parity(renderer, oracle, name):
     scene, cam, _ = configs.workload(name, x_pix=SMALL[name])
     colors = configs.log_spaced_colors(16)
     g = _gpu(renderer, scene, cam, colors, precision=abi.PREC_FP64_PLAIN)
+    assert renderer.stats()["launches"] == 1
     r = _ref(oracle, scene, cam, colors)
     s = summarize(g, r)
     print(name, s)

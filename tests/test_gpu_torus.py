@@ -42,6 +42,7 @@ def test_torus_fp64_parity(renderer, oracle):
     assert np.all(g["xyz"] == 0)  # the CIE functions vanish at 1.3 mm
     st = renderer.stats()
     assert st["rays"] == 256 and st["step_attempts"] > 0
+    assert st["launches"] == 1 and st["tail_rays"] == 0  # the per-bin kernel: one launch, no tail pass
 
 
 def test_torus_mixed_parity(renderer, oracle):
