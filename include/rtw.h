@@ -230,7 +230,8 @@ typedef struct rtw_render_params {
     double promote_dr;          /* MIXED: FP64 stages while r - r_horizon < promote_dr M
                                    (0: default 1e-3; < 0: never) */
     double promote_sin;         /* MIXED: FP64 stages while sin(theta) < promote_sin
-                                   (0: default 1e-2; < 0: never) */
+                                   (0: default 2e-3 in the trace kernel, 1e-2 in
+                                   the per-bin kernels (Powehi 0.1); < 0: never) */
     int32_t block_warps;        /* warps per CTA, 1..4 (0: default 4) */
     int32_t ctas_per_sm;        /* resident CTAs per SM (0: default) */
     void* stream;               /* cudaStream_t to run on; NULL: the context's

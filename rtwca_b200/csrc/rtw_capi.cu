@@ -746,7 +746,10 @@ rtw_status rtw_render(rtw_ctx* ctx, const rtw_scene* scene, const rtw_camera* ca
     // terms that cancel to O(1) and FP32 stages lose every digit before the
     // (1 + 10 tol) r+ stop. Poles: sin(theta) < 1e-2.
     const double pdr = prm->promote_dr < 0 ? -1.0 : (prm->promote_dr > 0 ? prm->promote_dr : 1e-3);
-    const double psn = prm->promote_sin < 0 ? 0.0 : (prm->promote_sin > 0 ? std::min(prm->promote_sin, 1.0) : 1e-2);
+    // pole promotion of the trace kernel: default sin(theta) < 2e-3 (1e-2 measured
+    // 4 % slower on the Kerr disk, with the same parity: near-axis FP64 attempts
+    // hold their whole warp)
+    const double psn = prm->promote_sin < 0 ? 0.0 : (prm->promote_sin > 0 ? std::min(prm->promote_sin, 1.0) : 2e-3);
     p.promote_dr = pdr * scene->mass;
     p.promote_theta = std::asin(psn);
     p.fsal = prm->integrator == RTW_DP45_FSAL;

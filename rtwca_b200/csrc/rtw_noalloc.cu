@@ -211,7 +211,7 @@ extern "C" rtw_status rtw_render_noalloc(const rtw_scene* scene, const rtw_camer
     p.total_rays = total;
     p.max_dt_scale = prm->max_dt_scale;
     const double pdr = prm->promote_dr < 0 ? -1.0 : (prm->promote_dr > 0 ? prm->promote_dr : 1e-3);
-    const double psn = prm->promote_sin < 0 ? 0.0 : (prm->promote_sin > 0 ? (prm->promote_sin < 1 ? prm->promote_sin : 1.0) : 1e-2);
+    const double psn = prm->promote_sin < 0 ? 0.0 : (prm->promote_sin > 0 ? (prm->promote_sin < 1 ? prm->promote_sin : 1.0) : 2e-3);
     p.promote_dr = pdr * scene->mass;
     p.promote_theta = std::asin(psn);
     p.fsal = prm->integrator == RTW_DP45_FSAL;
