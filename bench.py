@@ -283,10 +283,10 @@ def op_model(renderer, scene_kind, stats, n_bins):
 
 
 # DRAM bytes per step attempt of the FP32-mixed Kerr trace kernel, from one ncu
-# capture at 512^2: the main launch's dram__bytes_read+write (23.4 + 1.1 MB; the
+# capture at 512^2: the main launch's dram__bytes_read+write (22.1 + 1.1 MB; the
 # outputs, 17 B per ray, are still in L2 when the launch ends) over the render's
 # step attempts (the tail launch, 10 % of that render's time, returned no counters)
-TRAFFIC_B_PER_ATTEMPT = 24.49e6 / 357227515
+TRAFFIC_B_PER_ATTEMPT = 23.20e6 / 357227232
 
 
 def batched_leg(r, world, rank, stream, barrier_fn):
